@@ -1,0 +1,284 @@
+"""Synthetic, seeded initial states for the VVM step.
+
+Every array uses the reference model's host layout: 2D fields are
+``[nx][nz]`` float64 with k (height) the fast index, ghost cells included
+(``nx = NX + 2``, ``nz = NZ + 2``; src/Declare.hpp:33,82-83).
+
+The 1D base state is built with the reference's own discrete formulas
+(src/Init.cpp:14-135): hydrostatic Exner function from the surface pressure,
+anelastic densities at cell centres (``rhou``) and faces (``rhow``), the
+``(k-1/2) dz`` level heights and the mixing-length profile ``lambda2``.
+Only the input profiles differ from the reference's analytic sounding: the
+warm-bubble case uses theta = 300 K + 3 K/km and qv at a fixed relative
+humidity of the model's Tetens saturation mixing ratio (src/Init.cpp:88),
+solved together with the pressure by fixed-point iteration.
+
+The 2D state follows src/Init.cpp:186-255: theta = base + bubble, qv = base
+profile everywhere, qc = qr = 0, zeta diagnosed from (u, w), ubarTop = the
+mean of u on the top interior row.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+GRAVITY = 9.80665
+CP = 1003.5
+CV = 716.5
+RD = 287.0
+LV = 2.5e6
+P0 = 1e5
+PSURF = 96500.0
+
+
+@dataclass
+class GridSpec:
+    """Interior sizes and spacings of one case (reference vvm_config.txt keys)."""
+    NX: int
+    NZ: int
+    dx: float
+    dz: float
+    dt: float
+    case: int = 1
+    moisture_nudge_time: float = 0.0
+
+    @property
+    def nx(self) -> int:
+        return self.NX + 2
+
+    @property
+    def nz(self) -> int:
+        return self.NZ + 2
+
+
+@dataclass
+class VVMState:
+    """Complete model state in the reference's host layout."""
+    grid: GridSpec
+    fields: dict = field(default_factory=dict)    # name -> (nx, nz)
+    hist: dict = field(default_factory=dict)      # name -> (nx, nz, 2)
+    prof: dict = field(default_factory=dict)      # name -> (nz,)
+    scalars: dict = field(default_factory=dict)   # ubarTop, ubarTopp, dubarTop_advect, step
+    precip: np.ndarray | None = None
+
+    def copy(self) -> "VVMState":
+        return VVMState(self.grid,
+                        {k: v.copy() for k, v in self.fields.items()},
+                        {k: v.copy() for k, v in self.hist.items()},
+                        {k: v.copy() for k, v in self.prof.items()},
+                        {k: (v.copy() if isinstance(v, np.ndarray) else v)
+                         for k, v in self.scalars.items()},
+                        None if self.precip is None else self.precip.copy())
+
+
+FIELDS_2D = ("zeta", "zetap", "th", "thp", "qv", "qvp", "qc", "qcp", "qr", "qrp",
+             "u", "w", "RKM", "RKH")
+HIST = ("dzeta_advect", "dth_buoyancy", "dth_advect", "dqv_advect", "dqc_advect",
+        "dqr_advect", "dqr_VT")
+PROFILES = ("rhou", "rhow", "thb", "thvb", "qvb", "pib", "pb", "thb_init", "qvb0",
+            "z", "z_zeta", "lambda2")
+
+
+def _center1d(a: np.ndarray) -> None:
+    # src/Boundary.cpp:3-7
+    a[0] = a[1]
+    a[-1] = a[-2]
+
+
+def _center2d(a: np.ndarray) -> None:
+    # src/Boundary.cpp:9-19: periodic x on interior rows, then zero gradient in z
+    a[0, 1:-1] = a[-2, 1:-1]
+    a[-1, 1:-1] = a[1, 1:-1]
+    a[:, 0] = a[:, 1]
+    a[:, -1] = a[:, -2]
+
+
+def _westdown2d(a: np.ndarray) -> None:
+    # src/Boundary.cpp:21-30: periodic x, zero on rows 0, 1 and nz-1
+    a[0, 1:-1] = a[-2, 1:-1]
+    a[-1, 1:-1] = a[1, 1:-1]
+    a[:, 0] = 0.0
+    a[:, 1] = 0.0
+    a[:, -1] = 0.0
+
+
+def tetens_qvs(T: np.ndarray, p: np.ndarray) -> np.ndarray:
+    """Saturation mixing ratio of the model (src/Init.cpp:88, MicroPhysics.cpp:12)."""
+    return (380.0 / p) * np.exp(17.27 * (T - 273.0) / (T - 36.0))
+
+
+def base_state(g: GridSpec, theta_of_z, rh: float | np.ndarray, qv_of_z=None) -> dict:
+    """1D base state on the reference's staggering (src/Init.cpp:14-135).
+
+    ``theta_of_z(z)`` gives the base potential temperature at cell-centre
+    heights ``z = (k - 1/2) dz``. Moisture is either ``rh`` times the Tetens
+    saturation value (solved jointly with the hydrostatic pressure) or, when
+    ``qv_of_z`` is given, that profile directly.
+    """
+    nz, dz = g.nz, g.dz
+    k = np.arange(nz)
+    zc = (k - 0.5) * dz
+    thb = np.zeros(nz)
+    thb[1:nz - 1] = theta_of_z(zc[1:nz - 1])
+    _center1d(thb)
+    rh_arr = np.broadcast_to(np.asarray(rh, dtype=np.float64), (nz,)) if qv_of_z is None else None
+
+    qvb = np.zeros(nz)
+    if qv_of_z is not None:
+        qvb[1:nz - 1] = qv_of_z(zc[1:nz - 1])
+        _center1d(qvb)
+
+    pisfc = (PSURF / P0) ** (RD / CP)
+
+    def hydrostatic(q):
+        thvb = thb * (1.0 + 0.61 * q)                         # src/Init.cpp:38
+        _center1d(thvb)
+        pib = np.zeros(nz)
+        for kk in range(1, nz - 1):                           # src/Init.cpp:46-52
+            if kk == 1:
+                pib[kk] = pisfc - GRAVITY * 0.5 * dz / (CP * thvb[kk])
+            else:
+                tvbavg = 0.5 * (thvb[kk] + thvb[kk - 1])
+                pib[kk] = pib[kk - 1] - GRAVITY * dz / (CP * tvbavg)
+        _center1d(pib)
+        if np.any(pib[1:nz - 1] <= 0.0):
+            raise ValueError("base state: the Exner function reaches zero below the model "
+                             "top; lower NZ*dz or the lapse rate")
+        return thvb, pib
+
+    if qv_of_z is None:
+        for _ in range(100):
+            thvb, pib = hydrostatic(qvb)
+            pb = P0 * pib ** (CP / RD)                        # src/Init.cpp:86
+            qnew = np.zeros(nz)
+            qnew[1:nz - 1] = rh_arr[1:nz - 1] * tetens_qvs(thb[1:nz - 1] * pib[1:nz - 1],
+                                                            pb[1:nz - 1])
+            _center1d(qnew)
+            done = np.array_equal(qnew, qvb)
+            qvb = qnew
+            if done:
+                break
+    thvb, pib = hydrostatic(qvb)
+
+    rhou = np.zeros(nz)
+    rhou[1:nz - 1] = P0 * pib[1:nz - 1] ** (CV / RD) / (RD * thvb[1:nz - 1])   # src/Init.cpp:68
+    _center1d(rhou)
+    rhow = np.zeros(nz)
+    for kk in range(2, nz):                                   # src/Init.cpp:74-82
+        rhow[kk] = 0.5 * (rhou[kk] + rhou[kk - 1])
+    rhow[1] = rhow[2] - (rhow[3] - rhow[2])
+    rhow[0] = rhow[1]
+    rhou[0] = rhow[0]
+
+    pb = np.zeros(nz)
+    pb[1:nz - 1] = P0 * pib[1:nz - 1] ** (CP / RD)
+    _center1d(pb)
+
+    thb_init = thb.copy()
+    qvb0 = qvb.copy()
+    thvb_step1 = thb + 0.61 * qvb                             # src/Init.cpp:119 (additive)
+
+    z = np.zeros(nz)
+    z_zeta = np.zeros(nz)
+    lambda2 = np.zeros(nz)
+    for kk in range(1, nz - 1):                               # src/Init.cpp:125-129
+        z[kk] = (kk - 0.5) * dz
+        z_zeta[kk] = (kk - 1) * dz
+        lambda2[kk] = 1.0 / (1.0 / math.pow(0.23 * math.sqrt(g.dx * dz), 2)
+                             + 1.0 / math.pow(0.4 * 0.4 * z[kk], 2))
+    z[0], z[-1] = z[1], z[-2]
+    z_zeta[0], z_zeta[-1] = z_zeta[1], z_zeta[-2]
+    return dict(thb=thb, thvb=thvb_step1, qvb=qvb, pib=pib, pb=pb, rhou=rhou, rhow=rhow,
+                thb_init=thb_init, qvb0=qvb0, z=z, z_zeta=z_zeta, lambda2=lambda2)
+
+
+def _assemble(g: GridSpec, prof: dict, th: np.ndarray, u: np.ndarray,
+              w: np.ndarray | None = None, qv: np.ndarray | None = None) -> VVMState:
+    nx, nz = g.nx, g.nz
+    st = VVMState(g)
+    f = st.fields
+    for name in FIELDS_2D:
+        f[name] = np.zeros((nx, nz))
+    f["th"][:] = th
+    _center2d(f["th"])
+    f["qv"][:] = prof["qvb"][None, :] if qv is None else qv
+    if qv is not None:
+        _center2d(f["qv"])
+    f["u"][:] = u
+    _center2d(f["u"])
+    if w is not None:
+        f["w"][:] = w
+        _westdown2d(f["w"])
+    # zeta from (u, w): src/Init.cpp:231-241
+    uu, ww, rhow = f["u"], f["w"], prof["rhow"]
+    zeta = f["zeta"]
+    pw_px = (ww[1:nx - 1, 1:nz - 1] - ww[0:nx - 2, 1:nz - 1]) * (1.0 / g.dx)
+    pu_pz = (uu[1:nx - 1, 1:nz - 1] - uu[1:nx - 1, 0:nz - 2]) * (1.0 / g.dz)
+    zeta[1:nx - 1, 1:nz - 1] = (pw_px - pu_pz) / rhow[None, 1:nz - 1]
+    _westdown2d(zeta)
+    # ubarTop: src/Init.cpp:244-248 (sequential sum, as the reference does)
+    s = 0.0
+    for i in range(1, nx - 1):
+        s += uu[i, nz - 2]
+    ubar = s / float(nx - 2)
+    for name in HIST:
+        st.hist[name] = np.zeros((nx, nz, 2))
+    st.prof = {k: np.array(v, dtype=np.float64) for k, v in prof.items()}
+    st.scalars = dict(ubarTop=ubar, ubarTopp=0.0, dubarTop_advect=np.zeros(2), step=0)
+    st.precip = np.zeros(nx)
+    return st
+
+
+def warm_bubble(NX: int = 128, NZ: int = 64, dx: float = 200.0, dz: float = 200.0,
+                dt: float = 1.0, amp: float = 2.0, radius: float = 2000.0,
+                xc_frac: float = 0.5, zc: float = 2000.0, dthdz: float = 3e-3,
+                rh: float = 0.8, case: int = 1) -> VVMState:
+    """Plain VVM warm bubble: theta = 300 K + dthdz*z, qv at ``rh`` of saturation,
+    a cosine bubble of amplitude ``amp`` and radius ``radius`` centred at
+    (``xc_frac`` of the domain, ``zc``), u = w = 0."""
+    g = GridSpec(NX, NZ, dx, dz, dt, case)
+    prof = base_state(g, lambda z: 300.0 + dthdz * z, rh)
+    nx, nz = g.nx, g.nz
+    i = np.arange(nx)[:, None]
+    k = np.arange(nz)[None, :]
+    x = (i - 0.5) * dx
+    z = (k - 0.5) * dz
+    r = np.sqrt(((x - xc_frac * NX * dx) / radius) ** 2 + ((z - zc) / radius) ** 2)
+    bubble = np.where(r <= 1.0, 0.5 * amp * (np.cos(np.pi * r) + 1.0), 0.0)
+    th = np.zeros((nx, nz))
+    th[1:nx - 1, 1:nz - 1] = prof["thb"][None, 1:nz - 1] + bubble[1:nx - 1, 1:nz - 1]
+    return _assemble(g, prof, th, np.zeros((nx, nz)))
+
+
+def random_state(NX: int = 32, NZ: int = 16, dx: float = 200.0, dz: float = 200.0,
+                 dt: float = 1.0, seed: int = 0, step_parity_hist: bool = True) -> VVMState:
+    """A warm-bubble base state with seeded random perturbations in every
+    prognostic field, nonzero u/w/RKM and AB2 history: exercises every branch
+    of the per-routine kernels (signs of u and w, negative water, Ri ranges)."""
+    rng = np.random.default_rng(seed)
+    st = warm_bubble(NX, NZ, dx, dz, dt, amp=2.0, radius=0.25 * NX * dx)
+    g = st.grid
+    nx, nz = g.nx, g.nz
+    f = st.fields
+    f["th"][1:-1, 1:-1] += rng.normal(0.0, 0.5, (nx - 2, nz - 2))
+    f["qv"][1:-1, 1:-1] *= 1.0 + rng.normal(0.0, 0.1, (nx - 2, nz - 2))
+    f["qc"][1:-1, 1:-1] = np.maximum(rng.normal(5e-4, 8e-4, (nx - 2, nz - 2)), -1e-5)
+    # qr stays >= 0: the fall speed takes qr**0.1346 (src/Advection.cpp:165)
+    f["qr"][1:-1, 1:-1] = np.maximum(rng.normal(3e-4, 5e-4, (nx - 2, nz - 2)), 0.0)
+    f["u"][1:-1, 1:-1] = rng.normal(0.0, 3.0, (nx - 2, nz - 2))
+    f["w"][1:-1, 2:-1] = rng.normal(0.0, 2.0, (nx - 2, nz - 3))
+    f["zeta"][1:-1, 2:-1] = rng.normal(0.0, 0.02, (nx - 2, nz - 3))
+    f["RKM"][1:-1, 1:-1] = rng.uniform(10.0, 400.0, (nx - 2, nz - 2))
+    f["RKH"][1:-1, 1:-1] = rng.uniform(10.0, 400.0, (nx - 2, nz - 2))
+    for name in ("th", "qv", "qc", "qr", "u", "RKM", "RKH"):
+        _center2d(f[name])
+    _westdown2d(f["w"])
+    _westdown2d(f["zeta"])
+    for name in HIST:
+        st.hist[name][1:-1, 1:-1, :] = rng.normal(0.0, 1e-4, (nx - 2, nz - 2, 2))
+    st.scalars["ubarTop"] = float(rng.normal(0.0, 1.0))
+    st.scalars["dubarTop_advect"] = rng.normal(0.0, 1e-3, 2)
+    st.scalars["step"] = 3
+    return st
