@@ -1,0 +1,880 @@
+// Physics kernels of the VVM step (everything except the elliptic solves).
+//
+// T is the storage and stencil arithmetic type: double for the plain FP64
+// step, float for the mixed-precision step. Profiles stay double and are
+// rounded to T on load. Domain-wide sums always accumulate in double.
+//
+// Each kernel restates one or more reference routines and keeps their index
+// ranges, boundary treatment and expression order; the file:line citations
+// name the reference code. Halo fills are fused into the producing kernel
+// (store_center / store_westdown write every ghost image of a cell).
+#pragma once
+
+#include "vvm_common.cuh"
+
+namespace vvm {
+
+// Per-level coefficient profiles precomputed on the host (double, [nz]),
+// each formed with the reference's own expression.
+struct Profiles {
+    const double *rhou, *rhow, *thvb, *thb_init, *qvb0, *pib, *pb, *lambda2;
+    const double *vt_c1;      // (1E-3*rhow[k])*0.5            Advection.cpp:165
+    const double *vt_fac;     // pow(rhow[k]/rhow[1], -0.5)    Advection.cpp:165
+    const double *pc;         // 380/(pow(pib,Cp/Rd)*P0)       MicroPhysics.cpp:10,82
+    const double *dtcgr_th;   // dt*CGR of Nudge_theta (0 below k_start)
+    const double *dtcgr_zeta; // dt*CGR of Nudge_zeta (0 below k_start or case 2)
+    const double *q1ls, *q2ls;  // large-scale forcing profiles (may be all zero)
+    double pf1, pf2;          // 1E-3*rhou[1], pow(rhou[1]/rhow[1], -0.5)  Iteration.cpp:115
+};
+
+// AB2 bookkeeping shared by every prognostic tendency
+// (e.g. Advection.cpp:69-71): slot (step+1)%2 receives the new tendency,
+// slot step%2 holds the previous one, and on step 0 both become the new one.
+struct AB2 {
+    int sn, so, first;
+    __host__ __device__ static AB2 of(int step) { return AB2{(step + 1) & 1, step & 1, step == 0}; }
+};
+
+template <typename T>
+__device__ __forceinline__ T ab2_push(T* hn, T* ho, size_t idx, T tend, const AB2& s) {
+    T old = s.first ? tend : ho[idx];
+    hn[idx] = tend;
+    if (s.first) ho[idx] = tend;
+    return old;
+}
+
+// ---------------------------------------------------------------------------
+// Vorticity advection + buoyancy + westdown halo of zetap
+// (Iteration::pzeta_pt: Advection.cpp:84-149, Buoyancy.cpp:11-58,
+// Boundary.cpp:21-30). One thread per interior zeta point (i, k),
+// i = 1..nx-2, k = 2..nz-2.
+
+template <typename T>
+struct PZetaArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    const T *zeta, *u, *w, *th, *qv, *qc, *qr;
+    T* zetap;
+    T *hz_n, *hz_o, *hb_n, *hb_o;  // dzeta_advect, dth_buoyancy slots
+    AB2 ab;
+};
+
+// Staggered mass fluxes of Advection_zeta (Advection.cpp:90-91), interior only.
+template <typename T>
+__device__ __forceinline__ T zeta_Uw(const PZetaArgs<T>& a, int i, int k) {
+    const Dims& d = a.d;
+    return T(0.25) * (T(a.p.rhou[k]) * (a.u[d.at(i + 1, k)] + a.u[d.at(i, k)]) +
+                      T(a.p.rhou[k - 1]) * (a.u[d.at(i + 1, k - 1)] + a.u[d.at(i, k - 1)]));
+}
+template <typename T>
+__device__ __forceinline__ T zeta_Wu(const PZetaArgs<T>& a, int i, int k) {
+    const Dims& d = a.d;
+    return T(0.25) * (T(a.p.rhow[k + 1]) * (a.w[d.at(i, k + 1)] + a.w[d.at(i - 1, k + 1)]) +
+                      T(a.p.rhow[k]) * (a.w[d.at(i, k)] + a.w[d.at(i - 1, k)]));
+}
+
+// x flux at face (i+1/2, k) for i = 1..nx-2 (Advection.cpp:107,111-114).
+template <typename T>
+__device__ __forceinline__ T zeta_flux_u(const PZetaArgs<T>& a, int i, int k) {
+    const Dims& d = a.d;
+    const T* z = a.zeta;
+    T U = zeta_Uw(a, i, k);
+    T f = U * (z[d.at(i + 1, k)] + z[d.at(i, k)]);
+    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
+        T Um = zeta_Uw(a, i - 1, k), Up = zeta_Uw(a, i + 1, k);
+        T z0 = z[d.at(i - 1, k)], z1 = z[d.at(i, k)], z2 = z[d.at(i + 1, k)], z3 = z[d.at(i + 2, k)];
+        f += T(-1. / 3.) * (plus_part(U) * (z2 - z1) - sqrt(plus_part(U) * plus_part(Um)) * (z1 - z0) -
+                            minus_part(U) * (z2 - z1) - sqrt(fabs(minus_part(U) * minus_part(Up))) * (z3 - z2));
+    }
+    return f;
+}
+
+// z flux at face (i, k+1/2) for k = 1..nz-2 (Advection.cpp:108,115-118).
+template <typename T>
+__device__ __forceinline__ T zeta_flux_w(const PZetaArgs<T>& a, int i, int k) {
+    const Dims& d = a.d;
+    const T* z = a.zeta;
+    T W = zeta_Wu(a, i, k);
+    T f = W * (z[d.at(i, k + 1)] + z[d.at(i, k)]);
+    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
+        T Wm = zeta_Wu(a, i, k - 1), Wp = zeta_Wu(a, i, k + 1);
+        T z0 = z[d.at(i, k - 1)], z1 = z[d.at(i, k)], z2 = z[d.at(i, k + 1)], z3 = z[d.at(i, k + 2)];
+        f += T(-1. / 3.) * (plus_part(W) * (z2 - z1) - sqrt(plus_part(W) * plus_part(Wm)) * (z1 - z0) -
+                            minus_part(W) * (z2 - z1) - sqrt(fabs(minus_part(W) * minus_part(Wp))) * (z3 - z2));
+    }
+    return f;
+}
+
+template <typename T>
+__device__ __forceinline__ T thv_at(const PZetaArgs<T>& a, int i, int k) {  // Buoyancy.cpp:3-9
+    size_t id = a.d.at(i, k);
+    return a.th[id] * (T(1) + T(0.608) * a.qv[id]);
+}
+
+template <typename T>
+__global__ void k_pzeta(PZetaArgs<T> a) {
+    const Dims& d = a.d;
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > d.nx - 2 || k > d.nz - 2) return;
+    const size_t id = d.at(i, k);
+    const T dt15 = T(1.5 * a.c.dt), dt05 = T(0.5 * a.c.dt);
+    // Advection_zeta: flux differences; flux_u at i-1 = 0 is the halo copy of
+    // flux_u at nx-2 (BoundaryProcess2D_center on flux_u, Advection.cpp:123).
+    T fu_i = zeta_flux_u(a, i, k);
+    T fu_m = zeta_flux_u(a, (i == 1) ? d.nx - 2 : i - 1, k);
+    T fw_k = zeta_flux_w(a, i, k);
+    T fw_m = zeta_flux_w(a, i, k - 1);
+    T rw = T(a.p.rhow[k]);
+    T px = (fu_i - fu_m) * T(a.c.r2dx) / rw;
+    T pz = (fw_k - fw_m) * T(a.c.r2dz) / rw;
+    T tz = -px - pz;
+    T oz = ab2_push(a.hz_n, a.hz_o, id, tz, a.ab);
+    T zp = a.zeta[id] + dt15 * tz - dt05 * oz;
+    // Bouyancy (Buoyancy.cpp:25-48)
+    T g_rw = T(a.c.gravity) / rw;
+    T b = g_rw * T(0.5) *
+          ((thv_at(a, i, k) - thv_at(a, i - 1, k)) / T(a.p.thvb[k]) +
+           (thv_at(a, i, k - 1) - thv_at(a, i - 1, k - 1)) / T(a.p.thvb[k - 1])) * T(a.c.rdx);
+    T bc = g_rw * (T(0.5) * (a.qc[id] + a.qc[d.at(i, k - 1)]) -
+                   T(0.5) * (a.qc[d.at(i - 1, k)] + a.qc[d.at(i - 1, k - 1)])) * T(a.c.rdx);
+    T br = g_rw * (T(0.5) * (a.qr[id] + a.qr[d.at(i, k - 1)]) -
+                   T(0.5) * (a.qr[d.at(i - 1, k)] + a.qr[d.at(i - 1, k - 1)])) * T(a.c.rdx);
+    T tb = b + (-bc - br);
+    T ob = ab2_push(a.hb_n, a.hb_o, id, tb, a.ab);
+    zp += (dt15 * tb) - (dt05 * ob);
+    store_westdown(a.zetap, d, i, k, zp);
+}
+
+// ---------------------------------------------------------------------------
+// Scalar advection (Advection_thermo, Advection.cpp:25-81) of th, qv, qc, qr,
+// rain sedimentation (Advection_qrVT, Advection.cpp:153-192), the surface
+// precipitation diagnostic (Iteration.cpp:114-119) and the per-block partial
+// sums of NegativeValueProcess (MicroPhysics.cpp:116-138). Writes the raw
+// interior future values; k_apply finishes them. One thread per interior
+// cell (i = 1..nx-2, k = 1..nz-2).
+
+enum : int { F_TH = 1, F_QV = 2, F_QC = 4, F_QR = 8 };
+
+template <typename T>
+struct PAdvArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    const T *u, *w;
+    const T* now[4];   // th, qv, qc, qr
+    T* fut[4];         // thp, qvp, qcp, qrp
+    T* hn[4];          // d*_advect new slot
+    T* ho[4];          // d*_advect old slot
+    T *hvt_n, *hvt_o;  // dqr_VT
+    T* precip;         // [nx]
+    double* partial;   // [gridDim.x*gridDim.y][6]: (pos, neg) of qv, qc, qr
+    int mask;          // F_* fields to advect
+    int nvp_mask;      // F_* fields whose NVP sums are wanted
+    int do_vt;         // sedimentation of qr (with F_QR)
+    int do_precip;     // surface rain diagnostic
+    AB2 ab;
+};
+
+// x flux at face (i-1/2, k), i = 1..nx-2 (Advection.cpp:36,40-44).
+template <typename T>
+__device__ __forceinline__ T scal_flux_u(const PAdvArgs<T>& a, const T* v, int i, int k) {
+    const Dims& d = a.d;
+    T ru = T(a.p.rhou[k]);
+    T ui = a.u[d.at(i, k)];
+    T v0 = v[d.at(i, k)], vm = v[d.at(i - 1, k)];
+    T f = ru * ui * (v0 + vm);
+    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
+        T um = a.u[d.at(i - 1, k)], up = a.u[d.at(i + 1, k)];
+        T vmm = v[d.at(i - 2, k)], vp = v[d.at(i + 1, k)];
+        f += T(-1. / 3.) * (ru * plus_part(ui) * (v0 - vm) -
+                            sqrt(ru * plus_part(ui) * ru * plus_part(um)) * (vm - vmm) -
+                            ru * minus_part(ui) * (v0 - vm) -
+                            sqrt(fabs(ru * minus_part(ui) * ru * minus_part(up))) * (vp - v0));
+    }
+    return f;
+}
+
+// z flux at face (i, k-1/2), k = 1..nz-2 (Advection.cpp:37,46-50).
+template <typename T>
+__device__ __forceinline__ T scal_flux_w(const PAdvArgs<T>& a, const T* v, int i, int k) {
+    const Dims& d = a.d;
+    T rk = T(a.p.rhow[k]);
+    T wk = a.w[d.at(i, k)];
+    T v0 = v[d.at(i, k)], vm = v[d.at(i, k - 1)];
+    T f = rk * wk * (v0 + vm);
+    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
+        T rkm = T(a.p.rhow[k - 1]), rkp = T(a.p.rhow[k + 1]);
+        T wm = a.w[d.at(i, k - 1)], wp = a.w[d.at(i, k + 1)];
+        T vmm = v[d.at(i, k - 2)], vp = v[d.at(i, k + 1)];
+        f += T(-1. / 3.) * (rk * plus_part(wk) * (v0 - vm) -
+                            sqrt(rk * plus_part(wk) * rkm * plus_part(wm)) * (vm - vmm) -
+                            rk * minus_part(wk) * (v0 - vm) -
+                            sqrt(fabs(rk * minus_part(wk) * rkp * minus_part(wp))) * (vp - v0));
+    }
+    return f;
+}
+
+// Sedimentation flux at (i, k-1/2), k = 1..nz-2 (Advection.cpp:165-166).
+template <typename T>
+__device__ __forceinline__ T vt_flux(const PAdvArgs<T>& a, const T* qr, int i, int k) {
+    T s = qr[a.d.at(i, k)] + qr[a.d.at(i, k - 1)];
+    T VT = T(1E-2) * (T(3634) * pow(T(a.p.vt_c1[k]) * s, T(0.1346)) * T(a.p.vt_fac[k]));
+    return T(a.p.rhow[k]) * VT * s;
+}
+
+template <typename T>
+__global__ void k_padv(PAdvArgs<T> a) {
+    __shared__ double sh[32 * 6];
+    const Dims& d = a.d;
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const bool act = (i <= d.nx - 2 && k <= d.nz - 2);
+    double sums[6] = {0, 0, 0, 0, 0, 0};
+    if (act) {
+        const size_t id = d.at(i, k);
+        const T dt15 = T(1.5 * a.c.dt), dt05 = T(0.5 * a.c.dt);
+        const T ru = T(a.p.rhou[k]);
+        for (int f = 0; f < 4; f++) {
+            if (!(a.mask & (1 << f))) continue;
+            const T* v = a.now[f];
+            // flux_u at nx-1 is the halo copy of flux_u at 1; flux_w at nz-1
+            // is zeroed (Advection.cpp:55-58).
+            T fu_p = scal_flux_u(a, v, (i == d.nx - 2) ? 1 : i + 1, k);
+            T fu_0 = scal_flux_u(a, v, i, k);
+            T fw_p = (k == d.nz - 2) ? T(0) : scal_flux_w(a, v, i, k + 1);
+            T fw_0 = scal_flux_w(a, v, i, k);
+            T px = (fu_p - fu_0) * T(a.c.r2dx) / ru;
+            T pz = (fw_p - fw_0) * T(a.c.r2dz) / ru;
+            T t = -px - pz;
+            T o = ab2_push(a.hn[f], a.ho[f], id, t, a.ab);
+            T out = v[id] + dt15 * t - dt05 * o;
+            if (f == 3 && a.do_vt) {
+                T gp = (k == d.nz - 2) ? T(0) : vt_flux(a, v, i, k + 1);
+                T g0 = vt_flux(a, v, i, k);
+                T tv = (gp - g0) * T(a.c.r2dz) / ru;
+                T ov = ab2_push(a.hvt_n, a.hvt_o, id, tv, a.ab);
+                out += dt15 * tv - dt05 * ov;
+            }
+            a.fut[f][id] = out;
+            if (f >= 1 && (a.nvp_mask & (1 << f))) {
+                if (out >= T(0)) sums[2 * (f - 1)] += (double)out;
+                else sums[2 * (f - 1) + 1] += (double)out;
+            }
+        }
+        if (a.do_precip && k == 1) {
+            const T* qr = a.now[3];
+            T q1 = qr[d.at(i, 1)];
+            T VT = T(1E-2) * (T(3634) * pow(T(a.p.pf1) * q1, T(0.1346)) * T(a.p.pf2));
+            T rain = -T(a.p.rhou[1]) * (T(0.5) * (a.w[d.at(i, 2)] + T(0)) - VT) * q1;
+            a.precip[i] = (rain < T(0)) ? T(0) : rain;
+        }
+    }
+    if (a.nvp_mask) {
+        block_sum(sums, sh);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            double* out = a.partial + (size_t)(blockIdx.x + gridDim.x * blockIdx.y) * 6;
+#pragma unroll
+            for (int j = 0; j < 6; j++) out[j] = sums[j];
+        }
+    }
+}
+
+// Final sums of NegativeValueProcess and its rescaling factor
+// (MicroPhysics.cpp:125-127): nvp[2f] = 1 if positives are rescaled,
+// nvp[2f+1] = 1 - |neg/pos|. One block; fixed summation order.
+__global__ void k_nvp_final(const double* partial, int nblocks, double* nvp);
+
+// ---------------------------------------------------------------------------
+// Finishes th, qv, qc, qr after advection or microphysics: the rescaling of
+// NegativeValueProcess, AddForcing (AddForcing.cpp:6-28) and the
+// BoundaryProcess2D_center halo. One thread per interior cell.
+
+template <typename T>
+struct ApplyArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    T* fut[4];               // thp, qvp, qcp, qrp (in place)
+    const double* nvp;       // [6] from k_nvp_final
+    const T* th_forcing;     // init_th_forcing (may be null)
+    int mask;                // fields to finish
+    int nvp_mask;            // fields to clip/rescale
+    int forcing;             // add Q1LS/Q2LS
+    int forcing_th;          // add dt*init_th_forcing (status_for_adding_forcing)
+    int halo;                // write ghost images
+};
+
+template <typename T>
+__device__ __forceinline__ T nvp_apply(T v, const double* nvp, int f) {
+    if (!(v >= T(0))) return T(0);                        // MicroPhysics.cpp:121-122
+    if (nvp[2 * f] != 0.0 && v > T(0)) return v * T(nvp[2 * f + 1]);   // MicroPhysics.cpp:130
+    return v;
+}
+
+template <typename T>
+__global__ void k_apply(ApplyArgs<T> a) {
+    const Dims& d = a.d;
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > d.nx - 2 || k > d.nz - 2) return;
+    const size_t id = d.at(i, k);
+    const T dt = T(a.c.dt);
+    for (int f = 0; f < 4; f++) {
+        if (!(a.mask & (1 << f))) continue;
+        T v = a.fut[f][id];
+        if (f >= 1 && (a.nvp_mask & (1 << f))) v = nvp_apply(v, a.nvp, f - 1);
+        if (f == 0) {
+            if (a.forcing) v += dt * T(a.p.q1ls[k]);
+            if (a.forcing_th) v += dt * a.th_forcing[id];
+        }
+        if (f == 1 && a.forcing) v += dt * T(a.p.q2ls[k]);
+        if (a.halo) store_center(a.fut[f], d, i, k, v);
+        else a.fut[f][id] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BoundaryProcess2D_all (Boundary.cpp:32-52) as a standalone pass.
+
+template <typename T>
+struct HaloArgs {
+    Dims d;
+    T *zetap, *w;        // westdown
+    T* center[5];        // thp, u, qvp, qcp, qrp
+};
+
+template <typename T>
+__global__ void k_halo_all(HaloArgs<T> a) {
+    const Dims& d = a.d;
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > d.nx - 2 || k > d.nz - 2) return;
+    const size_t id = d.at(i, k);
+    if (k >= 2) {
+        store_westdown(a.zetap, d, i, k, a.zetap[id]);
+        store_westdown(a.w, d, i, k, a.w[id]);
+    }
+#pragma unroll
+    for (int f = 0; f < 5; f++) store_center(a.center[f], d, i, k, a.center[f][id]);
+}
+
+// ---------------------------------------------------------------------------
+// Kessler warm rain, applied cell by cell in the reference's order:
+// autoconversion (MicroPhysics.cpp:29-51), accretion (:54-77), evaporation
+// (:80-114), saturation adjustment (:7-26); then the NVP partial sums of qvp,
+// qcp, qrp. One thread per interior cell.
+
+template <typename T>
+struct KesslerArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    T *thp, *qvp, *qcp, *qrp;
+    T *d_auto, *d_accr, *d_evap, *d_cond;  // diagnostics (may be null)
+    double* partial;
+    int nvp;  // accumulate NVP sums
+};
+
+template <typename T>
+__global__ void k_kessler(KesslerArgs<T> a) {
+    __shared__ double sh[32 * 6];
+    const Dims& d = a.d;
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const bool act = (i <= d.nx - 2 && k <= d.nz - 2);
+    double sums[6] = {0, 0, 0, 0, 0, 0};
+    if (act) {
+        const size_t id = d.at(i, k);
+        const T dt = T(a.c.dt), lv = T(a.c.lv), cp = T(a.c.cp);
+        const T pib = T(a.p.pib[k]), rhou = T(a.p.rhou[k]), pc = T(a.p.pc[k]), pb = T(a.p.pb[k]);
+        T th = a.thp[id], qv = a.qvp[id], qc = a.qcp[id], qr = a.qrp[id];
+        // autoconversion
+        {
+            T qcplus = smax(T(0), qc);
+            T ar = T(0.001) * (qcplus - T(0.001));
+            ar = smax(T(0), ar);
+            T arcrdt = smin(ar * dt, qcplus);
+            qc = qc - arcrdt;
+            qr = qr + arcrdt;
+            if (a.d_auto) a.d_auto[id] = arcrdt;
+        }
+        // accretion
+        {
+            T qcplus = smax(T(0), qc), qrplus = smax(T(0), qr);
+            T cr = T(2.2) * qcplus * (pow(qrplus, T(0.875)));
+            T arcrdt = smin(cr * dt, qcplus);
+            qc = qc - arcrdt;
+            qr = qr + arcrdt;
+            if (a.d_accr) a.d_accr[id] = arcrdt;
+        }
+        // evaporation of rain
+        {
+            T qrplus = smax(T(0), qr), qvplus = smax(T(0), qv);
+            T qvs = pc * exp(T(17.27) * (pib * th - T(273.)) / (pib * th - T(36.)));
+            T deficit = smax((T(1.) - qvplus / qvs), T(0.));
+            T coef = T(1.6) + T(124.9) * pow((T(1E-3) * rhou * qrplus), T(0.2046));
+            T er = coef * deficit * (pow(T(1E-3) * rhou * qrplus, T(0.525))) /
+                   ((T(5.4E5) + T(2.55E6) / (T(1E-2) * pb * qvs)) * T(1E-3) * rhou);
+            T erdt = smin(qrplus, smax(T(0.), er * dt));
+            qr = qr - erdt;
+            qv = qv + erdt;
+            th = th - lv * erdt / (cp * pib);
+            if (a.d_evap) a.d_evap[id] = erdt;
+        }
+        // saturation adjustment
+        {
+            T qvs = pc * exp(T(17.27) * (pib * th - T(273.)) / (pib * th - T(36.)));
+            T tm = th * pib - T(36.);
+            T phi = qvs * (T(17.27) * T(237.) * lv) / (cp * (tm * tm));
+            T C = (qv - qvs) / (T(1) + phi);
+            if (fabs(C) > qc && C < T(0)) C = -qc;
+            qv = qv - C;
+            qc = qc + C;
+            th = th + lv / (cp * pib) * C;
+            if (a.d_cond) a.d_cond[id] = C;
+        }
+        a.thp[id] = th;
+        a.qvp[id] = qv;
+        a.qcp[id] = qc;
+        a.qrp[id] = qr;
+        if (a.nvp) {
+            T q[3] = {qv, qc, qr};
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+                if (q[f] >= T(0)) sums[2 * f] += (double)q[f];
+                else sums[2 * f + 1] += (double)q[f];
+            }
+        }
+    }
+    if (a.nvp) {
+        block_sum(sums, sh);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            double* out = a.partial + (size_t)(blockIdx.x + gridDim.x * blockIdx.y) * 6;
+#pragma unroll
+            for (int j = 0; j < 6; j++) out[j] = sums[j];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Eddy coefficients (Turbulence::RKM_RKH, Turbulent.cpp:5-45) with their
+// center halo. One thread per interior cell.
+
+template <typename T>
+struct RKArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    const T *u, *w, *thp;
+    T *RKM, *RKH;
+};
+
+template <typename T>
+__global__ void k_rkm_rkh(RKArgs<T> a) {
+    const Dims& d = a.d;
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > d.nx - 2 || k > d.nz - 2) return;
+    const T* u = a.u;
+    const T* w = a.w;
+    T Rzeta = T(0.5) * ((w[d.at(i + 1, k + 1)] + w[d.at(i + 1, k)]) - (w[d.at(i - 1, k + 1)] + w[d.at(i - 1, k)])) * T(a.c.r2dx) +
+              T(0.5) * ((u[d.at(i + 1, k + 1)] + u[d.at(i, k + 1)]) - (u[d.at(i + 1, k - 1)] + u[d.at(i, k - 1)])) * T(a.c.r2dz);
+    T rot = (u[d.at(i + 1, k)] - u[d.at(i, k)]) * T(a.c.rdx) + (w[d.at(i, k + 1)] - w[d.at(i, k)]) * T(a.c.rdz);
+    T Rotat = rot * rot;
+    T th0 = a.thp[d.at(i, k)];
+    T def2 = Rzeta * Rzeta + T(2.) * Rotat;
+    T Ri = (T(a.c.gravity) / th0 * (a.thp[d.at(i, k + 1)] - a.thp[d.at(i, k - 1)]) * T(a.c.r2dz)) / def2;
+    T lam = T(a.p.lambda2[k]);
+    T km, kh;
+    if (Ri < T(0)) {
+        km = lam * sqrt(def2) * sqrt(T(1.) - T(16.) * Ri);
+        kh = lam * sqrt(def2) * T(1.4) * sqrt(T(1.) - T(40.) * Ri);
+    } else if (T(0) < Ri && Ri < T(0.25)) {
+        km = lam * sqrt(def2) * pow(T(1.) - T(4.) * Ri, T(4));
+        kh = lam * sqrt(def2) * T(1.4) * (T(1.) - T(1.2) * Ri) * pow(T(1.) - T(4.) * Ri, T(4));
+    } else {
+        km = T(0.);
+        kh = T(0.);
+    }
+    const T kmax = T(0.8 * a.c.dx * a.c.dz / a.c.dt);
+    km = smax(km, T(10.));
+    kh = smax(kh, T(10.));
+    km = smin(km, kmax);
+    kh = smin(kh, kmax);
+    store_center(a.RKM, d, i, k, km);
+    store_center(a.RKH, d, i, k, kh);
+}
+
+// ---------------------------------------------------------------------------
+// In-place Gauss-Seidel diffusion (Turbulence::Mparam / Hparam,
+// Turbulent.cpp:68-114), exact to round-off, with the top-layer nudging of
+// theta and zeta fused in (NumericalProcess.cpp:60-85).
+//
+// The reference sweeps k outer, i inner and reads the already-updated left
+// (i-1) and lower (k-1) neighbours, so row k is the first-order linear
+// recurrence v'[i] = A[i] + B[i] v'[i-1] with v'[0] the untouched ghost, where
+// B[i] is the left-face coefficient and A[i] collects everything else
+// (including the updated row k-1). One block of 1024 threads owns one field
+// and walks the rows in order; each row is solved with an affine-map scan:
+// a thread composes the maps of its contiguous chunk, warps scan those with
+// shuffles, warp 0 scans the warp totals. The updated row stays in registers
+// for the next row.
+
+template <typename T>
+struct GSArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    T* v[5];          // zetap (Mparam, RKM), thp, qvp, qcp, qrp (Hparam, RKH)
+    const T *RKM, *RKH;
+    int mask;         // bit f: diffuse field f
+    int nudge;        // fuse Nudge_theta (field 1) and Nudge_zeta (field 0)
+};
+
+constexpr int kGSThreads = 1024;
+constexpr int kGSMaxPerThread = 8;   // NX up to 8192
+
+template <typename T>
+__global__ void __launch_bounds__(kGSThreads) k_gs_diffuse(GSArgs<T> a) {
+    __shared__ T shA[32], shB[32];
+    const int f = blockIdx.x;
+    if (!(a.mask & (1 << f))) return;
+    const Dims& d = a.d;
+    T* v = a.v[f];
+    const bool mom = (f == 0);
+    const T* K = mom ? a.RKM : a.RKH;
+    const int NX = d.nx - 2;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int per = (NX + kGSThreads - 1) / kGSThreads;
+    const int i0 = 1 + tid * per;
+    const T cx = T(a.c.rdx2 * a.c.dt);
+    T vdn[kGSMaxPerThread];
+    // row 0 (ghost) is the "updated" row below row 1: never modified
+#pragma unroll
+    for (int e = 0; e < kGSMaxPerThread; e++) {
+        int i = i0 + e;
+        vdn[e] = (e < per && i <= NX) ? v[d.at(i, 0)] : T(0);
+    }
+    for (int k = 1; k <= d.nz - 2; k++) {
+        const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
+        T Aa[kGSMaxPerThread], Bb[kGSMaxPerThread];
+        T cA = T(0), cB = T(1);  // composition of this thread's maps (identity)
+#pragma unroll
+        for (int e = 0; e < kGSMaxPerThread; e++) {
+            int i = i0 + e;
+            Aa[e] = T(0);
+            Bb[e] = T(1);
+            if (e < per && i <= NX) {
+                T v0 = v[d.at(i, k)], vr = v[d.at(i + 1, k)], vu = v[d.at(i, k + 1)];
+                T ax, bx, czu, czd;
+                if (mom) {  // Turbulent.cpp:83-88
+                    T Kc = K[d.at(i, k)], Kd = K[d.at(i, k - 1)], Kl = K[d.at(i - 1, k)], Kld = K[d.at(i - 1, k - 1)];
+                    ax = T(0.5) * (Kc + Kd);
+                    bx = T(0.5) * (Kl + Kld);
+                    czu = T(a.p.rhou[k]) * T(0.5) * (Kc + Kl);
+                    czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd + Kld);
+                } else {    // Turbulent.cpp:107-112
+                    T Kc = K[d.at(i, k)], Kr = K[d.at(i + 1, k)], Kl = K[d.at(i - 1, k)];
+                    T Ku = K[d.at(i, k + 1)], Kd = K[d.at(i, k - 1)];
+                    ax = T(0.5) * (Kr + Kc);
+                    bx = T(0.5) * (Kc + Kl);
+                    czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku + Kc);
+                    czd = T(a.p.rhow[k]) * T(0.5) * (Kc + Kd);
+                }
+                Aa[e] = v0 + cx * (ax * (vr - v0) - bx * v0) + cz * (czu * (vu - v0) - czd * (v0 - vdn[e]));
+                Bb[e] = cx * bx;
+                cA = Aa[e] + Bb[e] * cA;
+                cB = Bb[e] * cB;
+            }
+        }
+        // inclusive warp scan of the chunk maps (earlier maps on lower lanes)
+        T sA = cA, sB = cB;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T pA = __shfl_up_sync(0xffffffffu, sA, o);
+            T pB = __shfl_up_sync(0xffffffffu, sB, o);
+            if (lane >= o) {
+                sA = sA + sB * pA;
+                sB = sB * pB;
+            }
+        }
+        if (lane == 31) { shA[wid] = sA; shB[wid] = sB; }
+        __syncthreads();
+        if (wid == 0) {
+            T wA = shA[lane], wB = shB[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                T pA = __shfl_up_sync(0xffffffffu, wA, o);
+                T pB = __shfl_up_sync(0xffffffffu, wB, o);
+                if (lane >= o) {
+                    wA = wA + wB * pA;
+                    wB = wB * pB;
+                }
+            }
+            shA[lane] = wA;
+            shB[lane] = wB;
+        }
+        __syncthreads();
+        // exclusive prefix of this thread = (warps before) then (lanes before)
+        T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
+        if (lane == 0) { eA = T(0); eB = T(1); }
+        T pA = (wid > 0) ? shA[wid - 1] : T(0), pB = (wid > 0) ? shB[wid - 1] : T(1);
+        T x = v[d.at(0, k)];                 // ghost v'[0]: never updated
+        x = pA + pB * x;
+        x = eA + eB * x;
+        const T dcgr = mom ? T(a.p.dtcgr_zeta[k]) : T(a.p.dtcgr_th[k]);
+#pragma unroll
+        for (int e = 0; e < kGSMaxPerThread; e++) {
+            int i = i0 + e;
+            if (e < per && i <= NX) {
+                x = Aa[e] + Bb[e] * x;
+                vdn[e] = x;
+                T out = x;
+                if (a.nudge && f == 0) out = x - dcgr * x;                                  // Nudge_zeta
+                if (a.nudge && f == 1) out = x - dcgr * (x - T(a.p.thb_init[k]));           // Nudge_theta
+                v[d.at(i, k)] = out;
+            }
+        }
+        __syncthreads();  // shA/shB reuse and row k+1 reads after row k writes
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Top-layer nudging as standalone passes (NumericalProcess.cpp:60-96).
+
+template <typename T>
+struct NudgeArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    T *thp, *zetap, *qvp;
+    const T* qv;
+    int do_th, do_zeta;
+    double tau;       // moisture_nudge_time, 0 = off
+};
+
+template <typename T>
+__global__ void k_nudge(NudgeArgs<T> a) {
+    const Dims& d = a.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= d.nx || k >= d.nz) return;
+    const size_t id = d.at(i, k);
+    const bool inner = (i >= 1 && i <= d.nx - 2 && k >= 1 && k <= d.nz - 2);
+    if (inner && a.do_th) {
+        T x = a.thp[id];
+        a.thp[id] = x - T(a.p.dtcgr_th[k]) * (x - T(a.p.thb_init[k]));
+    }
+    if (inner && a.do_zeta) {
+        T x = a.zetap[id];
+        a.zetap[id] = x - T(a.p.dtcgr_zeta[k]) * x;
+    }
+    if (a.tau != 0.0)  // every cell, ghosts included (NumericalProcess.cpp:90-94)
+        a.qvp[id] = a.qvp[id] + T(a.c.dt) * (T(a.p.qvb0[k]) - a.qv[id]) / T(a.tau);
+}
+
+// ---------------------------------------------------------------------------
+// Horizontal means (Iteration::updateMean, Iteration.cpp:42-86): thb, qvb and
+// thvb = thb (1 + 0.608 qvb) per level with their 1D halos. One block per
+// interior level. Optionally rotates ubarTop (nextTimeStep, :166-167).
+
+template <typename T>
+struct MeanArgs {
+    Dims d;
+    const T *thp, *qvp;
+    double *thb, *qvb, *thvb;
+    double* ubar;   // [0] ubarTop, [1] ubarTopp
+    int rotate_ubar;
+};
+
+template <typename T>
+__global__ void k_update_mean(MeanArgs<T> a) {
+    __shared__ double sh[32 * 2];
+    const Dims& d = a.d;
+    const int k = 1 + blockIdx.x;
+    double s[2] = {0, 0};
+    for (int i = 1 + threadIdx.x; i <= d.nx - 2; i += blockDim.x) {
+        s[0] += (double)a.thp[d.at(i, k)];
+        s[1] += (double)a.qvp[d.at(i, k)];
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        double n = (double)(d.nx - 2.);
+        double tb = s[0] / n, qb = s[1] / n, tv = tb * (1 + 0.608 * qb);
+        a.thb[k] = tb;
+        a.qvb[k] = qb;
+        a.thvb[k] = tv;
+        if (k == 1) { a.thb[0] = tb; a.qvb[0] = qb; a.thvb[0] = tv; }
+        if (k == d.nz - 2) { a.thb[d.nz - 1] = tb; a.qvb[d.nz - 1] = qb; a.thvb[d.nz - 1] = tv; }
+        if (k == 1 && a.rotate_ubar) a.ubar[0] = a.ubar[1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Domain-mean top wind tendency (PoissonSolver::pubarTop_pt,
+// PoissonSolver.cpp:655-676). One block.
+
+template <typename T>
+struct PubarArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    const T *u, *w, *RKM;
+    double* ubar;     // [0] ubarTop, [1] ubarTopp
+    double* dubar;    // dubarTop_advect[2]
+    AB2 ab;
+};
+
+template <typename T>
+__global__ void k_pubartop(PubarArgs<T> a) {
+    __shared__ double sh[32 * 3];
+    const Dims& d = a.d;
+    const int t = d.nz - 2, b = d.nz - 3, top = d.nz - 1;
+    const double* rhou = a.p.rhou;
+    const double* rhow = a.p.rhow;
+    double s[3] = {0, 0, 0};
+    for (int i = 1 + threadIdx.x; i < d.nx - 1; i += blockDim.x) {
+        double ut = a.u[d.at(i, t)], ub = a.u[d.at(i, b)], utop = a.u[d.at(i, top)];
+        double wt = a.w[d.at(i, t)], wtm = a.w[d.at(i - 1, t)];
+        const T* K = a.RKM;
+        s[0] += 0.25 * (rhou[t] * ut + rhou[b] * ub) * (wt + wtm);
+        s[1] += rhow[top] * 0.25 * ((double)K[d.at(i, top)] + K[d.at(i, t)] + K[d.at(i - 1, top)] + K[d.at(i - 1, t)]) *
+                (a.c.rdz * (utop - ut));
+        s[2] += rhow[t] * 0.25 * ((double)K[d.at(i, t)] + K[d.at(i, b)] + K[d.at(i - 1, t)] + K[d.at(i - 1, b)]) *
+                (a.c.rdx * (wt - wtm) + a.c.rdz * (ut - ub));
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        double n = (double)(d.nx - 2.);
+        double down = s[0] / n, kup = s[1] / n, kdown = s[2] / n;
+        double pa = (-down) * a.c.rdz / rhou[t];
+        double pb = (kup - kdown) * a.c.rdz / rhou[t];
+        double tend = -pa + pb;
+        double old = a.ab.first ? tend : a.dubar[a.ab.so];
+        a.dubar[a.ab.sn] = tend;
+        if (a.ab.first) a.dubar[a.ab.so] = tend;
+        a.ubar[1] = a.ubar[0] + 1.5 * a.c.dt * tend - 0.5 * a.c.dt * old;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// cal_u (PoissonSolver.cpp:580-653): the top-row wind from the periodic chi
+// problem and the column integral below it.
+//
+// Top row: chi[i-1] - 2 chi[i] + chi[i+1] = h[i] only enters through
+// uxi = (chi[i] - chi[i-1])/dx with its mean removed. The differences satisfy
+// d[i+1] - d[i] = h[i], so uxi is an exclusive prefix sum of h (any constant
+// cancels in the mean removal); the reference reaches the same values with
+// CG to 1e-12. One block.
+
+template <typename T>
+struct CalUArgs {
+    Dims d;
+    Consts c;
+    Profiles p;
+    T* u;
+    const T *w, *zetap;
+    const double* ubar;   // [1] = ubarTopp
+};
+
+constexpr int kCalUThreads = 1024;
+
+template <typename T>
+__global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) {
+    __shared__ double sh[32 * 1];
+    __shared__ double scan[32];
+    const Dims& d = a.d;
+    const int NX = d.nx - 2, t = d.nz - 2;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int per = (NX + kCalUThreads - 1) / kCalUThreads;
+    const int i0 = 1 + tid * per;
+    const double c = a.p.rhow[t] / a.p.rhou[t];
+    double h[kGSMaxPerThread];
+    double s[1] = {0};
+#pragma unroll
+    for (int e = 0; e < kGSMaxPerThread; e++) {
+        int i = i0 + e;
+        h[e] = 0;
+        if (e < per && i <= NX) {
+            h[e] = -(0. - a.p.rhow[t] * (double)a.w[d.at(i, t)]) / a.p.rhou[t] * a.c.dx;
+            s[0] += h[e];
+        }
+    }
+    (void)c;
+    block_sum(s, sh);
+    const double hmean = s[0] / NX;
+    double loc = 0;
+#pragma unroll
+    for (int e = 0; e < kGSMaxPerThread; e++) {
+        int i = i0 + e;
+        if (e < per && i <= NX) { h[e] = h[e] - hmean; loc += h[e]; }
+    }
+    // exclusive scan of the chunk totals
+    double incl = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double p = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += p;
+    }
+    if (lane == 31) scan[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        double x = scan[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            double p = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += p;
+        }
+        scan[lane] = x;
+    }
+    __syncthreads();
+    double run = incl - loc + (wid > 0 ? scan[wid - 1] : 0.0);
+    double ux[kGSMaxPerThread];
+    double s2[1] = {0};
+#pragma unroll
+    for (int e = 0; e < kGSMaxPerThread; e++) {
+        int i = i0 + e;
+        ux[e] = 0;
+        if (e < per && i <= NX) {
+            ux[e] = run * a.c.rdx;
+            run += h[e];
+            s2[0] += ux[e];
+        }
+    }
+    block_sum(s2, sh);
+    const double umean = s2[0] / NX;
+    const double ubarp = a.ubar[1];
+#pragma unroll
+    for (int e = 0; e < kGSMaxPerThread; e++) {
+        int i = i0 + e;
+        if (e < per && i <= NX) {
+            T v = T((ux[e] - umean) + ubarp);
+            a.u[d.at(i, t)] = v;
+            if (i == NX) a.u[d.at(0, t)] = v;
+            if (i == 1) a.u[d.at(d.nx - 1, t)] = v;
+        }
+    }
+}
+
+// Column integral u(i, k) = u(i, nz-2) + sum_{m=k}^{nz-3} (dw/dx - rhow zeta)(-dz)
+// from the top down (PoissonSolver.cpp:644-651), with the center halo of u.
+// One thread per interior column.
+template <typename T>
+__global__ void k_cal_u_columns(CalUArgs<T> a) {
+    const Dims& d = a.d;
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > d.nx - 2) return;
+    const int t = d.nz - 2;
+    const T utop = a.u[d.at(i, t)];
+    store_center(a.u, d, i, t, utop);
+    T area = T(0);
+    const T rdx = T(a.c.rdx), mdz = T(-a.c.dz);
+    for (int k = d.nz - 3; k >= 1; k--) {
+        area += ((a.w[d.at(i, k + 1)] - a.w[d.at(i - 1, k + 1)]) * rdx - T(a.p.rhow[k + 1]) * a.zetap[d.at(i, k + 1)]) * mdz;
+        store_center(a.u, d, i, k, area + utop);
+    }
+}
+
+}  // namespace vvm

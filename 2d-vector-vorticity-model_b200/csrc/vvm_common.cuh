@@ -1,0 +1,121 @@
+// Device layout and shared helpers of the VVM step kernels (sm_100a).
+//
+// Every 2D field of a case is one x-contiguous array [nz][pitch] with the
+// reference's ghost cells kept in place (i = 0 and nx-1, k = 0 and nz-1), so
+// cell (i, k) of the reference's model.var[i][k] lives at k*pitch + i. Rows
+// are padded to a multiple of 32 cells: a warp reading one row segment touches
+// whole 128-byte lines. Profiles are [nz] doubles.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vvm {
+
+constexpr int kPad = 32;
+
+struct Dims {
+    int nx, nz, pitch;  // pitch >= nx, multiple of kPad
+    __host__ __device__ __forceinline__ size_t at(int i, int k) const {
+        return (size_t)k * pitch + i;
+    }
+    __host__ __device__ __forceinline__ size_t cells() const { return (size_t)nz * pitch; }
+};
+
+// Physical constants and grid metrics of one case (src/Declare.hpp:78-96,
+// src/main.cpp:68-72). Reciprocals are formed exactly as the reference
+// forms them.
+struct Consts {
+    double dx, dz, dt, rdx, r2dx, rdz, r2dz, rdx2, rdz2;
+    double gravity, cp, cv, rd, lv, p0;
+};
+
+template <typename T>
+__device__ __forceinline__ T plus_part(T v) { return T(0.5) * (v + fabs(v)); }   // Advection.cpp:17-19
+template <typename T>
+__device__ __forceinline__ T minus_part(T v) { return T(0.5) * (v - fabs(v)); }  // Advection.cpp:21-23
+
+// std::max / std::min semantics (the first argument wins ties and NaN), as
+// used throughout the reference's microphysics and turbulence.
+template <typename T>
+__device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+template <typename T>
+__device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
+
+// Writes the value of interior cell (i, k) and every ghost cell that
+// BoundaryProcess2D_center (src/Boundary.cpp:9-19) fills from it: the
+// periodic x ghosts of rows 1..nz-2, then the zero-gradient z ghosts of every
+// column including the corner cells. Each ghost cell has exactly one source
+// cell, so a grid over the interior fills the halo without a second pass.
+template <typename T>
+__device__ __forceinline__ void store_center(T* a, const Dims& d, int i, int k, T v) {
+    const bool gl = (i == d.nx - 2), gr = (i == 1);
+    a[d.at(i, k)] = v;
+    if (gl) a[d.at(0, k)] = v;
+    if (gr) a[d.at(d.nx - 1, k)] = v;
+    if (k == 1) {
+        a[d.at(i, 0)] = v;
+        if (gl) a[d.at(0, 0)] = v;
+        if (gr) a[d.at(d.nx - 1, 0)] = v;
+    }
+    if (k == d.nz - 2) {
+        a[d.at(i, d.nz - 1)] = v;
+        if (gl) a[d.at(0, d.nz - 1)] = v;
+        if (gr) a[d.at(d.nx - 1, d.nz - 1)] = v;
+    }
+}
+
+// Same for BoundaryProcess2D_westdown (src/Boundary.cpp:21-30) on a field
+// whose interior values exist for k = 2..nz-2: periodic x ghosts, rows 0, 1
+// and nz-1 zero everywhere (written by the k = 2 and k = nz-2 cells).
+template <typename T>
+__device__ __forceinline__ void store_westdown(T* a, const Dims& d, int i, int k, T v) {
+    const bool gl = (i == d.nx - 2), gr = (i == 1);
+    a[d.at(i, k)] = v;
+    if (gl) a[d.at(0, k)] = v;
+    if (gr) a[d.at(d.nx - 1, k)] = v;
+    if (k == 2) {
+        a[d.at(i, 0)] = T(0);
+        a[d.at(i, 1)] = T(0);
+        if (gl) { a[d.at(0, 0)] = T(0); a[d.at(0, 1)] = T(0); }
+        if (gr) { a[d.at(d.nx - 1, 0)] = T(0); a[d.at(d.nx - 1, 1)] = T(0); }
+    }
+    if (k == d.nz - 2) {
+        a[d.at(i, d.nz - 1)] = T(0);
+        if (gl) a[d.at(0, d.nz - 1)] = T(0);
+        if (gr) a[d.at(d.nx - 1, d.nz - 1)] = T(0);
+    }
+}
+
+// Warp and block sums in a fixed order (deterministic for a fixed launch
+// shape). All reductions of the step accumulate in FP64.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sums N values per thread over the (1D or 2D) block; every thread gets the
+// totals. `sh` needs 32*N doubles of shared memory.
+template <int N>
+__device__ __forceinline__ void block_sum(double (&v)[N], double* sh) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+#pragma unroll
+    for (int j = 0; j < N; j++) v[j] = warp_sum(v[j]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < N; j++) sh[j * 32 + wid] = v[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        double t = (lane < nw) ? sh[j * 32 + lane] : 0.0;
+        v[j] = warp_sum(t);
+    }
+    __syncthreads();
+}
+
+}  // namespace vvm

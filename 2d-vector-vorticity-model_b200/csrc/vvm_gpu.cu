@@ -1,0 +1,1330 @@
+// libvvmgpu.so: the B200 VVM time step behind the C ABI of include/vvm_gpu.h.
+//
+// Host code: device memory of one context, coefficient profiles formed with
+// the reference's expressions, the multigrid-preconditioned CG of cal_w, and
+// the launch sequence of one step (src/Iteration.cpp:262-434).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/vvm_gpu.h"
+#include "poisson_kernels.cuh"
+#include "step_kernels.cuh"
+
+using namespace vvm;
+
+// ===========================================================================
+// Non-template kernels
+
+namespace vvm {
+
+__global__ void k_nvp_final(const double* partial, int nblocks, double* nvp) {
+    __shared__ double sh[32 * 6];
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int j = 0; j < 6; j++) s[j] += partial[(size_t)b * 6 + j];
+    block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        for (int f = 0; f < 3; f++) {
+            double pos = s[2 * f], neg = s[2 * f + 1];
+            // MicroPhysics.cpp:125-127
+            bool skip = (pos == 0. || fabs(neg) > pos);
+            nvp[2 * f] = skip ? 0.0 : 1.0;
+            nvp[2 * f + 1] = skip ? 1.0 : 1. - fabs(neg / pos);
+        }
+    }
+}
+
+__global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mode) {
+    __shared__ double sh[32];
+    double s[1] = {0};
+    for (int b = threadIdx.x; b < n; b += blockDim.x) s[0] += partial[b];
+    block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        double v = s[0];
+        switch (mode) {
+            case CG_SET_BB: sc->bb = v; break;
+            case CG_SET_RR: sc->rr = v; break;
+            case CG_SET_RZ: sc->rz = v; break;
+            case CG_PQ_ALPHA: sc->pq = v; sc->alpha = (v != 0.0) ? sc->rz / v : 0.0; break;
+            case CG_RZ_BETA:
+                sc->rz_new = v;
+                sc->beta = (sc->rz != 0.0) ? v / sc->rz : 0.0;
+                sc->rz = v;
+                break;
+        }
+    }
+}
+
+// b = rhow_k^2 (zetap[i+1][k] - zetap[i][k]) dx for k = 2..nz-2, i = 1..nx-2
+// (PoissonSolver.cpp:444-450); stores f = -b / rhow_k and partial ||b||^2.
+template <typename T>
+__global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const T* zetap, double* f,
+                              int pitch_f, double* partial) {
+    __shared__ double sh[32];
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    double s[1] = {0};
+    if (ii < d.nx - 2 && kk < d.nz - 3) {
+        const int i = ii + 1, k = kk + 2;
+        double b = rhow[k] * rhow[k] * ((double)zetap[d.at(i + 1, k)] - (double)zetap[d.at(i, k)]) * dx;
+        f[(size_t)kk * pitch_f + ii] = -b / rhow[k];
+        s[0] = b * b;
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
+}
+
+// Reference-ordered b vector ((k-2)*NX + (i-1)) to f = -b/rhow_k, partial ||b||^2.
+__global__ void k_rhs_from_b(int NX, int NK, const double* rhow, const double* b, double* f,
+                             int pitch_f, double* partial) {
+    __shared__ double sh[32];
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    double s[1] = {0};
+    if (ii < NX && kk < NK) {
+        double bv = b[(size_t)kk * NX + ii];
+        f[(size_t)kk * pitch_f + ii] = -bv / rhow[kk + 2];
+        s[0] = bv * bv;
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
+}
+
+__global__ void k_pack_solution(int NX, int NK, const double* x, int pitch, double* out) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii < NX && kk < NK) out[(size_t)kk * NX + ii] = x[(size_t)kk * pitch + ii];
+}
+
+__global__ void k_unpack_solution(int NX, int NK, const double* in, double* x, int pitch) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii < NX && kk < NK) x[(size_t)kk * pitch + ii] = in[(size_t)kk * NX + ii];
+}
+
+// w = W / rhow_k for k = 2..nz-2 (PoissonSolver.cpp:469-475), westdown halo.
+template <typename T>
+__global__ void k_w_from_W(Dims d, const double* rhow, const double* W, int pitch_f, T* w) {
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 2 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > d.nx - 2 || k > d.nz - 2) return;
+    double v = W[(size_t)(k - 2) * pitch_f + (i - 1)] / rhow[k];
+    store_westdown(w, d, i, k, T(v));
+}
+
+// x64 += (double) d32 (iterative refinement).
+__global__ void k_refine_add(int NX, int NK, int pitch, double* x, const float* dlt) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii < NX && kk < NK) {
+        size_t id = (size_t)kk * pitch + ii;
+        x[id] += (double)dlt[id];
+    }
+}
+
+__global__ void k_to_float(int NX, int NK, int pitch, const double* a, float* b) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii < NX && kk < NK) {
+        size_t id = (size_t)kk * pitch + ii;
+        b[id] = (float)a[id];
+    }
+}
+
+// Host [nx][nz] (k fast, stride sk per element) <-> device [nz][pitch].
+template <typename T>
+__global__ void k_from_host_layout(Dims d, const double* src, int sk, int off, T* dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < d.nx && k < d.nz) dst[d.at(i, k)] = T(src[((size_t)i * d.nz + k) * sk + off]);
+}
+
+template <typename T>
+__global__ void k_to_host_layout(Dims d, const T* src, int sk, int off, double* dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < d.nx && k < d.nz) dst[((size_t)i * d.nz + k) * sk + off] = (double)src[d.at(i, k)];
+}
+
+}  // namespace vvm
+
+// ===========================================================================
+// Host helpers
+
+namespace {
+
+struct CudaError {
+    std::string msg;
+};
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            throw CudaError{std::string(#call) + ": " + cudaGetErrorString(e_)};             \
+    } while (0)
+
+#define CKL()                                                                                \
+    do {                                                                                     \
+        cudaError_t e_ = cudaGetLastError();                                                 \
+        if (e_ != cudaSuccess) throw CudaError{std::string("launch: ") + cudaGetErrorString(e_)}; \
+    } while (0)
+
+inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+inline int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// Owns device allocations of one context.
+struct Arena {
+    std::vector<void*> ptrs;
+    template <typename X>
+    X* alloc(size_t n) {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(X)));
+        CK(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(X)));
+        ptrs.push_back(p);
+        return static_cast<X*>(p);
+    }
+    ~Arena() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+constexpr int kCoarseMax = 8;
+
+// Multigrid hierarchy for the symmetric w-equation operator, precision P.
+template <typename P>
+struct Multigrid {
+    int NK = 0, nlev = 0;
+    std::vector<int> nx, pitch;
+    std::vector<P*> f, x, y;
+    std::vector<double*> cx, lo, inv, cp;
+    double *ru = nullptr, *rd = nullptr;
+    int nc = 0;
+    double *Q = nullptr, *clo = nullptr, *cinv = nullptr, *ccp = nullptr, *xh = nullptr;
+    P omega = P(2.0 / 3.0);
+
+    void build(Arena& ar, int NX, int NKr, const std::vector<double>& cx0, const std::vector<double>& ru_h,
+               const std::vector<double>& rd_h) {
+        NK = NKr;
+        int n = NX;
+        nx.push_back(n);
+        while (n % 2 == 0 && n > kCoarseMax) {
+            n /= 2;
+            nx.push_back(n);
+        }
+        nlev = (int)nx.size();
+        nc = nx.back();
+        ru = ar.alloc<double>(NK);
+        rd = ar.alloc<double>(NK);
+        CK(cudaMemcpy(ru, ru_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(rd, rd_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+        for (int l = 0; l < nlev; l++) {
+            int pl = round_up(nx[l], kPad);
+            pitch.push_back(pl);
+            f.push_back(l == 0 ? nullptr : ar.alloc<P>((size_t)NK * pl));
+            x.push_back(ar.alloc<P>((size_t)NK * pl));
+            y.push_back(ar.alloc<P>((size_t)NK * pl));
+            std::vector<double> c(NK), lo_h(NK), inv_h(NK), cp_h(NK);
+            double sc = std::pow(0.25, l);
+            for (int k = 0; k < NK; k++) c[k] = cx0[k] * sc;
+            factor_line(c, 0.0, lo_h, inv_h, cp_h, ru_h, rd_h);
+            double* dcx = ar.alloc<double>(NK);
+            CK(cudaMemcpy(dcx, c.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+            cx.push_back(dcx);
+            if (l < nlev - 1) {
+                double *dlo = ar.alloc<double>(NK), *dinv = ar.alloc<double>(NK), *dcp = ar.alloc<double>(NK);
+                CK(cudaMemcpy(dlo, lo_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(dinv, inv_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(dcp, cp_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+                lo.push_back(dlo);
+                inv.push_back(dinv);
+                cp.push_back(dcp);
+            } else {
+                lo.push_back(nullptr);
+                inv.push_back(nullptr);
+                cp.push_back(nullptr);
+                build_coarse(ar, c, ru_h, rd_h);
+            }
+        }
+    }
+
+    // Thomas factors of tridiag(-rd, 2c*g + ru + rd, -ru) (g scales the x part
+    // for Fourier modes: g = 1 for line Jacobi, mu_m/2 on the coarsest level).
+    static void factor_line(const std::vector<double>& c, double mu, std::vector<double>& lo,
+                            std::vector<double>& inv, std::vector<double>& cp, const std::vector<double>& ru,
+                            const std::vector<double>& rd) {
+        int NK = (int)c.size();
+        double cprev = 0;
+        for (int k = 0; k < NK; k++) {
+            double xpart = (mu == 0.0) ? 2.0 * c[k] : c[k] * mu;
+            double diag = xpart + ru[k] + rd[k];
+            double l = (k > 0) ? -rd[k] : 0.0;
+            double u = (k < NK - 1) ? -ru[k] : 0.0;
+            double den = diag - l * cprev;
+            inv[k] = 1.0 / den;
+            cp[k] = u * inv[k];
+            lo[k] = l;
+            cprev = cp[k];
+        }
+    }
+
+    void build_coarse(Arena& ar, const std::vector<double>& c, const std::vector<double>& ru_h,
+                      const std::vector<double>& rd_h) {
+        const double pi = 3.14159265358979323846;
+        std::vector<double> Qh((size_t)nc * nc), mu(nc);
+        int m = 0;
+        for (int j = 0; j < nc; j++) Qh[(size_t)j * nc + m] = 1.0 / std::sqrt((double)nc);
+        mu[m++] = 0.0;
+        for (int fr = 1; 2 * fr < nc; fr++) {
+            for (int j = 0; j < nc; j++) {
+                Qh[(size_t)j * nc + m] = std::sqrt(2.0 / nc) * std::cos(2 * pi * fr * j / nc);
+                Qh[(size_t)j * nc + m + 1] = std::sqrt(2.0 / nc) * std::sin(2 * pi * fr * j / nc);
+            }
+            mu[m] = mu[m + 1] = 2.0 - 2.0 * std::cos(2 * pi * fr / nc);
+            m += 2;
+        }
+        if (nc % 2 == 0) {
+            for (int j = 0; j < nc; j++) Qh[(size_t)j * nc + m] = ((j & 1) ? -1.0 : 1.0) / std::sqrt((double)nc);
+            mu[m++] = 4.0;
+        }
+        std::vector<double> lo_a((size_t)nc * NK), inv_a((size_t)nc * NK), cp_a((size_t)nc * NK);
+        for (int q = 0; q < nc; q++) {
+            std::vector<double> lo_h(NK), inv_h(NK), cp_h(NK);
+            // mu == 0 must mean "no x part", not the line-Jacobi default
+            std::vector<double> cz(NK, 0.0);
+            const std::vector<double>& cc = (mu[q] == 0.0) ? cz : c;
+            factor_line(cc, mu[q] == 0.0 ? 1.0 : mu[q], lo_h, inv_h, cp_h, ru_h, rd_h);
+            for (int k = 0; k < NK; k++) {
+                lo_a[(size_t)q * NK + k] = lo_h[k];
+                inv_a[(size_t)q * NK + k] = inv_h[k];
+                cp_a[(size_t)q * NK + k] = cp_h[k];
+            }
+        }
+        Q = ar.alloc<double>((size_t)nc * nc);
+        clo = ar.alloc<double>((size_t)nc * NK);
+        cinv = ar.alloc<double>((size_t)nc * NK);
+        ccp = ar.alloc<double>((size_t)nc * NK);
+        xh = ar.alloc<double>((size_t)nc * NK);
+        CK(cudaMemcpy(Q, Qh.data(), Qh.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(clo, lo_a.data(), lo_a.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(cinv, inv_a.data(), inv_a.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ccp, cp_a.data(), cp_a.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+
+    ZOps zops() const { return ZOps{ru, rd, NK}; }
+
+    // z = M r; returns the buffer holding z (level-0 y, owned by the hierarchy).
+    P* apply(const P* r, cudaStream_t st) {
+        const P* fl = r;
+        for (int l = 0; l < nlev - 1; l++) {
+            SmoothArgs<P> s{nx[l], pitch[l], NK, zops(), cx[l], LineFactors{lo[l], inv[l], cp[l]},
+                            fl, nullptr, nullptr, 0, 0, x[l], omega};
+            k_mg_smooth<P><<<cdiv(nx[l], 128), 128, 0, st>>>(s);
+            CKL();
+            RestrictArgs<P> ra{nx[l], pitch[l], NK, zops(), cx[l], fl, x[l], f[l + 1], pitch[l + 1]};
+            dim3 b(32, 8), g(cdiv(nx[l + 1], 32), cdiv(NK, 8));
+            k_mg_restrict<P><<<g, b, 0, st>>>(ra);
+            CKL();
+            fl = f[l + 1];
+        }
+        int L = nlev - 1;
+        CoarseArgs<P> ca{nc, pitch[L], NK, Q, clo, cinv, ccp, (L == 0) ? r : f[L], (L == 0) ? y[0] : x[L], xh};
+        k_mg_coarse<P><<<1, round_up(nc, 32), 0, st>>>(ca);
+        CKL();
+        if (L == 0) return y[0];
+        for (int l = L - 1; l >= 0; l--) {
+            const P* coarse = (l + 1 == L) ? x[L] : y[l + 1];
+            const P* fl2 = (l == 0) ? r : f[l];
+            SmoothArgs<P> s{nx[l], pitch[l], NK, zops(), cx[l], LineFactors{lo[l], inv[l], cp[l]},
+                            fl2, x[l], coarse, pitch[l + 1], nx[l + 1], y[l], omega};
+            k_mg_smooth<P><<<cdiv(nx[l], 128), 128, 0, st>>>(s);
+            CKL();
+        }
+        return y[0];
+    }
+};
+
+// Preconditioned CG on S d = g in precision P with the level-0 vectors below.
+template <typename P>
+struct PCG {
+    Multigrid<P> mg;
+    int NX = 0, NK = 0, pitch = 0;
+    P *r = nullptr, *p = nullptr, *q = nullptr;
+    double* partial = nullptr;
+    int npart = 0;
+    double* rhow_k = nullptr;
+    CGScalars* sc = nullptr;
+    CGScalars* sc_host = nullptr;
+
+    void build(Arena& ar, int NXr, int NKr, const std::vector<double>& rhou, const std::vector<double>& rhow) {
+        NX = NXr;
+        NK = NKr;
+        std::vector<double> cx0(NK), ru(NK), rd(NK), rw(NK);
+        for (int kk = 0; kk < NK; kk++) {
+            int k = kk + 2;
+            cx0[kk] = 1.0 / rhow[k];
+            ru[kk] = 1.0 / rhou[k];
+            rd[kk] = 1.0 / rhou[k - 1];
+            rw[kk] = rhow[k];
+        }
+        mg.build(ar, NX, NK, cx0, ru, rd);
+        pitch = mg.pitch[0];
+        r = ar.alloc<P>((size_t)NK * pitch);
+        p = ar.alloc<P>((size_t)NK * pitch);
+        q = ar.alloc<P>((size_t)NK * pitch);
+        dim3 g = grid();
+        npart = g.x * g.y;
+        partial = ar.alloc<double>(npart);
+        rhow_k = ar.alloc<double>(NK);
+        CK(cudaMemcpy(rhow_k, rw.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+        sc = ar.alloc<CGScalars>(1);
+        CK(cudaMallocHost(&sc_host, sizeof(CGScalars)));
+    }
+    void release() {
+        if (sc_host) cudaFreeHost(sc_host);
+        sc_host = nullptr;
+    }
+    dim3 block() const { return dim3(64, 4); }
+    dim3 grid() const { return dim3(cdiv(NX, 64), cdiv(NK, 4)); }
+    VecArgs<P> vargs() const { return VecArgs<P>{NX, pitch, NK, mg.zops(), mg.cx[0], rhow_k}; }
+
+    double read_rr(cudaStream_t st) {
+        CK(cudaMemcpyAsync(sc_host, sc, sizeof(CGScalars), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return sc_host->rr;
+    }
+
+    // Solves S x = g. x holds the initial guess when `warm`, else it is zeroed.
+    // Stops when ||rhow (g - S x)|| <= rtol * ||rhow g||_ref where ref2 is the
+    // squared reference norm (||b||^2). Returns iterations; relres out.
+    int solve(const P* g, P* x, bool warm, double ref2, double rtol, int maxit, cudaStream_t st,
+              double* relres) {
+        VecArgs<P> v = vargs();
+        dim3 B = block(), G = grid();
+        if (!warm) CK(cudaMemsetAsync(x, 0, (size_t)NK * pitch * sizeof(P), st));
+        k_cg_residual<P><<<G, B, 0, st>>>(v, g, x, r, partial);
+        CKL();
+        k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR);
+        CKL();
+        double rr = read_rr(st);
+        double target = rtol * std::sqrt(ref2);
+        if (std::sqrt(rr) <= target || ref2 == 0.0) {
+            *relres = (ref2 > 0) ? std::sqrt(rr / ref2) : 0.0;
+            return 0;
+        }
+        P* z = mg.apply(r, st);
+        k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial);
+        CKL();
+        k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RZ);
+        CKL();
+        k_cg_dir<P><<<G, B, 0, st>>>(v, sc, z, p, 1);
+        CKL();
+        int it = 0;
+        for (it = 1; it <= maxit; it++) {
+            k_cg_spmv<P><<<G, B, 0, st>>>(v, p, q, partial);
+            CKL();
+            k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_PQ_ALPHA);
+            CKL();
+            k_cg_update<P><<<G, B, 0, st>>>(v, sc, x, r, p, q, partial);
+            CKL();
+            k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR);
+            CKL();
+            rr = read_rr(st);
+            if (std::sqrt(rr) <= target || !std::isfinite(rr)) break;
+            z = mg.apply(r, st);
+            k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial);
+            CKL();
+            k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_RZ_BETA);
+            CKL();
+            k_cg_dir<P><<<G, B, 0, st>>>(v, sc, z, p, 0);
+            CKL();
+        }
+        *relres = std::sqrt(rr / ref2);
+        return it > maxit ? maxit : it;
+    }
+};
+
+enum { H_ZETA = 0, H_BUOY, H_TH, H_QV, H_QC, H_QR, H_VT, NHIST };
+
+template <typename T>
+struct Fields {
+    T *zeta[2] = {}, *th[2] = {}, *qv[2] = {}, *qc[2] = {}, *qr[2] = {};
+    T *u = nullptr, *w = nullptr, *RKM = nullptr, *RKH = nullptr;
+    T* hist[NHIST][2] = {};
+    T *d_auto = nullptr, *d_accr = nullptr, *d_evap = nullptr, *d_cond = nullptr;
+    T *precip = nullptr, *th_forcing = nullptr;
+};
+
+}  // namespace
+
+// ===========================================================================
+// Context
+
+struct vvm_gpu_ctx {
+    vvm_gpu_desc desc{};
+    int device = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    Dims d{};
+    Consts c{};
+    bool mixed = false;
+    Arena ar;
+    Fields<double> f64;
+    Fields<float> f32;
+    int cur = 0;       // buffer index of the "now" time level
+    int step = 0;
+    bool has_state = false, has_forcing_th = false, has_q = false;
+    // profiles
+    double *rhou = nullptr, *rhow = nullptr, *thvb = nullptr, *thb = nullptr, *qvb = nullptr,
+           *thb_init = nullptr, *qvb0 = nullptr, *pib = nullptr, *pb = nullptr, *lambda2 = nullptr,
+           *z = nullptr, *z_zeta = nullptr, *vt_c1 = nullptr, *vt_fac = nullptr, *pc = nullptr,
+           *dtcgr_th = nullptr, *dtcgr_zeta = nullptr, *q1ls = nullptr, *q2ls = nullptr;
+    double pf1 = 0, pf2 = 0;
+    std::vector<double> h_rhou, h_rhow;
+    double* ubar = nullptr;   // [0] ubarTop, [1] ubarTopp
+    double* dubar = nullptr;  // [2]
+    double *partial = nullptr, *nvp = nullptr;
+    int npart = 0;
+    double* staging = nullptr;   // nx*nz*2 doubles
+    // Poisson
+    bool poisson_ready = false;
+    std::unique_ptr<PCG<double>> pcg64;
+    std::unique_ptr<PCG<float>> pcg32;
+    double *Wf = nullptr, *W = nullptr, *r64 = nullptr;   // level-0 layout, FP64
+    float *g32 = nullptr, *d32 = nullptr;
+    double* wpartial = nullptr;
+    int wnpart = 0;
+    double* sc_host = nullptr;
+    int last_iters = 0;
+    double last_relres = 0;
+    std::string err;
+
+    ~vvm_gpu_ctx() {
+        if (pcg64) pcg64->release();
+        if (pcg32) pcg32->release();
+        if (sc_host) cudaFreeHost(sc_host);
+        if (own) cudaStreamDestroy(own);
+    }
+
+    Profiles profiles() const {
+        return Profiles{rhou, rhow, thvb, thb_init, qvb0, pib, pb, lambda2, vt_c1, vt_fac, pc,
+                        dtcgr_th, dtcgr_zeta, q1ls, q2ls, pf1, pf2};
+    }
+    dim3 blk() const { return dim3(64, 4); }
+    dim3 grid_interior(int k0) const { return dim3(cdiv(d.nx - 2, 64), cdiv(d.nz - 1 - k0, 4)); }
+    dim3 grid_all() const { return dim3(cdiv(d.nx, 64), cdiv(d.nz, 4)); }
+};
+
+namespace {
+
+std::string g_create_error;
+
+int fail(vvm_gpu_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+template <typename T>
+Fields<T>& fields(vvm_gpu_ctx* c);
+template <>
+Fields<double>& fields<double>(vvm_gpu_ctx* c) { return c->f64; }
+template <>
+Fields<float>& fields<float>(vvm_gpu_ctx* c) { return c->f32; }
+
+template <typename T>
+void alloc_fields(vvm_gpu_ctx* c) {
+    Fields<T>& F = fields<T>(c);
+    size_t n = c->d.cells();
+    for (int b = 0; b < 2; b++) {
+        F.zeta[b] = c->ar.alloc<T>(n);
+        F.th[b] = c->ar.alloc<T>(n);
+        F.qv[b] = c->ar.alloc<T>(n);
+        F.qc[b] = c->ar.alloc<T>(n);
+        F.qr[b] = c->ar.alloc<T>(n);
+    }
+    F.u = c->ar.alloc<T>(n);
+    F.w = c->ar.alloc<T>(n);
+    F.RKM = c->ar.alloc<T>(n);
+    F.RKH = c->ar.alloc<T>(n);
+    for (int h = 0; h < NHIST; h++)
+        for (int s = 0; s < 2; s++) F.hist[h][s] = c->ar.alloc<T>(n);
+    F.d_auto = c->ar.alloc<T>(n);
+    F.d_accr = c->ar.alloc<T>(n);
+    F.d_evap = c->ar.alloc<T>(n);
+    F.d_cond = c->ar.alloc<T>(n);
+    F.precip = c->ar.alloc<T>(c->d.nx);
+    F.th_forcing = c->ar.alloc<T>(n);
+}
+
+// ---------------------------------------------------------------- routines
+
+template <typename T>
+void launch_pzeta(vvm_gpu_ctx* c) {
+    Fields<T>& F = fields<T>(c);
+    int now = c->cur, fut = 1 - c->cur;
+    AB2 ab = AB2::of(c->step);
+    PZetaArgs<T> a{c->d, c->c, c->profiles(), F.zeta[now], F.u, F.w, F.th[now], F.qv[now], F.qc[now], F.qr[now],
+                   F.zeta[fut], F.hist[H_ZETA][ab.sn], F.hist[H_ZETA][ab.so], F.hist[H_BUOY][ab.sn],
+                   F.hist[H_BUOY][ab.so], ab};
+    k_pzeta<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(a);
+    CKL();
+}
+
+template <typename T>
+void launch_padv(vvm_gpu_ctx* c, int mask, int nvp_mask, bool vt, bool precip) {
+    Fields<T>& F = fields<T>(c);
+    int now = c->cur, fut = 1 - c->cur;
+    AB2 ab = AB2::of(c->step);
+    PAdvArgs<T> a{};
+    a.d = c->d;
+    a.c = c->c;
+    a.p = c->profiles();
+    a.u = F.u;
+    a.w = F.w;
+    T* nows[4] = {F.th[now], F.qv[now], F.qc[now], F.qr[now]};
+    T* futs[4] = {F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]};
+    int hid[4] = {H_TH, H_QV, H_QC, H_QR};
+    for (int f = 0; f < 4; f++) {
+        a.now[f] = nows[f];
+        a.fut[f] = futs[f];
+        a.hn[f] = F.hist[hid[f]][ab.sn];
+        a.ho[f] = F.hist[hid[f]][ab.so];
+    }
+    a.hvt_n = F.hist[H_VT][ab.sn];
+    a.hvt_o = F.hist[H_VT][ab.so];
+    a.precip = F.precip;
+    a.partial = c->partial;
+    a.mask = mask;
+    a.nvp_mask = nvp_mask;
+    a.do_vt = vt;
+    a.do_precip = precip;
+    a.ab = ab;
+    dim3 g = c->grid_interior(1);
+    k_padv<T><<<g, c->blk(), 0, c->stream>>>(a);
+    CKL();
+    if (nvp_mask) {
+        k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp);
+        CKL();
+    }
+}
+
+template <typename T>
+void launch_apply(vvm_gpu_ctx* c, int mask, int nvp_mask, bool forcing, bool halo) {
+    Fields<T>& F = fields<T>(c);
+    int fut = 1 - c->cur;
+    ApplyArgs<T> a{};
+    a.d = c->d;
+    a.c = c->c;
+    a.p = c->profiles();
+    a.fut[0] = F.th[fut];
+    a.fut[1] = F.qv[fut];
+    a.fut[2] = F.qc[fut];
+    a.fut[3] = F.qr[fut];
+    a.nvp = c->nvp;
+    a.th_forcing = F.th_forcing;
+    a.mask = mask;
+    a.nvp_mask = nvp_mask;
+    a.forcing = forcing && c->has_q;
+    // status_for_adding_forcing (Iteration.cpp:276-277)
+    a.forcing_th = forcing && c->has_forcing_th && (c->step * c->desc.dt <= c->desc.addforcingtime);
+    a.halo = halo;
+    k_apply<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(a);
+    CKL();
+}
+
+template <typename T>
+void launch_halo_all(vvm_gpu_ctx* c) {
+    Fields<T>& F = fields<T>(c);
+    int fut = 1 - c->cur;
+    HaloArgs<T> a{c->d, F.zeta[fut], F.w, {F.th[fut], F.u, F.qv[fut], F.qc[fut], F.qr[fut]}};
+    k_halo_all<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(a);
+    CKL();
+}
+
+template <typename T>
+void launch_pubartop(vvm_gpu_ctx* c) {
+    Fields<T>& F = fields<T>(c);
+    PubarArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.RKM, c->ubar, c->dubar, AB2::of(c->step)};
+    k_pubartop<T><<<1, 1024, 0, c->stream>>>(a);
+    CKL();
+}
+
+template <typename T>
+void launch_kessler(vvm_gpu_ctx* c, bool halo) {
+    Fields<T>& F = fields<T>(c);
+    int fut = 1 - c->cur;
+    KesslerArgs<T> a{c->d, c->c, c->profiles(), F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut],
+                     F.d_auto, F.d_accr, F.d_evap, F.d_cond, c->partial, 1};
+    dim3 g = c->grid_interior(1);
+    k_kessler<T><<<g, c->blk(), 0, c->stream>>>(a);
+    CKL();
+    k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp);
+    CKL();
+    launch_apply<T>(c, halo ? (F_TH | F_QV | F_QC | F_QR) : (F_QV | F_QC | F_QR), F_QV | F_QC | F_QR, false, halo);
+}
+
+template <typename T>
+void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
+    Fields<T>& F = fields<T>(c);
+    int fut = 1 - c->cur;
+    RKArgs<T> r{c->d, c->c, c->profiles(), F.u, F.w, F.th[fut], F.RKM, F.RKH};
+    k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r);
+    CKL();
+    GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
+                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0};
+    k_gs_diffuse<T><<<5, kGSThreads, 0, c->stream>>>(g);
+    CKL();
+}
+
+template <typename T>
+void launch_nudge(vvm_gpu_ctx* c, bool th_zeta, bool qv) {
+    Fields<T>& F = fields<T>(c);
+    int now = c->cur, fut = 1 - c->cur;
+    NudgeArgs<T> a{c->d, c->c, c->profiles(), F.th[fut], F.zeta[fut], F.qv[fut], F.qv[now],
+                   th_zeta ? 1 : 0, (th_zeta && c->desc.case_id != 2) ? 1 : 0,
+                   qv ? c->desc.moisture_nudge_time : 0.0};
+    k_nudge<T><<<c->grid_all(), c->blk(), 0, c->stream>>>(a);
+    CKL();
+}
+
+template <typename T>
+void launch_update_mean(vvm_gpu_ctx* c, bool rotate) {
+    Fields<T>& F = fields<T>(c);
+    int fut = 1 - c->cur;
+    MeanArgs<T> a{c->d, F.th[fut], F.qv[fut], c->thb, c->qvb, c->thvb, c->ubar, rotate ? 1 : 0};
+    k_update_mean<T><<<c->d.nz - 2, 256, 0, c->stream>>>(a);
+    CKL();
+}
+
+// ---------------------------------------------------------------- Poisson
+
+void ensure_poisson(vvm_gpu_ctx* c) {
+    if (c->poisson_ready) return;
+    int NX = c->d.nx - 2, NK = c->d.nz - 3;
+    c->pcg64.reset(new PCG<double>());
+    c->pcg64->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
+    int pitch = c->pcg64->pitch;
+    c->Wf = c->ar.alloc<double>((size_t)NK * pitch);
+    c->W = c->ar.alloc<double>((size_t)NK * pitch);
+    c->r64 = c->ar.alloc<double>((size_t)NK * pitch);
+    if (c->mixed) {
+        c->pcg32.reset(new PCG<float>());
+        c->pcg32->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
+        c->g32 = c->ar.alloc<float>((size_t)NK * pitch);
+        c->d32 = c->ar.alloc<float>((size_t)NK * pitch);
+    }
+    dim3 g(cdiv(NX, 64), cdiv(NK, 4));
+    c->wnpart = g.x * g.y;
+    c->wpartial = c->ar.alloc<double>(c->wnpart);
+    if (!c->sc_host) CK(cudaMallocHost(&c->sc_host, sizeof(double)));
+    c->poisson_ready = true;
+}
+
+double read_scalar(vvm_gpu_ctx* c, const double* dptr) {
+    CK(cudaMemcpyAsync(c->sc_host, dptr, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return *c->sc_host;
+}
+
+// Solves S W = Wf (FP64 rhs in c->Wf, ||b||^2 = bb) into c->W.
+int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
+    int maxit = c->desc.poisson_maxit > 0 ? c->desc.poisson_maxit : 200;
+    if (bb == 0.0) {
+        CK(cudaMemsetAsync(c->W, 0, (size_t)c->pcg64->NK * c->pcg64->pitch * sizeof(double), c->stream));
+        c->last_iters = 0;
+        c->last_relres = 0.0;
+        return VVM_GPU_OK;
+    }
+    if (!c->mixed) {
+        double rel = 0;
+        int it = c->pcg64->solve(c->Wf, c->W, warm, bb, tol, maxit, c->stream, &rel);
+        c->last_iters = it;
+        c->last_relres = rel;
+        return (rel <= tol) ? VVM_GPU_OK : VVM_GPU_ENOCONV;
+    }
+    // Mixed precision: FP64 residual and correction, FP32 inner PCG.
+    PCG<double>& P64 = *c->pcg64;
+    PCG<float>& P32 = *c->pcg32;
+    VecArgs<double> v = P64.vargs();
+    dim3 B = P64.block(), G = P64.grid();
+    if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), c->stream));
+    int total = 0;
+    double rel = 0;
+    for (int outer = 0; outer < 20; outer++) {
+        k_cg_residual<double><<<G, B, 0, c->stream>>>(v, c->Wf, c->W, c->r64, c->wpartial);
+        CKL();
+        k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, P64.sc, CG_SET_RR);
+        CKL();
+        double rr = P64.read_rr(c->stream);
+        rel = std::sqrt(rr / bb);
+        if (rel <= tol || !std::isfinite(rel) || total >= maxit) break;
+        k_to_float<<<G, B, 0, c->stream>>>(P64.NX, P64.NK, P64.pitch, c->r64, c->g32);
+        CKL();
+        double irel = 0;
+        // inner: reduce the FP64 residual by ~1e-4 relative to itself
+        int it = P32.solve(c->g32, c->d32, false, rr, 1e-4, maxit, c->stream, &irel);
+        total += std::max(it, 1);
+        k_refine_add<<<G, B, 0, c->stream>>>(P64.NX, P64.NK, P64.pitch, c->W, c->d32);
+        CKL();
+    }
+    c->last_iters = total;
+    c->last_relres = rel;
+    return (rel <= tol) ? VVM_GPU_OK : VVM_GPU_ENOCONV;
+}
+
+template <typename T>
+int launch_cal_w(vvm_gpu_ctx* c) {
+    ensure_poisson(c);
+    Fields<T>& F = fields<T>(c);
+    int fut = 1 - c->cur;
+    int NX = c->d.nx - 2, NK = c->d.nz - 3;
+    int pitch = c->pcg64->pitch;
+    dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
+    k_poisson_rhs<T><<<G, B, 0, c->stream>>>(c->d, c->c.dx, c->rhow, F.zeta[fut], c->Wf, pitch, c->wpartial);
+    CKL();
+    k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, c->pcg64->sc, CG_SET_BB);
+    CKL();
+    CK(cudaMemcpyAsync(c->sc_host, &c->pcg64->sc->bb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double bb = *c->sc_host;
+    int rc = solve_w(c, bb, c->desc.poisson_tol, c->desc.warm_start != 0);
+    k_w_from_W<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(c->d, c->rhow, c->W, pitch, F.w);
+    CKL();
+    return rc;
+}
+
+template <typename T>
+void launch_cal_u(vvm_gpu_ctx* c) {
+    Fields<T>& F = fields<T>(c);
+    int fut = 1 - c->cur;
+    CalUArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.zeta[fut], c->ubar};
+    k_cal_u_top<T><<<1, kCalUThreads, 0, c->stream>>>(a);
+    CKL();
+    k_cal_u_columns<T><<<cdiv(c->d.nx - 2, 128), 128, 0, c->stream>>>(a);
+    CKL();
+}
+
+// ---------------------------------------------------------------- one step
+
+template <typename T>
+int run_step(vvm_gpu_ctx* c) {
+    c->step++;                                                 // Iteration.cpp:246
+    launch_pzeta<T>(c);                                        // pzeta_pt
+    launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
+    launch_apply<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true); // NVP, AddForcing, halos
+    launch_pubartop<T>(c);                                     // pubarTop_pt
+    int rc = launch_cal_w<T>(c);                               // cal_w
+    launch_cal_u<T>(c);                                        // cal_u
+    launch_kessler<T>(c, true);                                // Kessler + NVP x3 + halos
+    // The first updateMean of the step (Iteration.cpp:408) only writes thb,
+    // qvb, thvb, which nextTimeStep's updateMean overwrites before any read.
+    launch_turbulence<T>(c, true);                             // RKM_RKH + diffusion + theta/zeta nudging
+    if (c->desc.moisture_nudge_time != 0.0) launch_nudge<T>(c, false, true);
+    launch_update_mean<T>(c, true);                            // nextTimeStep: means, ubarTop
+    c->cur = 1 - c->cur;                                       // time levels by pointer swap
+    return rc;
+}
+
+// ---------------------------------------------------------------- transfer
+
+template <typename T>
+void upload_field(vvm_gpu_ctx* c, const double* host, int sk, int off, T* dst) {
+    size_t n = (size_t)c->d.nx * c->d.nz * sk;
+    CK(cudaMemcpyAsync(c->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
+    k_from_host_layout<T><<<g, b, 0, c->stream>>>(c->d, c->staging, sk, off, dst);
+    CKL();
+}
+
+template <typename T>
+void download_field(vvm_gpu_ctx* c, const T* src, int sk, int off, double* host, bool first_of_pair) {
+    size_t n = (size_t)c->d.nx * c->d.nz * sk;
+    dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
+    k_to_host_layout<T><<<g, b, 0, c->stream>>>(c->d, src, sk, off, c->staging);
+    CKL();
+    if (!first_of_pair) {
+        CK(cudaMemcpyAsync(host, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+}
+
+void upload_profile(vvm_gpu_ctx* c, const double* h, double* dptr) {
+    CK(cudaMemcpy(dptr, h, c->d.nz * sizeof(double), cudaMemcpyHostToDevice));
+}
+
+template <typename T>
+int upload_prognostic_t(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
+    Fields<T>& F = fields<T>(c);
+    int now = c->cur, fut = 1 - c->cur;
+    const double* req[] = {s->zeta, s->th, s->qv, s->qc, s->qr, s->u, s->w};
+    for (const double* p : req)
+        if (!p) return fail(c, VVM_GPU_EINVAL, "upload: prognostic field pointer is NULL");
+    upload_field<T>(c, s->zeta, 1, 0, F.zeta[now]);
+    upload_field<T>(c, s->th, 1, 0, F.th[now]);
+    upload_field<T>(c, s->qv, 1, 0, F.qv[now]);
+    upload_field<T>(c, s->qc, 1, 0, F.qc[now]);
+    upload_field<T>(c, s->qr, 1, 0, F.qr[now]);
+    upload_field<T>(c, s->u, 1, 0, F.u);
+    upload_field<T>(c, s->w, 1, 0, F.w);
+    (void)fut;
+    return VVM_GPU_OK;
+}
+
+template <typename T>
+int upload_state_t(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
+    Fields<T>& F = fields<T>(c);
+    int rc = upload_prognostic_t<T>(c, s);
+    if (rc) return rc;
+    int fut = 1 - c->cur;
+    size_t n = c->d.cells();
+    auto up_or_zero = [&](const double* h, int sk, int off, T* dst) {
+        if (h) upload_field<T>(c, h, sk, off, dst);
+        else CK(cudaMemsetAsync(dst, 0, n * sizeof(T), c->stream));
+    };
+    up_or_zero(s->zetap, 1, 0, F.zeta[fut]);
+    up_or_zero(s->thp, 1, 0, F.th[fut]);
+    up_or_zero(s->qvp, 1, 0, F.qv[fut]);
+    up_or_zero(s->qcp, 1, 0, F.qc[fut]);
+    up_or_zero(s->qrp, 1, 0, F.qr[fut]);
+    up_or_zero(s->RKM, 1, 0, F.RKM);
+    up_or_zero(s->RKH, 1, 0, F.RKH);
+    double* hs[NHIST] = {s->dzeta_advect, s->dth_buoyancy, s->dth_advect, s->dqv_advect,
+                         s->dqc_advect, s->dqr_advect, s->dqr_VT};
+    for (int h = 0; h < NHIST; h++)
+        for (int sl = 0; sl < 2; sl++) up_or_zero(hs[h], 2, sl, F.hist[h][sl]);
+    c->has_forcing_th = (s->init_th_forcing != nullptr);
+    up_or_zero(s->init_th_forcing, 1, 0, F.th_forcing);
+    if (s->precip) {
+        std::vector<T> pr(c->d.nx);
+        for (int i = 0; i < c->d.nx; i++) pr[i] = T(s->precip[i]);
+        CK(cudaMemcpy(F.precip, pr.data(), c->d.nx * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    return VVM_GPU_OK;
+}
+
+// Coefficient profiles (double) with the reference's expressions.
+int upload_profiles(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
+    const int nz = c->d.nz;
+    const double* req[] = {s->rhou, s->rhow, s->thb, s->thvb, s->qvb, s->pib, s->pb,
+                           s->thb_init, s->qvb0, s->z, s->z_zeta, s->lambda2};
+    for (const double* p : req)
+        if (!p) return fail(c, VVM_GPU_EINVAL, "upload: profile pointer is NULL");
+    upload_profile(c, s->rhou, c->rhou);
+    upload_profile(c, s->rhow, c->rhow);
+    upload_profile(c, s->thb, c->thb);
+    upload_profile(c, s->thvb, c->thvb);
+    upload_profile(c, s->qvb, c->qvb);
+    upload_profile(c, s->pib, c->pib);
+    upload_profile(c, s->pb, c->pb);
+    upload_profile(c, s->thb_init, c->thb_init);
+    upload_profile(c, s->qvb0, c->qvb0);
+    upload_profile(c, s->z, c->z);
+    upload_profile(c, s->z_zeta, c->z_zeta);
+    upload_profile(c, s->lambda2, c->lambda2);
+    const vvm_gpu_desc& D = c->desc;
+    std::vector<double> vt1(nz), vtf(nz), pc(nz), cth(nz, 0.0), cze(nz, 0.0), q1(nz, 0.0), q2(nz, 0.0);
+    for (int k = 0; k < nz; k++) {
+        vt1[k] = 1E-3 * s->rhow[k] * 0.5;                            // Advection.cpp:165
+        vtf[k] = std::pow(s->rhow[k] / s->rhow[1], -0.5);
+        pc[k] = 380. / (std::pow(s->pib[k], D.cp / D.rd) * D.p0);    // MicroPhysics.cpp:10
+    }
+    int ks = (int)(12000. / D.dz + 1);                               // NumericalProcess.cpp:62
+    if (ks < nz - 1 && (nz - 1) - ks >= 0) {
+        const double* z = s->z;
+        const double* zz = s->z_zeta;
+        int kb = (nz - 1) - ks;
+        for (int k = ks; k < nz - 1; k++) {
+            double CGR = (1. / 3600.) * (z[k] - z[kb]) / (z[nz - 1] - z[kb]);
+            cth[k] = D.dt * CGR;
+            if (D.case_id != 2) {
+                double CGRz = (1. / 360.) * (zz[k] - zz[kb]) / (zz[nz - 1] - zz[kb]);
+                cze[k] = D.dt * CGRz;
+            }
+        }
+    }
+    c->has_q = false;
+    if (s->Q1LS) { q1.assign(s->Q1LS, s->Q1LS + nz); c->has_q = true; }
+    if (s->Q2LS) { q2.assign(s->Q2LS, s->Q2LS + nz); c->has_q = true; }
+    upload_profile(c, vt1.data(), c->vt_c1);
+    upload_profile(c, vtf.data(), c->vt_fac);
+    upload_profile(c, pc.data(), c->pc);
+    upload_profile(c, cth.data(), c->dtcgr_th);
+    upload_profile(c, cze.data(), c->dtcgr_zeta);
+    upload_profile(c, q1.data(), c->q1ls);
+    upload_profile(c, q2.data(), c->q2ls);
+    c->pf1 = 1E-3 * s->rhou[1];                                      // Iteration.cpp:115
+    c->pf2 = std::pow(s->rhou[1] / s->rhow[1], -0.5);
+    bool changed = c->h_rhou.empty() ||
+                   !std::equal(c->h_rhou.begin(), c->h_rhou.end(), s->rhou) ||
+                   !std::equal(c->h_rhow.begin(), c->h_rhow.end(), s->rhow);
+    c->h_rhou.assign(s->rhou, s->rhou + nz);
+    c->h_rhow.assign(s->rhow, s->rhow + nz);
+    if (changed && c->poisson_ready) {
+        // the elliptic operator depends on rhou/rhow: rebuild on next use
+        c->poisson_ready = false;
+        c->pcg64.reset();
+        c->pcg32.reset();
+    }
+    double ub[2] = {s->ubarTop, s->ubarTopp};
+    CK(cudaMemcpy(c->ubar, ub, sizeof(ub), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->dubar, s->dubarTop_advect, 2 * sizeof(double), cudaMemcpyHostToDevice));
+    c->step = s->step;
+    return VVM_GPU_OK;
+}
+
+template <typename T>
+int download_prognostic_t(vvm_gpu_ctx* c, vvm_gpu_host_state* s) {
+    Fields<T>& F = fields<T>(c);
+    int now = c->cur;
+    struct { double* h; T* dptr; } m[] = {{s->zeta, F.zeta[now]}, {s->th, F.th[now]}, {s->qv, F.qv[now]},
+                                           {s->qc, F.qc[now]}, {s->qr, F.qr[now]}, {s->u, F.u}, {s->w, F.w}};
+    for (auto& e : m)
+        if (e.h) download_field<T>(c, e.dptr, 1, 0, e.h, false);
+    return VVM_GPU_OK;
+}
+
+template <typename T>
+int download_state_t(vvm_gpu_ctx* c, vvm_gpu_host_state* s) {
+    Fields<T>& F = fields<T>(c);
+    download_prognostic_t<T>(c, s);
+    int fut = 1 - c->cur;
+    struct { double* h; T* dptr; } m[] = {{s->zetap, F.zeta[fut]}, {s->thp, F.th[fut]}, {s->qvp, F.qv[fut]},
+                                           {s->qcp, F.qc[fut]}, {s->qrp, F.qr[fut]}, {s->RKM, F.RKM},
+                                           {s->RKH, F.RKH}};
+    for (auto& e : m)
+        if (e.h) download_field<T>(c, e.dptr, 1, 0, e.h, false);
+    double* hs[NHIST] = {s->dzeta_advect, s->dth_buoyancy, s->dth_advect, s->dqv_advect,
+                         s->dqc_advect, s->dqr_advect, s->dqr_VT};
+    for (int h = 0; h < NHIST; h++) {
+        if (!hs[h]) continue;
+        download_field<T>(c, F.hist[h][0], 2, 0, hs[h], true);
+        download_field<T>(c, F.hist[h][1], 2, 1, hs[h], false);
+    }
+    auto down_prof = [&](double* h, const double* dptr) {
+        if (h) CK(cudaMemcpy(h, dptr, c->d.nz * sizeof(double), cudaMemcpyDeviceToHost));
+    };
+    CK(cudaStreamSynchronize(c->stream));
+    down_prof(s->thb, c->thb);
+    down_prof(s->qvb, c->qvb);
+    down_prof(s->thvb, c->thvb);
+    down_prof(s->rhou, c->rhou);
+    down_prof(s->rhow, c->rhow);
+    if (s->precip) {
+        std::vector<T> pr(c->d.nx);
+        CK(cudaMemcpy(pr.data(), F.precip, c->d.nx * sizeof(T), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < c->d.nx; i++) s->precip[i] = (double)pr[i];
+    }
+    double ub[2];
+    CK(cudaMemcpy(ub, c->ubar, sizeof(ub), cudaMemcpyDeviceToHost));
+    s->ubarTop = ub[0];
+    s->ubarTopp = ub[1];
+    CK(cudaMemcpy(s->dubarTop_advect, c->dubar, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+    s->step = c->step;
+    return VVM_GPU_OK;
+}
+
+// Runs `fn` with the context's device current, mapping exceptions to statuses.
+template <typename Fn>
+int guarded(vvm_gpu_ctx* c, Fn fn) {
+    if (!c) return VVM_GPU_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    int rc;
+    try {
+        rc = fn();
+    } catch (const CudaError& e) {
+        rc = fail(c, VVM_GPU_ECUDA, e.msg);
+    }
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+#define DISPATCH(c, fn) ((c)->mixed ? fn<float> : fn<double>)
+
+int need_state(vvm_gpu_ctx* c) {
+    return c->has_state ? VVM_GPU_OK : fail(c, VVM_GPU_ESTATE, "no state uploaded");
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+
+extern "C" {
+
+void vvm_gpu_desc_default(vvm_gpu_desc* d, int NX, int NZ, double dx, double dz, double dt) {
+    std::memset(d, 0, sizeof(*d));
+    d->NX = NX;
+    d->NZ = NZ;
+    d->dx = dx;
+    d->dz = dz;
+    d->dt = dt;
+    d->gravity = 9.80665;
+    d->cp = 1003.5;
+    d->cv = 716.5;
+    d->rd = 287.;
+    d->lv = 2.5E6;
+    d->p0 = 1E5;
+    d->psurf = 96500.;
+    d->poisson_tol = 1e-10;
+    d->poisson_maxit = 200;
+    d->case_id = 1;
+    d->precision = VVM_PREC_FP64;
+    d->solver = VVM_SOLVER_MGPCG;
+    d->warm_start = 1;
+}
+
+int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
+    if (!desc || !out) return fail(nullptr, VVM_GPU_EINVAL, "create: NULL argument");
+    *out = nullptr;
+    const vvm_gpu_desc& D = *desc;
+    if (D.NX < 4 || D.NZ < 4) return fail(nullptr, VVM_GPU_EINVAL, "create: NX and NZ must be >= 4");
+    if (D.NX > kGSThreads * kGSMaxPerThread)
+        return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
+    if (!(D.dx > 0) || !(D.dz > 0) || !(D.dt > 0)) return fail(nullptr, VVM_GPU_EINVAL, "create: dx, dz, dt must be > 0");
+    if (D.precision != VVM_PREC_FP64 && D.precision != VVM_PREC_MIXED)
+        return fail(nullptr, VVM_GPU_EINVAL, "create: unknown precision");
+    if (D.solver != VVM_SOLVER_MGPCG && D.solver != VVM_SOLVER_LEARNED)
+        return fail(nullptr, VVM_GPU_EINVAL, "create: unknown solver");
+    std::unique_ptr<vvm_gpu_ctx> c(new vvm_gpu_ctx());
+    c->desc = D;
+    c->device = device;
+    c->mixed = (D.precision == VVM_PREC_MIXED);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    try {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+        c->stream = c->own;
+        c->d.nx = D.NX + 2;
+        c->d.nz = D.NZ + 2;
+        c->d.pitch = round_up(c->d.nx, kPad);
+        Consts& k = c->c;
+        k.dx = D.dx;
+        k.dz = D.dz;
+        k.dt = D.dt;
+        k.rdx = 1.0 / D.dx;                      // Declare.hpp:80-83
+        k.r2dx = k.rdx / 2.0;
+        k.rdz = 1.0 / D.dz;
+        k.r2dz = k.rdz / 2.0;
+        k.rdx2 = k.rdx * k.rdx;
+        k.rdz2 = k.rdz * k.rdz;
+        k.gravity = D.gravity;
+        k.cp = D.cp;
+        k.cv = D.cv;
+        k.rd = D.rd;
+        k.lv = D.lv;
+        k.p0 = D.p0;
+        if (c->mixed) alloc_fields<float>(c.get());
+        else alloc_fields<double>(c.get());
+        int nz = c->d.nz;
+        double** profs[] = {&c->rhou, &c->rhow, &c->thvb, &c->thb, &c->qvb, &c->thb_init, &c->qvb0,
+                            &c->pib, &c->pb, &c->lambda2, &c->z, &c->z_zeta, &c->vt_c1, &c->vt_fac,
+                            &c->pc, &c->dtcgr_th, &c->dtcgr_zeta, &c->q1ls, &c->q2ls};
+        for (double** p : profs) *p = c->ar.alloc<double>(nz);
+        c->ubar = c->ar.alloc<double>(2);
+        c->dubar = c->ar.alloc<double>(2);
+        dim3 g = c->grid_interior(1);
+        c->npart = g.x * g.y;
+        c->partial = c->ar.alloc<double>((size_t)c->npart * 6);
+        c->nvp = c->ar.alloc<double>(6);
+        c->staging = c->ar.alloc<double>((size_t)c->d.nx * c->d.nz * 2);
+    } catch (const CudaError& e) {
+        cudaSetDevice(prev);
+        return fail(nullptr, VVM_GPU_ECUDA, e.msg);
+    }
+    cudaSetDevice(prev);
+    *out = c.release();
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_destroy(vvm_gpu_ctx* ctx) {
+    if (!ctx) return VVM_GPU_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+    cudaSetDevice(prev);
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_set_stream(vvm_gpu_ctx* ctx, void* stream) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own;
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_synchronize(vvm_gpu_ctx* ctx) {
+    return guarded(ctx, [&] { CK(cudaStreamSynchronize(ctx->stream)); return VVM_GPU_OK; });
+}
+
+int vvm_gpu_last_error(vvm_gpu_ctx* ctx, char* buf, size_t len) {
+    const std::string& m = ctx ? ctx->err : g_create_error;
+    if (buf && len) {
+        std::snprintf(buf, len, "%s", m.c_str());
+    }
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_upload_state(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st) {
+    if (!st) return fail(ctx, VVM_GPU_EINVAL, "upload: NULL state");
+    return guarded(ctx, [&] {
+        int rc = upload_profiles(ctx, st);
+        if (rc) return rc;
+        rc = DISPATCH(ctx, upload_state_t)(ctx, st);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->has_state = true;
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_download_state(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
+    if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
+    return guarded(ctx, [&] { return need_state(ctx) ? need_state(ctx) : DISPATCH(ctx, download_state_t)(ctx, st); });
+}
+
+int vvm_gpu_upload_prognostic(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st) {
+    if (!st) return fail(ctx, VVM_GPU_EINVAL, "upload: NULL state");
+    return guarded(ctx, [&] { return need_state(ctx) ? need_state(ctx) : DISPATCH(ctx, upload_prognostic_t)(ctx, st); });
+}
+
+int vvm_gpu_download_prognostic(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
+    if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
+    return guarded(ctx, [&] { return need_state(ctx) ? need_state(ctx) : DISPATCH(ctx, download_prognostic_t)(ctx, st); });
+}
+
+int vvm_gpu_set_step(vvm_gpu_ctx* ctx, int step) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    ctx->step = step;
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_get_step(vvm_gpu_ctx* ctx, int* step) {
+    if (!ctx || !step) return VVM_GPU_EINVAL;
+    *step = ctx->step;
+    return VVM_GPU_OK;
+}
+
+#define ROUTINE(name, ...)                                                    \
+    int name(vvm_gpu_ctx* ctx) {                                              \
+        return guarded(ctx, [&]() -> int {                                    \
+            if (int rc = need_state(ctx)) return rc;                          \
+            __VA_ARGS__;                                                      \
+        });                                                                   \
+    }
+
+ROUTINE(vvm_gpu_pzeta, { DISPATCH(ctx, launch_pzeta)(ctx); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_pth, {
+    DISPATCH(ctx, launch_padv)(ctx, F_TH, 0, false, false);
+    DISPATCH(ctx, launch_apply)(ctx, F_TH, 0, false, true);
+    return VVM_GPU_OK;
+})
+ROUTINE(vvm_gpu_pqv, {
+    DISPATCH(ctx, launch_padv)(ctx, F_QV, F_QV, false, false);
+    DISPATCH(ctx, launch_apply)(ctx, F_QV, F_QV, false, true);
+    return VVM_GPU_OK;
+})
+ROUTINE(vvm_gpu_pqc, {
+    DISPATCH(ctx, launch_padv)(ctx, F_QC, F_QC, false, false);
+    DISPATCH(ctx, launch_apply)(ctx, F_QC, F_QC, false, true);
+    return VVM_GPU_OK;
+})
+ROUTINE(vvm_gpu_pqr, {
+    DISPATCH(ctx, launch_padv)(ctx, F_QR, F_QR, true, true);
+    DISPATCH(ctx, launch_apply)(ctx, F_QR, F_QR, false, true);
+    return VVM_GPU_OK;
+})
+ROUTINE(vvm_gpu_add_forcing, { DISPATCH(ctx, launch_apply)(ctx, F_TH | F_QV, 0, true, false); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_halo_all, { DISPATCH(ctx, launch_halo_all)(ctx); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_pubartop, { DISPATCH(ctx, launch_pubartop)(ctx); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_cal_w, { return DISPATCH(ctx, launch_cal_w)(ctx); })
+ROUTINE(vvm_gpu_cal_u, { DISPATCH(ctx, launch_cal_u)(ctx); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_kessler, { DISPATCH(ctx, launch_kessler)(ctx, false); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_update_mean, { DISPATCH(ctx, launch_update_mean)(ctx, false); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_turbulence, { DISPATCH(ctx, launch_turbulence)(ctx, false); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_nudge, {
+    DISPATCH(ctx, launch_nudge)(ctx, true, ctx->desc.moisture_nudge_time != 0.0);
+    return VVM_GPU_OK;
+})
+ROUTINE(vvm_gpu_next_step, {
+    DISPATCH(ctx, launch_update_mean)(ctx, true);
+    ctx->cur = 1 - ctx->cur;
+    return VVM_GPU_OK;
+})
+
+int vvm_gpu_step(vvm_gpu_ctx* ctx, int nsteps) {
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        if (nsteps < 0) return fail(ctx, VVM_GPU_EINVAL, "step: nsteps < 0");
+        int worst = VVM_GPU_OK;
+        for (int s = 0; s < nsteps; s++) {
+            int rc = DISPATCH(ctx, run_step)(ctx);
+            if (rc != VVM_GPU_OK) worst = rc;
+        }
+        if (worst == VVM_GPU_ENOCONV) fail(ctx, worst, "cal_w: Poisson solve did not reach its tolerance");
+        return worst;
+    });
+}
+
+int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_W, double tol, int* iters,
+                                 double* relres) {
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        ensure_poisson(ctx);
+        int NX = ctx->d.nx - 2, NK = ctx->d.nz - 3, pitch = ctx->pcg64->pitch;
+        dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
+        k_rhs_from_b<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->rhow, d_b, ctx->Wf, pitch, ctx->wpartial);
+        CKL();
+        k_cg_scalar<<<1, 1024, 0, ctx->stream>>>(ctx->wpartial, ctx->wnpart, ctx->pcg64->sc, CG_SET_BB);
+        CKL();
+        double bb = read_scalar(ctx, &ctx->pcg64->sc->bb);
+        bool warm = ctx->desc.warm_start != 0;
+        if (warm) {
+            k_unpack_solution<<<G, B, 0, ctx->stream>>>(NX, NK, d_W, ctx->W, pitch);
+            CKL();
+        }
+        int rc = solve_w(ctx, bb, tol, warm);
+        k_pack_solution<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->W, pitch, d_W);
+        CKL();
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (iters) *iters = ctx->last_iters;
+        if (relres) *relres = ctx->last_relres;
+        if (rc == VVM_GPU_ENOCONV) fail(ctx, rc, "poisson_solve: tolerance not reached");
+        return rc;
+    });
+}
+
+int vvm_gpu_poisson_solve(vvm_gpu_ctx* ctx, const double* b, double* W, double tol, int* iters,
+                          double* relres) {
+    if (!b || !W) return fail(ctx, VVM_GPU_EINVAL, "poisson_solve: NULL argument");
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        size_t n = (size_t)(ctx->d.nx - 2) * (ctx->d.nz - 3);
+        double* db = ctx->staging;
+        double* dw = ctx->staging + n;
+        CK(cudaMemcpyAsync(db, b, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(dw, W, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        int rc = vvm_gpu_poisson_solve_device(ctx, db, dw, tol, iters, relres);
+        CK(cudaMemcpyAsync(W, dw, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return rc;
+    });
+}
+
+int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    if (iters) *iters = ctx->last_iters;
+    if (relres) *relres = ctx->last_relres;
+    return VVM_GPU_OK;
+}
+
+}  // extern "C"

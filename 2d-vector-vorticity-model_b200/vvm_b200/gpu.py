@@ -1,0 +1,287 @@
+"""ctypes binding of libvvmgpu.so (include/vvm_gpu.h).
+
+The host side mirrors the reference's own objects: a ``VVMGpu`` owns one
+device context built from a ``vvm_gpu_desc`` (Config_VVM, src/Declare.hpp:27),
+takes and returns states in the reference model's [nx][nz] layout
+(``VVMState``), and exposes one method per reference routine of
+vvm::Iteration::TimeMarching (src/Iteration.cpp:262-434) plus the fused
+``step``. Failures raise ``VVMGpuError`` with the library's message.
+
+There is no CPU fallback: loading fails loudly when the library or a GPU is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from .initial_state import HIST, VVMState
+
+PKG = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG / "lib" / "libvvmgpu.so"
+
+VVM_PREC_FP64, VVM_PREC_MIXED = 0, 1
+VVM_SOLVER_MGPCG, VVM_SOLVER_LEARNED = 0, 1
+STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOCONV", 4: "ESTATE"}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class VVMGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [("NX", ctypes.c_int), ("NZ", ctypes.c_int),
+                ("dx", ctypes.c_double), ("dz", ctypes.c_double), ("dt", ctypes.c_double),
+                ("gravity", ctypes.c_double), ("cp", ctypes.c_double), ("cv", ctypes.c_double),
+                ("rd", ctypes.c_double), ("lv", ctypes.c_double), ("p0", ctypes.c_double),
+                ("psurf", ctypes.c_double), ("poisson_tol", ctypes.c_double),
+                ("poisson_maxit", ctypes.c_int), ("case_id", ctypes.c_int),
+                ("moisture_nudge_time", ctypes.c_double), ("addforcingtime", ctypes.c_double),
+                ("precision", ctypes.c_int), ("solver", ctypes.c_int),
+                ("warm_start", ctypes.c_int), ("flags", ctypes.c_int)]
+
+
+_F2 = ("zeta", "zetap", "th", "thp", "qv", "qvp", "qc", "qcp", "qr", "qrp", "u", "w", "RKM", "RKH")
+_H = ("dzeta_advect", "dth_buoyancy", "dth_advect", "dqv_advect", "dqc_advect", "dqr_advect",
+      "dqr_VT")
+_P = ("rhou", "rhow", "thb", "thvb", "qvb", "pib", "pb", "thb_init", "qvb0", "z", "z_zeta",
+      "lambda2")
+
+
+class HostState(ctypes.Structure):
+    _fields_ = ([(n, _dp) for n in _F2] + [(n, _dp) for n in _H] + [(n, _dp) for n in _P] +
+                [("Q1LS", _dp), ("Q2LS", _dp), ("init_th_forcing", _dp), ("precip", _dp),
+                 ("ubarTop", ctypes.c_double), ("ubarTopp", ctypes.c_double),
+                 ("dubarTop_advect", ctypes.c_double * 2), ("step", ctypes.c_int)])
+
+
+ROUTINES = ("pzeta", "pth", "pqv", "pqc", "pqr", "add_forcing", "halo_all", "pubartop", "cal_w",
+            "cal_u", "kessler", "update_mean", "turbulence", "nudge", "next_step")
+
+EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu_set_stream",
+           "vvm_gpu_synchronize", "vvm_gpu_last_error", "vvm_gpu_upload_state",
+           "vvm_gpu_download_state", "vvm_gpu_upload_prognostic", "vvm_gpu_download_prognostic",
+           "vvm_gpu_set_step", "vvm_gpu_get_step", "vvm_gpu_step", "vvm_gpu_poisson_solve",
+           "vvm_gpu_poisson_solve_device", "vvm_gpu_last_solve") + tuple(
+               "vvm_gpu_" + r for r in ROUTINES)
+
+_lib = None
+
+
+def load_library(path: Path | None = None):
+    """Loads libvvmgpu.so (no compute; works without a GPU)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is not built; run __graft_entry__.build()")
+    L = ctypes.CDLL(str(p))
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.vvm_gpu_desc_default.argtypes = [ctypes.POINTER(Desc), ip, ip, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double]
+    L.vvm_gpu_desc_default.restype = None
+    L.vvm_gpu_create.argtypes = [ctypes.POINTER(Desc), ip, ctypes.POINTER(vp)]
+    L.vvm_gpu_destroy.argtypes = [vp]
+    L.vvm_gpu_set_stream.argtypes = [vp, vp]
+    L.vvm_gpu_synchronize.argtypes = [vp]
+    L.vvm_gpu_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    for n in ("upload_state", "download_state", "upload_prognostic", "download_prognostic"):
+        getattr(L, "vvm_gpu_" + n).argtypes = [vp, ctypes.POINTER(HostState)]
+    L.vvm_gpu_set_step.argtypes = [vp, ip]
+    L.vvm_gpu_get_step.argtypes = [vp, ctypes.POINTER(ip)]
+    L.vvm_gpu_step.argtypes = [vp, ip]
+    L.vvm_gpu_poisson_solve.argtypes = [vp, _dp, _dp, ctypes.c_double, ctypes.POINTER(ip), _dp]
+    L.vvm_gpu_poisson_solve_device.argtypes = [vp, vp, vp, ctypes.c_double,
+                                               ctypes.POINTER(ip), _dp]
+    L.vvm_gpu_last_solve.argtypes = [vp, ctypes.POINTER(ip), _dp]
+    for r in ROUTINES:
+        getattr(L, "vvm_gpu_" + r).argtypes = [vp]
+    if path is None:
+        _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+class VVMGpu:
+    """One GPU context of the VVM step (a `vvm` model living in HBM)."""
+
+    def __init__(self, grid, precision: int = VVM_PREC_FP64, solver: int = VVM_SOLVER_MGPCG,
+                 poisson_tol: float = 1e-10, warm_start: bool = True, device: int = 0,
+                 addforcingtime: float = 0.0, poisson_maxit: int = 200):
+        self.L = load_library()
+        self.grid = grid
+        d = Desc()
+        self.L.vvm_gpu_desc_default(ctypes.byref(d), grid.NX, grid.NZ, float(grid.dx),
+                                    float(grid.dz), float(grid.dt))
+        d.case_id = int(grid.case)
+        d.moisture_nudge_time = float(grid.moisture_nudge_time)
+        d.addforcingtime = float(addforcingtime)
+        d.precision = int(precision)
+        d.solver = int(solver)
+        d.poisson_tol = float(poisson_tol)
+        d.poisson_maxit = int(poisson_maxit)
+        d.warm_start = 1 if warm_start else 0
+        self.desc = d
+        h = ctypes.c_void_p()
+        rc = self.L.vvm_gpu_create(ctypes.byref(d), int(device), ctypes.byref(h))
+        if rc != 0:
+            raise VVMGpuError(rc, self._err(None))
+        self.h = h
+        self._keep = []
+
+    def _err(self, h):
+        buf = ctypes.create_string_buffer(512)
+        self.L.vvm_gpu_last_error(h, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise VVMGpuError(rc, self._err(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vvm_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state -----------------------------------------------------------
+    def _host_state(self, st: VVMState, with_all: bool):
+        hs = HostState()
+        keep = []
+
+        def put(name, a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            setattr(hs, name, _ptr(a))
+
+        for n in _F2:
+            if n in st.fields and (with_all or n in ("zeta", "th", "qv", "qc", "qr", "u", "w")):
+                put(n, st.fields[n])
+        if with_all:
+            for n in _H:
+                if n in st.hist:
+                    put(n, st.hist[n])
+            for n in _P:
+                put(n, st.prof[n])
+            for n in ("Q1LS", "Q2LS"):
+                if n in st.prof:
+                    put(n, st.prof[n])
+            if "init_th_forcing" in st.fields:
+                put("init_th_forcing", st.fields["init_th_forcing"])
+            if st.precip is not None:
+                put("precip", st.precip)
+            hs.ubarTop = float(st.scalars["ubarTop"])
+            hs.ubarTopp = float(st.scalars.get("ubarTopp", 0.0))
+            hs.dubarTop_advect[0] = float(st.scalars["dubarTop_advect"][0])
+            hs.dubarTop_advect[1] = float(st.scalars["dubarTop_advect"][1])
+            hs.step = int(st.scalars.get("step", 0))
+        return hs, keep
+
+    def upload(self, st: VVMState):
+        hs, keep = self._host_state(st, True)
+        self._check(self.L.vvm_gpu_upload_state(self.h, ctypes.byref(hs)))
+
+    def download(self) -> VVMState:
+        g = self.grid
+        st = VVMState(g)
+        nx, nz = g.nx, g.nz
+        st.fields = {n: np.zeros((nx, nz)) for n in _F2}
+        st.hist = {n: np.zeros((nx, nz, 2)) for n in _H}
+        st.prof = {n: np.zeros(nz) for n in ("thb", "qvb", "thvb", "rhou", "rhow")}
+        st.precip = np.zeros(nx)
+        hs = HostState()
+        for n, a in st.fields.items():
+            setattr(hs, n, _ptr(a))
+        for n, a in st.hist.items():
+            setattr(hs, n, _ptr(a))
+        for n, a in st.prof.items():
+            setattr(hs, n, _ptr(a))
+        hs.precip = _ptr(st.precip)
+        self._check(self.L.vvm_gpu_download_state(self.h, ctypes.byref(hs)))
+        st.scalars = dict(ubarTop=hs.ubarTop, ubarTopp=hs.ubarTopp,
+                          dubarTop_advect=np.array([hs.dubarTop_advect[0], hs.dubarTop_advect[1]]),
+                          step=hs.step)
+        return st
+
+    def upload_prognostic(self, fields: dict):
+        hs = HostState()
+        keep = []
+        for n in ("zeta", "th", "qv", "qc", "qr", "u", "w"):
+            a = np.ascontiguousarray(fields[n], dtype=np.float64)
+            keep.append(a)
+            setattr(hs, n, _ptr(a))
+        self._check(self.L.vvm_gpu_upload_prognostic(self.h, ctypes.byref(hs)))
+
+    def download_prognostic(self, out: dict):
+        hs = HostState()
+        for n in ("zeta", "th", "qv", "qc", "qr", "u", "w"):
+            setattr(hs, n, _ptr(out[n]))
+        self._check(self.L.vvm_gpu_download_prognostic(self.h, ctypes.byref(hs)))
+
+    # -- stepping ----------------------------------------------------------
+    @property
+    def step_count(self) -> int:
+        v = ctypes.c_int()
+        self._check(self.L.vvm_gpu_get_step(self.h, ctypes.byref(v)))
+        return v.value
+
+    @step_count.setter
+    def step_count(self, v: int):
+        self._check(self.L.vvm_gpu_set_step(self.h, int(v)))
+
+    def call(self, routine: str):
+        self._check(getattr(self.L, "vvm_gpu_" + routine)(self.h))
+
+    def step(self, nsteps: int = 1):
+        self._check(self.L.vvm_gpu_step(self.h, int(nsteps)))
+
+    def time_marching_routines(self, nsteps: int = 1):
+        """The reference's TimeMarching body, one C-ABI call per routine
+        (src/Iteration.cpp:246-434)."""
+        for _ in range(nsteps):
+            self.step_count = self.step_count + 1
+            for r in ("pzeta", "pth", "pqv", "pqc", "pqr", "add_forcing", "halo_all",
+                      "pubartop", "cal_w", "cal_u", "halo_all", "kessler", "halo_all",
+                      "update_mean", "turbulence", "nudge", "next_step"):
+                self.call(r)
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self.L.vvm_gpu_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)))
+
+    def synchronize(self):
+        self._check(self.L.vvm_gpu_synchronize(self.h))
+
+    def last_solve(self):
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        self._check(self.L.vvm_gpu_last_solve(self.h, ctypes.byref(it), ctypes.byref(rel)))
+        return it.value, rel.value
+
+    def poisson_solve(self, b: np.ndarray, W0: np.ndarray | None = None, tol: float = 1e-10):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        W = np.zeros_like(b) if W0 is None else np.ascontiguousarray(W0, dtype=np.float64).copy()
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        self._check(self.L.vvm_gpu_poisson_solve(self.h, _ptr(b), _ptr(W), float(tol),
+                                                 ctypes.byref(it), ctypes.byref(rel)))
+        return W, it.value, rel.value
+
+    def poisson_solve_device(self, d_b: int, d_W: int, tol: float = 1e-10):
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        self._check(self.L.vvm_gpu_poisson_solve_device(self.h, ctypes.c_void_p(d_b),
+                                                        ctypes.c_void_p(d_W), float(tol),
+                                                        ctypes.byref(it), ctypes.byref(rel)))
+        return it.value, rel.value

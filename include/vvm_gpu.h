@@ -1,0 +1,167 @@
+/*
+ * vvm_gpu.h -- C ABI of the B200 VVM time step (libvvmgpu.so).
+ *
+ * The reference model (Aaron-Hsieh-0129/2D-Vector-Vorticity-Model) has no
+ * plugin layer: its step is a sequence of static member functions of
+ * `class vvm` called from vvm::Iteration::TimeMarching
+ * (src/Iteration.cpp:262-434), each `static void F(vvm &model)`. Its only
+ * device boundary is the GPU_POISSON translation unit, which swaps in
+ * another definition of the same members behind InitAMGX / CleanupAMGX hooks
+ * (src/PoissonSolver_GPU_mpi.cpp, src/main.cpp:85-87,141-145). This header is
+ * the same kind of swap at the granularity of the whole step: one entry per
+ * reference routine (so a GPU_STEP build of TimeMarching replaces each body
+ * one for one), plus a fused multi-step entry and a standalone Poisson solve.
+ *
+ * Conventions
+ *  - Every entry returns an int status: 0 = OK, see VVM_GPU_E* below; the
+ *    message of the last failure is available from vvm_gpu_last_error().
+ *  - Host arrays use the reference model's layout (src/Declare.hpp:400-427):
+ *    2D fields are [nx][nz] doubles with k (height) the fast index, ghost
+ *    cells included (nx = NX + 2, nz = NZ + 2); AB2 histories are
+ *    [nx][nz][2]; profiles are [nz]. On the device every field is stored
+ *    x-contiguous ([k][i], rows padded to a multiple of 32 cells) and stays
+ *    resident in HBM across calls; upload/download transpose.
+ *  - One context owns its device memory and stream; calls on one context must
+ *    come from one host thread at a time.
+ *  - The routine entries advance no step counter: TimeMarching increments
+ *    model.step before the physics (src/Iteration.cpp:246), so a caller does
+ *    the same with vvm_gpu_set_step(). vvm_gpu_step() does it itself.
+ */
+#ifndef VVM_GPU_H
+#define VVM_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VVM_GPU_OK 0
+#define VVM_GPU_EINVAL 1     /* bad argument or descriptor */
+#define VVM_GPU_ECUDA 2      /* CUDA runtime error (message has details) */
+#define VVM_GPU_ENOCONV 3    /* Poisson solve did not reach its tolerance */
+#define VVM_GPU_ESTATE 4     /* call out of order (e.g. step before upload) */
+
+/* Arithmetic of the step. */
+#define VVM_PREC_FP64 0   /* every field and solve in FP64 (the plain GPU step) */
+#define VVM_PREC_MIXED 1  /* FP32 fields, stencils, microphysics and inner CG;
+                             FP64 Poisson residual, refinement and reductions */
+
+/* Preconditioner of the Poisson CG (cal_w). */
+#define VVM_SOLVER_MGPCG 0    /* geometric multigrid: x-semicoarsening, z-line relaxation */
+#define VVM_SOLVER_LEARNED 1  /* learned BF16 conv preconditioner in flexible CG,
+                                 multigrid-PCG as fallback */
+
+/* Model description; mirrors Config_VVM (src/Declare.hpp:27-70) and the
+ * constants main.cpp passes (src/main.cpp:68-72). */
+typedef struct vvm_gpu_desc {
+    int NX, NZ;                  /* interior cells (VVM_XRANGE/dx, VVM_ZRANGE/dz) */
+    double dx, dz, dt;           /* grid spacings [m], time step [s] */
+    double gravity, cp, cv, rd, lv, p0, psurf;   /* 9.80665 1003.5 716.5 287 2.5e6 1e5 96500 */
+    double poisson_tol;          /* relative residual ||b - A W||/||b|| of cal_w */
+    int poisson_maxit;           /* CG iteration cap (0 = default 200) */
+    int case_id;                 /* VVM_CASE; zeta nudging is skipped for case 2 */
+    double moisture_nudge_time;  /* VVM_MOISTURE_NUDGE_TIME; 0 disables Nudge_qv */
+    double addforcingtime;       /* random th forcing while step*dt <= this */
+    int precision;               /* VVM_PREC_* */
+    int solver;                  /* VVM_SOLVER_* */
+    int warm_start;              /* 1: start cal_w from the previous W (the
+                                    reference starts from zero) */
+    int flags;                   /* reserved, 0 */
+} vvm_gpu_desc;
+
+/* Fills a descriptor with the reference's constants for an NX x NZ grid. */
+void vvm_gpu_desc_default(vvm_gpu_desc* d, int NX, int NZ, double dx, double dz, double dt);
+
+typedef struct vvm_gpu_ctx vvm_gpu_ctx;
+
+/* Host view of the model state, reference layout. Pointers may be NULL on
+ * download to skip a field; on upload every prognostic pointer is required
+ * (the *p fields, histories and diagnostics may be NULL = zero). */
+typedef struct vvm_gpu_host_state {
+    /* [nx][nz] */
+    double *zeta, *zetap, *th, *thp, *qv, *qvp, *qc, *qcp, *qr, *qrp, *u, *w, *RKM, *RKH;
+    /* [nx][nz][2] AB2 tendency histories */
+    double *dzeta_advect, *dth_buoyancy, *dth_advect, *dqv_advect, *dqc_advect, *dqr_advect,
+        *dqr_VT;
+    /* [nz] profiles */
+    double *rhou, *rhow, *thb, *thvb, *qvb, *pib, *pb, *thb_init, *qvb0, *z, *z_zeta, *lambda2;
+    double *Q1LS, *Q2LS;          /* [nz] large-scale forcing (NULL = none) */
+    double *init_th_forcing;      /* [nx][nz] random th forcing field (NULL = zero) */
+    double *precip;               /* [nx] surface rain diagnostic */
+    /* scalars */
+    double ubarTop, ubarTopp;
+    double dubarTop_advect[2];
+    int step;
+} vvm_gpu_host_state;
+
+/* -- lifetime --------------------------------------------------------------
+ * Replaces `vvm model(config)` + PoissonSolver::InitPoissonMatrix
+ * (src/main.cpp:74,88; src/Declare.hpp:78-96; src/PoissonSolver.cpp:681-813). */
+int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out);
+/* Replaces the vvm destructor (src/Declare.hpp:98-249) / CleanupAMGX. */
+int vvm_gpu_destroy(vvm_gpu_ctx* ctx);
+/* Runs the context's kernels on `stream` (a cudaStream_t) from now on;
+ * NULL restores the context's own stream. */
+int vvm_gpu_set_stream(vvm_gpu_ctx* ctx, void* stream);
+int vvm_gpu_synchronize(vvm_gpu_ctx* ctx);
+/* Message of the last failure on this context (or of vvm_gpu_create when
+ * ctx is NULL). */
+int vvm_gpu_last_error(vvm_gpu_ctx* ctx, char* buf, size_t len);
+
+/* -- state transfer (host [i][k] <-> device [k][i]) -----------------------
+ * Replaces Init::Init1d/Init2d as the source of the state (src/Init.cpp:14-266). */
+int vvm_gpu_upload_state(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st);
+int vvm_gpu_download_state(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st);
+/* Prognostic fields only (zeta, th, qv, qc, qr, u, w): the per-step traffic
+ * of an output call. */
+int vvm_gpu_upload_prognostic(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st);
+int vvm_gpu_download_prognostic(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st);
+int vvm_gpu_set_step(vvm_gpu_ctx* ctx, int step);
+int vvm_gpu_get_step(vvm_gpu_ctx* ctx, int* step);
+
+/* -- one entry per reference routine (src/Iteration.cpp:262-434) ---------- */
+int vvm_gpu_pzeta(vvm_gpu_ctx* ctx);        /* Iteration::pzeta_pt, Iteration.cpp:29-34 */
+int vvm_gpu_pth(vvm_gpu_ctx* ctx);          /* Iteration::pth_pt, Iteration.cpp:36-40 */
+int vvm_gpu_pqv(vvm_gpu_ctx* ctx);          /* Iteration::pqv_pt, Iteration.cpp:90-98 */
+int vvm_gpu_pqc(vvm_gpu_ctx* ctx);          /* Iteration::pqc_pt, Iteration.cpp:100-107 */
+int vvm_gpu_pqr(vvm_gpu_ctx* ctx);          /* Iteration::pqr_pt, Iteration.cpp:109-124 */
+int vvm_gpu_add_forcing(vvm_gpu_ctx* ctx);  /* vvm::AddForcing, AddForcing.cpp:6-28 */
+int vvm_gpu_halo_all(vvm_gpu_ctx* ctx);     /* BoundaryProcess2D_all, Boundary.cpp:32-52 */
+int vvm_gpu_pubartop(vvm_gpu_ctx* ctx);     /* PoissonSolver::pubarTop_pt, PoissonSolver.cpp:655-676 */
+int vvm_gpu_cal_w(vvm_gpu_ctx* ctx);        /* PoissonSolver::cal_w, PoissonSolver.cpp:439-479 */
+int vvm_gpu_cal_u(vvm_gpu_ctx* ctx);        /* PoissonSolver::cal_u, PoissonSolver.cpp:580-653 */
+/* autoconversion, accretion, evaporation, condensation, then
+ * NegativeValueProcess on qvp, qcp, qrp (Iteration.cpp:303-311,
+ * MicroPhysics.cpp:7-138); halos are left to vvm_gpu_halo_all as in the
+ * reference. */
+int vvm_gpu_kessler(vvm_gpu_ctx* ctx);
+int vvm_gpu_update_mean(vvm_gpu_ctx* ctx);  /* Iteration::updateMean, Iteration.cpp:42-86 */
+int vvm_gpu_turbulence(vvm_gpu_ctx* ctx);   /* Turbulence::RKM_RKH, Turbulent.cpp:5-114 */
+/* Nudge_theta, Nudge_zeta (case != 2), Nudge_qv (NumericalProcess.cpp:60-96). */
+int vvm_gpu_nudge(vvm_gpu_ctx* ctx);
+int vvm_gpu_next_step(vvm_gpu_ctx* ctx);    /* Iteration::nextTimeStep, Iteration.cpp:153-204 */
+
+/* -- fused path -------------------------------------------------------------
+ * nsteps complete steps of TimeMarching's body (step++ first), with fused
+ * kernels and the time levels rotated by pointer swap. */
+int vvm_gpu_step(vvm_gpu_ctx* ctx, int nsteps);
+
+/* -- standalone elliptic solve (tests, solves/s) ------------------------------
+ * Solves A W = b for the cal_w matrix (src/PoissonSolver.cpp:760-796) to
+ * ||b - A W||_2 / ||b||_2 <= tol. Host arrays of (NX)*(NZ-1) doubles, unknown
+ * index (k-2)*NX + (i-1), k = 2..nz-2, i = 1..nx-2 -- the reference's vector
+ * ordering. W is used as the initial guess when warm_start is set. */
+int vvm_gpu_poisson_solve(vvm_gpu_ctx* ctx, const double* b, double* W, double tol,
+                          int* iters, double* relres);
+/* Same on device buffers (cudaMalloc'd, same ordering); no host copies. */
+int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_W,
+                                 double tol, int* iters, double* relres);
+
+/* Iterations and final relative residual of the last cal_w solve. */
+int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
