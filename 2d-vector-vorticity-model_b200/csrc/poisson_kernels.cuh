@@ -18,12 +18,11 @@
 //
 // Preconditioner: geometric multigrid with semicoarsening in x (NX -> NX/2;
 // the x coupling of level l is cx/4^l, rows unchanged), one damped z-line
-// Jacobi sweep before and after the coarse correction (each column's
-// tridiagonal z operator solved exactly, Thomas with per-level factors),
-// full-weighting restriction, linear interpolation, and an exact solve on the
-// coarsest level (real Fourier modes in x, one tridiagonal solve per mode).
-// With the same damped sweep before and after and P = 2 R^T the V-cycle is a
-// symmetric positive definite preconditioner.
+// Jacobi sweep (omega = 2/3) before and after the coarse correction, each
+// column's tridiagonal z operator solved exactly by a partitioned solver,
+// full-weighting restriction, linear interpolation, and an exact solve of the
+// one-column coarsest level. With the same damped sweep before and after and
+// P = 2 R^T the V-cycle is a symmetric positive definite preconditioner.
 #pragma once
 
 #include "vvm_common.cuh"
@@ -33,10 +32,6 @@ namespace vvm {
 struct ZOps {          // per-row z coefficients, [NK] doubles
     const double *ru, *rd;
     int NK;
-};
-
-struct LineFactors {   // Thomas factors of one level's line operator, [NK]
-    const double *lo, *inv, *cp;
 };
 
 template <typename P>
@@ -61,63 +56,135 @@ __device__ __forceinline__ P prolong_at(const P* xc, int pitch_c, int nc, int kk
     return P(0.5) * (xc[row + j0] + xc[row + j1]);
 }
 
+// ---------------------------------------------------------------------------
+// Partitioned (spike) solve of the z-line operator of one level.
+//
+// Every column of a level has the same tridiagonal z operator, so all its
+// factors are precomputed on the host: the column's NK rows are cut into S
+// segments (segment s = rows [s*NK/S, (s+1)*NK/S)); within a segment
+// x = y - gL x[a-1] - gR x[b] where y solves the segment's own block and the
+// spikes gL, gR its couplings; the 2S segment-end unknowns satisfy a small
+// system whose inverse Minv (2S x 2S) is also precomputed. A block of
+// 32 x S threads owns 32 adjacent columns (lanes: coalesced rows) and all S
+// segments (warps); the only serial chain is the segment's own Thomas pass.
+
+constexpr int kMaxSeg = 32;
+
+struct LineLevel {
+    int nxl, pitch, NK, S;
+    const double* cx;                 // x coupling of the level, [NK]
+    const double *lo, *inv, *cp;      // segment-local Thomas factors, [NK]
+    const double *gL, *gR;            // spikes, [NK]
+    const double* Minv;               // [2S][2S]
+};
+
+// y = (segment-local) T^{-1} r for rows [a, a+len), in registers.
+template <typename P, int LS>
+__device__ __forceinline__ void seg_thomas(const LineLevel& L, int a, int len, P (&r)[LS]) {
+    P prev = P(0);
+#pragma unroll
+    for (int j = 0; j < LS; j++) {
+        if (j < len) {
+            prev = (r[j] - P(L.lo[a + j]) * prev) * P(L.inv[a + j]);
+            r[j] = prev;
+        }
+    }
+    P next = P(0);
+#pragma unroll
+    for (int j = LS - 1; j >= 0; j--) {
+        if (j < len) {
+            next = r[j] - P(L.cp[a + j]) * next;
+            r[j] = next;
+        }
+    }
+}
+
+// One damped line-Jacobi sweep (or, with xin = xc = null and omega = 1, an
+// exact line solve) for the 32-column strip starting at col0:
+//   out = X + omega * Dline^{-1} (f - S X),  X = xin + P xc.
+// shY: shared [2*kMaxSeg][32] of P. Every thread of the block must call it.
+template <typename P, int LS>
+__device__ __forceinline__ void line_sweep(const LineLevel& L, const ZOps& z, int col0, const P* f,
+                                           const P* xin, const P* xc, int pitch_c, int nc, P* out, P omega,
+                                           P* shY) {
+    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+    const int i = col0 + lane;
+    const bool act = (i < L.nxl) && (s < L.S);
+    const int a = (s * L.NK) / L.S, b = ((s + 1) * L.NK) / L.S, len = b - a;
+    const bool has_x = (xin != nullptr) || (xc != nullptr);
+    P y[LS], X[LS];
+    if (act) {
+        const int il = (i == 0) ? L.nxl - 1 : i - 1, ir = (i == L.nxl - 1) ? 0 : i + 1;
+        auto Xat = [&](int kk, int col) -> P {
+            P v = xin ? xin[(size_t)kk * L.pitch + col] : P(0);
+            if (xc) v += prolong_at(xc, pitch_c, nc, kk, col);
+            return v;
+        };
+#pragma unroll
+        for (int j = 0; j < LS; j++) {
+            X[j] = P(0);
+            y[j] = P(0);
+            if (j < len) {
+                const int kk = a + j;
+                P r = f[(size_t)kk * L.pitch + i];
+                if (has_x) {
+                    const P c = P(L.cx[kk]), ru = P(z.ru[kk]), rd = P(z.rd[kk]);
+                    P x0 = Xat(kk, i);
+                    P sx = (P(2) * c + ru + rd) * x0 - c * (Xat(kk, il) + Xat(kk, ir));
+                    if (kk + 1 < L.NK) sx -= ru * Xat(kk + 1, i);
+                    if (kk > 0) sx -= rd * Xat(kk - 1, i);
+                    r -= sx;
+                    X[j] = x0;
+                }
+                y[j] = r;
+            }
+        }
+        seg_thomas<P, LS>(L, a, len, y);
+        P ylast = y[0];
+#pragma unroll
+        for (int j = 0; j < LS; j++)
+            if (j == len - 1) ylast = y[j];
+        shY[(2 * s) * 32 + lane] = y[0];
+        shY[(2 * s + 1) * 32 + lane] = ylast;
+    }
+    __syncthreads();
+    if (act) {
+        const int S2 = 2 * L.S;
+        P XL = P(0), XR = P(0);
+        if (s > 0) {
+            const double* m = L.Minv + (size_t)(2 * (s - 1) + 1) * S2;
+            for (int q = 0; q < S2; q++) XL += P(m[q]) * shY[q * 32 + lane];
+        }
+        if (s + 1 < L.S) {
+            const double* m = L.Minv + (size_t)(2 * (s + 1)) * S2;
+            for (int q = 0; q < S2; q++) XR += P(m[q]) * shY[q * 32 + lane];
+        }
+#pragma unroll
+        for (int j = 0; j < LS; j++) {
+            if (j < len) {
+                const int kk = a + j;
+                P e = y[j] - P(L.gL[kk]) * XL - P(L.gR[kk]) * XR;
+                out[(size_t)kk * L.pitch + i] = X[j] + omega * e;
+            }
+        }
+    }
+    __syncthreads();
+}
+
 template <typename P>
-struct SmoothArgs {
-    int nxl, pitch, NK;
+struct SweepArgs {
+    LineLevel L;
     ZOps z;
-    const double* cx;
-    LineFactors lf;
-    const P* f;        // right-hand side of this level
-    const P* xin;      // current iterate (null = zero)
-    const P* xc;       // coarse correction to add first (null = none)
+    const P *f, *xin, *xc;
     int pitch_c, nc;
-    P* out;            // xin + Pxc + omega * Dline^{-1} (f - S (xin + Pxc))
+    P* out;
     P omega;
 };
 
-// Value of the iterate X = xin + P xc at (kk, i).
-template <typename P>
-__device__ __forceinline__ P smooth_X(const SmoothArgs<P>& a, int kk, int i) {
-    P v = a.xin ? a.xin[(size_t)kk * a.pitch + i] : P(0);
-    if (a.xc) v += prolong_at(a.xc, a.pitch_c, a.nc, kk, i);
-    return v;
-}
-
-// One damped z-line Jacobi sweep; one thread per column.
-template <typename P>
-__global__ void k_mg_smooth(SmoothArgs<P> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nxl) return;
-    const int NK = a.NK;
-    const bool has_x = (a.xin != nullptr) || (a.xc != nullptr);
-    const int il = (i == 0) ? a.nxl - 1 : i - 1, ir = (i == a.nxl - 1) ? 0 : i + 1;
-    // forward elimination; y_k parked in out
-    P yprev = P(0);
-    P xm = P(0), x0 = has_x ? smooth_X(a, 0, i) : P(0);
-    for (int kk = 0; kk < NK; kk++) {
-        P r = a.f[(size_t)kk * a.pitch + i];
-        P xp = P(0);
-        if (has_x) {
-            xp = (kk + 1 < NK) ? smooth_X(a, kk + 1, i) : P(0);
-            const P c = P(a.cx[kk]), ru = P(a.z.ru[kk]), rd = P(a.z.rd[kk]);
-            P sx = (P(2) * c + ru + rd) * x0 - c * (smooth_X(a, kk, il) + smooth_X(a, kk, ir)) - ru * xp - rd * xm;
-            r -= sx;
-        }
-        P y = (r - P(a.lf.lo[kk]) * yprev) * P(a.lf.inv[kk]);
-        a.out[(size_t)kk * a.pitch + i] = y;
-        yprev = y;
-        xm = x0;
-        x0 = xp;
-    }
-    // back substitution
-    P xnext = P(0);
-    for (int kk = NK - 1; kk >= 0; kk--) {
-        size_t id = (size_t)kk * a.pitch + i;
-        P e = a.out[id] - P(a.lf.cp[kk]) * xnext;
-        xnext = e;
-        P base = has_x ? smooth_X(a, kk, i) : P(0);
-        a.out[id] = base + a.omega * e;
-    }
+template <typename P, int LS>
+__global__ void __launch_bounds__(32 * kMaxSeg) k_line_sweep(SweepArgs<P> a) {
+    __shared__ P shY[2 * kMaxSeg * 32];
+    line_sweep<P, LS>(a.L, a.z, blockIdx.x * 32, a.f, a.xin, a.xc, a.pitch_c, a.nc, a.out, a.omega, shY);
 }
 
 template <typename P>
@@ -132,11 +199,7 @@ struct RestrictArgs {
 
 // fc[j] = 1/4 r[2j-1] + 1/2 r[2j] + 1/4 r[2j+1], r = f - S x (periodic).
 template <typename P>
-__global__ void k_mg_restrict(RestrictArgs<P> a) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
-    const int nc = a.nxl >> 1;
-    if (j >= nc || kk >= a.NK) return;
+__device__ __forceinline__ void restrict_point(const RestrictArgs<P>& a, int j, int kk) {
     const int i0 = 2 * j, im = (i0 == 0) ? a.nxl - 1 : i0 - 1, ip = i0 + 1;
     const size_t row = (size_t)kk * a.pitch;
     P r0 = a.f[row + i0] - s_apply(a.x, a.pitch, a.nxl, a.NK, a.z, a.cx, kk, i0);
@@ -146,46 +209,75 @@ __global__ void k_mg_restrict(RestrictArgs<P> a) {
 }
 
 template <typename P>
-struct CoarseArgs {
-    int nc, pitch, NK;
-    const double* Q;      // [nc][nc] orthonormal real Fourier basis, Q[j*nc + m]
-    const double *lo, *inv, *cp;   // per mode factors, [nc][NK]
-    const P* f;
-    P* x;
-    double* xh;           // scratch [NK][nc]
+__global__ void k_mg_restrict(RestrictArgs<P> a) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= (a.nxl >> 1) || kk >= a.NK) return;
+    restrict_point(a, j, kk);
+}
+
+// The coarse end of the V-cycle in one block, with block barriers between
+// phases. Levels wider than 32 columns are swept strip by strip. When NX is a
+// power of two the last level has one column, its operator has no x part,
+// and one exact line solve (omega = 1) finishes it; otherwise the last level
+// has an odd column count and gets coarse_sweeps damped sweeps from zero.
+constexpr int kMaxCoarseLevels = 8;
+
+template <typename P>
+struct CoarseCycleArgs {
+    int nlev;                          // levels handled by the block (>= 1)
+    LineLevel L[kMaxCoarseLevels];
+    ZOps z;
+    const P* f0;                       // rhs of its first level
+    P* f[kMaxCoarseLevels];            // rhs of the following levels
+    P* x[kMaxCoarseLevels];            // pre-smoothed iterates; coarsest solution
+    P* y[kMaxCoarseLevels];            // post-smoothed results (y[0] = output)
+    P omega;
+    int coarse_sweeps;                 // 1 = exact solve of a single column
 };
 
-// Exact coarsest-level solve: x = Q (per-mode tridiagonal)^{-1} Q^T f.
-template <typename P>
-__global__ void k_mg_coarse(CoarseArgs<P> a) {
-    const int m = threadIdx.x;
-    const int nc = a.nc, NK = a.NK;
-    if (m < nc) {
-        const double* lo = a.lo + (size_t)m * NK;
-        const double* inv = a.inv + (size_t)m * NK;
-        const double* cp = a.cp + (size_t)m * NK;
-        double yprev = 0;
-        for (int kk = 0; kk < NK; kk++) {
-            double fh = 0;
-            for (int j = 0; j < nc; j++) fh += a.Q[j * nc + m] * (double)a.f[(size_t)kk * a.pitch + j];
-            double y = (fh - lo[kk] * yprev) * inv[kk];
-            a.xh[(size_t)kk * nc + m] = y;
-            yprev = y;
-        }
-        double xnext = 0;
-        for (int kk = NK - 1; kk >= 0; kk--) {
-            double e = a.xh[(size_t)kk * nc + m] - cp[kk] * xnext;
-            a.xh[(size_t)kk * nc + m] = e;
-            xnext = e;
+template <typename P, int LS>
+__device__ __forceinline__ void sweep_all(const LineLevel& L, const ZOps& z, const P* f, const P* xin,
+                                          const P* xc, int pitch_c, int nc, P* out, P omega, P* shY) {
+    for (int c0 = 0; c0 < L.nxl; c0 += 32) line_sweep<P, LS>(L, z, c0, f, xin, xc, pitch_c, nc, out, omega, shY);
+}
+
+template <typename P, int LS>
+__global__ void __launch_bounds__(32 * kMaxSeg) k_mg_coarse_cycle(CoarseCycleArgs<P> a) {
+    __shared__ P shY[2 * kMaxSeg * 32];
+    const int n = a.nlev;
+    for (int l = 0; l < n - 1; l++) {
+        const P* fl = (l == 0) ? a.f0 : a.f[l];
+        sweep_all<P, LS>(a.L[l], a.z, fl, nullptr, nullptr, 0, 0, a.x[l], a.omega, shY);
+        RestrictArgs<P> ra{a.L[l].nxl, a.L[l].pitch, a.L[l].NK, a.z, a.L[l].cx, fl, a.x[l], a.f[l + 1],
+                           a.L[l + 1].pitch};
+        const int nc = a.L[l].nxl >> 1, tot = nc * a.L[l].NK;
+        for (int t = threadIdx.x; t < tot; t += blockDim.x) restrict_point(ra, t % nc, t / nc);
+        __syncthreads();
+    }
+    {
+        const int c = n - 1;
+        const P* fl = (n == 1) ? a.f0 : a.f[c];
+        P* target = (n == 1) ? a.y[0] : a.x[c];
+        P* other = (n == 1) ? a.x[0] : a.y[c];
+        const int K = a.coarse_sweeps;
+        if (K <= 1) {
+            sweep_all<P, LS>(a.L[c], a.z, fl, nullptr, nullptr, 0, 0, target, P(1), shY);
+        } else {
+            P* dst = (K & 1) ? target : other;
+            const P* cur = nullptr;
+            for (int it = 0; it < K; it++) {
+                sweep_all<P, LS>(a.L[c], a.z, fl, cur, nullptr, 0, 0, dst, a.omega, shY);
+                cur = dst;
+                dst = (dst == target) ? other : target;
+            }
         }
     }
-    __syncthreads();
-    if (m < nc) {
-        for (int kk = 0; kk < NK; kk++) {
-            double v = 0;
-            for (int q = 0; q < nc; q++) v += a.Q[m * nc + q] * a.xh[(size_t)kk * nc + q];
-            a.x[(size_t)kk * a.pitch + m] = P(v);
-        }
+    for (int l = n - 2; l >= 0; l--) {
+        const P* fl = (l == 0) ? a.f0 : a.f[l];
+        const P* coarse = (l + 1 == n - 1) ? a.x[n - 1] : a.y[l + 1];
+        sweep_all<P, LS>(a.L[l], a.z, fl, a.x[l], coarse, a.L[l + 1].pitch, a.L[l + 1].nxl, a.y[l], a.omega,
+                         shY);
     }
 }
 

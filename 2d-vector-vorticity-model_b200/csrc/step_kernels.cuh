@@ -10,6 +10,8 @@
 // (store_center / store_westdown write every ghost image of a cell).
 #pragma once
 
+#include <type_traits>
+
 #include "vvm_common.cuh"
 
 namespace vvm {
@@ -25,7 +27,16 @@ struct Profiles {
     const double *dtcgr_zeta; // dt*CGR of Nudge_zeta (0 below k_start or case 2)
     const double *q1ls, *q2ls;  // large-scale forcing profiles (may be all zero)
     double pf1, pf2;          // 1E-3*rhou[1], pow(rhou[1]/rhow[1], -0.5)  Iteration.cpp:115
+    // Mixed step only: th and qv are stored as perturbations from the
+    // reference profiles ref[0] = th0 (thb_init) and ref[1] = qv0 (qvb0).
+    // For each: d0[k] = ref[k] - ref[k-1], s0[k] = ref[k] + ref[k-1],
+    // g0[k] = ref[k+1] - ref[k-1], dn[k] = ref[k] - (nudging target)[k].
+    const double *ref[2], *d0[2], *s0[2], *g0[2], *dn[2];
 };
+
+// True for the mixed step, whose th and qv arrays hold perturbations.
+template <typename T>
+constexpr bool kPert = std::is_same<T, float>::value;
 
 // AB2 bookkeeping shared by every prognostic tendency
 // (e.g. Advection.cpp:69-71): slot (step+1)%2 receives the new tendency,
@@ -112,6 +123,17 @@ __device__ __forceinline__ T thv_at(const PZetaArgs<T>& a, int i, int k) {  // B
     return a.th[id] * (T(1) + T(0.608) * a.qv[id]);
 }
 
+// thv(i,k) - thv(i-1,k) from perturbations th', qv' about th0(k), qv0(k):
+// dth' + 0.608 (th0 dqv' + qv0 dth' + (th'q')_i - (th'q')_{i-1}); the large
+// reference values never enter a difference.
+template <typename T>
+__device__ __forceinline__ T thv_dx(const PZetaArgs<T>& a, int i, int k) {
+    size_t id = a.d.at(i, k), im = a.d.at(i - 1, k);
+    T t1 = a.th[id], t0 = a.th[im], q1 = a.qv[id], q0 = a.qv[im];
+    T dt = t1 - t0, dq = q1 - q0;
+    return dt + T(0.608) * (T(a.p.ref[0][k]) * dq + T(a.p.ref[1][k]) * dt + (t1 * q1 - t0 * q0));
+}
+
 template <typename T>
 __global__ void k_pzeta(PZetaArgs<T> a) {
     const Dims& d = a.d;
@@ -134,9 +156,15 @@ __global__ void k_pzeta(PZetaArgs<T> a) {
     T zp = a.zeta[id] + dt15 * tz - dt05 * oz;
     // Bouyancy (Buoyancy.cpp:25-48)
     T g_rw = T(a.c.gravity) / rw;
-    T b = g_rw * T(0.5) *
-          ((thv_at(a, i, k) - thv_at(a, i - 1, k)) / T(a.p.thvb[k]) +
-           (thv_at(a, i, k - 1) - thv_at(a, i - 1, k - 1)) / T(a.p.thvb[k - 1])) * T(a.c.rdx);
+    T b;
+    if constexpr (!kPert<T>) {
+        b = g_rw * T(0.5) *
+            ((thv_at(a, i, k) - thv_at(a, i - 1, k)) / T(a.p.thvb[k]) +
+             (thv_at(a, i, k - 1) - thv_at(a, i - 1, k - 1)) / T(a.p.thvb[k - 1])) * T(a.c.rdx);
+    } else {
+        b = g_rw * T(0.5) * (thv_dx(a, i, k) / T(a.p.thvb[k]) + thv_dx(a, i, k - 1) / T(a.p.thvb[k - 1])) *
+            T(a.c.rdx);
+    }
     T bc = g_rw * (T(0.5) * (a.qc[id] + a.qc[d.at(i, k - 1)]) -
                    T(0.5) * (a.qc[d.at(i - 1, k)] + a.qc[d.at(i - 1, k - 1)])) * T(a.c.rdx);
     T br = g_rw * (T(0.5) * (a.qr[id] + a.qr[d.at(i, k - 1)]) -
@@ -216,6 +244,26 @@ __device__ __forceinline__ T scal_flux_w(const PAdvArgs<T>& a, const T* v, int i
     return f;
 }
 
+// z flux of a perturbation v' about profile v0 (mixed step): the main term
+// carries v' only, the 3rd-order differences add d0[k] = v0[k] - v0[k-1].
+template <typename T>
+__device__ __forceinline__ T scal_flux_w_pert(const PAdvArgs<T>& a, const T* v, const double* d0, int i, int k) {
+    const Dims& d = a.d;
+    T rk = T(a.p.rhow[k]);
+    T wk = a.w[d.at(i, k)];
+    T v0 = v[d.at(i, k)], vm = v[d.at(i, k - 1)];
+    T f = rk * wk * (v0 + vm);
+    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
+        T rkm = T(a.p.rhow[k - 1]), rkp = T(a.p.rhow[k + 1]);
+        T wm = a.w[d.at(i, k - 1)], wp = a.w[d.at(i, k + 1)];
+        T vmm = v[d.at(i, k - 2)], vp = v[d.at(i, k + 1)];
+        T dk = (v0 - vm) + T(d0[k]), dkm = (vm - vmm) + T(d0[k - 1]), dkp = (vp - v0) + T(d0[k + 1]);
+        f += T(-1. / 3.) * (rk * plus_part(wk) * dk - sqrt(rk * plus_part(wk) * rkm * plus_part(wm)) * dkm -
+                            rk * minus_part(wk) * dk - sqrt(fabs(rk * minus_part(wk) * rkp * minus_part(wp))) * dkp);
+    }
+    return f;
+}
+
 // Sedimentation flux at (i, k-1/2), k = 1..nz-2 (Advection.cpp:165-166).
 template <typename T>
 __device__ __forceinline__ T vt_flux(const PAdvArgs<T>& a, const T* qr, int i, int k) {
@@ -241,12 +289,30 @@ __global__ void k_padv(PAdvArgs<T> a) {
             const T* v = a.now[f];
             // flux_u at nx-1 is the halo copy of flux_u at 1; flux_w at nz-1
             // is zeroed (Advection.cpp:55-58).
-            T fu_p = scal_flux_u(a, v, (i == d.nx - 2) ? 1 : i + 1, k);
+            const int ip = (i == d.nx - 2) ? 1 : i + 1;
+            T fu_p = scal_flux_u(a, v, ip, k);
             T fu_0 = scal_flux_u(a, v, i, k);
-            T fw_p = (k == d.nz - 2) ? T(0) : scal_flux_w(a, v, i, k + 1);
-            T fw_0 = scal_flux_w(a, v, i, k);
-            T px = (fu_p - fu_0) * T(a.c.r2dx) / ru;
-            T pz = (fw_p - fw_0) * T(a.c.r2dz) / ru;
+            T px, pz;
+            if (!kPert<T> || f >= 2) {
+                T fw_p = (k == d.nz - 2) ? T(0) : scal_flux_w(a, v, i, k + 1);
+                T fw_0 = scal_flux_w(a, v, i, k);
+                px = (fu_p - fu_0) * T(a.c.r2dx) / ru;
+                pz = (fw_p - fw_0) * T(a.c.r2dz) / ru;
+            } else {
+                // v = v0(k) + v': the v0 parts of both fluxes are added in
+                // difference form, 2 v0 (u[i+1] - u[i]) in x and
+                // s0[k+1] (m[k+1] - m[k]) + m[k] g0[k] in z, m = rhow w.
+                const double* d0 = a.p.d0[f];
+                T fw_p = (k == d.nz - 2) ? T(0) : scal_flux_w_pert(a, v, d0, i, k + 1);
+                T fw_0 = scal_flux_w_pert(a, v, d0, i, k);
+                T m0 = T(a.p.rhow[k]) * a.w[d.at(i, k)];
+                T refz = (k == d.nz - 2) ? -m0 * T(a.p.s0[f][k])
+                                         : T(a.p.s0[f][k + 1]) * (T(a.p.rhow[k + 1]) * a.w[d.at(i, k + 1)] - m0) +
+                                               m0 * T(a.p.g0[f][k]);
+                T refx = T(2.0 * a.p.ref[f][k]) * (a.u[d.at(ip, k)] - a.u[d.at(i, k)]);
+                px = (fu_p - fu_0) * T(a.c.r2dx) / ru + refx * T(a.c.r2dx);
+                pz = (fw_p - fw_0 + refz) * T(a.c.r2dz) / ru;
+            }
             T t = -px - pz;
             T o = ab2_push(a.hn[f], a.ho[f], id, t, a.ab);
             T out = v[id] + dt15 * t - dt05 * o;
@@ -259,8 +325,10 @@ __global__ void k_padv(PAdvArgs<T> a) {
             }
             a.fut[f][id] = out;
             if (f >= 1 && (a.nvp_mask & (1 << f))) {
-                if (out >= T(0)) sums[2 * (f - 1)] += (double)out;
-                else sums[2 * (f - 1) + 1] += (double)out;
+                double full = (double)out;
+                if (kPert<T> && f == 1) full += a.p.ref[1][k];
+                if (full >= 0.0) sums[2 * (f - 1)] += full;
+                else sums[2 * (f - 1) + 1] += full;
             }
         }
         if (a.do_precip && k == 1) {
@@ -324,7 +392,14 @@ __global__ void k_apply(ApplyArgs<T> a) {
     for (int f = 0; f < 4; f++) {
         if (!(a.mask & (1 << f))) continue;
         T v = a.fut[f][id];
-        if (f >= 1 && (a.nvp_mask & (1 << f))) v = nvp_apply(v, a.nvp, f - 1);
+        if (f >= 1 && (a.nvp_mask & (1 << f))) {
+            if (kPert<T> && f == 1) {   // NegativeValueProcess acts on the full qv
+                double full = a.p.ref[1][k] + (double)v;
+                v = T(nvp_apply(full, a.nvp, 0) - a.p.ref[1][k]);
+            } else {
+                v = nvp_apply(v, a.nvp, f - 1);
+            }
+        }
         if (f == 0) {
             if (a.forcing) v += dt * T(a.p.q1ls[k]);
             if (a.forcing_th) v += dt * a.th_forcing[id];
@@ -377,8 +452,59 @@ struct KesslerArgs {
     int nvp;  // accumulate NVP sums
 };
 
+// One cell of Kessler warm rain in compute type C; writes the four rates.
+template <typename C>
+__device__ __forceinline__ void kessler_cell(C& th, C& qv, C& qc, C& qr, C dt, C lv, C cp, C pib, C rhou,
+                                             C pc, C pb, C rates[4]) {
+    {   // autoconversion
+        C qcplus = smax(C(0), qc);
+        C ar = C(0.001) * (qcplus - C(0.001));
+        ar = smax(C(0), ar);
+        C arcrdt = smin(ar * dt, qcplus);
+        qc = qc - arcrdt;
+        qr = qr + arcrdt;
+        rates[0] = arcrdt;
+    }
+    {   // accretion
+        C qcplus = smax(C(0), qc), qrplus = smax(C(0), qr);
+        C cr = C(2.2) * qcplus * (pow(qrplus, C(0.875)));
+        C arcrdt = smin(cr * dt, qcplus);
+        qc = qc - arcrdt;
+        qr = qr + arcrdt;
+        rates[1] = arcrdt;
+    }
+    {   // evaporation of rain
+        C qrplus = smax(C(0), qr), qvplus = smax(C(0), qv);
+        C qvs = pc * exp(C(17.27) * (pib * th - C(273.)) / (pib * th - C(36.)));
+        C deficit = smax((C(1.) - qvplus / qvs), C(0.));
+        C coef = C(1.6) + C(124.9) * pow((C(1E-3) * rhou * qrplus), C(0.2046));
+        C er = coef * deficit * (pow(C(1E-3) * rhou * qrplus, C(0.525))) /
+               ((C(5.4E5) + C(2.55E6) / (C(1E-2) * pb * qvs)) * C(1E-3) * rhou);
+        C erdt = smin(qrplus, smax(C(0.), er * dt));
+        qr = qr - erdt;
+        qv = qv + erdt;
+        th = th - lv * erdt / (cp * pib);
+        rates[2] = erdt;
+    }
+    {   // saturation adjustment
+        C qvs = pc * exp(C(17.27) * (pib * th - C(273.)) / (pib * th - C(36.)));
+        C tm = th * pib - C(36.);
+        C phi = qvs * (C(17.27) * C(237.) * lv) / (cp * (tm * tm));
+        C cnd = (qv - qvs) / (C(1) + phi);
+        if (fabs(cnd) > qc && cnd < C(0)) cnd = -qc;
+        qv = qv - cnd;
+        qc = qc + cnd;
+        th = th + lv / (cp * pib) * cnd;
+        rates[3] = cnd;
+    }
+}
+
+// The mixed step runs this kernel's arithmetic in FP64 on its FP32 storage:
+// the saturation adjustment subtracts qvs from qv, which cancel to a few
+// units of the FP32 epsilon near saturation.
 template <typename T>
 __global__ void k_kessler(KesslerArgs<T> a) {
+    using C = double;
     __shared__ double sh[32 * 6];
     const Dims& d = a.d;
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -387,63 +513,26 @@ __global__ void k_kessler(KesslerArgs<T> a) {
     double sums[6] = {0, 0, 0, 0, 0, 0};
     if (act) {
         const size_t id = d.at(i, k);
-        const T dt = T(a.c.dt), lv = T(a.c.lv), cp = T(a.c.cp);
-        const T pib = T(a.p.pib[k]), rhou = T(a.p.rhou[k]), pc = T(a.p.pc[k]), pb = T(a.p.pb[k]);
-        T th = a.thp[id], qv = a.qvp[id], qc = a.qcp[id], qr = a.qrp[id];
-        // autoconversion
-        {
-            T qcplus = smax(T(0), qc);
-            T ar = T(0.001) * (qcplus - T(0.001));
-            ar = smax(T(0), ar);
-            T arcrdt = smin(ar * dt, qcplus);
-            qc = qc - arcrdt;
-            qr = qr + arcrdt;
-            if (a.d_auto) a.d_auto[id] = arcrdt;
+        const C th0 = kPert<T> ? a.p.ref[0][k] : 0.0, qv0 = kPert<T> ? a.p.ref[1][k] : 0.0;
+        C th = th0 + (C)a.thp[id], qv = qv0 + (C)a.qvp[id], qc = a.qcp[id], qr = a.qrp[id];
+        C rates[4];
+        kessler_cell<C>(th, qv, qc, qr, a.c.dt, a.c.lv, a.c.cp, a.p.pib[k], a.p.rhou[k], a.p.pc[k], a.p.pb[k],
+                        rates);
+        if (a.d_auto) {
+            a.d_auto[id] = T(rates[0]);
+            a.d_accr[id] = T(rates[1]);
+            a.d_evap[id] = T(rates[2]);
+            a.d_cond[id] = T(rates[3]);
         }
-        // accretion
-        {
-            T qcplus = smax(T(0), qc), qrplus = smax(T(0), qr);
-            T cr = T(2.2) * qcplus * (pow(qrplus, T(0.875)));
-            T arcrdt = smin(cr * dt, qcplus);
-            qc = qc - arcrdt;
-            qr = qr + arcrdt;
-            if (a.d_accr) a.d_accr[id] = arcrdt;
-        }
-        // evaporation of rain
-        {
-            T qrplus = smax(T(0), qr), qvplus = smax(T(0), qv);
-            T qvs = pc * exp(T(17.27) * (pib * th - T(273.)) / (pib * th - T(36.)));
-            T deficit = smax((T(1.) - qvplus / qvs), T(0.));
-            T coef = T(1.6) + T(124.9) * pow((T(1E-3) * rhou * qrplus), T(0.2046));
-            T er = coef * deficit * (pow(T(1E-3) * rhou * qrplus, T(0.525))) /
-                   ((T(5.4E5) + T(2.55E6) / (T(1E-2) * pb * qvs)) * T(1E-3) * rhou);
-            T erdt = smin(qrplus, smax(T(0.), er * dt));
-            qr = qr - erdt;
-            qv = qv + erdt;
-            th = th - lv * erdt / (cp * pib);
-            if (a.d_evap) a.d_evap[id] = erdt;
-        }
-        // saturation adjustment
-        {
-            T qvs = pc * exp(T(17.27) * (pib * th - T(273.)) / (pib * th - T(36.)));
-            T tm = th * pib - T(36.);
-            T phi = qvs * (T(17.27) * T(237.) * lv) / (cp * (tm * tm));
-            T C = (qv - qvs) / (T(1) + phi);
-            if (fabs(C) > qc && C < T(0)) C = -qc;
-            qv = qv - C;
-            qc = qc + C;
-            th = th + lv / (cp * pib) * C;
-            if (a.d_cond) a.d_cond[id] = C;
-        }
-        a.thp[id] = th;
-        a.qvp[id] = qv;
-        a.qcp[id] = qc;
-        a.qrp[id] = qr;
+        a.thp[id] = T(th - th0);
+        a.qvp[id] = T(qv - qv0);
+        a.qcp[id] = T(qc);
+        a.qrp[id] = T(qr);
         if (a.nvp) {
-            T q[3] = {qv, qc, qr};
+            C q[3] = {qv, qc, qr};
 #pragma unroll
             for (int f = 0; f < 3; f++) {
-                if (q[f] >= T(0)) sums[2 * f] += (double)q[f];
+                if (q[f] >= C(0)) sums[2 * f] += (double)q[f];
                 else sums[2 * f + 1] += (double)q[f];
             }
         }
@@ -484,8 +573,13 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
     T rot = (u[d.at(i + 1, k)] - u[d.at(i, k)]) * T(a.c.rdx) + (w[d.at(i, k + 1)] - w[d.at(i, k)]) * T(a.c.rdz);
     T Rotat = rot * rot;
     T th0 = a.thp[d.at(i, k)];
+    T dth = a.thp[d.at(i, k + 1)] - a.thp[d.at(i, k - 1)];
+    if constexpr (kPert<T>) {       // perturbation storage: add the profile parts
+        th0 += T(a.p.ref[0][k]);
+        dth += T(a.p.g0[0][k]);
+    }
     T def2 = Rzeta * Rzeta + T(2.) * Rotat;
-    T Ri = (T(a.c.gravity) / th0 * (a.thp[d.at(i, k + 1)] - a.thp[d.at(i, k - 1)]) * T(a.c.r2dz)) / def2;
+    T Ri = (T(a.c.gravity) / th0 * dth * T(a.c.r2dz)) / def2;
     T lam = T(a.p.lambda2[k]);
     T km, kh;
     if (Ri < T(0)) {
@@ -536,7 +630,10 @@ struct GSArgs {
 constexpr int kGSThreads = 1024;
 constexpr int kGSMaxPerThread = 8;   // NX up to 8192
 
-template <typename T>
+// Row k of the sweep solves v'[i] = A0[i] + C[i] v'(i, k-1) + B[i] v'[i-1]:
+// A0, C and B use only old values, so those of row k+1 are formed while
+// row k is being scanned (the global-memory latency hides behind the scan).
+template <typename T, int PER>
 __global__ void __launch_bounds__(kGSThreads) k_gs_diffuse(GSArgs<T> a) {
     __shared__ T shA[32], shB[32];
     const int f = blockIdx.x;
@@ -547,35 +644,29 @@ __global__ void __launch_bounds__(kGSThreads) k_gs_diffuse(GSArgs<T> a) {
     const T* K = mom ? a.RKM : a.RKH;
     const int NX = d.nx - 2;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int per = (NX + kGSThreads - 1) / kGSThreads;
-    const int i0 = 1 + tid * per;
+    const int i0 = 1 + tid * PER;
     const T cx = T(a.c.rdx2 * a.c.dt);
-    T vdn[kGSMaxPerThread];
-    // row 0 (ghost) is the "updated" row below row 1: never modified
-#pragma unroll
-    for (int e = 0; e < kGSMaxPerThread; e++) {
-        int i = i0 + e;
-        vdn[e] = (e < per && i <= NX) ? v[d.at(i, 0)] : T(0);
-    }
-    for (int k = 1; k <= d.nz - 2; k++) {
+    T vdn[PER], A0[PER], Cc[PER], Bb[PER];
+    // coefficients of row k from old values (Turbulent.cpp:83-88 for zeta,
+    // :107-112 for the scalars)
+    auto coeffs = [&](int k) {
         const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
-        T Aa[kGSMaxPerThread], Bb[kGSMaxPerThread];
-        T cA = T(0), cB = T(1);  // composition of this thread's maps (identity)
 #pragma unroll
-        for (int e = 0; e < kGSMaxPerThread; e++) {
+        for (int e = 0; e < PER; e++) {
             int i = i0 + e;
-            Aa[e] = T(0);
-            Bb[e] = T(1);
-            if (e < per && i <= NX) {
+            A0[e] = T(0);
+            Cc[e] = T(0);
+            Bb[e] = T(0);
+            if (i <= NX) {
                 T v0 = v[d.at(i, k)], vr = v[d.at(i + 1, k)], vu = v[d.at(i, k + 1)];
                 T ax, bx, czu, czd;
-                if (mom) {  // Turbulent.cpp:83-88
+                if (mom) {
                     T Kc = K[d.at(i, k)], Kd = K[d.at(i, k - 1)], Kl = K[d.at(i - 1, k)], Kld = K[d.at(i - 1, k - 1)];
                     ax = T(0.5) * (Kc + Kd);
                     bx = T(0.5) * (Kl + Kld);
                     czu = T(a.p.rhou[k]) * T(0.5) * (Kc + Kl);
                     czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd + Kld);
-                } else {    // Turbulent.cpp:107-112
+                } else {
                     T Kc = K[d.at(i, k)], Kr = K[d.at(i + 1, k)], Kl = K[d.at(i - 1, k)];
                     T Ku = K[d.at(i, k + 1)], Kd = K[d.at(i, k - 1)];
                     ax = T(0.5) * (Kr + Kc);
@@ -583,12 +674,41 @@ __global__ void __launch_bounds__(kGSThreads) k_gs_diffuse(GSArgs<T> a) {
                     czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku + Kc);
                     czd = T(a.p.rhow[k]) * T(0.5) * (Kc + Kd);
                 }
-                Aa[e] = v0 + cx * (ax * (vr - v0) - bx * v0) + cz * (czu * (vu - v0) - czd * (v0 - vdn[e]));
+                T du = vu - v0, dd = v0;
+                if (kPert<T> && (f == 1 || f == 2)) {   // th', qv' about a profile
+                    du += T(a.p.d0[f - 1][k + 1]);
+                    dd += T(a.p.d0[f - 1][k]);
+                }
+                // v + cx (ax (vr - v) - bx (v - v'[i-1])) + cz (czu du - czd (dd - v'below))
+                A0[e] = v0 + cx * (ax * (vr - v0) - bx * v0) + cz * (czu * du - czd * dd);
+                Cc[e] = cz * czd;
                 Bb[e] = cx * bx;
-                cA = Aa[e] + Bb[e] * cA;
-                cB = Bb[e] * cB;
             }
         }
+    };
+    // row 0 (ghost) stands for the updated row below row 1: never modified
+#pragma unroll
+    for (int e = 0; e < PER; e++) {
+        int i = i0 + e;
+        vdn[e] = (i <= NX) ? v[d.at(i, 0)] : T(0);
+    }
+    coeffs(1);
+    for (int k = 1; k <= d.nz - 2; k++) {
+        T Aa[PER], Bk[PER];
+        T cA = T(0), cB = T(1);  // composition of this thread's maps (identity)
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+            Aa[e] = A0[e] + Cc[e] * vdn[e];
+            Bk[e] = Bb[e];
+            if (i0 + e <= NX) {
+                cA = Aa[e] + Bk[e] * cA;
+                cB = Bk[e] * cB;
+            }
+        }
+        const T xg = v[d.at(0, k)];   // ghost v'[0] of this row: never updated
+        // next row's coefficients (old values only; row k+1 is written after
+        // the barriers below and only in the next pass)
+        if (k + 1 <= d.nz - 2) coeffs(k + 1);
         // inclusive warp scan of the chunk maps (earlier maps on lower lanes)
         T sA = cA, sB = cB;
 #pragma unroll
@@ -621,23 +741,23 @@ __global__ void __launch_bounds__(kGSThreads) k_gs_diffuse(GSArgs<T> a) {
         T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
         if (lane == 0) { eA = T(0); eB = T(1); }
         T pA = (wid > 0) ? shA[wid - 1] : T(0), pB = (wid > 0) ? shB[wid - 1] : T(1);
-        T x = v[d.at(0, k)];                 // ghost v'[0]: never updated
-        x = pA + pB * x;
+        T x = pA + pB * xg;
         x = eA + eB * x;
         const T dcgr = mom ? T(a.p.dtcgr_zeta[k]) : T(a.p.dtcgr_th[k]);
+        const T tref = kPert<T> ? T(-a.p.dn[0][k]) : T(a.p.thb_init[k]);   // nudging target of th
 #pragma unroll
-        for (int e = 0; e < kGSMaxPerThread; e++) {
+        for (int e = 0; e < PER; e++) {
             int i = i0 + e;
-            if (e < per && i <= NX) {
-                x = Aa[e] + Bb[e] * x;
+            if (i <= NX) {
+                x = Aa[e] + Bk[e] * x;
                 vdn[e] = x;
                 T out = x;
                 if (a.nudge && f == 0) out = x - dcgr * x;                                  // Nudge_zeta
-                if (a.nudge && f == 1) out = x - dcgr * (x - T(a.p.thb_init[k]));           // Nudge_theta
+                if (a.nudge && f == 1) out = x - dcgr * (x - tref);                          // Nudge_theta
                 v[d.at(i, k)] = out;
             }
         }
-        __syncthreads();  // shA/shB reuse and row k+1 reads after row k writes
+        __syncthreads();  // shA/shB reuse
     }
 }
 
@@ -665,14 +785,15 @@ __global__ void k_nudge(NudgeArgs<T> a) {
     const bool inner = (i >= 1 && i <= d.nx - 2 && k >= 1 && k <= d.nz - 2);
     if (inner && a.do_th) {
         T x = a.thp[id];
-        a.thp[id] = x - T(a.p.dtcgr_th[k]) * (x - T(a.p.thb_init[k]));
+        T tref = kPert<T> ? T(-a.p.dn[0][k]) : T(a.p.thb_init[k]);
+        a.thp[id] = x - T(a.p.dtcgr_th[k]) * (x - tref);
     }
     if (inner && a.do_zeta) {
         T x = a.zetap[id];
         a.zetap[id] = x - T(a.p.dtcgr_zeta[k]) * x;
     }
     if (a.tau != 0.0)  // every cell, ghosts included (NumericalProcess.cpp:90-94)
-        a.qvp[id] = a.qvp[id] + T(a.c.dt) * (T(a.p.qvb0[k]) - a.qv[id]) / T(a.tau);
+        a.qvp[id] = a.qvp[id] + T(a.c.dt) * ((kPert<T> ? T(-a.p.dn[1][k]) : T(a.p.qvb0[k])) - a.qv[id]) / T(a.tau);
 }
 
 // ---------------------------------------------------------------------------
@@ -683,6 +804,7 @@ __global__ void k_nudge(NudgeArgs<T> a) {
 template <typename T>
 struct MeanArgs {
     Dims d;
+    const double *ref_th, *ref_qv;   // perturbation profiles (null in the FP64 step)
     const T *thp, *qvp;
     double *thb, *qvb, *thvb;
     double* ubar;   // [0] ubarTop, [1] ubarTopp
@@ -702,7 +824,9 @@ __global__ void k_update_mean(MeanArgs<T> a) {
     block_sum(s, sh);
     if (threadIdx.x == 0) {
         double n = (double)(d.nx - 2.);
-        double tb = s[0] / n, qb = s[1] / n, tv = tb * (1 + 0.608 * qb);
+        double tb = s[0] / n, qb = s[1] / n;
+        if (a.ref_th) { tb += a.ref_th[k]; qb += a.ref_qv[k]; }
+        double tv = tb * (1 + 0.608 * qb);
         a.thb[k] = tb;
         a.qvb[k] = qb;
         a.thvb[k] = tv;
@@ -860,19 +984,38 @@ __global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) {
 
 // Column integral u(i, k) = u(i, nz-2) + sum_{m=k}^{nz-3} (dw/dx - rhow zeta)(-dz)
 // from the top down (PoissonSolver.cpp:644-651), with the center halo of u.
-// One thread per interior column.
+// A block owns 32 columns (lanes) and kColSeg z-segments (warps): each thread
+// sums its segment, the segment totals are scanned from the top in shared
+// memory, then each thread writes its rows.
+constexpr int kColSeg = 8;
+
 template <typename T>
-__global__ void k_cal_u_columns(CalUArgs<T> a) {
+__global__ void __launch_bounds__(32 * kColSeg) k_cal_u_columns(CalUArgs<T> a) {
+    __shared__ T tot[kColSeg][32];
     const Dims& d = a.d;
-    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > d.nx - 2) return;
-    const int t = d.nz - 2;
-    const T utop = a.u[d.at(i, t)];
-    store_center(a.u, d, i, t, utop);
-    T area = T(0);
+    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+    const int i = 1 + blockIdx.x * 32 + lane;
+    const bool act = (i <= d.nx - 2);
+    const int t = d.nz - 2, nrow = d.nz - 3;               // rows k = 1..nz-3
+    // segment s covers rows from the top: k in (khi - len, khi]
+    const int r0 = (s * nrow) / kColSeg, r1 = ((s + 1) * nrow) / kColSeg;
     const T rdx = T(a.c.rdx), mdz = T(-a.c.dz);
-    for (int k = d.nz - 3; k >= 1; k--) {
-        area += ((a.w[d.at(i, k + 1)] - a.w[d.at(i - 1, k + 1)]) * rdx - T(a.p.rhow[k + 1]) * a.zetap[d.at(i, k + 1)]) * mdz;
+    auto term = [&](int k) -> T {
+        return ((a.w[d.at(i, k + 1)] - a.w[d.at(i - 1, k + 1)]) * rdx - T(a.p.rhow[k + 1]) * a.zetap[d.at(i, k + 1)]) * mdz;
+    };
+    T sum = T(0);
+    if (act)
+        for (int r = r0; r < r1; r++) sum += term(t - 1 - r);
+    tot[s][lane] = sum;
+    __syncthreads();
+    if (!act) return;
+    const T utop = a.u[d.at(i, t)];
+    T area = T(0);
+    for (int q = 0; q < s; q++) area += tot[q][lane];
+    if (s == 0) store_center(a.u, d, i, t, utop);
+    for (int r = r0; r < r1; r++) {
+        int k = t - 1 - r;
+        area += term(k);
         store_center(a.u, d, i, k, area + utop);
     }
 }

@@ -138,18 +138,28 @@ __global__ void k_to_float(int NX, int NK, int pitch, const double* a, float* b)
 }
 
 // Host [nx][nz] (k fast, stride sk per element) <-> device [nz][pitch].
+// `ref` (optional, [nz]) is subtracted on the way in and added on the way
+// out: the mixed step stores th and qv as perturbations from a profile.
 template <typename T>
-__global__ void k_from_host_layout(Dims d, const double* src, int sk, int off, T* dst) {
+__global__ void k_from_host_layout(Dims d, const double* src, int sk, int off, const double* ref, T* dst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i < d.nx && k < d.nz) dst[d.at(i, k)] = T(src[((size_t)i * d.nz + k) * sk + off]);
+    if (i < d.nx && k < d.nz) {
+        double v = src[((size_t)i * d.nz + k) * sk + off];
+        if (ref) v -= ref[k];
+        dst[d.at(i, k)] = T(v);
+    }
 }
 
 template <typename T>
-__global__ void k_to_host_layout(Dims d, const T* src, int sk, int off, double* dst) {
+__global__ void k_to_host_layout(Dims d, const T* src, int sk, int off, const double* ref, double* dst) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i < d.nx && k < d.nz) dst[((size_t)i * d.nz + k) * sk + off] = (double)src[d.at(i, k)];
+    if (i < d.nx && k < d.nz) {
+        double v = (double)src[d.at(i, k)];
+        if (ref) v += ref[k];
+        dst[((size_t)i * d.nz + k) * sk + off] = v;
+    }
 }
 
 }  // namespace vvm
@@ -195,159 +205,205 @@ struct Arena {
     }
 };
 
-constexpr int kCoarseMax = 8;
-
 // Multigrid hierarchy for the symmetric w-equation operator, precision P.
+//
+// Levels halve the column count while it is even (x-semicoarsening); a
+// power-of-two NX ends at one column, whose operator has no x part and is
+// solved exactly by one line solve. Otherwise the coarsest level has an odd
+// column count (at most kMaxOddCoarse) and gets 2*nc + 8 damped line sweeps.
+// Levels of at most 32 columns run inside one block (k_mg_coarse_cycle).
+constexpr int kMaxOddCoarse = 256;
+
+struct HostLine {   // host copy of one level's line factors
+    std::vector<double> lo, inv, cp, gL, gR, Minv;
+};
+
+// Dense inverse by Gauss-Jordan with partial pivoting (n <= 64).
+static void invert(std::vector<double>& A, int n) {
+    std::vector<double> I((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) I[(size_t)i * n + i] = 1.0;
+    for (int c = 0; c < n; c++) {
+        int piv = c;
+        for (int r = c + 1; r < n; r++)
+            if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)piv * n + c])) piv = r;
+        if (piv != c)
+            for (int j = 0; j < n; j++) {
+                std::swap(A[(size_t)c * n + j], A[(size_t)piv * n + j]);
+                std::swap(I[(size_t)c * n + j], I[(size_t)piv * n + j]);
+            }
+        double d = A[(size_t)c * n + c];
+        for (int j = 0; j < n; j++) {
+            A[(size_t)c * n + j] /= d;
+            I[(size_t)c * n + j] /= d;
+        }
+        for (int r = 0; r < n; r++) {
+            if (r == c) continue;
+            double f = A[(size_t)r * n + c];
+            if (f == 0.0) continue;
+            for (int j = 0; j < n; j++) {
+                A[(size_t)r * n + j] -= f * A[(size_t)c * n + j];
+                I[(size_t)r * n + j] -= f * I[(size_t)c * n + j];
+            }
+        }
+    }
+    A.swap(I);
+}
+
+// Segment factors, spikes and reduced inverse of tridiag(-rd, xdiag + ru + rd, -ru)
+// (first row without the -rd coupling, last without -ru: W = 0 beyond).
+static HostLine factor_partitioned(const std::vector<double>& xdiag, const std::vector<double>& ru,
+                                   const std::vector<double>& rd, int S) {
+    const int NK = (int)xdiag.size();
+    HostLine h;
+    h.lo.assign(NK, 0.0);
+    h.inv.assign(NK, 0.0);
+    h.cp.assign(NK, 0.0);
+    h.gL.assign(NK, 0.0);
+    h.gR.assign(NK, 0.0);
+    std::vector<double> first(S), last(S);
+    for (int s = 0; s < S; s++) {
+        int a = (s * NK) / S, b = ((s + 1) * NK) / S;
+        double cprev = 0.0;
+        for (int j = a; j < b; j++) {
+            double l = (j > a) ? -rd[j] : 0.0;
+            double u = (j < b - 1) ? -ru[j] : 0.0;
+            double den = (xdiag[j] + ru[j] + rd[j]) - l * cprev;
+            h.lo[j] = l;
+            h.inv[j] = 1.0 / den;
+            h.cp[j] = u * h.inv[j];
+            cprev = h.cp[j];
+        }
+        auto solve = [&](std::vector<double>& v) {   // v on [a, b) in place
+            double prev = 0.0;
+            for (int j = a; j < b; j++) { prev = (v[j] - h.lo[j] * prev) * h.inv[j]; v[j] = prev; }
+            double next = 0.0;
+            for (int j = b - 1; j >= a; j--) { next = v[j] - h.cp[j] * next; v[j] = next; }
+        };
+        std::vector<double> e(NK, 0.0);
+        if (a > 0) { e[a] = -rd[a]; solve(e); for (int j = a; j < b; j++) h.gL[j] = e[j]; }
+        std::fill(e.begin(), e.end(), 0.0);
+        if (b < NK) { e[b - 1] = -ru[b - 1]; solve(e); for (int j = a; j < b; j++) h.gR[j] = e[j]; }
+    }
+    const int n = 2 * S;
+    std::vector<double> M((size_t)n * n, 0.0);
+    for (int s = 0; s < S; s++) {
+        int a = (s * NK) / S, b = ((s + 1) * NK) / S;
+        for (int r = 0; r < 2; r++) {
+            int row = 2 * s + r, j = r ? b - 1 : a;
+            M[(size_t)row * n + row] += 1.0;
+            if (s > 0) M[(size_t)row * n + 2 * (s - 1) + 1] += h.gL[j];
+            if (s + 1 < S) M[(size_t)row * n + 2 * (s + 1)] += h.gR[j];
+        }
+    }
+    invert(M, n);
+    h.Minv = M;
+    return h;
+}
+
 template <typename P>
 struct Multigrid {
-    int NK = 0, nlev = 0;
+    int NK = 0, nlev = 0, S = 0, LS = 8, lc = 0;   // lc: first level run in the coarse block
+    bool exact_coarsest = true;
+    int coarse_sweeps = 1;
     std::vector<int> nx, pitch;
     std::vector<P*> f, x, y;
-    std::vector<double*> cx, lo, inv, cp;
+    std::vector<LineLevel> lines;
     double *ru = nullptr, *rd = nullptr;
-    int nc = 0;
-    double *Q = nullptr, *clo = nullptr, *cinv = nullptr, *ccp = nullptr, *xh = nullptr;
     P omega = P(2.0 / 3.0);
+
+    double* upload(Arena& ar, const std::vector<double>& v) {
+        double* d = ar.alloc<double>(v.size());
+        CK(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        return d;
+    }
 
     void build(Arena& ar, int NX, int NKr, const std::vector<double>& cx0, const std::vector<double>& ru_h,
                const std::vector<double>& rd_h) {
         NK = NKr;
+        LS = NK <= 256 ? 8 : (NK <= 512 ? 16 : 32);
+        S = (NK + LS - 1) / LS;
         int n = NX;
         nx.push_back(n);
-        while (n % 2 == 0 && n > kCoarseMax) {
+        while (n % 2 == 0 && n > 1) {
             n /= 2;
             nx.push_back(n);
         }
         nlev = (int)nx.size();
-        nc = nx.back();
-        ru = ar.alloc<double>(NK);
-        rd = ar.alloc<double>(NK);
-        CK(cudaMemcpy(ru, ru_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(rd, rd_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+        exact_coarsest = (nx.back() == 1);
+        coarse_sweeps = exact_coarsest ? 1 : 2 * nx.back() + 8;
+        lc = nlev - 1;
+        while (lc > 0 && nx[lc - 1] <= 32) lc--;
+        if (nlev - lc > kMaxCoarseLevels) lc = nlev - kMaxCoarseLevels;
+        ru = upload(ar, ru_h);
+        rd = upload(ar, rd_h);
         for (int l = 0; l < nlev; l++) {
             int pl = round_up(nx[l], kPad);
             pitch.push_back(pl);
             f.push_back(l == 0 ? nullptr : ar.alloc<P>((size_t)NK * pl));
             x.push_back(ar.alloc<P>((size_t)NK * pl));
             y.push_back(ar.alloc<P>((size_t)NK * pl));
-            std::vector<double> c(NK), lo_h(NK), inv_h(NK), cp_h(NK);
+            std::vector<double> c(NK), xd(NK);
             double sc = std::pow(0.25, l);
-            for (int k = 0; k < NK; k++) c[k] = cx0[k] * sc;
-            factor_line(c, 0.0, lo_h, inv_h, cp_h, ru_h, rd_h);
-            double* dcx = ar.alloc<double>(NK);
-            CK(cudaMemcpy(dcx, c.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
-            cx.push_back(dcx);
-            if (l < nlev - 1) {
-                double *dlo = ar.alloc<double>(NK), *dinv = ar.alloc<double>(NK), *dcp = ar.alloc<double>(NK);
-                CK(cudaMemcpy(dlo, lo_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
-                CK(cudaMemcpy(dinv, inv_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
-                CK(cudaMemcpy(dcp, cp_h.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
-                lo.push_back(dlo);
-                inv.push_back(dinv);
-                cp.push_back(dcp);
-            } else {
-                lo.push_back(nullptr);
-                inv.push_back(nullptr);
-                cp.push_back(nullptr);
-                build_coarse(ar, c, ru_h, rd_h);
-            }
-        }
-    }
-
-    // Thomas factors of tridiag(-rd, 2c*g + ru + rd, -ru) (g scales the x part
-    // for Fourier modes: g = 1 for line Jacobi, mu_m/2 on the coarsest level).
-    static void factor_line(const std::vector<double>& c, double mu, std::vector<double>& lo,
-                            std::vector<double>& inv, std::vector<double>& cp, const std::vector<double>& ru,
-                            const std::vector<double>& rd) {
-        int NK = (int)c.size();
-        double cprev = 0;
-        for (int k = 0; k < NK; k++) {
-            double xpart = (mu == 0.0) ? 2.0 * c[k] : c[k] * mu;
-            double diag = xpart + ru[k] + rd[k];
-            double l = (k > 0) ? -rd[k] : 0.0;
-            double u = (k < NK - 1) ? -ru[k] : 0.0;
-            double den = diag - l * cprev;
-            inv[k] = 1.0 / den;
-            cp[k] = u * inv[k];
-            lo[k] = l;
-            cprev = cp[k];
-        }
-    }
-
-    void build_coarse(Arena& ar, const std::vector<double>& c, const std::vector<double>& ru_h,
-                      const std::vector<double>& rd_h) {
-        const double pi = 3.14159265358979323846;
-        std::vector<double> Qh((size_t)nc * nc), mu(nc);
-        int m = 0;
-        for (int j = 0; j < nc; j++) Qh[(size_t)j * nc + m] = 1.0 / std::sqrt((double)nc);
-        mu[m++] = 0.0;
-        for (int fr = 1; 2 * fr < nc; fr++) {
-            for (int j = 0; j < nc; j++) {
-                Qh[(size_t)j * nc + m] = std::sqrt(2.0 / nc) * std::cos(2 * pi * fr * j / nc);
-                Qh[(size_t)j * nc + m + 1] = std::sqrt(2.0 / nc) * std::sin(2 * pi * fr * j / nc);
-            }
-            mu[m] = mu[m + 1] = 2.0 - 2.0 * std::cos(2 * pi * fr / nc);
-            m += 2;
-        }
-        if (nc % 2 == 0) {
-            for (int j = 0; j < nc; j++) Qh[(size_t)j * nc + m] = ((j & 1) ? -1.0 : 1.0) / std::sqrt((double)nc);
-            mu[m++] = 4.0;
-        }
-        std::vector<double> lo_a((size_t)nc * NK), inv_a((size_t)nc * NK), cp_a((size_t)nc * NK);
-        for (int q = 0; q < nc; q++) {
-            std::vector<double> lo_h(NK), inv_h(NK), cp_h(NK);
-            // mu == 0 must mean "no x part", not the line-Jacobi default
-            std::vector<double> cz(NK, 0.0);
-            const std::vector<double>& cc = (mu[q] == 0.0) ? cz : c;
-            factor_line(cc, mu[q] == 0.0 ? 1.0 : mu[q], lo_h, inv_h, cp_h, ru_h, rd_h);
+            bool exact = (l == nlev - 1) && exact_coarsest;
             for (int k = 0; k < NK; k++) {
-                lo_a[(size_t)q * NK + k] = lo_h[k];
-                inv_a[(size_t)q * NK + k] = inv_h[k];
-                cp_a[(size_t)q * NK + k] = cp_h[k];
+                c[k] = cx0[k] * sc;
+                xd[k] = exact ? 0.0 : 2.0 * c[k];
             }
+            HostLine h = factor_partitioned(xd, ru_h, rd_h, S);
+            LineLevel L{nx[l], pl, NK, S, upload(ar, c), upload(ar, h.lo), upload(ar, h.inv), upload(ar, h.cp),
+                        upload(ar, h.gL), upload(ar, h.gR), upload(ar, h.Minv)};
+            lines.push_back(L);
         }
-        Q = ar.alloc<double>((size_t)nc * nc);
-        clo = ar.alloc<double>((size_t)nc * NK);
-        cinv = ar.alloc<double>((size_t)nc * NK);
-        ccp = ar.alloc<double>((size_t)nc * NK);
-        xh = ar.alloc<double>((size_t)nc * NK);
-        CK(cudaMemcpy(Q, Qh.data(), Qh.size() * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(clo, lo_a.data(), lo_a.size() * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(cinv, inv_a.data(), inv_a.size() * sizeof(double), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ccp, cp_a.data(), cp_a.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
 
     ZOps zops() const { return ZOps{ru, rd, NK}; }
 
-    // z = M r; returns the buffer holding z (level-0 y, owned by the hierarchy).
+    void sweep(int l, const P* fl, const P* xin, const P* xc, int pc, int nc, P* out, P om, cudaStream_t st) {
+        SweepArgs<P> a{lines[l], zops(), fl, xin, xc, pc, nc, out, om};
+        dim3 g(cdiv(nx[l], 32)), b(32 * S);
+        if (LS == 8) k_line_sweep<P, 8><<<g, b, 0, st>>>(a);
+        else if (LS == 16) k_line_sweep<P, 16><<<g, b, 0, st>>>(a);
+        else k_line_sweep<P, 32><<<g, b, 0, st>>>(a);
+        CKL();
+    }
+
+    // z = M r (one V(1,1) cycle); returns the buffer holding z.
     P* apply(const P* r, cudaStream_t st) {
         const P* fl = r;
-        for (int l = 0; l < nlev - 1; l++) {
-            SmoothArgs<P> s{nx[l], pitch[l], NK, zops(), cx[l], LineFactors{lo[l], inv[l], cp[l]},
-                            fl, nullptr, nullptr, 0, 0, x[l], omega};
-            k_mg_smooth<P><<<cdiv(nx[l], 128), 128, 0, st>>>(s);
-            CKL();
-            RestrictArgs<P> ra{nx[l], pitch[l], NK, zops(), cx[l], fl, x[l], f[l + 1], pitch[l + 1]};
+        for (int l = 0; l < lc; l++) {
+            sweep(l, fl, nullptr, nullptr, 0, 0, x[l], omega, st);
+            RestrictArgs<P> ra{nx[l], pitch[l], NK, zops(), lines[l].cx, fl, x[l], f[l + 1], pitch[l + 1]};
             dim3 b(32, 8), g(cdiv(nx[l + 1], 32), cdiv(NK, 8));
             k_mg_restrict<P><<<g, b, 0, st>>>(ra);
             CKL();
             fl = f[l + 1];
         }
-        int L = nlev - 1;
-        CoarseArgs<P> ca{nc, pitch[L], NK, Q, clo, cinv, ccp, (L == 0) ? r : f[L], (L == 0) ? y[0] : x[L], xh};
-        k_mg_coarse<P><<<1, round_up(nc, 32), 0, st>>>(ca);
-        CKL();
-        if (L == 0) return y[0];
-        for (int l = L - 1; l >= 0; l--) {
-            const P* coarse = (l + 1 == L) ? x[L] : y[l + 1];
-            const P* fl2 = (l == 0) ? r : f[l];
-            SmoothArgs<P> s{nx[l], pitch[l], NK, zops(), cx[l], LineFactors{lo[l], inv[l], cp[l]},
-                            fl2, x[l], coarse, pitch[l + 1], nx[l + 1], y[l], omega};
-            k_mg_smooth<P><<<cdiv(nx[l], 128), 128, 0, st>>>(s);
-            CKL();
+        // levels lc..nlev-1 in one block
+        CoarseCycleArgs<P> ca{};
+        ca.nlev = nlev - lc;
+        for (int j = 0; j < ca.nlev; j++) {
+            ca.L[j] = lines[lc + j];
+            ca.f[j] = f[lc + j];
+            ca.x[j] = x[lc + j];
+            ca.y[j] = y[lc + j];
         }
-        return y[0];
+        ca.z = zops();
+        ca.f0 = fl;
+        ca.omega = omega;
+        ca.coarse_sweeps = coarse_sweeps;
+        if (LS == 8) k_mg_coarse_cycle<P, 8><<<1, 32 * S, 0, st>>>(ca);
+        else if (LS == 16) k_mg_coarse_cycle<P, 16><<<1, 32 * S, 0, st>>>(ca);
+        else k_mg_coarse_cycle<P, 32><<<1, 32 * S, 0, st>>>(ca);
+        CKL();
+        P* res = y[lc];
+        for (int l = lc - 1; l >= 0; l--) {
+            const P* fl2 = (l == 0) ? r : f[l];
+            sweep(l, fl2, x[l], res, pitch[l + 1], nx[l + 1], y[l], omega, st);
+            res = y[l];
+        }
+        return res;
     }
+
 };
 
 // Preconditioned CG on S d = g in precision P with the level-0 vectors below.
@@ -392,7 +448,7 @@ struct PCG {
     }
     dim3 block() const { return dim3(64, 4); }
     dim3 grid() const { return dim3(cdiv(NX, 64), cdiv(NK, 4)); }
-    VecArgs<P> vargs() const { return VecArgs<P>{NX, pitch, NK, mg.zops(), mg.cx[0], rhow_k}; }
+    VecArgs<P> vargs() const { return VecArgs<P>{NX, pitch, NK, mg.zops(), mg.lines[0].cx, rhow_k}; }
 
     double read_rr(cudaStream_t st) {
         CK(cudaMemcpyAsync(sc_host, sc, sizeof(CGScalars), cudaMemcpyDeviceToHost, st));
@@ -485,6 +541,8 @@ struct vvm_gpu_ctx {
            *z = nullptr, *z_zeta = nullptr, *vt_c1 = nullptr, *vt_fac = nullptr, *pc = nullptr,
            *dtcgr_th = nullptr, *dtcgr_zeta = nullptr, *q1ls = nullptr, *q2ls = nullptr;
     double pf1 = 0, pf2 = 0;
+    // perturbation profiles of th (0) and qv (1); used by the mixed step
+    double *pref[2] = {}, *pd0[2] = {}, *ps0[2] = {}, *pg0[2] = {}, *pdn[2] = {};
     std::vector<double> h_rhou, h_rhow;
     double* ubar = nullptr;   // [0] ubarTop, [1] ubarTopp
     double* dubar = nullptr;  // [2]
@@ -513,8 +571,13 @@ struct vvm_gpu_ctx {
 
     Profiles profiles() const {
         return Profiles{rhou, rhow, thvb, thb_init, qvb0, pib, pb, lambda2, vt_c1, vt_fac, pc,
-                        dtcgr_th, dtcgr_zeta, q1ls, q2ls, pf1, pf2};
+                        dtcgr_th, dtcgr_zeta, q1ls, q2ls, pf1, pf2,
+                        {pref[0], pref[1]}, {pd0[0], pd0[1]}, {ps0[0], ps0[1]}, {pg0[0], pg0[1]},
+                        {pdn[0], pdn[1]}};
     }
+    // profile subtracted from a stored field (mixed step: th and qv only)
+    const double* offset_th() const { return mixed ? pref[0] : nullptr; }
+    const double* offset_qv() const { return mixed ? pref[1] : nullptr; }
     dim3 blk() const { return dim3(64, 4); }
     dim3 grid_interior(int k0) const { return dim3(cdiv(d.nx - 2, 64), cdiv(d.nz - 1 - k0, 4)); }
     dim3 grid_all() const { return dim3(cdiv(d.nx, 64), cdiv(d.nz, 4)); }
@@ -678,7 +741,11 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
     CKL();
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
                 F.RKM, F.RKH, 0x1f, nudge ? 1 : 0};
-    k_gs_diffuse<T><<<5, kGSThreads, 0, c->stream>>>(g);
+    const int per = cdiv(c->d.nx - 2, kGSThreads);
+    if (per <= 1) k_gs_diffuse<T, 1><<<5, kGSThreads, 0, c->stream>>>(g);
+    else if (per <= 2) k_gs_diffuse<T, 2><<<5, kGSThreads, 0, c->stream>>>(g);
+    else if (per <= 4) k_gs_diffuse<T, 4><<<5, kGSThreads, 0, c->stream>>>(g);
+    else k_gs_diffuse<T, 8><<<5, kGSThreads, 0, c->stream>>>(g);
     CKL();
 }
 
@@ -697,7 +764,8 @@ template <typename T>
 void launch_update_mean(vvm_gpu_ctx* c, bool rotate) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
-    MeanArgs<T> a{c->d, F.th[fut], F.qv[fut], c->thb, c->qvb, c->thvb, c->ubar, rotate ? 1 : 0};
+    MeanArgs<T> a{c->d, c->offset_th(), c->offset_qv(), F.th[fut], F.qv[fut], c->thb, c->qvb, c->thvb,
+                  c->ubar, rotate ? 1 : 0};
     k_update_mean<T><<<c->d.nz - 2, 256, 0, c->stream>>>(a);
     CKL();
 }
@@ -806,7 +874,7 @@ void launch_cal_u(vvm_gpu_ctx* c) {
     CalUArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.zeta[fut], c->ubar};
     k_cal_u_top<T><<<1, kCalUThreads, 0, c->stream>>>(a);
     CKL();
-    k_cal_u_columns<T><<<cdiv(c->d.nx - 2, 128), 128, 0, c->stream>>>(a);
+    k_cal_u_columns<T><<<cdiv(c->d.nx - 2, 32), 32 * kColSeg, 0, c->stream>>>(a);
     CKL();
 }
 
@@ -834,19 +902,20 @@ int run_step(vvm_gpu_ctx* c) {
 // ---------------------------------------------------------------- transfer
 
 template <typename T>
-void upload_field(vvm_gpu_ctx* c, const double* host, int sk, int off, T* dst) {
+void upload_field(vvm_gpu_ctx* c, const double* host, int sk, int off, T* dst, const double* ref = nullptr) {
     size_t n = (size_t)c->d.nx * c->d.nz * sk;
     CK(cudaMemcpyAsync(c->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
-    k_from_host_layout<T><<<g, b, 0, c->stream>>>(c->d, c->staging, sk, off, dst);
+    k_from_host_layout<T><<<g, b, 0, c->stream>>>(c->d, c->staging, sk, off, ref, dst);
     CKL();
 }
 
 template <typename T>
-void download_field(vvm_gpu_ctx* c, const T* src, int sk, int off, double* host, bool first_of_pair) {
+void download_field(vvm_gpu_ctx* c, const T* src, int sk, int off, double* host, bool first_of_pair,
+                    const double* ref = nullptr) {
     size_t n = (size_t)c->d.nx * c->d.nz * sk;
     dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
-    k_to_host_layout<T><<<g, b, 0, c->stream>>>(c->d, src, sk, off, c->staging);
+    k_to_host_layout<T><<<g, b, 0, c->stream>>>(c->d, src, sk, off, ref, c->staging);
     CKL();
     if (!first_of_pair) {
         CK(cudaMemcpyAsync(host, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -866,8 +935,8 @@ int upload_prognostic_t(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
     for (const double* p : req)
         if (!p) return fail(c, VVM_GPU_EINVAL, "upload: prognostic field pointer is NULL");
     upload_field<T>(c, s->zeta, 1, 0, F.zeta[now]);
-    upload_field<T>(c, s->th, 1, 0, F.th[now]);
-    upload_field<T>(c, s->qv, 1, 0, F.qv[now]);
+    upload_field<T>(c, s->th, 1, 0, F.th[now], c->offset_th());
+    upload_field<T>(c, s->qv, 1, 0, F.qv[now], c->offset_qv());
     upload_field<T>(c, s->qc, 1, 0, F.qc[now]);
     upload_field<T>(c, s->qr, 1, 0, F.qr[now]);
     upload_field<T>(c, s->u, 1, 0, F.u);
@@ -883,13 +952,13 @@ int upload_state_t(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
     if (rc) return rc;
     int fut = 1 - c->cur;
     size_t n = c->d.cells();
-    auto up_or_zero = [&](const double* h, int sk, int off, T* dst) {
-        if (h) upload_field<T>(c, h, sk, off, dst);
+    auto up_or_zero = [&](const double* h, int sk, int off, T* dst, const double* ref = nullptr) {
+        if (h) upload_field<T>(c, h, sk, off, dst, ref);
         else CK(cudaMemsetAsync(dst, 0, n * sizeof(T), c->stream));
     };
     up_or_zero(s->zetap, 1, 0, F.zeta[fut]);
-    up_or_zero(s->thp, 1, 0, F.th[fut]);
-    up_or_zero(s->qvp, 1, 0, F.qv[fut]);
+    up_or_zero(s->thp, 1, 0, F.th[fut], c->offset_th());
+    up_or_zero(s->qvp, 1, 0, F.qv[fut], c->offset_qv());
     up_or_zero(s->qcp, 1, 0, F.qc[fut]);
     up_or_zero(s->qrp, 1, 0, F.qr[fut]);
     up_or_zero(s->RKM, 1, 0, F.RKM);
@@ -958,6 +1027,24 @@ int upload_profiles(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
     upload_profile(c, cze.data(), c->dtcgr_zeta);
     upload_profile(c, q1.data(), c->q1ls);
     upload_profile(c, q2.data(), c->q2ls);
+    // perturbation profiles (reference profile with its 1D center halo)
+    const double* tgt[2] = {s->thb_init, s->qvb0};
+    for (int j = 0; j < 2; j++) {
+        std::vector<double> r(tgt[j], tgt[j] + nz), d0(nz, 0.0), s0(nz, 0.0), g0(nz, 0.0), dn(nz, 0.0);
+        r[0] = r[1];
+        r[nz - 1] = r[nz - 2];
+        for (int k = 1; k < nz; k++) {
+            d0[k] = r[k] - r[k - 1];
+            s0[k] = r[k] + r[k - 1];
+        }
+        for (int k = 1; k < nz - 1; k++) g0[k] = r[k + 1] - r[k - 1];
+        for (int k = 0; k < nz; k++) dn[k] = r[k] - tgt[j][k];
+        upload_profile(c, r.data(), c->pref[j]);
+        upload_profile(c, d0.data(), c->pd0[j]);
+        upload_profile(c, s0.data(), c->ps0[j]);
+        upload_profile(c, g0.data(), c->pg0[j]);
+        upload_profile(c, dn.data(), c->pdn[j]);
+    }
     c->pf1 = 1E-3 * s->rhou[1];                                      // Iteration.cpp:115
     c->pf2 = std::pow(s->rhou[1] / s->rhow[1], -0.5);
     bool changed = c->h_rhou.empty() ||
@@ -982,10 +1069,11 @@ template <typename T>
 int download_prognostic_t(vvm_gpu_ctx* c, vvm_gpu_host_state* s) {
     Fields<T>& F = fields<T>(c);
     int now = c->cur;
-    struct { double* h; T* dptr; } m[] = {{s->zeta, F.zeta[now]}, {s->th, F.th[now]}, {s->qv, F.qv[now]},
-                                           {s->qc, F.qc[now]}, {s->qr, F.qr[now]}, {s->u, F.u}, {s->w, F.w}};
+    struct { double* h; T* dptr; const double* ref; } m[] = {
+        {s->zeta, F.zeta[now], nullptr}, {s->th, F.th[now], c->offset_th()}, {s->qv, F.qv[now], c->offset_qv()},
+        {s->qc, F.qc[now], nullptr}, {s->qr, F.qr[now], nullptr}, {s->u, F.u, nullptr}, {s->w, F.w, nullptr}};
     for (auto& e : m)
-        if (e.h) download_field<T>(c, e.dptr, 1, 0, e.h, false);
+        if (e.h) download_field<T>(c, e.dptr, 1, 0, e.h, false, e.ref);
     return VVM_GPU_OK;
 }
 
@@ -994,11 +1082,12 @@ int download_state_t(vvm_gpu_ctx* c, vvm_gpu_host_state* s) {
     Fields<T>& F = fields<T>(c);
     download_prognostic_t<T>(c, s);
     int fut = 1 - c->cur;
-    struct { double* h; T* dptr; } m[] = {{s->zetap, F.zeta[fut]}, {s->thp, F.th[fut]}, {s->qvp, F.qv[fut]},
-                                           {s->qcp, F.qc[fut]}, {s->qrp, F.qr[fut]}, {s->RKM, F.RKM},
-                                           {s->RKH, F.RKH}};
+    struct { double* h; T* dptr; const double* ref; } m[] = {
+        {s->zetap, F.zeta[fut], nullptr}, {s->thp, F.th[fut], c->offset_th()}, {s->qvp, F.qv[fut], c->offset_qv()},
+        {s->qcp, F.qc[fut], nullptr}, {s->qrp, F.qr[fut], nullptr}, {s->RKM, F.RKM, nullptr},
+        {s->RKH, F.RKH, nullptr}};
     for (auto& e : m)
-        if (e.h) download_field<T>(c, e.dptr, 1, 0, e.h, false);
+        if (e.h) download_field<T>(c, e.dptr, 1, 0, e.h, false, e.ref);
     double* hs[NHIST] = {s->dzeta_advect, s->dth_buoyancy, s->dth_advect, s->dqv_advect,
                          s->dqc_advect, s->dqr_advect, s->dqr_VT};
     for (int h = 0; h < NHIST; h++) {
@@ -1088,6 +1177,14 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     if (D.NX < 4 || D.NZ < 4) return fail(nullptr, VVM_GPU_EINVAL, "create: NX and NZ must be >= 4");
     if (D.NX > kGSThreads * kGSMaxPerThread)
         return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
+    if (D.NZ - 1 > 32 * kMaxSeg)
+        return fail(nullptr, VVM_GPU_EINVAL, "create: NZ exceeds 1025");
+    {
+        int odd = D.NX;
+        while (odd % 2 == 0) odd /= 2;
+        if (odd > kMaxOddCoarse)
+            return fail(nullptr, VVM_GPU_EINVAL, "create: the odd factor of NX must be <= 256");
+    }
     if (!(D.dx > 0) || !(D.dz > 0) || !(D.dt > 0)) return fail(nullptr, VVM_GPU_EINVAL, "create: dx, dz, dt must be > 0");
     if (D.precision != VVM_PREC_FP64 && D.precision != VVM_PREC_MIXED)
         return fail(nullptr, VVM_GPU_EINVAL, "create: unknown precision");
@@ -1129,6 +1226,13 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
                             &c->pib, &c->pb, &c->lambda2, &c->z, &c->z_zeta, &c->vt_c1, &c->vt_fac,
                             &c->pc, &c->dtcgr_th, &c->dtcgr_zeta, &c->q1ls, &c->q2ls};
         for (double** p : profs) *p = c->ar.alloc<double>(nz);
+        for (int j = 0; j < 2; j++) {
+            c->pref[j] = c->ar.alloc<double>(nz);
+            c->pd0[j] = c->ar.alloc<double>(nz);
+            c->ps0[j] = c->ar.alloc<double>(nz);
+            c->pg0[j] = c->ar.alloc<double>(nz);
+            c->pdn[j] = c->ar.alloc<double>(nz);
+        }
         c->ubar = c->ar.alloc<double>(2);
         c->dubar = c->ar.alloc<double>(2);
         dim3 g = c->grid_interior(1);
