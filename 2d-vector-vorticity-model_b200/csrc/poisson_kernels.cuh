@@ -64,9 +64,10 @@ __device__ __forceinline__ P prolong_at(const P* xc, int pitch_c, int nc, int kk
 // segments (segment s = rows [s*NK/S, (s+1)*NK/S)); within a segment
 // x = y - gL x[a-1] - gR x[b] where y solves the segment's own block and the
 // spikes gL, gR its couplings; the 2S segment-end unknowns satisfy a small
-// system whose inverse Minv (2S x 2S) is also precomputed. A block of
+// pentadiagonal system whose banded LU is also precomputed. A block of
 // 32 x S threads owns 32 adjacent columns (lanes: coalesced rows) and all S
-// segments (warps); the only serial chain is the segment's own Thomas pass.
+// segments (warps); the serial chains are the segment's own Thomas pass and
+// warp 0's banded solve of the 2S segment ends (one lane per column).
 
 constexpr int kMaxSeg = 32;
 
@@ -75,7 +76,7 @@ struct LineLevel {
     const double* cx;                 // x coupling of the level, [NK]
     const double *lo, *inv, *cp;      // segment-local Thomas factors, [NK]
     const double *gL, *gR;            // spikes, [NK]
-    const double* Minv;               // [2S][2S]
+    const double* band;               // banded LU of the reduced system, [5][2S]
 };
 
 // y = (segment-local) T^{-1} r for rows [a, a+len), in registers.
@@ -99,66 +100,110 @@ __device__ __forceinline__ void seg_thomas(const LineLevel& L, int a, int len, P
     }
 }
 
+// Solves the pentadiagonal reduced system of the segment ends in place in
+// sh[i*32 + lane] (i = 0..n-1): forward with the unit-lower band (l1, l2),
+// backward with the upper band (u1, u2) and 1/diag. Coefficient e of row i is
+// band[(e*n + i)*bstride]. One lane per column; only one warp calls it.
+template <typename P>
+__device__ __forceinline__ void reduced_solve(const double* band, int bstride, int n, P* sh, int lane) {
+    P z1 = P(0), z2 = P(0);
+    for (int i = 0; i < n; i++) {
+        P z = sh[i * 32 + lane] - P(band[(size_t)(0 * n + i) * bstride]) * z1 - P(band[(size_t)(1 * n + i) * bstride]) * z2;
+        sh[i * 32 + lane] = z;
+        z2 = z1;
+        z1 = z;
+    }
+    P x1 = P(0), x2 = P(0);
+    for (int i = n - 1; i >= 0; i--) {
+        P x = (sh[i * 32 + lane] - P(band[(size_t)(2 * n + i) * bstride]) * x1 -
+               P(band[(size_t)(3 * n + i) * bstride]) * x2) * P(band[(size_t)(4 * n + i) * bstride]);
+        sh[i * 32 + lane] = x;
+        x2 = x1;
+        x1 = x;
+    }
+}
+
+// After each warp parked its segment's first/last y in shY: solves for the
+// segment-end unknowns (warp 0) and returns this thread's couplings
+// x[a-1] (XL) and x[b] (XR). Contains two block barriers.
+template <typename P>
+__device__ __forceinline__ void segment_couplings(const double* band, int bstride, int S, P* shY, int lane, int s,
+                                                  bool lane_ok, P& XL, P& XR) {
+    __syncthreads();
+    if (s == 0 && lane_ok) reduced_solve(band, bstride, 2 * S, shY, lane);
+    __syncthreads();
+    XL = (s > 0 && s < S) ? shY[(2 * s - 1) * 32 + lane] : P(0);
+    XR = (s + 1 < S) ? shY[(2 * s + 2) * 32 + lane] : P(0);
+}
+
 // One damped line-Jacobi sweep (or, with xin = xc = null and omega = 1, an
 // exact line solve) for the 32-column strip starting at col0:
 //   out = X + omega * Dline^{-1} (f - S X),  X = xin + P xc.
-// shY: shared [2*kMaxSeg][32] of P. Every thread of the block must call it.
+// Each thread loads its column's segment rows (and one row above and below)
+// once; x neighbours come from the adjacent lanes by shuffle, and only the
+// strip's edge lanes load a halo column. shY: shared [2*kMaxSeg][32] of P.
+// Every thread of the block must call it.
 template <typename P, int LS>
 __device__ __forceinline__ void line_sweep(const LineLevel& L, const ZOps& z, int col0, const P* f,
                                            const P* xin, const P* xc, int pitch_c, int nc, P* out, P omega,
                                            P* shY) {
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
     const int i = col0 + lane;
-    const bool act = (i < L.nxl) && (s < L.S);
-    const int a = (s * L.NK) / L.S, b = ((s + 1) * L.NK) / L.S, len = b - a;
+    const bool wact = (s < L.S);                 // warp has a segment
+    const bool act = wact && (i < L.nxl);
+    const int a = wact ? (s * L.NK) / L.S : 0, b = wact ? ((s + 1) * L.NK) / L.S : 0, len = b - a;
     const bool has_x = (xin != nullptr) || (xc != nullptr);
+    auto Xat = [&](int kk, int col) -> P {
+        P v = xin ? xin[(size_t)kk * L.pitch + col] : P(0);
+        if (xc) v += prolong_at(xc, pitch_c, nc, kk, col);
+        return v;
+    };
     P y[LS], X[LS];
-    if (act) {
-        const int il = (i == 0) ? L.nxl - 1 : i - 1, ir = (i == L.nxl - 1) ? 0 : i + 1;
-        auto Xat = [&](int kk, int col) -> P {
-            P v = xin ? xin[(size_t)kk * L.pitch + col] : P(0);
-            if (xc) v += prolong_at(xc, pitch_c, nc, kk, col);
-            return v;
-        };
+    if (wact) {
+        const int il = (i == 0) ? L.nxl - 1 : i - 1, ir = (i >= L.nxl - 1) ? 0 : i + 1;
+        const bool own_l = (lane > 0), own_r = (lane < 31) && (i + 1 < L.nxl);
+        P Xv[LS + 2];
+        P fv[LS];
+#pragma unroll
+        for (int j = 0; j < LS + 2; j++) {
+            const int kk = a - 1 + j;
+            Xv[j] = (has_x && act && j <= len + 1 && kk >= 0 && kk < L.NK) ? Xat(kk, i) : P(0);
+        }
+#pragma unroll
+        for (int j = 0; j < LS; j++) fv[j] = (act && j < len) ? f[(size_t)(a + j) * L.pitch + i] : P(0);
 #pragma unroll
         for (int j = 0; j < LS; j++) {
-            X[j] = P(0);
-            y[j] = P(0);
-            if (j < len) {
-                const int kk = a + j;
-                P r = f[(size_t)kk * L.pitch + i];
-                if (has_x) {
-                    const P c = P(L.cx[kk]), ru = P(z.ru[kk]), rd = P(z.rd[kk]);
-                    P x0 = Xat(kk, i);
-                    P sx = (P(2) * c + ru + rd) * x0 - c * (Xat(kk, il) + Xat(kk, ir));
-                    if (kk + 1 < L.NK) sx -= ru * Xat(kk + 1, i);
-                    if (kk > 0) sx -= rd * Xat(kk - 1, i);
-                    r -= sx;
-                    X[j] = x0;
+            P xl = P(0), xr = P(0);
+            if (has_x) {
+                xl = __shfl_up_sync(0xffffffffu, Xv[j + 1], 1);
+                xr = __shfl_down_sync(0xffffffffu, Xv[j + 1], 1);
+                if (act && j < len) {
+                    if (!own_l) xl = Xat(a + j, il);
+                    if (!own_r) xr = Xat(a + j, ir);
                 }
-                y[j] = r;
             }
+            X[j] = Xv[j + 1];
+            P r = fv[j];
+            if (has_x && act && j < len) {
+                const int kk = a + j;
+                const P c = P(L.cx[kk]), ru = P(z.ru[kk]), rd = P(z.rd[kk]);
+                r -= (P(2) * c + ru + rd) * Xv[j + 1] - c * (xl + xr) - ru * Xv[j + 2] - rd * Xv[j];
+            }
+            y[j] = r;
         }
-        seg_thomas<P, LS>(L, a, len, y);
-        P ylast = y[0];
+        if (act) {
+            seg_thomas<P, LS>(L, a, len, y);
+            P ylast = y[0];
 #pragma unroll
-        for (int j = 0; j < LS; j++)
-            if (j == len - 1) ylast = y[j];
-        shY[(2 * s) * 32 + lane] = y[0];
-        shY[(2 * s + 1) * 32 + lane] = ylast;
+            for (int j = 0; j < LS; j++)
+                if (j == len - 1) ylast = y[j];
+            shY[(2 * s) * 32 + lane] = y[0];
+            shY[(2 * s + 1) * 32 + lane] = ylast;
+        }
     }
-    __syncthreads();
+    P XL, XR;
+    segment_couplings(L.band, 1, L.S, shY, lane, s, col0 + lane < L.nxl, XL, XR);
     if (act) {
-        const int S2 = 2 * L.S;
-        P XL = P(0), XR = P(0);
-        if (s > 0) {
-            const double* m = L.Minv + (size_t)(2 * (s - 1) + 1) * S2;
-            for (int q = 0; q < S2; q++) XL += P(m[q]) * shY[q * 32 + lane];
-        }
-        if (s + 1 < L.S) {
-            const double* m = L.Minv + (size_t)(2 * (s + 1)) * S2;
-            for (int q = 0; q < S2; q++) XR += P(m[q]) * shY[q * 32 + lane];
-        }
 #pragma unroll
         for (int j = 0; j < LS; j++) {
             if (j < len) {
@@ -208,12 +253,188 @@ __device__ __forceinline__ void restrict_point(const RestrictArgs<P>& a, int j, 
     a.fc[(size_t)kk * a.pitch_c + j] = P(0.25) * rm + P(0.5) * r0 + P(0.25) * rp;
 }
 
-template <typename P>
-__global__ void k_mg_restrict(RestrictArgs<P> a) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
-    if (j >= (a.nxl >> 1) || kk >= a.NK) return;
-    restrict_point(a, j, kk);
+// Pre-smoothing from a zero iterate fused with the restriction of the new
+// residual: x = omega * Dline^{-1} f (no neighbour values needed), then
+// r = f - S x and fc = full weighting of r. A block's 32 lanes cover fine
+// columns c0-2 .. c0+29 (periodic) and own c0 .. c0+27: it stores x there,
+// forms r on lanes 1..30 and the 14 coarse values whose three fine residuals
+// it holds. Neighbouring blocks recompute the 4 overlap columns.
+constexpr int kOwned = 28;
+
+template <typename P, int LS>
+__global__ void __launch_bounds__(32 * kMaxSeg) k_presmooth_restrict(LineLevel L, ZOps z, const P* f, P* xout,
+                                                                      P* fc, int pitch_c, P omega) {
+    __shared__ P shY[2 * kMaxSeg * 32];
+    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+    const int c0 = blockIdx.x * kOwned;
+    const int col = (c0 - 2 + lane + L.nxl) % L.nxl;
+    const bool wact = (s < L.S);
+    const int a = wact ? (s * L.NK) / L.S : 0, b = wact ? ((s + 1) * L.NK) / L.S : 0, len = b - a;
+    const bool owned = (lane >= 2) && (lane < 2 + kOwned) && (c0 + lane - 2 < L.nxl);
+    P y[LS], fv[LS];
+    if (wact) {
+#pragma unroll
+        for (int j = 0; j < LS; j++) {
+            fv[j] = (j < len) ? f[(size_t)(a + j) * L.pitch + col] : P(0);
+            y[j] = fv[j];
+        }
+        seg_thomas<P, LS>(L, a, len, y);
+        P ylast = y[0];
+#pragma unroll
+        for (int j = 0; j < LS; j++)
+            if (j == len - 1) ylast = y[j];
+        shY[(2 * s) * 32 + lane] = y[0];
+        shY[(2 * s + 1) * 32 + lane] = ylast;
+    }
+    P XL, XR;
+    segment_couplings(L.band, 1, L.S, shY, lane, s, true, XL, XR);
+    __syncthreads();   // every warp has read its couplings before shY is reused
+    P x[LS];
+    if (wact) {
+#pragma unroll
+        for (int j = 0; j < LS; j++) {
+            x[j] = P(0);
+            if (j < len) {
+                const int kk = a + j;
+                x[j] = omega * (y[j] - P(L.gL[kk]) * XL - P(L.gR[kk]) * XR);
+                if (owned) xout[(size_t)kk * L.pitch + col] = x[j];
+            }
+        }
+        // segment ends of x for the z neighbours of the residual
+        P xlast = x[0];
+#pragma unroll
+        for (int j = 0; j < LS; j++)
+            if (j == len - 1) xlast = x[j];
+        shY[(2 * s) * 32 + lane] = x[0];
+        shY[(2 * s + 1) * 32 + lane] = xlast;
+    }
+    __syncthreads();
+    if (wact) {
+        const P xbelow = (s > 0) ? shY[(2 * s - 1) * 32 + lane] : P(0);     // x at row a-1
+        const P xabove = (s + 1 < L.S) ? shY[(2 * s + 2) * 32 + lane] : P(0);  // x at row b
+#pragma unroll
+        for (int j = 0; j < LS; j++) {
+            const P xl = __shfl_up_sync(0xffffffffu, x[j], 1);
+            const P xr = __shfl_down_sync(0xffffffffu, x[j], 1);
+            P r = P(0);
+            if (j < len) {
+                const int kk = a + j;
+                const P c = P(L.cx[kk]), ru = P(z.ru[kk]), rd = P(z.rd[kk]);
+                P xd = (j == 0) ? xbelow : x[(j > 0) ? j - 1 : 0];
+                P xu = (j == len - 1) ? xabove : x[(j + 1 < LS) ? j + 1 : LS - 1];
+                r = fv[j] - ((P(2) * c + ru + rd) * x[j] - c * (xl + xr) - ru * xu - rd * xd);
+            }
+            const P rm = __shfl_up_sync(0xffffffffu, r, 1);
+            const P rp = __shfl_down_sync(0xffffffffu, r, 1);
+            if (j < len && owned && (lane & 1) == 0)
+                fc[(size_t)(a + j) * pitch_c + (col >> 1)] = P(0.25) * rm + P(0.5) * r + P(0.25) * rp;
+        }
+    }
+}
+
+// Exact solve on a level of nc <= 32 columns. The operator is separable (x
+// coefficients depend on the row only, periodic in x), so a real orthonormal
+// Fourier basis Q (nc x nc) diagonalises its x part: mode m needs the
+// tridiagonal z solve of (cx mu_m + ru + rd, -ru, -rd), mu_m the eigenvalue
+// of the periodic [-1 2 -1]. One block: f and Q are staged in shared memory,
+// each (mode lane, segment warp) transforms its rows and runs the partitioned
+// solve with that mode's precomputed factors (warp 0 solving every mode's
+// reduced system), and the inverse transform writes x.
+struct ModeSolve {
+    int nc, pitch, NK, S;
+    const double* Q;                  // [nc][nc], Q[col*nc + m]
+    const double *lo, *inv, *cp, *gL, *gR;   // [NK][nc]: mode fastest (coalesced)
+    const double* band;               // [5][2S][nc]
+};
+
+// Segment Thomas pass of one mode (factors interleaved by mode, stride nc).
+template <typename P, int LS>
+__device__ __forceinline__ void seg_thomas_modes(const ModeSolve& M, int m, int a, int len, P (&r)[LS]) {
+    const int nc = M.nc;
+    P prev = P(0);
+#pragma unroll
+    for (int j = 0; j < LS; j++) {
+        if (j < len) {
+            const size_t e = (size_t)(a + j) * nc + m;
+            prev = (r[j] - P(M.lo[e]) * prev) * P(M.inv[e]);
+            r[j] = prev;
+        }
+    }
+    P next = P(0);
+#pragma unroll
+    for (int j = LS - 1; j >= 0; j--) {
+        if (j < len) {
+            next = r[j] - P(M.cp[(size_t)(a + j) * nc + m]) * next;
+            r[j] = next;
+        }
+    }
+}
+
+template <typename P, int LS>
+__global__ void __launch_bounds__(32 * kMaxSeg) k_coarse_modes(ModeSolve M, const P* f, P* x) {
+    extern __shared__ unsigned char smem_raw[];
+    P* fs = reinterpret_cast<P*>(smem_raw);             // [NK][nc]
+    P* xh = fs + (size_t)M.NK * M.nc;                   // [NK][nc]
+    __shared__ P shY[2 * kMaxSeg * 32];
+    __shared__ P Qs[32 * 32];    // Q[col][m]: forward transform, lanes = m
+    __shared__ P QT[32 * 32];    // Q[col][m] at [m][col]: inverse, lanes = col
+    const int nc = M.nc, NK = M.NK, S = M.S;
+    for (int t = threadIdx.x; t < NK * nc; t += blockDim.x) {
+        int kk = t / nc, c = t % nc;
+        fs[t] = f[(size_t)kk * M.pitch + c];
+    }
+    for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
+        Qs[t] = P(M.Q[t]);
+        QT[(t % nc) * nc + t / nc] = P(M.Q[t]);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
+    const bool act = (s < S) && (lane < nc);
+    const int a = (s < S) ? (s * NK) / S : 0, b = (s < S) ? ((s + 1) * NK) / S : 0, len = b - a;
+    const int m = lane;
+    P y[LS];
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < LS; j++) {
+            P v = P(0);
+            if (j < len) {
+                const P* row = fs + (size_t)(a + j) * nc;
+#pragma unroll 8
+                for (int c = 0; c < nc; c++) v += Qs[c * nc + m] * row[c];
+            }
+            y[j] = v;
+        }
+        seg_thomas_modes<P, LS>(M, m, a, len, y);
+        P ylast = y[0];
+#pragma unroll
+        for (int j = 0; j < LS; j++)
+            if (j == len - 1) ylast = y[j];
+        shY[(2 * s) * 32 + lane] = y[0];
+        shY[(2 * s + 1) * 32 + lane] = ylast;
+    }
+    P XL, XR;
+    segment_couplings(M.band + m, nc, S, shY, lane, s, lane < nc, XL, XR);
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < LS; j++) {
+            if (j < len) {
+                const int kk = a + j;
+                xh[(size_t)kk * nc + m] = y[j] - P(M.gL[(size_t)kk * nc + m]) * XL - P(M.gR[(size_t)kk * nc + m]) * XR;
+            }
+        }
+    }
+    __syncthreads();
+    if (act) {   // lane = output column
+        const int cc = lane;
+        for (int j = 0; j < len; j++) {
+            const int kk = a + j;
+            const P* row = xh + (size_t)kk * nc;
+            P v = P(0);
+#pragma unroll 8
+            for (int q = 0; q < nc; q++) v += QT[q * nc + cc] * row[q];
+            x[(size_t)kk * M.pitch + cc] = v;
+        }
+    }
 }
 
 // The coarse end of the V-cycle in one block, with block barriers between
@@ -381,7 +602,48 @@ __global__ void k_cg_residual(VecArgs<P> v, const P* f, const P* x, P* r, double
 
 enum : int { CG_SET_BB = 0, CG_SET_RR, CG_SET_RZ, CG_PQ_ALPHA, CG_RZ_BETA };
 
+// Device-side loop state of a graph-captured solve.
+struct CGCtl {
+    int it;          // CG iterations of the current (inner) solve
+    int total;       // CG iterations summed over refinement passes
+    int outer;       // refinement passes
+    int pad;
+    double rr0;      // squared initial residual of the inner solve
+    double relres;   // final ||b - A W|| / ||b||
+};
+
 // Finishes a partial-sum array (fixed order) and updates the CG scalars.
+// CG_RZ_BETA with ctl != null takes beta = 0 on the first iteration.
 __global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mode);
+__global__ void k_cg_scalar_it(const double* partial, int n, CGScalars* sc, const CGCtl* ctl);
+
+// p = z (first iteration of ctl) or z + beta p.
+template <typename P>
+__global__ void k_cg_dir_it(VecArgs<P> v, const CGScalars* sc, const CGCtl* ctl, const P* z, P* p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < v.nx && kk < v.NK) {
+        size_t id = (size_t)kk * v.pitch + i;
+        p[id] = (ctl->it == 0) ? z[id] : P((double)z[id] + sc->beta * (double)p[id]);
+    }
+}
+
+// W = 0 when ||b|| = 0 (the solution of A W = 0), read on the device.
+__global__ void k_zero_if_b0(int NX, int NK, int pitch, const CGScalars* sc, double* W);
+
+// Loop conditions of graph-captured solves (one thread). `init` starts a
+// loop, otherwise one iteration has finished and `body_kernels` kernels of
+// its body ran (added to *exec, the context's count of executed kernels).
+//   plain  : continue while ||rhow r||^2 > tol^2 ||b||^2, it < maxit
+//   inner  : continue while ||rhow r||^2 > rtol^2 rr0, it < maxit
+//   outer  : continue while the FP64 residual is above tol and the inner
+//            iterations so far are below maxit
+__global__ void k_loop_plain(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double tol2,
+                             int maxit, int init, long long* exec, int body_kernels);
+__global__ void k_loop_inner(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double rtol2,
+                             int maxit, int init, long long* exec, int body_kernels);
+__global__ void k_loop_outer(const CGScalars* sc64, CGCtl* ctl, const CGCtl* inner,
+                             cudaGraphConditionalHandle h, double tol2, int maxit, int init, long long* exec,
+                             int body_kernels);
 
 }  // namespace vvm

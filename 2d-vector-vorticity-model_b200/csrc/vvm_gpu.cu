@@ -61,6 +61,67 @@ __global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mod
     }
 }
 
+__global__ void k_cg_scalar_it(const double* partial, int n, CGScalars* sc, const CGCtl* ctl) {
+    __shared__ double sh[32];
+    double s[1] = {0};
+    for (int b = threadIdx.x; b < n; b += blockDim.x) s[0] += partial[b];
+    block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        double v = s[0];
+        sc->rz_new = v;
+        sc->beta = (ctl->it == 0 || sc->rz == 0.0) ? 0.0 : v / sc->rz;
+        sc->rz = v;
+    }
+}
+
+__global__ void k_zero_if_b0(int NX, int NK, int pitch, const CGScalars* sc, double* W) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii < NX && kk < NK && sc->bb == 0.0) W[(size_t)kk * pitch + ii] = 0.0;
+}
+
+__global__ void k_loop_plain(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double tol2,
+                             int maxit, int init, long long* exec, int body_kernels) {
+    if (init) ctl->it = 0;
+    else { ctl->it++; *exec += body_kernels; }
+    const double rr = sc->rr, bb = sc->bb;
+    bool more = (bb > 0.0) && (rr > tol2 * bb) && (ctl->it < maxit) && isfinite(rr);
+    ctl->total = ctl->it;
+    ctl->relres = (bb > 0.0) ? sqrt(rr / bb) : 0.0;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+__global__ void k_loop_inner(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double rtol2,
+                             int maxit, int init, long long* exec, int body_kernels) {
+    if (init) {
+        ctl->it = 0;
+        ctl->rr0 = sc->rr;
+    } else {
+        ctl->it++;
+        *exec += body_kernels;
+    }
+    const double rr = sc->rr;
+    bool more = (ctl->rr0 > 0.0) && (rr > rtol2 * ctl->rr0) && (ctl->it < maxit) && isfinite(rr);
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+__global__ void k_loop_outer(const CGScalars* sc64, CGCtl* ctl, const CGCtl* inner,
+                             cudaGraphConditionalHandle h, double tol2, int maxit, int init, long long* exec,
+                             int body_kernels) {
+    if (init) {
+        ctl->outer = 0;
+        ctl->total = 0;
+    } else {
+        ctl->outer++;
+        ctl->total += (inner->it > 0 ? inner->it : 1);
+        *exec += body_kernels;
+    }
+    const double rr = sc64->rr, bb = sc64->bb;
+    ctl->relres = (bb > 0.0) ? sqrt(rr / bb) : 0.0;
+    bool more = (bb > 0.0) && (rr > tol2 * bb) && isfinite(rr) && (ctl->total < maxit) && (ctl->outer < 20);
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
 // b = rhow_k^2 (zetap[i+1][k] - zetap[i][k]) dx for k = 2..nz-2, i = 1..nx-2
 // (PoissonSolver.cpp:444-450); stores f = -b / rhow_k and partial ||b||^2.
 template <typename T>
@@ -116,6 +177,19 @@ __global__ void k_w_from_W(Dims d, const double* rhow, const double* W, int pitc
     if (i > d.nx - 2 || k > d.nz - 2) return;
     double v = W[(size_t)(k - 2) * pitch_f + (i - 1)] / rhow[k];
     store_westdown(w, d, i, k, T(v));
+}
+
+// Initial guess of the next cal_w from the last two solutions:
+// W <- 2 W - Wprev, Wprev <- W (old).
+__global__ void k_extrapolate(int NX, int NK, int pitch, double* W, double* Wprev) {
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ii < NX && kk < NK) {
+        size_t id = (size_t)kk * pitch + ii;
+        double w = W[id];
+        W[id] = 2.0 * w - Wprev[id];
+        Wprev[id] = w;
+    }
 }
 
 // x64 += (double) d32 (iterative refinement).
@@ -214,8 +288,85 @@ struct Arena {
 // Levels of at most 32 columns run inside one block (k_mg_coarse_cycle).
 constexpr int kMaxOddCoarse = 256;
 
+// Launch counter and, when enabled, per-kernel-class device time from CUDA
+// events recorded around each launch on the launching stream.
+struct Stats {
+    bool on = false;
+    long long launches = 0;
+    double ms[VVM_K_COUNT] = {};
+    long long cnt[VVM_K_COUNT] = {};
+    struct Rec {
+        int id;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t ev() {
+        if (pool.empty()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            return e;
+        }
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    void resolve() {
+        for (auto& r : pending) {
+            CK(cudaEventSynchronize(r.b));
+            float t = 0;
+            CK(cudaEventElapsedTime(&t, r.a, r.b));
+            ms[r.id] += t;
+            cnt[r.id]++;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+    void reset() {
+        resolve();
+        for (int i = 0; i < VVM_K_COUNT; i++) { ms[i] = 0; cnt[i] = 0; }
+        launches = 0;
+    }
+    ~Stats() {
+        for (auto& r : pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+struct Timed {
+    Stats* s;
+    int id;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    Timed(Stats* s_, int id_, cudaStream_t st_) : s(s_), id(id_), st(st_) {
+        if (!s) return;
+        s->launches++;
+        if (s->on) {
+            a = s->ev();
+            CK(cudaEventRecord(a, st));
+        }
+    }
+    ~Timed() {
+        if (!a) return;
+        cudaEvent_t b = s->ev();
+        cudaEventRecord(b, st);
+        s->pending.push_back({id, a, b});
+        if (s->pending.size() > 8192) s->resolve();
+    }
+};
+
+#define LAUNCH(S, ID, ST, ...)      \
+    do {                            \
+        Timed t_((S), (ID), (ST));  \
+        __VA_ARGS__;                \
+    } while (0)
+
 struct HostLine {   // host copy of one level's line factors
-    std::vector<double> lo, inv, cp, gL, gR, Minv;
+    std::vector<double> lo, inv, cp, gL, gR;
+    // banded LU of the 2S x 2S reduced system (lower and upper bandwidth 2):
+    // [5][2S] = l1, l2, u1, u2, 1/diag
+    std::vector<double> band;
 };
 
 // Dense inverse by Gauss-Jordan with partial pivoting (n <= 64).
@@ -284,6 +435,10 @@ static HostLine factor_partitioned(const std::vector<double>& xdiag, const std::
         std::fill(e.begin(), e.end(), 0.0);
         if (b < NK) { e[b - 1] = -ru[b - 1]; solve(e); for (int j = a; j < b; j++) h.gR[j] = e[j]; }
     }
+    // Reduced system of the segment ends, unknowns (first_s, last_s):
+    //   x_j + gL_s[j] last_{s-1} + gR_s[j] first_{s+1} = y_j,  j = a_s, b_s - 1.
+    // In the order (first_0, last_0, first_1, ...) it is pentadiagonal; its LU
+    // without pivoting (I + small spikes) stays in the band.
     const int n = 2 * S;
     std::vector<double> M((size_t)n * n, 0.0);
     for (int s = 0; s < S; s++) {
@@ -295,14 +450,29 @@ static HostLine factor_partitioned(const std::vector<double>& xdiag, const std::
             if (s + 1 < S) M[(size_t)row * n + 2 * (s + 1)] += h.gR[j];
         }
     }
-    invert(M, n);
-    h.Minv = M;
+    for (int c = 0; c < n; c++)        // Doolittle in place: M = L U
+        for (int r = c + 1; r < n && r <= c + 2; r++) {
+            double f = M[(size_t)r * n + c] / M[(size_t)c * n + c];
+            M[(size_t)r * n + c] = f;
+            for (int j = c + 1; j < n && j <= c + 2; j++) M[(size_t)r * n + j] -= f * M[(size_t)c * n + j];
+        }
+    h.band.assign((size_t)5 * n, 0.0);
+    for (int i = 0; i < n; i++) {
+        h.band[0 * n + i] = (i >= 1) ? M[(size_t)i * n + i - 1] : 0.0;
+        h.band[1 * n + i] = (i >= 2) ? M[(size_t)i * n + i - 2] : 0.0;
+        h.band[2 * n + i] = (i + 1 < n) ? M[(size_t)i * n + i + 1] : 0.0;
+        h.band[3 * n + i] = (i + 2 < n) ? M[(size_t)i * n + i + 2] : 0.0;
+        h.band[4 * n + i] = 1.0 / M[(size_t)i * n + i];
+    }
     return h;
 }
 
 template <typename P>
 struct Multigrid {
     int NK = 0, nlev = 0, S = 0, LS = 8, lc = 0;   // lc: first level run in the coarse block
+    bool modes = false;        // level lc is solved exactly by Fourier modes
+    ModeSolve ms{};
+    size_t mode_smem = 0;
     bool exact_coarsest = true;
     int coarse_sweeps = 1;
     std::vector<int> nx, pitch;
@@ -310,6 +480,7 @@ struct Multigrid {
     std::vector<LineLevel> lines;
     double *ru = nullptr, *rd = nullptr;
     P omega = P(2.0 / 3.0);
+    Stats* stats = nullptr;
 
     double* upload(Arena& ar, const std::vector<double>& v) {
         double* d = ar.alloc<double>(v.size());
@@ -334,6 +505,17 @@ struct Multigrid {
         lc = nlev - 1;
         while (lc > 0 && nx[lc - 1] <= 32) lc--;
         if (nlev - lc > kMaxCoarseLevels) lc = nlev - kMaxCoarseLevels;
+        // exact Fourier-mode solve on the first level of at most 32 columns
+        // when its two shared-memory tiles fit
+        for (int l = 0; l < nlev; l++) {
+            if (nx[l] <= 32 && (size_t)2 * NK * nx[l] * sizeof(P) <= 160 * 1024) {
+                modes = true;
+                lc = l;
+                nlev = l + 1;   // coarser levels are not needed
+                nx.resize(nlev);
+                break;
+            }
+        }
         ru = upload(ar, ru_h);
         rd = upload(ar, rd_h);
         for (int l = 0; l < nlev; l++) {
@@ -351,9 +533,59 @@ struct Multigrid {
             }
             HostLine h = factor_partitioned(xd, ru_h, rd_h, S);
             LineLevel L{nx[l], pl, NK, S, upload(ar, c), upload(ar, h.lo), upload(ar, h.inv), upload(ar, h.cp),
-                        upload(ar, h.gL), upload(ar, h.gR), upload(ar, h.Minv)};
+                        upload(ar, h.gL), upload(ar, h.gR), upload(ar, h.band)};
             lines.push_back(L);
+            if (modes && l == lc) build_modes(ar, c, ru_h, rd_h, pl);
         }
+    }
+
+    // Orthonormal real Fourier basis of nc periodic columns and the per-mode
+    // partitioned factors of (cx mu_m + ru + rd, -ru, -rd).
+    void build_modes(Arena& ar, const std::vector<double>& c, const std::vector<double>& ru_h,
+                     const std::vector<double>& rd_h, int pl) {
+        const int nc = nx[lc];
+        const double pi = 3.14159265358979323846;
+        std::vector<double> Q((size_t)nc * nc, 0.0), mu(nc, 0.0);
+        int m = 0;
+        for (int j = 0; j < nc; j++) Q[(size_t)j * nc + m] = 1.0 / std::sqrt((double)nc);
+        mu[m++] = 0.0;
+        for (int fr = 1; 2 * fr < nc; fr++) {
+            for (int j = 0; j < nc; j++) {
+                Q[(size_t)j * nc + m] = std::sqrt(2.0 / nc) * std::cos(2 * pi * fr * j / nc);
+                Q[(size_t)j * nc + m + 1] = std::sqrt(2.0 / nc) * std::sin(2 * pi * fr * j / nc);
+            }
+            mu[m] = mu[m + 1] = 2.0 - 2.0 * std::cos(2 * pi * fr / nc);
+            m += 2;
+        }
+        if (nc % 2 == 0) {
+            for (int j = 0; j < nc; j++) Q[(size_t)j * nc + m] = ((j & 1) ? -1.0 : 1.0) / std::sqrt((double)nc);
+            mu[m++] = 4.0;
+        }
+        std::vector<double> lo((size_t)NK * nc), inv((size_t)NK * nc), cp((size_t)NK * nc), gL((size_t)NK * nc),
+            gR((size_t)NK * nc), Mi((size_t)5 * 2 * S * nc);
+        const size_t S2 = 2 * (size_t)S;
+        for (int q = 0; q < nc; q++) {   // mode fastest: lanes (modes) read consecutive words
+            std::vector<double> xd(NK);
+            for (int k = 0; k < NK; k++) xd[k] = c[k] * mu[q];
+            HostLine h = factor_partitioned(xd, ru_h, rd_h, S);
+            for (int k = 0; k < NK; k++) {
+                lo[(size_t)k * nc + q] = h.lo[k];
+                inv[(size_t)k * nc + q] = h.inv[k];
+                cp[(size_t)k * nc + q] = h.cp[k];
+                gL[(size_t)k * nc + q] = h.gL[k];
+                gR[(size_t)k * nc + q] = h.gR[k];
+            }
+            for (size_t e = 0; e < 5 * S2; e++) Mi[e * nc + q] = h.band[e];
+        }
+        ms = ModeSolve{nc, pl, NK, S, upload(ar, Q), upload(ar, lo), upload(ar, inv), upload(ar, cp),
+                       upload(ar, gL), upload(ar, gR), upload(ar, Mi)};
+        mode_smem = (size_t)2 * NK * nc * sizeof(P);
+        auto setattr = [&](auto kern) {
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mode_smem));
+        };
+        if (LS == 8) setattr(k_coarse_modes<P, 8>);
+        else if (LS == 16) setattr(k_coarse_modes<P, 16>);
+        else setattr(k_coarse_modes<P, 32>);
     }
 
     ZOps zops() const { return ZOps{ru, rd, NK}; }
@@ -361,9 +593,9 @@ struct Multigrid {
     void sweep(int l, const P* fl, const P* xin, const P* xc, int pc, int nc, P* out, P om, cudaStream_t st) {
         SweepArgs<P> a{lines[l], zops(), fl, xin, xc, pc, nc, out, om};
         dim3 g(cdiv(nx[l], 32)), b(32 * S);
-        if (LS == 8) k_line_sweep<P, 8><<<g, b, 0, st>>>(a);
-        else if (LS == 16) k_line_sweep<P, 16><<<g, b, 0, st>>>(a);
-        else k_line_sweep<P, 32><<<g, b, 0, st>>>(a);
+        if (LS == 8) LAUNCH(stats, VVM_K_MG_SWEEP, st, k_line_sweep<P, 8><<<g, b, 0, st>>>(a));
+        else if (LS == 16) LAUNCH(stats, VVM_K_MG_SWEEP, st, k_line_sweep<P, 16><<<g, b, 0, st>>>(a));
+        else LAUNCH(stats, VVM_K_MG_SWEEP, st, k_line_sweep<P, 32><<<g, b, 0, st>>>(a));
         CKL();
     }
 
@@ -371,31 +603,42 @@ struct Multigrid {
     P* apply(const P* r, cudaStream_t st) {
         const P* fl = r;
         for (int l = 0; l < lc; l++) {
-            sweep(l, fl, nullptr, nullptr, 0, 0, x[l], omega, st);
-            RestrictArgs<P> ra{nx[l], pitch[l], NK, zops(), lines[l].cx, fl, x[l], f[l + 1], pitch[l + 1]};
-            dim3 b(32, 8), g(cdiv(nx[l + 1], 32), cdiv(NK, 8));
-            k_mg_restrict<P><<<g, b, 0, st>>>(ra);
+            // pre-smoothing from zero fused with the restriction of its residual
+            dim3 g(cdiv(nx[l], kOwned)), b(32 * S);
+            if (LS == 8) LAUNCH(stats, VVM_K_MG_SWEEP, st, k_presmooth_restrict<P, 8><<<g, b, 0, st>>>(lines[l], zops(), fl, x[l], f[l + 1], pitch[l + 1], omega));
+            else if (LS == 16) LAUNCH(stats, VVM_K_MG_SWEEP, st, k_presmooth_restrict<P, 16><<<g, b, 0, st>>>(lines[l], zops(), fl, x[l], f[l + 1], pitch[l + 1], omega));
+            else LAUNCH(stats, VVM_K_MG_SWEEP, st, k_presmooth_restrict<P, 32><<<g, b, 0, st>>>(lines[l], zops(), fl, x[l], f[l + 1], pitch[l + 1], omega));
             CKL();
             fl = f[l + 1];
         }
-        // levels lc..nlev-1 in one block
-        CoarseCycleArgs<P> ca{};
-        ca.nlev = nlev - lc;
-        for (int j = 0; j < ca.nlev; j++) {
-            ca.L[j] = lines[lc + j];
-            ca.f[j] = f[lc + j];
-            ca.x[j] = x[lc + j];
-            ca.y[j] = y[lc + j];
+        P* res;
+        if (modes) {
+            P* out = (lc == 0) ? y[0] : x[lc];
+            if (LS == 8) LAUNCH(stats, VVM_K_MG_COARSE, st, k_coarse_modes<P, 8><<<1, 32 * S, mode_smem, st>>>(ms, fl, out));
+            else if (LS == 16) LAUNCH(stats, VVM_K_MG_COARSE, st, k_coarse_modes<P, 16><<<1, 32 * S, mode_smem, st>>>(ms, fl, out));
+            else LAUNCH(stats, VVM_K_MG_COARSE, st, k_coarse_modes<P, 32><<<1, 32 * S, mode_smem, st>>>(ms, fl, out));
+            CKL();
+            res = out;
+        } else {
+            // levels lc..nlev-1 in one block
+            CoarseCycleArgs<P> ca{};
+            ca.nlev = nlev - lc;
+            for (int j = 0; j < ca.nlev; j++) {
+                ca.L[j] = lines[lc + j];
+                ca.f[j] = f[lc + j];
+                ca.x[j] = x[lc + j];
+                ca.y[j] = y[lc + j];
+            }
+            ca.z = zops();
+            ca.f0 = fl;
+            ca.omega = omega;
+            ca.coarse_sweeps = coarse_sweeps;
+            if (LS == 8) LAUNCH(stats, VVM_K_MG_COARSE, st, k_mg_coarse_cycle<P, 8><<<1, 32 * S, 0, st>>>(ca));
+            else if (LS == 16) LAUNCH(stats, VVM_K_MG_COARSE, st, k_mg_coarse_cycle<P, 16><<<1, 32 * S, 0, st>>>(ca));
+            else LAUNCH(stats, VVM_K_MG_COARSE, st, k_mg_coarse_cycle<P, 32><<<1, 32 * S, 0, st>>>(ca));
+            CKL();
+            res = y[lc];
         }
-        ca.z = zops();
-        ca.f0 = fl;
-        ca.omega = omega;
-        ca.coarse_sweeps = coarse_sweeps;
-        if (LS == 8) k_mg_coarse_cycle<P, 8><<<1, 32 * S, 0, st>>>(ca);
-        else if (LS == 16) k_mg_coarse_cycle<P, 16><<<1, 32 * S, 0, st>>>(ca);
-        else k_mg_coarse_cycle<P, 32><<<1, 32 * S, 0, st>>>(ca);
-        CKL();
-        P* res = y[lc];
         for (int l = lc - 1; l >= 0; l--) {
             const P* fl2 = (l == 0) ? r : f[l];
             sweep(l, fl2, x[l], res, pitch[l + 1], nx[l + 1], y[l], omega, st);
@@ -403,7 +646,6 @@ struct Multigrid {
         }
         return res;
     }
-
 };
 
 // Preconditioned CG on S d = g in precision P with the level-0 vectors below.
@@ -417,6 +659,8 @@ struct PCG {
     double* rhow_k = nullptr;
     CGScalars* sc = nullptr;
     CGScalars* sc_host = nullptr;
+    CGCtl* ctl = nullptr;   // loop state of graph-captured solves
+    Stats* stats = nullptr;
 
     void build(Arena& ar, int NXr, int NKr, const std::vector<double>& rhou, const std::vector<double>& rhow) {
         NX = NXr;
@@ -429,6 +673,7 @@ struct PCG {
             rd[kk] = 1.0 / rhou[k - 1];
             rw[kk] = rhow[k];
         }
+        mg.stats = stats;
         mg.build(ar, NX, NK, cx0, ru, rd);
         pitch = mg.pitch[0];
         r = ar.alloc<P>((size_t)NK * pitch);
@@ -440,6 +685,7 @@ struct PCG {
         rhow_k = ar.alloc<double>(NK);
         CK(cudaMemcpy(rhow_k, rw.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
         sc = ar.alloc<CGScalars>(1);
+        ctl = ar.alloc<CGCtl>(1);
         CK(cudaMallocHost(&sc_host, sizeof(CGScalars)));
     }
     void release() {
@@ -456,49 +702,78 @@ struct PCG {
         return sc_host->rr;
     }
 
+    // One PCG iteration for a graph-captured loop (x, r resident, r holding
+    // the current residual): z = M r, beta (0 on the loop's first pass),
+    // p, q = S p, alpha, x += alpha p, r -= alpha q, ||rhow r||^2. Returns the
+    // number of kernels recorded.
+    int record_iteration(P* x, cudaStream_t st) {
+        const long long n0 = stats->launches;
+        VecArgs<P> v = vargs();
+        dim3 B = block(), G = grid();
+        P* z = mg.apply(r, st);
+        LAUNCH(stats, VVM_K_CG, st, k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial));
+        CKL();
+        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar_it<<<1, 1024, 0, st>>>(partial, npart, sc, ctl));
+        CKL();
+        LAUNCH(stats, VVM_K_CG, st, k_cg_dir_it<P><<<G, B, 0, st>>>(v, sc, ctl, z, p));
+        CKL();
+        LAUNCH(stats, VVM_K_CG, st, k_cg_spmv<P><<<G, B, 0, st>>>(v, p, q, partial));
+        CKL();
+        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_PQ_ALPHA));
+        CKL();
+        LAUNCH(stats, VVM_K_CG, st, k_cg_update<P><<<G, B, 0, st>>>(v, sc, x, r, p, q, partial));
+        CKL();
+        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR));
+        CKL();
+        return (int)(stats->launches - n0);
+    }
+
     // Solves S x = g. x holds the initial guess when `warm`, else it is zeroed.
-    // Stops when ||rhow (g - S x)|| <= rtol * ||rhow g||_ref where ref2 is the
-    // squared reference norm (||b||^2). Returns iterations; relres out.
+    // Stops when ||rhow (g - S x)||^2 <= rtol^2 * ref2; ref2 < 0 takes the
+    // initial residual as the reference. Returns iterations; relres out
+    // (relative to ref2). The stopping tests are the ones the graph-captured
+    // loops evaluate on the device (k_loop_plain / k_loop_inner).
     int solve(const P* g, P* x, bool warm, double ref2, double rtol, int maxit, cudaStream_t st,
               double* relres) {
         VecArgs<P> v = vargs();
         dim3 B = block(), G = grid();
         if (!warm) CK(cudaMemsetAsync(x, 0, (size_t)NK * pitch * sizeof(P), st));
-        k_cg_residual<P><<<G, B, 0, st>>>(v, g, x, r, partial);
+        LAUNCH(stats, VVM_K_CG, st, k_cg_residual<P><<<G, B, 0, st>>>(v, g, x, r, partial));
         CKL();
-        k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR);
+        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR));
         CKL();
         double rr = read_rr(st);
-        double target = rtol * std::sqrt(ref2);
-        if (std::sqrt(rr) <= target || ref2 == 0.0) {
+        if (ref2 < 0.0) ref2 = rr;
+        const double stop2 = (rtol * rtol) * ref2;
+        if (!(ref2 > 0.0) || !(rr > stop2)) {
             *relres = (ref2 > 0) ? std::sqrt(rr / ref2) : 0.0;
             return 0;
         }
         P* z = mg.apply(r, st);
-        k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial);
+        LAUNCH(stats, VVM_K_CG, st, k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial));
         CKL();
-        k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RZ);
+        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RZ));
         CKL();
-        k_cg_dir<P><<<G, B, 0, st>>>(v, sc, z, p, 1);
+        LAUNCH(stats, VVM_K_CG, st, k_cg_dir<P><<<G, B, 0, st>>>(v, sc, z, p, 1));
         CKL();
         int it = 0;
         for (it = 1; it <= maxit; it++) {
-            k_cg_spmv<P><<<G, B, 0, st>>>(v, p, q, partial);
+            LAUNCH(stats, VVM_K_CG, st, k_cg_spmv<P><<<G, B, 0, st>>>(v, p, q, partial));
             CKL();
-            k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_PQ_ALPHA);
+            LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_PQ_ALPHA));
             CKL();
-            k_cg_update<P><<<G, B, 0, st>>>(v, sc, x, r, p, q, partial);
+            LAUNCH(stats, VVM_K_CG, st, k_cg_update<P><<<G, B, 0, st>>>(v, sc, x, r, p, q, partial));
             CKL();
-            k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR);
+            LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR));
             CKL();
             rr = read_rr(st);
-            if (std::sqrt(rr) <= target || !std::isfinite(rr)) break;
+            if (!(rr > stop2) || !std::isfinite(rr) || it >= maxit) break;
             z = mg.apply(r, st);
-            k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial);
+            LAUNCH(stats, VVM_K_CG, st, k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial));
             CKL();
-            k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_RZ_BETA);
+            LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_RZ_BETA));
             CKL();
-            k_cg_dir<P><<<G, B, 0, st>>>(v, sc, z, p, 0);
+            LAUNCH(stats, VVM_K_CG, st, k_cg_dir<P><<<G, B, 0, st>>>(v, sc, z, p, 0));
             CKL();
         }
         *relres = std::sqrt(rr / ref2);
@@ -554,15 +829,38 @@ struct vvm_gpu_ctx {
     std::unique_ptr<PCG<double>> pcg64;
     std::unique_ptr<PCG<float>> pcg32;
     double *Wf = nullptr, *W = nullptr, *r64 = nullptr;   // level-0 layout, FP64
+    double* Wprev = nullptr;   // previous cal_w solution (initial-guess extrapolation)
+    int nsolves = 0;
+    // CUDA graphs of one whole step, by (time-level buffer, step parity)
+    cudaGraphExec_t gexec[2][2] = {};
+    long long gstatic[2][2] = {};      // kernels outside the solver loops
+    cudaStream_t cap[2] = {};          // streams for capturing loop bodies
+    CGCtl* wctl = nullptr;             // outer loop state of the mixed solve
+    long long* d_exec = nullptr;       // kernels executed inside graph loops
+    bool last_graph = false;           // the last cal_w ran inside a graph
+    bool graphs_off = false;
     float *g32 = nullptr, *d32 = nullptr;
     double* wpartial = nullptr;
     int wnpart = 0;
     double* sc_host = nullptr;
     int last_iters = 0;
     double last_relres = 0;
+    Stats stats;
     std::string err;
 
+    void drop_graphs() {
+        for (auto& row : gexec)
+            for (auto& g : row)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+    }
+
     ~vvm_gpu_ctx() {
+        drop_graphs();
+        for (auto s : cap)
+            if (s) cudaStreamDestroy(s);
         if (pcg64) pcg64->release();
         if (pcg32) pcg32->release();
         if (sc_host) cudaFreeHost(sc_host);
@@ -635,7 +933,7 @@ void launch_pzeta(vvm_gpu_ctx* c) {
     PZetaArgs<T> a{c->d, c->c, c->profiles(), F.zeta[now], F.u, F.w, F.th[now], F.qv[now], F.qc[now], F.qr[now],
                    F.zeta[fut], F.hist[H_ZETA][ab.sn], F.hist[H_ZETA][ab.so], F.hist[H_BUOY][ab.sn],
                    F.hist[H_BUOY][ab.so], ab};
-    k_pzeta<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_PZETA, c->stream, k_pzeta<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(a));
     CKL();
 }
 
@@ -669,10 +967,10 @@ void launch_padv(vvm_gpu_ctx* c, int mask, int nvp_mask, bool vt, bool precip) {
     a.do_precip = precip;
     a.ab = ab;
     dim3 g = c->grid_interior(1);
-    k_padv<T><<<g, c->blk(), 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_PADV, c->stream, k_padv<T><<<g, c->blk(), 0, c->stream>>>(a));
     CKL();
     if (nvp_mask) {
-        k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp);
+        LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp));
         CKL();
     }
 }
@@ -697,7 +995,7 @@ void launch_apply(vvm_gpu_ctx* c, int mask, int nvp_mask, bool forcing, bool hal
     // status_for_adding_forcing (Iteration.cpp:276-277)
     a.forcing_th = forcing && c->has_forcing_th && (c->step * c->desc.dt <= c->desc.addforcingtime);
     a.halo = halo;
-    k_apply<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_apply<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(a));
     CKL();
 }
 
@@ -706,7 +1004,7 @@ void launch_halo_all(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     HaloArgs<T> a{c->d, F.zeta[fut], F.w, {F.th[fut], F.u, F.qv[fut], F.qc[fut], F.qr[fut]}};
-    k_halo_all<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_halo_all<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(a));
     CKL();
 }
 
@@ -714,7 +1012,7 @@ template <typename T>
 void launch_pubartop(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     PubarArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.RKM, c->ubar, c->dubar, AB2::of(c->step)};
-    k_pubartop<T><<<1, 1024, 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_PUBAR, c->stream, k_pubartop<T><<<1, 1024, 0, c->stream>>>(a));
     CKL();
 }
 
@@ -725,9 +1023,9 @@ void launch_kessler(vvm_gpu_ctx* c, bool halo) {
     KesslerArgs<T> a{c->d, c->c, c->profiles(), F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut],
                      F.d_auto, F.d_accr, F.d_evap, F.d_cond, c->partial, 1};
     dim3 g = c->grid_interior(1);
-    k_kessler<T><<<g, c->blk(), 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_KESSLER, c->stream, k_kessler<T><<<g, c->blk(), 0, c->stream>>>(a));
     CKL();
-    k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp);
+    LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp));
     CKL();
     launch_apply<T>(c, halo ? (F_TH | F_QV | F_QC | F_QR) : (F_QV | F_QC | F_QR), F_QV | F_QC | F_QR, false, halo);
 }
@@ -737,15 +1035,15 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     RKArgs<T> r{c->d, c->c, c->profiles(), F.u, F.w, F.th[fut], F.RKM, F.RKH};
-    k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r);
+    LAUNCH(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r));
     CKL();
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
                 F.RKM, F.RKH, 0x1f, nudge ? 1 : 0};
     const int per = cdiv(c->d.nx - 2, kGSThreads);
-    if (per <= 1) k_gs_diffuse<T, 1><<<5, kGSThreads, 0, c->stream>>>(g);
-    else if (per <= 2) k_gs_diffuse<T, 2><<<5, kGSThreads, 0, c->stream>>>(g);
-    else if (per <= 4) k_gs_diffuse<T, 4><<<5, kGSThreads, 0, c->stream>>>(g);
-    else k_gs_diffuse<T, 8><<<5, kGSThreads, 0, c->stream>>>(g);
+    if (per <= 1) LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 1><<<5, kGSThreads, 0, c->stream>>>(g));
+    else if (per <= 2) LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 2><<<5, kGSThreads, 0, c->stream>>>(g));
+    else if (per <= 4) LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 4><<<5, kGSThreads, 0, c->stream>>>(g));
+    else LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 8><<<5, kGSThreads, 0, c->stream>>>(g));
     CKL();
 }
 
@@ -756,7 +1054,7 @@ void launch_nudge(vvm_gpu_ctx* c, bool th_zeta, bool qv) {
     NudgeArgs<T> a{c->d, c->c, c->profiles(), F.th[fut], F.zeta[fut], F.qv[fut], F.qv[now],
                    th_zeta ? 1 : 0, (th_zeta && c->desc.case_id != 2) ? 1 : 0,
                    qv ? c->desc.moisture_nudge_time : 0.0};
-    k_nudge<T><<<c->grid_all(), c->blk(), 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_MEAN, c->stream, k_nudge<T><<<c->grid_all(), c->blk(), 0, c->stream>>>(a));
     CKL();
 }
 
@@ -766,7 +1064,7 @@ void launch_update_mean(vvm_gpu_ctx* c, bool rotate) {
     int fut = 1 - c->cur;
     MeanArgs<T> a{c->d, c->offset_th(), c->offset_qv(), F.th[fut], F.qv[fut], c->thb, c->qvb, c->thvb,
                   c->ubar, rotate ? 1 : 0};
-    k_update_mean<T><<<c->d.nz - 2, 256, 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_MEAN, c->stream, k_update_mean<T><<<c->d.nz - 2, 256, 0, c->stream>>>(a));
     CKL();
 }
 
@@ -774,15 +1072,20 @@ void launch_update_mean(vvm_gpu_ctx* c, bool rotate) {
 
 void ensure_poisson(vvm_gpu_ctx* c) {
     if (c->poisson_ready) return;
+    c->drop_graphs();
     int NX = c->d.nx - 2, NK = c->d.nz - 3;
     c->pcg64.reset(new PCG<double>());
+    c->pcg64->stats = &c->stats;
     c->pcg64->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
     int pitch = c->pcg64->pitch;
     c->Wf = c->ar.alloc<double>((size_t)NK * pitch);
     c->W = c->ar.alloc<double>((size_t)NK * pitch);
     c->r64 = c->ar.alloc<double>((size_t)NK * pitch);
+    c->Wprev = c->ar.alloc<double>((size_t)NK * pitch);
+    c->nsolves = 0;
     if (c->mixed) {
         c->pcg32.reset(new PCG<float>());
+        c->pcg32->stats = &c->stats;
         c->pcg32->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
         c->g32 = c->ar.alloc<float>((size_t)NK * pitch);
         c->d32 = c->ar.alloc<float>((size_t)NK * pitch);
@@ -824,21 +1127,21 @@ int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
     if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), c->stream));
     int total = 0;
     double rel = 0;
-    for (int outer = 0; outer < 20; outer++) {
-        k_cg_residual<double><<<G, B, 0, c->stream>>>(v, c->Wf, c->W, c->r64, c->wpartial);
+    for (int outer = 0;; outer++) {
+        LAUNCH(&c->stats, VVM_K_CG, c->stream, k_cg_residual<double><<<G, B, 0, c->stream>>>(v, c->Wf, c->W, c->r64, c->wpartial));
         CKL();
-        k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, P64.sc, CG_SET_RR);
+        LAUNCH(&c->stats, VVM_K_CG, c->stream, k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, P64.sc, CG_SET_RR));
         CKL();
         double rr = P64.read_rr(c->stream);
         rel = std::sqrt(rr / bb);
-        if (rel <= tol || !std::isfinite(rel) || total >= maxit) break;
-        k_to_float<<<G, B, 0, c->stream>>>(P64.NX, P64.NK, P64.pitch, c->r64, c->g32);
+        if (!(rr > (tol * tol) * bb) || !std::isfinite(rr) || total >= maxit || outer >= 20) break;
+        LAUNCH(&c->stats, VVM_K_CG, c->stream, k_to_float<<<G, B, 0, c->stream>>>(P64.NX, P64.NK, P64.pitch, c->r64, c->g32));
         CKL();
         double irel = 0;
-        // inner: reduce the FP64 residual by ~1e-4 relative to itself
-        int it = P32.solve(c->g32, c->d32, false, rr, 1e-4, maxit, c->stream, &irel);
+        // inner: reduce its initial residual by 1e-4
+        int it = P32.solve(c->g32, c->d32, false, -1.0, 1e-4, maxit, c->stream, &irel);
         total += std::max(it, 1);
-        k_refine_add<<<G, B, 0, c->stream>>>(P64.NX, P64.NK, P64.pitch, c->W, c->d32);
+        LAUNCH(&c->stats, VVM_K_CG, c->stream, k_refine_add<<<G, B, 0, c->stream>>>(P64.NX, P64.NK, P64.pitch, c->W, c->d32));
         CKL();
     }
     c->last_iters = total;
@@ -846,23 +1149,172 @@ int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
     return (rel <= tol) ? VVM_GPU_OK : VVM_GPU_ENOCONV;
 }
 
+// ---------------------------------------------------------------- graphs
+
+cudaGraphConditionalHandle new_handle(cudaStream_t st) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g;
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, nullptr, nullptr));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    return h;
+}
+
+// Appends a WHILE node (condition h) to the graph being captured on st and
+// returns its body graph; capture on st continues after the node.
+cudaGraph_t add_while(cudaStream_t st, cudaGraphConditionalHandle h) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &p));
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return p.conditional.phGraph_out[0];
+}
+
+struct BodyCapture {   // stream capture into a conditional node's body graph
+    cudaStream_t s;
+    BodyCapture(cudaStream_t s_, cudaGraph_t body) : s(s_) {
+        CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    }
+    void end() {
+        cudaGraph_t g;
+        CK(cudaStreamEndCapture(s, &g));
+    }
+};
+
+// Records the cal_w solve with device-side loop control (graph capture on
+// c->stream). The FP64 step: one PCG loop to tol. The mixed step: FP64
+// residual refinement around an FP32 PCG loop. Returns the number of
+// kernels recorded inside loop bodies (excluded from the per-launch count).
+long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
+    PCG<double>& P64 = *c->pcg64;
+    cudaStream_t st = c->stream;
+    dim3 B = P64.block(), G = P64.grid();
+    VecArgs<double> v = P64.vargs();
+    const long long n_start = c->stats.launches;
+    long long in_bodies = 0;
+    if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
+    LAUNCH(&c->stats, VVM_K_CG, st, k_zero_if_b0<<<G, B, 0, st>>>(P64.NX, P64.NK, P64.pitch, P64.sc, c->W));
+    CKL();
+    if (!c->mixed) {
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P64.r, P64.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P64.partial, P64.npart, P64.sc, CG_SET_RR));
+        CKL();
+        cudaGraphConditionalHandle h = new_handle(st);
+        LAUNCH(&c->stats, VVM_K_CG, st, k_loop_plain<<<1, 1, 0, st>>>(P64.sc, P64.ctl, h, tol * tol, maxit, 1, c->d_exec, 0));
+        CKL();
+        cudaGraph_t body = add_while(st, h);
+        BodyCapture bc(c->cap[0], body);
+        const long long n0 = c->stats.launches;
+        int nb = P64.record_iteration(c->W, bc.s);
+        LAUNCH(&c->stats, VVM_K_CG, bc.s, k_loop_plain<<<1, 1, 0, bc.s>>>(P64.sc, P64.ctl, h, tol * tol, maxit, 0, c->d_exec, nb + 1));
+        CKL();
+        bc.end();
+        in_bodies += c->stats.launches - n0;
+        return in_bodies;
+    }
+    PCG<float>& P32 = *c->pcg32;
+    VecArgs<float> v32 = P32.vargs();
+    LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->W, c->r64, c->wpartial));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(c->wpartial, c->wnpart, P64.sc, CG_SET_RR));
+    CKL();
+    cudaGraphConditionalHandle ho = new_handle(st);
+    LAUNCH(&c->stats, VVM_K_CG, st, k_loop_outer<<<1, 1, 0, st>>>(P64.sc, c->wctl, P32.ctl, ho, tol * tol, maxit, 1, c->d_exec, 0));
+    CKL();
+    cudaGraph_t outer = add_while(st, ho);
+    {
+        BodyCapture oc(c->cap[0], outer);
+        cudaStream_t os = oc.s;
+        const long long n0 = c->stats.launches;
+        LAUNCH(&c->stats, VVM_K_CG, os, k_to_float<<<G, B, 0, os>>>(P64.NX, P64.NK, P64.pitch, c->r64, c->g32));
+        CKL();
+        CK(cudaMemsetAsync(c->d32, 0, (size_t)P32.NK * P32.pitch * sizeof(float), os));
+        LAUNCH(&c->stats, VVM_K_CG, os, k_cg_residual<float><<<G, B, 0, os>>>(v32, c->g32, c->d32, P32.r, P32.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, os, k_cg_scalar<<<1, 1024, 0, os>>>(P32.partial, P32.npart, P32.sc, CG_SET_RR));
+        CKL();
+        cudaGraphConditionalHandle hi = new_handle(os);
+        LAUNCH(&c->stats, VVM_K_CG, os, k_loop_inner<<<1, 1, 0, os>>>(P32.sc, P32.ctl, hi, 1e-8, maxit, 1, c->d_exec, 0));
+        CKL();
+        cudaGraph_t inner = add_while(os, hi);
+        long long n_inner;
+        {
+            BodyCapture ic(c->cap[1], inner);
+            const long long m0 = c->stats.launches;
+            int nb = P32.record_iteration(c->d32, ic.s);
+            LAUNCH(&c->stats, VVM_K_CG, ic.s, k_loop_inner<<<1, 1, 0, ic.s>>>(P32.sc, P32.ctl, hi, 1e-8, maxit, 0, c->d_exec, nb + 1));
+            CKL();
+            ic.end();
+            n_inner = c->stats.launches - m0;
+        }
+        LAUNCH(&c->stats, VVM_K_CG, os, k_refine_add<<<G, B, 0, os>>>(P64.NX, P64.NK, P64.pitch, c->W, c->d32));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, os, k_cg_residual<double><<<G, B, 0, os>>>(v, c->Wf, c->W, c->r64, c->wpartial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, os, k_cg_scalar<<<1, 1024, 0, os>>>(c->wpartial, c->wnpart, P64.sc, CG_SET_RR));
+        CKL();
+        const int n_outer = (int)(c->stats.launches - n0 - n_inner) + 1;   // + its own check
+        LAUNCH(&c->stats, VVM_K_CG, os, k_loop_outer<<<1, 1, 0, os>>>(P64.sc, c->wctl, P32.ctl, ho, tol * tol, maxit, 0, c->d_exec, n_outer));
+        CKL();
+        oc.end();
+        in_bodies += c->stats.launches - n0;
+    }
+    (void)n_start;
+    return in_bodies;
+}
+
 template <typename T>
-int launch_cal_w(vvm_gpu_ctx* c) {
+int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     ensure_poisson(c);
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     int NX = c->d.nx - 2, NK = c->d.nz - 3;
     int pitch = c->pcg64->pitch;
     dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
-    k_poisson_rhs<T><<<G, B, 0, c->stream>>>(c->d, c->c.dx, c->rhow, F.zeta[fut], c->Wf, pitch, c->wpartial);
+    LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_poisson_rhs<T><<<G, B, 0, c->stream>>>(c->d, c->c.dx, c->rhow, F.zeta[fut], c->Wf, pitch, c->wpartial));
     CKL();
-    k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, c->pcg64->sc, CG_SET_BB);
+    LAUNCH(&c->stats, VVM_K_CG, c->stream, k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, c->pcg64->sc, CG_SET_BB));
     CKL();
+    const bool warm = c->desc.warm_start != 0;
+    const int maxit = c->desc.poisson_maxit > 0 ? c->desc.poisson_maxit : 200;
+    if (recorded_in_loops) {   // graph capture: the loops run on the device
+        if (warm) {
+            LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_extrapolate<<<G, B, 0, c->stream>>>(NX, NK, pitch, c->W, c->Wprev));
+            CKL();
+        }
+        *recorded_in_loops = record_solve(c, c->desc.poisson_tol, maxit, warm);
+        c->nsolves++;
+        LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_w_from_W<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(c->d, c->rhow, c->W, pitch, F.w));
+        CKL();
+        return VVM_GPU_OK;
+    }
     CK(cudaMemcpyAsync(c->sc_host, &c->pcg64->sc->bb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     double bb = *c->sc_host;
-    int rc = solve_w(c, bb, c->desc.poisson_tol, c->desc.warm_start != 0);
-    k_w_from_W<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(c->d, c->rhow, c->W, pitch, F.w);
+    if (warm) {
+        // the previous solution(s) as the initial guess: linear extrapolation
+        // once two exist (the reference starts every solve from zero)
+        if (c->nsolves >= 2) {
+            LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_extrapolate<<<G, B, 0, c->stream>>>(NX, NK, pitch, c->W, c->Wprev));
+            CKL();
+        } else {
+            CK(cudaMemcpyAsync(c->Wprev, c->W, (size_t)NK * pitch * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c->stream));
+        }
+    }
+    int rc = solve_w(c, bb, c->desc.poisson_tol, warm);
+    c->nsolves++;
+    LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_w_from_W<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(c->d, c->rhow, c->W, pitch, F.w));
     CKL();
     return rc;
 }
@@ -872,22 +1324,22 @@ void launch_cal_u(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     CalUArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.zeta[fut], c->ubar};
-    k_cal_u_top<T><<<1, kCalUThreads, 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_top<T><<<1, kCalUThreads, 0, c->stream>>>(a));
     CKL();
-    k_cal_u_columns<T><<<cdiv(c->d.nx - 2, 32), 32 * kColSeg, 0, c->stream>>>(a);
+    LAUNCH(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_columns<T><<<cdiv(c->d.nx - 2, 32), 32 * kColSeg, 0, c->stream>>>(a));
     CKL();
 }
 
 // ---------------------------------------------------------------- one step
 
 template <typename T>
-int run_step(vvm_gpu_ctx* c) {
+int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     c->step++;                                                 // Iteration.cpp:246
     launch_pzeta<T>(c);                                        // pzeta_pt
     launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
     launch_apply<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true); // NVP, AddForcing, halos
     launch_pubartop<T>(c);                                     // pubarTop_pt
-    int rc = launch_cal_w<T>(c);                               // cal_w
+    int rc = launch_cal_w<T>(c, recorded_in_loops);            // cal_w
     launch_cal_u<T>(c);                                        // cal_u
     launch_kessler<T>(c, true);                                // Kessler + NVP x3 + halos
     // The first updateMean of the step (Iteration.cpp:408) only writes thb,
@@ -899,6 +1351,69 @@ int run_step(vvm_gpu_ctx* c) {
     return rc;
 }
 
+// The step as one CUDA graph: every kernel of run_step, with the cal_w
+// iterations as device-controlled WHILE nodes (no host round trip). Graphs
+// are keyed by the time-level buffer and the parity of the step they run
+// (the AB2 slots alternate with it) and captured on first use.
+template <typename T>
+cudaGraphExec_t step_graph(vvm_gpu_ctx* c) {
+    const int b = c->cur, par = (c->step + 1) & 1;
+    if (c->gexec[b][par]) return c->gexec[b][par];
+    ensure_poisson(c);
+    const int step0 = c->step, cur0 = c->cur, ns0 = c->nsolves;
+    const long long l0 = c->stats.launches;
+    cudaStream_t saved = c->stream;
+    c->stream = c->own;
+    cudaGraph_t g = nullptr;
+    long long in_loops = 0;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    try {
+        run_step<T>(c, &in_loops);
+    } catch (...) {
+        cudaStreamEndCapture(c->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        c->stream = saved;
+        c->step = step0;
+        c->cur = cur0;
+        c->nsolves = ns0;
+        throw;
+    }
+    CK(cudaStreamEndCapture(c->stream, &g));
+    c->stream = saved;
+    c->step = step0;
+    c->cur = cur0;
+    c->nsolves = ns0;
+    c->gstatic[b][par] = c->stats.launches - l0 - in_loops;
+    c->stats.launches = l0;
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw CudaError{std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+    c->gexec[b][par] = ex;
+    return ex;
+}
+
+template <typename T>
+int step_once(vvm_gpu_ctx* c) {
+    const bool forcing_now = c->has_forcing_th && ((c->step + 1) * c->desc.dt <= c->desc.addforcingtime);
+    const bool warm = c->desc.warm_start != 0;
+    const bool use_graph = !c->graphs_off && !c->stats.on && c->step >= 0 && !forcing_now &&
+                           c->poisson_ready && (!warm || c->nsolves >= 2);
+    if (!use_graph) {
+        c->last_graph = false;
+        return run_step<T>(c);
+    }
+    cudaGraphExec_t ex = step_graph<T>(c);
+    const int b = c->cur, par = (c->step + 1) & 1;
+    CK(cudaGraphLaunch(ex, c->stream));
+    c->stats.launches += c->gstatic[b][par];
+    c->step++;
+    c->cur = 1 - c->cur;
+    c->nsolves++;
+    c->last_graph = true;
+    return VVM_GPU_OK;
+}
+
 // ---------------------------------------------------------------- transfer
 
 template <typename T>
@@ -906,7 +1421,7 @@ void upload_field(vvm_gpu_ctx* c, const double* host, int sk, int off, T* dst, c
     size_t n = (size_t)c->d.nx * c->d.nz * sk;
     CK(cudaMemcpyAsync(c->staging, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
-    k_from_host_layout<T><<<g, b, 0, c->stream>>>(c->d, c->staging, sk, off, ref, dst);
+    LAUNCH(&c->stats, VVM_K_MEAN, c->stream, k_from_host_layout<T><<<g, b, 0, c->stream>>>(c->d, c->staging, sk, off, ref, dst));
     CKL();
 }
 
@@ -915,7 +1430,7 @@ void download_field(vvm_gpu_ctx* c, const T* src, int sk, int off, double* host,
                     const double* ref = nullptr) {
     size_t n = (size_t)c->d.nx * c->d.nz * sk;
     dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
-    k_to_host_layout<T><<<g, b, 0, c->stream>>>(c->d, src, sk, off, ref, c->staging);
+    LAUNCH(&c->stats, VVM_K_MEAN, c->stream, k_to_host_layout<T><<<g, b, 0, c->stream>>>(c->d, src, sk, off, ref, c->staging));
     CKL();
     if (!first_of_pair) {
         CK(cudaMemcpyAsync(host, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1240,6 +1755,9 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         c->partial = c->ar.alloc<double>((size_t)c->npart * 6);
         c->nvp = c->ar.alloc<double>(6);
         c->staging = c->ar.alloc<double>((size_t)c->d.nx * c->d.nz * 2);
+        c->wctl = c->ar.alloc<CGCtl>(1);
+        c->d_exec = c->ar.alloc<long long>(1);
+        for (auto& cs : c->cap) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     } catch (const CudaError& e) {
         cudaSetDevice(prev);
         return fail(nullptr, VVM_GPU_ECUDA, e.msg);
@@ -1281,8 +1799,13 @@ int vvm_gpu_last_error(vvm_gpu_ctx* ctx, char* buf, size_t len) {
 int vvm_gpu_upload_state(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st) {
     if (!st) return fail(ctx, VVM_GPU_EINVAL, "upload: NULL state");
     return guarded(ctx, [&] {
+        ctx->drop_graphs();   // kernel arguments depend on the uploaded flags
         int rc = upload_profiles(ctx, st);
         if (rc) return rc;
+        if (ctx->poisson_ready) {   // a new state: no solver history
+            CK(cudaMemsetAsync(ctx->W, 0, (size_t)ctx->pcg64->NK * ctx->pcg64->pitch * sizeof(double), ctx->stream));
+            ctx->nsolves = 0;
+        }
         rc = DISPATCH(ctx, upload_state_t)(ctx, st);
         if (rc) return rc;
         CK(cudaStreamSynchronize(ctx->stream));
@@ -1350,7 +1873,7 @@ ROUTINE(vvm_gpu_pqr, {
 ROUTINE(vvm_gpu_add_forcing, { DISPATCH(ctx, launch_apply)(ctx, F_TH | F_QV, 0, true, false); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_halo_all, { DISPATCH(ctx, launch_halo_all)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_pubartop, { DISPATCH(ctx, launch_pubartop)(ctx); return VVM_GPU_OK; })
-ROUTINE(vvm_gpu_cal_w, { return DISPATCH(ctx, launch_cal_w)(ctx); })
+ROUTINE(vvm_gpu_cal_w, { ctx->last_graph = false; return DISPATCH(ctx, launch_cal_w)(ctx, nullptr); })
 ROUTINE(vvm_gpu_cal_u, { DISPATCH(ctx, launch_cal_u)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_kessler, { DISPATCH(ctx, launch_kessler)(ctx, false); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_update_mean, { DISPATCH(ctx, launch_update_mean)(ctx, false); return VVM_GPU_OK; })
@@ -1371,7 +1894,7 @@ int vvm_gpu_step(vvm_gpu_ctx* ctx, int nsteps) {
         if (nsteps < 0) return fail(ctx, VVM_GPU_EINVAL, "step: nsteps < 0");
         int worst = VVM_GPU_OK;
         for (int s = 0; s < nsteps; s++) {
-            int rc = DISPATCH(ctx, run_step)(ctx);
+            int rc = DISPATCH(ctx, step_once)(ctx);
             if (rc != VVM_GPU_OK) worst = rc;
         }
         if (worst == VVM_GPU_ENOCONV) fail(ctx, worst, "cal_w: Poisson solve did not reach its tolerance");
@@ -1386,18 +1909,19 @@ int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_
         ensure_poisson(ctx);
         int NX = ctx->d.nx - 2, NK = ctx->d.nz - 3, pitch = ctx->pcg64->pitch;
         dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
-        k_rhs_from_b<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->rhow, d_b, ctx->Wf, pitch, ctx->wpartial);
+        LAUNCH(&ctx->stats, VVM_K_POISSON_RHS, ctx->stream, k_rhs_from_b<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->rhow, d_b, ctx->Wf, pitch, ctx->wpartial));
         CKL();
-        k_cg_scalar<<<1, 1024, 0, ctx->stream>>>(ctx->wpartial, ctx->wnpart, ctx->pcg64->sc, CG_SET_BB);
+        LAUNCH(&ctx->stats, VVM_K_CG, ctx->stream, k_cg_scalar<<<1, 1024, 0, ctx->stream>>>(ctx->wpartial, ctx->wnpart, ctx->pcg64->sc, CG_SET_BB));
         CKL();
         double bb = read_scalar(ctx, &ctx->pcg64->sc->bb);
         bool warm = ctx->desc.warm_start != 0;
         if (warm) {
-            k_unpack_solution<<<G, B, 0, ctx->stream>>>(NX, NK, d_W, ctx->W, pitch);
+            LAUNCH(&ctx->stats, VVM_K_POISSON_RHS, ctx->stream, k_unpack_solution<<<G, B, 0, ctx->stream>>>(NX, NK, d_W, ctx->W, pitch));
             CKL();
         }
         int rc = solve_w(ctx, bb, tol, warm);
-        k_pack_solution<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->W, pitch, d_W);
+        ctx->last_graph = false;
+        LAUNCH(&ctx->stats, VVM_K_POISSON_RHS, ctx->stream, k_pack_solution<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->W, pitch, d_W));
         CKL();
         CK(cudaStreamSynchronize(ctx->stream));
         if (iters) *iters = ctx->last_iters;
@@ -1424,11 +1948,51 @@ int vvm_gpu_poisson_solve(vvm_gpu_ctx* ctx, const double* b, double* W, double t
     });
 }
 
+int vvm_gpu_profile(vvm_gpu_ctx* ctx, int enable) {
+    return guarded(ctx, [&]() -> int {
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->stats.reset();
+        CK(cudaMemset(ctx->d_exec, 0, sizeof(long long)));
+        ctx->stats.on = (enable != 0);
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_profile_read(vvm_gpu_ctx* ctx, int kernel_class, double* ms, long long* launches) {
+    if (kernel_class < 0 || kernel_class >= VVM_K_COUNT) return fail(ctx, VVM_GPU_EINVAL, "profile_read: bad class");
+    return guarded(ctx, [&]() -> int {
+        ctx->stats.resolve();
+        if (ms) *ms = ctx->stats.ms[kernel_class];
+        if (launches) *launches = ctx->stats.cnt[kernel_class];
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_launch_count(vvm_gpu_ctx* ctx, long long* launches) {
+    if (!ctx || !launches) return VVM_GPU_EINVAL;
+    return guarded(ctx, [&]() -> int {
+        long long in_loops = 0;
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaMemcpy(&in_loops, ctx->d_exec, sizeof(long long), cudaMemcpyDeviceToHost));
+        *launches = ctx->stats.launches + in_loops;
+        return VVM_GPU_OK;
+    });
+}
+
 int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres) {
     if (!ctx) return VVM_GPU_EINVAL;
-    if (iters) *iters = ctx->last_iters;
-    if (relres) *relres = ctx->last_relres;
-    return VVM_GPU_OK;
+    return guarded(ctx, [&]() -> int {
+        if (ctx->last_graph && ctx->poisson_ready) {   // loop state lives on the device
+            CGCtl h{};
+            CK(cudaStreamSynchronize(ctx->stream));
+            CK(cudaMemcpy(&h, ctx->mixed ? ctx->wctl : ctx->pcg64->ctl, sizeof(CGCtl), cudaMemcpyDeviceToHost));
+            ctx->last_iters = h.total;
+            ctx->last_relres = h.relres;
+        }
+        if (iters) *iters = ctx->last_iters;
+        if (relres) *relres = ctx->last_relres;
+        return VVM_GPU_OK;
+    });
 }
 
 }  // extern "C"

@@ -61,6 +61,10 @@ class HostState(ctypes.Structure):
                  ("dubarTop_advect", ctypes.c_double * 2), ("step", ctypes.c_int)])
 
 
+# Kernel classes of vvm_gpu_profile_read (VVM_K_* in include/vvm_gpu.h).
+KERNEL_CLASSES = ("pzeta", "padv", "apply", "pubar", "poisson_rhs", "cg", "mg_sweep", "mg_restrict",
+                  "mg_coarse", "cal_u", "kessler", "rkm", "gs", "mean")
+
 ROUTINES = ("pzeta", "pth", "pqv", "pqc", "pqr", "add_forcing", "halo_all", "pubartop", "cal_w",
             "cal_u", "kessler", "update_mean", "turbulence", "nudge", "next_step")
 
@@ -68,7 +72,8 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_synchronize", "vvm_gpu_last_error", "vvm_gpu_upload_state",
            "vvm_gpu_download_state", "vvm_gpu_upload_prognostic", "vvm_gpu_download_prognostic",
            "vvm_gpu_set_step", "vvm_gpu_get_step", "vvm_gpu_step", "vvm_gpu_poisson_solve",
-           "vvm_gpu_poisson_solve_device", "vvm_gpu_last_solve") + tuple(
+           "vvm_gpu_poisson_solve_device", "vvm_gpu_last_solve", "vvm_gpu_profile",
+           "vvm_gpu_profile_read", "vvm_gpu_launch_count") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -101,6 +106,9 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_poisson_solve_device.argtypes = [vp, vp, vp, ctypes.c_double,
                                                ctypes.POINTER(ip), _dp]
     L.vvm_gpu_last_solve.argtypes = [vp, ctypes.POINTER(ip), _dp]
+    L.vvm_gpu_profile.argtypes = [vp, ip]
+    L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
+    L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     for r in ROUTINES:
         getattr(L, "vvm_gpu_" + r).argtypes = [vp]
     if path is None:
@@ -265,6 +273,25 @@ class VVMGpu:
 
     def synchronize(self):
         self._check(self.L.vvm_gpu_synchronize(self.h))
+
+    def profile(self, enable: bool = True):
+        """Starts (and resets) or stops the per-kernel-class event timers."""
+        self._check(self.L.vvm_gpu_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        """{class: (device ms, launches)} accumulated since profile(True)."""
+        out = {}
+        for k, name in enumerate(KERNEL_CLASSES):
+            ms, n = ctypes.c_double(), ctypes.c_longlong()
+            self._check(self.L.vvm_gpu_profile_read(self.h, k, ctypes.byref(ms), ctypes.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out
+
+    @property
+    def launch_count(self) -> int:
+        n = ctypes.c_longlong()
+        self._check(self.L.vvm_gpu_launch_count(self.h, ctypes.byref(n)))
+        return n.value
 
     def last_solve(self):
         it, rel = ctypes.c_int(), ctypes.c_double()

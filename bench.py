@@ -1,0 +1,405 @@
+"""Benchmark of the VVM time step on B200 (one JSON line on stdout).
+
+Workload: the warm-bubble VVM step (Kessler warm rain, turbulence, nudging,
+anelastic w-equation solved to ||b - A W|| / ||b|| <= 1e-10) on an
+NX=2048 x NZ=256 grid, dx = dz = 100 m, dt = 1 s, synthetic seeded initial
+state (theta = 300 K + 3 K/km, 80 % RH, +2 K cosine bubble of radius 2 km).
+A "step" is one call of the reference's TimeMarching body.
+
+Our arm (default): the mixed-precision step (FP32 fields and stencils,
+FP32 inner CG with FP64 residual, refinement and reductions, multigrid
+preconditioner) is the headline `value`; the plain FP64 multigrid-PCG step is
+timed the same way and reported beside it. Every timed step is bracketed by
+CUDA events on the stream the library launches on; L2 is flushed (a 256 MB
+write) between timed steps, outside the timed windows. `e2e` repeats the
+headline through the C ABI with the prognostic fields copied from pinned host
+memory before and back after every step.
+
+Reference arm (--impl reference): the reference's own TimeMarching, built from
+its sources into oracle/_ref/libvvmref.so (serial: its OpenMP loops race and
+this image has no libgomp), on the same grid and initial state; each step is
+one full-grid reference step.
+
+Multi-GPU (torchrun): one independent replica per GPU ("replicas only": one
+2D domain does not shard), max time over ranks, value = all ranks' cell-steps
+per second.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+for p in (str(REPO / "2d-vector-vorticity-model_b200"), str(REPO)):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+NX, NZ, DX, DT = 2048, 256, 100.0, 1.0
+METRIC = "cell-steps/s"
+WORKLOAD = "VVM warm-bubble step, Kessler + turbulence, NX=2048 NZ=256 dx=dz=100 m dt=1 s"
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons every 200 ms."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------- byte model
+
+def class_bytes(cls: str, launches: int, grid, elem: int, cg_iters: float) -> float:
+    """Algorithmic (compulsory) bytes of `launches` launches of a kernel class:
+    each array a kernel must read or write touched once. cells = nx*nz of one
+    field; unknowns = NX*(NZ-1) of the elliptic problem."""
+    cells = grid.nx * grid.nz
+    unk = grid.NX * (grid.NZ - 1)
+    per_launch = {
+        "pzeta": 12 * cells * elem,        # zeta u w th qv qc qr + 2 old hist in; zetap + 2 hist out
+        "padv": 20 * cells * elem,         # u w + 4 fields + 5 old hist in; 4 fields + 5 hist out
+        "apply": 8 * cells * elem,         # 4 fields in place
+        "kessler": 12 * cells * elem,      # 4 in, 4 out, 4 rates out
+        "rkm": 5 * cells * elem,           # u w thp in; RKM RKH out
+        "gs": 12 * cells * elem,           # 5 fields in place + RKM RKH
+        "cal_u": 3 * cells * elem / 2,     # w zetap in, u out (two launches)
+    }
+    if cls in per_launch:
+        return per_launch[cls] * launches
+    if cls == "mg_sweep":
+        # one V-cycle: pre-sweeps read f, write x (2 arrays); post-sweeps read
+        # f, x, half a coarse array, write y (3.5 arrays); fine levels halve
+        nfine, total, n = 0, 0.0, grid.NX
+        while n > 32 and n % 2 == 0:
+            total += 5.5 * (grid.NZ - 1) * n * elem
+            nfine += 1
+            n //= 2
+        return total / max(2 * nfine, 1) * launches
+    if cls == "cg":
+        # per iteration: spmv 2, update 6, dot 2, direction 3 arrays of the unknowns
+        return 13 * unk * elem * cg_iters
+    return float("nan")
+
+
+# ----------------------------------------------------------------- our arm
+
+def timed_steps(torch, g, steps, flush):
+    import torch as T
+    st = T.cuda.current_stream()
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = T.cuda.Event(enable_timing=True), T.cuda.Event(enable_timing=True)
+        e0.record(st)
+        g.step(1)
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def run_variant(torch, precision, steps, warmup, flush, device):
+    from vvm_b200.gpu import VVMGpu
+    from vvm_b200.initial_state import warm_bubble
+    st = warm_bubble(NX, NZ, DX, DX, DT)
+    g = VVMGpu(st.grid, precision=precision, device=device)
+    g.set_stream(torch.cuda.current_stream().cuda_stream)
+    g.upload(st)
+    g.step(warmup)
+    g.synchronize()
+    n0 = g.launch_count
+    times = timed_steps(torch, g, steps, flush)
+    launches = g.launch_count - n0
+    it, rel = g.last_solve()
+    # per-kernel-class device time over two more steps (events around launches)
+    g.profile(True)
+    g.step(2)
+    prof = g.profile_read()
+    g.profile(False)
+    return g, st, times, launches, prof, it, rel
+
+
+def roofline(prof, grid, elem, hbm, peak_kind, iters_per_step):
+    cls, (ms, n) = max(prof.items(), key=lambda kv: kv[1][0])
+    nbytes = class_bytes(cls, n, grid, elem, iters_per_step * 2)
+    achieved = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+    traffic = None
+    tf = REPO / "profiles" / "roofline_traffic.txt"
+    if tf.exists():
+        for ln in tf.read_text().splitlines():
+            f = ln.split()
+            if len(f) >= 3 and f[0] == cls and f[1] == ("fp32" if elem == 4 else "fp64"):
+                traffic = float(f[2])
+    return {"kernel": cls, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": (achieved / hbm) if achieved else None, "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": nbytes / max(n, 1), "avg_launch_us": 1e3 * ms / max(n, 1),
+            "launches": n, "traffic": traffic}
+
+
+def cpu_baseline(steps_hint=1):
+    """The reference's own step on the host cores: one full-grid step
+    (a bounded sample of about 10-30 s)."""
+    from oracle.models import PortModel, RefModel, ref_available
+    from vvm_b200.initial_state import warm_bubble
+    st = warm_bubble(NX, NZ, DX, DX, DT)
+    kind = "reference" if ref_available() else "port"
+    m = RefModel(st.grid) if kind == "reference" else PortModel(st.grid)
+    m.load(st)
+    t0 = time.perf_counter()
+    n = 0
+    while n < steps_hint or time.perf_counter() - t0 < 5.0:
+        m.one_step()
+        n += 1
+        if time.perf_counter() - t0 > 30.0:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": NX * NZ * n / dt, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": f"{n} full-grid step(s) of the same workload, serial build, {dt:.1f} s"}
+
+
+def our_arm(args, rank, world, device):
+    import torch
+    torch.cuda.set_device(device)
+    # an explicit stream: the library and the timing events must share it
+    # (handle 0, the legacy stream, would hand the library its own stream)
+    torch.cuda.set_stream(torch.cuda.Stream(device=device))
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")  # 256 MB > L2
+    from vvm_b200.gpu import VVM_PREC_FP64, VVM_PREC_MIXED
+    hbm, peak_kind = peaks()
+    results = {}
+    with ClockSampler(device) as clk:
+        for name, prec in (("mixed", VVM_PREC_MIXED), ("fp64", VVM_PREC_FP64)):
+            if dist_on():
+                dist_barrier()
+            g, st, times, launches, prof, it, rel = run_variant(torch, prec, args.steps, args.warmup,
+                                                                 flush, device)
+            results[name] = dict(g=g, st=st, times=times, launches=launches, prof=prof, it=it, rel=rel)
+    clocks = clk.summary()
+    head = results["mixed"]
+    total_ms = sum(head["times"])
+    total_ms = dist_max(total_ms)
+    cells = NX * NZ
+    value = world * cells * args.steps / (total_ms * 1e-3)
+    fp64_ms = dist_max(sum(results["fp64"]["times"]))
+    fp64_value = world * cells * args.steps / (fp64_ms * 1e-3)
+
+    # e2e through the C ABI with host buffers (pinned) copied in and out each step
+    g = head["g"]
+    import torch as T
+    pinned = {n: T.empty((st_nx(), st_nz()), dtype=T.float64).pin_memory().numpy()
+              for n in ("zeta", "th", "qv", "qc", "qr", "u", "w")}
+    g.download_prognostic(pinned)
+    stream = T.cuda.current_stream()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = T.cuda.Event(enable_timing=True), T.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.upload_prognostic(pinned)
+        g.step(1)
+        g.download_prognostic(pinned)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    e2e_ms = dist_max(e2e_ms)
+    field_bytes = 7 * st_nx() * st_nz() * 8
+
+    def poisson_ms(prof):
+        return sum(prof[c][0] for c in ("poisson_rhs", "cg", "mg_sweep", "mg_restrict", "mg_coarse")) / 2
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "NX": NX, "NZ": NZ, "dx_m": DX, "dz_m": DX, "dt_s": DT,
+                   "precision": "mixed: FP32 fields/stencils/inner CG, FP64 residual/refinement/"
+                                "reductions/Kessler arithmetic", "solver": "multigrid-PCG",
+                   "poisson_tol": 1e-10, "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas x{world}"},
+        "poisson_ms_per_solve": poisson_ms(head["prof"]),
+        "poisson_solves_per_s": 1e3 / poisson_ms(head["prof"]),
+        "poisson_iterations_last": head["it"], "poisson_relres_last": head["rel"],
+        "plain_fp64": {"value": fp64_value, "ms_per_step": fp64_ms / args.steps,
+                       "poisson_ms_per_solve": poisson_ms(results["fp64"]["prof"]),
+                       "poisson_iterations_last": results["fp64"]["it"],
+                       "roofline": roofline(results["fp64"]["prof"], head["st"].grid, 8, hbm, peak_kind,
+                                            results["fp64"]["it"])},
+        "speedup_vs_plain_fp64": value / fp64_value,
+        "roofline": roofline(head["prof"], head["st"].grid, 4, hbm, peak_kind, head["it"]),
+        "kernel_ms_per_step": {k: v[0] / 2 for k, v in head["prof"].items()},
+        "e2e": {"value": world * cells * args.steps / (e2e_ms * 1e-3), "unit": METRIC,
+                "h2d_bytes_per_step": field_bytes, "d2h_bytes_per_step": field_bytes},
+        "gpu_launches": head["launches"],
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    return line
+
+
+def st_nx():
+    return NX + 2
+
+
+def st_nz():
+    return NZ + 2
+
+
+# ----------------------------------------------------------- reference arm
+
+def reference_arm(args):
+    from oracle.models import RefModel, ref_available
+    from vvm_b200.initial_state import warm_bubble
+    if not ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libvvmref.so is not built "
+                "(the reference sources were not present when build() ran)"}
+    st = warm_bubble(NX, NZ, DX, DX, DT)
+    m = RefModel(st.grid)
+    m.load(st)
+    for _ in range(min(args.warmup, 1)):
+        m.one_step()
+    nsteps = max(1, min(args.steps, 8))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        m.one_step()
+    dt = time.perf_counter() - t0
+    v = NX * NZ * nsteps / dt
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 0,
+            "steps": nsteps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * dt / nsteps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "NX": NX, "NZ": NZ, "dx_m": DX, "dz_m": DX, "dt_s": DT,
+                       "solver": "Eigen BiCGSTAB + IncompleteLUT (tol 1e-22), serial build"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
+                             "sample": f"{nsteps} full-grid reference step(s) (warm-up "
+                                       f"{min(args.warmup, 1)}); the reference's OpenMP loops "
+                                       f"race and no libgomp is installed, so the serial build"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# ------------------------------------------------------------ distributed
+
+_DIST = {"on": False}
+
+
+def dist_on():
+    return _DIST["on"]
+
+
+def dist_barrier():
+    import torch.distributed as D
+    D.barrier()
+
+
+def dist_max(x: float) -> float:
+    if not _DIST["on"]:
+        return x
+    import torch
+    import torch.distributed as D
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    D.all_reduce(t, op=D.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)), flush=True)
+        return
+    if args.warmup < 3:
+        args.warmup = 3
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as D
+        torch.cuda.set_device(local)
+        D.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                             device_id=torch.device(f"cuda:{local}"))
+        _DIST["on"] = True
+    line = our_arm(args, rank, world, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as D
+        D.barrier()
+        D.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

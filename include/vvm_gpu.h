@@ -161,6 +161,34 @@ int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_
 /* Iterations and final relative residual of the last cal_w solve. */
 int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres);
 
+/* -- timers -------------------------------------------------------------------
+ * The reference keeps per-phase wall timers of each step (t_advection,
+ * t_poisson, t_microphysics, t_diffusion, t_all; src/Iteration.cpp:286-435).
+ * Here, with profiling enabled, every kernel launch is bracketed by CUDA
+ * events on the context's stream and accumulated per kernel class
+ * (VVM_K_*); phases are the sums of their classes. The launch counter runs
+ * always. Enabling resets both. */
+#define VVM_K_PZETA 0       /* vorticity advection + buoyancy */
+#define VVM_K_PADV 1        /* scalar advection + sedimentation + NVP sums */
+#define VVM_K_APPLY 2       /* NVP rescale, forcing, halos */
+#define VVM_K_PUBAR 3       /* pubarTop */
+#define VVM_K_POISSON_RHS 4 /* cal_w right-hand side, w from W */
+#define VVM_K_CG 5          /* CG vector kernels and reductions */
+#define VVM_K_MG_SWEEP 6    /* multigrid z-line sweeps */
+#define VVM_K_MG_RESTRICT 7 /* multigrid restriction */
+#define VVM_K_MG_COARSE 8   /* multigrid coarse-level block */
+#define VVM_K_CAL_U 9       /* cal_u top row and column integral */
+#define VVM_K_KESSLER 10    /* Kessler + NVP sums */
+#define VVM_K_RKM 11        /* eddy coefficients */
+#define VVM_K_GS 12         /* Gauss-Seidel diffusion (+ nudging) */
+#define VVM_K_MEAN 13       /* updateMean, nudging passes, transfers */
+#define VVM_K_COUNT 14
+int vvm_gpu_profile(vvm_gpu_ctx* ctx, int enable);
+/* Accumulated device milliseconds and launches of one kernel class. */
+int vvm_gpu_profile_read(vvm_gpu_ctx* ctx, int kernel_class, double* ms, long long* launches);
+/* Kernel launches of this context since creation or the last profile(1). */
+int vvm_gpu_launch_count(vvm_gpu_ctx* ctx, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif

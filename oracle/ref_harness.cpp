@@ -9,6 +9,10 @@
 // of oracle/ref_config.hpp, the reference's src/Declare.hpp (minus its
 // Config.hpp include) and then this file, so `class vvm`, `Config_VVM` and the
 // Eigen sparse types are already declared when this text is reached.
+#include <fcntl.h>
+#include <unistd.h>
+
+#include <cstdio>
 #include <cstring>
 #include <iostream>
 #include <sstream>
@@ -18,11 +22,30 @@ namespace {
 
 // Silences the per-step `std::cout << model.step` of
 // Iteration::TimeMarching (src/Iteration.cpp:229) while a call runs.
+// Also silences C stdio on fd 1 (the vvm destructor's printf "Free vvm",
+// src/Declare.hpp:99, and cal_w's solver warnings, src/PoissonSolver.cpp:464),
+// so a caller's stdout carries only its own output.
 struct CoutMute {
     std::ostringstream sink;  // declared first: constructed before `saved` uses it
     std::streambuf* saved;
-    CoutMute() : saved(std::cout.rdbuf(sink.rdbuf())) {}
-    ~CoutMute() { std::cout.rdbuf(saved); }
+    int fd_saved;
+    CoutMute() : saved(std::cout.rdbuf(sink.rdbuf())) {
+        std::fflush(stdout);
+        fd_saved = dup(1);
+        int dn = open("/dev/null", O_WRONLY);
+        if (dn >= 0) {
+            dup2(dn, 1);
+            close(dn);
+        }
+    }
+    ~CoutMute() {
+        std::fflush(stdout);
+        if (fd_saved >= 0) {
+            dup2(fd_saved, 1);
+            close(fd_saved);
+        }
+        std::cout.rdbuf(saved);
+    }
 };
 
 // One time step exactly as vvm::Iteration::TimeMarching runs it for the
@@ -156,7 +179,10 @@ double* ref_scalar(void* h, const char* name) {
 
 int* ref_step_ptr(void* h) { return &static_cast<vvm*>(h)->step; }
 
-void ref_init_poisson(void* h) { vvm::PoissonSolver::InitPoissonMatrix(*static_cast<vvm*>(h)); }
+void ref_init_poisson(void* h) {
+    CoutMute mute;
+    vvm::PoissonSolver::InitPoissonMatrix(*static_cast<vvm*>(h));
+}
 
 // Runs one reference routine by name; returns 0, or -1 for an unknown name.
 int ref_call(void* h, const char* name) {
@@ -218,6 +244,7 @@ void ref_apply_A(void* h, const double* x, double* y) {
 // guess, tolerance model.tolerance, at most 10000 iterations.
 int ref_solve_A(void* h, const double* b, double* x, int* iters, double* err) {
     vvm& m = *static_cast<vvm*>(h);
+    CoutMute mute;
     int n = (m.nx - 2) * (m.nz - 3);
     Eigen::Map<const Eigen::VectorXd> bv(b, n);
     Eigen::BiCGSTAB<Eigen::SparseMatrix<double>, Eigen::IncompleteLUT<double> > solver;
