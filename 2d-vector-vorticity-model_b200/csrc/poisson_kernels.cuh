@@ -103,31 +103,44 @@ __device__ __forceinline__ void seg_thomas(const LineLevel& L, int a, int len, P
 // Solves the pentadiagonal reduced system of the segment ends in place in
 // sh[i*32 + lane] (i = 0..n-1): forward with the unit-lower band (l1, l2),
 // backward with the upper band (u1, u2) and 1/diag. Coefficient e of row i is
-// band[(e*n + i)*bstride]. One lane per column; only one warp calls it.
+// band[(e*n + i)*bstride], read from shared memory: the 2n-step recurrence
+// is a serial chain, so each step must not wait on a global load.
+// One lane per column; only one warp calls it.
 template <typename P>
-__device__ __forceinline__ void reduced_solve(const double* band, int bstride, int n, P* sh, int lane) {
+__device__ __forceinline__ void reduced_solve(const P* band, int bstride, int n, P* sh, int lane) {
     P z1 = P(0), z2 = P(0);
     for (int i = 0; i < n; i++) {
-        P z = sh[i * 32 + lane] - P(band[(size_t)(0 * n + i) * bstride]) * z1 - P(band[(size_t)(1 * n + i) * bstride]) * z2;
+        P z = sh[i * 32 + lane] - band[(0 * n + i) * bstride] * z1 - band[(1 * n + i) * bstride] * z2;
         sh[i * 32 + lane] = z;
         z2 = z1;
         z1 = z;
     }
     P x1 = P(0), x2 = P(0);
     for (int i = n - 1; i >= 0; i--) {
-        P x = (sh[i * 32 + lane] - P(band[(size_t)(2 * n + i) * bstride]) * x1 -
-               P(band[(size_t)(3 * n + i) * bstride]) * x2) * P(band[(size_t)(4 * n + i) * bstride]);
+        P x = (sh[i * 32 + lane] - band[(2 * n + i) * bstride] * x1 - band[(3 * n + i) * bstride] * x2) *
+              band[(4 * n + i) * bstride];
         sh[i * 32 + lane] = x;
         x2 = x1;
         x1 = x;
     }
 }
 
+// Copies count band coefficients to shared memory (all threads of the block;
+// ordered before their use by the first barrier of segment_couplings).
+template <typename P>
+__device__ __forceinline__ void stage_band(const double* g, int count, P* sh) {
+    for (int t = threadIdx.x; t < count; t += blockDim.x) sh[t] = P(g[t]);
+}
+
+// Shared scratch of a line-solve block: segment ends, then the staged band.
+constexpr int kShY = 2 * kMaxSeg * 32;
+constexpr int kShBand = 10 * kMaxSeg;
+
 // After each warp parked its segment's first/last y in shY: solves for the
 // segment-end unknowns (warp 0) and returns this thread's couplings
 // x[a-1] (XL) and x[b] (XR). Contains two block barriers.
 template <typename P>
-__device__ __forceinline__ void segment_couplings(const double* band, int bstride, int S, P* shY, int lane, int s,
+__device__ __forceinline__ void segment_couplings(const P* band, int bstride, int S, P* shY, int lane, int s,
                                                   bool lane_ok, P& XL, P& XR) {
     __syncthreads();
     if (s == 0 && lane_ok) reduced_solve(band, bstride, 2 * S, shY, lane);
@@ -141,7 +154,7 @@ __device__ __forceinline__ void segment_couplings(const double* band, int bstrid
 //   out = X + omega * Dline^{-1} (f - S X),  X = xin + P xc.
 // Each thread loads its column's segment rows (and one row above and below)
 // once; x neighbours come from the adjacent lanes by shuffle, and only the
-// strip's edge lanes load a halo column. shY: shared [2*kMaxSeg][32] of P.
+// strip's edge lanes load a halo column. shY: shared [kShY + kShBand] of P.
 // Every thread of the block must call it.
 template <typename P, int LS>
 __device__ __forceinline__ void line_sweep(const LineLevel& L, const ZOps& z, int col0, const P* f,
@@ -150,6 +163,8 @@ __device__ __forceinline__ void line_sweep(const LineLevel& L, const ZOps& z, in
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
     const int i = col0 + lane;
     const bool wact = (s < L.S);                 // warp has a segment
+    P* shB = shY + kShY;
+    stage_band(L.band, 10 * L.S, shB);
     const bool act = wact && (i < L.nxl);
     const int a = wact ? (s * L.NK) / L.S : 0, b = wact ? ((s + 1) * L.NK) / L.S : 0, len = b - a;
     const bool has_x = (xin != nullptr) || (xc != nullptr);
@@ -202,7 +217,7 @@ __device__ __forceinline__ void line_sweep(const LineLevel& L, const ZOps& z, in
         }
     }
     P XL, XR;
-    segment_couplings(L.band, 1, L.S, shY, lane, s, col0 + lane < L.nxl, XL, XR);
+    segment_couplings(shB, 1, L.S, shY, lane, s, col0 + lane < L.nxl, XL, XR);
     if (act) {
 #pragma unroll
         for (int j = 0; j < LS; j++) {
@@ -228,7 +243,7 @@ struct SweepArgs {
 
 template <typename P, int LS>
 __global__ void __launch_bounds__(32 * kMaxSeg) k_line_sweep(SweepArgs<P> a) {
-    __shared__ P shY[2 * kMaxSeg * 32];
+    __shared__ P shY[kShY + kShBand];
     line_sweep<P, LS>(a.L, a.z, blockIdx.x * 32, a.f, a.xin, a.xc, a.pitch_c, a.nc, a.out, a.omega, shY);
 }
 
@@ -264,13 +279,15 @@ constexpr int kOwned = 28;
 template <typename P, int LS>
 __global__ void __launch_bounds__(32 * kMaxSeg) k_presmooth_restrict(LineLevel L, ZOps z, const P* f, P* xout,
                                                                       P* fc, int pitch_c, P omega) {
-    __shared__ P shY[2 * kMaxSeg * 32];
+    __shared__ P shY[kShY + kShBand];
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
     const int c0 = blockIdx.x * kOwned;
     const int col = (c0 - 2 + lane + L.nxl) % L.nxl;
     const bool wact = (s < L.S);
     const int a = wact ? (s * L.NK) / L.S : 0, b = wact ? ((s + 1) * L.NK) / L.S : 0, len = b - a;
     const bool owned = (lane >= 2) && (lane < 2 + kOwned) && (c0 + lane - 2 < L.nxl);
+    P* shB = shY + kShY;
+    stage_band(L.band, 10 * L.S, shB);
     P y[LS], fv[LS];
     if (wact) {
 #pragma unroll
@@ -287,7 +304,7 @@ __global__ void __launch_bounds__(32 * kMaxSeg) k_presmooth_restrict(LineLevel L
         shY[(2 * s + 1) * 32 + lane] = ylast;
     }
     P XL, XR;
-    segment_couplings(L.band, 1, L.S, shY, lane, s, true, XL, XR);
+    segment_couplings(shB, 1, L.S, shY, lane, s, true, XL, XR);
     __syncthreads();   // every warp has read its couplings before shY is reused
     P x[LS];
     if (wact) {
@@ -373,8 +390,9 @@ __device__ __forceinline__ void seg_thomas_modes(const ModeSolve& M, int m, int 
 template <typename P, int LS>
 __global__ void __launch_bounds__(32 * kMaxSeg) k_coarse_modes(ModeSolve M, const P* f, P* x) {
     extern __shared__ unsigned char smem_raw[];
-    P* fs = reinterpret_cast<P*>(smem_raw);             // [NK][nc]
-    P* xh = fs + (size_t)M.NK * M.nc;                   // [NK][nc]
+    P* fs = reinterpret_cast<P*>(smem_raw);             // [NK][nc]: f, later the mode solution
+    P* xh = fs;                                         // (f is dead after the first barrier)
+    P* bs = fs + (size_t)M.NK * M.nc;                   // [5][2S][nc] band
     __shared__ P shY[2 * kMaxSeg * 32];
     __shared__ P Qs[32 * 32];    // Q[col][m]: forward transform, lanes = m
     __shared__ P QT[32 * 32];    // Q[col][m] at [m][col]: inverse, lanes = col
@@ -383,6 +401,7 @@ __global__ void __launch_bounds__(32 * kMaxSeg) k_coarse_modes(ModeSolve M, cons
         int kk = t / nc, c = t % nc;
         fs[t] = f[(size_t)kk * M.pitch + c];
     }
+    stage_band(M.band, 10 * S * nc, bs);
     for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) {
         Qs[t] = P(M.Q[t]);
         QT[(t % nc) * nc + t / nc] = P(M.Q[t]);
@@ -413,7 +432,7 @@ __global__ void __launch_bounds__(32 * kMaxSeg) k_coarse_modes(ModeSolve M, cons
         shY[(2 * s + 1) * 32 + lane] = ylast;
     }
     P XL, XR;
-    segment_couplings(M.band + m, nc, S, shY, lane, s, lane < nc, XL, XR);
+    segment_couplings(bs + m, nc, S, shY, lane, s, lane < nc, XL, XR);
     if (act) {
 #pragma unroll
         for (int j = 0; j < LS; j++) {
@@ -465,7 +484,7 @@ __device__ __forceinline__ void sweep_all(const LineLevel& L, const ZOps& z, con
 
 template <typename P, int LS>
 __global__ void __launch_bounds__(32 * kMaxSeg) k_mg_coarse_cycle(CoarseCycleArgs<P> a) {
-    __shared__ P shY[2 * kMaxSeg * 32];
+    __shared__ P shY[kShY + kShBand];
     const int n = a.nlev;
     for (int l = 0; l < n - 1; l++) {
         const P* fl = (l == 0) ? a.f0 : a.f[l];

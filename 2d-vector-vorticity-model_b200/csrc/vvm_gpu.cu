@@ -506,9 +506,10 @@ struct Multigrid {
         while (lc > 0 && nx[lc - 1] <= 32) lc--;
         if (nlev - lc > kMaxCoarseLevels) lc = nlev - kMaxCoarseLevels;
         // exact Fourier-mode solve on the first level of at most 32 columns
-        // when its two shared-memory tiles fit
+        // when its shared-memory tiles (f / solution and the reduced-system
+        // bands, next to 32 KB of static tiles) fit in 227 KB
         for (int l = 0; l < nlev; l++) {
-            if (nx[l] <= 32 && (size_t)2 * NK * nx[l] * sizeof(P) <= 160 * 1024) {
+            if (nx[l] <= 32 && ((size_t)NK + 10 * (size_t)S) * nx[l] * sizeof(P) <= 192 * 1024) {
                 modes = true;
                 lc = l;
                 nlev = l + 1;   // coarser levels are not needed
@@ -579,7 +580,7 @@ struct Multigrid {
         }
         ms = ModeSolve{nc, pl, NK, S, upload(ar, Q), upload(ar, lo), upload(ar, inv), upload(ar, cp),
                        upload(ar, gL), upload(ar, gR), upload(ar, Mi)};
-        mode_smem = (size_t)2 * NK * nc * sizeof(P);
+        mode_smem = ((size_t)NK * nc + (size_t)10 * S * nc) * sizeof(P);
         auto setattr = [&](auto kern) {
             CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mode_smem));
         };

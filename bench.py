@@ -324,7 +324,7 @@ def reference_arm(args):
     m.load(st)
     for _ in range(min(args.warmup, 1)):
         m.one_step()
-    nsteps = max(1, min(args.steps, 8))
+    nsteps = max(1, min(args.steps, 4))
     t0 = time.perf_counter()
     for _ in range(nsteps):
         m.one_step()
