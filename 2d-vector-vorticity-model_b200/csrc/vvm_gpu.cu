@@ -1659,6 +1659,9 @@ int need_state(vvm_gpu_ctx* c) {
 
 }  // namespace
 
+// Message of a failed context-free entry, returned by vvm_gpu_last_error(NULL, ...).
+void vvm_set_context_free_error(const std::string& msg) { g_create_error = msg; }
+
 // ===========================================================================
 // C ABI
 

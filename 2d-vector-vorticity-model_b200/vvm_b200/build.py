@@ -39,7 +39,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
            "-Xptxas", "-v" if verbose else "-O3",
-           str(CSRC / "vvm_gpu.cu"), "-o", str(tmp), "-l:libstdc++.so.6"]
+           str(CSRC / "vvm_gpu.cu"), str(CSRC / "poisson_noalloc.cu"), "-o", str(tmp), "-l:libstdc++.so.6"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)

@@ -73,7 +73,7 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_download_state", "vvm_gpu_upload_prognostic", "vvm_gpu_download_prognostic",
            "vvm_gpu_set_step", "vvm_gpu_get_step", "vvm_gpu_step", "vvm_gpu_poisson_solve",
            "vvm_gpu_poisson_solve_device", "vvm_gpu_last_solve", "vvm_gpu_profile",
-           "vvm_gpu_profile_read", "vvm_gpu_launch_count") + tuple(
+           "vvm_gpu_profile_read", "vvm_gpu_launch_count", "vvm_gpu_poisson_solve_noalloc") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -106,6 +106,8 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_poisson_solve_device.argtypes = [vp, vp, vp, ctypes.c_double,
                                                ctypes.POINTER(ip), _dp]
     L.vvm_gpu_last_solve.argtypes = [vp, ctypes.POINTER(ip), _dp]
+    L.vvm_gpu_poisson_solve_noalloc.argtypes = [ip, ip, _dp, _dp, vp, vp, ctypes.c_double, ip, vp,
+                                                ctypes.POINTER(ip), _dp]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -118,6 +120,27 @@ def load_library(path: Path | None = None):
 
 def _ptr(a):
     return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def poisson_solve_noalloc(NX: int, NZ: int, rhou: np.ndarray, rhow: np.ndarray, d_b: int, d_W: int,
+                          tol: float = 1e-10, maxit: int = 10000, stream: int = 0):
+    """vvm_gpu_poisson_solve_noalloc: the cal_w solve on caller-owned device
+    buffers (raw pointers, NX*(NZ-1) doubles) with no context and no device
+    allocation. Returns (iterations, relative residual)."""
+    L = load_library()
+    rhou = np.ascontiguousarray(rhou, dtype=np.float64)
+    rhow = np.ascontiguousarray(rhow, dtype=np.float64)
+    if rhou.size < NZ + 2 or rhow.size < NZ + 2:
+        raise ValueError("rhou and rhow need NZ+2 values")
+    it, rel = ctypes.c_int(), ctypes.c_double()
+    rc = L.vvm_gpu_poisson_solve_noalloc(int(NX), int(NZ), _ptr(rhou), _ptr(rhow), ctypes.c_void_p(d_b),
+                                         ctypes.c_void_p(d_W), float(tol), int(maxit),
+                                         ctypes.c_void_p(stream), ctypes.byref(it), ctypes.byref(rel))
+    if rc != 0:
+        buf = ctypes.create_string_buffer(512)
+        L.vvm_gpu_last_error(None, buf, 512)
+        raise VVMGpuError(rc, buf.value.decode())
+    return it.value, rel.value
 
 
 class VVMGpu:

@@ -161,6 +161,41 @@ int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_
 /* Iterations and final relative residual of the last cal_w solve. */
 int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres);
 
+/* -- elliptic solve that allocates nothing ------------------------------------
+ * No counterpart in the reference.
+ *
+ * Solves the same system as vvm_gpu_poisson_solve_device (same unknown
+ * ordering, same stopping test ||b - A W||_2 / ||b||_2 <= tol) without a
+ * context, and without allocating device memory. It is for callers that
+ * cannot allocate during the solve, for example a host model that reserves
+ * the device memory for its own pool at start-up and forbids allocation in
+ * its time loop, or a GPU_POISSON-style replacement of cal_w that has b and W
+ * on the device but keeps no context of this library.
+ *
+ * rhou, rhow: host profiles of NZ+2 doubles (the model's [nz] arrays).
+ * d_b, d_W: device buffers of NX*(NZ-1) doubles on the current device; the
+ * incoming W is ignored (the solve starts from W = 0). Runs FP64 CG with exact
+ * z-line solves as preconditioner, at most maxit iterations, on `stream`
+ * (NULL: the legacy default stream), and returns after the solve completed.
+ *
+ * Working memory is a fixed file-scope device array of
+ * VVM_NOALLOC_SCRATCH_BYTES per device, so NX*(NZ-1) may not exceed
+ * VVM_NOALLOC_MAX_UNKNOWNS and NZ-1 may not exceed VVM_NOALLOC_MAX_ROWS;
+ * larger problems return VVM_GPU_EINVAL (message from
+ * vvm_gpu_last_error(NULL, ...), like every failure of this entry).
+ * None of that memory has to start at zero: each call writes every word
+ * before reading it. The first call on each device does a one-time set-up
+ * (it looks up the array's device address, which may load the library's
+ * device code): make it, with that device current, before any stream capture
+ * begins. Calls that overlap on one device (two host threads, or two streams
+ * without ordering between them) share the one array and race: serialise them. */
+#define VVM_NOALLOC_MAX_UNKNOWNS 131072
+#define VVM_NOALLOC_MAX_ROWS 1024
+#define VVM_NOALLOC_SCRATCH_BYTES 4251712
+int vvm_gpu_poisson_solve_noalloc(int NX, int NZ, const double* rhou, const double* rhow,
+                                  const double* d_b, double* d_W, double tol, int maxit,
+                                  void* stream, int* iters, double* relres);
+
 /* -- timers -------------------------------------------------------------------
  * The reference keeps per-phase wall timers of each step (t_advection,
  * t_poisson, t_microphysics, t_diffusion, t_all; src/Iteration.cpp:286-435).
