@@ -607,14 +607,16 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
 // theta and zeta fused in (NumericalProcess.cpp:60-85).
 //
 // The reference sweeps k outer, i inner and reads the already-updated left
-// (i-1) and lower (k-1) neighbours, so row k is the first-order linear
-// recurrence v'[i] = A[i] + B[i] v'[i-1] with v'[0] the untouched ghost, where
-// B[i] is the left-face coefficient and A[i] collects everything else
-// (including the updated row k-1). One block of 1024 threads owns one field
-// and walks the rows in order; each row is solved with an affine-map scan:
-// a thread composes the maps of its contiguous chunk, warps scan those with
-// shuffles, warp 0 scans the warp totals. The updated row stays in registers
-// for the next row.
+// (i-1) and lower (k-1) neighbours, so cell (i, k) obeys
+//   v'(i,k) = A0(i,k) + C(i,k) v'(i,k-1) + B(i,k) v'(i-1,k),
+// where A0, C and B depend on old values only: B is the left-face
+// coefficient, C the lower-face one, A0 collects the rest. Two kernels:
+// k_gs_coeffs forms A0, C, B for every cell of the five fields in parallel;
+// k_gs_scan then runs the recurrence, one block per field walking the rows in
+// order. Row k is a first-order linear recurrence along i (v'(0,k) the
+// untouched ghost), solved as a scan of affine maps: each thread composes
+// the maps of its PER contiguous cells, warps scan those with shuffles, and
+// every warp scans the warp totals itself, so a row costs one block barrier.
 
 template <typename T>
 struct GSArgs {
@@ -625,91 +627,125 @@ struct GSArgs {
     const T *RKM, *RKH;
     int mask;         // bit f: diffuse field f
     int nudge;        // fuse Nudge_theta (field 1) and Nudge_zeta (field 0)
+    T *A0, *C, *B;    // per-cell coefficients, [5][cells] each
 };
 
-constexpr int kGSThreads = 1024;
+constexpr int kGSMaxThreads = 1024;
 constexpr int kGSMaxPerThread = 8;   // NX up to 8192
+// rows in flight of the 1024-thread scan (64 registers a thread)
+template <typename T>
+constexpr int kGSWideRing = sizeof(T) == 4 ? 1 : 0;
 
-// Row k of the sweep solves v'[i] = A0[i] + C[i] v'(i, k-1) + B[i] v'[i-1]:
-// A0, C and B use only old values, so those of row k+1 are formed while
-// row k is being scanned (the global-memory latency hides behind the scan).
-template <typename T, int PER>
-__global__ void __launch_bounds__(kGSThreads) k_gs_diffuse(GSArgs<T> a) {
-    __shared__ T shA[32], shB[32];
+// A0, C, B of cell (i, k) of field blockIdx.z, i = 0..pitch-1, k = 1..nz-2
+// (Turbulent.cpp:83-88 for zeta, :107-112 for the scalars). The ghost i = 0
+// gets the constant map v'(0, k) = v(0, k) (never updated), cells beyond
+// NX the identity map, so a row's scan needs no edge cases.
+template <typename T>
+__global__ void k_gs_coeffs(GSArgs<T> a) {
+    const int f = blockIdx.z;
+    if (!(a.mask & (1 << f))) return;
+    const Dims& d = a.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= d.pitch || k > d.nz - 2) return;
+    const T* v = a.v[f];
+    if (i == 0 || i > d.nx - 2) {
+        const size_t e = (size_t)f * d.cells() + d.at(i, k);
+        a.A0[e] = (i == 0) ? v[d.at(0, k)] : T(0);
+        a.C[e] = T(0);
+        a.B[e] = (i == 0) ? T(0) : T(1);
+        return;
+    }
+    const bool mom = (f == 0);
+    const T* K = mom ? a.RKM : a.RKH;
+    const T cx = T(a.c.rdx2 * a.c.dt);
+    const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
+    T v0 = v[d.at(i, k)], vr = v[d.at(i + 1, k)], vu = v[d.at(i, k + 1)];
+    T ax, bx, czu, czd;
+    if (mom) {
+        T Kc = K[d.at(i, k)], Kd = K[d.at(i, k - 1)], Kl = K[d.at(i - 1, k)], Kld = K[d.at(i - 1, k - 1)];
+        ax = T(0.5) * (Kc + Kd);
+        bx = T(0.5) * (Kl + Kld);
+        czu = T(a.p.rhou[k]) * T(0.5) * (Kc + Kl);
+        czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd + Kld);
+    } else {
+        T Kc = K[d.at(i, k)], Kr = K[d.at(i + 1, k)], Kl = K[d.at(i - 1, k)];
+        T Ku = K[d.at(i, k + 1)], Kd = K[d.at(i, k - 1)];
+        ax = T(0.5) * (Kr + Kc);
+        bx = T(0.5) * (Kc + Kl);
+        czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku + Kc);
+        czd = T(a.p.rhow[k]) * T(0.5) * (Kc + Kd);
+    }
+    T du = vu - v0, dd = v0;
+    if (kPert<T> && (f == 1 || f == 2)) {   // th', qv' about a profile
+        du += T(a.p.d0[f - 1][k + 1]);
+        dd += T(a.p.d0[f - 1][k]);
+    }
+    // v + cx (ax (vr - v) - bx (v - v'[i-1])) + cz (czu du - czd (dd - v'below))
+    const size_t e = (size_t)f * d.cells() + d.at(i, k);
+    a.A0[e] = v0 + cx * (ax * (vr - v0) - bx * v0) + cz * (czu * du - czd * dd);
+    a.C[e] = cz * czd;
+    a.B[e] = cx * bx;
+}
+
+// The recurrence of field blockIdx.x, rows 1..nz-2 in order. A ring of D
+// rows of coefficients in registers: row k+D is loaded into the slot that row
+// k has just used (D = 0: each row is loaded when it is scanned). The row loop
+// is unrolled by D so every slot is a fixed set of registers: nothing copies
+// a register whose load is still in flight. At most MAXT threads.
+template <typename T, int PER, int D, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_gs_scan(GSArgs<T> a) {
+    __shared__ T shA[2][32], shB[2][32];
     const int f = blockIdx.x;
     if (!(a.mask & (1 << f))) return;
     const Dims& d = a.d;
     T* v = a.v[f];
     const bool mom = (f == 0);
-    const T* K = mom ? a.RKM : a.RKH;
-    const int NX = d.nx - 2;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int NX = d.nx - 2, kend = d.nz - 2;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     const int i0 = 1 + tid * PER;
-    const T cx = T(a.c.rdx2 * a.c.dt);
-    T vdn[PER], A0[PER], Cc[PER], Bb[PER];
-    // coefficients of row k from old values (Turbulent.cpp:83-88 for zeta,
-    // :107-112 for the scalars)
-    auto coeffs = [&](int k) {
-        const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
+    const size_t fo = (size_t)f * d.cells();
+    const T* __restrict__ gA = a.A0 + fo;
+    const T* __restrict__ gC = a.C + fo;
+    const T* __restrict__ gB = a.B + fo;
+    constexpr int R = D > 0 ? D : 1;
+    // ring slots: coefficients, the row's left ghost and its nudging scalars
+    T ra[R][PER], rc[R][PER], rb[R][PER], rg[R], rdc[R], rtr[R];
+    auto load = [&](int k, T (&A)[PER], T (&Cc)[PER], T (&Bb)[PER], T& g, T& dc, T& tr) {
 #pragma unroll
         for (int e = 0; e < PER; e++) {
-            int i = i0 + e;
-            A0[e] = T(0);
-            Cc[e] = T(0);
-            Bb[e] = T(0);
-            if (i <= NX) {
-                T v0 = v[d.at(i, k)], vr = v[d.at(i + 1, k)], vu = v[d.at(i, k + 1)];
-                T ax, bx, czu, czd;
-                if (mom) {
-                    T Kc = K[d.at(i, k)], Kd = K[d.at(i, k - 1)], Kl = K[d.at(i - 1, k)], Kld = K[d.at(i - 1, k - 1)];
-                    ax = T(0.5) * (Kc + Kd);
-                    bx = T(0.5) * (Kl + Kld);
-                    czu = T(a.p.rhou[k]) * T(0.5) * (Kc + Kl);
-                    czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd + Kld);
-                } else {
-                    T Kc = K[d.at(i, k)], Kr = K[d.at(i + 1, k)], Kl = K[d.at(i - 1, k)];
-                    T Ku = K[d.at(i, k + 1)], Kd = K[d.at(i, k - 1)];
-                    ax = T(0.5) * (Kr + Kc);
-                    bx = T(0.5) * (Kc + Kl);
-                    czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku + Kc);
-                    czd = T(a.p.rhow[k]) * T(0.5) * (Kc + Kd);
-                }
-                T du = vu - v0, dd = v0;
-                if (kPert<T> && (f == 1 || f == 2)) {   // th', qv' about a profile
-                    du += T(a.p.d0[f - 1][k + 1]);
-                    dd += T(a.p.d0[f - 1][k]);
-                }
-                // v + cx (ax (vr - v) - bx (v - v'[i-1])) + cz (czu du - czd (dd - v'below))
-                A0[e] = v0 + cx * (ax * (vr - v0) - bx * v0) + cz * (czu * du - czd * dd);
-                Cc[e] = cz * czd;
-                Bb[e] = cx * bx;
-            }
+            const int i = i0 + e;
+            const bool ok = (k <= kend) && (i <= NX);
+            A[e] = ok ? gA[d.at(i, k)] : T(0);
+            Cc[e] = ok ? gC[d.at(i, k)] : T(0);
+            Bb[e] = ok ? gB[d.at(i, k)] : T(0);
         }
+        g = (k <= kend) ? v[d.at(0, k)] : T(0);   // ghost v'(0, k): never updated
+        const int kc = (k <= kend) ? k : kend;
+        dc = mom ? T(a.p.dtcgr_zeta[kc]) : T(a.p.dtcgr_th[kc]);
+        tr = kPert<T> ? T(-a.p.dn[0][kc]) : T(a.p.thb_init[kc]);   // nudging target of th
     };
-    // row 0 (ghost) stands for the updated row below row 1: never modified
+    T vdn[PER];
 #pragma unroll
-    for (int e = 0; e < PER; e++) {
-        int i = i0 + e;
-        vdn[e] = (i <= NX) ? v[d.at(i, 0)] : T(0);
-    }
-    coeffs(1);
-    for (int k = 1; k <= d.nz - 2; k++) {
+    for (int e = 0; e < PER; e++) vdn[e] = (i0 + e <= NX) ? v[d.at(i0 + e, 0)] : T(0);
+    // row k from one ring slot; the slot is refilled with row k+D once read
+    auto row = [&](int k, T (&A)[PER], T (&Cc)[PER], T (&Bb)[PER], T& g, T& dc, T& tr) {
+        const int par = k & 1;
+        if (D == 0) load(k, A, Cc, Bb, g, dc, tr);
         T Aa[PER], Bk[PER];
-        T cA = T(0), cB = T(1);  // composition of this thread's maps (identity)
+        T cA = T(0), cB = T(1);   // composition of this thread's maps
 #pragma unroll
         for (int e = 0; e < PER; e++) {
-            Aa[e] = A0[e] + Cc[e] * vdn[e];
+            Aa[e] = A[e] + Cc[e] * vdn[e];
             Bk[e] = Bb[e];
             if (i0 + e <= NX) {
                 cA = Aa[e] + Bk[e] * cA;
                 cB = Bk[e] * cB;
             }
         }
-        const T xg = v[d.at(0, k)];   // ghost v'[0] of this row: never updated
-        // next row's coefficients (old values only; row k+1 is written after
-        // the barriers below and only in the next pass)
-        if (k + 1 <= d.nz - 2) coeffs(k + 1);
-        // inclusive warp scan of the chunk maps (earlier maps on lower lanes)
+        const T xg = g, dcgr = dc, tref = tr;
+        if (D > 0) load(k + D, A, Cc, Bb, g, dc, tr);
+        // inclusive warp scan of the thread maps (earlier maps on lower lanes)
         T sA = cA, sB = cB;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -720,45 +756,230 @@ __global__ void __launch_bounds__(kGSThreads) k_gs_diffuse(GSArgs<T> a) {
                 sB = sB * pB;
             }
         }
-        if (lane == 31) { shA[wid] = sA; shB[wid] = sB; }
-        __syncthreads();
-        if (wid == 0) {
-            T wA = shA[lane], wB = shB[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                T pA = __shfl_up_sync(0xffffffffu, wA, o);
-                T pB = __shfl_up_sync(0xffffffffu, wB, o);
-                if (lane >= o) {
-                    wA = wA + wB * pA;
-                    wB = wB * pB;
-                }
-            }
-            shA[lane] = wA;
-            shB[lane] = wB;
+        if (lane == 31) {
+            shA[par][wid] = sA;
+            shB[par][wid] = sB;
         }
         __syncthreads();
-        // exclusive prefix of this thread = (warps before) then (lanes before)
+        // every warp scans the warp totals (double-buffered by row parity:
+        // the next barrier separates these reads from the next writes)
+        T wA = (lane < nw) ? shA[par][lane] : T(0), wB = (lane < nw) ? shB[par][lane] : T(1);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            if (o >= nw) break;
+            T pA = __shfl_up_sync(0xffffffffu, wA, o);
+            T pB = __shfl_up_sync(0xffffffffu, wB, o);
+            if (lane >= o) {
+                wA = wA + wB * pA;
+                wB = wB * pB;
+            }
+        }
+        T pA = __shfl_sync(0xffffffffu, wA, (wid > 0) ? wid - 1 : 0);
+        T pB = __shfl_sync(0xffffffffu, wB, (wid > 0) ? wid - 1 : 0);
+        if (wid == 0) {
+            pA = T(0);
+            pB = T(1);
+        }
+        // exclusive prefix of this thread: warps before, then lanes before
         T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
-        if (lane == 0) { eA = T(0); eB = T(1); }
-        T pA = (wid > 0) ? shA[wid - 1] : T(0), pB = (wid > 0) ? shB[wid - 1] : T(1);
+        if (lane == 0) {
+            eA = T(0);
+            eB = T(1);
+        }
         T x = pA + pB * xg;
         x = eA + eB * x;
-        const T dcgr = mom ? T(a.p.dtcgr_zeta[k]) : T(a.p.dtcgr_th[k]);
-        const T tref = kPert<T> ? T(-a.p.dn[0][k]) : T(a.p.thb_init[k]);   // nudging target of th
 #pragma unroll
         for (int e = 0; e < PER; e++) {
-            int i = i0 + e;
+            const int i = i0 + e;
             if (i <= NX) {
                 x = Aa[e] + Bk[e] * x;
                 vdn[e] = x;
                 T out = x;
-                if (a.nudge && f == 0) out = x - dcgr * x;                                  // Nudge_zeta
-                if (a.nudge && f == 1) out = x - dcgr * (x - tref);                          // Nudge_theta
+                if (a.nudge && f == 0) out = x - dcgr * x;                 // Nudge_zeta
+                if (a.nudge && f == 1) out = x - dcgr * (x - tref);         // Nudge_theta
                 v[d.at(i, k)] = out;
             }
         }
-        __syncthreads();  // shA/shB reuse
+    };
+#pragma unroll
+    for (int r = 0; r < D; r++) load(1 + r, ra[r], rc[r], rb[r], rg[r], rdc[r], rtr[r]);
+    for (int k = 1; k <= kend; k += R) {
+#pragma unroll
+        for (int r = 0; r < R; r++)
+            if (k + r <= kend) row(k + r, ra[r], rc[r], rb[r], rg[r], rdc[r], rtr[r]);
     }
+}
+
+
+// cp.async helpers: 16-byte global -> shared copies, grouped per row.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// The recurrence of field blockIdx.x with the row's coefficients staged in
+// shared memory by cp.async, D rows ahead. Thread t owns cells
+// [t*PER, t*PER + PER) of the padded row (the ghost and the padding carry the
+// constant and identity maps of k_gs_coeffs), so copies, loads and stores are
+// 16-byte vectors. A thread reads back only what it copied itself, so the
+// ring needs no barrier: cp.async.wait_group orders it. Dynamic shared
+// memory: D * 3 * blockDim.x * PER values of T, at most kGSRingBytes.
+constexpr size_t kGSRingBytes = 220 * 1024;
+
+// Most threads whose ring fits (the launch bound, so registers follow it).
+template <typename T, int PER, int D>
+constexpr int gs_max_threads() {
+    const size_t t = kGSRingBytes / ((size_t)D * 3 * PER * sizeof(T)) / 32 * 32;
+    return t > 1024 ? 1024 : (int)t;
+}
+
+template <typename T, int PER, int D>
+__global__ void __launch_bounds__(gs_max_threads<T, PER, D>()) k_gs_scan_async(GSArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T shA[2][32], shB[2][32];
+    const int f = blockIdx.x;
+    if (!(a.mask & (1 << f))) return;
+    const Dims& d = a.d;
+    T* v = a.v[f];
+    const bool mom = (f == 0);
+    const int NX = d.nx - 2, kend = d.nz - 2;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+    const int i0 = tid * PER;
+    const bool act = i0 < d.pitch;       // pitch is a multiple of PER
+    const size_t fo = (size_t)f * d.cells();
+    const T* gsrc[3] = {a.A0 + fo, a.C + fo, a.B + fo};
+    T* ring = reinterpret_cast<T*>(smem_raw);
+    constexpr int kVec = 16 / sizeof(T);  // values per 16-byte copy
+    auto slot = [&](int r, int arr) { return ring + ((size_t)(r * 3 + arr) * blockDim.x + tid) * PER; };
+    auto issue = [&](int k, int r) {      // row k into slot r (one commit group, possibly empty)
+        if (act && k <= kend) {
+#pragma unroll
+            for (int arr = 0; arr < 3; arr++) {
+                const T* src = gsrc[arr] + d.at(i0, k);
+                T* dst = slot(r, arr);
+#pragma unroll
+                for (int q = 0; q < PER; q += kVec) cp_async16(dst + q, src + q);
+            }
+        }
+        cp_async_commit();
+    };
+    auto scal = [&](int k, T& dc, T& tr) {
+        const int kc = (k <= kend) ? k : kend;
+        dc = mom ? T(a.p.dtcgr_zeta[kc]) : T(a.p.dtcgr_th[kc]);
+        tr = kPert<T> ? T(-a.p.dn[0][kc]) : T(a.p.thb_init[kc]);   // nudging target of th
+    };
+    T vdn[PER];
+#pragma unroll
+    for (int e = 0; e < PER; e++) {
+        const int i = i0 + e;
+        vdn[e] = (i >= 1 && i <= NX) ? v[d.at(i, 0)] : T(0);
+    }
+    T dcr[D], trr[D];                     // nudging scalars of the ring's rows
+#pragma unroll
+    for (int r = 0; r < D; r++) {
+        issue(1 + r, r);
+        scal(1 + r, dcr[r], trr[r]);
+    }
+    auto row = [&](int k, int r) {
+        const int par = k & 1;
+        const T dcgr = dcr[r], tref = trr[r];
+        scal(k + D, dcr[r], trr[r]);
+        cp_async_wait<D - 1>();           // row k's group has landed
+        T Aa[PER], Bk[PER];
+        if (act) {
+            const T* sa = slot(r, 0);
+            const T* sc = slot(r, 1);
+            const T* sb = slot(r, 2);
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+                Aa[e] = sa[e] + sc[e] * vdn[e];
+                Bk[e] = sb[e];
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+                Aa[e] = T(0);
+                Bk[e] = T(1);
+            }
+        }
+        T cA = T(0), cB = T(1);   // composition of this thread's maps
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+            cA = Aa[e] + Bk[e] * cA;
+            cB = Bk[e] * cB;
+        }
+        issue(k + D, r);          // the slot's values are in registers now
+        T sA = cA, sB = cB;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T pA = __shfl_up_sync(0xffffffffu, sA, o);
+            T pB = __shfl_up_sync(0xffffffffu, sB, o);
+            if (lane >= o) {
+                sA = sA + sB * pA;
+                sB = sB * pB;
+            }
+        }
+        if (lane == 31) {
+            shA[par][wid] = sA;
+            shB[par][wid] = sB;
+        }
+        __syncthreads();
+        T wA = (lane < nw) ? shA[par][lane] : T(0), wB = (lane < nw) ? shB[par][lane] : T(1);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            if (o >= nw) break;
+            T pA = __shfl_up_sync(0xffffffffu, wA, o);
+            T pB = __shfl_up_sync(0xffffffffu, wB, o);
+            if (lane >= o) {
+                wA = wA + wB * pA;
+                wB = wB * pB;
+            }
+        }
+        T pA = __shfl_sync(0xffffffffu, wA, (wid > 0) ? wid - 1 : 0);
+        T pB = __shfl_sync(0xffffffffu, wB, (wid > 0) ? wid - 1 : 0);
+        if (wid == 0) {
+            pA = T(0);
+            pB = T(1);
+        }
+        T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
+        if (lane == 0) {
+            eA = T(0);
+            eB = T(1);
+        }
+        T x = eA + eB * pA;       // the ghost's constant map makes the carry-in irrelevant
+        T out[PER];
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+            x = Aa[e] + Bk[e] * x;
+            vdn[e] = x;
+            out[e] = x;
+            if (a.nudge && f == 0) out[e] = x - dcgr * x;                 // Nudge_zeta
+            if (a.nudge && f == 1) out[e] = x - dcgr * (x - tref);         // Nudge_theta
+        }
+        T* dst = v + d.at(i0, k);
+        if (act && i0 >= 1 && i0 + PER - 1 <= NX) {
+#pragma unroll
+            for (int q = 0; q < PER; q += kVec) {
+                if constexpr (sizeof(T) == 4)
+                    *reinterpret_cast<float4*>(dst + q) = make_float4(out[q], out[q + 1], out[q + 2], out[q + 3]);
+                else
+                    *reinterpret_cast<double2*>(dst + q) = make_double2(out[q], out[q + 1]);
+            }
+        } else if (act) {
+#pragma unroll
+            for (int e = 0; e < PER; e++)
+                if (i0 + e >= 1 && i0 + e <= NX) dst[e] = out[e];
+        }
+    };
+    for (int k = 1; k <= kend; k += D) {
+#pragma unroll
+        for (int r = 0; r < D; r++)
+            if (k + r <= kend) row(k + r, r);
+    }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------

@@ -13,6 +13,7 @@
 
 #include "../../include/vvm_gpu.h"
 #include "poisson_kernels.cuh"
+#include "spectral_kernels.cuh"
 #include "step_kernels.cuh"
 
 using namespace vvm;
@@ -649,10 +650,84 @@ struct Multigrid {
     }
 };
 
+// Exact Fourier-mode preconditioner (spectral_kernels.cuh); NX a power of two.
+template <typename P>
+struct Spectral {
+    SpecArgs<P> a{};
+    P* out = nullptr;
+    size_t smem = 0;
+    int threads = 0;
+    Stats* stats = nullptr;
+
+    static bool supports(int NX) { return NX >= 4 && NX <= 8192 && (NX & (NX - 1)) == 0; }
+
+    static P* upload(Arena& ar, const std::vector<double>& v) {
+        std::vector<P> h(v.begin(), v.end());
+        P* d = ar.alloc<P>(h.size());
+        CK(cudaMemcpy(d, h.data(), h.size() * sizeof(P), cudaMemcpyHostToDevice));
+        return d;
+    }
+
+    void build(Arena& ar, int NX, int NK, int pitch, const std::vector<double>& cx0, const std::vector<double>& ru,
+               const std::vector<double>& rd) {
+        int logN = 0;
+        while ((1 << logN) < NX) logN++;
+        const int M = NX / 2 + 1, mp = round_up(M, 32);
+        const double pi = 3.14159265358979323846;
+        std::vector<double> twr(NX / 2), twi(NX / 2);
+        for (int j = 0; j < NX / 2; j++) {
+            twr[j] = std::cos(2.0 * pi * j / NX);
+            twi[j] = -std::sin(2.0 * pi * j / NX);
+        }
+        std::vector<double> inv((size_t)NK * mp, 0.0), cp((size_t)NK * mp, 0.0);
+        for (int m = 0; m < M; m++) {
+            const double mu = 2.0 - 2.0 * std::cos(2.0 * pi * m / NX);
+            double up_over_piv = 0.0;   // ru_{k-1} / piv_{k-1}
+            for (int k = 0; k < NK; k++) {
+                const double piv = cx0[k] * mu + ru[k] + rd[k] - (k > 0 ? rd[k] * up_over_piv : 0.0);
+                inv[(size_t)k * mp + m] = 1.0 / piv;
+                cp[(size_t)k * mp + m] = (k + 1 < NK) ? -ru[k] / piv : 0.0;
+                up_over_piv = ru[k] / piv;
+            }
+        }
+        a.NX = NX;
+        a.logN = logN;
+        a.NK = NK;
+        a.pitch = pitch;
+        a.mpitch = mp;
+        a.twr = upload(ar, twr);
+        a.twi = upload(ar, twi);
+        a.inv = upload(ar, inv);
+        a.cp = upload(ar, cp);
+        a.rd = upload(ar, rd);
+        a.sre = ar.alloc<P>((size_t)NK * mp);
+        a.sim = ar.alloc<P>((size_t)NK * mp);
+        out = ar.alloc<P>((size_t)NK * pitch);
+        smem = 2 * (size_t)NX * sizeof(P);
+        threads = std::max(32, std::min(NX / 2, 512));
+        CK(cudaFuncSetAttribute(k_spec_forward<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_spec_inverse<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+
+    // z = S^{-1} r (to round-off); returns the buffer holding z.
+    P* apply(const P* r, cudaStream_t st) {
+        const int rows2 = cdiv(a.NK, 2);
+        LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_forward<P><<<rows2, threads, smem, st>>>(a, r));
+        CKL();
+        LAUNCH(stats, VVM_K_MG_COARSE, st, k_spec_modes<P><<<cdiv(a.NX / 2 + 1, 64), 64, 0, st>>>(a));
+        CKL();
+        LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_inverse<P><<<rows2, threads, smem, st>>>(a, out));
+        CKL();
+        return out;
+    }
+};
+
 // Preconditioned CG on S d = g in precision P with the level-0 vectors below.
 template <typename P>
 struct PCG {
     Multigrid<P> mg;
+    Spectral<P> sp;
+    bool spectral = false;   // Fourier-mode preconditioner instead of the V-cycle
     int NX = 0, NK = 0, pitch = 0;
     P *r = nullptr, *p = nullptr, *q = nullptr;
     double* partial = nullptr;
@@ -677,6 +752,10 @@ struct PCG {
         mg.stats = stats;
         mg.build(ar, NX, NK, cx0, ru, rd);
         pitch = mg.pitch[0];
+        if (spectral) {
+            sp.stats = stats;
+            sp.build(ar, NX, NK, pitch, cx0, ru, rd);
+        }
         r = ar.alloc<P>((size_t)NK * pitch);
         p = ar.alloc<P>((size_t)NK * pitch);
         q = ar.alloc<P>((size_t)NK * pitch);
@@ -696,6 +775,7 @@ struct PCG {
     dim3 block() const { return dim3(64, 4); }
     dim3 grid() const { return dim3(cdiv(NX, 64), cdiv(NK, 4)); }
     VecArgs<P> vargs() const { return VecArgs<P>{NX, pitch, NK, mg.zops(), mg.lines[0].cx, rhow_k}; }
+    P* precond(const P* r, cudaStream_t st) { return spectral ? sp.apply(r, st) : mg.apply(r, st); }
 
     double read_rr(cudaStream_t st) {
         CK(cudaMemcpyAsync(sc_host, sc, sizeof(CGScalars), cudaMemcpyDeviceToHost, st));
@@ -711,7 +791,7 @@ struct PCG {
         const long long n0 = stats->launches;
         VecArgs<P> v = vargs();
         dim3 B = block(), G = grid();
-        P* z = mg.apply(r, st);
+        P* z = precond(r, st);
         LAUNCH(stats, VVM_K_CG, st, k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial));
         CKL();
         LAUNCH(stats, VVM_K_CG, st, k_cg_scalar_it<<<1, 1024, 0, st>>>(partial, npart, sc, ctl));
@@ -750,7 +830,7 @@ struct PCG {
             *relres = (ref2 > 0) ? std::sqrt(rr / ref2) : 0.0;
             return 0;
         }
-        P* z = mg.apply(r, st);
+        P* z = precond(r, st);
         LAUNCH(stats, VVM_K_CG, st, k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial));
         CKL();
         LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RZ));
@@ -769,7 +849,7 @@ struct PCG {
             CKL();
             rr = read_rr(st);
             if (!(rr > stop2) || !std::isfinite(rr) || it >= maxit) break;
-            z = mg.apply(r, st);
+            z = precond(r, st);
             LAUNCH(stats, VVM_K_CG, st, k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial));
             CKL();
             LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_RZ_BETA));
@@ -791,6 +871,7 @@ struct Fields {
     T* hist[NHIST][2] = {};
     T *d_auto = nullptr, *d_accr = nullptr, *d_evap = nullptr, *d_cond = nullptr;
     T *precip = nullptr, *th_forcing = nullptr;
+    T *gsA = nullptr, *gsC = nullptr, *gsB = nullptr;   // Gauss-Seidel coefficients, [5][cells]
 };
 
 }  // namespace
@@ -805,6 +886,7 @@ struct vvm_gpu_ctx {
     Dims d{};
     Consts c{};
     bool mixed = false;
+    bool spectral = false;   // VVM_SOLVER_SPECTRAL
     Arena ar;
     Fields<double> f64;
     Fields<float> f32;
@@ -900,6 +982,9 @@ template <>
 Fields<float>& fields<float>(vvm_gpu_ctx* c) { return c->f32; }
 
 template <typename T>
+void gs_set_smem();
+
+template <typename T>
 void alloc_fields(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     size_t n = c->d.cells();
@@ -922,6 +1007,10 @@ void alloc_fields(vvm_gpu_ctx* c) {
     F.d_cond = c->ar.alloc<T>(n);
     F.precip = c->ar.alloc<T>(c->d.nx);
     F.th_forcing = c->ar.alloc<T>(n);
+    F.gsA = c->ar.alloc<T>(5 * n);
+    F.gsC = c->ar.alloc<T>(5 * n);
+    F.gsB = c->ar.alloc<T>(5 * n);
+    gs_set_smem<T>();
 }
 
 // ---------------------------------------------------------------- routines
@@ -1031,6 +1120,31 @@ void launch_kessler(vvm_gpu_ctx* c, bool halo) {
     launch_apply<T>(c, halo ? (F_TH | F_QV | F_QC | F_QR) : (F_QV | F_QC | F_QR), F_QV | F_QC | F_QR, false, halo);
 }
 
+// Launch shape of k_gs_scan_async for a padded row of `pitch` cells of
+// `elem` bytes: D = 0 selects the register-prefetch kernel.
+struct GSPlan {
+    int per, threads, D;
+    size_t smem;
+};
+inline GSPlan gs_plan(int pitch, size_t elem) {
+    constexpr size_t kBudget = kGSRingBytes;
+    GSPlan p{};
+    p.per = (pitch / 8 <= 1024) ? 8 : 16;
+    p.threads = round_up(pitch / p.per, 32);
+    const size_t row = 3 * (size_t)p.threads * p.per * elem;
+    p.D = (p.per == 8 && 4 * row <= kBudget) ? 4 : (2 * row <= kBudget ? 2 : 0);
+    p.smem = p.D * row;
+    return p;
+}
+
+template <typename T>
+void gs_set_smem() {
+    const int mx = (int)kGSRingBytes;
+    CK(cudaFuncSetAttribute(k_gs_scan_async<T, 8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_scan_async<T, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_scan_async<T, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+}
+
 template <typename T>
 void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
     Fields<T>& F = fields<T>(c);
@@ -1039,12 +1153,23 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
     LAUNCH(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r));
     CKL();
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
-                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0};
-    const int per = cdiv(c->d.nx - 2, kGSThreads);
-    if (per <= 1) LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 1><<<5, kGSThreads, 0, c->stream>>>(g));
-    else if (per <= 2) LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 2><<<5, kGSThreads, 0, c->stream>>>(g));
-    else if (per <= 4) LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 4><<<5, kGSThreads, 0, c->stream>>>(g));
-    else LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_diffuse<T, 8><<<5, kGSThreads, 0, c->stream>>>(g));
+                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, F.gsC, F.gsB};
+    const int NX = c->d.nx - 2, pitch = c->d.pitch;
+    dim3 cb(64, 4), cg(cdiv(pitch, 64), cdiv(c->d.nz - 2, 4), 5);
+    LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_coeffs<T><<<cg, cb, 0, c->stream>>>(g));
+    CKL();
+    // One block per field, PER cells a thread, coefficient rows staged in
+    // shared memory D rows ahead; when even two rows do not fit, the
+    // register-prefetch variant.
+    const GSPlan p = gs_plan(pitch, sizeof(T));
+    if (p.D == 4 && p.per == 8)
+        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan_async<T, 8, 4><<<5, p.threads, p.smem, c->stream>>>(g));
+    else if (p.D == 2 && p.per == 8)
+        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan_async<T, 8, 2><<<5, p.threads, p.smem, c->stream>>>(g));
+    else if (p.D == 2 && p.per == 16)
+        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan_async<T, 16, 2><<<5, p.threads, p.smem, c->stream>>>(g));
+    else
+        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan<T, 8, kGSWideRing<T>, 1024><<<5, round_up(cdiv(NX, 8), 32), 0, c->stream>>>(g));
     CKL();
 }
 
@@ -1077,6 +1202,7 @@ void ensure_poisson(vvm_gpu_ctx* c) {
     int NX = c->d.nx - 2, NK = c->d.nz - 3;
     c->pcg64.reset(new PCG<double>());
     c->pcg64->stats = &c->stats;
+    c->pcg64->spectral = c->spectral;
     c->pcg64->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
     int pitch = c->pcg64->pitch;
     c->Wf = c->ar.alloc<double>((size_t)NK * pitch);
@@ -1084,7 +1210,7 @@ void ensure_poisson(vvm_gpu_ctx* c) {
     c->r64 = c->ar.alloc<double>((size_t)NK * pitch);
     c->Wprev = c->ar.alloc<double>((size_t)NK * pitch);
     c->nsolves = 0;
-    if (c->mixed) {
+    if (c->mixed && !c->spectral) {
         c->pcg32.reset(new PCG<float>());
         c->pcg32->stats = &c->stats;
         c->pcg32->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
@@ -1113,7 +1239,7 @@ int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
         c->last_relres = 0.0;
         return VVM_GPU_OK;
     }
-    if (!c->mixed) {
+    if (!c->mixed || c->spectral) {   // exact preconditioner: FP64 CG needs one iteration
         double rel = 0;
         int it = c->pcg64->solve(c->Wf, c->W, warm, bb, tol, maxit, c->stream, &rel);
         c->last_iters = it;
@@ -1205,7 +1331,7 @@ long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
     if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
     LAUNCH(&c->stats, VVM_K_CG, st, k_zero_if_b0<<<G, B, 0, st>>>(P64.NX, P64.NK, P64.pitch, P64.sc, c->W));
     CKL();
-    if (!c->mixed) {
+    if (!c->mixed || c->spectral) {
         LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P64.r, P64.partial));
         CKL();
         LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P64.partial, P64.npart, P64.sc, CG_SET_RR));
@@ -1694,7 +1820,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     *out = nullptr;
     const vvm_gpu_desc& D = *desc;
     if (D.NX < 4 || D.NZ < 4) return fail(nullptr, VVM_GPU_EINVAL, "create: NX and NZ must be >= 4");
-    if (D.NX > kGSThreads * kGSMaxPerThread)
+    if (D.NX > kGSMaxThreads * kGSMaxPerThread)
         return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
     if (D.NZ - 1 > 32 * kMaxSeg)
         return fail(nullptr, VVM_GPU_EINVAL, "create: NZ exceeds 1025");
@@ -1707,12 +1833,15 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     if (!(D.dx > 0) || !(D.dz > 0) || !(D.dt > 0)) return fail(nullptr, VVM_GPU_EINVAL, "create: dx, dz, dt must be > 0");
     if (D.precision != VVM_PREC_FP64 && D.precision != VVM_PREC_MIXED)
         return fail(nullptr, VVM_GPU_EINVAL, "create: unknown precision");
-    if (D.solver != VVM_SOLVER_MGPCG && D.solver != VVM_SOLVER_LEARNED)
+    if (D.solver != VVM_SOLVER_MGPCG && D.solver != VVM_SOLVER_LEARNED && D.solver != VVM_SOLVER_SPECTRAL)
         return fail(nullptr, VVM_GPU_EINVAL, "create: unknown solver");
+    if (D.solver == VVM_SOLVER_SPECTRAL && !Spectral<double>::supports(D.NX))
+        return fail(nullptr, VVM_GPU_EINVAL, "create: the spectral solver needs NX a power of two (4..8192)");
     std::unique_ptr<vvm_gpu_ctx> c(new vvm_gpu_ctx());
     c->desc = D;
     c->device = device;
     c->mixed = (D.precision == VVM_PREC_MIXED);
+    c->spectral = (D.solver == VVM_SOLVER_SPECTRAL);
     int prev = 0;
     cudaGetDevice(&prev);
     try {
@@ -1989,7 +2118,8 @@ int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres) {
         if (ctx->last_graph && ctx->poisson_ready) {   // loop state lives on the device
             CGCtl h{};
             CK(cudaStreamSynchronize(ctx->stream));
-            CK(cudaMemcpy(&h, ctx->mixed ? ctx->wctl : ctx->pcg64->ctl, sizeof(CGCtl), cudaMemcpyDeviceToHost));
+            const bool refined = ctx->mixed && !ctx->spectral;   // FP32 inner loops in an FP64 outer loop
+            CK(cudaMemcpy(&h, refined ? ctx->wctl : ctx->pcg64->ctl, sizeof(CGCtl), cudaMemcpyDeviceToHost));
             ctx->last_iters = h.total;
             ctx->last_relres = h.relres;
         }

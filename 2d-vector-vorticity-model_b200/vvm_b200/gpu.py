@@ -23,7 +23,7 @@ PKG = Path(__file__).resolve().parent.parent
 LIB_PATH = PKG / "lib" / "libvvmgpu.so"
 
 VVM_PREC_FP64, VVM_PREC_MIXED = 0, 1
-VVM_SOLVER_MGPCG, VVM_SOLVER_LEARNED = 0, 1
+VVM_SOLVER_MGPCG, VVM_SOLVER_LEARNED, VVM_SOLVER_SPECTRAL = 0, 1, 2
 STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOCONV", 4: "ESTATE"}
 
 _dp = ctypes.POINTER(ctypes.c_double)

@@ -6,10 +6,12 @@ NX=2048 x NZ=256 grid, dx = dz = 100 m, dt = 1 s, synthetic seeded initial
 state (theta = 300 K + 3 K/km, 80 % RH, +2 K cosine bubble of radius 2 km).
 A "step" is one call of the reference's TimeMarching body.
 
-Our arm (default): the mixed-precision step (FP32 fields and stencils,
-FP32 inner CG with FP64 residual, refinement and reductions, multigrid
-preconditioner) is the headline `value`; the plain FP64 multigrid-PCG step is
-timed the same way and reported beside it. Every timed step is bracketed by
+Our arm (default): the mixed-precision step (FP32 fields and stencils, FP64
+Kessler arithmetic and reductions) with the cal_w solve by FP64 CG
+preconditioned with the exact Fourier-mode solve (VVM_SOLVER_SPECTRAL) is the
+headline `value`. The plain FP64 multigrid-PCG step is timed the same way and
+reported beside it (`plain_fp64`), with the two other combinations under
+`variants`. Every timed step is bracketed by
 CUDA events on the stream the library launches on; L2 is flushed (a 256 MB
 write) between timed steps, outside the timed windows. `e2e` repeats the
 headline through the C ABI with the prognostic fields copied from pinned host
@@ -164,11 +166,11 @@ def timed_steps(torch, g, steps, flush):
     return times
 
 
-def run_variant(torch, precision, steps, warmup, flush, device):
+def run_variant(torch, precision, solver, steps, warmup, flush, device):
     from vvm_b200.gpu import VVMGpu
     from vvm_b200.initial_state import warm_bubble
     st = warm_bubble(NX, NZ, DX, DX, DT)
-    g = VVMGpu(st.grid, precision=precision, device=device)
+    g = VVMGpu(st.grid, precision=precision, solver=solver, device=device)
     g.set_stream(torch.cuda.current_stream().cuda_stream)
     g.upload(st)
     g.step(warmup)
@@ -230,23 +232,31 @@ def our_arm(args, rank, world, device):
     # (handle 0, the legacy stream, would hand the library its own stream)
     torch.cuda.set_stream(torch.cuda.Stream(device=device))
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{device}")  # 256 MB > L2
-    from vvm_b200.gpu import VVM_PREC_FP64, VVM_PREC_MIXED
+    from vvm_b200.gpu import (VVM_PREC_FP64, VVM_PREC_MIXED, VVM_SOLVER_MGPCG,
+                              VVM_SOLVER_SPECTRAL)
     hbm, peak_kind = peaks()
     results = {}
+    variants = (("mixed_spectral", VVM_PREC_MIXED, VVM_SOLVER_SPECTRAL),
+                ("fp64_mgpcg", VVM_PREC_FP64, VVM_SOLVER_MGPCG),
+                ("fp64_spectral", VVM_PREC_FP64, VVM_SOLVER_SPECTRAL),
+                ("mixed_mgpcg", VVM_PREC_MIXED, VVM_SOLVER_MGPCG))
     with ClockSampler(device) as clk:
-        for name, prec in (("mixed", VVM_PREC_MIXED), ("fp64", VVM_PREC_FP64)):
+        for name, prec, solver in variants:
             if dist_on():
                 dist_barrier()
-            g, st, times, launches, prof, it, rel = run_variant(torch, prec, args.steps, args.warmup,
-                                                                 flush, device)
+            g, st, times, launches, prof, it, rel = run_variant(torch, prec, solver, args.steps,
+                                                                 args.warmup, flush, device)
             results[name] = dict(g=g, st=st, times=times, launches=launches, prof=prof, it=it, rel=rel)
+            if name not in ("mixed_spectral",):
+                g.close()
+                results[name]["g"] = None
     clocks = clk.summary()
-    head = results["mixed"]
-    total_ms = sum(head["times"])
-    total_ms = dist_max(total_ms)
+    head = results["mixed_spectral"]
     cells = NX * NZ
+    vms = {name: dist_max(sum(r["times"])) for name, r in results.items()}
+    total_ms = vms["mixed_spectral"]
     value = world * cells * args.steps / (total_ms * 1e-3)
-    fp64_ms = dist_max(sum(results["fp64"]["times"]))
+    fp64_ms = vms["fp64_mgpcg"]
     fp64_value = world * cells * args.steps / (fp64_ms * 1e-3)
 
     # e2e through the C ABI with host buffers (pinned) copied in and out each step
@@ -278,19 +288,29 @@ def our_arm(args, rank, world, device):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "NX": NX, "NZ": NZ, "dx_m": DX, "dz_m": DX, "dt_s": DT,
-                   "precision": "mixed: FP32 fields/stencils/inner CG, FP64 residual/refinement/"
-                                "reductions/Kessler arithmetic", "solver": "multigrid-PCG",
+                   "precision": "mixed: FP32 fields/stencils, FP64 Kessler arithmetic, FP64 "
+                                "Poisson CG/residual/reductions",
+                   "solver": "FP64 CG with the exact Fourier-mode (row FFT + per-mode z "
+                             "tridiagonal) preconditioner",
                    "poisson_tol": 1e-10, "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world}"},
         "poisson_ms_per_solve": poisson_ms(head["prof"]),
         "poisson_solves_per_s": 1e3 / poisson_ms(head["prof"]),
         "poisson_iterations_last": head["it"], "poisson_relres_last": head["rel"],
-        "plain_fp64": {"value": fp64_value, "ms_per_step": fp64_ms / args.steps,
-                       "poisson_ms_per_solve": poisson_ms(results["fp64"]["prof"]),
-                       "poisson_iterations_last": results["fp64"]["it"],
-                       "roofline": roofline(results["fp64"]["prof"], head["st"].grid, 8, hbm, peak_kind,
-                                            results["fp64"]["it"])},
+        "plain_fp64": {"solver": "multigrid-PCG", "value": fp64_value,
+                       "ms_per_step": fp64_ms / args.steps,
+                       "poisson_ms_per_solve": poisson_ms(results["fp64_mgpcg"]["prof"]),
+                       "poisson_iterations_last": results["fp64_mgpcg"]["it"],
+                       "poisson_relres_last": results["fp64_mgpcg"]["rel"],
+                       "roofline": roofline(results["fp64_mgpcg"]["prof"], head["st"].grid, 8, hbm,
+                                            peak_kind, results["fp64_mgpcg"]["it"])},
         "speedup_vs_plain_fp64": value / fp64_value,
+        "variants": {name: {"value": world * cells * args.steps / (vms[name] * 1e-3),
+                            "ms_per_step": vms[name] / args.steps,
+                            "poisson_ms_per_solve": poisson_ms(results[name]["prof"]),
+                            "poisson_iterations_last": results[name]["it"],
+                            "poisson_relres_last": results[name]["rel"]}
+                     for name in ("fp64_spectral", "mixed_mgpcg")},
         "roofline": roofline(head["prof"], head["st"].grid, 4, hbm, peak_kind, head["it"]),
         "kernel_ms_per_step": {k: v[0] / 2 for k, v in head["prof"].items()},
         "e2e": {"value": world * cells * args.steps / (e2e_ms * 1e-3), "unit": METRIC,

@@ -51,6 +51,10 @@ extern "C" {
 #define VVM_SOLVER_MGPCG 0    /* geometric multigrid: x-semicoarsening, z-line relaxation */
 #define VVM_SOLVER_LEARNED 1  /* learned BF16 conv preconditioner in flexible CG,
                                  multigrid-PCG as fallback */
+#define VVM_SOLVER_SPECTRAL 2 /* FP64 CG preconditioned by the exact Fourier-mode
+                                 solve (row FFTs in x, one tridiagonal z solve per
+                                 mode); NX a power of two; the FP64 CG also serves
+                                 VVM_PREC_MIXED (one iteration reaches 1e-14) */
 
 /* Model description; mirrors Config_VVM (src/Declare.hpp:27-70) and the
  * constants main.cpp passes (src/main.cpp:68-72). */
