@@ -10,6 +10,8 @@
 // (store_center / store_westdown write every ghost image of a cell).
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include <type_traits>
 
 #include "vvm_common.cuh"
@@ -612,11 +614,12 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
 // where A0, C and B depend on old values only: B is the left-face
 // coefficient, C the lower-face one, A0 collects the rest. Two kernels:
 // k_gs_coeffs forms A0, C, B for every cell of the five fields in parallel;
-// k_gs_scan then runs the recurrence, one block per field walking the rows in
-// order. Row k is a first-order linear recurrence along i (v'(0,k) the
-// untouched ghost), solved as a scan of affine maps: each thread composes
-// the maps of its PER contiguous cells, warps scan those with shuffles, and
-// every warp scans the warp totals itself, so a row costs one block barrier.
+// k_gs_cluster then runs the recurrence, one thread-block cluster per field.
+// Row k is a first-order linear recurrence along i (v'(0,k) the untouched
+// ghost), solved as a scan of affine maps: each thread composes the maps of
+// its PER contiguous cells and the warp scans those with shuffles; warps pass
+// the carry along the row to the next warp, so consecutive warps work on
+// consecutive rows at the same time (a wavefront across the cluster).
 
 template <typename T>
 struct GSArgs {
@@ -628,13 +631,11 @@ struct GSArgs {
     int mask;         // bit f: diffuse field f
     int nudge;        // fuse Nudge_theta (field 1) and Nudge_zeta (field 0)
     T *A0, *C, *B;    // per-cell coefficients, [5][cells] each
+    int* err;         // device error word (kGSErrWait), may be null
 };
 
-constexpr int kGSMaxThreads = 1024;
-constexpr int kGSMaxPerThread = 8;   // NX up to 8192
-// rows in flight of the 1024-thread scan (64 registers a thread)
-template <typename T>
-constexpr int kGSWideRing = sizeof(T) == 4 ? 1 : 0;
+constexpr int kGSMaxNX = 8192;
+constexpr int kGSMaxPerThread = 8;      // cells a thread of the cal_u column integral
 
 // A0, C, B of cell (i, k) of field blockIdx.z, i = 0..pitch-1, k = 1..nz-2
 // (Turbulent.cpp:83-88 for zeta, :107-112 for the scalars). The ghost i = 0
@@ -688,129 +689,6 @@ __global__ void k_gs_coeffs(GSArgs<T> a) {
     a.B[e] = cx * bx;
 }
 
-// The recurrence of field blockIdx.x, rows 1..nz-2 in order. A ring of D
-// rows of coefficients in registers: row k+D is loaded into the slot that row
-// k has just used (D = 0: each row is loaded when it is scanned). The row loop
-// is unrolled by D so every slot is a fixed set of registers: nothing copies
-// a register whose load is still in flight. At most MAXT threads.
-template <typename T, int PER, int D, int MAXT>
-__global__ void __launch_bounds__(MAXT) k_gs_scan(GSArgs<T> a) {
-    __shared__ T shA[2][32], shB[2][32];
-    const int f = blockIdx.x;
-    if (!(a.mask & (1 << f))) return;
-    const Dims& d = a.d;
-    T* v = a.v[f];
-    const bool mom = (f == 0);
-    const int NX = d.nx - 2, kend = d.nz - 2;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-    const int i0 = 1 + tid * PER;
-    const size_t fo = (size_t)f * d.cells();
-    const T* __restrict__ gA = a.A0 + fo;
-    const T* __restrict__ gC = a.C + fo;
-    const T* __restrict__ gB = a.B + fo;
-    constexpr int R = D > 0 ? D : 1;
-    // ring slots: coefficients, the row's left ghost and its nudging scalars
-    T ra[R][PER], rc[R][PER], rb[R][PER], rg[R], rdc[R], rtr[R];
-    auto load = [&](int k, T (&A)[PER], T (&Cc)[PER], T (&Bb)[PER], T& g, T& dc, T& tr) {
-#pragma unroll
-        for (int e = 0; e < PER; e++) {
-            const int i = i0 + e;
-            const bool ok = (k <= kend) && (i <= NX);
-            A[e] = ok ? gA[d.at(i, k)] : T(0);
-            Cc[e] = ok ? gC[d.at(i, k)] : T(0);
-            Bb[e] = ok ? gB[d.at(i, k)] : T(0);
-        }
-        g = (k <= kend) ? v[d.at(0, k)] : T(0);   // ghost v'(0, k): never updated
-        const int kc = (k <= kend) ? k : kend;
-        dc = mom ? T(a.p.dtcgr_zeta[kc]) : T(a.p.dtcgr_th[kc]);
-        tr = kPert<T> ? T(-a.p.dn[0][kc]) : T(a.p.thb_init[kc]);   // nudging target of th
-    };
-    T vdn[PER];
-#pragma unroll
-    for (int e = 0; e < PER; e++) vdn[e] = (i0 + e <= NX) ? v[d.at(i0 + e, 0)] : T(0);
-    // row k from one ring slot; the slot is refilled with row k+D once read
-    auto row = [&](int k, T (&A)[PER], T (&Cc)[PER], T (&Bb)[PER], T& g, T& dc, T& tr) {
-        const int par = k & 1;
-        if (D == 0) load(k, A, Cc, Bb, g, dc, tr);
-        T Aa[PER], Bk[PER];
-        T cA = T(0), cB = T(1);   // composition of this thread's maps
-#pragma unroll
-        for (int e = 0; e < PER; e++) {
-            Aa[e] = A[e] + Cc[e] * vdn[e];
-            Bk[e] = Bb[e];
-            if (i0 + e <= NX) {
-                cA = Aa[e] + Bk[e] * cA;
-                cB = Bk[e] * cB;
-            }
-        }
-        const T xg = g, dcgr = dc, tref = tr;
-        if (D > 0) load(k + D, A, Cc, Bb, g, dc, tr);
-        // inclusive warp scan of the thread maps (earlier maps on lower lanes)
-        T sA = cA, sB = cB;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            T pA = __shfl_up_sync(0xffffffffu, sA, o);
-            T pB = __shfl_up_sync(0xffffffffu, sB, o);
-            if (lane >= o) {
-                sA = sA + sB * pA;
-                sB = sB * pB;
-            }
-        }
-        if (lane == 31) {
-            shA[par][wid] = sA;
-            shB[par][wid] = sB;
-        }
-        __syncthreads();
-        // every warp scans the warp totals (double-buffered by row parity:
-        // the next barrier separates these reads from the next writes)
-        T wA = (lane < nw) ? shA[par][lane] : T(0), wB = (lane < nw) ? shB[par][lane] : T(1);
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            if (o >= nw) break;
-            T pA = __shfl_up_sync(0xffffffffu, wA, o);
-            T pB = __shfl_up_sync(0xffffffffu, wB, o);
-            if (lane >= o) {
-                wA = wA + wB * pA;
-                wB = wB * pB;
-            }
-        }
-        T pA = __shfl_sync(0xffffffffu, wA, (wid > 0) ? wid - 1 : 0);
-        T pB = __shfl_sync(0xffffffffu, wB, (wid > 0) ? wid - 1 : 0);
-        if (wid == 0) {
-            pA = T(0);
-            pB = T(1);
-        }
-        // exclusive prefix of this thread: warps before, then lanes before
-        T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
-        if (lane == 0) {
-            eA = T(0);
-            eB = T(1);
-        }
-        T x = pA + pB * xg;
-        x = eA + eB * x;
-#pragma unroll
-        for (int e = 0; e < PER; e++) {
-            const int i = i0 + e;
-            if (i <= NX) {
-                x = Aa[e] + Bk[e] * x;
-                vdn[e] = x;
-                T out = x;
-                if (a.nudge && f == 0) out = x - dcgr * x;                 // Nudge_zeta
-                if (a.nudge && f == 1) out = x - dcgr * (x - tref);         // Nudge_theta
-                v[d.at(i, k)] = out;
-            }
-        }
-    };
-#pragma unroll
-    for (int r = 0; r < D; r++) load(1 + r, ra[r], rc[r], rb[r], rg[r], rdc[r], rtr[r]);
-    for (int k = 1; k <= kend; k += R) {
-#pragma unroll
-        for (int r = 0; r < R; r++)
-            if (k + r <= kend) row(k + r, ra[r], rc[r], rb[r], rg[r], rdc[r], rtr[r]);
-    }
-}
-
-
 // cp.async helpers: 16-byte global -> shared copies, grouped per row.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -820,166 +698,282 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// The recurrence of field blockIdx.x with the row's coefficients staged in
-// shared memory by cp.async, D rows ahead. Thread t owns cells
-// [t*PER, t*PER + PER) of the padded row (the ghost and the padding carry the
-// constant and identity maps of k_gs_coeffs), so copies, loads and stores are
-// 16-byte vectors. A thread reads back only what it copied itself, so the
-// ring needs no barrier: cp.async.wait_group orders it. Dynamic shared
-// memory: D * 3 * blockDim.x * PER values of T, at most kGSRingBytes.
-constexpr size_t kGSRingBytes = 220 * 1024;
+constexpr int kGSSpinLimit = 1 << 22;   // polls before a wait gives up
+constexpr int kGSErrWait = 1;           // device error word: a Gauss-Seidel wait gave up
+constexpr size_t kGSRingBytes = 200 * 1024;   // cp.async ring of coefficient rows
+constexpr int kGSCarry = 64;            // inbox slots (rows) of a warp
+constexpr int kGSAckEvery = 16;         // rows between acknowledgements
 
-// Most threads whose ring fits (the launch bound, so registers follow it).
-template <typename T, int PER, int D>
-constexpr int gs_max_threads() {
-    const size_t t = kGSRingBytes / ((size_t)D * 3 * PER * sizeof(T)) / 32 * 32;
-    return t > 1024 ? 1024 : (int)t;
+// Flags between CTAs of a cluster: acquire / release at cluster scope through
+// generic addresses (local shared memory, or a peer CTA's mapped into the
+// cluster window).
+__device__ __forceinline__ int ld_acquire_cluster(const int* p) {
+    int v;
+    asm volatile("ld.acquire.cluster.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cluster(int* p, int v) {
+    asm volatile("st.release.cluster.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_cluster_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.cluster.b64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_cluster_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.cluster.b64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
+    return v;
 }
 
-template <typename T, int PER, int D>
-__global__ void __launch_bounds__(gs_max_threads<T, PER, D>()) k_gs_scan_async(GSArgs<T> a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ T shA[2][32], shB[2][32];
-    const int f = blockIdx.x;
-    if (!(a.mask & (1 << f))) return;
-    const Dims& d = a.d;
-    T* v = a.v[f];
-    const bool mom = (f == 0);
-    const int NX = d.nx - 2, kend = d.nz - 2;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-    const int i0 = tid * PER;
-    const bool act = i0 < d.pitch;       // pitch is a multiple of PER
-    const size_t fo = (size_t)f * d.cells();
-    const T* gsrc[3] = {a.A0 + fo, a.C + fo, a.B + fo};
-    T* ring = reinterpret_cast<T*>(smem_raw);
-    constexpr int kVec = 16 / sizeof(T);  // values per 16-byte copy
-    auto slot = [&](int r, int arr) { return ring + ((size_t)(r * 3 + arr) * blockDim.x + tid) * PER; };
-    auto issue = [&](int k, int r) {      // row k into slot r (one commit group, possibly empty)
-        if (act && k <= kend) {
-#pragma unroll
-            for (int arr = 0; arr < 3; arr++) {
-                const T* src = gsrc[arr] + d.at(i0, k);
-                T* dst = slot(r, arr);
-#pragma unroll
-                for (int q = 0; q < PER; q += kVec) cp_async16(dst + q, src + q);
-            }
-        }
-        cp_async_commit();
-    };
-    auto scal = [&](int k, T& dc, T& tr) {
-        const int kc = (k <= kend) ? k : kend;
-        dc = mom ? T(a.p.dtcgr_zeta[kc]) : T(a.p.dtcgr_th[kc]);
-        tr = kPert<T> ? T(-a.p.dn[0][kc]) : T(a.p.thb_init[kc]);   // nudging target of th
-    };
-    T vdn[PER];
-#pragma unroll
-    for (int e = 0; e < PER; e++) {
-        const int i = i0 + e;
-        vdn[e] = (i >= 1 && i <= NX) ? v[d.at(i, 0)] : T(0);
-    }
-    T dcr[D], trr[D];                     // nudging scalars of the ring's rows
-#pragma unroll
-    for (int r = 0; r < D; r++) {
-        issue(1 + r, r);
-        scal(1 + r, dcr[r], trr[r]);
-    }
-    auto row = [&](int k, int r) {
-        const int par = k & 1;
-        const T dcgr = dcr[r], tref = trr[r];
-        scal(k + D, dcr[r], trr[r]);
-        cp_async_wait<D - 1>();           // row k's group has landed
-        T Aa[PER], Bk[PER];
-        if (act) {
-            const T* sa = slot(r, 0);
-            const T* sc = slot(r, 1);
-            const T* sb = slot(r, 2);
-#pragma unroll
-            for (int e = 0; e < PER; e++) {
-                Aa[e] = sa[e] + sc[e] * vdn[e];
-                Bk[e] = sb[e];
-            }
+// A carry travels as row-tagged 64-bit words: (row << 32) | 32 bits of the
+// value (one word for float, two for double). A 64-bit store is seen whole,
+// so a reader that finds its row in every word holds that row's value; no
+// flag and no fence is needed.
+template <typename T>
+struct Tagged {
+    static constexpr int kWords = sizeof(T) / 4;
+    __device__ static void put(unsigned long long* w, T x, int row) {
+        const unsigned long long tag = (unsigned long long)(unsigned)row << 32;
+        if constexpr (sizeof(T) == 4) {
+            st_relaxed_cluster_u64(w, tag | __float_as_uint(x));
         } else {
+            const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+            st_relaxed_cluster_u64(w, tag | (b >> 32));
+            st_relaxed_cluster_u64(w + 1, tag | (b & 0xffffffffull));
+        }
+    }
+    // true and x set when every word carries `row`
+    __device__ static bool get(const unsigned long long* w, int row, T& x) {
+        const unsigned long long w0 = ld_relaxed_cluster_u64(w);
+        if ((int)(w0 >> 32) != row) return false;
+        if constexpr (sizeof(T) == 4) {
+            x = __uint_as_float((unsigned)w0);
+        } else {
+            const unsigned long long w1 = ld_relaxed_cluster_u64(w + 1);
+            if ((int)(w1 >> 32) != row) return false;
+            x = __longlong_as_double((long long)((w0 << 32) | (w1 & 0xffffffffull)));
+        }
+        return true;
+    }
+};
+
+// The recurrence of one field spread over a cluster of CS CTAs. The padded
+// row is cut into chunks of 32*PER cells, one per warp; global warp g sits in
+// CTA g / W as its warp g % W (W warps a CTA). Each warp walks the rows in
+// order on its own: it waits for the carry-in that warp g-1 left, row-tagged,
+// in its own inbox (written locally, or into this CTA's shared memory from
+// the previous CTA through the cluster window), acknowledges every
+// kGSAckEvery-th row in warp g-1's shared memory (a release store, so its
+// reads of the inbox come first), and, once warp g+1 has acknowledged the row
+// that last used the inbox slot it is about to reuse, writes its carry-out
+// into warp g+1's inbox. Everything is polled in local shared memory. Cluster barriers open (all inboxes
+// initialised before any peer writes) and close (no CTA exits while a peer may
+// still write into it) the kernel. Each wait polls at most kGSSpinLimit
+// times; a warp that gives up raises the abort flag of every CTA of the
+// cluster and the device error word, so every wait ends. Coefficient rows are
+// staged in shared memory by cp.async, D rows ahead (a thread reads back only
+// what it copied); the rows' nudging scalars are tabulated in shared memory at
+// the start. Dynamic shared memory: D * 3 * blockDim.x * PER values of T, then
+// 2 * nz values of T.
+constexpr int kGSClusterWarps = 10;   // warps a CTA at most (NX = 8192: 9)
+
+template <typename T, int PER, int D, int CS>
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(32 * kGSClusterWarps) k_gs_cluster(GSArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int kW = Tagged<T>::kWords;
+    __shared__ unsigned long long inbox[kGSClusterWarps][kGSCarry][kW];
+    __shared__ int ack_in[kGSClusterWarps], abort_flag;
+    namespace cgx = cooperative_groups;
+    cgx::cluster_group cl = cgx::this_cluster();
+    const int crank = (int)cl.block_rank();
+    const int f = blockIdx.x / CS;
+    const Dims& d = a.d;
+    const int NX = d.nx - 2, kend = d.nz - 2;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, W = blockDim.x >> 5;
+    for (int j = tid; j < kGSClusterWarps * kGSCarry * kW; j += blockDim.x)
+        (&inbox[0][0][0])[j] = 0ull;    // tag 0: no row
+    if (tid < kGSClusterWarps) ack_in[tid] = 0;
+    if (tid == 0) abort_flag = 0;
+    // nudging of row k: out = x - dn[k] (x - tn[k]) (dn = 0: none)
+    T* dn_tab = reinterpret_cast<T*>(smem_raw) + (size_t)D * 3 * blockDim.x * PER;
+    T* tn_tab = dn_tab + d.nz;
+    for (int k = tid; k < d.nz; k += blockDim.x) {
+        T dn = T(0), tn = T(0);
+        if (a.nudge && f == 0) dn = T(a.p.dtcgr_zeta[k]);                      // Nudge_zeta
+        if (a.nudge && f == 1) {                                                 // Nudge_theta
+            dn = T(a.p.dtcgr_th[k]);
+            tn = kPert<T> ? T(-a.p.dn[0][k]) : T(a.p.thb_init[k]);
+        }
+        dn_tab[k] = dn;
+        tn_tab[k] = tn;
+    }
+    cl.sync();
+    const int gwn = (d.pitch + 32 * PER - 1) / (32 * PER);   // warps with cells
+    const int g = crank * W + wid;
+    const bool run = (a.mask & (1 << f)) && g < gwn;
+    if (run) {
+        T* v = a.v[f];
+        const bool mom = (f == 0);
+        const int i0 = (g * 32 + lane) * PER;
+        const bool act = i0 < d.pitch;       // pitch is a multiple of PER
+        const size_t fo = (size_t)f * d.cells();
+        const T* gsrc[3] = {a.A0 + fo, a.C + fo, a.B + fo};
+        T* ring = reinterpret_cast<T*>(smem_raw);
+        constexpr int kVec = 16 / sizeof(T);
+        auto slot = [&](int r, int arr) { return ring + ((size_t)(r * 3 + arr) * blockDim.x + tid) * PER; };
+        auto issue = [&](int k, int r) {
+            if (act && k <= kend) {
+#pragma unroll
+                for (int arr = 0; arr < 3; arr++) {
+                    const T* src = gsrc[arr] + d.at(i0, k);
+                    T* dst = slot(r, arr);
+#pragma unroll
+                    for (int q = 0; q < PER; q += kVec) cp_async16(dst + q, src + q);
+                }
+            }
+            cp_async_commit();
+        };
+        // neighbours in the chain and their flags
+        const bool has_pred = g > 0, has_succ = g + 1 < gwn;
+        const int pc = (g - 1) / W, pw = (g - 1) % W, sc = (g + 1) / W, sw = (g + 1) % W;
+        int* pred_ack = has_pred ? cl.map_shared_rank(&ack_in[pw], pc) : nullptr;
+        unsigned long long* succ_box = has_succ ? cl.map_shared_rank(&inbox[sw][0][0], sc) : nullptr;
+        auto give_up = [&]() {   // lane 0 of a warp whose wait ran out: stop the cluster
+            for (int r = 0; r < CS; r++) *(volatile int*)cl.map_shared_rank(&abort_flag, r) = 1;
+            if (a.err) atomicOr(a.err, kGSErrWait);
+        };
+        auto wait_carry = [&](int k, T& x) {   // all lanes; warp-uniform result
+            bool okw = false;
+            const unsigned long long* w = &inbox[wid][k % kGSCarry][0];
+            for (int it = 0; it < kGSSpinLimit; it++) {
+                if (Tagged<T>::get(w, k, x)) {
+                    okw = true;
+                    break;
+                }
+                if (*(volatile int*)&abort_flag) break;
+            }
+            const bool all = __all_sync(0xffffffffu, okw);
+            if (!all && lane == 0 && !*(volatile int*)&abort_flag) give_up();
+            return all;
+        };
+        auto wait_ge = [&](const int* p, int target) {   // all lanes; warp-uniform result
+            bool okw = false;
+            for (int it = 0; it < kGSSpinLimit; it++) {
+                if (ld_acquire_cluster(p) >= target) {
+                    okw = true;
+                    break;
+                }
+                if (*(volatile int*)&abort_flag) break;
+            }
+            const bool all = __all_sync(0xffffffffu, okw);
+            if (!all && lane == 0 && !*(volatile int*)&abort_flag) give_up();
+            return all;
+        };
+        T vdn[PER];
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+            const int i = i0 + e;
+            vdn[e] = (act && i >= 1 && i <= NX) ? v[d.at(i, 0)] : T(0);
+        }
+#pragma unroll
+        for (int r = 0; r < D; r++) issue(1 + r, r);
+        bool ok = true;
+        int ack_seen = 0;   // last acknowledgement read from warp g+1
+        auto row = [&](int k, int r) {
+            const T dn = dn_tab[k], tn = tn_tab[k];
+            const int s = k % kGSCarry;
+            // read the carry-in early: when warp g-1 is ahead (the steady
+            // state) it is there and the read overlaps the scan below
+            T xin = T(0);             // warp 0 starts at the ghost's constant map
+            bool have = !has_pred || Tagged<T>::get(&inbox[wid][s][0], k, xin);
+            cp_async_wait<D - 1>();
+            T Aa[PER], Bk[PER];
+            if (act) {
+                const T* sa = slot(r, 0);
+                const T* scc = slot(r, 1);
+                const T* sb = slot(r, 2);
+#pragma unroll
+                for (int e = 0; e < PER; e++) {
+                    Aa[e] = sa[e] + scc[e] * vdn[e];
+                    Bk[e] = sb[e];
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < PER; e++) {
+                    Aa[e] = T(0);
+                    Bk[e] = T(1);
+                }
+            }
+            T cA = T(0), cB = T(1);
 #pragma unroll
             for (int e = 0; e < PER; e++) {
-                Aa[e] = T(0);
-                Bk[e] = T(1);
+                cA = Aa[e] + Bk[e] * cA;
+                cB = Bk[e] * cB;
             }
-        }
-        T cA = T(0), cB = T(1);   // composition of this thread's maps
+            issue(k + D, r);
+            T sA = cA, sB = cB;
 #pragma unroll
-        for (int e = 0; e < PER; e++) {
-            cA = Aa[e] + Bk[e] * cA;
-            cB = Bk[e] * cB;
-        }
-        issue(k + D, r);          // the slot's values are in registers now
-        T sA = cA, sB = cB;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            T pA = __shfl_up_sync(0xffffffffu, sA, o);
-            T pB = __shfl_up_sync(0xffffffffu, sB, o);
-            if (lane >= o) {
-                sA = sA + sB * pA;
-                sB = sB * pB;
+            for (int o = 1; o < 32; o <<= 1) {
+                T qA = __shfl_up_sync(0xffffffffu, sA, o);
+                T qB = __shfl_up_sync(0xffffffffu, sB, o);
+                if (lane >= o) {
+                    sA = sA + sB * qA;
+                    sB = sB * qB;
+                }
             }
-        }
-        if (lane == 31) {
-            shA[par][wid] = sA;
-            shB[par][wid] = sB;
-        }
-        __syncthreads();
-        T wA = (lane < nw) ? shA[par][lane] : T(0), wB = (lane < nw) ? shB[par][lane] : T(1);
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            if (o >= nw) break;
-            T pA = __shfl_up_sync(0xffffffffu, wA, o);
-            T pB = __shfl_up_sync(0xffffffffu, wB, o);
-            if (lane >= o) {
-                wA = wA + wB * pA;
-                wB = wB * pB;
+            const T tA = __shfl_sync(0xffffffffu, sA, 31), tB = __shfl_sync(0xffffffffu, sB, 31);
+            T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
+            if (lane == 0) {
+                eA = T(0);
+                eB = T(1);
             }
-        }
-        T pA = __shfl_sync(0xffffffffu, wA, (wid > 0) ? wid - 1 : 0);
-        T pB = __shfl_sync(0xffffffffu, wB, (wid > 0) ? wid - 1 : 0);
-        if (wid == 0) {
-            pA = T(0);
-            pB = T(1);
-        }
-        T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
-        if (lane == 0) {
-            eA = T(0);
-            eB = T(1);
-        }
-        T x = eA + eB * pA;       // the ghost's constant map makes the carry-in irrelevant
-        T out[PER];
-#pragma unroll
-        for (int e = 0; e < PER; e++) {
-            x = Aa[e] + Bk[e] * x;
-            vdn[e] = x;
-            out[e] = x;
-            if (a.nudge && f == 0) out[e] = x - dcgr * x;                 // Nudge_zeta
-            if (a.nudge && f == 1) out[e] = x - dcgr * (x - tref);         // Nudge_theta
-        }
-        T* dst = v + d.at(i0, k);
-        if (act && i0 >= 1 && i0 + PER - 1 <= NX) {
-#pragma unroll
-            for (int q = 0; q < PER; q += kVec) {
-                if constexpr (sizeof(T) == 4)
-                    *reinterpret_cast<float4*>(dst + q) = make_float4(out[q], out[q + 1], out[q + 2], out[q + 3]);
-                else
-                    *reinterpret_cast<double2*>(dst + q) = make_double2(out[q], out[q + 1]);
+            if (has_pred) {
+                if (!__all_sync(0xffffffffu, have)) ok = ok && wait_carry(k, xin);
+                if (k % kGSAckEvery == 0) {
+                    __syncwarp();
+                    if (lane == 0) st_release_cluster(pred_ack, k);
+                }
             }
-        } else if (act) {
+            if (has_succ) {
+                // slot s last held row k - kGSCarry; acknowledgements come in
+                // steps of kGSAckEvery rows, so the flag is read (acquire)
+                // only when the last one seen does not cover that row
+                if (ack_seen < k - kGSCarry) {
+                    ok = ok && wait_ge(&ack_in[wid], k - kGSCarry);
+                    ack_seen = ld_acquire_cluster(&ack_in[wid]);
+                }
+                if (lane == 0) Tagged<T>::put(succ_box + (size_t)s * kW, tA + tB * xin, k);
+            }
+            T x = eA + eB * xin;
+            T out[PER];
 #pragma unroll
-            for (int e = 0; e < PER; e++)
-                if (i0 + e >= 1 && i0 + e <= NX) dst[e] = out[e];
+            for (int e = 0; e < PER; e++) {
+                x = Aa[e] + Bk[e] * x;
+                vdn[e] = x;
+                out[e] = x - dn * (x - tn);
+            }
+            T* dst = v + d.at(i0, k);
+            if (act && i0 >= 1 && i0 + PER - 1 <= NX) {
+#pragma unroll
+                for (int q = 0; q < PER; q += kVec) {
+                    if constexpr (sizeof(T) == 4)
+                        *reinterpret_cast<float4*>(dst + q) = make_float4(out[q], out[q + 1], out[q + 2], out[q + 3]);
+                    else
+                        *reinterpret_cast<double2*>(dst + q) = make_double2(out[q], out[q + 1]);
+                }
+            } else if (act) {
+#pragma unroll
+                for (int e = 0; e < PER; e++)
+                    if (i0 + e >= 1 && i0 + e <= NX) dst[e] = out[e];
+            }
+        };
+        for (int k = 1; k <= kend && ok; k += D) {
+#pragma unroll
+            for (int r = 0; r < D; r++)
+                if (k + r <= kend && ok) row(k + r, r);
         }
-    };
-    for (int k = 1; k <= kend; k += D) {
-#pragma unroll
-        for (int r = 0; r < D; r++)
-            if (k + r <= kend) row(k + r, r);
+        cp_async_wait<0>();
     }
-    cp_async_wait<0>();
+    cl.sync();
 }
 
 // ---------------------------------------------------------------------------

@@ -920,6 +920,7 @@ struct vvm_gpu_ctx {
     cudaStream_t cap[2] = {};          // streams for capturing loop bodies
     CGCtl* wctl = nullptr;             // outer loop state of the mixed solve
     long long* d_exec = nullptr;       // kernels executed inside graph loops
+    int* d_err = nullptr;              // device error word (kGSErrWait), checked when the host syncs
     bool last_graph = false;           // the last cal_w ran inside a graph
     bool graphs_off = false;
     float *g32 = nullptr, *d32 = nullptr;
@@ -1120,29 +1121,53 @@ void launch_kessler(vvm_gpu_ctx* c, bool halo) {
     launch_apply<T>(c, halo ? (F_TH | F_QV | F_QC | F_QR) : (F_QV | F_QC | F_QR), F_QV | F_QC | F_QR, false, halo);
 }
 
-// Launch shape of k_gs_scan_async for a padded row of `pitch` cells of
-// `elem` bytes: D = 0 selects the register-prefetch kernel.
+// Launch shape of k_gs_cluster for a padded row of `pitch` cells of `elem`
+// bytes: chunks of 32*kGSPer cells (one warp each) over a cluster of cs CTAs
+// of w warps, coefficient rows d ahead.
+constexpr int kGSPer = 4;
 struct GSPlan {
-    int per, threads, D;
+    int cs, w, d;
     size_t smem;
 };
-inline GSPlan gs_plan(int pitch, size_t elem) {
-    constexpr size_t kBudget = kGSRingBytes;
+inline GSPlan gs_plan(int pitch, int nz, size_t elem) {
     GSPlan p{};
-    p.per = (pitch / 8 <= 1024) ? 8 : 16;
-    p.threads = round_up(pitch / p.per, 32);
-    const size_t row = 3 * (size_t)p.threads * p.per * elem;
-    p.D = (p.per == 8 && 4 * row <= kBudget) ? 4 : (2 * row <= kBudget ? 2 : 0);
-    p.smem = p.D * row;
+    const int gwn = cdiv(pitch, 32 * kGSPer);
+    p.cs = gwn >= 8 ? 8 : (gwn >= 4 ? 4 : (gwn >= 2 ? 2 : 1));
+    p.w = cdiv(gwn, p.cs);   // <= kGSClusterWarps for pitch <= 8224 (checked at create)
+    const size_t row = 3 * (size_t)p.w * 32 * kGSPer * elem;
+    const size_t tab = 2 * (size_t)nz * elem;   // nudging scalars
+    p.d = (8 * row + tab <= kGSRingBytes) ? 8 : (4 * row + tab <= kGSRingBytes ? 4 : 2);
+    p.smem = p.d * row + tab;
     return p;
+}
+
+template <typename T, int D, int CS>
+void gs_launch(vvm_gpu_ctx* c, const GSArgs<T>& g, const GSPlan& p) {
+    LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_cluster<T, kGSPer, D, CS><<<5 * CS, 32 * p.w, p.smem, c->stream>>>(g));
+}
+
+template <typename T, int D>
+void gs_launch_d(vvm_gpu_ctx* c, const GSArgs<T>& g, const GSPlan& p) {
+    if (p.cs == 8) gs_launch<T, D, 8>(c, g, p);
+    else if (p.cs == 4) gs_launch<T, D, 4>(c, g, p);
+    else if (p.cs == 2) gs_launch<T, D, 2>(c, g, p);
+    else gs_launch<T, D, 1>(c, g, p);
+}
+
+template <typename T, int D>
+void gs_set_smem_d() {
+    const int mx = (int)kGSRingBytes;
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
 }
 
 template <typename T>
 void gs_set_smem() {
-    const int mx = (int)kGSRingBytes;
-    CK(cudaFuncSetAttribute(k_gs_scan_async<T, 8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(k_gs_scan_async<T, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(k_gs_scan_async<T, 16, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    gs_set_smem_d<T, 8>();
+    gs_set_smem_d<T, 4>();
+    gs_set_smem_d<T, 2>();
 }
 
 template <typename T>
@@ -1153,23 +1178,16 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
     LAUNCH(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r));
     CKL();
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
-                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, F.gsC, F.gsB};
-    const int NX = c->d.nx - 2, pitch = c->d.pitch;
+                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, F.gsC, F.gsB, c->d_err};
+    const int pitch = c->d.pitch;
     dim3 cb(64, 4), cg(cdiv(pitch, 64), cdiv(c->d.nz - 2, 4), 5);
     LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_coeffs<T><<<cg, cb, 0, c->stream>>>(g));
     CKL();
-    // One block per field, PER cells a thread, coefficient rows staged in
-    // shared memory D rows ahead; when even two rows do not fit, the
-    // register-prefetch variant.
-    const GSPlan p = gs_plan(pitch, sizeof(T));
-    if (p.D == 4 && p.per == 8)
-        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan_async<T, 8, 4><<<5, p.threads, p.smem, c->stream>>>(g));
-    else if (p.D == 2 && p.per == 8)
-        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan_async<T, 8, 2><<<5, p.threads, p.smem, c->stream>>>(g));
-    else if (p.D == 2 && p.per == 16)
-        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan_async<T, 16, 2><<<5, p.threads, p.smem, c->stream>>>(g));
-    else
-        LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_scan<T, 8, kGSWideRing<T>, 1024><<<5, round_up(cdiv(NX, 8), 32), 0, c->stream>>>(g));
+    // the recurrence: one cluster per field (see k_gs_cluster)
+    const GSPlan p = gs_plan(pitch, c->d.nz, sizeof(T));
+    if (p.d == 8) gs_launch_d<T, 8>(c, g, p);
+    else if (p.d == 4) gs_launch_d<T, 4>(c, g, p);
+    else gs_launch_d<T, 2>(c, g, p);
     CKL();
 }
 
@@ -1783,6 +1801,16 @@ int need_state(vvm_gpu_ctx* c) {
     return c->has_state ? VVM_GPU_OK : fail(c, VVM_GPU_ESTATE, "no state uploaded");
 }
 
+// Reads and clears the device error word (after the stream's work is done).
+int device_errors(vvm_gpu_ctx* c) {
+    if (!c->d_err) return VVM_GPU_OK;
+    int h = 0;
+    CK(cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!h) return VVM_GPU_OK;
+    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    return fail(c, VVM_GPU_ECUDA, "Gauss-Seidel diffusion: a wait between warps gave up; the state is invalid");
+}
+
 }  // namespace
 
 // Message of a failed context-free entry, returned by vvm_gpu_last_error(NULL, ...).
@@ -1820,7 +1848,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     *out = nullptr;
     const vvm_gpu_desc& D = *desc;
     if (D.NX < 4 || D.NZ < 4) return fail(nullptr, VVM_GPU_EINVAL, "create: NX and NZ must be >= 4");
-    if (D.NX > kGSMaxThreads * kGSMaxPerThread)
+    if (D.NX > kGSMaxNX || gs_plan(round_up(D.NX + 2, kPad), D.NZ + 2, 8).w > kGSClusterWarps)
         return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
     if (D.NZ - 1 > 32 * kMaxSeg)
         return fail(nullptr, VVM_GPU_EINVAL, "create: NZ exceeds 1025");
@@ -1890,6 +1918,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         c->staging = c->ar.alloc<double>((size_t)c->d.nx * c->d.nz * 2);
         c->wctl = c->ar.alloc<CGCtl>(1);
         c->d_exec = c->ar.alloc<long long>(1);
+        c->d_err = c->ar.alloc<int>(1);
         for (auto& cs : c->cap) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     } catch (const CudaError& e) {
         cudaSetDevice(prev);
@@ -1918,7 +1947,10 @@ int vvm_gpu_set_stream(vvm_gpu_ctx* ctx, void* stream) {
 }
 
 int vvm_gpu_synchronize(vvm_gpu_ctx* ctx) {
-    return guarded(ctx, [&] { CK(cudaStreamSynchronize(ctx->stream)); return VVM_GPU_OK; });
+    return guarded(ctx, [&] {
+        CK(cudaStreamSynchronize(ctx->stream));
+        return device_errors(ctx);
+    });
 }
 
 int vvm_gpu_last_error(vvm_gpu_ctx* ctx, char* buf, size_t len) {
@@ -1949,7 +1981,11 @@ int vvm_gpu_upload_state(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st) {
 
 int vvm_gpu_download_state(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
     if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
-    return guarded(ctx, [&] { return need_state(ctx) ? need_state(ctx) : DISPATCH(ctx, download_state_t)(ctx, st); });
+    return guarded(ctx, [&] {
+        if (int rc = need_state(ctx)) return rc;
+        if (int rc = DISPATCH(ctx, download_state_t)(ctx, st)) return rc;
+        return device_errors(ctx);
+    });
 }
 
 int vvm_gpu_upload_prognostic(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st) {
@@ -1959,7 +1995,11 @@ int vvm_gpu_upload_prognostic(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st) {
 
 int vvm_gpu_download_prognostic(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
     if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
-    return guarded(ctx, [&] { return need_state(ctx) ? need_state(ctx) : DISPATCH(ctx, download_prognostic_t)(ctx, st); });
+    return guarded(ctx, [&] {
+        if (int rc = need_state(ctx)) return rc;
+        if (int rc = DISPATCH(ctx, download_prognostic_t)(ctx, st)) return rc;
+        return device_errors(ctx);
+    });
 }
 
 int vvm_gpu_set_step(vvm_gpu_ctx* ctx, int step) {
