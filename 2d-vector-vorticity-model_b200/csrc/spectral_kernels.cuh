@@ -7,9 +7,10 @@
 //   (cx_k mu_m + ru_k + rd_k) w_k - ru_k w_{k+1} - rd_k w_{k-1} = f_k,
 //   mu_m = 2 - 2 cos(2 pi m / NX),
 // a real tridiagonal system in z per mode. S^{-1} r is then: a forward FFT of
-// every row, one Thomas solve per mode (real and imaginary parts alike), and
-// an inverse FFT. In PCG this preconditioner is S^{-1} up to round-off, so
-// one iteration reaches the FP64 residual floor. NX must be a power of two.
+// every row, one tridiagonal solve per mode (real and imaginary parts alike),
+// and an inverse FFT. It is S^{-1} up to round-off: the solver applies it to
+// the right-hand side directly and checks the FP64 residual, with CG
+// iterations only if that check fails. NX must be a power of two.
 //
 // Row transforms run in shared memory, one block per pair of rows: the two
 // real rows are the real and imaginary parts of one complex row, whose FFT
@@ -24,12 +25,20 @@
 
 namespace vvm {
 
+// The z solve of each mode uses the twisted (two-sided) factorisation: rows
+// 0..mid are eliminated downwards (y_k = (f_k + rd_k y_{k-1}) inv_k, leaving
+// w_k + cp_k w_{k+1} = y_k), rows NK-1..mid+1 upwards (z_k = (f_k + ru_k
+// z_{k+1}) inv_k, leaving w_k + cp_k w_{k-1} = z_k); the two middle rows give
+// w_mid = (y_mid - cp_mid z_{mid+1}) den and w_{mid+1} = z_{mid+1} -
+// cp_{mid+1} w_mid, den = 1 / (1 - cp_mid cp_{mid+1}); both halves then
+// back-substitute outwards. inv and cp hold the factors of each row's half.
 template <typename P>
 struct SpecArgs {
-    int NX, logN, NK, pitch, mpitch;
+    int NX, logN, NK, pitch, mpitch, mid;
     const P *twr, *twi;      // exp(-2 pi i j / NX), j < NX/2
-    const P *inv, *cp;       // per-mode Thomas factors, [NK][mpitch]
-    const P* rd;             // lower coupling of each row, [NK]
+    const P *inv, *cp;       // per-mode factors, [NK][mpitch]
+    const P* den;            // per-mode meeting factor, [mpitch]
+    const P *rd, *ru;        // couplings of each row to the rows below / above, [NK]
     P *sre, *sim;            // spectra, [NK][mpitch]
 };
 
@@ -90,58 +99,89 @@ __global__ void k_spec_forward(SpecArgs<P> a, const P* r) {
     }
 }
 
-// The z solve of every mode m = 0..NX/2 in place on the spectra (one thread
-// per mode; real and imaginary parts share the factors). The recurrence is
+// The z solve of every mode m = 0..NX/2 in place on the spectra: two adjacent
+// threads per mode, the even one for the rows 0..mid, the odd one for
+// mid+1..NK-1 (real and imaginary parts share the factors). Each chain is
 // serial in k, so rows are taken kModeBatch at a time: the batch's loads are
-// issued together and the chain then runs from registers, one memory round
-// trip per batch instead of one per row.
+// issued together and the chain then runs from registers.
 constexpr int kModeBatch = 16;
 
 template <typename P>
 __global__ void __launch_bounds__(64) k_spec_modes(SpecArgs<P> a) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m > a.NX / 2) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = t >> 1, half = t & 1;
+    const bool on = m <= a.NX / 2;          // the pair is inactive together (m is shared)
     const size_t mp = a.mpitch;
     P* __restrict__ sre = a.sre;
     P* __restrict__ sim = a.sim;
     const P* __restrict__ inv = a.inv;
     const P* __restrict__ cpv = a.cp;
-    const P* __restrict__ rdv = a.rd;
-    const int NK = a.NK;
+    const int NK = a.NK, mid = a.mid;
+    // this half's rows in elimination order: k = k0 + dir * j, j < n
+    const int dir = half ? -1 : 1;
+    const int k0 = half ? NK - 1 : 0;
+    const int n = half ? NK - 1 - mid : mid + 1;
+    const P* __restrict__ lc = half ? a.ru : a.rd;   // coupling to the previously eliminated row
     P yr = P(0), yi = P(0);
-    for (int k0 = 0; k0 < NK; k0 += kModeBatch) {
-        P fr[kModeBatch], fi[kModeBatch], iv[kModeBatch], rd[kModeBatch];
+    if (on) {
+        for (int j0 = 0; j0 < n; j0 += kModeBatch) {
+            P fr[kModeBatch], fi[kModeBatch], iv[kModeBatch], cl[kModeBatch];
 #pragma unroll
-        for (int j = 0; j < kModeBatch; j++) {
-            const int kk = k0 + j;
-            if (kk < NK) {
-                const size_t e = (size_t)kk * mp + m;
-                fr[j] = sre[e];
-                fi[j] = sim[e];
-                iv[j] = inv[e];
-                rd[j] = rdv[kk];
+            for (int j = 0; j < kModeBatch; j++) {
+                if (j0 + j < n) {
+                    const int kk = k0 + dir * (j0 + j);
+                    const size_t e = (size_t)kk * mp + m;
+                    fr[j] = sre[e];
+                    fi[j] = sim[e];
+                    iv[j] = inv[e];
+                    cl[j] = lc[kk];
+                }
             }
-        }
 #pragma unroll
-        for (int j = 0; j < kModeBatch; j++) {
-            const int kk = k0 + j;
-            if (kk < NK) {
-                yr = (fr[j] + rd[j] * yr) * iv[j];
-                yi = (fi[j] + rd[j] * yi) * iv[j];
-                const size_t e = (size_t)kk * mp + m;
-                sre[e] = yr;
-                sim[e] = yi;
+            for (int j = 0; j < kModeBatch; j++) {
+                if (j0 + j < n) {
+                    const int kk = k0 + dir * (j0 + j);
+                    yr = (fr[j] + cl[j] * yr) * iv[j];
+                    yi = (fi[j] + cl[j] * yi) * iv[j];
+                    const size_t e = (size_t)kk * mp + m;
+                    sre[e] = yr;
+                    sim[e] = yi;
+                }
             }
         }
     }
-    // yr, yi hold row NK-1, which is final; back-substitute rows NK-2 .. 0
-    for (int k1 = NK - 2; k1 >= 0; k1 -= kModeBatch) {
+    // meeting rows: the even lane holds y_mid, the odd lane z_{mid+1}
+    const int klast = k0 + dir * (n - 1);
+    const P clast = on ? cpv[(size_t)klast * mp + m] : P(0);
+    const P orr = __shfl_xor_sync(0xffffffffu, yr, 1);
+    const P oi = __shfl_xor_sync(0xffffffffu, yi, 1);
+    const P oc = __shfl_xor_sync(0xffffffffu, clast, 1);
+    if (!on) return;
+    const P dn = a.den[m];
+    P ymr, ymi, zr, zi, cpm, cqm;
+    if (half == 0) {
+        ymr = yr; ymi = yi; cpm = clast; zr = orr; zi = oi; cqm = oc;
+    } else {
+        ymr = orr; ymi = oi; cpm = oc; zr = yr; zi = yi; cqm = clast;
+    }
+    const P wpr = (ymr - cpm * zr) * dn, wpi = (ymi - cpm * zi) * dn;      // w_mid
+    if (half == 0) {
+        yr = wpr;
+        yi = wpi;
+    } else {
+        yr = zr - cqm * wpr;                                                  // w_{mid+1}
+        yi = zi - cqm * wpi;
+    }
+    sre[(size_t)klast * mp + m] = yr;
+    sim[(size_t)klast * mp + m] = yi;
+    // back-substitute outwards: w_k = y_k - cp_k w_next over this half's
+    // remaining rows, nearest the middle first
+    for (int j0 = n - 2; j0 >= 0; j0 -= kModeBatch) {
         P fr[kModeBatch], fi[kModeBatch], c[kModeBatch];
 #pragma unroll
         for (int j = 0; j < kModeBatch; j++) {
-            const int kk = k1 - j;
-            if (kk >= 0) {
-                const size_t e = (size_t)kk * mp + m;
+            if (j0 - j >= 0) {
+                const size_t e = (size_t)(k0 + dir * (j0 - j)) * mp + m;
                 fr[j] = sre[e];
                 fi[j] = sim[e];
                 c[j] = cpv[e];
@@ -149,11 +189,10 @@ __global__ void __launch_bounds__(64) k_spec_modes(SpecArgs<P> a) {
         }
 #pragma unroll
         for (int j = 0; j < kModeBatch; j++) {
-            const int kk = k1 - j;
-            if (kk >= 0) {
+            if (j0 - j >= 0) {
                 yr = fr[j] - c[j] * yr;
                 yi = fi[j] - c[j] * yi;
-                const size_t e = (size_t)kk * mp + m;
+                const size_t e = (size_t)(k0 + dir * (j0 - j)) * mp + m;
                 sre[e] = yr;
                 sim[e] = yi;
             }

@@ -207,61 +207,74 @@ struct PAdvArgs {
     AB2 ab;
 };
 
-// x flux at face (i-1/2, k), i = 1..nx-2 (Advection.cpp:36,40-44).
+// The velocity part of one face's flux, shared by every advected field:
+// flux = base (v0 + vm) - 1/3 (c1 (v0 - vm) - c2 (vm - vmm) - c3 (v0 - vm)
+// - c4 (vp - v0)), the bracket only away from the boundaries (hi = 0 there).
+// Each coefficient is formed exactly as the per-field expressions of
+// Advection.cpp:40-50 form it.
 template <typename T>
-__device__ __forceinline__ T scal_flux_u(const PAdvArgs<T>& a, const T* v, int i, int k) {
+struct Face {
+    T base, c1, c2, c3, c4;
+    bool hi;
+};
+
+// x face (i-1/2, k), i = 1..nx-2 (Advection.cpp:36,40-44).
+template <typename T>
+__device__ __forceinline__ Face<T> face_u(const PAdvArgs<T>& a, int i, int k) {
     const Dims& d = a.d;
-    T ru = T(a.p.rhou[k]);
-    T ui = a.u[d.at(i, k)];
-    T v0 = v[d.at(i, k)], vm = v[d.at(i - 1, k)];
-    T f = ru * ui * (v0 + vm);
-    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
-        T um = a.u[d.at(i - 1, k)], up = a.u[d.at(i + 1, k)];
-        T vmm = v[d.at(i - 2, k)], vp = v[d.at(i + 1, k)];
-        f += T(-1. / 3.) * (ru * plus_part(ui) * (v0 - vm) -
-                            sqrt(ru * plus_part(ui) * ru * plus_part(um)) * (vm - vmm) -
-                            ru * minus_part(ui) * (v0 - vm) -
-                            sqrt(fabs(ru * minus_part(ui) * ru * minus_part(up))) * (vp - v0));
+    Face<T> F;
+    const T ru = T(a.p.rhou[k]);
+    const T ui = a.u[d.at(i, k)];
+    F.base = ru * ui;
+    F.hi = (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3);
+    F.c1 = F.c2 = F.c3 = F.c4 = T(0);
+    if (F.hi) {
+        const T um = a.u[d.at(i - 1, k)], up = a.u[d.at(i + 1, k)];
+        F.c1 = ru * plus_part(ui);
+        F.c2 = sqrt(ru * plus_part(ui) * ru * plus_part(um));
+        F.c3 = ru * minus_part(ui);
+        F.c4 = sqrt(fabs(ru * minus_part(ui) * ru * minus_part(up)));
     }
+    return F;
+}
+
+// z face (i, k-1/2), k = 1..nz-2 (Advection.cpp:37,46-50).
+template <typename T>
+__device__ __forceinline__ Face<T> face_w(const PAdvArgs<T>& a, int i, int k) {
+    const Dims& d = a.d;
+    Face<T> F;
+    const T rk = T(a.p.rhow[k]);
+    const T wk = a.w[d.at(i, k)];
+    F.base = rk * wk;
+    F.hi = (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3);
+    F.c1 = F.c2 = F.c3 = F.c4 = T(0);
+    if (F.hi) {
+        const T rkm = T(a.p.rhow[k - 1]), rkp = T(a.p.rhow[k + 1]);
+        const T wm = a.w[d.at(i, k - 1)], wp = a.w[d.at(i, k + 1)];
+        F.c1 = rk * plus_part(wk);
+        F.c2 = sqrt(rk * plus_part(wk) * rkm * plus_part(wm));
+        F.c3 = rk * minus_part(wk);
+        F.c4 = sqrt(fabs(rk * minus_part(wk) * rkp * minus_part(wp)));
+    }
+    return F;
+}
+
+// Flux through a face from the field values vmm, vm | v0, vp across it.
+template <typename T>
+__device__ __forceinline__ T face_flux(const Face<T>& F, T vmm, T vm, T v0, T vp) {
+    T f = F.base * (v0 + vm);
+    if (F.hi) f += T(-1. / 3.) * (F.c1 * (v0 - vm) - F.c2 * (vm - vmm) - F.c3 * (v0 - vm) - F.c4 * (vp - v0));
     return f;
 }
 
-// z flux at face (i, k-1/2), k = 1..nz-2 (Advection.cpp:37,46-50).
+// The same with the third-order differences of a perturbation v' about a
+// profile: dk = (v0 - vm) + d0[k] etc. (mixed step, z faces of th and qv).
 template <typename T>
-__device__ __forceinline__ T scal_flux_w(const PAdvArgs<T>& a, const T* v, int i, int k) {
-    const Dims& d = a.d;
-    T rk = T(a.p.rhow[k]);
-    T wk = a.w[d.at(i, k)];
-    T v0 = v[d.at(i, k)], vm = v[d.at(i, k - 1)];
-    T f = rk * wk * (v0 + vm);
-    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
-        T rkm = T(a.p.rhow[k - 1]), rkp = T(a.p.rhow[k + 1]);
-        T wm = a.w[d.at(i, k - 1)], wp = a.w[d.at(i, k + 1)];
-        T vmm = v[d.at(i, k - 2)], vp = v[d.at(i, k + 1)];
-        f += T(-1. / 3.) * (rk * plus_part(wk) * (v0 - vm) -
-                            sqrt(rk * plus_part(wk) * rkm * plus_part(wm)) * (vm - vmm) -
-                            rk * minus_part(wk) * (v0 - vm) -
-                            sqrt(fabs(rk * minus_part(wk) * rkp * minus_part(wp))) * (vp - v0));
-    }
-    return f;
-}
-
-// z flux of a perturbation v' about profile v0 (mixed step): the main term
-// carries v' only, the 3rd-order differences add d0[k] = v0[k] - v0[k-1].
-template <typename T>
-__device__ __forceinline__ T scal_flux_w_pert(const PAdvArgs<T>& a, const T* v, const double* d0, int i, int k) {
-    const Dims& d = a.d;
-    T rk = T(a.p.rhow[k]);
-    T wk = a.w[d.at(i, k)];
-    T v0 = v[d.at(i, k)], vm = v[d.at(i, k - 1)];
-    T f = rk * wk * (v0 + vm);
-    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
-        T rkm = T(a.p.rhow[k - 1]), rkp = T(a.p.rhow[k + 1]);
-        T wm = a.w[d.at(i, k - 1)], wp = a.w[d.at(i, k + 1)];
-        T vmm = v[d.at(i, k - 2)], vp = v[d.at(i, k + 1)];
-        T dk = (v0 - vm) + T(d0[k]), dkm = (vm - vmm) + T(d0[k - 1]), dkp = (vp - v0) + T(d0[k + 1]);
-        f += T(-1. / 3.) * (rk * plus_part(wk) * dk - sqrt(rk * plus_part(wk) * rkm * plus_part(wm)) * dkm -
-                            rk * minus_part(wk) * dk - sqrt(fabs(rk * minus_part(wk) * rkp * minus_part(wp))) * dkp);
+__device__ __forceinline__ T face_flux_pert(const Face<T>& F, T vmm, T vm, T v0, T vp, T dkm0, T dk0, T dkp0) {
+    T f = F.base * (v0 + vm);
+    if (F.hi) {
+        const T dk = (v0 - vm) + dk0, dkm = (vm - vmm) + dkm0, dkp = (vp - v0) + dkp0;
+        f += T(-1. / 3.) * (F.c1 * dk - F.c2 * dkm - F.c3 * dk - F.c4 * dkp);
     }
     return f;
 }
@@ -286,18 +299,32 @@ __global__ void k_padv(PAdvArgs<T> a) {
         const size_t id = d.at(i, k);
         const T dt15 = T(1.5 * a.c.dt), dt05 = T(0.5 * a.c.dt);
         const T ru = T(a.p.rhou[k]);
+        // velocity parts of the four faces, shared by the four fields;
+        // flux_u at nx-1 is the halo copy of flux_u at 1, flux_w at nz-1 is
+        // zeroed (Advection.cpp:55-58)
+        const int ip = (i == d.nx - 2) ? 1 : i + 1;
+        const Face<T> Fu0 = face_u(a, i, k), Fup = face_u(a, ip, k);
+        const Face<T> Fw0 = face_w(a, i, k);
+        const bool top = (k == d.nz - 2);
+        Face<T> Fwp = Fw0;
+        if (!top) Fwp = face_w(a, i, k + 1);
+        auto X = [&](const T* v, int ii, int kk) { return v[d.at(ii, kk)]; };
         for (int f = 0; f < 4; f++) {
             if (!(a.mask & (1 << f))) continue;
             const T* v = a.now[f];
-            // flux_u at nx-1 is the halo copy of flux_u at 1; flux_w at nz-1
-            // is zeroed (Advection.cpp:55-58).
-            const int ip = (i == d.nx - 2) ? 1 : i + 1;
-            T fu_p = scal_flux_u(a, v, ip, k);
-            T fu_0 = scal_flux_u(a, v, i, k);
+            // x faces i-1/2 and ip-1/2, z faces k-1/2 and k+1/2 (third-order
+            // neighbours read only where the bracket applies)
+            T fu_0 = face_flux(Fu0, Fu0.hi ? X(v, i - 2, k) : T(0), X(v, i - 1, k), X(v, i, k),
+                               Fu0.hi ? X(v, i + 1, k) : T(0));
+            T fu_p = face_flux(Fup, Fup.hi ? X(v, ip - 2, k) : T(0), X(v, ip - 1, k), X(v, ip, k),
+                               Fup.hi ? X(v, ip + 1, k) : T(0));
             T px, pz;
             if (!kPert<T> || f >= 2) {
-                T fw_p = (k == d.nz - 2) ? T(0) : scal_flux_w(a, v, i, k + 1);
-                T fw_0 = scal_flux_w(a, v, i, k);
+                T fw_0 = face_flux(Fw0, Fw0.hi ? X(v, i, k - 2) : T(0), X(v, i, k - 1), X(v, i, k),
+                                   Fw0.hi ? X(v, i, k + 1) : T(0));
+                T fw_p = top ? T(0)
+                             : face_flux(Fwp, Fwp.hi ? X(v, i, k - 1) : T(0), X(v, i, k), X(v, i, k + 1),
+                                         Fwp.hi ? X(v, i, k + 2) : T(0));
                 px = (fu_p - fu_0) * T(a.c.r2dx) / ru;
                 pz = (fw_p - fw_0) * T(a.c.r2dz) / ru;
             } else {
@@ -305,12 +332,18 @@ __global__ void k_padv(PAdvArgs<T> a) {
                 // difference form, 2 v0 (u[i+1] - u[i]) in x and
                 // s0[k+1] (m[k+1] - m[k]) + m[k] g0[k] in z, m = rhow w.
                 const double* d0 = a.p.d0[f];
-                T fw_p = (k == d.nz - 2) ? T(0) : scal_flux_w_pert(a, v, d0, i, k + 1);
-                T fw_0 = scal_flux_w_pert(a, v, d0, i, k);
+                T fw_0 = Fw0.hi ? face_flux_pert(Fw0, X(v, i, k - 2), X(v, i, k - 1), X(v, i, k), X(v, i, k + 1),
+                                                 T(d0[k - 1]), T(d0[k]), T(d0[k + 1]))
+                                : face_flux(Fw0, T(0), X(v, i, k - 1), X(v, i, k), T(0));
+                T fw_p = T(0);
+                if (!top)
+                    fw_p = Fwp.hi ? face_flux_pert(Fwp, X(v, i, k - 1), X(v, i, k), X(v, i, k + 1), X(v, i, k + 2),
+                                                   T(d0[k]), T(d0[k + 1]), T(d0[k + 2]))
+                                  : face_flux(Fwp, T(0), X(v, i, k), X(v, i, k + 1), T(0));
                 T m0 = T(a.p.rhow[k]) * a.w[d.at(i, k)];
-                T refz = (k == d.nz - 2) ? -m0 * T(a.p.s0[f][k])
-                                         : T(a.p.s0[f][k + 1]) * (T(a.p.rhow[k + 1]) * a.w[d.at(i, k + 1)] - m0) +
-                                               m0 * T(a.p.g0[f][k]);
+                T refz = top ? -m0 * T(a.p.s0[f][k])
+                             : T(a.p.s0[f][k + 1]) * (T(a.p.rhow[k + 1]) * a.w[d.at(i, k + 1)] - m0) +
+                                   m0 * T(a.p.g0[f][k]);
                 T refx = T(2.0 * a.p.ref[f][k]) * (a.u[d.at(ip, k)] - a.u[d.at(i, k)]);
                 px = (fu_p - fu_0) * T(a.c.r2dx) / ru + refx * T(a.c.r2dx);
                 pz = (fw_p - fw_0 + refz) * T(a.c.r2dz) / ru;

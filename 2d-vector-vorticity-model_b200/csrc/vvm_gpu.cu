@@ -679,27 +679,41 @@ struct Spectral {
             twr[j] = std::cos(2.0 * pi * j / NX);
             twi[j] = -std::sin(2.0 * pi * j / NX);
         }
-        std::vector<double> inv((size_t)NK * mp, 0.0), cp((size_t)NK * mp, 0.0);
+        // twisted factorisation of each mode's z operator (spectral_kernels.cuh):
+        // rows 0..mid eliminated downwards, mid+1..NK-1 upwards
+        const int mid = (NK - 1) / 2;
+        std::vector<double> inv((size_t)NK * mp, 0.0), cp((size_t)NK * mp, 0.0), den(mp, 0.0);
         for (int m = 0; m < M; m++) {
             const double mu = 2.0 - 2.0 * std::cos(2.0 * pi * m / NX);
             double up_over_piv = 0.0;   // ru_{k-1} / piv_{k-1}
-            for (int k = 0; k < NK; k++) {
+            for (int k = 0; k <= mid; k++) {
                 const double piv = cx0[k] * mu + ru[k] + rd[k] - (k > 0 ? rd[k] * up_over_piv : 0.0);
                 inv[(size_t)k * mp + m] = 1.0 / piv;
-                cp[(size_t)k * mp + m] = (k + 1 < NK) ? -ru[k] / piv : 0.0;
+                cp[(size_t)k * mp + m] = -ru[k] / piv;
                 up_over_piv = ru[k] / piv;
             }
+            double dn_over_piv = 0.0;   // rd_{k+1} / piv_{k+1}
+            for (int k = NK - 1; k > mid; k--) {
+                const double piv = cx0[k] * mu + ru[k] + rd[k] - (k + 1 < NK ? ru[k] * dn_over_piv : 0.0);
+                inv[(size_t)k * mp + m] = 1.0 / piv;
+                cp[(size_t)k * mp + m] = -rd[k] / piv;
+                dn_over_piv = rd[k] / piv;
+            }
+            den[m] = 1.0 / (1.0 - cp[(size_t)mid * mp + m] * cp[(size_t)(mid + 1) * mp + m]);
         }
         a.NX = NX;
         a.logN = logN;
         a.NK = NK;
         a.pitch = pitch;
         a.mpitch = mp;
+        a.mid = mid;
         a.twr = upload(ar, twr);
         a.twi = upload(ar, twi);
         a.inv = upload(ar, inv);
         a.cp = upload(ar, cp);
+        a.den = upload(ar, den);
         a.rd = upload(ar, rd);
+        a.ru = upload(ar, ru);
         a.sre = ar.alloc<P>((size_t)NK * mp);
         a.sim = ar.alloc<P>((size_t)NK * mp);
         out = ar.alloc<P>((size_t)NK * pitch);
@@ -709,15 +723,19 @@ struct Spectral {
         CK(cudaFuncSetAttribute(k_spec_inverse<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
 
-    // z = S^{-1} r (to round-off); returns the buffer holding z.
-    P* apply(const P* r, cudaStream_t st) {
+    // dst = S^{-1} r (to round-off).
+    void apply_to(const P* r, P* dst, cudaStream_t st) {
         const int rows2 = cdiv(a.NK, 2);
         LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_forward<P><<<rows2, threads, smem, st>>>(a, r));
         CKL();
-        LAUNCH(stats, VVM_K_MG_COARSE, st, k_spec_modes<P><<<cdiv(a.NX / 2 + 1, 64), 64, 0, st>>>(a));
+        LAUNCH(stats, VVM_K_MG_COARSE, st, k_spec_modes<P><<<cdiv(2 * (a.NX / 2 + 1), 64), 64, 0, st>>>(a));
         CKL();
-        LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_inverse<P><<<rows2, threads, smem, st>>>(a, out));
+        LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_inverse<P><<<rows2, threads, smem, st>>>(a, dst));
         CKL();
+    }
+    // z = S^{-1} r; returns the buffer holding z.
+    P* apply(const P* r, cudaStream_t st) {
+        apply_to(r, out, st);
         return out;
     }
 };
@@ -1257,7 +1275,15 @@ int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
         c->last_relres = 0.0;
         return VVM_GPU_OK;
     }
-    if (!c->mixed || c->spectral) {   // exact preconditioner: FP64 CG needs one iteration
+    if (c->spectral) {   // direct solve W = S^{-1} f, checked; CG from there if the check fails
+        double rel = 0;
+        c->pcg64->sp.apply_to(c->Wf, c->W, c->stream);
+        int it = c->pcg64->solve(c->Wf, c->W, true, bb, tol, maxit, c->stream, &rel);
+        c->last_iters = it;
+        c->last_relres = rel;
+        return (rel <= tol) ? VVM_GPU_OK : VVM_GPU_ENOCONV;
+    }
+    if (!c->mixed) {
         double rel = 0;
         int it = c->pcg64->solve(c->Wf, c->W, warm, bb, tol, maxit, c->stream, &rel);
         c->last_iters = it;
@@ -1346,7 +1372,8 @@ long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
     VecArgs<double> v = P64.vargs();
     const long long n_start = c->stats.launches;
     long long in_bodies = 0;
-    if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
+    if (c->spectral) P64.sp.apply_to(c->Wf, c->W, st);   // direct solve; the loop below checks it
+    else if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
     LAUNCH(&c->stats, VVM_K_CG, st, k_zero_if_b0<<<G, B, 0, st>>>(P64.NX, P64.NK, P64.pitch, P64.sc, c->W));
     CKL();
     if (!c->mixed || c->spectral) {
@@ -1433,7 +1460,7 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     const bool warm = c->desc.warm_start != 0;
     const int maxit = c->desc.poisson_maxit > 0 ? c->desc.poisson_maxit : 200;
     if (recorded_in_loops) {   // graph capture: the loops run on the device
-        if (warm) {
+        if (warm && !c->spectral) {
             LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_extrapolate<<<G, B, 0, c->stream>>>(NX, NK, pitch, c->W, c->Wprev));
             CKL();
         }
@@ -1446,7 +1473,7 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     CK(cudaMemcpyAsync(c->sc_host, &c->pcg64->sc->bb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     double bb = *c->sc_host;
-    if (warm) {
+    if (warm && !c->spectral) {
         // the previous solution(s) as the initial guess: linear extrapolation
         // once two exist (the reference starts every solve from zero)
         if (c->nsolves >= 2) {

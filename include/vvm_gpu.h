@@ -51,10 +51,12 @@ extern "C" {
 #define VVM_SOLVER_MGPCG 0    /* geometric multigrid: x-semicoarsening, z-line relaxation */
 #define VVM_SOLVER_LEARNED 1  /* learned BF16 conv preconditioner in flexible CG,
                                  multigrid-PCG as fallback */
-#define VVM_SOLVER_SPECTRAL 2 /* FP64 CG preconditioned by the exact Fourier-mode
-                                 solve (row FFTs in x, one tridiagonal z solve per
-                                 mode); NX a power of two; the FP64 CG also serves
-                                 VVM_PREC_MIXED (one iteration reaches 1e-14) */
+#define VVM_SOLVER_SPECTRAL 2 /* exact Fourier-mode solve (row FFTs in x, one
+                                 tridiagonal z solve per mode) applied directly in
+                                 FP64, its residual checked, FP64 CG preconditioned
+                                 by it only if the check fails (the iterations
+                                 vvm_gpu_last_solve reports); NX a power of two;
+                                 serves VVM_PREC_MIXED as well */
 
 /* Model description; mirrors Config_VVM (src/Declare.hpp:27-70) and the
  * constants main.cpp passes (src/main.cpp:68-72). */

@@ -1,8 +1,9 @@
-"""The Fourier-mode preconditioned solver (VVM_SOLVER_SPECTRAL) against the
-reference and against the multigrid-PCG path.
+"""The Fourier-mode solver (VVM_SOLVER_SPECTRAL) against the reference and
+against the multigrid-PCG path.
 
-Its preconditioner is the exact inverse of the cal_w operator up to
-round-off, so CG stops after one or two iterations at the FP64 floor. The
+The Fourier-mode solve is the exact inverse of the cal_w operator up to
+round-off: it is applied directly and its FP64 residual checked, so no CG
+iteration normally follows (last_solve reports those iterations). The
 reference comparisons use the same relative-L2 tolerances as the multigrid
 path (tests/test_gpu_step.py).
 """
@@ -41,7 +42,7 @@ def test_spectral_poisson_manufactured_solution(gpu):
     g = gpu.VVMGpu(st.grid, warm_start=False, solver=gpu.VVM_SOLVER_SPECTRAL)
     g.upload(st)
     W, it, rel = g.poisson_solve(z["b"], tol=1e-10)
-    assert rel <= 1e-13 and 1 <= it <= 2, (it, rel)
+    assert rel <= 1e-13 and it <= 1, (it, rel)   # CG iterations after the direct solve
     m = PortModel(st.grid)
     m.load(st)
     assert rel_l2(m.apply_A(W), z["b"]) <= 1e-13
