@@ -3,6 +3,7 @@
 // Host code: device memory of one context, coefficient profiles formed with
 // the reference's expressions, the multigrid-preconditioned CG of cal_w, and
 // the launch sequence of one step (src/Iteration.cpp:262-434).
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -267,12 +268,15 @@ inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 // Owns device allocations of one context.
 struct Arena {
     std::vector<void*> ptrs;
+    std::vector<size_t> bytes;
     template <typename X>
     X* alloc(size_t n) {
         void* p = nullptr;
-        CK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(X)));
-        CK(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(X)));
+        const size_t nb = std::max<size_t>(n, 1) * sizeof(X);
+        CK(cudaMalloc(&p, nb));
+        CK(cudaMemset(p, 0, nb));
         ptrs.push_back(p);
+        bytes.push_back(nb);
         return static_cast<X*>(p);
     }
     ~Arena() {
@@ -288,6 +292,9 @@ struct Arena {
 // column count (at most kMaxOddCoarse) and gets 2*nc + 8 damped line sweeps.
 // Levels of at most 32 columns run inside one block (k_mg_coarse_cycle).
 constexpr int kMaxOddCoarse = 256;
+// Dynamic shared memory of the Fourier-mode coarse solve at most (f / solution
+// and the reduced-system bands, next to 32 KB of static tiles within 227 KB).
+constexpr int kModeSmemMax = 192 * 1024;
 
 // Launch counter and, when enabled, per-kernel-class device time from CUDA
 // events recorded around each launch on the launching stream.
@@ -510,7 +517,7 @@ struct Multigrid {
         // when its shared-memory tiles (f / solution and the reduced-system
         // bands, next to 32 KB of static tiles) fit in 227 KB
         for (int l = 0; l < nlev; l++) {
-            if (nx[l] <= 32 && ((size_t)NK + 10 * (size_t)S) * nx[l] * sizeof(P) <= 192 * 1024) {
+            if (nx[l] <= 32 && ((size_t)NK + 10 * (size_t)S) * nx[l] * sizeof(P) <= (size_t)kModeSmemMax) {
                 modes = true;
                 lc = l;
                 nlev = l + 1;   // coarser levels are not needed
@@ -583,7 +590,10 @@ struct Multigrid {
                        upload(ar, gL), upload(ar, gR), upload(ar, Mi)};
         mode_smem = ((size_t)NK * nc + (size_t)10 * S * nc) * sizeof(P);
         auto setattr = [&](auto kern) {
-            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mode_smem));
+            // the attribute is per kernel, not per context: set the largest any
+            // context may use (the fit test above), so contexts of other sizes
+            // in the same process never lower it under each other
+            CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kModeSmemMax));
         };
         if (LS == 8) setattr(k_coarse_modes<P, 8>);
         else if (LS == 16) setattr(k_coarse_modes<P, 16>);
@@ -719,8 +729,10 @@ struct Spectral {
         out = ar.alloc<P>((size_t)NK * pitch);
         smem = 2 * (size_t)NX * sizeof(P);
         threads = std::max(32, std::min(NX / 2, 512));
-        CK(cudaFuncSetAttribute(k_spec_forward<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CK(cudaFuncSetAttribute(k_spec_inverse<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // per-kernel attribute: the largest row any context may have (NX = 8192)
+        const int smax = 2 * 8192 * (int)sizeof(P);
+        CK(cudaFuncSetAttribute(k_spec_forward<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
+        CK(cudaFuncSetAttribute(k_spec_inverse<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
     }
 
     // dst = S^{-1} r (to round-off).
@@ -905,6 +917,8 @@ struct vvm_gpu_ctx {
     Consts c{};
     bool mixed = false;
     bool spectral = false;   // VVM_SOLVER_SPECTRAL
+    int tune_gs_cs = 0;      // cap on the CTAs of a Gauss-Seidel cluster (0: automatic)
+    int tune_fft = 0;        // threads of a row-FFT block (0: automatic)
     Arena ar;
     Fields<double> f64;
     Fields<float> f32;
@@ -1147,10 +1161,14 @@ struct GSPlan {
     int cs, w, d;
     size_t smem;
 };
-inline GSPlan gs_plan(int pitch, int nz, size_t elem) {
+// max_cs > 0 caps the CTAs of a cluster (the autotuner's knob); the cap
+// never goes below the size whose CTAs would need more than
+// kGSClusterWarps warps.
+inline GSPlan gs_plan(int pitch, int nz, size_t elem, int max_cs = 0) {
     GSPlan p{};
     const int gwn = cdiv(pitch, 32 * kGSPer);
     p.cs = gwn >= 8 ? 8 : (gwn >= 4 ? 4 : (gwn >= 2 ? 2 : 1));
+    while (max_cs > 0 && p.cs > max_cs && cdiv(gwn, p.cs / 2) <= kGSClusterWarps) p.cs /= 2;
     p.w = cdiv(gwn, p.cs);   // <= kGSClusterWarps for pitch <= 8224 (checked at create)
     const size_t row = 3 * (size_t)p.w * 32 * kGSPer * elem;
     const size_t tab = 2 * (size_t)nz * elem;   // nudging scalars
@@ -1202,7 +1220,7 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
     LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_coeffs<T><<<cg, cb, 0, c->stream>>>(g));
     CKL();
     // the recurrence: one cluster per field (see k_gs_cluster)
-    const GSPlan p = gs_plan(pitch, c->d.nz, sizeof(T));
+    const GSPlan p = gs_plan(pitch, c->d.nz, sizeof(T), c->tune_gs_cs);
     if (p.d == 8) gs_launch_d<T, 8>(c, g, p);
     else if (p.d == 4) gs_launch_d<T, 4>(c, g, p);
     else gs_launch_d<T, 2>(c, g, p);
@@ -1232,6 +1250,15 @@ void launch_update_mean(vvm_gpu_ctx* c, bool rotate) {
 
 // ---------------------------------------------------------------- Poisson
 
+// Applies the launch-shape knobs that live inside the solver objects.
+void apply_tuning(vvm_gpu_ctx* c) {
+    if (c->pcg64 && c->pcg64->spectral) {
+        const int half = std::max(32, (c->d.nx - 2) / 2);
+        const int def = std::min(half, 512);
+        c->pcg64->sp.threads = c->tune_fft > 0 ? std::max(32, std::min(c->tune_fft, std::min(half, 1024))) : def;
+    }
+}
+
 void ensure_poisson(vvm_gpu_ctx* c) {
     if (c->poisson_ready) return;
     c->drop_graphs();
@@ -1258,6 +1285,7 @@ void ensure_poisson(vvm_gpu_ctx* c) {
     c->wpartial = c->ar.alloc<double>(c->wnpart);
     if (!c->sc_host) CK(cudaMallocHost(&c->sc_host, sizeof(double)));
     c->poisson_ready = true;
+    apply_tuning(c);
 }
 
 double read_scalar(vvm_gpu_ctx* c, const double* dptr) {
@@ -1584,6 +1612,324 @@ int step_once(vvm_gpu_ctx* c) {
     c->nsolves++;
     c->last_graph = true;
     return VVM_GPU_OK;
+}
+
+// ---------------------------------------------------------------- snapshots
+
+// A device copy of every buffer of a context plus its host-side counters:
+// the autotuner runs real steps and puts the cases back exactly afterwards.
+struct Snapshot {
+    std::vector<void*> copies;
+    int step = 0, cur = 0, nsolves = 0, last_iters = 0;
+    double last_relres = 0;
+    long long launches = 0;
+    void take(vvm_gpu_ctx* c) {
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t j = 0; j < c->ar.ptrs.size(); j++) {
+            void* q = nullptr;
+            CK(cudaMalloc(&q, c->ar.bytes[j]));
+            CK(cudaMemcpy(q, c->ar.ptrs[j], c->ar.bytes[j], cudaMemcpyDeviceToDevice));
+            copies.push_back(q);
+        }
+        step = c->step;
+        cur = c->cur;
+        nsolves = c->nsolves;
+        last_iters = c->last_iters;
+        last_relres = c->last_relres;
+        launches = c->stats.launches;
+    }
+    void restore(vvm_gpu_ctx* c) {
+        CK(cudaStreamSynchronize(c->stream));
+        for (size_t j = 0; j < copies.size(); j++)
+            CK(cudaMemcpy(c->ar.ptrs[j], copies[j], c->ar.bytes[j], cudaMemcpyDeviceToDevice));
+        c->step = step;
+        c->cur = cur;
+        c->nsolves = nsolves;
+        c->last_iters = last_iters;
+        c->last_relres = last_relres;
+        c->stats.launches = launches;
+    }
+    ~Snapshot() {
+        for (void* q : copies) cudaFree(q);
+    }
+};
+
+// True when the case's next step may run from a captured graph (the test of
+// step_once).
+bool graph_ready(vvm_gpu_ctx* c) {
+    const bool forcing_now = c->has_forcing_th && ((c->step + 1) * c->desc.dt <= c->desc.addforcingtime);
+    const bool warm = c->desc.warm_start != 0;
+    return !c->graphs_off && !c->stats.on && c->step >= 0 && !forcing_now && c->poisson_ready &&
+           (!warm || c->nsolves >= 2);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- batches
+
+// Independent cases of any sizes that advance together: one CUDA graph per
+// step holds every case's step as a parallel branch (captured by forking the
+// batch stream to each case's stream and joining back), keyed like a case's
+// own graphs by (time-level buffer, step parity).
+struct vvm_gpu_batch {
+    int device = 0;
+    std::vector<vvm_gpu_ctx*> cases;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> joins;
+    cudaGraphExec_t gexec[2][2] = {};
+    std::vector<long long> gstatic[2][2];   // kernels outside loops, per case
+    std::string err;
+
+    void drop_graphs() {
+        for (auto& row : gexec)
+            for (auto& g : row)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+    }
+    ~vvm_gpu_batch() {
+        drop_graphs();
+        for (auto* c : cases) vvm_gpu_destroy(c);
+        for (auto e : joins) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int batch_fail(vvm_gpu_batch* b, int code, const std::string& msg) {
+    if (b) b->err = msg;
+    return code;
+}
+
+// Captures one step of the cases `idx` as a graph on the batch stream;
+// gstatic receives each case's kernel count outside loops.
+cudaGraphExec_t batch_capture(vvm_gpu_batch* b, const std::vector<int>& idx, std::vector<long long>& gstatic) {
+    gstatic.assign(b->cases.size(), 0);
+    struct Saved {
+        cudaStream_t stream;
+        int step, cur, nsolves;
+        long long launches;
+    };
+    std::vector<Saved> sv;
+    for (int i : idx) {
+        vvm_gpu_ctx* c = b->cases[i];
+        ensure_poisson(c);
+        sv.push_back({c->stream, c->step, c->cur, c->nsolves, c->stats.launches});
+    }
+    auto put_back = [&]() {
+        for (size_t j = 0; j < idx.size(); j++) {
+            vvm_gpu_ctx* c = b->cases[idx[j]];
+            c->stream = sv[j].stream;
+            c->step = sv[j].step;
+            c->cur = sv[j].cur;
+            c->nsolves = sv[j].nsolves;
+            c->stats.launches = sv[j].launches;
+        }
+    };
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+    try {
+        CK(cudaEventRecord(b->fork, b->stream));
+        for (int i : idx) {
+            vvm_gpu_ctx* c = b->cases[i];
+            c->stream = c->own;
+            CK(cudaStreamWaitEvent(c->own, b->fork, 0));
+            const long long l0 = c->stats.launches;
+            long long in_loops = 0;
+            if (c->mixed) run_step<float>(c, &in_loops);
+            else run_step<double>(c, &in_loops);
+            gstatic[i] = c->stats.launches - l0 - in_loops;
+            CK(cudaEventRecord(b->joins[i], c->own));
+            CK(cudaStreamWaitEvent(b->stream, b->joins[i], 0));
+        }
+    } catch (...) {
+        cudaStreamEndCapture(b->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        put_back();
+        throw;
+    }
+    CK(cudaStreamEndCapture(b->stream, &g));
+    put_back();
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw CudaError{std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+    return ex;
+}
+
+// Orders the batch stream after every case's stream (into = true) or every
+// case's stream after the batch stream.
+void batch_fence(vvm_gpu_batch* b, bool into) {
+    for (size_t i = 0; i < b->cases.size(); i++) {
+        vvm_gpu_ctx* c = b->cases[i];
+        if (into) {
+            CK(cudaEventRecord(b->joins[i], c->stream));
+            CK(cudaStreamWaitEvent(b->stream, b->joins[i], 0));
+        } else {
+            CK(cudaEventRecord(b->joins[i], b->stream));
+            CK(cudaStreamWaitEvent(c->stream, b->joins[i], 0));
+        }
+    }
+}
+
+int batch_step(vvm_gpu_batch* b, int nsteps) {
+    int worst = VVM_GPU_OK;
+    std::vector<int> all(b->cases.size());
+    for (size_t i = 0; i < all.size(); i++) all[i] = (int)i;
+    bool on_batch = false;   // work since the last fence sits on the batch stream
+    for (int s = 0; s < nsteps; s++) {
+        vvm_gpu_ctx* c0 = b->cases[0];
+        bool ready = true;
+        for (auto* c : b->cases) {
+            if (c->step != c0->step || c->cur != c0->cur)
+                return batch_fail(b, VVM_GPU_ESTATE, "batch_step: the cases are not at the same step");
+            ready = ready && graph_ready(c);
+        }
+        if (!ready) {   // the first steps, or timers on: each case on its own stream
+            if (on_batch) {
+                batch_fence(b, false);
+                on_batch = false;
+            }
+            for (auto* c : b->cases) {
+                int rc = c->mixed ? step_once<float>(c) : step_once<double>(c);
+                if (rc != VVM_GPU_OK) worst = rc;
+            }
+            continue;
+        }
+        const int bi = c0->cur, par = (c0->step + 1) & 1;
+        if (!b->gexec[bi][par]) b->gexec[bi][par] = batch_capture(b, all, b->gstatic[bi][par]);
+        if (!on_batch) {
+            batch_fence(b, true);
+            on_batch = true;
+        }
+        CK(cudaGraphLaunch(b->gexec[bi][par], b->stream));
+        for (size_t i = 0; i < b->cases.size(); i++) {
+            vvm_gpu_ctx* c = b->cases[i];
+            c->stats.launches += b->gstatic[bi][par][i];
+            c->step++;
+            c->cur = 1 - c->cur;
+            c->nsolves++;
+            c->last_graph = true;
+        }
+    }
+    if (on_batch) batch_fence(b, false);
+    return worst;
+}
+
+// Milliseconds a step of the cases `idx` takes as one graph (one launch to
+// warm up, then `reps` timed launches of the same graph on the batch stream).
+double batch_time(vvm_gpu_batch* b, const std::vector<int>& idx, int reps) {
+    std::vector<long long> gs;
+    cudaGraphExec_t ex = batch_capture(b, idx, gs);
+    CK(cudaGraphLaunch(ex, b->stream));
+    CK(cudaEventRecord(b->t0, b->stream));
+    for (int r = 0; r < reps; r++) CK(cudaGraphLaunch(ex, b->stream));
+    CK(cudaEventRecord(b->t1, b->stream));
+    CK(cudaEventSynchronize(b->t1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, b->t0, b->t1));
+    cudaGraphExecDestroy(ex);
+    return ms / std::max(reps, 1);
+}
+
+// Autotuner: for each group of cases with the same grid, precision and
+// solver, coordinate descent over the launch-shape knobs that leave the
+// arithmetic unchanged (the Gauss-Seidel cluster size, the row-FFT block),
+// timing one step of the group's cases as a graph per candidate. Every case
+// is put back exactly afterwards.
+int batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
+    const size_t n = b->cases.size();
+    CK(cudaStreamSynchronize(b->stream));
+    std::vector<std::unique_ptr<Snapshot>> snaps(n);
+    for (size_t i = 0; i < n; i++) {
+        snaps[i].reset(new Snapshot());
+        snaps[i]->take(b->cases[i]);
+    }
+    int rc = VVM_GPU_OK;
+    // bring every case to a step that runs from a graph (restored below)
+    for (int guard = 0; guard < 4 && rc == VVM_GPU_OK; guard++) {
+        bool ready = true;
+        for (auto* c : b->cases) ready = ready && graph_ready(c);
+        if (ready) break;
+        rc = batch_step(b, 1);
+    }
+    std::vector<std::vector<int>> groups;
+    std::vector<std::array<int, 4>> keys;
+    for (size_t i = 0; i < n; i++) {
+        vvm_gpu_ctx* c = b->cases[i];
+        std::array<int, 4> k = {c->d.nx, c->d.nz, c->mixed ? 1 : 0, c->spectral ? 1 : 0};
+        size_t gi = 0;
+        while (gi < keys.size() && keys[gi] != k) gi++;
+        if (gi == keys.size()) {
+            keys.push_back(k);
+            groups.emplace_back();
+        }
+        groups[gi].push_back((int)i);
+    }
+    auto set_all = [&](const std::vector<int>& idx, int cs, int fft) {
+        for (int i : idx) {
+            vvm_gpu_ctx* c = b->cases[i];
+            c->tune_gs_cs = cs;
+            c->tune_fft = fft;
+            apply_tuning(c);
+        }
+    };
+    for (size_t gi = 0; gi < groups.size() && rc == VVM_GPU_OK; gi++) {
+        const std::vector<int>& idx = groups[gi];
+        vvm_gpu_ctx* c = b->cases[idx[0]];
+        int best_cs = c->tune_gs_cs, best_fft = c->tune_fft;
+        double best = batch_time(b, idx, reps);
+        for (int cs : {8, 4, 2, 1}) {
+            set_all(idx, cs, best_fft);
+            const double t = batch_time(b, idx, reps);
+            if (t < best) {
+                best = t;
+                best_cs = cs;
+            }
+        }
+        set_all(idx, best_cs, best_fft);
+        if (c->spectral) {
+            for (int th : {128, 256, 512}) {
+                set_all(idx, best_cs, th);
+                const double t = batch_time(b, idx, reps);
+                if (t < best) {
+                    best = t;
+                    best_fft = th;
+                }
+            }
+        }
+        set_all(idx, best_cs, best_fft);
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    for (size_t i = 0; i < n; i++) {
+        snaps[i]->restore(b->cases[i]);
+        b->cases[i]->drop_graphs();
+    }
+    b->drop_graphs();
+    if (ngroups) *ngroups = (int)groups.size();
+    return rc;
+}
+
+template <typename Fn>
+int batch_guarded(vvm_gpu_batch* b, Fn fn) {
+    if (!b) return VVM_GPU_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != b->device) cudaSetDevice(b->device);
+    int rc;
+    try {
+        rc = fn();
+    } catch (const CudaError& e) {
+        rc = batch_fail(b, VVM_GPU_ECUDA, e.msg);
+    }
+    if (prev != b->device) cudaSetDevice(prev);
+    return rc;
 }
 
 // ---------------------------------------------------------------- transfer
@@ -2177,6 +2523,121 @@ int vvm_gpu_launch_count(vvm_gpu_ctx* ctx, long long* launches) {
         *launches = ctx->stats.launches + in_loops;
         return VVM_GPU_OK;
     });
+}
+
+int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_cluster_ctas, int fft_threads) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    if (gs_cluster_ctas < 0 || gs_cluster_ctas > 8 || fft_threads < 0 || fft_threads > 1024)
+        return fail(ctx, VVM_GPU_EINVAL, "set_tuning: knob out of range");
+    return guarded(ctx, [&]() -> int {
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->tune_gs_cs = gs_cluster_ctas;
+        ctx->tune_fft = fft_threads;
+        apply_tuning(ctx);
+        ctx->drop_graphs();
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_cluster_ctas, int* fft_threads) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    const size_t elem = ctx->mixed ? sizeof(float) : sizeof(double);
+    if (gs_cluster_ctas) *gs_cluster_ctas = gs_plan(ctx->d.pitch, ctx->d.nz, elem, ctx->tune_gs_cs).cs;
+    if (fft_threads) {
+        *fft_threads = 0;
+        if (ctx->spectral) {
+            const int half = std::max(32, (ctx->d.nx - 2) / 2);
+            *fft_threads = ctx->tune_fft > 0 ? std::max(32, std::min(ctx->tune_fft, std::min(half, 1024)))
+                                             : std::min(half, 512);
+        }
+    }
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_batch_create(const vvm_gpu_desc* descs, int ncases, int device, vvm_gpu_batch** out) {
+    if (!descs || !out || ncases <= 0) return fail(nullptr, VVM_GPU_EINVAL, "batch_create: bad arguments");
+    *out = nullptr;
+    std::unique_ptr<vvm_gpu_batch> b(new vvm_gpu_batch());
+    b->device = device;
+    for (int i = 0; i < ncases; i++) {
+        vvm_gpu_ctx* c = nullptr;
+        int rc = vvm_gpu_create(&descs[i], device, &c);
+        if (rc != VVM_GPU_OK) {
+            g_create_error = "batch_create: case " + std::to_string(i) + ": " + g_create_error;
+            return rc;
+        }
+        b->cases.push_back(c);
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->t1);
+    b->joins.assign(ncases, nullptr);
+    for (int i = 0; i < ncases && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) return fail(nullptr, VVM_GPU_ECUDA, std::string("batch_create: ") + cudaGetErrorString(e));
+    *out = b.release();
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_batch_destroy(vvm_gpu_batch* b) {
+    if (!b) return VVM_GPU_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    delete b;
+    cudaSetDevice(prev);
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_batch_case(vvm_gpu_batch* b, int i, vvm_gpu_ctx** ctx) {
+    if (!b || !ctx) return VVM_GPU_EINVAL;
+    if (i < 0 || i >= (int)b->cases.size()) return batch_fail(b, VVM_GPU_EINVAL, "batch_case: index out of range");
+    *ctx = b->cases[i];
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_batch_step(vvm_gpu_batch* b, int nsteps) {
+    if (!b) return VVM_GPU_EINVAL;
+    if (nsteps < 0) return batch_fail(b, VVM_GPU_EINVAL, "batch_step: nsteps < 0");
+    return batch_guarded(b, [&]() -> int {
+        for (auto* c : b->cases)
+            if (!c->has_state) return batch_fail(b, VVM_GPU_ESTATE, "batch_step: a case has no state uploaded");
+        int rc = batch_step(b, nsteps);
+        if (rc == VVM_GPU_ENOCONV) batch_fail(b, rc, "batch_step: a Poisson solve did not reach its tolerance");
+        return rc;
+    });
+}
+
+int vvm_gpu_batch_synchronize(vvm_gpu_batch* b) {
+    return batch_guarded(b, [&]() -> int {
+        CK(cudaStreamSynchronize(b->stream));
+        for (size_t i = 0; i < b->cases.size(); i++) {
+            vvm_gpu_ctx* c = b->cases[i];
+            CK(cudaStreamSynchronize(c->stream));
+            if (int rc = device_errors(c)) return batch_fail(b, rc, "case " + std::to_string(i) + ": " + c->err);
+        }
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
+    if (!b) return VVM_GPU_EINVAL;
+    return batch_guarded(b, [&]() -> int {
+        for (auto* c : b->cases)
+            if (!c->has_state) return batch_fail(b, VVM_GPU_ESTATE, "batch_autotune: a case has no state uploaded");
+        return batch_autotune(b, reps > 0 ? reps : 3, ngroups);
+    });
+}
+
+int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len) {
+    if (!b || !buf || len == 0) return VVM_GPU_EINVAL;
+    std::snprintf(buf, len, "%s", b->err.c_str());
+    return VVM_GPU_OK;
 }
 
 int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres) {

@@ -73,7 +73,10 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_download_state", "vvm_gpu_upload_prognostic", "vvm_gpu_download_prognostic",
            "vvm_gpu_set_step", "vvm_gpu_get_step", "vvm_gpu_step", "vvm_gpu_poisson_solve",
            "vvm_gpu_poisson_solve_device", "vvm_gpu_last_solve", "vvm_gpu_profile",
-           "vvm_gpu_profile_read", "vvm_gpu_launch_count", "vvm_gpu_poisson_solve_noalloc") + tuple(
+           "vvm_gpu_profile_read", "vvm_gpu_launch_count", "vvm_gpu_poisson_solve_noalloc",
+           "vvm_gpu_set_tuning", "vvm_gpu_get_tuning", "vvm_gpu_batch_create", "vvm_gpu_batch_destroy",
+           "vvm_gpu_batch_case", "vvm_gpu_batch_step", "vvm_gpu_batch_synchronize",
+           "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -108,6 +111,15 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_last_solve.argtypes = [vp, ctypes.POINTER(ip), _dp]
     L.vvm_gpu_poisson_solve_noalloc.argtypes = [ip, ip, _dp, _dp, vp, vp, ctypes.c_double, ip, vp,
                                                 ctypes.POINTER(ip), _dp]
+    L.vvm_gpu_set_tuning.argtypes = [vp, ip, ip]
+    L.vvm_gpu_get_tuning.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.vvm_gpu_batch_create.argtypes = [ctypes.POINTER(Desc), ip, ip, ctypes.POINTER(vp)]
+    L.vvm_gpu_batch_destroy.argtypes = [vp]
+    L.vvm_gpu_batch_case.argtypes = [vp, ip, ctypes.POINTER(vp)]
+    L.vvm_gpu_batch_step.argtypes = [vp, ip]
+    L.vvm_gpu_batch_synchronize.argtypes = [vp]
+    L.vvm_gpu_batch_autotune.argtypes = [vp, ip, ctypes.POINTER(ip)]
+    L.vvm_gpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -151,8 +163,23 @@ class VVMGpu:
                  addforcingtime: float = 0.0, poisson_maxit: int = 200):
         self.L = load_library()
         self.grid = grid
+        self.owned = True
+        d = self.make_desc(self.L, grid, precision, solver, poisson_tol, warm_start, addforcingtime,
+                           poisson_maxit)
+        self.desc = d
+        h = ctypes.c_void_p()
+        rc = self.L.vvm_gpu_create(ctypes.byref(d), int(device), ctypes.byref(h))
+        if rc != 0:
+            raise VVMGpuError(rc, self._err(None))
+        self.h = h
+        self._keep = []
+
+    @staticmethod
+    def make_desc(L, grid, precision=VVM_PREC_FP64, solver=VVM_SOLVER_MGPCG, poisson_tol=1e-10,
+                  warm_start=True, addforcingtime=0.0, poisson_maxit=200):
+        """vvm_gpu_desc of a grid (reference defaults, then the options)."""
         d = Desc()
-        self.L.vvm_gpu_desc_default(ctypes.byref(d), grid.NX, grid.NZ, float(grid.dx),
+        L.vvm_gpu_desc_default(ctypes.byref(d), grid.NX, grid.NZ, float(grid.dx),
                                     float(grid.dz), float(grid.dt))
         d.case_id = int(grid.case)
         d.moisture_nudge_time = float(grid.moisture_nudge_time)
@@ -162,13 +189,14 @@ class VVMGpu:
         d.poisson_tol = float(poisson_tol)
         d.poisson_maxit = int(poisson_maxit)
         d.warm_start = 1 if warm_start else 0
-        self.desc = d
-        h = ctypes.c_void_p()
-        rc = self.L.vvm_gpu_create(ctypes.byref(d), int(device), ctypes.byref(h))
-        if rc != 0:
-            raise VVMGpuError(rc, self._err(None))
-        self.h = h
-        self._keep = []
+        return d
+
+    @classmethod
+    def _borrow(cls, L, handle, grid, desc):
+        """A view of a context another object owns (a batch's case)."""
+        self = cls.__new__(cls)
+        self.L, self.grid, self.desc, self.h, self.owned, self._keep = L, grid, desc, handle, False, []
+        return self
 
     def _err(self, h):
         buf = ctypes.create_string_buffer(512)
@@ -181,7 +209,8 @@ class VVMGpu:
 
     def close(self):
         if getattr(self, "h", None):
-            self.L.vvm_gpu_destroy(self.h)
+            if getattr(self, "owned", True):
+                self.L.vvm_gpu_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -316,6 +345,15 @@ class VVMGpu:
         self._check(self.L.vvm_gpu_launch_count(self.h, ctypes.byref(n)))
         return n.value
 
+    def set_tuning(self, gs_cluster_ctas: int = 0, fft_threads: int = 0):
+        """Launch-shape knobs (0: automatic); results do not change."""
+        self._check(self.L.vvm_gpu_set_tuning(self.h, int(gs_cluster_ctas), int(fft_threads)))
+
+    def tuning(self) -> tuple[int, int]:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.vvm_gpu_get_tuning(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def last_solve(self):
         it, rel = ctypes.c_int(), ctypes.c_double()
         self._check(self.L.vvm_gpu_last_solve(self.h, ctypes.byref(it), ctypes.byref(rel)))
@@ -335,3 +373,63 @@ class VVMGpu:
                                                         ctypes.c_void_p(d_W), float(tol),
                                                         ctypes.byref(it), ctypes.byref(rel)))
         return it.value, rel.value
+
+
+class VVMBatch:
+    """Independent cases of any sizes advancing together, one CUDA graph a
+    step for all of them (vvm_gpu_batch_*). `cases[i]` is a VVMGpu view of
+    case i (owned by the batch) for upload, download and queries."""
+
+    def __init__(self, grids, precision: int = VVM_PREC_MIXED, solver: int = VVM_SOLVER_SPECTRAL,
+                 device: int = 0, **desc_options):
+        self.L = load_library()
+        grids = list(grids)
+        descs = (Desc * len(grids))()
+        for i, g in enumerate(grids):
+            descs[i] = VVMGpu.make_desc(self.L, g, precision, solver, **desc_options)
+        h = ctypes.c_void_p()
+        rc = self.L.vvm_gpu_batch_create(descs, len(grids), int(device), ctypes.byref(h))
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            self.L.vvm_gpu_last_error(None, buf, 512)
+            raise VVMGpuError(rc, buf.value.decode())
+        self.h = h
+        self.cases = []
+        for i, g in enumerate(grids):
+            c = ctypes.c_void_p()
+            self._check(self.L.vvm_gpu_batch_case(self.h, i, ctypes.byref(c)))
+            self.cases.append(VVMGpu._borrow(self.L, c, g, descs[i]))
+
+    def _check(self, rc):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            self.L.vvm_gpu_batch_last_error(self.h, buf, 512)
+            raise VVMGpuError(rc, buf.value.decode())
+
+    def upload(self, states):
+        for c, st in zip(self.cases, states):
+            c.upload(st)
+
+    def step(self, n: int = 1):
+        self._check(self.L.vvm_gpu_batch_step(self.h, int(n)))
+
+    def synchronize(self):
+        self._check(self.L.vvm_gpu_batch_synchronize(self.h))
+
+    def autotune(self, reps: int = 3) -> int:
+        n = ctypes.c_int()
+        self._check(self.L.vvm_gpu_batch_autotune(self.h, int(reps), ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            for c in self.cases:
+                c.h = None
+            self.L.vvm_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

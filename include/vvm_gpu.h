@@ -167,6 +167,38 @@ int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_
 /* Iterations and final relative residual of the last cal_w solve. */
 int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres);
 
+/* -- launch-shape knobs --------------------------------------------------------
+ * Neither changes any result (the arithmetic of every cell is the same):
+ * gs_cluster_ctas caps the CTAs of each Gauss-Seidel cluster (1, 2, 4, 8; the
+ * cap never goes below what the row needs), fft_threads sets the threads of a
+ * row-FFT block of the spectral solve; 0 selects the automatic value. Setting
+ * them drops the context's captured graphs. get returns the values in use. */
+int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_cluster_ctas, int fft_threads);
+int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_cluster_ctas, int* fft_threads);
+
+/* -- batches of independent cases ------------------------------------------------
+ * The reference runs one case per process. A batch holds many cases of any
+ * sizes (one context each, created from descs[i] on `device`) that advance
+ * together: from the third step on, one CUDA graph per step runs every
+ * case's step as a parallel branch, launched on the batch's own stream.
+ * vvm_gpu_batch_case returns case i's context, owned by the batch, for
+ * upload, download, queries and the routine entries; every case must be at
+ * the same step when vvm_gpu_batch_step runs (VVM_GPU_ESTATE otherwise).
+ * vvm_gpu_batch_autotune times one step of each group of cases with the same
+ * grid, precision and solver for each value of the launch-shape knobs above
+ * (`reps` graph launches per candidate), keeps the fastest, and restores
+ * every case's state exactly; *ngroups receives the number of groups.
+ * vvm_gpu_batch_synchronize waits for the batch and reports any case's
+ * device error. Failures of batch calls: vvm_gpu_batch_last_error. */
+typedef struct vvm_gpu_batch vvm_gpu_batch;
+int vvm_gpu_batch_create(const vvm_gpu_desc* descs, int ncases, int device, vvm_gpu_batch** out);
+int vvm_gpu_batch_destroy(vvm_gpu_batch* b);
+int vvm_gpu_batch_case(vvm_gpu_batch* b, int i, vvm_gpu_ctx** ctx);
+int vvm_gpu_batch_step(vvm_gpu_batch* b, int nsteps);
+int vvm_gpu_batch_synchronize(vvm_gpu_batch* b);
+int vvm_gpu_batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups);
+int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len);
+
 /* -- elliptic solve that allocates nothing ------------------------------------
  * No counterpart in the reference.
  *

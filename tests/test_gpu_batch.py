@@ -1,0 +1,103 @@
+"""Batches of independent cases (vvm_gpu_batch_*) and the launch-shape knobs.
+
+A batch runs every case's step as a branch of one CUDA graph, with the same
+kernels a single context launches, so each case must come out bit for bit
+equal to the same case stepped on its own. The knobs the autotuner turns
+(Gauss-Seidel cluster size, row-FFT block) change no arithmetic, so results
+stay bit-identical under any setting, and the autotuner must leave every
+case's state exactly as it found it.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PROG = ("zeta", "th", "qv", "qc", "qr", "u", "w")
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from vvm_b200 import build, gpu as G
+    build.build()
+    return G
+
+
+def _states(shapes):
+    from vvm_b200.initial_state import warm_bubble
+    return [warm_bubble(nx, nz, 200.0, 200.0, radius=max(400.0, nx * 200 / 8)) for nx, nz in shapes]
+
+
+def _alone(G, st, n, precision, solver):
+    g = G.VVMGpu(st.grid, precision=precision, solver=solver)
+    g.upload(st)
+    g.step(n)
+    out = g.download()
+    g.close()
+    return out
+
+
+def _same(a, b):
+    return all(np.array_equal(a.fields[f], b.fields[f]) for f in PROG)
+
+
+@pytest.mark.parametrize("precision,solver,shapes", [
+    (1, 2, [(64, 32), (128, 48), (256, 32)]),           # mixed, spectral
+    (0, 0, [(64, 32), (96, 33), (128, 24)]),            # FP64, multigrid, non-power-of-two NX
+])
+def test_batch_equals_cases_alone(gpu, precision, solver, shapes):
+    sts = _states(shapes)
+    b = gpu.VVMBatch([s.grid for s in sts], precision=precision, solver=solver)
+    b.upload(sts)
+    b.step(3)          # the first steps run case by case, then the batch graph
+    b.step(4)
+    b.synchronize()
+    for st, c in zip(sts, b.cases):
+        assert _same(c.download(), _alone(gpu, st, 7, precision, solver))
+    b.close()
+
+
+def test_autotune_restores_state_and_keeps_results(gpu):
+    shapes = [(64, 32), (64, 32), (256, 32)]
+    sts = _states(shapes)
+    b = gpu.VVMBatch([s.grid for s in sts], precision=1, solver=2)
+    b.upload(sts)
+    b.step(3)
+    b.synchronize()
+    before = [c.download() for c in b.cases]
+    ngroups = b.autotune(reps=2)
+    assert ngroups == 2
+    after = [c.download() for c in b.cases]
+    for x, y in zip(before, after):
+        assert _same(x, y)
+    for c in b.cases:
+        cs, fft = c.tuning()
+        assert cs in (1, 2, 4, 8) and fft in (128, 256, 512, 32, 64)
+    b.step(4)
+    b.synchronize()
+    for st, c in zip(sts, b.cases):
+        assert _same(c.download(), _alone(gpu, st, 7, 1, 2))
+    b.close()
+
+
+def test_knobs_leave_results_unchanged(gpu):
+    st = _states([(512, 32)])[0]
+    ref = _alone(gpu, st, 5, 1, 2)
+    for cs, fft in ((1, 128), (2, 512), (4, 64)):
+        g = gpu.VVMGpu(st.grid, precision=1, solver=2)
+        g.set_tuning(cs, fft)
+        g.upload(st)
+        g.step(5)
+        assert g.tuning()[0] <= max(cs, 1) or cs == 1
+        assert _same(g.download(), ref), (cs, fft)
+        g.close()
+
+
+def test_batch_rejects_cases_at_different_steps(gpu):
+    sts = _states([(64, 32), (64, 32)])
+    b = gpu.VVMBatch([s.grid for s in sts], precision=1, solver=2)
+    b.upload(sts)
+    b.cases[0].step(1)
+    with pytest.raises(gpu.VVMGpuError) as e:
+        b.step(1)
+    assert e.value.code == 4
+    b.close()
