@@ -2634,6 +2634,12 @@ int vvm_gpu_batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
     });
 }
 
+int vvm_gpu_batch_stream(vvm_gpu_batch* b, void** stream) {
+    if (!b || !stream) return VVM_GPU_EINVAL;
+    *stream = b->stream;
+    return VVM_GPU_OK;
+}
+
 int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len) {
     if (!b || !buf || len == 0) return VVM_GPU_EINVAL;
     std::snprintf(buf, len, "%s", b->err.c_str());

@@ -76,7 +76,7 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_profile_read", "vvm_gpu_launch_count", "vvm_gpu_poisson_solve_noalloc",
            "vvm_gpu_set_tuning", "vvm_gpu_get_tuning", "vvm_gpu_batch_create", "vvm_gpu_batch_destroy",
            "vvm_gpu_batch_case", "vvm_gpu_batch_step", "vvm_gpu_batch_synchronize",
-           "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error") + tuple(
+           "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -120,6 +120,7 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_batch_synchronize.argtypes = [vp]
     L.vvm_gpu_batch_autotune.argtypes = [vp, ip, ctypes.POINTER(ip)]
     L.vvm_gpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    L.vvm_gpu_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -415,6 +416,13 @@ class VVMBatch:
 
     def synchronize(self):
         self._check(self.L.vvm_gpu_batch_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the batch graphs (for timing events)."""
+        p = ctypes.c_void_p()
+        self._check(self.L.vvm_gpu_batch_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
 
     def autotune(self, reps: int = 3) -> int:
         n = ctypes.c_int()

@@ -24,7 +24,9 @@ one full-grid reference step.
 
 Multi-GPU (torchrun): one independent replica per GPU ("replicas only": one
 2D domain does not shard), max time over ranks, value = all ranks' cell-steps
-per second.
+per second. The `ensemble` object measures BASELINE configuration 3, 256
+independent cases of uneven grids in one CUDA graph a step, split over the
+ranks by cost (strong scaling: the ensemble is fixed).
 """
 from __future__ import annotations
 
@@ -318,6 +320,8 @@ def our_arm(args, rank, world, device):
         "gpu_launches": head["launches"],
         "clocks": clocks,
     }
+    if not args.no_ensemble:
+        line["ensemble"] = ensemble_arm(args, rank, world, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     return line
@@ -329,6 +333,54 @@ def st_nx():
 
 def st_nz():
     return NZ + 2
+
+
+# ------------------------------------------------------------------ ensemble
+
+ENSEMBLE_CASES, ENSEMBLE_SEED = 256, 3
+
+
+def ensemble_arm(args, rank, world, device):
+    """256 seeded warm-bubble cases of uneven grids
+    (vvm_b200.ensemble), mixed precision with the spectral solve, one batch
+    graph a step on each rank; the cases are split over the ranks by cost.
+    The ensemble is fixed, so more ranks is strong scaling."""
+    import torch
+    from vvm_b200.ensemble import ensemble_specs, ensemble_state, shard_by_cost
+    from vvm_b200.gpu import VVM_PREC_MIXED, VVM_SOLVER_SPECTRAL, VVMBatch
+    specs = ensemble_specs(ENSEMBLE_CASES, ENSEMBLE_SEED)
+    costs = [sp["NX"] * sp["NZ"] for sp in specs]
+    mine = shard_by_cost(costs, world)[rank]
+    sts = [ensemble_state(specs[i]) for i in mine]
+    b = VVMBatch([st.grid for st in sts], precision=VVM_PREC_MIXED, solver=VVM_SOLVER_SPECTRAL,
+                 device=device)
+    b.upload(sts)
+    b.step(3)
+    b.synchronize()
+    groups = b.autotune(reps=2)
+    b.step(args.warmup)
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.stream, device=torch.device(f"cuda:{device}"))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist_on():
+        dist_barrier()
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    b.synchronize()
+    max_ms = dist_max(e0.elapsed_time(e1))
+    total = sum(costs)
+    b.close()
+    return {"workload": f"{ENSEMBLE_CASES} warm-bubble cases (seed {ENSEMBLE_SEED}): NX in "
+                        "{256,512,1024,2048}, NZ in {64,96,128}, amplitude U(1,3) K, centre "
+                        "U(0.2,0.8), radius U(1,3) km, dx=dz=200 m, dt=1 s",
+            "metric": METRIC, "value": total * args.steps / (max_ms * 1e-3), "unit": METRIC,
+            "ms_per_step": max_ms / args.steps, "cells_per_step": total, "cases": ENSEMBLE_CASES,
+            "cases_this_rank": len(mine), "scaling": "strong",
+            "sharding": "by cells, longest first to the least-loaded rank; no exchange",
+            "precision": "mixed", "solver": "spectral", "graph": "one CUDA graph a step for all cases",
+            "autotune_groups": groups, "l2": "working set larger than L2"}
 
 
 # ----------------------------------------------------------- reference arm
@@ -405,6 +457,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-case batched ensemble")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

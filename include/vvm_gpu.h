@@ -197,6 +197,8 @@ int vvm_gpu_batch_case(vvm_gpu_batch* b, int i, vvm_gpu_ctx** ctx);
 int vvm_gpu_batch_step(vvm_gpu_batch* b, int nsteps);
 int vvm_gpu_batch_synchronize(vvm_gpu_batch* b);
 int vvm_gpu_batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups);
+/* The stream the batch graphs run on (cudaStream_t), for events around them. */
+int vvm_gpu_batch_stream(vvm_gpu_batch* b, void** stream);
 int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len);
 
 /* -- elliptic solve that allocates nothing ------------------------------------
