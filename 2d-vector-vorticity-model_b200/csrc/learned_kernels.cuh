@@ -1,0 +1,210 @@
+// Kernels of the learned preconditioner: a linear multi-level 3x3
+// convolutional network on the cal_w residual, BF16 activations and weights
+// with FP32 accumulation.
+//
+// Activations are stored NHWC: pixel (y, x) of a level holds its C = 32
+// channels contiguously, 64 bytes, row-major in (y, x). Rows are periodic in
+// x (the cal_w operator is) and zero-padded in y (W = 0 outside the rows).
+//
+// The 32 -> 32 convolutions run on the tensor cores (tcgen05): one CTA of 128
+// threads computes 128 consecutive pixels of one row as D[128 x 32] =
+// sum over the 9 taps and 2 K-steps of 16 channels of A_tap[128 x 16] x
+// B_tap[16 x 32]. A_tap is the input tile shifted by the tap: the CTA stages
+// rows y-1..y+1, pixels x0-1..x0+128, in shared memory in the canonical
+// K-major no-swizzle layout (for each group of 8 channels, the pixels
+// 16 bytes apart), so a shift of one pixel is a shift of 16 bytes of the
+// operand's start address and no im2col copy is made. The accumulator lives
+// in 32 TMEM columns; each warp reads back its 32 lanes (pixels).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "vvm_common.cuh"
+
+namespace vvm {
+
+constexpr int kNetC = 32;        // channels
+constexpr int kConvTile = 128;   // pixels of a CTA (the MMA's M)
+constexpr int kConvSpan = kConvTile + 2;
+constexpr int kNetErrWait = 2;   // device error word: an MMA completion wait gave up
+constexpr int kMmaSpinLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor of tcgen05 (K-major, no swizzle): start
+// address, the byte offset between the two 8-element K chunks (LBO) and
+// between groups of 8 rows (SBO), all in 16-byte units; version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;                  // version
+    return d;                                // base offset 0, legacy LBO mode, layout SWIZZLE_NONE
+}
+
+// Instruction descriptor of kind::f16: D in FP32, A and B in BF16, both
+// K-major, N = 32, M = 128.
+constexpr uint32_t kConvIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kNetC >> 3) << 17) |
+                                ((uint32_t)(kConvTile >> 4) << 24);
+
+struct ConvArgs {
+    const __nv_bfloat16* in;   // [H][W][32]
+    __nv_bfloat16* out;        // [H][W][32]
+    const uint4* w;            // packed B operand: [9 taps][4 chunks][32 out] of 8 inputs
+    int H, W;
+    int* err;                  // device error word
+};
+
+// out = conv3x3(in, w), 32 -> 32 channels; grid = H * ceil(W / 128) CTAs of
+// 128 threads.
+__global__ void __launch_bounds__(kConvTile) k_conv32_tc(ConvArgs a) {
+    __shared__ __align__(128) uint4 sA[3][4][kConvSpan];   // [row][channel chunk][pixel]
+    __shared__ __align__(128) uint4 sB[9][4][kNetC];       // [tap][channel chunk][out channel]
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tiles = (a.W + kConvTile - 1) / kConvTile;
+    const int y = blockIdx.x / tiles, x0 = (blockIdx.x % tiles) * kConvTile;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(32)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // input tile: rows y-1..y+1 (zero outside), pixels x0-1..x0+128 (periodic)
+    for (int j = tid; j < 3 * kConvSpan * 4; j += kConvTile) {
+        const int kc = j & 3, p = (j >> 2) % kConvSpan, dy = (j >> 2) / kConvSpan;
+        const int yy = y + dy - 1;
+        int xx = (x0 + p - 1) % a.W;
+        if (xx < 0) xx += a.W;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (yy >= 0 && yy < a.H)
+            v = *reinterpret_cast<const uint4*>(a.in + ((size_t)yy * a.W + xx) * kNetC + kc * 8);
+        sA[dy][kc][p] = v;
+    }
+    for (int j = tid; j < 9 * 4 * kNetC; j += kConvTile) (&sB[0][0][0])[j] = a.w[j];
+    // make the generic-proxy shared stores visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    if (tid == 0) {
+        uint32_t acc = 0;
+        for (int dy = 0; dy < 3; dy++)
+            for (int dx = 0; dx < 3; dx++)
+                for (int ks = 0; ks < 2; ks++) {
+                    const uint64_t ad = umma_desc(smem_u32(&sA[dy][2 * ks][dx]), kConvSpan * 16, 128);
+                    const uint64_t bd = umma_desc(smem_u32(&sB[dy * 3 + dx][2 * ks][0]), kNetC * 16, 128);
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(tmem),
+                        "l"(ad), "l"(bd), "r"(kConvIdesc), "r"(acc), "r"(0u)
+                        : "memory");
+                    acc = 1;
+                }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+    }
+    // wait for the MMAs (bounded; on give-up, record it and wait once more so
+    // no MMA is in flight when TMEM is freed)
+    bool done = false;
+    for (int pass = 0; pass < 2 && !done; pass++) {
+        for (int it = 0; it < kMmaSpinLimit; it++) {
+            uint32_t ok;
+            asm volatile(
+                "{\n\t.reg .pred P1;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, P1;\n\t}\n"
+                : "=r"(ok)
+                : "r"(smem_u32(&mbar)), "r"(0u)
+                : "memory");
+            if (ok) {
+                done = true;
+                break;
+            }
+        }
+        if (!done && pass == 0 && tid == 0 && a.err) atomicOr(a.err, kNetErrWait);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (__all_sync(0xffffffffu, done)) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+              "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+              "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int x = x0 + tid;   // TMEM lane = pixel of the tile
+        if (x < a.W) {
+            uint4* dst = reinterpret_cast<uint4*>(a.out + ((size_t)y * a.W + x) * kNetC);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                __nv_bfloat162 h0 = __floats2bfloat162_rn(__uint_as_float(r[8 * q + 0]), __uint_as_float(r[8 * q + 1]));
+                __nv_bfloat162 h1 = __floats2bfloat162_rn(__uint_as_float(r[8 * q + 2]), __uint_as_float(r[8 * q + 3]));
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(__uint_as_float(r[8 * q + 4]), __uint_as_float(r[8 * q + 5]));
+                __nv_bfloat162 h3 = __floats2bfloat162_rn(__uint_as_float(r[8 * q + 6]), __uint_as_float(r[8 * q + 7]));
+                uint4 v;
+                v.x = *reinterpret_cast<uint32_t*>(&h0);
+                v.y = *reinterpret_cast<uint32_t*>(&h1);
+                v.z = *reinterpret_cast<uint32_t*>(&h2);
+                v.w = *reinterpret_cast<uint32_t*>(&h3);
+                dst[q] = v;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+}
+
+// Packs FP32 weights w[tap][in][out] into the B operand of k_conv32_tc:
+// [tap][in / 8][out] of 8 consecutive inputs in BF16. With flip, the packed
+// operand is that of the adjoint convolution: tap 8 - t, in and out swapped.
+__global__ void k_pack_conv32(const float* w, uint4* packed, int flip) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;   // (tap, chunk, out)
+    if (j >= 9 * 4 * kNetC) return;
+    const int co = j % kNetC, kc = (j / kNetC) % 4, t = j / (4 * kNetC);
+    float v[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+        const int ci = kc * 8 + e;
+        v[e] = flip ? w[((8 - t) * kNetC + co) * kNetC + ci] : w[(t * kNetC + ci) * kNetC + co];
+    }
+    __nv_bfloat162 h0 = __floats2bfloat162_rn(v[0], v[1]), h1 = __floats2bfloat162_rn(v[2], v[3]);
+    __nv_bfloat162 h2 = __floats2bfloat162_rn(v[4], v[5]), h3 = __floats2bfloat162_rn(v[6], v[7]);
+    uint4 o;
+    o.x = *reinterpret_cast<uint32_t*>(&h0);
+    o.y = *reinterpret_cast<uint32_t*>(&h1);
+    o.z = *reinterpret_cast<uint32_t*>(&h2);
+    o.w = *reinterpret_cast<uint32_t*>(&h3);
+    packed[j] = o;
+}
+
+__global__ void k_f32_to_bf16(const float* x, __nv_bfloat16* y, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = __float2bfloat16_rn(x[i]);
+}
+
+__global__ void k_bf16_to_f32(const __nv_bfloat16* x, float* y, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = __bfloat162float(x[i]);
+}
+
+}  // namespace vvm

@@ -15,6 +15,7 @@
 #include "../../include/vvm_gpu.h"
 #include "poisson_kernels.cuh"
 #include "spectral_kernels.cuh"
+#include "learned_kernels.cuh"
 #include "step_kernels.cuh"
 
 using namespace vvm;
@@ -2523,6 +2524,43 @@ int vvm_gpu_launch_count(vvm_gpu_ctx* ctx, long long* launches) {
         *launches = ctx->stats.launches + in_loops;
         return VVM_GPU_OK;
     });
+}
+
+int vvm_gpu_conv3x3_c32(const float* x, const float* w, float* y, int H, int W, int adjoint, int device) {
+    if (!x || !w || !y || H < 1 || W < 1) return fail(nullptr, VVM_GPU_EINVAL, "conv3x3_c32: bad arguments");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    int rc = VVM_GPU_OK;
+    try {
+        Arena ar;
+        const size_t n = (size_t)H * W * kNetC;
+        float* fx = ar.alloc<float>(n);
+        float* fw = ar.alloc<float>(9 * kNetC * kNetC);
+        int* err = ar.alloc<int>(1);
+        __nv_bfloat16* bx = ar.alloc<__nv_bfloat16>(n);
+        __nv_bfloat16* by = ar.alloc<__nv_bfloat16>(n);
+        uint4* pw = ar.alloc<uint4>(9 * 4 * kNetC);
+        CK(cudaMemcpy(fx, x, n * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(fw, w, 9 * kNetC * kNetC * sizeof(float), cudaMemcpyHostToDevice));
+        k_f32_to_bf16<<<256, 256>>>(fx, bx, n);
+        CKL();
+        k_pack_conv32<<<cdiv(9 * 4 * kNetC, 128), 128>>>(fw, pw, adjoint ? 1 : 0);
+        CKL();
+        ConvArgs a{bx, by, pw, H, W, err};
+        k_conv32_tc<<<H * cdiv(W, kConvTile), kConvTile>>>(a);
+        CKL();
+        k_bf16_to_f32<<<256, 256>>>(by, fx, n);
+        CKL();
+        CK(cudaMemcpy(y, fx, n * sizeof(float), cudaMemcpyDeviceToHost));
+        int h = 0;
+        CK(cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) rc = fail(nullptr, VVM_GPU_ECUDA, "conv3x3_c32: an MMA completion wait gave up");
+    } catch (const CudaError& e) {
+        rc = fail(nullptr, VVM_GPU_ECUDA, e.msg);
+    }
+    cudaSetDevice(prev);
+    return rc;
 }
 
 int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_cluster_ctas, int fft_threads) {

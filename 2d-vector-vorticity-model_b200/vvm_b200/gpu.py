@@ -76,7 +76,8 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_profile_read", "vvm_gpu_launch_count", "vvm_gpu_poisson_solve_noalloc",
            "vvm_gpu_set_tuning", "vvm_gpu_get_tuning", "vvm_gpu_batch_create", "vvm_gpu_batch_destroy",
            "vvm_gpu_batch_case", "vvm_gpu_batch_step", "vvm_gpu_batch_synchronize",
-           "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream") + tuple(
+           "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream",
+           "vvm_gpu_conv3x3_c32") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -121,6 +122,8 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_batch_autotune.argtypes = [vp, ip, ctypes.POINTER(ip)]
     L.vvm_gpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
     L.vvm_gpu_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    _fp = ctypes.POINTER(ctypes.c_float)
+    L.vvm_gpu_conv3x3_c32.argtypes = [_fp, _fp, _fp, ip, ip, ip, ip]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -441,3 +444,23 @@ class VVMBatch:
             self.close()
         except Exception:
             pass
+
+
+def conv3x3_c32(x: np.ndarray, w: np.ndarray, adjoint: bool = False, device: int = 0) -> np.ndarray:
+    """vvm_gpu_conv3x3_c32: x [H][W][32], w [9][32][32] (tap = 3 (dy+1) + dx+1,
+    in, out) -> [H][W][32] on the tensor cores (BF16 operands, FP32
+    accumulation, BF16 result)."""
+    L = load_library()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    H, W = x.shape[0], x.shape[1]
+    assert x.shape == (H, W, 32) and w.shape == (9, 32, 32)
+    y = np.empty_like(x)
+    fp = ctypes.POINTER(ctypes.c_float)
+    rc = L.vvm_gpu_conv3x3_c32(x.ctypes.data_as(fp), w.ctypes.data_as(fp), y.ctypes.data_as(fp), H, W,
+                               1 if adjoint else 0, int(device))
+    if rc != 0:
+        buf = ctypes.create_string_buffer(512)
+        L.vvm_gpu_last_error(None, buf, 512)
+        raise VVMGpuError(rc, buf.value.decode())
+    return y

@@ -167,6 +167,16 @@ int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_
 /* Iterations and final relative residual of the last cal_w solve. */
 int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres);
 
+/* -- the learned preconditioner's tensor-core convolution ------------------------
+ * One 3x3 convolution of 32 channels in and out (or, with adjoint != 0, its
+ * adjoint: taps mirrored, channels transposed) on the tensor cores, from and
+ * to host arrays: x, y [H][W][32] FP32 (rounded to BF16 on the device),
+ * w [9 taps][32 in][32 out] FP32 (BF16 on the device), periodic in the W
+ * direction and zero outside the H direction, FP32 accumulation, BF16 output.
+ * A diagnostic of the building block; the network runs it on device buffers.
+ * Failures: vvm_gpu_last_error(NULL, ...). */
+int vvm_gpu_conv3x3_c32(const float* x, const float* w, float* y, int H, int W, int adjoint, int device);
+
 /* -- launch-shape knobs --------------------------------------------------------
  * Neither changes any result (the arithmetic of every cell is the same):
  * gs_cluster_ctas caps the CTAs of each Gauss-Seidel cluster (1, 2, 4, 8; the
