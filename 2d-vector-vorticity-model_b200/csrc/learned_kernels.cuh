@@ -197,6 +197,281 @@ __global__ void k_pack_conv32(const float* w, uint4* packed, int flip) {
     packed[j] = o;
 }
 
+// ---------------------------------------------------------------------------
+// The rest of the network on the CUDA cores. Pixels of level l form an
+// [H][W] grid (H, W of level 0 multiples of 8; level l+1 halves both); a
+// thread handles one pixel, or one pixel's chunk of 8 channels (16 bytes).
+
+__device__ __forceinline__ void bf16x8_load(const __nv_bfloat16* p, float (&v)[8]) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float2 f = __bfloat1622float2(h[q]);
+        v[2 * q] = f.x;
+        v[2 * q + 1] = f.y;
+    }
+}
+
+__device__ __forceinline__ void bf16x8_store(__nv_bfloat16* p, const float (&v)[8]) {
+    uint4 u;
+    __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+    for (int q = 0; q < 4; q++) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+    *reinterpret_cast<uint4*>(p) = u;
+}
+
+__device__ __forceinline__ int wrapx(int x, int W) { return x < 0 ? x + W : (x >= W ? x - W : x); }
+
+// h[p][c] = sum_t wl[t][c] x[p + off(t)]  (1 -> 32 channels; x FP32 [H][W]).
+__global__ void k_net_lift(const float* x, const float* wl, __nv_bfloat16* h, int H, int W) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= H * W) return;
+    const int y = p / W, xx = p - y * W;
+    float xv[9];
+#pragma unroll
+    for (int t = 0; t < 9; t++) {
+        const int yy = y + t / 3 - 1, xs = wrapx(xx + t % 3 - 1, W);
+        xv[t] = (yy >= 0 && yy < H) ? x[(size_t)yy * W + xs] : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        float o[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            float acc = 0.f;
+#pragma unroll
+            for (int t = 0; t < 9; t++) acc += __ldg(wl + t * kNetC + 8 * q + e) * xv[t];
+            o[e] = acc;
+        }
+        bf16x8_store(h + (size_t)p * kNetC + 8 * q, o);
+    }
+}
+
+// z[p] = scale * sum_t sum_c wp[t][c] g[p + off(t)][c] for rows < hvalid, else 0
+// (32 -> 1 channel; z FP32 [H][W]).
+__global__ void k_net_proj(const __nv_bfloat16* g, const float* wp, float* z, int H, int W, int hvalid,
+                           float scale) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= H * W) return;
+    const int y = p / W, xx = p - y * W;
+    float acc = 0.f;
+    if (y < hvalid) {
+        for (int t = 0; t < 9; t++) {
+            const int yy = y + t / 3 - 1, xs = wrapx(xx + t % 3 - 1, W);
+            if (yy < 0 || yy >= H) continue;
+            const __nv_bfloat16* gp = g + ((size_t)yy * W + xs) * kNetC;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                float v[8];
+                bf16x8_load(gp + 8 * q, v);
+#pragma unroll
+                for (int e = 0; e < 8; e++) acc += __ldg(wp + t * kNetC + 8 * q + e) * v[e];
+            }
+        }
+    }
+    z[p] = acc * scale;
+}
+
+// Adjoint of k_net_proj (scale 1): dg[q][c] = sum_t wp[t][c] dz[q - off(t)].
+__global__ void k_net_proj_adj(const float* dz, const float* wp, __nv_bfloat16* dg, int H, int W) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= H * W) return;
+    const int y = p / W, xx = p - y * W;
+    float dv[9];
+#pragma unroll
+    for (int t = 0; t < 9; t++) {
+        const int yy = y - (t / 3 - 1), xs = wrapx(xx - (t % 3 - 1), W);
+        dv[t] = (yy >= 0 && yy < H) ? dz[(size_t)yy * W + xs] : 0.f;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        float o[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            float acc = 0.f;
+#pragma unroll
+            for (int t = 0; t < 9; t++) acc += __ldg(wp + t * kNetC + 8 * q + e) * dv[t];
+            o[e] = acc;
+        }
+        bf16x8_store(dg + (size_t)p * kNetC + 8 * q, o);
+    }
+}
+
+// out[y][x] = mult * sum of the 2x2 block of in at (2y, 2x); Ho x Wo coarse
+// pixels (mult 1/4: average pooling; 1: adjoint of nearest upsampling).
+__global__ void k_net_sum4(const __nv_bfloat16* in, __nv_bfloat16* out, int Ho, int Wo, float mult) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;   // (coarse pixel, chunk)
+    if (j >= Ho * Wo * 4) return;
+    const int q = j & 3, p = j >> 2, y = p / Wo, x = p - y * Wo;
+    const int Wf = 2 * Wo;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            float v[8];
+            bf16x8_load(in + ((size_t)(2 * y + a) * Wf + 2 * x + b) * kNetC + 8 * q, v);
+#pragma unroll
+            for (int e = 0; e < 8; e++) s[e] += v[e];
+        }
+#pragma unroll
+    for (int e = 0; e < 8; e++) s[e] *= mult;
+    bf16x8_store(out + (size_t)p * kNetC + 8 * q, s);
+}
+
+// out[y][x] = mult * lo[y/2][x/2] + skip[y][x] (out may be skip); H x W fine
+// pixels (mult 1: nearest upsampling plus the skip connection; 1/4: adjoint
+// of average pooling, accumulated).
+__global__ void k_net_up_add(const __nv_bfloat16* lo, const __nv_bfloat16* skip, __nv_bfloat16* out, int H, int W,
+                             float mult) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= H * W * 4) return;
+    const int q = j & 3, p = j >> 2, y = p / W, x = p - y * W;
+    float a[8], b[8];
+    bf16x8_load(lo + ((size_t)(y >> 1) * (W >> 1) + (x >> 1)) * kNetC + 8 * q, a);
+    bf16x8_load(skip + (size_t)p * kNetC + 8 * q, b);
+#pragma unroll
+    for (int e = 0; e < 8; e++) a[e] = mult * a[e] + b[e];
+    bf16x8_store(out + (size_t)p * kNetC + 8 * q, a);
+}
+
+// dW[t][ci][co] += sum_p X[p + off(t)][ci] dY[p][co] over one tile of 128
+// pixels of a row (grid = H * ceil(W / 128), 256 threads; 36 weights a thread).
+__global__ void __launch_bounds__(256) k_net_wgrad32(const __nv_bfloat16* X, const __nv_bfloat16* dY, float* dW,
+                                                     int H, int W) {
+    __shared__ __nv_bfloat16 sx[3][kConvSpan][kNetC];
+    __shared__ __nv_bfloat16 sy[kConvTile][kNetC];
+    const int tiles = (W + kConvTile - 1) / kConvTile;
+    const int y = blockIdx.x / tiles, x0 = (blockIdx.x % tiles) * kConvTile;
+    const int n = min(kConvTile, W - x0);
+    for (int j = threadIdx.x; j < 3 * kConvSpan * 4; j += blockDim.x) {
+        const int q = j & 3, p = (j >> 2) % kConvSpan, dy = (j >> 2) / kConvSpan;
+        const int yy = y + dy - 1, xx = ((x0 + p - 1) % W + W) % W;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (yy >= 0 && yy < H) v = *reinterpret_cast<const uint4*>(X + ((size_t)yy * W + xx) * kNetC + 8 * q);
+        *reinterpret_cast<uint4*>(&sx[dy][p][8 * q]) = v;
+    }
+    for (int j = threadIdx.x; j < kConvTile * 4; j += blockDim.x) {
+        const int q = j & 3, m = j >> 2;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (m < n) v = *reinterpret_cast<const uint4*>(dY + ((size_t)y * W + x0 + m) * kNetC + 8 * q);
+        *reinterpret_cast<uint4*>(&sy[m][8 * q]) = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < 9 * kNetC * kNetC; j += blockDim.x) {
+        const int co = j % kNetC, ci = (j / kNetC) % kNetC, t = j / (kNetC * kNetC);
+        const int dy = t / 3, dx = t % 3;
+        float acc = 0.f;
+        for (int m = 0; m < n; m++) acc += __bfloat162float(sx[dy][m + dx][ci]) * __bfloat162float(sy[m][co]);
+        atomicAdd(dW + j, acc);
+    }
+}
+
+// dw[t][c] += sum_p s[p + off(t)] d[p][c]: the weight gradient of the lift
+// (s = its FP32 input, d = the gradient of its output) and, with the roles
+// read the other way, of the projection (s = dz at p, d = g at p + off(t)).
+// mode 0: lift, s shifted; mode 1: projection, d shifted. One block of 288
+// threads (one weight each) per row.
+__global__ void k_net_wgrad_edge(const float* s, const __nv_bfloat16* d, float* dw, int H, int W, int mode) {
+    const int y = blockIdx.x;
+    const int j = threadIdx.x;   // (t, c)
+    if (j >= 9 * kNetC) return;
+    const int t = j / kNetC, c = j % kNetC, dy = t / 3 - 1, dx = t % 3 - 1;
+    const int yy = y + dy;
+    if (yy < 0 || yy >= H) return;
+    float acc = 0.f;
+    for (int x = 0; x < W; x++) {
+        const int xs = wrapx(x + dx, W);
+        if (mode == 0) acc += s[(size_t)yy * W + xs] * __bfloat162float(d[((size_t)y * W + x) * kNetC + c]);
+        else acc += s[(size_t)y * W + x] * __bfloat162float(d[((size_t)yy * W + xs) * kNetC + c]);
+    }
+    atomicAdd(dw + j, acc);
+}
+
+// Loss of one pair: the S-norm error that the preconditioner's Galerkin step
+// leaves, S the cal_w operator in symmetric form,
+//   (S a)[k][i] = (2 cx_k + ru_k + rd_k) a - cx_k (a[i-1] + a[i+1]) - ru_k a[k+1] - rd_k a[k-1]
+// on rows k < NK (periodic in i, zero beyond the rows):
+//   L = min_g ||t - g z||_S^2 / ||t||_S^2 = 1 - a^2 / (b c),
+//   a = (z, S t), b = (z, S z), c = (t, S t),
+// independent of the scale of z, as the step is. Partials of a, b, c per block
+// in FP64; S z and S t are kept for the gradient
+//   dL/dz = 2 a / (b c) (g S z - S t), g = a / b.
+__device__ __forceinline__ double s_apply_net(const float* a, const float* op, int H, int W, int NK, int k, int i) {
+    const double cx = op[k], ru = op[H + k], rd = op[2 * H + k];
+    const size_t row = (size_t)k * W;
+    const int il = i == 0 ? W - 1 : i - 1, ir = i == W - 1 ? 0 : i + 1;
+    double y = (2.0 * cx + ru + rd) * a[row + i] - cx * ((double)a[row + il] + (double)a[row + ir]);
+    if (k + 1 < NK) y -= ru * a[row + W + i];
+    if (k > 0) y -= rd * a[row - W + i];
+    return y;
+}
+
+__global__ void k_net_loss_partial(const float* z, const float* t, const float* op, int H, int W, int NK, float* sz,
+                                   float* st, double* part) {
+    __shared__ double sh[96];
+    double v[3] = {0, 0, 0};
+    const size_t n = (size_t)H * W;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(p / W), i = (int)(p - (size_t)k * W);
+        double a = 0.0, b = 0.0;
+        if (k < NK) {
+            a = s_apply_net(z, op, H, W, NK, k, i);
+            b = s_apply_net(t, op, H, W, NK, k, i);
+            v[0] += (double)z[p] * b;
+            v[1] += (double)z[p] * a;
+            v[2] += (double)t[p] * b;
+        }
+        sz[p] = (float)a;
+        st[p] = (float)b;
+    }
+    block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = v[0];
+        part[3 * blockIdx.x + 1] = v[1];
+        part[3 * blockIdx.x + 2] = v[2];
+    }
+}
+
+__global__ void k_net_loss_final(const double* part, int nb, double* out) {   // out: [L, a, b, c]
+    __shared__ double sh[96];
+    double v[3] = {0, 0, 0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        v[0] += part[3 * b];
+        v[1] += part[3 * b + 1];
+        v[2] += part[3 * b + 2];
+    }
+    block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        out[1] = v[0];
+        out[2] = v[1];
+        out[3] = v[2];
+        out[0] = (v[1] > 0 && v[2] > 0) ? 1.0 - v[0] * v[0] / (v[1] * v[2]) : 1.0;
+    }
+}
+
+__global__ void k_net_loss_grad(const float* sz, const float* st, size_t n, const double* lt, float* dz, float mult) {
+    const double a = lt[1], b = lt[2], c = lt[3];
+    const bool ok = b > 0 && c > 0;
+    const double f = ok ? mult * 2.0 * a / (b * c) : 0.0, g = ok ? a / b : 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dz[i] = (float)(f * (g * (double)sz[i] - (double)st[i]));
+}
+
+// Adam on FP32 master weights (gradients already averaged over the batch).
+__global__ void k_net_adam(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2,
+                           float eps, float bc1, float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
 __global__ void k_f32_to_bf16(const float* x, __nv_bfloat16* y, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         y[i] = __float2bfloat16_rn(x[i]);

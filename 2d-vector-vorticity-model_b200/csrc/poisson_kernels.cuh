@@ -526,7 +526,9 @@ __global__ void __launch_bounds__(32 * kMaxSeg) k_mg_coarse_cycle(CoarseCycleArg
 // partial[block] and are finished by k_cg_scalar in a fixed order.
 
 struct CGScalars {     // device-resident scalars of one solve
-    double rz, pq, rr, bb, alpha, beta, rz_new, pad;
+    double rz, pq, rr, bb, alpha, beta, rz_new;
+    double nrm;           // ||r1||^2 scaling the learned preconditioner's input
+    double dsd, gam;      // (d, S d) and the Galerkin step (d, r1) / (d, S d) of its correction d
 };
 
 template <typename P>
@@ -619,7 +621,8 @@ __global__ void k_cg_residual(VecArgs<P> v, const P* f, const P* x, P* r, double
     if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
 }
 
-enum : int { CG_SET_BB = 0, CG_SET_RR, CG_SET_RZ, CG_PQ_ALPHA, CG_RZ_BETA };
+enum : int { CG_SET_BB = 0, CG_SET_RR, CG_SET_RZ, CG_PQ_ALPHA, CG_RZ_BETA, CG_SET_NRM, CG_FCG_BETA, CG_NET_DSD,
+             CG_NET_GAMMA };
 
 // Device-side loop state of a graph-captured solve.
 struct CGCtl {

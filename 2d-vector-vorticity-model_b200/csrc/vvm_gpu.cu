@@ -60,6 +60,10 @@ __global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mod
                 sc->beta = (sc->rz != 0.0) ? v / sc->rz : 0.0;
                 sc->rz = v;
                 break;
+            case CG_SET_NRM: sc->nrm = v; break;
+            case CG_FCG_BETA: sc->beta = (sc->pq != 0.0) ? -v / sc->pq : 0.0; break;   // -(z, q) / (p, q)
+            case CG_NET_DSD: sc->dsd = v; break;
+            case CG_NET_GAMMA: sc->gam = (sc->dsd > 0.0) ? v / sc->dsd : 0.0; break;     // (d, r1) / (d, S d)
         }
     }
 }
@@ -753,6 +757,257 @@ struct Spectral {
     }
 };
 
+// ---------------------------------------------------------------- learned net
+
+// Solver layout (FP64 [NK][pitch]) -> network layout (FP32 [H0][W0], rows
+// >= NK zero): x = (a - sub) / sqrt(*nrm2) (sub may be null); and back:
+// a += z sqrt(*nrm2).
+__global__ void k_net_in(const double* a, const double* sub, int NX, int NK, int pitch, float* x, int H0,
+                         const double* nrm2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= NX || k >= H0) return;
+    const double s = (*nrm2 > 0) ? 1.0 / sqrt(*nrm2) : 0.0;
+    const size_t e = (size_t)k * pitch + i;
+    x[(size_t)k * NX + i] = (k < NK) ? (float)((a[e] - (sub ? sub[e] : 0.0)) * s) : 0.f;
+}
+
+// White noise in the solver layout: a[k][i] = N(0, 1) from a counter hash
+// (Box-Muller on two 32-bit uniforms), seeded.
+__global__ void k_white_noise(double* a, int NX, int NK, int pitch, unsigned seed) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= NX || k >= NK) return;
+    auto mix = [](unsigned x) {
+        x ^= x >> 16;
+        x *= 0x7feb352du;
+        x ^= x >> 15;
+        x *= 0x846ca68bu;
+        x ^= x >> 16;
+        return x;
+    };
+    const unsigned id = (unsigned)(k * NX + i);
+    const unsigned h1 = mix(id * 2u + 1u + seed * 0x9E3779B9u), h2 = mix(id * 2u + 2u + seed * 0x85EBCA6Bu);
+    const double u1 = (h1 + 1.0) / 4294967297.0, u2 = h2 / 4294967296.0;
+    a[(size_t)k * pitch + i] = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+__global__ void k_net_out(const float* z, int NX, int NK, int pitch, double* a, const double* nrm2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= NX || k >= NK) return;
+    a[(size_t)k * pitch + i] = (double)z[(size_t)k * NX + i] * sqrt(*nrm2 > 0 ? *nrm2 : 0.0);
+}
+
+// z += gam d (the Galerkin-scaled network correction).
+__global__ void k_net_galerkin(int NX, int NK, int pitch, const CGScalars* sc, const double* d, double* z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= NX || k >= NK) return;
+    const size_t e = (size_t)k * pitch + i;
+    z[e] += sc->gam * d[e];
+}
+
+// The learned preconditioner (learned_kernels.cuh): a linear 4-level network,
+// lift 1 -> 32, three levels of (2x2 average pool, 3x3 conv 32 -> 32 on the
+// tensor cores), three levels of (nearest upsampling + the skip from the same
+// level, 3x3 conv), projection 32 -> 1. Level 0 is the cal_w grid padded to
+// H0 = round_up(NK, 8) rows (W0 = NX, a multiple of 8). FP32 master weights
+// with Adam; BF16 operands and activations, FP32 accumulation.
+struct LearnedNet {
+    static constexpr int kLift = 0, kConvs = 9 * kNetC, kConvSize = 9 * kNetC * kNetC;
+    static constexpr int kProj = kConvs + 6 * kConvSize, kParams = kProj + 9 * kNetC;
+    // conv order in the parameter array: D1 D2 D3 (down, levels 1-3), U2 U1 U0 (up)
+    int NX = 0, NK = 0, H[4] = {}, W[4] = {};
+    float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+    uint4 *pk = nullptr, *pkT = nullptr;       // packed forward / adjoint operands, 6 x 1152
+    float *x0 = nullptr, *z0 = nullptr, *dz = nullptr;
+    __nv_bfloat16 *h[4] = {}, *pl[4] = {}, *u[3] = {}, *gg[3] = {};
+    __nv_bfloat16 *dgb[4] = {}, *dub[3] = {}, *dpb[4] = {}, *dh3 = nullptr;
+    double *part = nullptr, *lt = nullptr;
+    float *op = nullptr, *sz = nullptr, *st = nullptr;   // rows' cx, ru, rd ([3][H0]) for the loss; S z, S t
+    int* err = nullptr;
+    int adam_t = 0;
+    Stats* stats = nullptr;
+
+    static bool supports(int NX, int NK) { return NX >= 8 && NX % 8 == 0 && NK >= 1; }
+
+    // the cal_w operator's row coefficients (cx = 1/rhow_k, ru = 1/rhou_k,
+    // rd = 1/rhou_{k-1}, k = kk + 2) in the network's rows
+    void set_operator(const std::vector<double>& rhou, const std::vector<double>& rhow) {
+        std::vector<float> h(3 * (size_t)H[0], 0.f);
+        for (int kk = 0; kk < NK; kk++) {
+            const int k = kk + 2;
+            h[kk] = (float)(1.0 / rhow[k]);
+            h[H[0] + kk] = (float)(1.0 / rhou[k]);
+            h[2 * H[0] + kk] = (float)(1.0 / rhou[k - 1]);
+        }
+        CK(cudaMemcpy(op, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+
+    void build(Arena& ar, int NXr, int NKr, int seed) {
+        NX = NXr;
+        NK = NKr;
+        H[0] = round_up(NK, 8);
+        W[0] = NX;
+        for (int l = 1; l < 4; l++) {
+            H[l] = H[l - 1] / 2;
+            W[l] = W[l - 1] / 2;
+        }
+        w = ar.alloc<float>(kParams);
+        g = ar.alloc<float>(kParams);
+        m = ar.alloc<float>(kParams);
+        v = ar.alloc<float>(kParams);
+        pk = ar.alloc<uint4>(6 * 9 * 4 * kNetC);
+        pkT = ar.alloc<uint4>(6 * 9 * 4 * kNetC);
+        const size_t n0 = (size_t)H[0] * W[0];
+        x0 = ar.alloc<float>(n0);
+        z0 = ar.alloc<float>(n0);
+        dz = ar.alloc<float>(n0);
+        for (int l = 0; l < 4; l++) {
+            const size_t nl = (size_t)H[l] * W[l] * kNetC;
+            h[l] = ar.alloc<__nv_bfloat16>(nl);
+            dgb[l] = ar.alloc<__nv_bfloat16>(nl);
+            dpb[l] = ar.alloc<__nv_bfloat16>(nl);
+            if (l > 0) pl[l] = ar.alloc<__nv_bfloat16>(nl);
+            if (l < 3) {
+                u[l] = ar.alloc<__nv_bfloat16>(nl);
+                gg[l] = ar.alloc<__nv_bfloat16>(nl);
+                dub[l] = ar.alloc<__nv_bfloat16>(nl);
+            }
+        }
+        dh3 = ar.alloc<__nv_bfloat16>((size_t)H[3] * W[3] * kNetC);
+        part = ar.alloc<double>(3 * 1024);
+        lt = ar.alloc<double>(4);
+        op = ar.alloc<float>(3 * (size_t)H[0]);
+        sz = ar.alloc<float>(n0);
+        st = ar.alloc<float>(n0);
+        err = ar.alloc<int>(1);
+        init_weights(seed);
+    }
+
+    // Seeded initial weights: N(0, 1/fan_in) per layer (fan_in = 9 inputs for
+    // the lift, 9 * 32 otherwise), so each layer keeps the signal's scale.
+    void init_weights(int seed) {
+        std::vector<float> hw(kParams);
+        uint64_t st = 0x9E3779B97F4A7C15ull ^ (uint64_t)seed;
+        auto next = [&]() {   // xorshift64*
+            st ^= st >> 12;
+            st ^= st << 25;
+            st ^= st >> 27;
+            return (double)((st * 0x2545F4914F6CDD1Dull) >> 11) * (1.0 / 9007199254740992.0);
+        };
+        auto normal = [&]() {
+            double u1 = next(), u2 = next();
+            if (u1 < 1e-300) u1 = 1e-300;
+            return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+        };
+        for (int j = 0; j < kParams; j++) {
+            const double fan = (j < kConvs || j >= kProj) ? 9.0 : 9.0 * kNetC;
+            hw[j] = (float)(normal() / std::sqrt(fan));
+        }
+        set_weights(hw.data());
+    }
+
+    void set_weights(const float* hw) {
+        CK(cudaMemcpy(w, hw, kParams * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemset(m, 0, kParams * sizeof(float)));
+        CK(cudaMemset(v, 0, kParams * sizeof(float)));
+        adam_t = 0;
+        pack(nullptr);
+        CK(cudaStreamSynchronize(nullptr));
+    }
+
+    void pack(cudaStream_t st) {
+        for (int c = 0; c < 6; c++) {
+            const float* wc = w + kConvs + (size_t)c * kConvSize;
+            LAUNCH(stats, VVM_K_LEARNED, st, k_pack_conv32<<<cdiv(9 * 4 * kNetC, 128), 128, 0, st>>>(wc, pk + (size_t)c * 1152, 0));
+            CKL();
+            LAUNCH(stats, VVM_K_LEARNED, st, k_pack_conv32<<<cdiv(9 * 4 * kNetC, 128), 128, 0, st>>>(wc, pkT + (size_t)c * 1152, 1));
+            CKL();
+        }
+    }
+
+    void conv(int c, bool adj, const __nv_bfloat16* in, __nv_bfloat16* out, int l, cudaStream_t st) {
+        ConvArgs a{in, out, (adj ? pkT : pk) + (size_t)c * 1152, H[l], W[l], err};
+        LAUNCH(stats, VVM_K_LEARNED, st, k_conv32_tc<<<H[l] * cdiv(W[l], kConvTile), kConvTile, 0, st>>>(a));
+        CKL();
+    }
+    void sum4(const __nv_bfloat16* in, __nv_bfloat16* out, int lo, float mult, cudaStream_t st) {
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_sum4<<<cdiv(H[lo] * W[lo] * 4, 256), 256, 0, st>>>(in, out, H[lo], W[lo], mult));
+        CKL();
+    }
+    void up_add(const __nv_bfloat16* lo, const __nv_bfloat16* skip, __nv_bfloat16* out, int l, float mult,
+                cudaStream_t st) {
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_up_add<<<cdiv(H[l] * W[l] * 4, 256), 256, 0, st>>>(lo, skip, out, H[l], W[l], mult));
+        CKL();
+    }
+    void wgrad(const __nv_bfloat16* X, const __nv_bfloat16* dY, int c, int l, cudaStream_t st) {
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_wgrad32<<<H[l] * cdiv(W[l], kConvTile), 256, 0, st>>>(X, dY, g + kConvs + (size_t)c * kConvSize, H[l], W[l]));
+        CKL();
+    }
+
+    // z0 = net(x0), z0 rows >= NK set to zero.
+    void forward(cudaStream_t st) {
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_lift<<<cdiv(H[0] * W[0], 128), 128, 0, st>>>(x0, w + kLift, h[0], H[0], W[0]));
+        CKL();
+        for (int l = 1; l < 4; l++) {   // down: pool, conv D_l
+            sum4(h[l - 1], pl[l], l, 0.25f, st);
+            conv(l - 1, false, pl[l], h[l], l, st);
+        }
+        const __nv_bfloat16* lower = h[3];
+        for (int l = 2; l >= 0; l--) {   // up: upsample + skip, conv U_l (index 3 + (2 - l))
+            up_add(lower, h[l], u[l], l, 1.f, st);
+            conv(3 + (2 - l), false, u[l], gg[l], l, st);
+            lower = gg[l];
+        }
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_proj<<<cdiv(H[0] * W[0], 128), 128, 0, st>>>(gg[0], w + kProj, z0, H[0], W[0], NK, 1.f));
+        CKL();
+    }
+
+    // g += d loss / d w for the gradient dz of the output (after forward()).
+    void backward(cudaStream_t st) {
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_wgrad_edge<<<H[0], 9 * kNetC, 0, st>>>(dz, gg[0], g + kProj, H[0], W[0], 1));
+        CKL();
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_proj_adj<<<cdiv(H[0] * W[0], 128), 128, 0, st>>>(dz, w + kProj, dgb[0], H[0], W[0]));
+        CKL();
+        // up path, level 0 first: du_l = U_l^T dg_l; dg_{l+1} = up^T du_l; dh_l = du_l
+        for (int l = 0; l <= 2; l++) {
+            const int c = 3 + (2 - l);
+            conv(c, true, dgb[l], dub[l], l, st);
+            wgrad(u[l], dgb[l], c, l, st);
+            sum4(dub[l], l < 2 ? dgb[l + 1] : dh3, l + 1, 1.f, st);
+        }
+        // down path, level 3 first: dp_l = D_l^T dh_l; dh_{l-1} += pool^T dp_l
+        const __nv_bfloat16* dh = dh3;
+        for (int l = 3; l >= 1; l--) {
+            conv(l - 1, true, dh, dpb[l], l, st);
+            wgrad(pl[l], dh, l - 1, l, st);
+            up_add(dpb[l], dub[l - 1], dub[l - 1], l - 1, 0.25f, st);   // dh_{l-1} lives in du_{l-1}
+            dh = dub[l - 1];
+        }
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_wgrad_edge<<<H[0], 9 * kNetC, 0, st>>>(x0, dub[0], g + kLift, H[0], W[0], 0));
+        CKL();
+    }
+
+    // loss of z0 against target t (FP32 [H0][W0]): the S-norm error left by
+    // the best multiple of z0, into lt[0]; dz = mult * dL/dz.
+    void loss(const float* t, float mult, cudaStream_t s) {
+        const size_t n = (size_t)H[0] * W[0];
+        LAUNCH(stats, VVM_K_LEARNED, s, k_net_loss_partial<<<1024, 256, 0, s>>>(z0, t, op, H[0], W[0], NK, sz, st, part));
+        CKL();
+        LAUNCH(stats, VVM_K_LEARNED, s, k_net_loss_final<<<1, 1024, 0, s>>>(part, 1024, lt));
+        CKL();
+        LAUNCH(stats, VVM_K_LEARNED, s, k_net_loss_grad<<<1024, 256, 0, s>>>(sz, st, n, lt, dz, mult));
+        CKL();
+    }
+
+    void adam(float lr, cudaStream_t st) {
+        adam_t++;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float bc1 = 1.f - std::pow(b1, (float)adam_t), bc2 = 1.f - std::pow(b2, (float)adam_t);
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_adam<<<cdiv(kParams, 256), 256, 0, st>>>(w, g, m, v, kParams, lr, b1, b2, 1e-8f, bc1, bc2));
+        CKL();
+        pack(st);
+    }
+};
+
 // Preconditioned CG on S d = g in precision P with the level-0 vectors below.
 template <typename P>
 struct PCG {
@@ -919,6 +1174,14 @@ struct vvm_gpu_ctx {
     bool mixed = false;
     bool spectral = false;   // VVM_SOLVER_SPECTRAL
     int tune_gs_cs = 0;      // cap on the CTAs of a Gauss-Seidel cluster (0: automatic)
+    // learned preconditioner (VVM_SOLVER_LEARNED)
+    std::unique_ptr<LearnedNet> net;
+    double* z64 = nullptr;   // preconditioned residual, solver layout
+    double *za64 = nullptr, *r164 = nullptr, *d64 = nullptr, *sd64 = nullptr;   // the learned cycle's work arrays
+    int learned_mode = 0;    // 0: the cycle with the network; 1: without it; 2: identity
+    int learned_cap = 200;   // flexible-CG iterations before the multigrid-PCG fallback
+    int learned_iters = 0, learned_fallback = 0;
+    bool learned_collect = false;   // training-pair collection: solve with the plain solver
     int tune_fft = 0;        // threads of a row-FFT block (0: automatic)
     Arena ar;
     Fields<double> f64;
@@ -1295,6 +1558,119 @@ double read_scalar(vvm_gpu_ctx* c, const double* dptr) {
     return *c->sc_host;
 }
 
+void ensure_learned(vvm_gpu_ctx* c) {
+    ensure_poisson(c);
+    if (c->net) return;
+    const int NX = c->d.nx - 2, NK = c->d.nz - 3;
+    if (!LearnedNet::supports(NX, NK)) throw CudaError{"learned preconditioner: NX must be a multiple of 8"};
+    c->net.reset(new LearnedNet());
+    c->net->stats = &c->stats;
+    c->net->build(c->ar, NX, NK, 1);
+    c->net->set_operator(c->h_rhou, c->h_rhow);
+    const size_t n = (size_t)NK * c->pcg64->pitch;
+    c->z64 = c->ar.alloc<double>(n);
+    c->za64 = c->ar.alloc<double>(n);
+    c->r164 = c->ar.alloc<double>(n);
+    c->d64 = c->ar.alloc<double>(n);
+    c->sd64 = c->ar.alloc<double>(n);
+}
+
+// z64 = M r: a two-level cycle whose coarse correction is the network.
+//   za = L r                      (L: the exact z-line solve, the multigrid's
+//                                  level-0 line operator)
+//   r1 = r - S za
+//   d  = ||r1|| net(r1 / ||r1||)  (BF16 operands; trained on e1 = S^{-1} r1)
+//   za += gam d, gam = (d, r1) / (d, S d)
+//   z  = za + L (r - S za)
+// gam minimises the S-norm error of za along d, so an application is never
+// worse than the same cycle without the network, whatever the network says.
+// Mode 1 runs the cycle without the network (the method without it), mode 2
+// is the identity.
+void learned_precond(vvm_gpu_ctx* c, const double* r, cudaStream_t st) {
+    PCG<double>& P = *c->pcg64;
+    LearnedNet& N = *c->net;
+    VecArgs<double> v = P.vargs();
+    dim3 B = P.block(), G = P.grid();
+    if (c->learned_mode == 2) {
+        CK(cudaMemcpyAsync(c->z64, r, (size_t)P.NK * P.pitch * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        return;
+    }
+    P.mg.sweep(0, r, nullptr, nullptr, 0, 0, c->za64, 1.0, st);
+    if (c->learned_mode == 0) {
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, r, c->za64, c->r164, P.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->r164, c->r164, P.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_NRM));
+        CKL();
+        dim3 g0(cdiv(P.NX, 64), cdiv(N.H[0], 4));
+        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->r164, nullptr, P.NX, P.NK, P.pitch, N.x0, N.H[0], &P.sc->nrm));
+        CKL();
+        N.forward(st);
+        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_out<<<G, B, 0, st>>>(N.z0, P.NX, P.NK, P.pitch, c->d64, &P.sc->nrm));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_spmv<double><<<G, B, 0, st>>>(v, c->d64, c->sd64, P.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_NET_DSD));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->d64, c->r164, P.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_NET_GAMMA));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_galerkin<<<G, B, 0, st>>>(P.NX, P.NK, P.pitch, P.sc, c->d64, c->za64));
+        CKL();
+    }
+    P.mg.sweep(0, r, c->za64, nullptr, 0, 0, c->z64, 1.0, st);
+}
+
+// Flexible CG (the direction's coefficient beta = -(z, q_prev) / (p, q)_prev,
+// exact for a preconditioner that varies or is not symmetric) on S W = Wf
+// from W = 0, preconditioned by learned_precond, to the FP64 residual
+// ||rhow r||^2 <= tol^2 bb. Returns the iterations, or -cap if not converged.
+int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) {
+    PCG<double>& P = *c->pcg64;
+    VecArgs<double> v = P.vargs();
+    dim3 B = P.block(), G = P.grid();
+    cudaStream_t st = c->stream;
+    CK(cudaMemsetAsync(c->W, 0, (size_t)P.NK * P.pitch * sizeof(double), st));
+    LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P.r, P.partial));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RR));
+    CKL();
+    double rr = P.read_rr(st);
+    const double stop2 = tol * tol * bb;
+    *relres = std::sqrt(rr / bb);
+    if (!(rr > stop2)) return 0;
+    for (int it = 1; it <= cap; it++) {
+        learned_precond(c, P.r, st);
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, P.r, c->z64, P.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RZ));
+        CKL();
+        if (it > 1) {
+            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->z64, P.q, P.partial));
+            CKL();
+            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_FCG_BETA));
+            CKL();
+        }
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dir<double><<<G, B, 0, st>>>(v, P.sc, c->z64, P.p, it == 1 ? 1 : 0));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_spmv<double><<<G, B, 0, st>>>(v, P.p, P.q, P.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_PQ_ALPHA));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_update<double><<<G, B, 0, st>>>(v, P.sc, c->W, P.r, P.p, P.q, P.partial));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RR));
+        CKL();
+        rr = P.read_rr(st);
+        *relres = std::sqrt(rr / bb);
+        if (!(rr > stop2)) return it;
+        if (!std::isfinite(rr)) break;
+    }
+    return -cap;
+}
+
 // Solves S W = Wf (FP64 rhs in c->Wf, ||b||^2 = bb) into c->W.
 int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
     int maxit = c->desc.poisson_maxit > 0 ? c->desc.poisson_maxit : 200;
@@ -1303,6 +1679,19 @@ int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
         c->last_iters = 0;
         c->last_relres = 0.0;
         return VVM_GPU_OK;
+    }
+    if (c->desc.solver == VVM_SOLVER_LEARNED && !c->learned_collect) {
+        ensure_learned(c);
+        double rel = 0;
+        int it = fcg_learned(c, bb, tol, c->learned_cap, &rel);
+        c->learned_fallback = (it < 0) ? 1 : 0;
+        c->learned_iters = (it < 0) ? c->learned_cap : it;
+        if (it < 0) {   // the plain multigrid-PCG takes over from the current iterate
+            it = c->learned_cap + c->pcg64->solve(c->Wf, c->W, true, bb, tol, maxit, c->stream, &rel);
+        }
+        c->last_iters = it;
+        c->last_relres = rel;
+        return (rel <= tol) ? VVM_GPU_OK : VVM_GPU_ENOCONV;
     }
     if (c->spectral) {   // direct solve W = S^{-1} f, checked; CG from there if the check fails
         double rel = 0;
@@ -2244,6 +2633,8 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     c->device = device;
     c->mixed = (D.precision == VVM_PREC_MIXED);
     c->spectral = (D.solver == VVM_SOLVER_SPECTRAL);
+    // the learned solver's iterations are checked on the host (no graph)
+    c->graphs_off = (D.solver == VVM_SOLVER_LEARNED);
     int prev = 0;
     cudaGetDevice(&prev);
     try {
@@ -2561,6 +2952,175 @@ int vvm_gpu_conv3x3_c32(const float* x, const float* w, float* y, int H, int W, 
     }
     cudaSetDevice(prev);
     return rc;
+}
+
+int vvm_gpu_learned_shape(vvm_gpu_ctx* ctx, int* H0, int* W0, int* nparams) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    const int NX = ctx->d.nx - 2, NK = ctx->d.nz - 3;
+    if (!LearnedNet::supports(NX, NK)) return fail(ctx, VVM_GPU_EINVAL, "learned: NX must be a multiple of 8");
+    if (H0) *H0 = round_up(NK, 8);
+    if (W0) *W0 = NX;
+    if (nparams) *nparams = LearnedNet::kParams;
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_learned_weights(vvm_gpu_ctx* ctx, float* get, const float* set, int n) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    if (n != LearnedNet::kParams) return fail(ctx, VVM_GPU_EINVAL, "learned_weights: wrong parameter count");
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        ensure_learned(ctx);
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (set) ctx->net->set_weights(set);
+        if (get) CK(cudaMemcpy(get, ctx->net->w, n * sizeof(float), cudaMemcpyDeviceToHost));
+        return VVM_GPU_OK;
+    });
+}
+
+// Network input x and target t as host [H0][W0] FP32; out: z = net(x) (if
+// z), the gradient of L = ||z - t||^2 / ||t||^2 with respect to the weights
+// (if grad and t) and L.
+int vvm_gpu_learned_eval(vvm_gpu_ctx* ctx, const float* x, const float* t, float* z, float* grad, double* loss) {
+    if (!ctx || !x) return VVM_GPU_EINVAL;
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        ensure_learned(ctx);
+        LearnedNet& N = *ctx->net;
+        cudaStream_t st = ctx->stream;
+        const size_t n0 = (size_t)N.H[0] * N.W[0];
+        CK(cudaMemcpyAsync(N.x0, x, n0 * sizeof(float), cudaMemcpyHostToDevice, st));
+        N.forward(st);
+        if (z) CK(cudaMemcpyAsync(z, N.z0, n0 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (t) {
+            Arena tmp;
+            float* td = tmp.alloc<float>(n0);
+            CK(cudaMemcpyAsync(td, t, n0 * sizeof(float), cudaMemcpyHostToDevice, st));
+            CK(cudaMemsetAsync(N.g, 0, LearnedNet::kParams * sizeof(float), st));
+            N.loss(td, 1.f, st);
+            N.backward(st);
+            if (grad) CK(cudaMemcpyAsync(grad, N.g, LearnedNet::kParams * sizeof(float), cudaMemcpyDeviceToHost, st));
+            double lt[2];
+            CK(cudaMemcpyAsync(lt, N.lt, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (loss) *loss = lt[0];
+        }
+        CK(cudaStreamSynchronize(st));
+        int h = 0;
+        CK(cudaMemcpy(&h, N.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) return fail(ctx, VVM_GPU_ECUDA, "learned: an MMA completion wait gave up");
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, double lr, int seed,
+                          double* loss_first, double* loss_last) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    if (npairs < 1 || steps < 0 || batch < 1 || !(lr > 0))
+        return fail(ctx, VVM_GPU_EINVAL, "learned_train: bad arguments");
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        ensure_learned(ctx);
+        vvm_gpu_ctx* c = ctx;
+        LearnedNet& N = *c->net;
+        PCG<double>& P = *c->pcg64;
+        cudaStream_t st = c->stream;
+        const size_t n0 = (size_t)N.H[0] * N.W[0];
+        Arena tmp;
+        float* px = tmp.alloc<float>(n0 * npairs);
+        float* pt = tmp.alloc<float>(n0 * npairs);
+        // pairs (f, W) of the model's own steps, solved by the plain solver;
+        // the state is put back afterwards
+        Snapshot snap;
+        snap.take(c);
+        c->learned_collect = true;
+        VecArgs<double> v = P.vargs();
+        dim3 B = P.block(), G = P.grid(), g0(cdiv(P.NX, 64), cdiv(N.H[0], 4));
+        int rc = VVM_GPU_OK;
+        const int nmodel = (npairs + 1) / 2;   // the rest: white-noise right-hand sides
+        for (int i = 0; i < npairs && rc == VVM_GPU_OK; i++) {
+            if (i < nmodel) {
+                rc = c->mixed ? step_once<float>(c) : step_once<double>(c);
+            } else {   // the residuals flexible CG meets are rough: noise, solved by the plain solver
+                LAUNCH(&c->stats, VVM_K_LEARNED, st, k_white_noise<<<G, B, 0, st>>>(c->Wf, P.NX, P.NK, P.pitch, (unsigned)(seed * 7919 + i)));
+                CKL();
+                double rel = 0;
+                P.solve(c->Wf, c->W, false, -1.0, 1e-10, 400, st, &rel);
+            }
+            // what the line solve leaves: input r1 = f - S L f, target
+            // e1 = W - L f = S^{-1} r1, both over ||r1||
+            P.mg.sweep(0, c->Wf, nullptr, nullptr, 0, 0, c->z64, 1.0, st);
+            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->z64, c->r164, P.partial));
+            CKL();
+            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->r164, c->r164, P.partial));
+            CKL();
+            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_NRM));
+            CKL();
+            LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->r164, nullptr, P.NX, P.NK, P.pitch, px + n0 * i, N.H[0], &P.sc->nrm));
+            CKL();
+            LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->W, c->z64, P.NX, P.NK, P.pitch, pt + n0 * i, N.H[0], &P.sc->nrm));
+            CKL();
+        }
+        c->learned_collect = false;
+        CK(cudaStreamSynchronize(st));
+        snap.restore(c);
+        c->drop_graphs();
+        if (rc != VVM_GPU_OK) return rc;
+        // Adam over random mini-batches of the pairs
+        uint64_t s64 = 0x853C49E6748FEA9Bull ^ (uint64_t)(unsigned)seed;
+        auto pick = [&]() {
+            s64 ^= s64 << 13;
+            s64 ^= s64 >> 7;
+            s64 ^= s64 << 17;
+            return (int)(s64 % (uint64_t)npairs);
+        };
+        double* hl = nullptr;
+        CK(cudaMallocHost(&hl, 2 * sizeof(double)));
+        const int probe = std::min(steps, 10);
+        double first = 0, last = 0;
+        for (int s = 0; s < steps; s++) {
+            CK(cudaMemsetAsync(N.g, 0, LearnedNet::kParams * sizeof(float), st));
+            double lsum = 0;
+            const bool watch = (s < probe) || (s >= steps - probe);
+            for (int b = 0; b < batch; b++) {
+                const int i = pick();
+                CK(cudaMemcpyAsync(N.x0, px + n0 * i, n0 * sizeof(float), cudaMemcpyDeviceToDevice, st));
+                N.forward(st);
+                N.loss(pt + n0 * i, 1.f / batch, st);
+                N.backward(st);
+                if (watch) {
+                    CK(cudaMemcpyAsync(hl, N.lt, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    lsum += hl[0];
+                }
+            }
+            N.adam((float)lr, st);
+            if (s < probe) first += lsum / batch / probe;
+            if (s >= steps - probe) last += lsum / batch / probe;
+        }
+        CK(cudaStreamSynchronize(st));
+        cudaFreeHost(hl);
+        if (loss_first) *loss_first = first;
+        if (loss_last) *loss_last = last;
+        int h = 0;
+        CK(cudaMemcpy(&h, N.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) return fail(ctx, VVM_GPU_ECUDA, "learned: an MMA completion wait gave up");
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_learned_config(vvm_gpu_ctx* ctx, int mode, int cap) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    if (mode < 0 || mode > 2 || cap < 1) return fail(ctx, VVM_GPU_EINVAL, "learned_config: bad arguments");
+    ctx->learned_mode = mode;
+    ctx->learned_cap = cap;
+    return VVM_GPU_OK;
+}
+
+int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back) {
+    if (!ctx) return VVM_GPU_EINVAL;
+    if (fcg_iters) *fcg_iters = ctx->learned_iters;
+    if (fell_back) *fell_back = ctx->learned_fallback;
+    return VVM_GPU_OK;
 }
 
 int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_cluster_ctas, int fft_threads) {

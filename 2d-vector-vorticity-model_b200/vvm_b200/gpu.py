@@ -77,7 +77,9 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_set_tuning", "vvm_gpu_get_tuning", "vvm_gpu_batch_create", "vvm_gpu_batch_destroy",
            "vvm_gpu_batch_case", "vvm_gpu_batch_step", "vvm_gpu_batch_synchronize",
            "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream",
-           "vvm_gpu_conv3x3_c32") + tuple(
+           "vvm_gpu_conv3x3_c32", "vvm_gpu_learned_shape", "vvm_gpu_learned_weights",
+           "vvm_gpu_learned_eval", "vvm_gpu_learned_train", "vvm_gpu_learned_config",
+           "vvm_gpu_learned_last") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -124,6 +126,12 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
     _fp = ctypes.POINTER(ctypes.c_float)
     L.vvm_gpu_conv3x3_c32.argtypes = [_fp, _fp, _fp, ip, ip, ip, ip]
+    L.vvm_gpu_learned_shape.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.vvm_gpu_learned_weights.argtypes = [vp, _fp, _fp, ip]
+    L.vvm_gpu_learned_eval.argtypes = [vp, _fp, _fp, _fp, _fp, _dp]
+    L.vvm_gpu_learned_train.argtypes = [vp, ip, ip, ip, ctypes.c_double, ip, _dp, _dp]
+    L.vvm_gpu_learned_config.argtypes = [vp, ip, ip]
+    L.vvm_gpu_learned_last.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -356,6 +364,51 @@ class VVMGpu:
     def tuning(self) -> tuple[int, int]:
         a, b = ctypes.c_int(), ctypes.c_int()
         self._check(self.L.vvm_gpu_get_tuning(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    # -- learned preconditioner (VVM_SOLVER_LEARNED) -----------------------
+    def learned_shape(self) -> tuple[int, int, int]:
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.vvm_gpu_learned_shape(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def learned_weights(self, new: np.ndarray | None = None) -> np.ndarray:
+        fp = ctypes.POINTER(ctypes.c_float)
+        n = self.learned_shape()[2]
+        out = np.empty(n, dtype=np.float32)
+        src = None if new is None else np.ascontiguousarray(new, dtype=np.float32)
+        self._check(self.L.vvm_gpu_learned_weights(self.h, out.ctypes.data_as(fp),
+                                                   None if src is None else src.ctypes.data_as(fp), n))
+        return out
+
+    def learned_eval(self, x: np.ndarray, t: np.ndarray | None = None):
+        """z = net(x); with t also (dL/dweights, L)."""
+        fp = ctypes.POINTER(ctypes.c_float)
+        H0, W0, n = self.learned_shape()
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(H0, W0)
+        z = np.empty((H0, W0), dtype=np.float32)
+        grad = np.empty(n, dtype=np.float32) if t is not None else None
+        tt = None if t is None else np.ascontiguousarray(t, dtype=np.float32).reshape(H0, W0)
+        loss = ctypes.c_double()
+        self._check(self.L.vvm_gpu_learned_eval(self.h, x.ctypes.data_as(fp),
+                                                None if tt is None else tt.ctypes.data_as(fp),
+                                                z.ctypes.data_as(fp),
+                                                None if grad is None else grad.ctypes.data_as(fp),
+                                                ctypes.byref(loss)))
+        return (z, grad, loss.value) if t is not None else z
+
+    def learned_train(self, npairs: int, steps: int, batch: int = 4, lr: float = 1e-3, seed: int = 0):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.vvm_gpu_learned_train(self.h, int(npairs), int(steps), int(batch), float(lr),
+                                                 int(seed), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def learned_config(self, mode: int = 0, cap: int = 200):
+        self._check(self.L.vvm_gpu_learned_config(self.h, int(mode), int(cap)))
+
+    def learned_last(self) -> tuple[int, int]:
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.vvm_gpu_learned_last(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
     def last_solve(self):

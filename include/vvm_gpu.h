@@ -50,7 +50,7 @@ extern "C" {
 /* Preconditioner of the Poisson CG (cal_w). */
 #define VVM_SOLVER_MGPCG 0    /* geometric multigrid: x-semicoarsening, z-line relaxation */
 #define VVM_SOLVER_LEARNED 1  /* learned BF16 conv preconditioner in flexible CG,
-                                 multigrid-PCG as fallback */
+                                 multigrid-PCG as fallback (vvm_gpu_learned_*) */
 #define VVM_SOLVER_SPECTRAL 2 /* exact Fourier-mode solve (row FFTs in x, one
                                  tridiagonal z solve per mode) applied directly in
                                  FP64, its residual checked, FP64 CG preconditioned
@@ -177,6 +177,48 @@ int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres);
  * Failures: vvm_gpu_last_error(NULL, ...). */
 int vvm_gpu_conv3x3_c32(const float* x, const float* w, float* y, int H, int W, int adjoint, int device);
 
+/* -- learned preconditioner (VVM_SOLVER_LEARNED) -------------------------------
+ * No counterpart in the reference. The preconditioner is a two-level cycle
+ * whose coarse correction is learned: the exact z-line solve L of the
+ * residual r (the multigrid's finest line operator), za = L r; the network
+ * on what it leaves, r1 = r - S za, giving d = ||r1|| net(r1 / ||r1||); the
+ * Galerkin step za += gam d, gam = (d, r1) / (d, S d), which minimises the
+ * S-norm error along d, so that a poor network can slow nothing down; and a
+ * second line solve, z = za + L (r - S za). The network is linear, 4 levels
+ * of 3x3 convolutions (lift 1 -> 32 channels, three levels down by 2x2
+ * average pooling and three up by nearest upsampling with skips, projection
+ * 32 -> 1; the 32 -> 32 convolutions on the tensor cores, BF16 weights and
+ * activations, FP32 accumulation). Its grid is the cal_w grid padded to H0 = round_up(NZ-1, 8)
+ * rows by W0 = NX columns (NX a multiple of 8); arrays of it are [H0][W0].
+ * The solve is flexible CG from W = 0 to the same FP64 residual as the other
+ * solvers; after `cap` iterations the multigrid PCG takes over from the
+ * current iterate. Weights: nparams FP32 values (vvm_gpu_learned_shape), the
+ * lift [9][32], six convolutions [9 taps][32 in][32 out] (down at levels 1,
+ * 2, 3, up at levels 2, 1, 0) and the projection [9][32]; seeded initial
+ * values until set or trained.
+ *   _weights: copies them out (get) and/or in (set).
+ *   _eval: z = net(x); with t, the loss L = 1 - (z, S t)^2 / ((z, S z)(t, S t))
+ *     (the S-norm error of t left by the best multiple of z, relative to
+ *     ||t||_S^2; S the cal_w operator in symmetric form on the rows < NZ-1)
+ *     and dL/dweights.
+ *   _train: collects npairs pairs from the model's own next steps solved by
+ *     the plain solver (the state is put back afterwards) and as many from
+ *     white-noise right-hand sides: input r1 / ||r1||, r1 = rhs - S L rhs,
+ *     target (W - L rhs) / ||r1|| = S^{-1} r1 / ||r1||; then runs
+ *     `steps` Adam steps (learning rate lr) on random mini-batches of `batch`
+ *     pairs; returns the mean loss of the first and the last ten steps.
+ *   _config: mode 0 = the cycle with the network, 1 = the same cycle without
+ *     it (two line solves: the method without the network), 2 = identity;
+ *     cap = iterations before the multigrid fallback (default 200).
+ *   _last: flexible-CG iterations of the last solve, and whether it fell back. */
+int vvm_gpu_learned_shape(vvm_gpu_ctx* ctx, int* H0, int* W0, int* nparams);
+int vvm_gpu_learned_weights(vvm_gpu_ctx* ctx, float* get, const float* set, int n);
+int vvm_gpu_learned_eval(vvm_gpu_ctx* ctx, const float* x, const float* t, float* z, float* grad, double* loss);
+int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, double lr, int seed,
+                          double* loss_first, double* loss_last);
+int vvm_gpu_learned_config(vvm_gpu_ctx* ctx, int mode, int cap);
+int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back);
+
 /* -- launch-shape knobs --------------------------------------------------------
  * Neither changes any result (the arithmetic of every cell is the same):
  * gs_cluster_ctas caps the CTAs of each Gauss-Seidel cluster (1, 2, 4, 8; the
@@ -267,7 +309,8 @@ int vvm_gpu_poisson_solve_noalloc(int NX, int NZ, const double* rhou, const doub
 #define VVM_K_RKM 11        /* eddy coefficients */
 #define VVM_K_GS 12         /* Gauss-Seidel diffusion (+ nudging) */
 #define VVM_K_MEAN 13       /* updateMean, nudging passes, transfers */
-#define VVM_K_COUNT 14
+#define VVM_K_LEARNED 14    /* learned preconditioner: network forward, training */
+#define VVM_K_COUNT 15
 int vvm_gpu_profile(vvm_gpu_ctx* ctx, int enable);
 /* Accumulated device milliseconds and launches of one kernel class. */
 int vvm_gpu_profile_read(vvm_gpu_ctx* ctx, int kernel_class, double* ms, long long* launches);
