@@ -17,6 +17,7 @@
 // in 32 TMEM columns; each warp reads back its 32 lanes (pixels).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "vvm_common.cuh"
@@ -174,6 +175,264 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_tc(ConvArgs a) {
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// The same convolution for rows of at least kCBox pixels, streamed: a CTA
+// owns a strip of 128 pixels of R consecutive output rows and keeps the
+// input rows it needs in a ring of kCSlots shared-memory slots, so every
+// input row is read from global memory once per strip and the packed weights
+// once per CTA (against three rows and all weights per 128 output pixels in
+// k_conv32_tc).
+//
+// Loads are TMA (cp.async.bulk.tensor, no multicast) from a 3D tensor map of
+// the activations, dims {32 channels, W, H}: one box {8 channels, 144
+// pixels, 1 row} per 8-channel chunk lands as that chunk's canonical K-major
+// rows (pixel p at 16 p bytes) for pixels x0-8 .. x0+135, so tap dx of
+// output pixel x0+m reads box pixel 7+dx+m. The box is zero outside the
+// tensor, which gives the zero rows y = -1 and y = H; the periodic pixels
+// x0-1 = W-1 (first strip) and x0+128 = W (last strip) come from a second
+// map with 8-pixel boxes and are copied into place in shared memory.
+//
+// Thread 0 issues loads and MMAs; all four warps read the accumulator back.
+// Input row j goes to slot j % kCSlots; it is read by output rows j-2..j, so
+// the slot of row r-1 is refilled with row r-1+kCSlots once output r-1's MMAs
+// are done, kCSlots-3 rows ahead of its use.
+// Two TMEM accumulators (32 columns each) let the MMAs of row r run while row
+// r-1 is written out. Barriers: full[slot] (TMA bytes of an input row),
+// done[b] (MMAs of the row in accumulator b, by tcgen05.commit), empty[b]
+// (accumulator b read back, one arrive per warp). Every wait is bounded; a
+// wait that gives up sets kNetErrWait and an abort flag that ends the CTA's
+// remaining work, after a bounded wait for the copies and MMAs in flight.
+constexpr int kCSlots = 8;                        // 3 rows in use + 5 rows of prefetch
+constexpr int kCBox = 144;
+constexpr int kCRowBytes = kCBox * 16;            // one 8-channel chunk of a row
+constexpr int kCSlotBytes = 4 * kCRowBytes;       // 9216
+constexpr int kCWBytes = 9 * 4 * kNetC * 16;      // packed weights, 18432
+constexpr int kCWrapBytes = 2 * 4 * 8 * 16;       // [side][chunk][8 pixels], 1024 a slot
+constexpr int kCBars = kCSlots + 2 + 2 + 1;       // full[4], done[2], empty[2], weights
+constexpr int kConvStreamSmem = 128 + kCWBytes + kCSlots * (kCSlotBytes + kCWrapBytes) + 8 * kCBars + 16;
+
+struct ConvStreamArgs {
+    const __nv_bfloat16* in;   // [H][W][32] (the tensor maps' tensor)
+    __nv_bfloat16* out;        // [H][W][32]
+    const uint4* w;            // packed B operand, as for k_conv32_tc
+    int H, W, R;               // R: output rows per CTA
+    int* err;
+};
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on one phase of an mbarrier; gives up early when *abort is set.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+    for (int it = 0; it < kMmaSpinLimit; it++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255) == 255 && *abort) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kConvTile) k_conv32_stream(const __grid_constant__ CUtensorMap trow,
+                                                             const __grid_constant__ CUtensorMap twrap,
+                                                             ConvStreamArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    uint8_t* base = smem_raw + (((raw + 127) & ~127u) - raw);
+    uint8_t* sB = base;
+    uint8_t* sA = sB + kCWBytes;                                   // [slot][chunk][144 pixels]
+    uint8_t* sW = sA + kCSlots * kCSlotBytes;                      // [slot][side][chunk][8 pixels]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sW + kCSlots * kCWrapBytes);
+    volatile int* abort = reinterpret_cast<volatile int*>(bars + kCBars);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kCBars) + 1;
+    const uint32_t full0 = smem_u32(bars), done0 = full0 + 8 * kCSlots, empty0 = done0 + 16, wbar = empty0 + 16;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int strips = (a.W + kConvTile - 1) / kConvTile;
+    const int x0 = (blockIdx.x % strips) * kConvTile;
+    const int y0 = (blockIdx.x / strips) * a.R;
+    const int R = min(a.R, a.H - y0);
+    const int nin = R + 2;                       // input rows y0-1 .. y0+R
+    const bool left = x0 == 0, right = x0 + kConvTile >= a.W;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(64)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < kCBars; i++) {
+            const uint32_t cnt = (i >= kCSlots + 2 && i < kCSlots + 4) ? 4u : 1u;   // empty[]: one per warp
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full0 + 8 * i), "r"(cnt) : "memory");
+        }
+        *abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    int issued = 0, consumed = 0, committed = 0;   // thread 0's bookkeeping
+    auto load_row = [&](int j) {
+        const int sl = j % kCSlots, y = y0 - 1 + j;
+        const uint32_t bar = full0 + 8 * sl;
+        const uint32_t bytes = kCSlotBytes + (left ? 512u : 0u) + (right ? 512u : 0u);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        for (int kc = 0; kc < 4; kc++) {
+            tma_load_3d(smem_u32(sA + sl * kCSlotBytes + kc * kCRowBytes), &trow, kc * 8, x0 - 8, y, bar);
+            if (left) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + kc * 128), &twrap, kc * 8, a.W - 8, y, bar);
+            if (right) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + 512 + kc * 128), &twrap, kc * 8, 0, y, bar);
+        }
+        issued = j + 1;
+    };
+    auto take_row = [&](int j) -> bool {   // wait for input row j, then put its periodic pixels in place
+        const int sl = j % kCSlots;
+        if (!mbar_wait(full0 + 8 * sl, (uint32_t)((j / kCSlots) & 1), abort)) return false;
+        consumed = j + 1;
+        uint4* A = reinterpret_cast<uint4*>(sA + sl * kCSlotBytes);
+        const uint4* Wr = reinterpret_cast<const uint4*>(sW + sl * kCWrapBytes);
+        for (int kc = 0; kc < 4; kc++) {
+            if (left) A[kc * kCBox + 7] = Wr[kc * 8 + 7];
+            if (right) A[kc * kCBox + (a.W - x0 + 8)] = Wr[32 + kc * 8];
+        }
+        return true;
+    };
+
+    if (tid == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(wbar), "r"(kCWBytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_u32(sB)),
+                     "l"(reinterpret_cast<uint64_t>(a.w)), "r"(kCWBytes), "r"(wbar)
+                     : "memory");
+        for (int j = 0; j < min(kCSlots, nin); j++) load_row(j);
+    }
+    bool wdone = false;
+    for (int r = 0; r <= R; r++) {
+        if (r < R && tid == 0 && !*abort) {
+            bool ok = true;
+            if (r == 0) {
+                ok = mbar_wait(wbar, 0, abort);
+                wdone = ok;
+                for (int j = 0; j < 3 && ok; j++) ok = take_row(j);
+            } else {
+                ok = take_row(r + 2);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the copied pixels, for the MMAs
+            const int b = r & 1;
+            if (ok && r >= 2) ok = mbar_wait(empty0 + 8 * b, (uint32_t)(((r - 2) >> 1) & 1), abort);
+            if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                uint32_t acc = 0;
+                for (int dy = 0; dy < 3; dy++) {
+                    const uint8_t* row = sA + ((r + dy) % kCSlots) * kCSlotBytes;
+                    for (int dx = 0; dx < 3; dx++)
+                        for (int ks = 0; ks < 2; ks++) {
+                            const uint64_t ad = umma_desc(smem_u32(row + (2 * ks) * kCRowBytes + (7 + dx) * 16), kCRowBytes, 128);
+                            const uint64_t bd = umma_desc(smem_u32(sB + ((dy * 3 + dx) * 4 + 2 * ks) * kNetC * 16), kNetC * 16, 128);
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(
+                                    tmem + 32u * b),
+                                "l"(ad), "l"(bd), "r"(kConvIdesc), "r"(acc), "r"(0u)
+                                : "memory");
+                            acc = 1;
+                        }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 done0 + 8 * b)
+                             : "memory");
+                committed = r + 1;
+                // input row r-1+kCSlots reuses the slot of row r-1, free once
+                // output r-1's MMAs are done
+                const int jn = r - 1 + kCSlots;
+                if (r >= 1 && jn < nin) {
+                    ok = mbar_wait(done0 + 8 * ((r - 1) & 1), (uint32_t)(((r - 1) >> 1) & 1), abort);
+                    if (ok) load_row(jn);
+                }
+            }
+            if (!ok) {
+                if (a.err) atomicOr(a.err, kNetErrWait);
+                *abort = 1;
+            }
+        }
+        __syncwarp();
+        if (r >= 1) {   // write out output row r-1
+            const int q = r - 1, b = q & 1;
+            bool got = !*abort && mbar_wait(done0 + 8 * b, (uint32_t)((q >> 1) & 1), abort);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            got = __all_sync(0xffffffffu, got);
+            uint32_t v[32];
+            if (got) {
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(tmem + ((uint32_t)(warp * 32) << 16) + 32u * b)
+                    : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(empty0 + 8 * b) : "memory");
+            const int x = x0 + tid;
+            if (got && x < a.W) {
+                uint4* dst = reinterpret_cast<uint4*>(a.out + ((size_t)(y0 + q) * a.W + x) * kNetC);
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    __nv_bfloat162 h0 = __floats2bfloat162_rn(__uint_as_float(v[8 * c + 0]), __uint_as_float(v[8 * c + 1]));
+                    __nv_bfloat162 h1 = __floats2bfloat162_rn(__uint_as_float(v[8 * c + 2]), __uint_as_float(v[8 * c + 3]));
+                    __nv_bfloat162 h2 = __floats2bfloat162_rn(__uint_as_float(v[8 * c + 4]), __uint_as_float(v[8 * c + 5]));
+                    __nv_bfloat162 h3 = __floats2bfloat162_rn(__uint_as_float(v[8 * c + 6]), __uint_as_float(v[8 * c + 7]));
+                    uint4 o;
+                    o.x = *reinterpret_cast<uint32_t*>(&h0);
+                    o.y = *reinterpret_cast<uint32_t*>(&h1);
+                    o.z = *reinterpret_cast<uint32_t*>(&h2);
+                    o.w = *reinterpret_cast<uint32_t*>(&h3);
+                    dst[c] = o;
+                }
+            }
+        }
+    }
+    // after an abort: wait (bounded) for the copies and MMAs still in flight
+    // before the shared memory and TMEM go away
+    if (tid == 0 && *abort) {
+        volatile int never = 0;
+        if (!wdone) mbar_wait(wbar, 0, &never);
+        for (int j = consumed; j < issued; j++) mbar_wait(full0 + 8 * (j % kCSlots), (uint32_t)((j / kCSlots) & 1), &never);
+        if (committed > 0) {
+            const int q = committed - 1;
+            mbar_wait(done0 + 8 * (q & 1), (uint32_t)((q >> 1) & 1), &never);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+}
+
 // Packs FP32 weights w[tap][in][out] into the B operand of k_conv32_tc:
 // [tap][in / 8][out] of 8 consecutive inputs in BF16. With flip, the packed
 // operand is that of the adjoint convolution: tap 8 - t, in and out swapped.
@@ -224,9 +483,16 @@ __device__ __forceinline__ void bf16x8_store(__nv_bfloat16* p, const float (&v)[
 __device__ __forceinline__ int wrapx(int x, int W) { return x < 0 ? x + W : (x >= W ? x - W : x); }
 
 // h[p][c] = sum_t wl[t][c] x[p + off(t)]  (1 -> 32 channels; x FP32 [H][W]).
+// The 288 weights are staged in shared memory (read as broadcasts).
+// A thread computes one pixel's chunk of 8 channels, so a warp stores 512
+// contiguous bytes.
 __global__ void k_net_lift(const float* x, const float* wl, __nv_bfloat16* h, int H, int W) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= H * W) return;
+    __shared__ float sw[9 * kNetC];
+    for (int j = threadIdx.x; j < 9 * kNetC; j += blockDim.x) sw[j] = wl[j];
+    __syncthreads();
+    const long j = blockIdx.x * (long)blockDim.x + threadIdx.x;   // (pixel, chunk)
+    if (j >= 4L * H * W) return;
+    const int q = (int)(j & 3), p = (int)(j >> 2);
     const int y = p / W, xx = p - y * W;
     float xv[9];
 #pragma unroll
@@ -234,43 +500,46 @@ __global__ void k_net_lift(const float* x, const float* wl, __nv_bfloat16* h, in
         const int yy = y + t / 3 - 1, xs = wrapx(xx + t % 3 - 1, W);
         xv[t] = (yy >= 0 && yy < H) ? x[(size_t)yy * W + xs] : 0.f;
     }
+    float o[8];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        float o[8];
+    for (int e = 0; e < 8; e++) {
+        float acc = 0.f;
 #pragma unroll
-        for (int e = 0; e < 8; e++) {
-            float acc = 0.f;
-#pragma unroll
-            for (int t = 0; t < 9; t++) acc += __ldg(wl + t * kNetC + 8 * q + e) * xv[t];
-            o[e] = acc;
-        }
-        bf16x8_store(h + (size_t)p * kNetC + 8 * q, o);
+        for (int t = 0; t < 9; t++) acc += sw[t * kNetC + 8 * q + e] * xv[t];
+        o[e] = acc;
     }
+    bf16x8_store(h + (size_t)p * kNetC + 8 * q, o);
 }
 
 // z[p] = scale * sum_t sum_c wp[t][c] g[p + off(t)][c] for rows < hvalid, else 0
 // (32 -> 1 channel; z FP32 [H][W]).
+// Four consecutive threads share a pixel, one 8-channel chunk each (a warp's
+// loads of a tap are 512 contiguous bytes), and add their partial sums by
+// shuffles. blockDim.x is a multiple of 32.
 __global__ void k_net_proj(const __nv_bfloat16* g, const float* wp, float* z, int H, int W, int hvalid,
                            float scale) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= H * W) return;
+    __shared__ float sw[9 * kNetC];
+    for (int j = threadIdx.x; j < 9 * kNetC; j += blockDim.x) sw[j] = wp[j];
+    __syncthreads();
+    const long j = blockIdx.x * (long)blockDim.x + threadIdx.x;   // (pixel, chunk)
+    const bool in = j < 4L * H * W;
+    const int q = (int)(j & 3), p = in ? (int)(j >> 2) : 0;
     const int y = p / W, xx = p - y * W;
     float acc = 0.f;
-    if (y < hvalid) {
+    if (in && y < hvalid) {
+#pragma unroll
         for (int t = 0; t < 9; t++) {
             const int yy = y + t / 3 - 1, xs = wrapx(xx + t % 3 - 1, W);
             if (yy < 0 || yy >= H) continue;
-            const __nv_bfloat16* gp = g + ((size_t)yy * W + xs) * kNetC;
+            float v[8];
+            bf16x8_load(g + ((size_t)yy * W + xs) * kNetC + 8 * q, v);
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                float v[8];
-                bf16x8_load(gp + 8 * q, v);
-#pragma unroll
-                for (int e = 0; e < 8; e++) acc += __ldg(wp + t * kNetC + 8 * q + e) * v[e];
-            }
+            for (int e = 0; e < 8; e++) acc += sw[t * kNetC + 8 * q + e] * v[e];
         }
     }
-    z[p] = acc * scale;
+    acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+    acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+    if (in && q == 0) z[p] = acc * scale;
 }
 
 // Adjoint of k_net_proj (scale 1): dg[q][c] = sum_t wp[t][c] dz[q - off(t)].

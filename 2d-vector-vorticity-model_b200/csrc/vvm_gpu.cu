@@ -8,9 +8,14 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
+
+#include <cudaTypedefs.h>
 
 #include "../../include/vvm_gpu.h"
 #include "poisson_kernels.cuh"
@@ -810,6 +815,69 @@ __global__ void k_net_galerkin(int NX, int NK, int pitch, const CGScalars* sc, c
 // level, 3x3 conv), projection 32 -> 1. Level 0 is the cal_w grid padded to
 // H0 = round_up(NK, 8) rows (W0 = NX, a multiple of 8). FP32 master weights
 // with Adam; BF16 operands and activations, FP32 accumulation.
+// The 3x3 32 -> 32 convolution of the learned preconditioner: rows of at
+// least kCBox pixels go to the streamed TMA kernel, narrower ones to the
+// one-row-tile kernel. Tensor maps (3D {32, W, H} over BF16 activations,
+// boxes {8, 144, 1} and {8, 8, 1}) are encoded through the driver's
+// cuTensorMapEncodeTiled and cached per (tensor, H, W, box width): the map is
+// a function of those alone.
+CUtensorMap conv_map(const void* p, int H, int W, int boxw) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, int>, CUtensorMap> cache;
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_tuple(p, H, W, boxw);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    if (!enc) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        CK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) throw CudaError{"cuTensorMapEncodeTiled: not found in the driver"};
+        enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)kNetC, (cuuint64_t)W, (cuuint64_t)H};
+    cuuint64_t strides[2] = {(cuuint64_t)kNetC * 2, (cuuint64_t)W * kNetC * 2};
+    cuuint32_t box[3] = {8, (cuuint32_t)boxw, 1}, es[3] = {1, 1, 1};
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(p), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw CudaError{"cuTensorMapEncodeTiled failed"};
+    cache.emplace(key, m);
+    return m;
+}
+
+// Output rows per CTA of the streamed kernel: enough CTAs for two a SM (its
+// shared memory allows two).
+int conv_rows_per_cta(int H, int W) {
+    static int sms[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!sms[dev]) {
+        CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaFuncSetAttribute(k_conv32_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvStreamSmem));
+    }
+    const long tiles = (long)cdiv(W, kConvTile) * H;
+    return (int)std::max(1L, std::min((long)H, (tiles + 2L * sms[dev] - 1) / (2L * sms[dev])));
+}
+
+void conv32(const __nv_bfloat16* in, __nv_bfloat16* out, const uint4* w, int H, int W, int* err, cudaStream_t st,
+            Stats* stats) {
+    if (W >= kCBox) {
+        const int R = conv_rows_per_cta(H, W);
+        const CUtensorMap trow = conv_map(in, H, W, kCBox), twrap = conv_map(in, H, W, 8);
+        ConvStreamArgs a{in, out, w, H, W, R, err};
+        const int grid = cdiv(W, kConvTile) * cdiv(H, R);
+        LAUNCH(stats, VVM_K_LEARNED, st, k_conv32_stream<<<grid, kConvTile, kConvStreamSmem, st>>>(trow, twrap, a));
+    } else {
+        ConvArgs a{in, out, w, H, W, err};
+        LAUNCH(stats, VVM_K_LEARNED, st, k_conv32_tc<<<H * cdiv(W, kConvTile), kConvTile, 0, st>>>(a));
+    }
+    CKL();
+}
+
 struct LearnedNet {
     static constexpr int kLift = 0, kConvs = 9 * kNetC, kConvSize = 9 * kNetC * kNetC;
     static constexpr int kProj = kConvs + 6 * kConvSize, kParams = kProj + 9 * kNetC;
@@ -925,9 +993,7 @@ struct LearnedNet {
     }
 
     void conv(int c, bool adj, const __nv_bfloat16* in, __nv_bfloat16* out, int l, cudaStream_t st) {
-        ConvArgs a{in, out, (adj ? pkT : pk) + (size_t)c * 1152, H[l], W[l], err};
-        LAUNCH(stats, VVM_K_LEARNED, st, k_conv32_tc<<<H[l] * cdiv(W[l], kConvTile), kConvTile, 0, st>>>(a));
-        CKL();
+        conv32(in, out, (adj ? pkT : pk) + (size_t)c * 1152, H[l], W[l], err, st, stats);
     }
     void sum4(const __nv_bfloat16* in, __nv_bfloat16* out, int lo, float mult, cudaStream_t st) {
         LAUNCH(stats, VVM_K_LEARNED, st, k_net_sum4<<<cdiv(H[lo] * W[lo] * 4, 256), 256, 0, st>>>(in, out, H[lo], W[lo], mult));
@@ -945,7 +1011,7 @@ struct LearnedNet {
 
     // z0 = net(x0), z0 rows >= NK set to zero.
     void forward(cudaStream_t st) {
-        LAUNCH(stats, VVM_K_LEARNED, st, k_net_lift<<<cdiv(H[0] * W[0], 128), 128, 0, st>>>(x0, w + kLift, h[0], H[0], W[0]));
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_lift<<<cdiv(4 * H[0] * W[0], 256), 256, 0, st>>>(x0, w + kLift, h[0], H[0], W[0]));
         CKL();
         for (int l = 1; l < 4; l++) {   // down: pool, conv D_l
             sum4(h[l - 1], pl[l], l, 0.25f, st);
@@ -957,7 +1023,7 @@ struct LearnedNet {
             conv(3 + (2 - l), false, u[l], gg[l], l, st);
             lower = gg[l];
         }
-        LAUNCH(stats, VVM_K_LEARNED, st, k_net_proj<<<cdiv(H[0] * W[0], 128), 128, 0, st>>>(gg[0], w + kProj, z0, H[0], W[0], NK, 1.f));
+        LAUNCH(stats, VVM_K_LEARNED, st, k_net_proj<<<cdiv(4 * H[0] * W[0], 256), 256, 0, st>>>(gg[0], w + kProj, z0, H[0], W[0], NK, 1.f));
         CKL();
     }
 
@@ -2938,9 +3004,7 @@ int vvm_gpu_conv3x3_c32(const float* x, const float* w, float* y, int H, int W, 
         CKL();
         k_pack_conv32<<<cdiv(9 * 4 * kNetC, 128), 128>>>(fw, pw, adjoint ? 1 : 0);
         CKL();
-        ConvArgs a{bx, by, pw, H, W, err};
-        k_conv32_tc<<<H * cdiv(W, kConvTile), kConvTile>>>(a);
-        CKL();
+        conv32(bx, by, pw, H, W, err, nullptr, nullptr);
         k_bf16_to_f32<<<256, 256>>>(by, fx, n);
         CKL();
         CK(cudaMemcpy(y, fx, n * sizeof(float), cudaMemcpyDeviceToHost));

@@ -63,7 +63,7 @@ class HostState(ctypes.Structure):
 
 # Kernel classes of vvm_gpu_profile_read (VVM_K_* in include/vvm_gpu.h).
 KERNEL_CLASSES = ("pzeta", "padv", "apply", "pubar", "poisson_rhs", "cg", "mg_sweep", "mg_restrict",
-                  "mg_coarse", "cal_u", "kessler", "rkm", "gs", "mean")
+                  "mg_coarse", "cal_u", "kessler", "rkm", "gs", "mean", "learned")
 
 ROUTINES = ("pzeta", "pth", "pqv", "pqc", "pqr", "add_forcing", "halo_all", "pubartop", "cal_w",
             "cal_u", "kessler", "update_mean", "turbulence", "nudge", "next_step")
