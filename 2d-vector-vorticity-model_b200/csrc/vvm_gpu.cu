@@ -276,6 +276,14 @@ inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
 inline int cdiv(int a, int b) { return (a + b - 1) / b; }
 
 // Owns device allocations of one context.
+// Host -> device copy of set-up data, complete on return (a plain cudaMemcpy
+// from pageable memory may return before its DMA ends, and work on a
+// non-blocking stream is not ordered after the legacy stream).
+inline void upload_now(void* dst, const void* src, size_t nb) {
+    CK(cudaMemcpy(dst, src, nb, cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(nullptr));
+}
+
 struct Arena {
     std::vector<void*> ptrs;
     std::vector<size_t> bytes;
@@ -285,6 +293,9 @@ struct Arena {
         const size_t nb = std::max<size_t>(n, 1) * sizeof(X);
         CK(cudaMalloc(&p, nb));
         CK(cudaMemset(p, 0, nb));
+        // complete before returning: a context's stream may be non-blocking,
+        // and work on it is not ordered after the legacy stream
+        CK(cudaStreamSynchronize(nullptr));
         ptrs.push_back(p);
         bytes.push_back(nb);
         return static_cast<X*>(p);
@@ -502,7 +513,7 @@ struct Multigrid {
 
     double* upload(Arena& ar, const std::vector<double>& v) {
         double* d = ar.alloc<double>(v.size());
-        CK(cudaMemcpy(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+        upload_now(d, v.data(), v.size() * sizeof(double));
         return d;
     }
 
@@ -684,7 +695,7 @@ struct Spectral {
     static P* upload(Arena& ar, const std::vector<double>& v) {
         std::vector<P> h(v.begin(), v.end());
         P* d = ar.alloc<P>(h.size());
-        CK(cudaMemcpy(d, h.data(), h.size() * sizeof(P), cudaMemcpyHostToDevice));
+        upload_now(d, h.data(), h.size() * sizeof(P));
         return d;
     }
 
@@ -801,6 +812,76 @@ __global__ void k_net_out(const float* z, int NX, int NK, int pitch, double* a, 
     a[(size_t)k * pitch + i] = (double)z[(size_t)k * NX + i] * sqrt(*nrm2 > 0 ? *nrm2 : 0.0);
 }
 
+// Truncated flexible CG of the learned preconditioner (fcg_learned): up to
+// kFcgM-1 earlier directions (or their S images), in ring slots `slot`.
+constexpr int kFcgM = 8;
+struct FcgSet {
+    const double* a[kFcgM];
+    int slot[kFcgM];
+    int cnt;
+};
+
+// Partials of (z, q_j), j < cnt: row j of `partial` holds one value a block.
+__global__ void k_fcg_multidot(VecArgs<double> v, const double* z, FcgSet q, double* partial) {
+    __shared__ double sh[kFcgM * 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    double s[kFcgM] = {};
+    if (i < v.nx && kk < v.NK) {
+        const size_t id = (size_t)kk * v.pitch + i;
+        const double zv = z[id];
+#pragma unroll
+        for (int j = 0; j < kFcgM; j++)
+            if (j < q.cnt) s[j] = zv * q.a[j][id];
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const int b = blockIdx.x + gridDim.x * blockIdx.y, nb = gridDim.x * gridDim.y;
+        for (int j = 0; j < q.cnt; j++) partial[(size_t)j * nb + b] = s[j];
+    }
+}
+
+// beta_j = (z, q_j) / (p_j, q_j), the sums finished in a fixed order (one block).
+__global__ void k_fcg_beta(const double* partial, int npart, FcgSet q, const double* pq, double* beta) {
+    __shared__ double sh[32];
+    for (int j = 0; j < q.cnt; j++) {
+        double s[1] = {0};
+        for (int b = threadIdx.x; b < npart; b += blockDim.x) s[0] += partial[(size_t)j * npart + b];
+        block_sum(s, sh);
+        if (threadIdx.x == 0) {
+            const double d = pq[q.slot[j]];
+            beta[j] = (d != 0.0) ? s[0] / d : 0.0;
+        }
+    }
+}
+
+// out = z - sum_j beta_j p_j.
+__global__ void k_fcg_dir(VecArgs<double> v, const double* z, FcgSet p, const double* beta, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= v.nx || kk >= v.NK) return;
+    const size_t id = (size_t)kk * v.pitch + i;
+    double y = z[id];
+    for (int j = 0; j < p.cnt; j++) y -= beta[j] * p.a[j][id];
+    out[id] = y;
+}
+
+// alpha = (p, r) / (p, q) from the partials of both; keeps (p, q) for the ring slot.
+__global__ void k_fcg_alpha(const double* ppq, const double* ppr, int npart, CGScalars* sc, double* pq, int slot) {
+    __shared__ double sh[64];
+    double s[2] = {0, 0};
+    for (int b = threadIdx.x; b < npart; b += blockDim.x) {
+        s[0] += ppq[b];
+        s[1] += ppr[b];
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        sc->pq = s[0];
+        sc->alpha = (s[0] != 0.0) ? s[1] / s[0] : 0.0;
+        pq[slot] = s[0];
+    }
+}
+
 // z += gam d (the Galerkin-scaled network correction).
 __global__ void k_net_galerkin(int NX, int NK, int pitch, const CGScalars* sc, const double* d, double* z) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
@@ -870,10 +951,10 @@ void conv32(const __nv_bfloat16* in, __nv_bfloat16* out, const uint4* w, int H, 
         const CUtensorMap trow = conv_map(in, H, W, kCBox), twrap = conv_map(in, H, W, 8);
         ConvStreamArgs a{in, out, w, H, W, R, err};
         const int grid = cdiv(W, kConvTile) * cdiv(H, R);
-        LAUNCH(stats, VVM_K_LEARNED, st, k_conv32_stream<<<grid, kConvTile, kConvStreamSmem, st>>>(trow, twrap, a));
+        LAUNCH(stats, VVM_K_CONV, st, k_conv32_stream<<<grid, kConvTile, kConvStreamSmem, st>>>(trow, twrap, a));
     } else {
         ConvArgs a{in, out, w, H, W, err};
-        LAUNCH(stats, VVM_K_LEARNED, st, k_conv32_tc<<<H * cdiv(W, kConvTile), kConvTile, 0, st>>>(a));
+        LAUNCH(stats, VVM_K_CONV, st, k_conv32_tc<<<H * cdiv(W, kConvTile), kConvTile, 0, st>>>(a));
     }
     CKL();
 }
@@ -906,7 +987,7 @@ struct LearnedNet {
             h[H[0] + kk] = (float)(1.0 / rhou[k]);
             h[2 * H[0] + kk] = (float)(1.0 / rhou[k - 1]);
         }
-        CK(cudaMemcpy(op, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+        upload_now(op, h.data(), h.size() * sizeof(float));
     }
 
     void build(Arena& ar, int NXr, int NKr, int seed) {
@@ -1027,6 +1108,13 @@ struct LearnedNet {
         CKL();
     }
 
+    // The six 32 -> 32 convolutions of forward() alone, on the activations a
+    // forward() left (for timing them).
+    void convs_only(cudaStream_t st) {
+        for (int l = 1; l < 4; l++) conv(l - 1, false, pl[l], h[l], l, st);
+        for (int l = 2; l >= 0; l--) conv(3 + (2 - l), false, u[l], gg[l], l, st);
+    }
+
     // g += d loss / d w for the gradient dz of the output (after forward()).
     void backward(cudaStream_t st) {
         LAUNCH(stats, VVM_K_LEARNED, st, k_net_wgrad_edge<<<H[0], 9 * kNetC, 0, st>>>(dz, gg[0], g + kProj, H[0], W[0], 1));
@@ -1115,7 +1203,7 @@ struct PCG {
         npart = g.x * g.y;
         partial = ar.alloc<double>(npart);
         rhow_k = ar.alloc<double>(NK);
-        CK(cudaMemcpy(rhow_k, rw.data(), NK * sizeof(double), cudaMemcpyHostToDevice));
+        upload_now(rhow_k, rw.data(), NK * sizeof(double));
         sc = ar.alloc<CGScalars>(1);
         ctl = ar.alloc<CGCtl>(1);
         CK(cudaMallocHost(&sc_host, sizeof(CGScalars)));
@@ -1244,6 +1332,8 @@ struct vvm_gpu_ctx {
     std::unique_ptr<LearnedNet> net;
     double* z64 = nullptr;   // preconditioned residual, solver layout
     double *za64 = nullptr, *r164 = nullptr, *d64 = nullptr, *sd64 = nullptr;   // the learned cycle's work arrays
+    double *fcg_p[kFcgM] = {}, *fcg_q[kFcgM] = {};   // flexible-CG direction ring and its S images
+    double *fcg_part = nullptr, *fcg_pq = nullptr, *fcg_beta = nullptr;
     int learned_mode = 0;    // 0: the cycle with the network; 1: without it; 2: identity
     int learned_cap = 200;   // flexible-CG iterations before the multigrid-PCG fallback
     int learned_iters = 0, learned_fallback = 0;
@@ -1639,6 +1729,13 @@ void ensure_learned(vvm_gpu_ctx* c) {
     c->r164 = c->ar.alloc<double>(n);
     c->d64 = c->ar.alloc<double>(n);
     c->sd64 = c->ar.alloc<double>(n);
+    for (int j = 0; j < kFcgM; j++) {
+        c->fcg_p[j] = c->ar.alloc<double>(n);
+        c->fcg_q[j] = c->ar.alloc<double>(n);
+    }
+    c->fcg_part = c->ar.alloc<double>((size_t)kFcgM * c->pcg64->npart);
+    c->fcg_pq = c->ar.alloc<double>(kFcgM);
+    c->fcg_beta = c->ar.alloc<double>(kFcgM);
 }
 
 // z64 = M r: a two-level cycle whose coarse correction is the network.
@@ -1689,10 +1786,16 @@ void learned_precond(vvm_gpu_ctx* c, const double* r, cudaStream_t st) {
     P.mg.sweep(0, r, c->za64, nullptr, 0, 0, c->z64, 1.0, st);
 }
 
-// Flexible CG (the direction's coefficient beta = -(z, q_prev) / (p, q)_prev,
-// exact for a preconditioner that varies or is not symmetric) on S W = Wf
-// from W = 0, preconditioned by learned_precond, to the FP64 residual
-// ||rhow r||^2 <= tol^2 bb. Returns the iterations, or -cap if not converged.
+// Flexible CG with truncated orthogonalisation: the new direction is made
+// S-orthogonal to the last kFcgM-1 directions,
+//   p_k = z_k - sum_j ((z_k, q_j) / (p_j, q_j)) p_j,  q_j = S p_j,
+// alpha_k = (p_k, r_k) / (p_k, q_k). With a preconditioner that varies from
+// one application to the next (the network's Galerkin step makes it
+// nonlinear), keeping only the previous direction loses the Krylov speed-up;
+// a few more restore it. Directions and their S images live in a ring of
+// kFcgM slots. On S W = Wf from W = 0, preconditioned by learned_precond, to
+// the FP64 residual ||rhow r||^2 <= tol^2 bb. Returns the iterations, or -cap
+// if not converged.
 int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) {
     PCG<double>& P = *c->pcg64;
     VecArgs<double> v = P.vargs();
@@ -1709,23 +1812,30 @@ int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) 
     if (!(rr > stop2)) return 0;
     for (int it = 1; it <= cap; it++) {
         learned_precond(c, P.r, st);
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, P.r, c->z64, P.partial));
-        CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RZ));
-        CKL();
-        if (it > 1) {
-            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->z64, P.q, P.partial));
+        const int k = it - 1, slot = k % kFcgM, cnt = std::min(k, kFcgM - 1);
+        FcgSet ps{}, qs{};
+        for (int j = 0; j < cnt; j++) {
+            const int sj = (k - 1 - j) % kFcgM;
+            ps.a[j] = c->fcg_p[sj];
+            qs.a[j] = c->fcg_q[sj];
+            ps.slot[j] = qs.slot[j] = sj;
+        }
+        ps.cnt = qs.cnt = cnt;
+        if (cnt > 0) {
+            LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_multidot<<<G, B, 0, st>>>(v, c->z64, qs, c->fcg_part));
             CKL();
-            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_FCG_BETA));
+            LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_beta<<<1, 1024, 0, st>>>(c->fcg_part, P.npart, qs, c->fcg_pq, c->fcg_beta));
             CKL();
         }
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dir<double><<<G, B, 0, st>>>(v, P.sc, c->z64, P.p, it == 1 ? 1 : 0));
+        LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_dir<<<G, B, 0, st>>>(v, c->z64, ps, c->fcg_beta, c->fcg_p[slot]));
         CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_spmv<double><<<G, B, 0, st>>>(v, P.p, P.q, P.partial));
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_spmv<double><<<G, B, 0, st>>>(v, c->fcg_p[slot], c->fcg_q[slot], P.partial));
         CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_PQ_ALPHA));
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->fcg_p[slot], P.r, c->fcg_part));
         CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_update<double><<<G, B, 0, st>>>(v, P.sc, c->W, P.r, P.p, P.q, P.partial));
+        LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_alpha<<<1, 1024, 0, st>>>(P.partial, c->fcg_part, P.npart, P.sc, c->fcg_pq, slot));
+        CKL();
+        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_update<double><<<G, B, 0, st>>>(v, P.sc, c->W, P.r, c->fcg_p[slot], c->fcg_q[slot], P.partial));
         CKL();
         LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RR));
         CKL();
@@ -2084,9 +2194,10 @@ struct Snapshot {
         for (size_t j = 0; j < c->ar.ptrs.size(); j++) {
             void* q = nullptr;
             CK(cudaMalloc(&q, c->ar.bytes[j]));
-            CK(cudaMemcpy(q, c->ar.ptrs[j], c->ar.bytes[j], cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpyAsync(q, c->ar.ptrs[j], c->ar.bytes[j], cudaMemcpyDeviceToDevice, c->stream));
             copies.push_back(q);
         }
+        CK(cudaStreamSynchronize(c->stream));
         step = c->step;
         cur = c->cur;
         nsolves = c->nsolves;
@@ -2097,7 +2208,8 @@ struct Snapshot {
     void restore(vvm_gpu_ctx* c) {
         CK(cudaStreamSynchronize(c->stream));
         for (size_t j = 0; j < copies.size(); j++)
-            CK(cudaMemcpy(c->ar.ptrs[j], copies[j], c->ar.bytes[j], cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpyAsync(c->ar.ptrs[j], copies[j], c->ar.bytes[j], cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
         c->step = step;
         c->cur = cur;
         c->nsolves = nsolves;
@@ -2413,7 +2525,8 @@ void download_field(vvm_gpu_ctx* c, const T* src, int sk, int off, double* host,
 }
 
 void upload_profile(vvm_gpu_ctx* c, const double* h, double* dptr) {
-    CK(cudaMemcpy(dptr, h, c->d.nz * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(dptr, h, c->d.nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
 }
 
 template <typename T>
@@ -2461,7 +2574,8 @@ int upload_state_t(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
     if (s->precip) {
         std::vector<T> pr(c->d.nx);
         for (int i = 0; i < c->d.nx; i++) pr[i] = T(s->precip[i]);
-        CK(cudaMemcpy(F.precip, pr.data(), c->d.nx * sizeof(T), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(F.precip, pr.data(), c->d.nx * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
     }
     return VVM_GPU_OK;
 }
@@ -2548,8 +2662,9 @@ int upload_profiles(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
         c->pcg32.reset();
     }
     double ub[2] = {s->ubarTop, s->ubarTopp};
-    CK(cudaMemcpy(c->ubar, ub, sizeof(ub), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->dubar, s->dubarTop_advect, 2 * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(c->ubar, ub, sizeof(ub), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->dubar, s->dubarTop_advect, 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     c->step = s->step;
     return VVM_GPU_OK;
 }
@@ -2636,7 +2751,8 @@ int device_errors(vvm_gpu_ctx* c) {
     int h = 0;
     CK(cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (!h) return VVM_GPU_OK;
-    CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return fail(c, VVM_GPU_ECUDA, "Gauss-Seidel diffusion: a wait between warps gave up; the state is invalid");
 }
 
@@ -2956,7 +3072,8 @@ int vvm_gpu_profile(vvm_gpu_ctx* ctx, int enable) {
     return guarded(ctx, [&]() -> int {
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->stats.reset();
-        CK(cudaMemset(ctx->d_exec, 0, sizeof(long long)));
+        CK(cudaMemsetAsync(ctx->d_exec, 0, sizeof(long long), ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
         ctx->stats.on = (enable != 0);
         return VVM_GPU_OK;
     });
@@ -3165,6 +3282,47 @@ int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, do
         cudaFreeHost(hl);
         if (loss_first) *loss_first = first;
         if (loss_last) *loss_last = last;
+        int h = 0;
+        CK(cudaMemcpy(&h, N.err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (h) return fail(ctx, VVM_GPU_ECUDA, "learned: an MMA completion wait gave up");
+        return VVM_GPU_OK;
+    });
+}
+
+int vvm_gpu_learned_time(vvm_gpu_ctx* ctx, int reps, double* ms_forward, double* ms_convs) {
+    if (!ctx || reps < 1) return VVM_GPU_EINVAL;
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        ensure_learned(ctx);
+        LearnedNet& N = *ctx->net;
+        PCG<double>& P = *ctx->pcg64;
+        cudaStream_t st = ctx->stream;
+        dim3 B = P.block(), G = P.grid(), g0(cdiv(P.NX, 64), cdiv(N.H[0], 4));
+        // input: white noise over its norm, in the network's layout (work arrays only)
+        LAUNCH(&ctx->stats, VVM_K_LEARNED, st, k_white_noise<<<G, B, 0, st>>>(ctx->r164, P.NX, P.NK, P.pitch, 12345u));
+        CKL();
+        LAUNCH(&ctx->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(P.vargs(), ctx->r164, ctx->r164, P.partial));
+        CKL();
+        LAUNCH(&ctx->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_NRM));
+        CKL();
+        LAUNCH(&ctx->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(ctx->r164, nullptr, P.NX, P.NK, P.pitch, N.x0, N.H[0], &P.sc->nrm));
+        CKL();
+        N.forward(st);   // warm-up, and valid activations for convs_only
+        cudaEvent_t e[4];
+        for (auto& x : e) CK(cudaEventCreate(&x));
+        CK(cudaEventRecord(e[0], st));
+        for (int r = 0; r < reps; r++) N.forward(st);
+        CK(cudaEventRecord(e[1], st));
+        CK(cudaEventRecord(e[2], st));
+        for (int r = 0; r < reps; r++) N.convs_only(st);
+        CK(cudaEventRecord(e[3], st));
+        CK(cudaEventSynchronize(e[3]));
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, e[0], e[1]));
+        CK(cudaEventElapsedTime(&b, e[2], e[3]));
+        for (auto& x : e) cudaEventDestroy(x);
+        if (ms_forward) *ms_forward = a / reps;
+        if (ms_convs) *ms_convs = b / reps;
         int h = 0;
         CK(cudaMemcpy(&h, N.err, sizeof(int), cudaMemcpyDeviceToHost));
         if (h) return fail(ctx, VVM_GPU_ECUDA, "learned: an MMA completion wait gave up");

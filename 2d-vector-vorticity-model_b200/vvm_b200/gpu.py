@@ -63,7 +63,7 @@ class HostState(ctypes.Structure):
 
 # Kernel classes of vvm_gpu_profile_read (VVM_K_* in include/vvm_gpu.h).
 KERNEL_CLASSES = ("pzeta", "padv", "apply", "pubar", "poisson_rhs", "cg", "mg_sweep", "mg_restrict",
-                  "mg_coarse", "cal_u", "kessler", "rkm", "gs", "mean", "learned")
+                  "mg_coarse", "cal_u", "kessler", "rkm", "gs", "mean", "learned", "conv")
 
 ROUTINES = ("pzeta", "pth", "pqv", "pqc", "pqr", "add_forcing", "halo_all", "pubartop", "cal_w",
             "cal_u", "kessler", "update_mean", "turbulence", "nudge", "next_step")
@@ -79,7 +79,7 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream",
            "vvm_gpu_conv3x3_c32", "vvm_gpu_learned_shape", "vvm_gpu_learned_weights",
            "vvm_gpu_learned_eval", "vvm_gpu_learned_train", "vvm_gpu_learned_config",
-           "vvm_gpu_learned_last") + tuple(
+           "vvm_gpu_learned_last", "vvm_gpu_learned_time") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -132,6 +132,7 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_learned_train.argtypes = [vp, ip, ip, ip, ctypes.c_double, ip, _dp, _dp]
     L.vvm_gpu_learned_config.argtypes = [vp, ip, ip]
     L.vvm_gpu_learned_last.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
+    L.vvm_gpu_learned_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -405,6 +406,12 @@ class VVMGpu:
 
     def learned_config(self, mode: int = 0, cap: int = 200):
         self._check(self.L.vvm_gpu_learned_config(self.h, int(mode), int(cap)))
+
+    def learned_time(self, reps: int = 20) -> tuple[float, float]:
+        """(ms per network forward pass, ms per pass of its six convolutions)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.vvm_gpu_learned_time(self.h, int(reps), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def learned_last(self) -> tuple[int, int]:
         a, b = ctypes.c_int(), ctypes.c_int()

@@ -320,11 +320,88 @@ def our_arm(args, rank, world, device):
         "gpu_launches": head["launches"],
         "clocks": clocks,
     }
+    if not args.no_learned:
+        line["learned"] = learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms / args.steps)
     if not args.no_ensemble:
         line["ensemble"] = ensemble_arm(args, rank, world, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     return line
+
+
+def net_figures(grid):
+    """Algorithmic work of one forward pass of the learned preconditioner's
+    network on this grid (levels l = 0..3 of H0 = round_up(NZ-1, 8) by NX
+    pixels, halved per level): the 32 -> 32 convolutions are U0 at level 0, D1
+    and U1 at level 1, D2 and U2 at level 2, D3 at level 3; each reads its
+    input and writes its output once (BF16, 64 B a pixel) and does 2*9*32*32
+    FLOPs a pixel."""
+    H0, W0 = -(-(grid.NZ - 1) // 8) * 8, grid.NX
+    per_level = (1, 2, 2, 1)
+    px = sum(n * (H0 >> l) * (W0 >> l) for l, n in enumerate(per_level))
+    return {"convs": sum(per_level), "pixels": px, "bytes": 128.0 * px, "flops": 2.0 * 9 * 32 * 32 * px}
+
+
+def learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms_per_step, steps=3):
+    """Learned-preconditioned step (mixed-precision fields, FP64 flexible CG
+    to the same residual 1e-10) on the headline grid: the network is trained
+    on the model's own solves first (bounded: 32 pairs, 300 Adam steps), then
+    `steps` steps are timed with it and without it (the ablation). The
+    convolutions' roofline comes from repeated forward passes timed between
+    one pair of events."""
+    import torch
+    from vvm_b200.gpu import VVM_PREC_MIXED, VVM_SOLVER_LEARNED, VVMGpu
+    from vvm_b200.initial_state import warm_bubble
+    st = warm_bubble(NX, NZ, DX, DX, DT)
+    out = {}
+    w = None
+    for mode, name in ((0, "with_net"), (1, "without_net")):
+        g = VVMGpu(st.grid, precision=VVM_PREC_MIXED, solver=VVM_SOLVER_LEARNED, device=device)
+        g.set_stream(torch.cuda.current_stream().cuda_stream)
+        g.upload(st)
+        if w is None:
+            t0 = time.perf_counter()
+            lf, ll = g.learned_train(npairs=32, steps=300, batch=2, lr=2e-3, seed=2)
+            g.synchronize()
+            out["training"] = {"pairs": 32, "adam_steps": 300, "batch": 2, "seconds": time.perf_counter() - t0,
+                               "loss_first": lf, "loss_last": ll,
+                               "pairs_from": "16 model steps solved by multigrid-PCG + 16 white-noise rhs"}
+            w = g.learned_weights()
+        else:
+            g.learned_weights(w)
+        g.learned_config(mode=mode, cap=4000)
+        g.step(1)
+        g.synchronize()
+        if dist_on():
+            dist_barrier()
+        times = timed_steps(torch, g, steps, flush)
+        it, fell = g.learned_last()
+        _, rel = g.last_solve()
+        ms = dist_max(sum(times)) / steps
+        rec = {"ms_per_step": ms, "value": world * NX * NZ / (ms * 1e-3), "fcg_iterations_last": it,
+               "fell_back": bool(fell), "poisson_relres_last": rel}
+        if mode == 0:
+            fwd_ms, conv_ms = g.learned_time(reps=20)
+            nf = net_figures(st.grid)
+            rec["net_forward_ms"] = fwd_ms
+            rec["ms_per_fcg_iteration"] = ms / max(it, 1)
+            rec["conv_roofline"] = {
+                "kernel": "k_conv32_stream (3x3, 32 -> 32, BF16, tcgen05 + TMA); k_conv32_tc below 144 px",
+                "bound": "hbm", "achieved": nf["bytes"] / (conv_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": nf["bytes"] / (conv_ms * 1e-3) / 1e9 / hbm, "peak_source": peak_kind,
+                "tensor_tflops": nf["flops"] / (conv_ms * 1e-3) / 1e12,
+                "algorithmic_bytes_per_forward": nf["bytes"], "flops_per_forward": nf["flops"],
+                "ms_per_forward_convs": conv_ms, "convs_per_forward": nf["convs"],
+                "note": "20 passes between one event pair, activations L2-resident between launches; "
+                        "144 FLOP/B is below the BF16 ridge, so the bound is memory"}
+        out[name] = rec
+        g.close()
+    out["solver"] = ("flexible CG, FP64; preconditioner: z-line solve, tensor-core conv net on the "
+                     "remaining residual with a Galerkin step, z-line solve; multigrid-PCG fallback")
+    out["vs_plain_fp64_mgpcg"] = fp64_ms_per_step / out["with_net"]["ms_per_step"]
+    out["iterations_saved_by_net"] = (out["without_net"]["fcg_iterations_last"]
+                                      / max(out["with_net"]["fcg_iterations_last"], 1))
+    return out
 
 
 def st_nx():
@@ -458,6 +535,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-case batched ensemble")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner step")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

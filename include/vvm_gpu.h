@@ -191,7 +191,8 @@ int vvm_gpu_conv3x3_c32(const float* x, const float* w, float* y, int H, int W, 
  * activations, FP32 accumulation). Its grid is the cal_w grid padded to H0 = round_up(NZ-1, 8)
  * rows by W0 = NX columns (NX a multiple of 8); arrays of it are [H0][W0].
  * The solve is flexible CG from W = 0 to the same FP64 residual as the other
- * solvers; after `cap` iterations the multigrid PCG takes over from the
+ * solvers, each new direction S-orthogonalised against the previous seven
+ * (the preconditioner varies between applications, so one is not enough); after `cap` iterations the multigrid PCG takes over from the
  * current iterate. Weights: nparams FP32 values (vvm_gpu_learned_shape), the
  * lift [9][32], six convolutions [9 taps][32 in][32 out] (down at levels 1,
  * 2, 3, up at levels 2, 1, 0) and the projection [9][32]; seeded initial
@@ -217,6 +218,11 @@ int vvm_gpu_learned_eval(vvm_gpu_ctx* ctx, const float* x, const float* t, float
 int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, double lr, int seed,
                           double* loss_first, double* loss_last);
 int vvm_gpu_learned_config(vvm_gpu_ctx* ctx, int mode, int cap);
+/* Times `reps` network forward passes on a white-noise input, and `reps`
+ * passes of its six tensor-core convolutions alone, each between one pair of
+ * events on the context's stream: milliseconds per pass. Changes no model
+ * state (only the preconditioner's work arrays). */
+int vvm_gpu_learned_time(vvm_gpu_ctx* ctx, int reps, double* ms_forward, double* ms_convs);
 int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back);
 
 /* -- launch-shape knobs --------------------------------------------------------
@@ -309,8 +315,9 @@ int vvm_gpu_poisson_solve_noalloc(int NX, int NZ, const double* rhou, const doub
 #define VVM_K_RKM 11        /* eddy coefficients */
 #define VVM_K_GS 12         /* Gauss-Seidel diffusion (+ nudging) */
 #define VVM_K_MEAN 13       /* updateMean, nudging passes, transfers */
-#define VVM_K_LEARNED 14    /* learned preconditioner: network forward, training */
-#define VVM_K_COUNT 15
+#define VVM_K_LEARNED 14    /* learned preconditioner: network (not its convolutions), training */
+#define VVM_K_CONV 15       /* learned preconditioner: tensor-core 3x3 convolutions */
+#define VVM_K_COUNT 16
 int vvm_gpu_profile(vvm_gpu_ctx* ctx, int enable);
 /* Accumulated device milliseconds and launches of one kernel class. */
 int vvm_gpu_profile_read(vvm_gpu_ctx* ctx, int kernel_class, double* ms, long long* launches);
