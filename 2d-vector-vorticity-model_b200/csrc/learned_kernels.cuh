@@ -192,23 +192,27 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_tc(ConvArgs a) {
 // x0-1 = W-1 (first strip) and x0+128 = W (last strip) come from a second
 // map with 8-pixel boxes and are copied into place in shared memory.
 //
-// Thread 0 issues loads and MMAs; all four warps read the accumulator back.
-// Input row j goes to slot j % kCSlots; it is read by output rows j-2..j, so
-// the slot of row r-1 is refilled with row r-1+kCSlots once output r-1's MMAs
-// are done, kCSlots-3 rows ahead of its use.
-// Two TMEM accumulators (32 columns each) let the MMAs of row r run while row
-// r-1 is written out. Barriers: full[slot] (TMA bytes of an input row),
-// done[b] (MMAs of the row in accumulator b, by tcgen05.commit), empty[b]
-// (accumulator b read back, one arrive per warp). Every wait is bounded; a
-// wait that gives up sets kNetErrWait and an abort flag that ends the CTA's
-// remaining work, after a bounded wait for the copies and MMAs in flight.
-constexpr int kCSlots = 8;                        // 3 rows in use + 5 rows of prefetch
+// Warp-specialised: lane 0 of warp 4 issues the loads and the MMAs; warps
+// 0-3 read the accumulators back (warp w owns TMEM lanes 32w..32w+31, the
+// tile's pixels) and store them. Input row j goes to slot j % kCSlots; it is
+// read by output rows j-2..j, so the slot of row r-2 is refilled with row
+// r-2+kCSlots once output r-2's MMAs are done, which never holds up the
+// issue of row r. kCAcc TMEM accumulators (32 columns each) let the MMA warp
+// run kCAcc rows ahead of the write-back. Barriers: full[slot] (TMA bytes of
+// an input row), done[b] (MMAs of the row in accumulator b, by
+// tcgen05.commit), empty[b] (accumulator b read back, one arrive per
+// epilogue warp), one for the weights. Every wait is bounded; a wait that
+// gives up sets kNetErrWait and an abort flag that ends the CTA's remaining
+// work, after a bounded wait for the copies and MMAs in flight.
+constexpr int kCSlots = 8;                        // ring of input rows
+constexpr int kCAcc = 4;                          // TMEM accumulators
+constexpr int kCThreads = 160;                    // 4 epilogue warps + 1 producer warp
 constexpr int kCBox = 144;
 constexpr int kCRowBytes = kCBox * 16;            // one 8-channel chunk of a row
 constexpr int kCSlotBytes = 4 * kCRowBytes;       // 9216
 constexpr int kCWBytes = 9 * 4 * kNetC * 16;      // packed weights, 18432
 constexpr int kCWrapBytes = 2 * 4 * 8 * 16;       // [side][chunk][8 pixels], 1024 a slot
-constexpr int kCBars = kCSlots + 2 + 2 + 1;       // full[4], done[2], empty[2], weights
+constexpr int kCBars = kCSlots + 2 * kCAcc + 1;   // full[], done[], empty[], weights
 constexpr int kConvStreamSmem = 128 + kCWBytes + kCSlots * (kCSlotBytes + kCWrapBytes) + 8 * kCBars + 16;
 
 struct ConvStreamArgs {
@@ -248,9 +252,9 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-__global__ void __launch_bounds__(kConvTile) k_conv32_stream(const __grid_constant__ CUtensorMap trow,
-                                                             const __grid_constant__ CUtensorMap twrap,
-                                                             ConvStreamArgs a) {
+__global__ void __launch_bounds__(kCThreads) k_conv32_stream(const __grid_constant__ CUtensorMap trow,
+                                                              const __grid_constant__ CUtensorMap twrap,
+                                                              ConvStreamArgs a) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     uint8_t* base = smem_raw + (((raw + 127) & ~127u) - raw);
@@ -260,7 +264,8 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_stream(const __grid_consta
     uint64_t* bars = reinterpret_cast<uint64_t*>(sW + kCSlots * kCWrapBytes);
     volatile int* abort = reinterpret_cast<volatile int*>(bars + kCBars);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kCBars) + 1;
-    const uint32_t full0 = smem_u32(bars), done0 = full0 + 8 * kCSlots, empty0 = done0 + 16, wbar = empty0 + 16;
+    const uint32_t full0 = smem_u32(bars), done0 = full0 + 8 * kCSlots, empty0 = done0 + 8 * kCAcc,
+                   wbar = empty0 + 8 * kCAcc;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int strips = (a.W + kConvTile - 1) / kConvTile;
@@ -272,14 +277,15 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_stream(const __grid_consta
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(64)
+                     "r"(32 * kCAcc)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
         for (int i = 0; i < kCBars; i++) {
-            const uint32_t cnt = (i >= kCSlots + 2 && i < kCSlots + 4) ? 4u : 1u;   // empty[]: one per warp
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full0 + 8 * i), "r"(cnt) : "memory");
+            const bool is_empty = i >= kCSlots + kCAcc && i < kCSlots + 2 * kCAcc;
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full0 + 8 * i), "r"(is_empty ? 4u : 1u)
+                         : "memory");
         }
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -289,55 +295,53 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_stream(const __grid_consta
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    int issued = 0, consumed = 0, committed = 0;   // thread 0's bookkeeping
-    auto load_row = [&](int j) {
-        const int sl = j % kCSlots, y = y0 - 1 + j;
-        const uint32_t bar = full0 + 8 * sl;
-        const uint32_t bytes = kCSlotBytes + (left ? 512u : 0u) + (right ? 512u : 0u);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-        for (int kc = 0; kc < 4; kc++) {
-            tma_load_3d(smem_u32(sA + sl * kCSlotBytes + kc * kCRowBytes), &trow, kc * 8, x0 - 8, y, bar);
-            if (left) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + kc * 128), &twrap, kc * 8, a.W - 8, y, bar);
-            if (right) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + 512 + kc * 128), &twrap, kc * 8, 0, y, bar);
-        }
-        issued = j + 1;
-    };
-    auto take_row = [&](int j) -> bool {   // wait for input row j, then put its periodic pixels in place
-        const int sl = j % kCSlots;
-        if (!mbar_wait(full0 + 8 * sl, (uint32_t)((j / kCSlots) & 1), abort)) return false;
-        consumed = j + 1;
-        uint4* A = reinterpret_cast<uint4*>(sA + sl * kCSlotBytes);
-        const uint4* Wr = reinterpret_cast<const uint4*>(sW + sl * kCWrapBytes);
-        for (int kc = 0; kc < 4; kc++) {
-            if (left) A[kc * kCBox + 7] = Wr[kc * 8 + 7];
-            if (right) A[kc * kCBox + (a.W - x0 + 8)] = Wr[32 + kc * 8];
-        }
-        return true;
-    };
-
-    if (tid == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(wbar), "r"(kCWBytes) : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         smem_u32(sB)),
-                     "l"(reinterpret_cast<uint64_t>(a.w)), "r"(kCWBytes), "r"(wbar)
-                     : "memory");
-        for (int j = 0; j < min(kCSlots, nin); j++) load_row(j);
-    }
-    bool wdone = false;
-    for (int r = 0; r <= R; r++) {
-        if (r < R && tid == 0 && !*abort) {
+    if (warp == 4) {
+        if (lane == 0) {
+            int issued = 0, consumed = 0, committed = 0;
+            bool wdone = false;
+            auto load_row = [&](int j) {
+                const int sl = j % kCSlots, y = y0 - 1 + j;
+                const uint32_t bar = full0 + 8 * sl;
+                const uint32_t bytes = kCSlotBytes + (left ? 512u : 0u) + (right ? 512u : 0u);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+                for (int kc = 0; kc < 4; kc++) {
+                    tma_load_3d(smem_u32(sA + sl * kCSlotBytes + kc * kCRowBytes), &trow, kc * 8, x0 - 8, y, bar);
+                    if (left) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + kc * 128), &twrap, kc * 8, a.W - 8, y, bar);
+                    if (right) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + 512 + kc * 128), &twrap, kc * 8, 0, y, bar);
+                }
+                issued = j + 1;
+            };
+            auto take_row = [&](int j) -> bool {   // wait for input row j, then put its periodic pixels in place
+                const int sl = j % kCSlots;
+                if (!mbar_wait(full0 + 8 * sl, (uint32_t)((j / kCSlots) & 1), abort)) return false;
+                consumed = j + 1;
+                uint4* A = reinterpret_cast<uint4*>(sA + sl * kCSlotBytes);
+                const uint4* Wr = reinterpret_cast<const uint4*>(sW + sl * kCWrapBytes);
+                for (int kc = 0; kc < 4; kc++) {
+                    if (left) A[kc * kCBox + 7] = Wr[kc * 8 + 7];
+                    if (right) A[kc * kCBox + (a.W - x0 + 8)] = Wr[32 + kc * 8];
+                }
+                return true;
+            };
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(wbar), "r"(kCWBytes) : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             smem_u32(sB)),
+                         "l"(reinterpret_cast<uint64_t>(a.w)), "r"(kCWBytes), "r"(wbar)
+                         : "memory");
+            for (int j = 0; j < min(kCSlots, nin); j++) load_row(j);
             bool ok = true;
-            if (r == 0) {
-                ok = mbar_wait(wbar, 0, abort);
-                wdone = ok;
-                for (int j = 0; j < 3 && ok; j++) ok = take_row(j);
-            } else {
-                ok = take_row(r + 2);
-            }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the copied pixels, for the MMAs
-            const int b = r & 1;
-            if (ok && r >= 2) ok = mbar_wait(empty0 + 8 * b, (uint32_t)(((r - 2) >> 1) & 1), abort);
-            if (ok) {
+            for (int r = 0; r < R && ok; r++) {
+                if (r == 0) {
+                    ok = mbar_wait(wbar, 0, abort);
+                    wdone = ok;
+                    for (int j = 0; j < 3 && ok; j++) ok = take_row(j);
+                } else {
+                    ok = take_row(r + 2);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the copied pixels, for the MMAs
+                const int b = r % kCAcc;
+                if (ok && r >= kCAcc) ok = mbar_wait(empty0 + 8 * b, (uint32_t)(((r - kCAcc) / kCAcc) & 1), abort);
+                if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 uint32_t acc = 0;
                 for (int dy = 0; dy < 3; dy++) {
@@ -360,45 +364,62 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_stream(const __grid_consta
                                  done0 + 8 * b)
                              : "memory");
                 committed = r + 1;
-                // input row r-1+kCSlots reuses the slot of row r-1, free once
-                // output r-1's MMAs are done
-                const int jn = r - 1 + kCSlots;
-                if (r >= 1 && jn < nin) {
-                    ok = mbar_wait(done0 + 8 * ((r - 1) & 1), (uint32_t)(((r - 1) >> 1) & 1), abort);
+                // input row r-2+kCSlots reuses the slot of row r-2, free once
+                // output r-2's MMAs are done
+                const int jn = r - 2 + kCSlots;
+                if (r >= 2 && jn < nin) {
+                    const int q = r - 2;
+                    ok = mbar_wait(done0 + 8 * (q % kCAcc), (uint32_t)((q / kCAcc) & 1), abort);
                     if (ok) load_row(jn);
                 }
             }
             if (!ok) {
                 if (a.err) atomicOr(a.err, kNetErrWait);
                 *abort = 1;
+                // wait (bounded) for the copies and MMAs in flight before the
+                // shared memory and TMEM go away
+                volatile int never = 0;
+                if (!wdone) mbar_wait(wbar, 0, &never);
+                for (int j = consumed; j < issued; j++)
+                    mbar_wait(full0 + 8 * (j % kCSlots), (uint32_t)((j / kCSlots) & 1), &never);
+                if (committed > 0) {
+                    const int q = committed - 1;
+                    mbar_wait(done0 + 8 * (q % kCAcc), (uint32_t)((q / kCAcc) & 1), &never);
+                }
             }
         }
-        __syncwarp();
-        if (r >= 1) {   // write out output row r-1
-            const int q = r - 1, b = q & 1;
-            bool got = !*abort && mbar_wait(done0 + 8 * b, (uint32_t)((q >> 1) & 1), abort);
+    } else {
+        // epilogue warps: write out output rows as their MMAs complete
+        for (int q = 0; q < R; q++) {
+            const int b = q % kCAcc;
+            bool got = !*abort && mbar_wait(done0 + 8 * b, (uint32_t)((q / kCAcc) & 1), abort);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             got = __all_sync(0xffffffffu, got);
-            uint32_t v[32];
-            if (got) {
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                    "[%32];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                    : "r"(tmem + ((uint32_t)(warp * 32) << 16) + 32u * b)
-                    : "memory");
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (!got) {   // give up; the producer's cleanup waits for what is in flight
+                if (lane == 0 && !*abort) {
+                    if (a.err) atomicOr(a.err, kNetErrWait);
+                    *abort = 1;
+                }
+                break;
             }
+            uint32_t v[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                "[%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + 32u * b)
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(empty0 + 8 * b) : "memory");
             const int x = x0 + tid;
-            if (got && x < a.W) {
+            if (x < a.W) {
                 uint4* dst = reinterpret_cast<uint4*>(a.out + ((size_t)(y0 + q) * a.W + x) * kNetC);
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
@@ -416,21 +437,10 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_stream(const __grid_consta
             }
         }
     }
-    // after an abort: wait (bounded) for the copies and MMAs still in flight
-    // before the shared memory and TMEM go away
-    if (tid == 0 && *abort) {
-        volatile int never = 0;
-        if (!wdone) mbar_wait(wbar, 0, &never);
-        for (int j = consumed; j < issued; j++) mbar_wait(full0 + 8 * (j % kCSlots), (uint32_t)((j / kCSlots) & 1), &never);
-        if (committed > 0) {
-            const int q = committed - 1;
-            mbar_wait(done0 + 8 * (q & 1), (uint32_t)((q >> 1) & 1), &never);
-        }
-    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32 * kCAcc) : "memory");
 }
 
 // Packs FP32 weights w[tap][in][out] into the B operand of k_conv32_tc:

@@ -929,8 +929,9 @@ CUtensorMap conv_map(const void* p, int H, int W, int boxw) {
     return m;
 }
 
-// Output rows per CTA of the streamed kernel: enough CTAs for two a SM (its
-// shared memory allows two).
+// Output rows per CTA of the streamed kernel: the fewest that fit the grid
+// into one wave of two CTAs a SM (its shared memory allows two); a grid just
+// over a wave would run its last CTAs alone, doubling the time.
 int conv_rows_per_cta(int H, int W) {
     static int sms[64] = {};
     int dev = 0;
@@ -940,8 +941,9 @@ int conv_rows_per_cta(int H, int W) {
         CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
         CK(cudaFuncSetAttribute(k_conv32_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, kConvStreamSmem));
     }
-    const long tiles = (long)cdiv(W, kConvTile) * H;
-    return (int)std::max(1L, std::min((long)H, (tiles + 2L * sms[dev] - 1) / (2L * sms[dev])));
+    const long strips = cdiv(W, kConvTile), slots = 2L * sms[dev];
+    const long groups = std::max(1L, std::min((long)H, slots / strips));
+    return (int)((H + groups - 1) / groups);
 }
 
 void conv32(const __nv_bfloat16* in, __nv_bfloat16* out, const uint4* w, int H, int W, int* err, cudaStream_t st,
@@ -951,7 +953,7 @@ void conv32(const __nv_bfloat16* in, __nv_bfloat16* out, const uint4* w, int H, 
         const CUtensorMap trow = conv_map(in, H, W, kCBox), twrap = conv_map(in, H, W, 8);
         ConvStreamArgs a{in, out, w, H, W, R, err};
         const int grid = cdiv(W, kConvTile) * cdiv(H, R);
-        LAUNCH(stats, VVM_K_CONV, st, k_conv32_stream<<<grid, kConvTile, kConvStreamSmem, st>>>(trow, twrap, a));
+        LAUNCH(stats, VVM_K_CONV, st, k_conv32_stream<<<grid, kCThreads, kConvStreamSmem, st>>>(trow, twrap, a));
     } else {
         ConvArgs a{in, out, w, H, W, err};
         LAUNCH(stats, VVM_K_CONV, st, k_conv32_tc<<<H * cdiv(W, kConvTile), kConvTile, 0, st>>>(a));
