@@ -669,19 +669,21 @@ __global__ void k_net_wgrad_edge(const float* s, const __nv_bfloat16* d, float* 
 }
 
 // Loss of one pair: the S-norm error that the preconditioner's Galerkin step
-// leaves, S the cal_w operator in symmetric form,
-//   (S a)[k][i] = (2 cx_k + ru_k + rd_k) a - cx_k (a[i-1] + a[i+1]) - ru_k a[k+1] - rd_k a[k-1]
+// leaves, S the operator the network works in (the cal_w operator in
+// symmetric form, diagonally scaled: see LearnedNet::set_operator),
+//   (S a)[k][i] = dg_k a - cx_k (a[i-1] + a[i+1]) - ru_k a[k+1] - rd_k a[k-1]
 // on rows k < NK (periodic in i, zero beyond the rows):
 //   L = min_g ||t - g z||_S^2 / ||t||_S^2 = 1 - a^2 / (b c),
 //   a = (z, S t), b = (z, S z), c = (t, S t),
 // independent of the scale of z, as the step is. Partials of a, b, c per block
 // in FP64; S z and S t are kept for the gradient
 //   dL/dz = 2 a / (b c) (g S z - S t), g = a / b.
+// op rows: cx, ru, rd, diagonal ([4][H]), the operator the network works in.
 __device__ __forceinline__ double s_apply_net(const float* a, const float* op, int H, int W, int NK, int k, int i) {
-    const double cx = op[k], ru = op[H + k], rd = op[2 * H + k];
+    const double cx = op[k], ru = op[H + k], rd = op[2 * H + k], dg = op[3 * H + k];
     const size_t row = (size_t)k * W;
     const int il = i == 0 ? W - 1 : i - 1, ir = i == W - 1 ? 0 : i + 1;
-    double y = (2.0 * cx + ru + rd) * a[row + i] - cx * ((double)a[row + il] + (double)a[row + ir]);
+    double y = dg * a[row + i] - cx * ((double)a[row + il] + (double)a[row + ir]);
     if (k + 1 < NK) y -= ru * a[row + W + i];
     if (k > 0) y -= rd * a[row - W + i];
     return y;

@@ -135,9 +135,11 @@ __global__ void k_loop_outer(const CGScalars* sc64, CGCtl* ctl, const CGCtl* inn
 }
 
 // b = rhow_k^2 (zetap[i+1][k] - zetap[i][k]) dx for k = 2..nz-2, i = 1..nx-2
-// (PoissonSolver.cpp:444-450); stores f = -b / rhow_k and partial ||b||^2.
+// (PoissonSolver.cpp:444-450); stores f = -b / rw_k and partial ||b||^2. rw_k
+// is the row's residual weight: rhow_k on uniform levels, rhow_k / a_k on
+// stretched ones (a_k the centre spacing around face k over dx).
 template <typename T>
-__global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const T* zetap, double* f,
+__global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const double* rw, const T* zetap, double* f,
                               int pitch_f, double* partial) {
     __shared__ double sh[32];
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
@@ -146,15 +148,15 @@ __global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const T* ze
     if (ii < d.nx - 2 && kk < d.nz - 3) {
         const int i = ii + 1, k = kk + 2;
         double b = rhow[k] * rhow[k] * ((double)zetap[d.at(i + 1, k)] - (double)zetap[d.at(i, k)]) * dx;
-        f[(size_t)kk * pitch_f + ii] = -b / rhow[k];
+        f[(size_t)kk * pitch_f + ii] = -b / rw[k];
         s[0] = b * b;
     }
     block_sum(s, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
 }
 
-// Reference-ordered b vector ((k-2)*NX + (i-1)) to f = -b/rhow_k, partial ||b||^2.
-__global__ void k_rhs_from_b(int NX, int NK, const double* rhow, const double* b, double* f,
+// Reference-ordered b vector ((k-2)*NX + (i-1)) to f = -b/rw_k, partial ||b||^2.
+__global__ void k_rhs_from_b(int NX, int NK, const double* rw, const double* b, double* f,
                              int pitch_f, double* partial) {
     __shared__ double sh[32];
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
@@ -162,7 +164,7 @@ __global__ void k_rhs_from_b(int NX, int NK, const double* rhow, const double* b
     double s[1] = {0};
     if (ii < NX && kk < NK) {
         double bv = b[(size_t)kk * NX + ii];
-        f[(size_t)kk * pitch_f + ii] = -bv / rhow[kk + 2];
+        f[(size_t)kk * pitch_f + ii] = -bv / rw[kk + 2];
         s[0] = bv * bv;
     }
     block_sum(s, sh);
@@ -776,15 +778,30 @@ struct Spectral {
 // ---------------------------------------------------------------- learned net
 
 // Solver layout (FP64 [NK][pitch]) -> network layout (FP32 [H0][W0], rows
-// >= NK zero): x = (a - sub) / sqrt(*nrm2) (sub may be null); and back:
-// a += z sqrt(*nrm2).
+// >= NK zero): x = scale_k (a - sub) / sqrt(*nrm2) (sub, scale may be null);
+// and back: a = scale_k z sqrt(*nrm2). The per-row scales map between the
+// solver's variables and the network's (LearnedNet::set_operator).
 __global__ void k_net_in(const double* a, const double* sub, int NX, int NK, int pitch, float* x, int H0,
-                         const double* nrm2) {
+                         const double* nrm2, const double* scale) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= NX || k >= H0) return;
     const double s = (*nrm2 > 0) ? 1.0 / sqrt(*nrm2) : 0.0;
     const size_t e = (size_t)k * pitch + i;
-    x[(size_t)k * NX + i] = (k < NK) ? (float)((a[e] - (sub ? sub[e] : 0.0)) * s) : 0.f;
+    x[(size_t)k * NX + i] = (k < NK) ? (float)((a[e] - (sub ? sub[e] : 0.0)) * s * (scale ? scale[k] : 1.0)) : 0.f;
+}
+
+// partial sums of (scale_k a)^2: the norm of the network's input.
+__global__ void k_net_sdot(VecArgs<double> v, const double* a, const double* scale, double* partial) {
+    __shared__ double sh[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    double s[1] = {0};
+    if (i < v.nx && kk < v.NK) {
+        const double x = a[(size_t)kk * v.pitch + i] * scale[kk];
+        s[0] = x * x;
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
 }
 
 // White noise in the solver layout: a[k][i] = N(0, 1) from a counter hash
@@ -806,10 +823,11 @@ __global__ void k_white_noise(double* a, int NX, int NK, int pitch, unsigned see
     a[(size_t)k * pitch + i] = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
 }
 
-__global__ void k_net_out(const float* z, int NX, int NK, int pitch, double* a, const double* nrm2) {
+__global__ void k_net_out(const float* z, int NX, int NK, int pitch, double* a, const double* nrm2,
+                          const double* scale) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= NX || k >= NK) return;
-    a[(size_t)k * pitch + i] = (double)z[(size_t)k * NX + i] * sqrt(*nrm2 > 0 ? *nrm2 : 0.0);
+    a[(size_t)k * pitch + i] = (double)z[(size_t)k * NX + i] * sqrt(*nrm2 > 0 ? *nrm2 : 0.0) * (scale ? scale[k] : 1.0);
 }
 
 // Truncated flexible CG of the learned preconditioner (fcg_learned): up to
@@ -972,7 +990,8 @@ struct LearnedNet {
     __nv_bfloat16 *h[4] = {}, *pl[4] = {}, *u[3] = {}, *gg[3] = {};
     __nv_bfloat16 *dgb[4] = {}, *dub[3] = {}, *dpb[4] = {}, *dh3 = nullptr;
     double *part = nullptr, *lt = nullptr;
-    float *op = nullptr, *sz = nullptr, *st = nullptr;   // rows' cx, ru, rd ([3][H0]) for the loss; S z, S t
+    float *op = nullptr, *sz = nullptr, *st = nullptr;   // rows' cx, ru, rd, diagonal ([4][H0]) for the loss; S z, S t
+    double *dsc = nullptr, *dsc_inv = nullptr;             // per row D_k^{-1/2}, D_k^{1/2} ([NK])
     int* err = nullptr;
     int adam_t = 0;
     Stats* stats = nullptr;
@@ -981,14 +1000,33 @@ struct LearnedNet {
 
     // the cal_w operator's row coefficients (cx = 1/rhow_k, ru = 1/rhou_k,
     // rd = 1/rhou_{k-1}, k = kk + 2) in the network's rows
-    void set_operator(const std::vector<double>& rhou, const std::vector<double>& rhow) {
-        std::vector<float> h(3 * (size_t)H[0], 0.f);
+    // The network works in the variables of S~ = D^{-1/2} S D^{-1/2}, D the
+    // diagonal of S (2 cx_k + ru_k + rd_k): every row of S~ has diagonal 1, so
+    // its coefficients vary little from level to level even where the
+    // densities span orders of magnitude (deep or stretched levels), which a
+    // translation-invariant network needs. Input D^{-1/2} r, output mapped
+    // back by D^{-1/2}, target D^{1/2} e; (e, S e) = (D^{1/2} e, S~ D^{1/2} e).
+    void set_operator(const std::vector<double>& rhou, const std::vector<double>& rhow,
+                      const std::vector<double>& ma, const std::vector<double>& mh) {
+        std::vector<double> cx(NK), ru(NK), rd(NK), s(NK), si(NK);
         for (int kk = 0; kk < NK; kk++) {
             const int k = kk + 2;
-            h[kk] = (float)(1.0 / rhow[k]);
-            h[H[0] + kk] = (float)(1.0 / rhou[k]);
-            h[2 * H[0] + kk] = (float)(1.0 / rhou[k - 1]);
+            cx[kk] = ma[k] / rhow[k];
+            ru[kk] = mh[k] / rhou[k];
+            rd[kk] = mh[k - 1] / rhou[k - 1];
+            const double dg = 2.0 * cx[kk] + ru[kk] + rd[kk];
+            s[kk] = 1.0 / std::sqrt(dg);
+            si[kk] = std::sqrt(dg);
         }
+        std::vector<float> h(4 * (size_t)H[0], 0.f);
+        for (int kk = 0; kk < NK; kk++) {
+            h[kk] = (float)(cx[kk] * s[kk] * s[kk]);
+            h[H[0] + kk] = (float)(ru[kk] * s[kk] * (kk + 1 < NK ? s[kk + 1] : s[kk]));
+            h[2 * H[0] + kk] = (float)(rd[kk] * s[kk] * (kk > 0 ? s[kk - 1] : s[kk]));
+            h[3 * H[0] + kk] = 1.f;
+        }
+        upload_now(dsc, s.data(), NK * sizeof(double));
+        upload_now(dsc_inv, si.data(), NK * sizeof(double));
         upload_now(op, h.data(), h.size() * sizeof(float));
     }
 
@@ -1026,7 +1064,9 @@ struct LearnedNet {
         dh3 = ar.alloc<__nv_bfloat16>((size_t)H[3] * W[3] * kNetC);
         part = ar.alloc<double>(3 * 1024);
         lt = ar.alloc<double>(4);
-        op = ar.alloc<float>(3 * (size_t)H[0]);
+        op = ar.alloc<float>(4 * (size_t)H[0]);
+        dsc = ar.alloc<double>(NK);
+        dsc_inv = ar.alloc<double>(NK);
         sz = ar.alloc<float>(n0);
         st = ar.alloc<float>(n0);
         err = ar.alloc<int>(1);
@@ -1180,16 +1220,20 @@ struct PCG {
     CGCtl* ctl = nullptr;   // loop state of graph-captured solves
     Stats* stats = nullptr;
 
-    void build(Arena& ar, int NXr, int NKr, const std::vector<double>& rhou, const std::vector<double>& rhow) {
+    // S = -diag(1/rw) A in symmetric form: cx_k = a_k / rhow_k, ru_k = h_k /
+    // rhou_k, rd_k = h_{k-1} / rhou_{k-1}, rw_k = rhow_k / a_k (a = h = 1 on
+    // uniform levels: the reference's matrix, PoissonSolver.cpp:760-796).
+    void build(Arena& ar, int NXr, int NKr, const std::vector<double>& rhou, const std::vector<double>& rhow,
+               const std::vector<double>& a, const std::vector<double>& h) {
         NX = NXr;
         NK = NKr;
         std::vector<double> cx0(NK), ru(NK), rd(NK), rw(NK);
         for (int kk = 0; kk < NK; kk++) {
             int k = kk + 2;
-            cx0[kk] = 1.0 / rhow[k];
-            ru[kk] = 1.0 / rhou[k];
-            rd[kk] = 1.0 / rhou[k - 1];
-            rw[kk] = rhow[k];
+            cx0[kk] = a[k] / rhow[k];
+            ru[kk] = h[k] / rhou[k];
+            rd[kk] = h[k - 1] / rhou[k - 1];
+            rw[kk] = rhow[k] / a[k];
         }
         mg.stats = stats;
         mg.build(ar, NX, NK, cx0, ru, rd);
@@ -1356,6 +1400,12 @@ struct vvm_gpu_ctx {
     // perturbation profiles of th (0) and qv (1); used by the mixed step
     double *pref[2] = {}, *pd0[2] = {}, *ps0[2] = {}, *pg0[2] = {}, *pdn[2] = {};
     std::vector<double> h_rhou, h_rhow;
+    // vertical metric of the cal_w operator: a_k = (z_k - z_{k-1}) / dx, h_k =
+    // dx / (2 (z_k - z_zeta_k)); exactly 1 on uniform levels. `stretched`:
+    // non-uniform levels, which only the Poisson entries support.
+    std::vector<double> h_a, h_h;
+    bool stretched = false;
+    double* rwres = nullptr;   // [nz] residual weight rw_k = rhow_k / a_k
     double* ubar = nullptr;   // [0] ubarTop, [1] ubarTopp
     double* dubar = nullptr;  // [2]
     double *partial = nullptr, *nvp = nullptr;
@@ -1688,7 +1738,7 @@ void ensure_poisson(vvm_gpu_ctx* c) {
     c->pcg64.reset(new PCG<double>());
     c->pcg64->stats = &c->stats;
     c->pcg64->spectral = c->spectral;
-    c->pcg64->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
+    c->pcg64->build(c->ar, NX, NK, c->h_rhou, c->h_rhow, c->h_a, c->h_h);
     int pitch = c->pcg64->pitch;
     c->Wf = c->ar.alloc<double>((size_t)NK * pitch);
     c->W = c->ar.alloc<double>((size_t)NK * pitch);
@@ -1698,7 +1748,7 @@ void ensure_poisson(vvm_gpu_ctx* c) {
     if (c->mixed && !c->spectral) {
         c->pcg32.reset(new PCG<float>());
         c->pcg32->stats = &c->stats;
-        c->pcg32->build(c->ar, NX, NK, c->h_rhou, c->h_rhow);
+        c->pcg32->build(c->ar, NX, NK, c->h_rhou, c->h_rhow, c->h_a, c->h_h);
         c->g32 = c->ar.alloc<float>((size_t)NK * pitch);
         c->d32 = c->ar.alloc<float>((size_t)NK * pitch);
     }
@@ -1724,7 +1774,7 @@ void ensure_learned(vvm_gpu_ctx* c) {
     c->net.reset(new LearnedNet());
     c->net->stats = &c->stats;
     c->net->build(c->ar, NX, NK, 1);
-    c->net->set_operator(c->h_rhou, c->h_rhow);
+    c->net->set_operator(c->h_rhou, c->h_rhow, c->h_a, c->h_h);
     const size_t n = (size_t)NK * c->pcg64->pitch;
     c->z64 = c->ar.alloc<double>(n);
     c->za64 = c->ar.alloc<double>(n);
@@ -1764,15 +1814,15 @@ void learned_precond(vvm_gpu_ctx* c, const double* r, cudaStream_t st) {
     if (c->learned_mode == 0) {
         LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, r, c->za64, c->r164, P.partial));
         CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->r164, c->r164, P.partial));
+        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_sdot<<<G, B, 0, st>>>(v, c->r164, N.dsc, P.partial));
         CKL();
         LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_NRM));
         CKL();
         dim3 g0(cdiv(P.NX, 64), cdiv(N.H[0], 4));
-        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->r164, nullptr, P.NX, P.NK, P.pitch, N.x0, N.H[0], &P.sc->nrm));
+        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->r164, nullptr, P.NX, P.NK, P.pitch, N.x0, N.H[0], &P.sc->nrm, N.dsc));
         CKL();
         N.forward(st);
-        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_out<<<G, B, 0, st>>>(N.z0, P.NX, P.NK, P.pitch, c->d64, &P.sc->nrm));
+        LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_out<<<G, B, 0, st>>>(N.z0, P.NX, P.NK, P.pitch, c->d64, &P.sc->nrm, N.dsc));
         CKL();
         LAUNCH(&c->stats, VVM_K_CG, st, k_cg_spmv<double><<<G, B, 0, st>>>(v, c->d64, c->sd64, P.partial));
         CKL();
@@ -2049,7 +2099,7 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     int NX = c->d.nx - 2, NK = c->d.nz - 3;
     int pitch = c->pcg64->pitch;
     dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
-    LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_poisson_rhs<T><<<G, B, 0, c->stream>>>(c->d, c->c.dx, c->rhow, F.zeta[fut], c->Wf, pitch, c->wpartial));
+    LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_poisson_rhs<T><<<G, B, 0, c->stream>>>(c->d, c->c.dx, c->rhow, c->rwres, F.zeta[fut], c->Wf, pitch, c->wpartial));
     CKL();
     LAUNCH(&c->stats, VVM_K_CG, c->stream, k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, c->pcg64->sc, CG_SET_BB));
     CKL();
@@ -2652,11 +2702,38 @@ int upload_profiles(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
     }
     c->pf1 = 1E-3 * s->rhou[1];                                      // Iteration.cpp:115
     c->pf2 = std::pow(s->rhou[1] / s->rhow[1], -0.5);
+    // vertical metric from the level heights: uniform levels (every spacing
+    // equal to dz) keep the reference's operator exactly (a = h = 1, whatever
+    // dx is, as the reference's matrix assumes); otherwise the stretched one
+    std::vector<double> ma(nz, 1.0), mh(nz, 1.0);
+    bool uniform = true;
+    for (int k = 1; k < nz - 1; k++) {
+        const double dzu = 2.0 * (s->z[k] - s->z_zeta[k]);
+        if (!(dzu > 0)) return fail(c, VVM_GPU_EINVAL, "upload: level heights z must lie above z_zeta");
+        if (std::fabs(dzu - c->desc.dz) > 1e-9 * c->desc.dz) uniform = false;
+        mh[k] = c->desc.dx / dzu;
+    }
+    for (int k = 2; k < nz - 1; k++) {
+        const double dzw = s->z[k] - s->z[k - 1];
+        if (!(dzw > 0)) return fail(c, VVM_GPU_EINVAL, "upload: level heights z must increase");
+        if (std::fabs(dzw - c->desc.dz) > 1e-9 * c->desc.dz) uniform = false;
+        ma[k] = dzw / c->desc.dx;
+    }
+    if (uniform) {
+        std::fill(ma.begin(), ma.end(), 1.0);
+        std::fill(mh.begin(), mh.end(), 1.0);
+    }
+    c->stretched = !uniform;
+    std::vector<double> rw(nz);
+    for (int k = 0; k < nz; k++) rw[k] = s->rhow[k] / ma[k];
+    upload_profile(c, rw.data(), c->rwres);
     bool changed = c->h_rhou.empty() ||
                    !std::equal(c->h_rhou.begin(), c->h_rhou.end(), s->rhou) ||
-                   !std::equal(c->h_rhow.begin(), c->h_rhow.end(), s->rhow);
+                   !std::equal(c->h_rhow.begin(), c->h_rhow.end(), s->rhow) || c->h_a != ma || c->h_h != mh;
     c->h_rhou.assign(s->rhou, s->rhou + nz);
     c->h_rhow.assign(s->rhow, s->rhow + nz);
+    c->h_a = ma;
+    c->h_h = mh;
     if (changed && c->poisson_ready) {
         // the elliptic operator depends on rhou/rhow: rebuild on next use
         c->poisson_ready = false;
@@ -2745,6 +2822,15 @@ int guarded(vvm_gpu_ctx* c, Fn fn) {
 
 int need_state(vvm_gpu_ctx* c) {
     return c->has_state ? VVM_GPU_OK : fail(c, VVM_GPU_ESTATE, "no state uploaded");
+}
+
+// The step's stencils use one level spacing dz (the reference's); a state on
+// stretched levels supports the Poisson entries only.
+int need_uniform(vvm_gpu_ctx* c) {
+    return c->stretched ? fail(c, VVM_GPU_EINVAL,
+                               "stretched vertical levels: only the Poisson solve and the learned "
+                               "preconditioner's entries support them")
+                        : VVM_GPU_OK;
 }
 
 // Reads and clears the device error word (after the stream's work is done).
@@ -2849,7 +2935,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         int nz = c->d.nz;
         double** profs[] = {&c->rhou, &c->rhow, &c->thvb, &c->thb, &c->qvb, &c->thb_init, &c->qvb0,
                             &c->pib, &c->pb, &c->lambda2, &c->z, &c->z_zeta, &c->vt_c1, &c->vt_fac,
-                            &c->pc, &c->dtcgr_th, &c->dtcgr_zeta, &c->q1ls, &c->q2ls};
+                            &c->pc, &c->dtcgr_th, &c->dtcgr_zeta, &c->q1ls, &c->q2ls, &c->rwres};
         for (double** p : profs) *p = c->ar.alloc<double>(nz);
         for (int j = 0; j < 2; j++) {
             c->pref[j] = c->ar.alloc<double>(nz);
@@ -2967,6 +3053,7 @@ int vvm_gpu_get_step(vvm_gpu_ctx* ctx, int* step) {
     int name(vvm_gpu_ctx* ctx) {                                              \
         return guarded(ctx, [&]() -> int {                                    \
             if (int rc = need_state(ctx)) return rc;                          \
+            if (int rc = need_uniform(ctx)) return rc;                        \
             __VA_ARGS__;                                                      \
         });                                                                   \
     }
@@ -3014,6 +3101,7 @@ int vvm_gpu_step(vvm_gpu_ctx* ctx, int nsteps) {
     return guarded(ctx, [&]() -> int {
         if (int rc = need_state(ctx)) return rc;
         if (nsteps < 0) return fail(ctx, VVM_GPU_EINVAL, "step: nsteps < 0");
+        if (int rc = need_uniform(ctx)) return rc;
         int worst = VVM_GPU_OK;
         for (int s = 0; s < nsteps; s++) {
             int rc = DISPATCH(ctx, step_once)(ctx);
@@ -3031,7 +3119,7 @@ int vvm_gpu_poisson_solve_device(vvm_gpu_ctx* ctx, const double* d_b, double* d_
         ensure_poisson(ctx);
         int NX = ctx->d.nx - 2, NK = ctx->d.nz - 3, pitch = ctx->pcg64->pitch;
         dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
-        LAUNCH(&ctx->stats, VVM_K_POISSON_RHS, ctx->stream, k_rhs_from_b<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->rhow, d_b, ctx->Wf, pitch, ctx->wpartial));
+        LAUNCH(&ctx->stats, VVM_K_POISSON_RHS, ctx->stream, k_rhs_from_b<<<G, B, 0, ctx->stream>>>(NX, NK, ctx->rwres, d_b, ctx->Wf, pitch, ctx->wpartial));
         CKL();
         LAUNCH(&ctx->stats, VVM_K_CG, ctx->stream, k_cg_scalar<<<1, 1024, 0, ctx->stream>>>(ctx->wpartial, ctx->wnpart, ctx->pcg64->sc, CG_SET_BB));
         CKL();
@@ -3195,8 +3283,15 @@ int vvm_gpu_learned_eval(vvm_gpu_ctx* ctx, const float* x, const float* t, float
     });
 }
 
-int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, double lr, int seed,
-                          double* loss_first, double* loss_last) {
+// Training of the learned preconditioner. Pair sources: the caller's nb
+// right-hand sides b_host (nb x NX*(NZ-1), reference ordering) followed by as
+// many white-noise ones when given; otherwise half the model's own next steps
+// and half white noise, or all white noise on stretched levels (no model
+// steps there). Every pair is solved by the plain multigrid PCG; the model
+// state is put back afterwards. The noise stands for the rough residuals
+// flexible CG meets.
+static int learned_train_impl(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, double lr, int seed,
+                       const double* b_host, double* loss_first, double* loss_last) {
     if (!ctx) return VVM_GPU_EINVAL;
     if (npairs < 1 || steps < 0 || batch < 1 || !(lr > 0))
         return fail(ctx, VVM_GPU_EINVAL, "learned_train: bad arguments");
@@ -3219,9 +3314,17 @@ int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, do
         VecArgs<double> v = P.vargs();
         dim3 B = P.block(), G = P.grid(), g0(cdiv(P.NX, 64), cdiv(N.H[0], 4));
         int rc = VVM_GPU_OK;
-        const int nmodel = (npairs + 1) / 2;   // the rest: white-noise right-hand sides
+        const int nmodel = (b_host || c->stretched) ? 0 : (npairs + 1) / 2;   // the rest: white noise
+        const int nb = b_host ? npairs / 2 : 0;
+        const size_t nun = (size_t)P.NX * P.NK;
         for (int i = 0; i < npairs && rc == VVM_GPU_OK; i++) {
-            if (i < nmodel) {
+            if (i < nb) {   // the caller's right-hand side, solved by the plain solver
+                CK(cudaMemcpyAsync(c->staging, b_host + nun * i, nun * sizeof(double), cudaMemcpyHostToDevice, st));
+                LAUNCH(&c->stats, VVM_K_POISSON_RHS, st, k_rhs_from_b<<<G, B, 0, st>>>(P.NX, P.NK, c->rwres, c->staging, c->Wf, P.pitch, c->wpartial));
+                CKL();
+                double rel = 0;
+                P.solve(c->Wf, c->W, false, -1.0, 1e-10, 400, st, &rel);
+            } else if (i < nmodel) {
                 rc = c->mixed ? step_once<float>(c) : step_once<double>(c);
             } else {   // the residuals flexible CG meets are rough: noise, solved by the plain solver
                 LAUNCH(&c->stats, VVM_K_LEARNED, st, k_white_noise<<<G, B, 0, st>>>(c->Wf, P.NX, P.NK, P.pitch, (unsigned)(seed * 7919 + i)));
@@ -3234,13 +3337,13 @@ int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, do
             P.mg.sweep(0, c->Wf, nullptr, nullptr, 0, 0, c->z64, 1.0, st);
             LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->z64, c->r164, P.partial));
             CKL();
-            LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->r164, c->r164, P.partial));
+            LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_sdot<<<G, B, 0, st>>>(v, c->r164, N.dsc, P.partial));
             CKL();
             LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_NRM));
             CKL();
-            LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->r164, nullptr, P.NX, P.NK, P.pitch, px + n0 * i, N.H[0], &P.sc->nrm));
+            LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->r164, nullptr, P.NX, P.NK, P.pitch, px + n0 * i, N.H[0], &P.sc->nrm, N.dsc));
             CKL();
-            LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->W, c->z64, P.NX, P.NK, P.pitch, pt + n0 * i, N.H[0], &P.sc->nrm));
+            LAUNCH(&c->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(c->W, c->z64, P.NX, P.NK, P.pitch, pt + n0 * i, N.H[0], &P.sc->nrm, N.dsc_inv));
             CKL();
         }
         c->learned_collect = false;
@@ -3291,6 +3394,19 @@ int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, do
     });
 }
 
+
+int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, double lr, int seed,
+                          double* loss_first, double* loss_last) {
+    return learned_train_impl(ctx, npairs, steps, batch, lr, seed, nullptr, loss_first, loss_last);
+}
+
+int vvm_gpu_learned_train_rhs(vvm_gpu_ctx* ctx, const double* b, int npairs, int steps, int batch, double lr,
+                              int seed, double* loss_first, double* loss_last) {
+    if (!b) return fail(ctx, VVM_GPU_EINVAL, "learned_train_rhs: b is NULL");
+    if (npairs < 1) return fail(ctx, VVM_GPU_EINVAL, "learned_train_rhs: npairs < 1");
+    return learned_train_impl(ctx, 2 * npairs, steps, batch, lr, seed, b, loss_first, loss_last);
+}
+
 int vvm_gpu_learned_time(vvm_gpu_ctx* ctx, int reps, double* ms_forward, double* ms_convs) {
     if (!ctx || reps < 1) return VVM_GPU_EINVAL;
     return guarded(ctx, [&]() -> int {
@@ -3303,11 +3419,11 @@ int vvm_gpu_learned_time(vvm_gpu_ctx* ctx, int reps, double* ms_forward, double*
         // input: white noise over its norm, in the network's layout (work arrays only)
         LAUNCH(&ctx->stats, VVM_K_LEARNED, st, k_white_noise<<<G, B, 0, st>>>(ctx->r164, P.NX, P.NK, P.pitch, 12345u));
         CKL();
-        LAUNCH(&ctx->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(P.vargs(), ctx->r164, ctx->r164, P.partial));
+        LAUNCH(&ctx->stats, VVM_K_LEARNED, st, k_net_sdot<<<G, B, 0, st>>>(P.vargs(), ctx->r164, N.dsc, P.partial));
         CKL();
         LAUNCH(&ctx->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_NRM));
         CKL();
-        LAUNCH(&ctx->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(ctx->r164, nullptr, P.NX, P.NK, P.pitch, N.x0, N.H[0], &P.sc->nrm));
+        LAUNCH(&ctx->stats, VVM_K_LEARNED, st, k_net_in<<<g0, B, 0, st>>>(ctx->r164, nullptr, P.NX, P.NK, P.pitch, N.x0, N.H[0], &P.sc->nrm, N.dsc));
         CKL();
         N.forward(st);   // warm-up, and valid activations for convs_only
         cudaEvent_t e[4];
@@ -3429,6 +3545,8 @@ int vvm_gpu_batch_step(vvm_gpu_batch* b, int nsteps) {
     return batch_guarded(b, [&]() -> int {
         for (auto* c : b->cases)
             if (!c->has_state) return batch_fail(b, VVM_GPU_ESTATE, "batch_step: a case has no state uploaded");
+        for (auto* c : b->cases)
+            if (c->stretched) return batch_fail(b, VVM_GPU_EINVAL, "batch_step: a case has stretched levels");
         int rc = batch_step(b, nsteps);
         if (rc == VVM_GPU_ENOCONV) batch_fail(b, rc, "batch_step: a Poisson solve did not reach its tolerance");
         return rc;

@@ -79,7 +79,7 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream",
            "vvm_gpu_conv3x3_c32", "vvm_gpu_learned_shape", "vvm_gpu_learned_weights",
            "vvm_gpu_learned_eval", "vvm_gpu_learned_train", "vvm_gpu_learned_config",
-           "vvm_gpu_learned_last", "vvm_gpu_learned_time") + tuple(
+           "vvm_gpu_learned_last", "vvm_gpu_learned_time", "vvm_gpu_learned_train_rhs") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -133,6 +133,8 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_learned_config.argtypes = [vp, ip, ip]
     L.vvm_gpu_learned_last.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip)]
     L.vvm_gpu_learned_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.vvm_gpu_learned_train_rhs.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ip, ip, ip, ctypes.c_double, ip,
+                                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -403,6 +405,18 @@ class VVMGpu:
         self._check(self.L.vvm_gpu_learned_train(self.h, int(npairs), int(steps), int(batch), float(lr),
                                                  int(seed), ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def learned_train_rhs(self, b: np.ndarray, steps: int, batch: int = 4, lr: float = 1e-3, seed: int = 0):
+        """Trains on the given right-hand sides b [npairs][NX*(NZ-1)] (each
+        solved by the plain solver); returns (mean loss of the first, last ten
+        Adam steps)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        npairs = b.shape[0]
+        l0, l1 = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.vvm_gpu_learned_train_rhs(self.h, b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                     int(npairs), int(steps), int(batch), float(lr), int(seed),
+                                                     ctypes.byref(l0), ctypes.byref(l1)))
+        return l0.value, l1.value
 
     def learned_config(self, mode: int = 0, cap: int = 200):
         self._check(self.L.vvm_gpu_learned_config(self.h, int(mode), int(cap)))

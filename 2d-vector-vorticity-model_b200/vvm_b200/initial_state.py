@@ -109,7 +109,8 @@ def tetens_qvs(T: np.ndarray, p: np.ndarray) -> np.ndarray:
     return (380.0 / p) * np.exp(17.27 * (T - 273.0) / (T - 36.0))
 
 
-def base_state(g: GridSpec, theta_of_z, rh: float | np.ndarray, qv_of_z=None) -> dict:
+def base_state(g: GridSpec, theta_of_z, rh: float | np.ndarray, qv_of_z=None,
+               zf: np.ndarray | None = None) -> dict:
     """1D base state on the reference's staggering (src/Init.cpp:14-135).
 
     ``theta_of_z(z)`` gives the base potential temperature at cell-centre
@@ -120,6 +121,11 @@ def base_state(g: GridSpec, theta_of_z, rh: float | np.ndarray, qv_of_z=None) ->
     nz, dz = g.nz, g.dz
     k = np.arange(nz)
     zc = (k - 0.5) * dz
+    if zf is not None:   # stretched levels: faces zf[1..nz-1] (zf[1] = 0), centres midway
+        zf = np.asarray(zf, dtype=np.float64)
+        zc = np.zeros(nz)
+        zc[1:nz - 1] = 0.5 * (zf[1:nz - 1] + zf[2:nz])
+        zc[0], zc[nz - 1] = zc[1], zc[nz - 2]
     thb = np.zeros(nz)
     thb[1:nz - 1] = theta_of_z(zc[1:nz - 1])
     _center1d(thb)
@@ -138,10 +144,12 @@ def base_state(g: GridSpec, theta_of_z, rh: float | np.ndarray, qv_of_z=None) ->
         pib = np.zeros(nz)
         for kk in range(1, nz - 1):                           # src/Init.cpp:46-52
             if kk == 1:
-                pib[kk] = pisfc - GRAVITY * 0.5 * dz / (CP * thvb[kk])
+                h1 = 0.5 * dz if zf is None else zc[1] - zf[1]
+                pib[kk] = pisfc - GRAVITY * h1 / (CP * thvb[kk])
             else:
                 tvbavg = 0.5 * (thvb[kk] + thvb[kk - 1])
-                pib[kk] = pib[kk - 1] - GRAVITY * dz / (CP * tvbavg)
+                hk = dz if zf is None else zc[kk] - zc[kk - 1]
+                pib[kk] = pib[kk - 1] - GRAVITY * hk / (CP * tvbavg)
         _center1d(pib)
         if np.any(pib[1:nz - 1] <= 0.0):
             raise ValueError("base state: the Exner function reaches zero below the model "
@@ -184,9 +192,15 @@ def base_state(g: GridSpec, theta_of_z, rh: float | np.ndarray, qv_of_z=None) ->
     z_zeta = np.zeros(nz)
     lambda2 = np.zeros(nz)
     for kk in range(1, nz - 1):                               # src/Init.cpp:125-129
-        z[kk] = (kk - 0.5) * dz
-        z_zeta[kk] = (kk - 1) * dz
-        lambda2[kk] = 1.0 / (1.0 / math.pow(0.23 * math.sqrt(g.dx * dz), 2)
+        if zf is None:
+            z[kk] = (kk - 0.5) * dz
+            z_zeta[kk] = (kk - 1) * dz
+            dzk = dz
+        else:
+            z[kk] = zc[kk]
+            z_zeta[kk] = zf[kk]
+            dzk = zf[kk + 1] - zf[kk]
+        lambda2[kk] = 1.0 / (1.0 / math.pow(0.23 * math.sqrt(g.dx * dzk), 2)
                              + 1.0 / math.pow(0.4 * 0.4 * z[kk], 2))
     z[0], z[-1] = z[1], z[-2]
     z_zeta[0], z_zeta[-1] = z_zeta[1], z_zeta[-2]
@@ -282,3 +296,74 @@ def random_state(NX: int = 32, NZ: int = 16, dx: float = 200.0, dz: float = 200.
     st.scalars["dubarTop_advect"] = rng.normal(0.0, 1e-3, 2)
     st.scalars["step"] = 3
     return st
+
+
+def stretched_faces(NZ: int, dz_bottom: float, dz_top: float) -> np.ndarray:
+    """Face heights of NZ levels whose thickness grows from dz_bottom to dz_top
+    along a tanh ramp centred at mid-depth: dz_j = dz_bottom + (dz_top -
+    dz_bottom) (1 + tanh((j - NZ/2) / (NZ/6))) / 2, j = 0..NZ-1, rescaled so the
+    first and last thicknesses are exactly dz_bottom and dz_top. Returned on
+    the model's nz = NZ + 2 index: zf[k] for k = 1..NZ+1 (zf[1] = 0; zf[0] =
+    zf[1]); the level heights of a stretched case."""
+    j = np.arange(NZ, dtype=np.float64)
+    t = (1.0 + np.tanh((j - NZ / 2.0) / (NZ / 6.0))) / 2.0
+    t = (t - t[0]) / (t[-1] - t[0])
+    dzs = dz_bottom + (dz_top - dz_bottom) * t
+    zf = np.zeros(NZ + 2)
+    zf[2:] = np.cumsum(dzs)
+    zf[0] = zf[1]
+    return zf
+
+
+def stratified_theta(z):
+    """theta [K]: 300 K + 3 K/km up to 12 km, then growing by e every 15 km
+    (a stratosphere), so that the Exner function stays positive to the top of
+    deep stretched grids."""
+    z = np.asarray(z, dtype=np.float64)
+    tp = 300.0 + 3e-3 * 12000.0
+    return np.where(z <= 12000.0, 300.0 + 3e-3 * z, tp * np.exp((z - 12000.0) / 15000.0))
+
+
+def stretched_poisson_case(NX: int = 2048, NZ: int = 256, dx: float = 250.0,
+                           dz_bottom: float = 100.0, dz_top: float = 500.0,
+                           seed: int = 4, blobs: int = 6) -> VVMState:
+    """A Poisson-only state on stretched levels (tanh ramp dz_bottom ->
+    dz_top): the base state of a stratified atmosphere (stratified_theta,
+    80 % relative humidity) and a vorticity field of `blobs` seeded
+    bubble/cold-pool dipoles (Gaussian vortex pairs 2-6 km wide, 1-3 km deep,
+    centred in the lowest 8 km), the shape of the right-hand sides that warm
+    bubbles and squall lines give cal_w. Only rhou, rhow, z, z_zeta and zeta
+    matter to the solve."""
+    zf = stretched_faces(NZ, dz_bottom, dz_top)
+    g = GridSpec(NX, NZ, dx, dz_bottom, 1.0)
+    prof = base_state(g, stratified_theta, 0.8, zf=zf)
+    nx, nz = g.nx, g.nz
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nx)[:, None] - 0.5) * dx
+    z = prof["z"][None, :]
+    L = NX * dx
+    zeta = np.zeros((nx, nz))
+    for _ in range(blobs):
+        xc, zc = rng.uniform(0.0, L), rng.uniform(1000.0, 8000.0)
+        wx, wz = rng.uniform(2000.0, 6000.0), rng.uniform(1000.0, 3000.0)
+        amp = rng.uniform(0.5, 2.0) * 1e-2 * rng.choice((-1.0, 1.0))
+        dxp = (x - xc + 0.5 * L) % L - 0.5 * L           # periodic distance
+        for sgn, off in ((1.0, -0.5 * wx), (-1.0, 0.5 * wx)):
+            zeta += sgn * amp * np.exp(-((dxp - off) / (0.5 * wx)) ** 2 - ((z - zc) / wz) ** 2)
+    th = np.zeros((nx, nz))
+    th[1:nx - 1, 1:nz - 1] = prof["thb"][None, 1:nz - 1]
+    st = _assemble(g, prof, th, np.zeros((nx, nz)))
+    st.fields["zeta"][1:nx - 1, 1:nz - 1] = zeta[1:nx - 1, 1:nz - 1]
+    st.fields["zetap"][:] = st.fields["zeta"]
+    _westdown2d(st.fields["zeta"])
+    _westdown2d(st.fields["zetap"])
+    return st
+
+
+def poisson_rhs(st: VVMState, field: str = "zeta") -> np.ndarray:
+    """The right-hand side cal_w forms from a vorticity field
+    (src/PoissonSolver.cpp:444-450): b = rhow_k^2 (zeta[i+1][k] - zeta[i][k]) dx
+    for k = 2..nz-2, i = 1..nx-2, in the reference's vector ordering."""
+    z, rhow, dx = st.fields[field], st.prof["rhow"], st.grid.dx
+    nx, nz = z.shape
+    return np.concatenate([rhow[k] * rhow[k] * (z[2:nx, k] - z[1:nx - 1, k]) * dx for k in range(2, nz - 1)])

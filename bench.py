@@ -322,6 +322,7 @@ def our_arm(args, rank, world, device):
     }
     if not args.no_learned:
         line["learned"] = learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms / args.steps)
+        line["poisson_stretched"] = stretched_poisson_arm(world, device)
     if not args.no_ensemble:
         line["ensemble"] = ensemble_arm(args, rank, world, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -401,6 +402,65 @@ def learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms_per_step, st
     out["vs_plain_fp64_mgpcg"] = fp64_ms_per_step / out["with_net"]["ms_per_step"]
     out["iterations_saved_by_net"] = (out["without_net"]["fcg_iterations_last"]
                                       / max(out["with_net"]["fcg_iterations_last"], 1))
+    return out
+
+
+def stretched_poisson_arm(world, device, reps=5):
+    """the cal_w solve on NX=2048, NZ=256 stretched
+    levels (dz 100 m -> 500 m, tanh ramp; dx = 250 m), right-hand sides of
+    seeded bubble/cold-pool vorticity dipoles. Learned-PCG (trained on 16 such
+    right-hand sides plus 16 white-noise ones) against FP64 multigrid-PCG and
+    the spectral solve, each to ||b - A W|| / ||b|| <= 1e-10 from W = 0, device
+    buffers, event-timed on the library's stream; `ms_per_solve` is the mean of
+    `reps` solves after two warm-up solves."""
+    import torch
+    from vvm_b200.gpu import VVM_SOLVER_LEARNED, VVM_SOLVER_MGPCG, VVM_SOLVER_SPECTRAL, VVMGpu
+    from vvm_b200.initial_state import poisson_rhs, stretched_poisson_case
+    nx, nz = 2048, 256
+    st = stretched_poisson_case(nx, nz, seed=7)
+    b = poisson_rhs(st)
+    dev = torch.device(f"cuda:{device}")
+    d_b = torch.from_numpy(b).to(dev)
+    d_W = torch.zeros_like(d_b)
+    train = np.stack([poisson_rhs(stretched_poisson_case(nx, nz, seed=100 + s)) for s in range(16)])
+    out = {"workload": "cal_w on NX=2048 NZ=256 stretched levels dz 100->500 m (tanh), dx=250 m; "
+                       "rhs from 6 seeded vorticity dipoles", "tol": 1e-10}
+    stream = torch.cuda.current_stream()
+    for name, solver, mode in (("mgpcg_fp64", VVM_SOLVER_MGPCG, None), ("spectral_fp64", VVM_SOLVER_SPECTRAL, None),
+                               ("learned_pcg", VVM_SOLVER_LEARNED, 0), ("learned_cycle_without_net", VVM_SOLVER_LEARNED, 1)):
+        g = VVMGpu(st.grid, solver=solver, device=device)
+        g.set_stream(stream.cuda_stream)
+        g.upload(st)
+        rec = {}
+        if mode is not None:
+            if mode == 0:
+                t0 = time.perf_counter()
+                rec["train"] = g.learned_train_rhs(train, steps=300, batch=2, lr=2e-3, seed=3)
+                g.synchronize()
+                rec["train_s"] = time.perf_counter() - t0
+                w = g.learned_weights()
+            else:
+                g.learned_weights(w)
+            g.learned_config(mode=mode, cap=4000)
+        for _ in range(2):
+            d_W.zero_()
+            g.poisson_solve_device(d_b.data_ptr(), d_W.data_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):   # every solve from W = 0 (a warm start would reuse the last answer)
+            d_W.zero_()
+            it, rel = g.poisson_solve_device(d_b.data_ptr(), d_W.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        ms = dist_max(e0.elapsed_time(e1)) / reps
+        rec.update({"ms_per_solve": ms, "solves_per_s": world * 1e3 / ms, "iterations": it, "relres": rel})
+        if mode is not None:
+            rec["fcg_iterations"], rec["fell_back"] = g.learned_last()
+        out[name] = rec
+        g.close()
+    out["learned_vs_mgpcg_time"] = out["mgpcg_fp64"]["ms_per_solve"] / out["learned_pcg"]["ms_per_solve"]
+    out["net_iteration_ratio"] = (out["learned_cycle_without_net"]["fcg_iterations"]
+                                  / max(out["learned_pcg"]["fcg_iterations"], 1))
     return out
 
 

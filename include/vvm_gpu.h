@@ -157,7 +157,16 @@ int vvm_gpu_step(vvm_gpu_ctx* ctx, int nsteps);
  * Solves A W = b for the cal_w matrix (src/PoissonSolver.cpp:760-796) to
  * ||b - A W||_2 / ||b||_2 <= tol. Host arrays of (NX)*(NZ-1) doubles, unknown
  * index (k-2)*NX + (i-1), k = 2..nz-2, i = 1..nx-2 -- the reference's vector
- * ordering. W is used as the initial guess when warm_start is set. */
+ * ordering. W is used as the initial guess when warm_start is set.
+ *
+ * Stretched levels (no counterpart in the reference, whose levels are
+ * uniform): when the uploaded heights z (centres) and z_zeta (faces) are not
+ * uniform with spacing dz, A is the same anelastic operator discretised on
+ * those levels, times dx^2: ru_k = rhow_k h_k / (a_k rhou_k), rd_k = rhow_k
+ * h_{k-1} / (a_k rhou_{k-1}), a_k = (z_k - z_{k-1}) / dx, h_k = dx / (2 (z_k -
+ * z_zeta_k)) (centres midway between faces); b is unchanged. Such a context
+ * supports the Poisson and learned-preconditioner entries only; the step and
+ * routine entries return VVM_GPU_EINVAL. */
 int vvm_gpu_poisson_solve(vvm_gpu_ctx* ctx, const double* b, double* W, double tol,
                           int* iters, double* relres);
 /* Same on device buffers (cudaMalloc'd, same ordering); no host copies. */
@@ -217,6 +226,13 @@ int vvm_gpu_learned_weights(vvm_gpu_ctx* ctx, float* get, const float* set, int 
 int vvm_gpu_learned_eval(vvm_gpu_ctx* ctx, const float* x, const float* t, float* z, float* grad, double* loss);
 int vvm_gpu_learned_train(vvm_gpu_ctx* ctx, int npairs, int steps, int batch, double lr, int seed,
                           double* loss_first, double* loss_last);
+/* As _train, with the caller's right-hand sides: b holds npairs vectors of
+ * NX*(NZ-1) values in vvm_gpu_poisson_solve's ordering; each is solved by the
+ * plain multigrid PCG to make its pair, and as many white-noise right-hand
+ * sides are added (the rough residuals flexible CG meets). The source of
+ * model-like pairs on stretched levels, where the step does not run. */
+int vvm_gpu_learned_train_rhs(vvm_gpu_ctx* ctx, const double* b, int npairs, int steps, int batch, double lr,
+                              int seed, double* loss_first, double* loss_last);
 int vvm_gpu_learned_config(vvm_gpu_ctx* ctx, int mode, int cap);
 /* Times `reps` network forward passes on a white-noise input, and `reps`
  * passes of its six tensor-core convolutions alone, each between one pair of

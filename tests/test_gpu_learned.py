@@ -121,16 +121,22 @@ def _net_case(G, NX=64, NZ=32):
 
 
 def s_apply_ref(a, st, NK):
-    """The cal_w operator in symmetric form (poisson_kernels.cuh) on rows
-    < NK of a [H0][W0] torch array, zero beyond: the energy norm of the loss."""
+    """The operator the network works in on rows < NK of a [H0][W0] torch
+    array, zero beyond: the cal_w operator in symmetric form (uniform levels:
+    cx = 1/rhow_k, ru = 1/rhou_k, rd = 1/rhou_{k-1}) diagonally scaled,
+    D^{-1/2} S D^{-1/2} with D = 2 cx + ru + rd: the energy norm of the loss."""
     import torch
     rhou, rhow = st.prof["rhou"], st.prof["rhow"]
     k = np.arange(NK) + 2
-    cx = torch.tensor(1.0 / rhow[k])[:, None]
-    ru = torch.tensor(1.0 / rhou[k])[:, None]
-    rd = torch.tensor(1.0 / rhou[k - 1])[:, None]
+    cx0, ru0, rd0 = 1.0 / rhow[k], 1.0 / rhou[k], 1.0 / rhou[k - 1]
+    s = 1.0 / np.sqrt(2 * cx0 + ru0 + rd0)
+    s_up = np.append(s[1:], s[-1])
+    s_dn = np.insert(s[:-1], 0, s[0])
+    cx = torch.tensor(cx0 * s * s)[:, None]
+    ru = torch.tensor(ru0 * s * s_up)[:, None]
+    rd = torch.tensor(rd0 * s * s_dn)[:, None]
     b = a[:NK]
-    y = (2 * cx + ru + rd) * b - cx * (torch.roll(b, 1, 1) + torch.roll(b, -1, 1))
+    y = b - cx * (torch.roll(b, 1, 1) + torch.roll(b, -1, 1))
     up = torch.zeros_like(b)
     up[:-1] = b[1:]
     dn = torch.zeros_like(b)
@@ -142,8 +148,8 @@ def s_apply_ref(a, st, NK):
 
 
 def test_network_forward_and_gradient_match_torch(G):
-    """The loss L = 1 - (z, S t)^2 / ((z, S z)(t, S t)) and dL/dweights against
-    torch autograd in FP64 on the same weights (the device rounds
+    """The loss L = 1 - (z, S t)^2 / ((z, S z)(t, S t)) (S the scaled operator
+    of s_apply_ref) and dL/dweights against torch autograd in FP64 on the same weights (the device rounds
     weights and activations to BF16: relative bounds 2e-2 on z and L, 5e-2 on
     the gradient). The target is the network's own output plus noise of half
     its norm, so that (z, S t) is far from zero: with an unrelated target that
