@@ -316,12 +316,21 @@ def stretched_faces(NZ: int, dz_bottom: float, dz_top: float) -> np.ndarray:
 
 
 def stratified_theta(z):
-    """theta [K]: 300 K + 3 K/km up to 12 km, then growing by e every 15 km
-    (a stratosphere), so that the Exner function stays positive to the top of
-    deep stretched grids."""
+    """theta [K]: 300 K + 3 K/km up to 12 km, then growing by e every 22 km,
+    close to an isothermal stratosphere at the tropopause temperature (~210 K:
+    e-folding c_p T / g), so that the Exner function stays positive to the top
+    of deep stretched grids."""
     z = np.asarray(z, dtype=np.float64)
     tp = 300.0 + 3e-3 * 12000.0
-    return np.where(z <= 12000.0, 300.0 + 3e-3 * z, tp * np.exp((z - 12000.0) / 15000.0))
+    return np.where(z <= 12000.0, 300.0 + 3e-3 * z, tp * np.exp((z - 12000.0) / 22000.0))
+
+
+def dry_aloft(z, rh_low):
+    """Relative humidity rh_low up to 10 km, decaying with a 1.5 km scale
+    above (a nearly dry stratosphere: with moist air aloft the coupled
+    moisture-hydrostatic solve of base_state runs away to unphysical qv)."""
+    z = np.asarray(z, dtype=np.float64)
+    return np.where(z <= 10000.0, rh_low, rh_low * np.exp(-(z - 10000.0) / 1500.0))
 
 
 def stretched_poisson_case(NX: int = 2048, NZ: int = 256, dx: float = 250.0,
@@ -333,10 +342,12 @@ def stretched_poisson_case(NX: int = 2048, NZ: int = 256, dx: float = 250.0,
     bubble/cold-pool dipoles (Gaussian vortex pairs 2-6 km wide, 1-3 km deep,
     centred in the lowest 8 km), the shape of the right-hand sides that warm
     bubbles and squall lines give cal_w. Only rhou, rhow, z, z_zeta and zeta
-    matter to the solve."""
+    matter to the solve. Relative humidity: dry_aloft(z, 0.8)."""
     zf = stretched_faces(NZ, dz_bottom, dz_top)
     g = GridSpec(NX, NZ, dx, dz_bottom, 1.0)
-    prof = base_state(g, stratified_theta, 0.8, zf=zf)
+    zc = np.zeros(NZ + 2)
+    zc[1:NZ + 1] = 0.5 * (zf[1:NZ + 1] + zf[2:NZ + 2])
+    prof = base_state(g, stratified_theta, dry_aloft(zc, 0.8), zf=zf)
     nx, nz = g.nx, g.nz
     rng = np.random.default_rng(seed)
     x = (np.arange(nx)[:, None] - 0.5) * dx
@@ -367,3 +378,40 @@ def poisson_rhs(st: VVMState, field: str = "zeta") -> np.ndarray:
     z, rhow, dx = st.fields[field], st.prof["rhow"], st.grid.dx
     nx, nz = z.shape
     return np.concatenate([rhow[k] * rhow[k] * (z[2:nx, k] - z[1:nx - 1, k]) * dx for k in range(2, nz - 1)])
+
+
+def squall_line(NX: int = 1024, NZ: int = 128, dx: float = 250.0, dz: float = 250.0, dt: float = 2.0,
+                seed: int = 2, pool_amp: float = -3.0, pool_width: float = 10000.0,
+                pool_depth: float = 1500.0, u_top: float = 10.0, shear_depth: float = 2500.0) -> VVMState:
+    """Sheared squall line on uniform levels: theta from stratified_theta
+    (300 K + 3 K/km to 12 km, a stratosphere above, so deep domains stay warmer
+    than the Tetens formula's 36 K singularity), qv at
+    90 % relative humidity below 1.5 km falling linearly to 30 % at 10 km and
+    dry_aloft above; u
+    rising linearly from 0 to u_top over the lowest shear_depth, constant
+    above; a cold pool of pool_amp (cosine-tapered, pool_width wide,
+    pool_depth deep) at mid-domain; seeded N(0, 0.1 K) noise in the lowest
+    1 km. w = 0; zeta follows from the shear."""
+    g = GridSpec(NX, NZ, dx, dz, dt, 1)
+    nz = g.nz
+    zc = (np.arange(nz) - 0.5) * dz
+    rh = np.clip(np.where(zc <= 1500.0, 0.9, 0.9 - 0.6 * (zc - 1500.0) / 8500.0), 0.3, 0.9)
+    rh = np.where(zc <= 10000.0, rh, dry_aloft(zc, 0.3))
+    prof = base_state(g, stratified_theta, rh)
+    nx = g.nx
+    i = np.arange(nx)[:, None]
+    x = (i - 0.5) * dx
+    z = prof["z"][None, :]
+    xc = 0.5 * NX * dx
+    rx = np.abs(x - xc) / (0.5 * pool_width)
+    rz = z / pool_depth
+    pool = np.where((rx <= 1.0) & (rz <= 1.0),
+                    pool_amp * np.cos(0.5 * np.pi * rx) ** 2 * np.cos(0.5 * np.pi * rz) ** 2, 0.0)
+    rng = np.random.default_rng(seed)
+    noise = np.where(z <= 1000.0, rng.normal(0.0, 0.1, (nx, nz)), 0.0)
+    th = np.zeros((nx, nz))
+    th[1:nx - 1, 1:nz - 1] = (prof["thb"][None, 1:nz - 1] + pool[1:nx - 1, 1:nz - 1]
+                              + noise[1:nx - 1, 1:nz - 1])
+    u = np.zeros((nx, nz))
+    u[1:nx - 1, 1:nz - 1] = (u_top * np.minimum(z / shear_depth, 1.0))[:, 1:nz - 1] * np.ones((nx - 2, 1))
+    return _assemble(g, prof, th, u)

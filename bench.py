@@ -323,6 +323,9 @@ def our_arm(args, rank, world, device):
     if not args.no_learned:
         line["learned"] = learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms / args.steps)
         line["poisson_stretched"] = stretched_poisson_arm(world, device)
+    if not args.no_long_runs:
+        from vvm_b200.precision_runs import run as long_run
+        line["config5_squall_line"] = long_run("config5", variants=("fp64_mgpcg", "mixed_spectral"))
     if not args.no_ensemble:
         line["ensemble"] = ensemble_arm(args, rank, world, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -596,6 +599,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-case batched ensemble")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner step")
+    ap.add_argument("--no-long-runs", action="store_true",
+                    help="skip the 1800-step 8192x256 squall line (mixed vs FP64 domain means)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
