@@ -270,6 +270,10 @@ class VVMGpu:
     def upload(self, st: VVMState):
         hs, keep = self._host_state(st, True)
         self._check(self.L.vvm_gpu_upload_state(self.h, ctypes.byref(hs)))
+        # inputs the step reads but never changes: download() returns them too,
+        # so a downloaded state is complete (a restart file holds it all)
+        self._const = {"prof": {n: np.array(st.prof[n]) for n in tuple(_P) + ("Q1LS", "Q2LS") if n in st.prof},
+                       "fields": {n: np.array(st.fields[n]) for n in ("init_th_forcing",) if n in st.fields}}
 
     def download(self) -> VVMState:
         g = self.grid
@@ -291,6 +295,12 @@ class VVMGpu:
         st.scalars = dict(ubarTop=hs.ubarTop, ubarTopp=hs.ubarTopp,
                           dubarTop_advect=np.array([hs.dubarTop_advect[0], hs.dubarTop_advect[1]]),
                           step=hs.step)
+        const = getattr(self, "_const", None)
+        if const:
+            for n, a in const["prof"].items():
+                st.prof.setdefault(n, a.copy())
+            for n, a in const["fields"].items():
+                st.fields.setdefault(n, a.copy())
         return st
 
     def upload_prognostic(self, fields: dict):
