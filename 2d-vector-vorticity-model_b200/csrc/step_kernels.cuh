@@ -287,8 +287,11 @@ __device__ __forceinline__ T vt_flux(const PAdvArgs<T>& a, const T* qr, int i, i
     return T(a.p.rhow[k]) * VT * s;
 }
 
+// Mixed step: at most 64 registers a thread, four 256-thread blocks a SM
+// (the kernel is latency-bound; 72 registers allowed three). The FP64 step
+// keeps its register count: a cap would spill.
 template <typename T>
-__global__ void k_padv(PAdvArgs<T> a) {
+__global__ void __launch_bounds__(256, (kPert<T> ? 4 : 1)) k_padv(PAdvArgs<T> a) {
     __shared__ double sh[32 * 6];
     const Dims& d = a.d;
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -299,6 +302,9 @@ __global__ void k_padv(PAdvArgs<T> a) {
         const size_t id = d.at(i, k);
         const T dt15 = T(1.5 * a.c.dt), dt05 = T(0.5 * a.c.dt);
         const T ru = T(a.p.rhou[k]);
+        // mixed step: one division for the cell's flux divergences (the FP64
+        // step keeps the reference's (difference * r2d) / rhou per term)
+        const T sx = kPert<T> ? T(a.c.r2dx) / ru : T(0), sz = kPert<T> ? T(a.c.r2dz) / ru : T(0);
         // velocity parts of the four faces, shared by the four fields;
         // flux_u at nx-1 is the halo copy of flux_u at 1, flux_w at nz-1 is
         // zeroed (Advection.cpp:55-58)
@@ -325,8 +331,13 @@ __global__ void k_padv(PAdvArgs<T> a) {
                 T fw_p = top ? T(0)
                              : face_flux(Fwp, Fwp.hi ? X(v, i, k - 1) : T(0), X(v, i, k), X(v, i, k + 1),
                                          Fwp.hi ? X(v, i, k + 2) : T(0));
-                px = (fu_p - fu_0) * T(a.c.r2dx) / ru;
-                pz = (fw_p - fw_0) * T(a.c.r2dz) / ru;
+                if constexpr (kPert<T>) {
+                    px = (fu_p - fu_0) * sx;
+                    pz = (fw_p - fw_0) * sz;
+                } else {
+                    px = (fu_p - fu_0) * T(a.c.r2dx) / ru;
+                    pz = (fw_p - fw_0) * T(a.c.r2dz) / ru;
+                }
             } else {
                 // v = v0(k) + v': the v0 parts of both fluxes are added in
                 // difference form, 2 v0 (u[i+1] - u[i]) in x and
@@ -345,8 +356,8 @@ __global__ void k_padv(PAdvArgs<T> a) {
                              : T(a.p.s0[f][k + 1]) * (T(a.p.rhow[k + 1]) * a.w[d.at(i, k + 1)] - m0) +
                                    m0 * T(a.p.g0[f][k]);
                 T refx = T(2.0 * a.p.ref[f][k]) * (a.u[d.at(ip, k)] - a.u[d.at(i, k)]);
-                px = (fu_p - fu_0) * T(a.c.r2dx) / ru + refx * T(a.c.r2dx);
-                pz = (fw_p - fw_0 + refz) * T(a.c.r2dz) / ru;
+                px = (fu_p - fu_0) * sx + refx * T(a.c.r2dx);
+                pz = (fw_p - fw_0 + refz) * sz;
             }
             T t = -px - pz;
             T o = ab2_push(a.hn[f], a.ho[f], id, t, a.ab);
@@ -354,7 +365,7 @@ __global__ void k_padv(PAdvArgs<T> a) {
             if (f == 3 && a.do_vt) {
                 T gp = (k == d.nz - 2) ? T(0) : vt_flux(a, v, i, k + 1);
                 T g0 = vt_flux(a, v, i, k);
-                T tv = (gp - g0) * T(a.c.r2dz) / ru;
+                T tv = kPert<T> ? (gp - g0) * sz : (gp - g0) * T(a.c.r2dz) / ru;
                 T ov = ab2_push(a.hvt_n, a.hvt_o, id, tv, a.ab);
                 out += dt15 * tv - dt05 * ov;
             }
