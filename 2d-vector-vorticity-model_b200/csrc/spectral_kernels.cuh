@@ -200,6 +200,133 @@ __global__ void __launch_bounds__(64) k_spec_modes(SpecArgs<P> a) {
     }
 }
 
+// The same solve with each half's chains cut into kModeSegs segments: a
+// block takes 32 consecutive modes (lane = mode, so every load is coalesced)
+// with 2 * kModeSegs warps, warp (h, s) owning segment s of half h (about
+// NK / (2 kModeSegs) rows). Both the elimination y_k = (f_k + c_k y_prev)
+// inv_k and the back-substitution w_k = y_k - cp_k w_next are first-order
+// affine recurrences: each warp composes its segment's map (A, B), the maps
+// meet in shared memory, each warp takes its carry-in by chaining the maps
+// of the segments before it, and applies its rows. The twisted meeting is as
+// in k_spec_modes. The serial chain drops from NK/2 rows to about
+// 2 NK / (2 kModeSegs) + kModeSegs steps.
+constexpr int kModeSegs = 16;
+
+template <typename P>
+__global__ void __launch_bounds__(64 * kModeSegs) k_spec_modes_seg(SpecArgs<P> a) {
+    __shared__ P shA[2][kModeSegs][32][3];   // (A re, A im, B) per half, segment, lane
+    __shared__ P shY[2][32][2];              // the halves' last rows after elimination
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int h = warp / kModeSegs, sg = warp % kModeSegs;
+    const int m = blockIdx.x * 32 + lane;
+    const bool on = m <= a.NX / 2;
+    const int NK = a.NK, mid = a.mid;
+    const size_t mp = a.mpitch;
+    P* __restrict__ sre = a.sre;
+    P* __restrict__ sim = a.sim;
+    const P* __restrict__ inv = a.inv;
+    const P* __restrict__ cpv = a.cp;
+    const P* __restrict__ lc = h ? a.ru : a.rd;
+    // this half's rows in elimination order: k(j) = k0 + dir j, j < n
+    const int n = h ? NK - 1 - mid : mid + 1;
+    const int dir = h ? -1 : 1, k0 = h ? NK - 1 : 0;
+    const int L = (n + kModeSegs - 1) / kModeSegs;
+    const int j0 = min(n, sg * L), j1 = min(n, j0 + L);
+    auto at = [&](int j) { return (size_t)(k0 + dir * j) * mp + m; };
+
+    // elimination: local map over rows j0..j1-1
+    P Ar = P(0), Ai = P(0), Bm = P(1);
+    if (on) {
+        for (int j = j0; j < j1; j++) {
+            const size_t e = at(j);
+            const P iv = inv[e], c = lc[k0 + dir * j] * iv;
+            Ar = sre[e] * iv + c * Ar;
+            Ai = sim[e] * iv + c * Ai;
+            Bm = c * Bm;
+        }
+    }
+    shA[h][sg][lane][0] = Ar;
+    shA[h][sg][lane][1] = Ai;
+    shA[h][sg][lane][2] = Bm;
+    if (threadIdx.x < 64) (&shY[0][0][0])[threadIdx.x * 2] = (&shY[0][0][0])[threadIdx.x * 2 + 1] = P(0);   // an empty half: 0
+    __syncthreads();
+    P yr = P(0), yi = P(0);
+    for (int t = 0; t < sg; t++) {
+        const P b = shA[h][t][lane][2];
+        yr = shA[h][t][lane][0] + b * yr;
+        yi = shA[h][t][lane][1] + b * yi;
+    }
+    if (on) {
+        for (int j = j0; j < j1; j++) {
+            const size_t e = at(j);
+            const P iv = inv[e], c = lc[k0 + dir * j];
+            yr = (sre[e] + c * yr) * iv;
+            yi = (sim[e] + c * yi) * iv;
+            sre[e] = yr;
+            sim[e] = yi;
+        }
+    }
+    if (j0 < j1 && j1 == n) {
+        shY[h][lane][0] = yr;
+        shY[h][lane][1] = yi;
+    }
+    __syncthreads();
+    // the meeting rows mid (half 0) and mid + 1 (half 1)
+    P wmr = P(0), wmi = P(0);
+    if (on) {
+        const P cpm = cpv[(size_t)mid * mp + m], dn = a.den[m];
+        const P cqm = (mid + 1 < NK) ? cpv[(size_t)(mid + 1) * mp + m] : P(0);
+        const P ymr = shY[0][lane][0], ymi = shY[0][lane][1], zr = shY[1][lane][0], zi = shY[1][lane][1];
+        const P w0r = (ymr - cpm * zr) * dn, w0i = (ymi - cpm * zi) * dn;
+        if (h == 0) {
+            wmr = w0r;
+            wmi = w0i;
+        } else {
+            wmr = zr - cqm * w0r;
+            wmi = zi - cqm * w0i;
+        }
+    }
+    // back-substitution outwards over rows j = n-2 .. 0; segment sg takes
+    // min(j1, n-1) - 1 down to j0
+    const int jt = min(j1, n - 1);
+    Ar = P(0);
+    Ai = P(0);
+    Bm = P(1);
+    if (on) {
+        for (int j = jt - 1; j >= j0; j--) {
+            const size_t e = at(j);
+            const P c = -cpv[e];
+            Ar = sre[e] + c * Ar;
+            Ai = sim[e] + c * Ai;
+            Bm = c * Bm;
+        }
+    }
+    __syncthreads();   // every warp has read shY and finished the first maps
+    shA[h][sg][lane][0] = Ar;
+    shA[h][sg][lane][1] = Ai;
+    shA[h][sg][lane][2] = Bm;
+    __syncthreads();
+    P wr = wmr, wi = wmi;
+    for (int t = kModeSegs - 1; t > sg; t--) {
+        const P b = shA[h][t][lane][2];
+        wr = shA[h][t][lane][0] + b * wr;
+        wi = shA[h][t][lane][1] + b * wi;
+    }
+    if (on) {
+        if (j0 < j1 && j1 == n) {   // the meeting row
+            sre[at(n - 1)] = wmr;
+            sim[at(n - 1)] = wmi;
+        }
+        for (int j = jt - 1; j >= j0; j--) {
+            const size_t e = at(j);
+            wr = sre[e] - cpv[e] * wr;
+            wi = sim[e] - cpv[e] * wi;
+            sre[e] = wr;
+            sim[e] = wi;
+        }
+    }
+}
+
 // Rows 2b and 2b+1 of out ([NK][pitch]) from their spectra, scaled by 1/NX.
 template <typename P>
 __global__ void k_spec_inverse(SpecArgs<P> a, P* out) {

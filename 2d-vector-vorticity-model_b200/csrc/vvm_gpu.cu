@@ -763,7 +763,7 @@ struct Spectral {
         const int rows2 = cdiv(a.NK, 2);
         LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_forward<P><<<rows2, threads, smem, st>>>(a, r));
         CKL();
-        LAUNCH(stats, VVM_K_MG_COARSE, st, k_spec_modes<P><<<cdiv(2 * (a.NX / 2 + 1), 64), 64, 0, st>>>(a));
+        LAUNCH(stats, VVM_K_MG_COARSE, st, k_spec_modes_seg<P><<<cdiv(a.NX / 2 + 1, 32), 64 * kModeSegs, 0, st>>>(a));
         CKL();
         LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_inverse<P><<<rows2, threads, smem, st>>>(a, dst));
         CKL();
