@@ -42,27 +42,59 @@ struct SpecArgs {
     P *sre, *sim;            // spectra, [NK][mpitch]
 };
 
+// The twiddles exp(-2 pi i j / N), j < N/2, copied into shared memory (tw:
+// N values, real parts then imaginary) before the first barrier of a kernel.
+template <typename P>
+__device__ __forceinline__ void load_twiddles(P* tw, const SpecArgs<P>& a) {
+    for (int j = threadIdx.x; j < a.NX / 2; j += blockDim.x) {
+        tw[j] = a.twr[j];
+        tw[a.NX / 2 + j] = a.twi[j];
+    }
+}
+
 // In-place radix-2 FFT of N = 2^logN points held bit-reversed in (re, im);
 // sign -1 forward, +1 inverse (unnormalised). All threads of the block call it.
+// Twiddles come from shared memory (load_twiddles); a thread takes its
+// butterflies of a stage two at a time, loading both before computing.
 template <typename P>
-__device__ __forceinline__ void fft_shared(P* re, P* im, const SpecArgs<P>& a, bool inverse) {
+__device__ __forceinline__ void fft_shared(P* re, P* im, const P* tw, const SpecArgs<P>& a, bool inverse) {
     const int N = a.NX;
+    const P* twr = tw;
+    const P* twi = tw + N / 2;
     for (int s = 1; s <= a.logN; s++) {
         const int half = 1 << (s - 1);
         const int tstride = N >> s;
-        for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
-            const int j = t & (half - 1);
-            const int i0 = ((t >> (s - 1)) << s) + j;
-            const int i1 = i0 + half;
-            const P wr = __ldg(a.twr + j * tstride);
-            const P wi = inverse ? -__ldg(a.twi + j * tstride) : __ldg(a.twi + j * tstride);
-            const P xr = re[i1], xi = im[i1];
+        for (int t = threadIdx.x; t < N / 2; t += 2 * blockDim.x) {
+            const int t2 = t + blockDim.x;
+            const bool two = t2 < N / 2;
+            const int j = t & (half - 1), j2 = t2 & (half - 1);
+            const int i0 = ((t >> (s - 1)) << s) + j, i1 = i0 + half;
+            const int k0 = ((t2 >> (s - 1)) << s) + j2, k1 = k0 + half;
+            const P wr = twr[j * tstride], wi0 = twi[j * tstride];
+            const P xr = re[i1], xi = im[i1], ur = re[i0], ui = im[i0];
+            P wr2 = P(0), wi2 = P(0), yr = P(0), yi = P(0), zr = P(0), zi = P(0);
+            if (two) {
+                wr2 = twr[j2 * tstride];
+                wi2 = twi[j2 * tstride];
+                yr = re[k1];
+                yi = im[k1];
+                zr = re[k0];
+                zi = im[k0];
+            }
+            const P wi = inverse ? -wi0 : wi0;
             const P vr = xr * wr - xi * wi, vi = xr * wi + xi * wr;
-            const P ur = re[i0], ui = im[i0];
             re[i0] = ur + vr;
             im[i0] = ui + vi;
             re[i1] = ur - vr;
             im[i1] = ui - vi;
+            if (two) {
+                const P wj = inverse ? -wi2 : wi2;
+                const P qr = yr * wr2 - yi * wj, qi = yr * wj + yi * wr2;
+                re[k0] = zr + qr;
+                im[k0] = zi + qi;
+                re[k1] = zr - qr;
+                im[k1] = zi - qi;
+            }
         }
         __syncthreads();
     }
@@ -76,15 +108,17 @@ __global__ void k_spec_forward(SpecArgs<P> a, const P* r) {
     extern __shared__ unsigned char smem_raw[];
     P* re = reinterpret_cast<P*>(smem_raw);
     P* im = re + a.NX;
+    P* tw = im + a.NX;
     const int k0 = 2 * blockIdx.x, k1 = k0 + 1;
     const bool two = k1 < a.NK;
+    load_twiddles(tw, a);
     for (int j = threadIdx.x; j < a.NX; j += blockDim.x) {
         const int jr = bitrev(j, a.logN);
         re[jr] = r[(size_t)k0 * a.pitch + j];
         im[jr] = two ? r[(size_t)k1 * a.pitch + j] : P(0);
     }
     __syncthreads();
-    fft_shared(re, im, a, false);
+    fft_shared(re, im, tw, a, false);
     const int N = a.NX;
     for (int m = threadIdx.x; m <= N / 2; m += blockDim.x) {
         const int mn = (N - m) & (N - 1);
@@ -333,9 +367,11 @@ __global__ void k_spec_inverse(SpecArgs<P> a, P* out) {
     extern __shared__ unsigned char smem_raw[];
     P* re = reinterpret_cast<P*>(smem_raw);
     P* im = re + a.NX;
+    P* tw = im + a.NX;
     const int k0 = 2 * blockIdx.x, k1 = k0 + 1;
     const bool two = k1 < a.NK;
     const int N = a.NX;
+    load_twiddles(tw, a);
     for (int j = threadIdx.x; j < N; j += blockDim.x) {
         // Hermitian extension: X[N-m] = conj X[m]
         const bool lo = j <= N / 2;
@@ -352,7 +388,7 @@ __global__ void k_spec_inverse(SpecArgs<P> a, P* out) {
         im[jr] = ai + br;
     }
     __syncthreads();
-    fft_shared(re, im, a, true);
+    fft_shared(re, im, tw, a, true);
     const P scale = P(1) / P(N);
     for (int j = threadIdx.x; j < N; j += blockDim.x) {
         out[(size_t)k0 * a.pitch + j] = re[j] * scale;

@@ -750,10 +750,10 @@ struct Spectral {
         a.sre = ar.alloc<P>((size_t)NK * mp);
         a.sim = ar.alloc<P>((size_t)NK * mp);
         out = ar.alloc<P>((size_t)NK * pitch);
-        smem = 2 * (size_t)NX * sizeof(P);
+        smem = 3 * (size_t)NX * sizeof(P);   // the row pair (re, im) and the twiddles
         threads = std::max(32, std::min(NX / 2, 512));
         // per-kernel attribute: the largest row any context may have (NX = 8192)
-        const int smax = 2 * 8192 * (int)sizeof(P);
+        const int smax = 3 * 8192 * (int)sizeof(P);
         CK(cudaFuncSetAttribute(k_spec_forward<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
         CK(cudaFuncSetAttribute(k_spec_inverse<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax));
     }
