@@ -820,10 +820,32 @@ struct Tagged {
 // 2 * nz values of T.
 constexpr int kGSClusterWarps = 10;   // warps a CTA at most (NX = 8192: 9)
 
+// The carry of a row pair: two row-tagged values (the pair's first row as tag).
+template <typename T>
+struct Tagged2 {
+    static constexpr int kWords = 2 * Tagged<T>::kWords;
+    __device__ static void put(unsigned long long* w, T x0, T x1, int row) {
+        Tagged<T>::put(w, x0, row);
+        Tagged<T>::put(w + Tagged<T>::kWords, x1, row);
+    }
+    __device__ static bool get(const unsigned long long* w, int row, T& x0, T& x1) {
+        return Tagged<T>::get(w, row, x0) && Tagged<T>::get(w + Tagged<T>::kWords, row, x1);
+    }
+};
+
+// Two rows a step. With V_i = (v'(i, k), v'(i, k+1)) the pair obeys
+// V_i = alpha_i + M_i V_{i-1}, M_i = [[B_k, 0], [C_{k+1} B_k, B_{k+1}]],
+// alpha_i = (a_i, A0_{k+1} + C_{k+1} a_i), a_i = A0_k + C_k v'(i, k-1): one scan
+// over the row advances both rows, so the serial chain has half as many
+// steps, each with five values a shuffle round instead of two (the rounds'
+// shuffles are independent and overlap). The cells are then applied with the
+// scalar formulas, row k first. An odd last row runs as a pair whose second
+// row is the identity and is not stored.
 template <typename T, int PER, int D, int CS>
 __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(32 * kGSClusterWarps) k_gs_cluster(GSArgs<T> a) {
+    static_assert(D % 2 == 0, "the ring holds whole row pairs");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int kW = Tagged<T>::kWords;
+    constexpr int kW = Tagged2<T>::kWords;
     __shared__ unsigned long long inbox[kGSClusterWarps][kGSCarry][kW];
     __shared__ int ack_in[kGSClusterWarps], abort_flag;
     namespace cgx = cooperative_groups;
@@ -856,7 +878,6 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(32 * kGSClusterWarp
     const bool run = (a.mask & (1 << f)) && g < gwn;
     if (run) {
         T* v = a.v[f];
-        const bool mom = (f == 0);
         const int i0 = (g * 32 + lane) * PER;
         const bool act = i0 < d.pitch;       // pitch is a multiple of PER
         const size_t fo = (size_t)f * d.cells();
@@ -885,11 +906,11 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(32 * kGSClusterWarp
             for (int r = 0; r < CS; r++) *(volatile int*)cl.map_shared_rank(&abort_flag, r) = 1;
             if (a.err) atomicOr(a.err, kGSErrWait);
         };
-        auto wait_carry = [&](int k, T& x) {   // all lanes; warp-uniform result
+        auto wait_carry = [&](int k, T& x0, T& x1) {   // all lanes; warp-uniform result
             bool okw = false;
             const unsigned long long* w = &inbox[wid][k % kGSCarry][0];
             for (int it = 0; it < kGSSpinLimit; it++) {
-                if (Tagged<T>::get(w, k, x)) {
+                if (Tagged2<T>::get(w, k, x0, x1)) {
                     okw = true;
                     break;
                 }
@@ -922,98 +943,130 @@ __global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(32 * kGSClusterWarp
         for (int r = 0; r < D; r++) issue(1 + r, r);
         bool ok = true;
         int ack_seen = 0;   // last acknowledgement read from warp g+1
-        auto row = [&](int k, int r) {
-            const T dn = dn_tab[k], tn = tn_tab[k];
+        auto pair = [&](int k, int r) {   // rows k and k+1 (k+1 may be past the last row)
+            const bool two = k + 1 <= kend;
+            const T dn0 = dn_tab[k], tn0 = tn_tab[k];
+            const T dn1 = two ? dn_tab[k + 1] : T(0), tn1 = two ? tn_tab[k + 1] : T(0);
             const int s = k % kGSCarry;
-            // read the carry-in early: when warp g-1 is ahead (the steady
-            // state) it is there and the read overlaps the scan below
-            T xin = T(0);             // warp 0 starts at the ghost's constant map
-            bool have = !has_pred || Tagged<T>::get(&inbox[wid][s][0], k, xin);
-            cp_async_wait<D - 1>();
-            T Aa[PER], Bk[PER];
+            // read the carry-in early: when warp g-1 is ahead it is there
+            T x0 = T(0), x1 = T(0);   // warp 0 starts at the ghost's constant map
+            bool have = !has_pred || Tagged2<T>::get(&inbox[wid][s][0], k, x0, x1);
+            cp_async_wait<D - 2>();
+            T Aa[PER], Bk[PER], A2[PER], C2[PER], B2[PER];
             if (act) {
                 const T* sa = slot(r, 0);
                 const T* scc = slot(r, 1);
                 const T* sb = slot(r, 2);
+                const T* ta = slot(r + 1, 0);
+                const T* tc = slot(r + 1, 1);
+                const T* tb = slot(r + 1, 2);
 #pragma unroll
                 for (int e = 0; e < PER; e++) {
                     Aa[e] = sa[e] + scc[e] * vdn[e];
                     Bk[e] = sb[e];
+                    A2[e] = two ? ta[e] : T(0);
+                    C2[e] = two ? tc[e] : T(0);
+                    B2[e] = two ? tb[e] : T(1);
                 }
             } else {
 #pragma unroll
                 for (int e = 0; e < PER; e++) {
                     Aa[e] = T(0);
                     Bk[e] = T(1);
+                    A2[e] = T(0);
+                    C2[e] = T(0);
+                    B2[e] = T(1);
                 }
             }
-            T cA = T(0), cB = T(1);
+            // the lane's map over its cells: (p0, p1) offsets, M = [[m00, 0], [m10, m11]]
+            T p0 = T(0), p1 = T(0), m00 = T(1), m10 = T(0), m11 = T(1);
 #pragma unroll
             for (int e = 0; e < PER; e++) {
-                cA = Aa[e] + Bk[e] * cA;
-                cB = Bk[e] * cB;
+                const T c0 = Aa[e], c1 = A2[e] + C2[e] * Aa[e];
+                const T n00 = Bk[e], n10 = C2[e] * Bk[e], n11 = B2[e];
+                p1 = c1 + n10 * p0 + n11 * p1;
+                p0 = c0 + n00 * p0;
+                m10 = n10 * m00 + n11 * m10;
+                m00 = n00 * m00;
+                m11 = n11 * m11;
             }
             issue(k + D, r);
-            T sA = cA, sB = cB;
+            issue(k + 1 + D, r + 1);
+            T s0 = p0, s1 = p1, s00 = m00, s10 = m10, s11 = m11;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                T qA = __shfl_up_sync(0xffffffffu, sA, o);
-                T qB = __shfl_up_sync(0xffffffffu, sB, o);
-                if (lane >= o) {
-                    sA = sA + sB * qA;
-                    sB = sB * qB;
+                const T q0 = __shfl_up_sync(0xffffffffu, s0, o), q1 = __shfl_up_sync(0xffffffffu, s1, o);
+                const T q00 = __shfl_up_sync(0xffffffffu, s00, o), q10 = __shfl_up_sync(0xffffffffu, s10, o);
+                const T q11 = __shfl_up_sync(0xffffffffu, s11, o);
+                if (lane >= o) {   // own map after the lower lanes'
+                    s1 = s1 + s10 * q0 + s11 * q1;
+                    s0 = s0 + s00 * q0;
+                    s10 = s10 * q00 + s11 * q10;
+                    s00 = s00 * q00;
+                    s11 = s11 * q11;
                 }
             }
-            const T tA = __shfl_sync(0xffffffffu, sA, 31), tB = __shfl_sync(0xffffffffu, sB, 31);
-            T eA = __shfl_up_sync(0xffffffffu, sA, 1), eB = __shfl_up_sync(0xffffffffu, sB, 1);
+            const T t0 = __shfl_sync(0xffffffffu, s0, 31), t1 = __shfl_sync(0xffffffffu, s1, 31);
+            const T t00 = __shfl_sync(0xffffffffu, s00, 31), t10 = __shfl_sync(0xffffffffu, s10, 31);
+            const T t11 = __shfl_sync(0xffffffffu, s11, 31);
+            T e0 = __shfl_up_sync(0xffffffffu, s0, 1), e1 = __shfl_up_sync(0xffffffffu, s1, 1);
+            T e00 = __shfl_up_sync(0xffffffffu, s00, 1), e10 = __shfl_up_sync(0xffffffffu, s10, 1);
+            T e11 = __shfl_up_sync(0xffffffffu, s11, 1);
             if (lane == 0) {
-                eA = T(0);
-                eB = T(1);
+                e0 = T(0);
+                e1 = T(0);
+                e00 = T(1);
+                e10 = T(0);
+                e11 = T(1);
             }
             if (has_pred) {
-                if (!__all_sync(0xffffffffu, have)) ok = ok && wait_carry(k, xin);
-                if (k % kGSAckEvery == 0) {
+                if (!__all_sync(0xffffffffu, have)) ok = ok && wait_carry(k, x0, x1);
+                if (((k - 1) >> 1) % (kGSAckEvery / 2) == 0) {   // every kGSAckEvery rows
                     __syncwarp();
                     if (lane == 0) st_release_cluster(pred_ack, k);
                 }
             }
             if (has_succ) {
-                // slot s last held row k - kGSCarry; acknowledgements come in
-                // steps of kGSAckEvery rows, so the flag is read (acquire)
-                // only when the last one seen does not cover that row
+                // slot s last held the pair at row k - kGSCarry
                 if (ack_seen < k - kGSCarry) {
                     ok = ok && wait_ge(&ack_in[wid], k - kGSCarry);
                     ack_seen = ld_acquire_cluster(&ack_in[wid]);
                 }
-                if (lane == 0) Tagged<T>::put(succ_box + (size_t)s * kW, tA + tB * xin, k);
+                if (lane == 0) Tagged2<T>::put(succ_box + (size_t)s * kW, t0 + t00 * x0, t1 + t10 * x0 + t11 * x1, k);
             }
-            T x = eA + eB * xin;
-            T out[PER];
+            T y0 = e0 + e00 * x0, y1 = e1 + e10 * x0 + e11 * x1;
+            T out0[PER], out1[PER];
 #pragma unroll
             for (int e = 0; e < PER; e++) {
-                x = Aa[e] + Bk[e] * x;
-                vdn[e] = x;
-                out[e] = x - dn * (x - tn);
+                y0 = Aa[e] + Bk[e] * y0;
+                y1 = (A2[e] + C2[e] * y0) + B2[e] * y1;
+                vdn[e] = y1;
+                out0[e] = y0 - dn0 * (y0 - tn0);
+                out1[e] = y1 - dn1 * (y1 - tn1);
             }
-            T* dst = v + d.at(i0, k);
-            if (act && i0 >= 1 && i0 + PER - 1 <= NX) {
+            auto store = [&](int kk, const T (&out)[PER]) {
+                T* dst = v + d.at(i0, kk);
+                if (act && i0 >= 1 && i0 + PER - 1 <= NX) {
 #pragma unroll
-                for (int q = 0; q < PER; q += kVec) {
-                    if constexpr (sizeof(T) == 4)
-                        *reinterpret_cast<float4*>(dst + q) = make_float4(out[q], out[q + 1], out[q + 2], out[q + 3]);
-                    else
-                        *reinterpret_cast<double2*>(dst + q) = make_double2(out[q], out[q + 1]);
+                    for (int q = 0; q < PER; q += kVec) {
+                        if constexpr (sizeof(T) == 4)
+                            *reinterpret_cast<float4*>(dst + q) = make_float4(out[q], out[q + 1], out[q + 2], out[q + 3]);
+                        else
+                            *reinterpret_cast<double2*>(dst + q) = make_double2(out[q], out[q + 1]);
+                    }
+                } else if (act) {
+#pragma unroll
+                    for (int e = 0; e < PER; e++)
+                        if (i0 + e >= 1 && i0 + e <= NX) dst[e] = out[e];
                 }
-            } else if (act) {
-#pragma unroll
-                for (int e = 0; e < PER; e++)
-                    if (i0 + e >= 1 && i0 + e <= NX) dst[e] = out[e];
-            }
+            };
+            store(k, out0);
+            if (two) store(k + 1, out1);
         };
         for (int k = 1; k <= kend && ok; k += D) {
 #pragma unroll
-            for (int r = 0; r < D; r++)
-                if (k + r <= kend && ok) row(k + r, r);
+            for (int r = 0; r < D; r += 2)
+                if (k + r <= kend && ok) pair(k + r, r);
         }
         cp_async_wait<0>();
     }
