@@ -52,49 +52,71 @@ __device__ __forceinline__ void load_twiddles(P* tw, const SpecArgs<P>& a) {
     }
 }
 
-// In-place radix-2 FFT of N = 2^logN points held bit-reversed in (re, im);
-// sign -1 forward, +1 inverse (unnormalised). All threads of the block call it.
-// Twiddles come from shared memory (load_twiddles); a thread takes its
-// butterflies of a stage two at a time, loading both before computing.
+// One radix-2 butterfly of the DIT FFT: (u, x) -> (u + w x, u - w x).
+template <typename P>
+__device__ __forceinline__ void fft_bfly(P& ur, P& ui, P& xr, P& xi, P wr, P wi) {
+    const P vr = xr * wr - xi * wi, vi = xr * wi + xi * wr;
+    const P r0 = ur + vr, i0 = ui + vi;
+    xr = ur - vr;
+    xi = ui - vi;
+    ur = r0;
+    ui = i0;
+}
+
+// In-place radix-2 DIT FFT of N = 2^logN points held bit-reversed in (re,
+// im); sign -1 forward, +1 inverse (unnormalised). All threads of the block
+// call it. Twiddles come from shared memory (load_twiddles). Stages go two at
+// a time: for stages s, s+1 (h = 2^(s-1)) a thread holds the four points
+// base + {0, h, 2h, 3h} of one group in registers, does stage s's two
+// butterflies (same twiddle) and stage s+1's two, each exactly as the
+// one-stage form does it (same operations, same table twiddles: the result
+// is bit for bit that of eleven single stages), with half the passes through
+// shared memory and half the barriers; an odd last stage runs alone.
 template <typename P>
 __device__ __forceinline__ void fft_shared(P* re, P* im, const P* tw, const SpecArgs<P>& a, bool inverse) {
     const int N = a.NX;
     const P* twr = tw;
     const P* twi = tw + N / 2;
-    for (int s = 1; s <= a.logN; s++) {
+    const P sg = inverse ? P(-1) : P(1);
+    int s = 1;
+    for (; s + 1 <= a.logN; s += 2) {
+        const int h = 1 << (s - 1);
+        const int ts1 = N >> s, ts2 = N >> (s + 1);
+        for (int t = threadIdx.x; t < N / 4; t += blockDim.x) {
+            const int j = t & (h - 1);
+            const int b0 = ((t >> (s - 1)) << (s + 1)) + j;
+            P r0 = re[b0], i0 = im[b0], r1 = re[b0 + h], i1 = im[b0 + h];
+            P r2 = re[b0 + 2 * h], i2 = im[b0 + 2 * h], r3 = re[b0 + 3 * h], i3 = im[b0 + 3 * h];
+            const P w1r = twr[j * ts1], w1i = sg * twi[j * ts1];
+            fft_bfly(r0, i0, r1, i1, w1r, w1i);   // stage s: (b0, b0+h), (b0+2h, b0+3h)
+            fft_bfly(r2, i2, r3, i3, w1r, w1i);
+            const P w2r = twr[j * ts2], w2i = sg * twi[j * ts2];
+            const P w3r = twr[(j + h) * ts2], w3i = sg * twi[(j + h) * ts2];
+            fft_bfly(r0, i0, r2, i2, w2r, w2i);   // stage s+1: (b0, b0+2h), (b0+h, b0+3h)
+            fft_bfly(r1, i1, r3, i3, w3r, w3i);
+            re[b0] = r0;
+            im[b0] = i0;
+            re[b0 + h] = r1;
+            im[b0 + h] = i1;
+            re[b0 + 2 * h] = r2;
+            im[b0 + 2 * h] = i2;
+            re[b0 + 3 * h] = r3;
+            im[b0 + 3 * h] = i3;
+        }
+        __syncthreads();
+    }
+    if (s == a.logN) {   // the last stage alone
         const int half = 1 << (s - 1);
         const int tstride = N >> s;
-        for (int t = threadIdx.x; t < N / 2; t += 2 * blockDim.x) {
-            const int t2 = t + blockDim.x;
-            const bool two = t2 < N / 2;
-            const int j = t & (half - 1), j2 = t2 & (half - 1);
+        for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
+            const int j = t & (half - 1);
             const int i0 = ((t >> (s - 1)) << s) + j, i1 = i0 + half;
-            const int k0 = ((t2 >> (s - 1)) << s) + j2, k1 = k0 + half;
-            const P wr = twr[j * tstride], wi0 = twi[j * tstride];
-            const P xr = re[i1], xi = im[i1], ur = re[i0], ui = im[i0];
-            P wr2 = P(0), wi2 = P(0), yr = P(0), yi = P(0), zr = P(0), zi = P(0);
-            if (two) {
-                wr2 = twr[j2 * tstride];
-                wi2 = twi[j2 * tstride];
-                yr = re[k1];
-                yi = im[k1];
-                zr = re[k0];
-                zi = im[k0];
-            }
-            const P wi = inverse ? -wi0 : wi0;
-            const P vr = xr * wr - xi * wi, vi = xr * wi + xi * wr;
-            re[i0] = ur + vr;
-            im[i0] = ui + vi;
-            re[i1] = ur - vr;
-            im[i1] = ui - vi;
-            if (two) {
-                const P wj = inverse ? -wi2 : wi2;
-                const P qr = yr * wr2 - yi * wj, qi = yr * wj + yi * wr2;
-                re[k0] = zr + qr;
-                im[k0] = zi + qi;
-                re[k1] = zr - qr;
-                im[k1] = zi - qi;
-            }
+            P ur = re[i0], ui = im[i0], xr = re[i1], xi = im[i1];
+            fft_bfly(ur, ui, xr, xi, twr[j * tstride], sg * twi[j * tstride]);
+            re[i0] = ur;
+            im[i0] = ui;
+            re[i1] = xr;
+            im[i1] = xi;
         }
         __syncthreads();
     }
