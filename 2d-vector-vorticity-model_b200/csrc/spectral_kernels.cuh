@@ -155,116 +155,18 @@ __global__ void k_spec_forward(SpecArgs<P> a, const P* r) {
     }
 }
 
-// The z solve of every mode m = 0..NX/2 in place on the spectra: two adjacent
-// threads per mode, the even one for the rows 0..mid, the odd one for
-// mid+1..NK-1 (real and imaginary parts share the factors). Each chain is
-// serial in k, so rows are taken kModeBatch at a time: the batch's loads are
-// issued together and the chain then runs from registers.
-constexpr int kModeBatch = 16;
-
-template <typename P>
-__global__ void __launch_bounds__(64) k_spec_modes(SpecArgs<P> a) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int m = t >> 1, half = t & 1;
-    const bool on = m <= a.NX / 2;          // the pair is inactive together (m is shared)
-    const size_t mp = a.mpitch;
-    P* __restrict__ sre = a.sre;
-    P* __restrict__ sim = a.sim;
-    const P* __restrict__ inv = a.inv;
-    const P* __restrict__ cpv = a.cp;
-    const int NK = a.NK, mid = a.mid;
-    // this half's rows in elimination order: k = k0 + dir * j, j < n
-    const int dir = half ? -1 : 1;
-    const int k0 = half ? NK - 1 : 0;
-    const int n = half ? NK - 1 - mid : mid + 1;
-    const P* __restrict__ lc = half ? a.ru : a.rd;   // coupling to the previously eliminated row
-    P yr = P(0), yi = P(0);
-    if (on) {
-        for (int j0 = 0; j0 < n; j0 += kModeBatch) {
-            P fr[kModeBatch], fi[kModeBatch], iv[kModeBatch], cl[kModeBatch];
-#pragma unroll
-            for (int j = 0; j < kModeBatch; j++) {
-                if (j0 + j < n) {
-                    const int kk = k0 + dir * (j0 + j);
-                    const size_t e = (size_t)kk * mp + m;
-                    fr[j] = sre[e];
-                    fi[j] = sim[e];
-                    iv[j] = inv[e];
-                    cl[j] = lc[kk];
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < kModeBatch; j++) {
-                if (j0 + j < n) {
-                    const int kk = k0 + dir * (j0 + j);
-                    yr = (fr[j] + cl[j] * yr) * iv[j];
-                    yi = (fi[j] + cl[j] * yi) * iv[j];
-                    const size_t e = (size_t)kk * mp + m;
-                    sre[e] = yr;
-                    sim[e] = yi;
-                }
-            }
-        }
-    }
-    // meeting rows: the even lane holds y_mid, the odd lane z_{mid+1}
-    const int klast = k0 + dir * (n - 1);
-    const P clast = on ? cpv[(size_t)klast * mp + m] : P(0);
-    const P orr = __shfl_xor_sync(0xffffffffu, yr, 1);
-    const P oi = __shfl_xor_sync(0xffffffffu, yi, 1);
-    const P oc = __shfl_xor_sync(0xffffffffu, clast, 1);
-    if (!on) return;
-    const P dn = a.den[m];
-    P ymr, ymi, zr, zi, cpm, cqm;
-    if (half == 0) {
-        ymr = yr; ymi = yi; cpm = clast; zr = orr; zi = oi; cqm = oc;
-    } else {
-        ymr = orr; ymi = oi; cpm = oc; zr = yr; zi = yi; cqm = clast;
-    }
-    const P wpr = (ymr - cpm * zr) * dn, wpi = (ymi - cpm * zi) * dn;      // w_mid
-    if (half == 0) {
-        yr = wpr;
-        yi = wpi;
-    } else {
-        yr = zr - cqm * wpr;                                                  // w_{mid+1}
-        yi = zi - cqm * wpi;
-    }
-    sre[(size_t)klast * mp + m] = yr;
-    sim[(size_t)klast * mp + m] = yi;
-    // back-substitute outwards: w_k = y_k - cp_k w_next over this half's
-    // remaining rows, nearest the middle first
-    for (int j0 = n - 2; j0 >= 0; j0 -= kModeBatch) {
-        P fr[kModeBatch], fi[kModeBatch], c[kModeBatch];
-#pragma unroll
-        for (int j = 0; j < kModeBatch; j++) {
-            if (j0 - j >= 0) {
-                const size_t e = (size_t)(k0 + dir * (j0 - j)) * mp + m;
-                fr[j] = sre[e];
-                fi[j] = sim[e];
-                c[j] = cpv[e];
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kModeBatch; j++) {
-            if (j0 - j >= 0) {
-                yr = fr[j] - c[j] * yr;
-                yi = fi[j] - c[j] * yi;
-                const size_t e = (size_t)(k0 + dir * (j0 - j)) * mp + m;
-                sre[e] = yr;
-                sim[e] = yi;
-            }
-        }
-    }
-}
-
-// The same solve with each half's chains cut into kModeSegs segments: a
-// block takes 32 consecutive modes (lane = mode, so every load is coalesced)
+// The z solve of every mode m = 0..NX/2 in place on the spectra, by the
+// twisted factorisation precomputed per mode (inv, cp, den): rows 0..mid are
+// eliminated from the bottom up (coupling rd), rows NK-1..mid+1 from the top
+// down (coupling ru), the two meet at rows mid, mid+1, and both halves
+// back-substitute outwards. Each half's chains are cut into kModeSegs
+// segments: a block takes 32 consecutive modes (lane = mode, so every load is coalesced)
 // with 2 * kModeSegs warps, warp (h, s) owning segment s of half h (about
 // NK / (2 kModeSegs) rows). Both the elimination y_k = (f_k + c_k y_prev)
 // inv_k and the back-substitution w_k = y_k - cp_k w_next are first-order
 // affine recurrences: each warp composes its segment's map (A, B), the maps
 // meet in shared memory, each warp takes its carry-in by chaining the maps
-// of the segments before it, and applies its rows. The twisted meeting is as
-// in k_spec_modes. The serial chain drops from NK/2 rows to about
+// of the segments before it, and applies its rows. The serial chain drops from NK/2 rows to about
 // 2 NK / (2 kModeSegs) + kModeSegs steps.
 constexpr int kModeSegs = 16;
 
