@@ -2,9 +2,11 @@
 // convolutional network on the cal_w residual, BF16 activations and weights
 // with FP32 accumulation.
 //
-// Activations are stored NHWC: pixel (y, x) of a level holds its C = 32
-// channels contiguously, 64 bytes, row-major in (y, x). Rows are periodic in
-// x (the cal_w operator is) and zero-padded in y (W = 0 outside the rows).
+// Activations are stored chunk-major, [H][4][W][8]: the 32 channels of a
+// pixel are 4 chunks of 8 (16 bytes), and chunk q of row y is a contiguous
+// run of W pixels (act_at). A row's chunk is then one 16 W-byte run, which
+// TMA reads in 128-byte lines. Rows are periodic in x (the cal_w operator
+// is) and zero-padded in y (W = 0 outside the rows).
 //
 // The 32 -> 32 convolutions run on the tensor cores (tcgen05): one CTA of 128
 // threads computes 128 consecutive pixels of one row as D[128 x 32] =
@@ -25,6 +27,11 @@
 namespace vvm {
 
 constexpr int kNetC = 32;        // channels
+
+// Element index of channel 8 q of pixel (y, x) in a level of width W.
+__device__ __forceinline__ size_t act_at(int y, int q, int x, int W) {
+    return (((size_t)y * 4 + q) * W + x) * 8;
+}
 constexpr int kConvTile = 128;   // pixels of a CTA (the MMA's M)
 constexpr int kConvSpan = kConvTile + 2;
 constexpr int kNetErrWait = 2;   // device error word: an MMA completion wait gave up
@@ -87,7 +94,7 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_tc(ConvArgs a) {
         if (xx < 0) xx += a.W;
         uint4 v = make_uint4(0, 0, 0, 0);
         if (yy >= 0 && yy < a.H)
-            v = *reinterpret_cast<const uint4*>(a.in + ((size_t)yy * a.W + xx) * kNetC + kc * 8);
+            v = *reinterpret_cast<const uint4*>(a.in + act_at(yy, kc, xx, a.W));
         sA[dy][kc][p] = v;
     }
     for (int j = tid; j < 9 * 4 * kNetC; j += kConvTile) (&sB[0][0][0])[j] = a.w[j];
@@ -153,7 +160,6 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_tc(ConvArgs a) {
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int x = x0 + tid;   // TMEM lane = pixel of the tile
         if (x < a.W) {
-            uint4* dst = reinterpret_cast<uint4*>(a.out + ((size_t)y * a.W + x) * kNetC);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 __nv_bfloat162 h0 = __floats2bfloat162_rn(__uint_as_float(r[8 * q + 0]), __uint_as_float(r[8 * q + 1]));
@@ -165,7 +171,7 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_tc(ConvArgs a) {
                 v.y = *reinterpret_cast<uint32_t*>(&h1);
                 v.z = *reinterpret_cast<uint32_t*>(&h2);
                 v.w = *reinterpret_cast<uint32_t*>(&h3);
-                dst[q] = v;
+                *reinterpret_cast<uint4*>(a.out + act_at(y, q, x, a.W)) = v;
             }
         }
     }
@@ -184,13 +190,15 @@ __global__ void __launch_bounds__(kConvTile) k_conv32_tc(ConvArgs a) {
 // k_conv32_tc).
 //
 // Loads are TMA (cp.async.bulk.tensor, no multicast) from a 3D tensor map of
-// the activations, dims {32 channels, W, H}: one box {8 channels, 144
-// pixels, 1 row} per 8-channel chunk lands as that chunk's canonical K-major
-// rows (pixel p at 16 p bytes) for pixels x0-8 .. x0+135, so tap dx of
-// output pixel x0+m reads box pixel 7+dx+m. The box is zero outside the
+// the chunk-major activations, dims {64 elements (8 pixels x 8 channels,
+// 128 bytes), W / 8 pixel blocks, 4 H chunk rows}: one box {64, 18, 1} per
+// 8-channel chunk (18 lines of 128 bytes) lands as that chunk's canonical
+// K-major rows (pixel p at 16 p bytes) for pixels x0-8 .. x0+135, so tap dx
+// of output pixel x0+m reads box pixel 7+dx+m. The box is zero outside the
 // tensor, which gives the zero rows y = -1 and y = H; the periodic pixels
 // x0-1 = W-1 (first strip) and x0+128 = W (last strip) come from a second
-// map with 8-pixel boxes and are copied into place in shared memory.
+// map with one-line boxes and are copied into place in shared memory.
+// Needs W a multiple of 8.
 //
 // Warp-specialised: lane 0 of warp 4 issues the loads and the MMAs; warps
 // 0-3 read the accumulators back (warp w owns TMEM lanes 32w..32w+31, the
@@ -305,9 +313,10 @@ __global__ void __launch_bounds__(kCThreads) k_conv32_stream(const __grid_consta
                 const uint32_t bytes = kCSlotBytes + (left ? 512u : 0u) + (right ? 512u : 0u);
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
                 for (int kc = 0; kc < 4; kc++) {
-                    tma_load_3d(smem_u32(sA + sl * kCSlotBytes + kc * kCRowBytes), &trow, kc * 8, x0 - 8, y, bar);
-                    if (left) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + kc * 128), &twrap, kc * 8, a.W - 8, y, bar);
-                    if (right) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + 512 + kc * 128), &twrap, kc * 8, 0, y, bar);
+                    // map coordinates: (element in an 8-pixel line, 8-pixel block, chunk row 4 y + kc)
+                    tma_load_3d(smem_u32(sA + sl * kCSlotBytes + kc * kCRowBytes), &trow, 0, (x0 - 8) / 8, 4 * y + kc, bar);
+                    if (left) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + kc * 128), &twrap, 0, a.W / 8 - 1, 4 * y + kc, bar);
+                    if (right) tma_load_3d(smem_u32(sW + sl * kCWrapBytes + 512 + kc * 128), &twrap, 0, 0, 4 * y + kc, bar);
                 }
                 issued = j + 1;
             };
@@ -420,7 +429,6 @@ __global__ void __launch_bounds__(kCThreads) k_conv32_stream(const __grid_consta
             if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(empty0 + 8 * b) : "memory");
             const int x = x0 + tid;
             if (x < a.W) {
-                uint4* dst = reinterpret_cast<uint4*>(a.out + ((size_t)(y0 + q) * a.W + x) * kNetC);
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
                     __nv_bfloat162 h0 = __floats2bfloat162_rn(__uint_as_float(v[8 * c + 0]), __uint_as_float(v[8 * c + 1]));
@@ -432,7 +440,7 @@ __global__ void __launch_bounds__(kCThreads) k_conv32_stream(const __grid_consta
                     o.y = *reinterpret_cast<uint32_t*>(&h1);
                     o.z = *reinterpret_cast<uint32_t*>(&h2);
                     o.w = *reinterpret_cast<uint32_t*>(&h3);
-                    dst[c] = o;
+                    *reinterpret_cast<uint4*>(a.out + act_at(y0 + q, c, x, a.W)) = o;
                 }
             }
         }
@@ -518,7 +526,7 @@ __global__ void k_net_lift(const float* x, const float* wl, __nv_bfloat16* h, in
         for (int t = 0; t < 9; t++) acc += sw[t * kNetC + 8 * q + e] * xv[t];
         o[e] = acc;
     }
-    bf16x8_store(h + (size_t)p * kNetC + 8 * q, o);
+    bf16x8_store(h + act_at(y, q, xx, W), o);
 }
 
 // z[p] = scale * sum_t sum_c wp[t][c] g[p + off(t)][c] for rows < hvalid, else 0
@@ -542,7 +550,7 @@ __global__ void k_net_proj(const __nv_bfloat16* g, const float* wp, float* z, in
             const int yy = y + t / 3 - 1, xs = wrapx(xx + t % 3 - 1, W);
             if (yy < 0 || yy >= H) continue;
             float v[8];
-            bf16x8_load(g + ((size_t)yy * W + xs) * kNetC + 8 * q, v);
+            bf16x8_load(g + act_at(yy, q, xs, W), v);
 #pragma unroll
             for (int e = 0; e < 8; e++) acc += sw[t * kNetC + 8 * q + e] * v[e];
         }
@@ -573,7 +581,7 @@ __global__ void k_net_proj_adj(const float* dz, const float* wp, __nv_bfloat16* 
             for (int t = 0; t < 9; t++) acc += __ldg(wp + t * kNetC + 8 * q + e) * dv[t];
             o[e] = acc;
         }
-        bf16x8_store(dg + (size_t)p * kNetC + 8 * q, o);
+        bf16x8_store(dg + act_at(y, q, xx, W), o);
     }
 }
 
@@ -590,13 +598,13 @@ __global__ void k_net_sum4(const __nv_bfloat16* in, __nv_bfloat16* out, int Ho, 
 #pragma unroll
         for (int b = 0; b < 2; b++) {
             float v[8];
-            bf16x8_load(in + ((size_t)(2 * y + a) * Wf + 2 * x + b) * kNetC + 8 * q, v);
+            bf16x8_load(in + act_at(2 * y + a, q, 2 * x + b, Wf), v);
 #pragma unroll
             for (int e = 0; e < 8; e++) s[e] += v[e];
         }
 #pragma unroll
     for (int e = 0; e < 8; e++) s[e] *= mult;
-    bf16x8_store(out + (size_t)p * kNetC + 8 * q, s);
+    bf16x8_store(out + act_at(y, q, x, Wo), s);
 }
 
 // out[y][x] = mult * lo[y/2][x/2] + skip[y][x] (out may be skip); H x W fine
@@ -608,11 +616,11 @@ __global__ void k_net_up_add(const __nv_bfloat16* lo, const __nv_bfloat16* skip,
     if (j >= H * W * 4) return;
     const int q = j & 3, p = j >> 2, y = p / W, x = p - y * W;
     float a[8], b[8];
-    bf16x8_load(lo + ((size_t)(y >> 1) * (W >> 1) + (x >> 1)) * kNetC + 8 * q, a);
-    bf16x8_load(skip + (size_t)p * kNetC + 8 * q, b);
+    bf16x8_load(lo + act_at(y >> 1, q, x >> 1, W >> 1), a);
+    bf16x8_load(skip + act_at(y, q, x, W), b);
 #pragma unroll
     for (int e = 0; e < 8; e++) a[e] = mult * a[e] + b[e];
-    bf16x8_store(out + (size_t)p * kNetC + 8 * q, a);
+    bf16x8_store(out + act_at(y, q, x, W), a);
 }
 
 // dW[t][ci][co] += sum_p X[p + off(t)][ci] dY[p][co] over one tile of 128
@@ -628,13 +636,13 @@ __global__ void __launch_bounds__(256) k_net_wgrad32(const __nv_bfloat16* X, con
         const int q = j & 3, p = (j >> 2) % kConvSpan, dy = (j >> 2) / kConvSpan;
         const int yy = y + dy - 1, xx = ((x0 + p - 1) % W + W) % W;
         uint4 v = make_uint4(0, 0, 0, 0);
-        if (yy >= 0 && yy < H) v = *reinterpret_cast<const uint4*>(X + ((size_t)yy * W + xx) * kNetC + 8 * q);
+        if (yy >= 0 && yy < H) v = *reinterpret_cast<const uint4*>(X + act_at(yy, q, xx, W));
         *reinterpret_cast<uint4*>(&sx[dy][p][8 * q]) = v;
     }
     for (int j = threadIdx.x; j < kConvTile * 4; j += blockDim.x) {
         const int q = j & 3, m = j >> 2;
         uint4 v = make_uint4(0, 0, 0, 0);
-        if (m < n) v = *reinterpret_cast<const uint4*>(dY + ((size_t)y * W + x0 + m) * kNetC + 8 * q);
+        if (m < n) v = *reinterpret_cast<const uint4*>(dY + act_at(y, q, x0 + m, W));
         *reinterpret_cast<uint4*>(&sy[m][8 * q]) = v;
     }
     __syncthreads();
@@ -662,8 +670,8 @@ __global__ void k_net_wgrad_edge(const float* s, const __nv_bfloat16* d, float* 
     float acc = 0.f;
     for (int x = 0; x < W; x++) {
         const int xs = wrapx(x + dx, W);
-        if (mode == 0) acc += s[(size_t)yy * W + xs] * __bfloat162float(d[((size_t)y * W + x) * kNetC + c]);
-        else acc += s[(size_t)y * W + x] * __bfloat162float(d[((size_t)yy * W + xs) * kNetC + c]);
+        if (mode == 0) acc += s[(size_t)yy * W + xs] * __bfloat162float(d[act_at(y, c >> 3, x, W) + (c & 7)]);
+        else acc += s[(size_t)y * W + x] * __bfloat162float(d[act_at(yy, c >> 3, xs, W) + (c & 7)]);
     }
     atomicAdd(dw + j, acc);
 }
@@ -753,14 +761,24 @@ __global__ void k_net_adam(float* w, const float* g, float* m, float* v, int n, 
     w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
 }
 
-__global__ void k_f32_to_bf16(const float* x, __nv_bfloat16* y, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        y[i] = __float2bfloat16_rn(x[i]);
+// [H][W][32] FP32 (host order) <-> chunk-major BF16 activations.
+__global__ void k_nhwc_to_act(const float* x, __nv_bfloat16* y, int H, int W) {
+    const size_t n = (size_t)H * W * kNetC;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % kNetC);
+        const size_t p = i / kNetC;
+        const int yy = (int)(p / W), xx = (int)(p - (size_t)yy * W);
+        y[act_at(yy, c >> 3, xx, W) + (c & 7)] = __float2bfloat16(x[i]);
+    }
 }
-
-__global__ void k_bf16_to_f32(const __nv_bfloat16* x, float* y, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        y[i] = __bfloat162float(x[i]);
+__global__ void k_act_to_nhwc(const __nv_bfloat16* x, float* y, int H, int W) {
+    const size_t n = (size_t)H * W * kNetC;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % kNetC);
+        const size_t p = i / kNetC;
+        const int yy = (int)(p / W), xx = (int)(p - (size_t)yy * W);
+        y[i] = __bfloat162float(x[act_at(yy, c >> 3, xx, W) + (c & 7)]);
+    }
 }
 
 }  // namespace vvm

@@ -915,11 +915,11 @@ __global__ void k_net_galerkin(int NX, int NK, int pitch, const CGScalars* sc, c
 // H0 = round_up(NK, 8) rows (W0 = NX, a multiple of 8). FP32 master weights
 // with Adam; BF16 operands and activations, FP32 accumulation.
 // The 3x3 32 -> 32 convolution of the learned preconditioner: rows of at
-// least kCBox pixels go to the streamed TMA kernel, narrower ones to the
-// one-row-tile kernel. Tensor maps (3D {32, W, H} over BF16 activations,
-// boxes {8, 144, 1} and {8, 8, 1}) are encoded through the driver's
-// cuTensorMapEncodeTiled and cached per (tensor, H, W, box width): the map is
-// a function of those alone.
+// least kCBox pixels (W a multiple of 8) go to the streamed TMA kernel, the
+// rest to the one-row-tile kernel. Tensor maps (3D {64, W / 8, 4 H} over the
+// chunk-major BF16 activations, boxes {64, 18, 1} and {64, 1, 1}) are encoded
+// through the driver's cuTensorMapEncodeTiled and cached per (tensor, H, W,
+// box width): the map is a function of those alone.
 CUtensorMap conv_map(const void* p, int H, int W, int boxw) {
     static std::mutex mu;
     static std::map<std::tuple<const void*, int, int, int>, CUtensorMap> cache;
@@ -935,10 +935,12 @@ CUtensorMap conv_map(const void* p, int H, int W, int boxw) {
         if (!fn || q != cudaDriverEntryPointSuccess) throw CudaError{"cuTensorMapEncodeTiled: not found in the driver"};
         enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
+    // chunk-major activations as {64 elements (8 pixels x 8 channels), W / 8
+    // pixel blocks, 4 H chunk rows}; boxw counts pixels (a multiple of 8)
     CUtensorMap m;
-    cuuint64_t dims[3] = {(cuuint64_t)kNetC, (cuuint64_t)W, (cuuint64_t)H};
-    cuuint64_t strides[2] = {(cuuint64_t)kNetC * 2, (cuuint64_t)W * kNetC * 2};
-    cuuint32_t box[3] = {8, (cuuint32_t)boxw, 1}, es[3] = {1, 1, 1};
+    cuuint64_t dims[3] = {64, (cuuint64_t)(W / 8), (cuuint64_t)(4 * H)};
+    cuuint64_t strides[2] = {128, (cuuint64_t)W * 16};
+    cuuint32_t box[3] = {64, (cuuint32_t)(boxw / 8), 1}, es[3] = {1, 1, 1};
     CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(p), dims, strides, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -966,7 +968,7 @@ int conv_rows_per_cta(int H, int W) {
 
 void conv32(const __nv_bfloat16* in, __nv_bfloat16* out, const uint4* w, int H, int W, int* err, cudaStream_t st,
             Stats* stats) {
-    if (W >= kCBox) {
+    if (W >= kCBox && W % 8 == 0) {
         const int R = conv_rows_per_cta(H, W);
         const CUtensorMap trow = conv_map(in, H, W, kCBox), twrap = conv_map(in, H, W, 8);
         ConvStreamArgs a{in, out, w, H, W, R, err};
@@ -3207,12 +3209,12 @@ int vvm_gpu_conv3x3_c32(const float* x, const float* w, float* y, int H, int W, 
         uint4* pw = ar.alloc<uint4>(9 * 4 * kNetC);
         CK(cudaMemcpy(fx, x, n * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(fw, w, 9 * kNetC * kNetC * sizeof(float), cudaMemcpyHostToDevice));
-        k_f32_to_bf16<<<256, 256>>>(fx, bx, n);
+        k_nhwc_to_act<<<256, 256>>>(fx, bx, H, W);
         CKL();
         k_pack_conv32<<<cdiv(9 * 4 * kNetC, 128), 128>>>(fw, pw, adjoint ? 1 : 0);
         CKL();
         conv32(bx, by, pw, H, W, err, nullptr, nullptr);
-        k_bf16_to_f32<<<256, 256>>>(by, fx, n);
+        k_act_to_nhwc<<<256, 256>>>(by, fx, H, W);
         CKL();
         CK(cudaMemcpy(y, fx, n * sizeof(float), cudaMemcpyDeviceToHost));
         int h = 0;
