@@ -502,15 +502,16 @@ __device__ __forceinline__ int wrapx(int x, int W) { return x < 0 ? x + W : (x >
 
 // h[p][c] = sum_t wl[t][c] x[p + off(t)]  (1 -> 32 channels; x FP32 [H][W]).
 // The 288 weights are staged in shared memory (read as broadcasts).
-// A thread computes one pixel's chunk of 8 channels, so a warp stores 512
-// contiguous bytes.
+// A thread computes one pixel's chunk of 8 channels; consecutive threads
+// take consecutive pixels of one chunk plane, so a warp stores 512 contiguous
+// bytes and reads the same weights.
 __global__ void k_net_lift(const float* x, const float* wl, __nv_bfloat16* h, int H, int W) {
     __shared__ float sw[9 * kNetC];
     for (int j = threadIdx.x; j < 9 * kNetC; j += blockDim.x) sw[j] = wl[j];
     __syncthreads();
-    const long j = blockIdx.x * (long)blockDim.x + threadIdx.x;   // (pixel, chunk)
+    const long j = blockIdx.x * (long)blockDim.x + threadIdx.x;   // (chunk, pixel): pixels fastest
     if (j >= 4L * H * W) return;
-    const int q = (int)(j & 3), p = (int)(j >> 2);
+    const int q = (int)(j / ((long)H * W)), p = (int)(j - (long)q * H * W);
     const int y = p / W, xx = p - y * W;
     float xv[9];
 #pragma unroll
@@ -590,7 +591,7 @@ __global__ void k_net_proj_adj(const float* dz, const float* wp, __nv_bfloat16* 
 __global__ void k_net_sum4(const __nv_bfloat16* in, __nv_bfloat16* out, int Ho, int Wo, float mult) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;   // (coarse pixel, chunk)
     if (j >= Ho * Wo * 4) return;
-    const int q = j & 3, p = j >> 2, y = p / Wo, x = p - y * Wo;
+    const int q = j / (Ho * Wo), p = j - q * (Ho * Wo), y = p / Wo, x = p - y * Wo;   // pixels fastest
     const int Wf = 2 * Wo;
     float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -614,7 +615,7 @@ __global__ void k_net_up_add(const __nv_bfloat16* lo, const __nv_bfloat16* skip,
                              float mult) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= H * W * 4) return;
-    const int q = j & 3, p = j >> 2, y = p / W, x = p - y * W;
+    const int q = j / (H * W), p = j - q * (H * W), y = p / W, x = p - y * W;   // pixels fastest
     float a[8], b[8];
     bf16x8_load(lo + act_at(y >> 1, q, x >> 1, W >> 1), a);
     bf16x8_load(skip + act_at(y, q, x, W), b);
