@@ -833,6 +833,7 @@ __global__ void k_net_out(const float* z, int NX, int NK, int pitch, double* a, 
 // Truncated flexible CG of the learned preconditioner (fcg_learned): up to
 // kFcgM-1 earlier directions (or their S images), in ring slots `slot`.
 constexpr int kFcgM = 8;
+constexpr int kFcgCheck = 4;   // iterations between the host's convergence checks
 struct FcgSet {
     const double* a[kFcgM];
     int slot[kFcgM];
@@ -1848,8 +1849,11 @@ void learned_precond(vvm_gpu_ctx* c, const double* r, cudaStream_t st) {
 // nonlinear), keeping only the previous direction loses the Krylov speed-up;
 // a few more restore it. Directions and their S images live in a ring of
 // kFcgM slots. On S W = Wf from W = 0, preconditioned by learned_precond, to
-// the FP64 residual ||rhow r||^2 <= tol^2 bb. Returns the iterations, or -cap
-// if not converged.
+// the FP64 residual ||rhow r||^2 <= tol^2 bb. The host reads the residual
+// every kFcgCheck iterations only, so it stays ahead of the device instead of
+// waiting on it each iteration; the up to kFcgCheck - 1 iterations past
+// convergence leave a smaller residual (the step lengths are guarded against
+// zero). Returns the iterations run, or -cap if not converged.
 int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) {
     PCG<double>& P = *c->pcg64;
     VecArgs<double> v = P.vargs();
@@ -1893,6 +1897,7 @@ int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) 
         CKL();
         LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RR));
         CKL();
+        if (it % kFcgCheck != 0 && it != cap) continue;
         rr = P.read_rr(st);
         *relres = std::sqrt(rr / bb);
         if (!(rr > stop2)) return it;
