@@ -11,6 +11,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <random>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -1407,6 +1408,7 @@ struct vvm_gpu_ctx {
     // dx / (2 (z_k - z_zeta_k)); exactly 1 on uniform levels. `stretched`:
     // non-uniform levels, which only the Poisson entries support.
     std::vector<double> h_a, h_h;
+    std::vector<double> h_forcing;   // [nx][nz] host copy of the last regenerated th forcing
     bool stretched = false;
     double* rwres = nullptr;   // [nz] residual weight rw_k = rhow_k / a_k
     double* ubar = nullptr;   // [0] ubarTop, [1] ubarTopp
@@ -2218,6 +2220,8 @@ cudaGraphExec_t step_graph(vvm_gpu_ctx* c) {
     return ex;
 }
 
+int regen_forcing(vvm_gpu_ctx* c, int t, double lo, double hi, double sd);
+
 template <typename T>
 int step_once(vvm_gpu_ctx* c) {
     const bool forcing_now = c->has_forcing_th && ((c->step + 1) * c->desc.dt <= c->desc.addforcingtime);
@@ -2226,6 +2230,10 @@ int step_once(vvm_gpu_ctx* c) {
                            c->poisson_ready && (!warm || c->nsolves >= 2);
     if (!use_graph) {
         c->last_graph = false;
+        // TimeMarching makes the step's forcing field before AddForcing
+        // (src/Iteration.cpp:276-283); nothing before AddForcing reads it
+        if (forcing_now && !(c->desc.flags & VVM_FLAG_FIXED_FORCING))
+            if (int rc = regen_forcing(c, c->step + 1, -0.001, 0.001, 1.)) return rc;
         return run_step<T>(c);
     }
     cudaGraphExec_t ex = step_graph<T>(c);
@@ -2570,6 +2578,59 @@ void upload_field(vvm_gpu_ctx* c, const double* host, int sk, int off, T* dst, c
     CKL();
 }
 
+// Init::RandomPerturbation (src/Init.cpp:488-515) on the host, with the
+// reference's own generator so the numbers are the same: std::mt19937 seeded
+// with t, std::normal_distribution<> of mean 0 and deviation 1 scaled by sd
+// and drawn again until inside [lo, hi], for the interior cells with
+// z = (k - 0.5) dz < 200 m (k outer, i inner; the others 0), then the ghost
+// images of BoundaryProcess2D_center (src/Boundary.cpp:9-19). out is
+// [nx][nz]. A cell that takes more than kMaxDraws draws fails (EINVAL).
+constexpr long long kMaxDraws = 1ll << 32;
+int random_perturbation(int NX, int NZ, double dz, int t, double lo, double hi, double sd, double* out) {
+    if (NX < 1 || NZ < 1 || !out || !(dz > 0) || !(lo <= hi) || !(sd > 0)) return VVM_GPU_EINVAL;
+    const int nx = NX + 2, nz = NZ + 2;
+    std::mt19937 gen(t);
+    std::normal_distribution<> dist(0.0, 1.0);
+    for (int k = 1; k < nz - 1; k++) {
+        const double z = (k - 0.5) * dz;
+        for (int i = 1; i < nx - 1; i++) {
+            double v = 0.;
+            if (z < 200) {
+                long long n = 0;
+                do {
+                    v = 0. + sd * dist(gen);
+                    if (++n > kMaxDraws) return VVM_GPU_EINVAL;
+                } while (v < lo || v > hi);
+            }
+            out[(size_t)i * nz + k] = v;
+        }
+    }
+    for (int k = 1; k <= nz - 2; k++) {
+        out[k] = out[(size_t)(nx - 2) * nz + k];
+        out[(size_t)(nx - 1) * nz + k] = out[(size_t)nz + k];
+    }
+    for (int i = 0; i < nx; i++) {
+        out[(size_t)i * nz] = out[(size_t)i * nz + 1];
+        out[(size_t)i * nz + nz - 1] = out[(size_t)i * nz + nz - 2];
+    }
+    return VVM_GPU_OK;
+}
+
+template <typename T>
+void upload_forcing(vvm_gpu_ctx* c) {
+    upload_field<T>(c, c->h_forcing.data(), 1, 0, fields<T>(c).th_forcing);
+}
+
+// The field of step t into the device's init_th_forcing (stream-ordered).
+int regen_forcing(vvm_gpu_ctx* c, int t, double lo, double hi, double sd) {
+    c->h_forcing.assign((size_t)c->d.nx * c->d.nz, 0.);
+    if (int rc = random_perturbation(c->d.nx - 2, c->d.nz - 2, c->desc.dz, t, lo, hi, sd, c->h_forcing.data()))
+        return fail(c, rc, "random_perturbation: needs min_range <= max_range and standard_deviation > 0");
+    (c->mixed ? upload_forcing<float> : upload_forcing<double>)(c);
+    c->has_forcing_th = true;
+    return VVM_GPU_OK;
+}
+
 template <typename T>
 void download_field(vvm_gpu_ctx* c, const T* src, int sk, int off, double* host, bool first_of_pair,
                     const double* ref = nullptr) {
@@ -2628,7 +2689,8 @@ int upload_state_t(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
                          s->dqc_advect, s->dqr_advect, s->dqr_VT};
     for (int h = 0; h < NHIST; h++)
         for (int sl = 0; sl < 2; sl++) up_or_zero(hs[h], 2, sl, F.hist[h][sl]);
-    c->has_forcing_th = (s->init_th_forcing != nullptr);
+    // regenerated each forced step unless the uploaded field is to be kept
+    c->has_forcing_th = (s->init_th_forcing != nullptr) || !(c->desc.flags & VVM_FLAG_FIXED_FORCING);
     up_or_zero(s->init_th_forcing, 1, 0, F.th_forcing);
     if (s->precip) {
         std::vector<T> pr(c->d.nx);
@@ -3087,6 +3149,19 @@ ROUTINE(vvm_gpu_pqr, {
     return VVM_GPU_OK;
 })
 ROUTINE(vvm_gpu_add_forcing, { DISPATCH(ctx, launch_apply)(ctx, F_TH | F_QV, 0, true, false); return VVM_GPU_OK; })
+
+int vvm_gpu_random_perturbation(vvm_gpu_ctx* ctx, int t, double min_range, double max_range,
+                                double standard_deviation) {
+    return guarded(ctx, [&]() -> int {
+        if (int rc = need_state(ctx)) return rc;
+        return regen_forcing(ctx, t, min_range, max_range, standard_deviation);
+    });
+}
+
+int vvm_gpu_random_perturbation_host(int NX, int NZ, double dz, int t, double min_range, double max_range,
+                                     double standard_deviation, double* out) {
+    return random_perturbation(NX, NZ, dz, t, min_range, max_range, standard_deviation, out);
+}
 ROUTINE(vvm_gpu_halo_all, { DISPATCH(ctx, launch_halo_all)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_pubartop, { DISPATCH(ctx, launch_pubartop)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_cal_w, { ctx->last_graph = false; return DISPATCH(ctx, launch_cal_w)(ctx, nullptr); })

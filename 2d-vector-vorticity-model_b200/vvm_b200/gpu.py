@@ -24,6 +24,7 @@ LIB_PATH = PKG / "lib" / "libvvmgpu.so"
 
 VVM_PREC_FP64, VVM_PREC_MIXED = 0, 1
 VVM_SOLVER_MGPCG, VVM_SOLVER_LEARNED, VVM_SOLVER_SPECTRAL = 0, 1, 2
+VVM_FLAG_FIXED_FORCING = 1
 STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOCONV", 4: "ESTATE"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -79,7 +80,8 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream",
            "vvm_gpu_conv3x3_c32", "vvm_gpu_learned_shape", "vvm_gpu_learned_weights",
            "vvm_gpu_learned_eval", "vvm_gpu_learned_train", "vvm_gpu_learned_config",
-           "vvm_gpu_learned_last", "vvm_gpu_learned_time", "vvm_gpu_learned_train_rhs") + tuple(
+           "vvm_gpu_learned_last", "vvm_gpu_learned_time", "vvm_gpu_learned_train_rhs",
+           "vvm_gpu_random_perturbation", "vvm_gpu_random_perturbation_host") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -135,6 +137,9 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_learned_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     L.vvm_gpu_learned_train_rhs.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ip, ip, ip, ctypes.c_double, ip,
                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    dbl = ctypes.c_double
+    L.vvm_gpu_random_perturbation.argtypes = [vp, ip, dbl, dbl, dbl]
+    L.vvm_gpu_random_perturbation_host.argtypes = [ip, ip, dbl, ip, dbl, dbl, dbl, _dp]
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -170,17 +175,31 @@ def poisson_solve_noalloc(NX: int, NZ: int, rhou: np.ndarray, rhow: np.ndarray, 
     return it.value, rel.value
 
 
+def random_perturbation_host(grid, t: int, min_range: float = -0.001, max_range: float = 0.001,
+                             standard_deviation: float = 1.0) -> np.ndarray:
+    """Init::RandomPerturbation's field of step t for `grid` ([nx][nz], ghost
+    cells filled), made on the host by the library (no GPU needed)."""
+    L = load_library()
+    out = np.zeros((grid.NX + 2, grid.NZ + 2))
+    rc = L.vvm_gpu_random_perturbation_host(int(grid.NX), int(grid.NZ), float(grid.dz), int(t),
+                                            float(min_range), float(max_range), float(standard_deviation),
+                                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    if rc != 0:
+        raise VVMGpuError(rc, "random_perturbation_host: needs min_range <= max_range and standard_deviation > 0")
+    return out
+
+
 class VVMGpu:
     """One GPU context of the VVM step (a `vvm` model living in HBM)."""
 
     def __init__(self, grid, precision: int = VVM_PREC_FP64, solver: int = VVM_SOLVER_MGPCG,
                  poisson_tol: float = 1e-10, warm_start: bool = True, device: int = 0,
-                 addforcingtime: float = 0.0, poisson_maxit: int = 200):
+                 addforcingtime: float = 0.0, poisson_maxit: int = 200, fixed_forcing: bool = False):
         self.L = load_library()
         self.grid = grid
         self.owned = True
         d = self.make_desc(self.L, grid, precision, solver, poisson_tol, warm_start, addforcingtime,
-                           poisson_maxit)
+                           poisson_maxit, fixed_forcing)
         self.desc = d
         h = ctypes.c_void_p()
         rc = self.L.vvm_gpu_create(ctypes.byref(d), int(device), ctypes.byref(h))
@@ -191,8 +210,10 @@ class VVMGpu:
 
     @staticmethod
     def make_desc(L, grid, precision=VVM_PREC_FP64, solver=VVM_SOLVER_MGPCG, poisson_tol=1e-10,
-                  warm_start=True, addforcingtime=0.0, poisson_maxit=200):
-        """vvm_gpu_desc of a grid (reference defaults, then the options)."""
+                  warm_start=True, addforcingtime=0.0, poisson_maxit=200, fixed_forcing=False):
+        """vvm_gpu_desc of a grid (reference defaults, then the options).
+        fixed_forcing keeps the uploaded init_th_forcing at every forced step
+        instead of regenerating it each step as TimeMarching does."""
         d = Desc()
         L.vvm_gpu_desc_default(ctypes.byref(d), grid.NX, grid.NZ, float(grid.dx),
                                     float(grid.dz), float(grid.dt))
@@ -204,6 +225,7 @@ class VVMGpu:
         d.poisson_tol = float(poisson_tol)
         d.poisson_maxit = int(poisson_maxit)
         d.warm_start = 1 if warm_start else 0
+        d.flags = VVM_FLAG_FIXED_FORCING if fixed_forcing else 0
         return d
 
     @classmethod
@@ -337,13 +359,25 @@ class VVMGpu:
 
     def time_marching_routines(self, nsteps: int = 1):
         """The reference's TimeMarching body, one C-ABI call per routine
-        (src/Iteration.cpp:246-434)."""
+        (src/Iteration.cpp:246-434), the forcing field of the step made before
+        AddForcing while step*dt <= addforcingtime (:276-283)."""
         for _ in range(nsteps):
-            self.step_count = self.step_count + 1
-            for r in ("pzeta", "pth", "pqv", "pqc", "pqr", "add_forcing", "halo_all",
-                      "pubartop", "cal_w", "cal_u", "halo_all", "kessler", "halo_all",
-                      "update_mean", "turbulence", "nudge", "next_step"):
+            step = self.step_count + 1
+            self.step_count = step
+            for r in ("pzeta", "pth", "pqv", "pqc", "pqr"):
                 self.call(r)
+            if step * self.desc.dt <= self.desc.addforcingtime and not (self.desc.flags & VVM_FLAG_FIXED_FORCING):
+                self.random_perturbation(step)
+            for r in ("add_forcing", "halo_all", "pubartop", "cal_w", "cal_u", "halo_all", "kessler",
+                      "halo_all", "update_mean", "turbulence", "nudge", "next_step"):
+                self.call(r)
+
+    def random_perturbation(self, t: int, min_range: float = -0.001, max_range: float = 0.001,
+                            standard_deviation: float = 1.0):
+        """Init::RandomPerturbation (src/Init.cpp:488-515) into the device's
+        init_th_forcing, with the reference's own generator."""
+        self._check(self.L.vvm_gpu_random_perturbation(self.h, int(t), float(min_range), float(max_range),
+                                                        float(standard_deviation)))
 
     def set_stream(self, stream_handle: int | None):
         self._check(self.L.vvm_gpu_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)))

@@ -73,8 +73,13 @@ typedef struct vvm_gpu_desc {
     int solver;                  /* VVM_SOLVER_* */
     int warm_start;              /* 1: start cal_w from the previous W (the
                                     reference starts from zero) */
-    int flags;                   /* reserved, 0 */
+    int flags;                   /* VVM_FLAG_* below, 0 = the reference's behaviour */
 } vvm_gpu_desc;
+
+/* desc.flags: keep the uploaded init_th_forcing at every forced step instead
+ * of regenerating it each step the way TimeMarching does
+ * (src/Iteration.cpp:276-283; see vvm_gpu_random_perturbation). */
+#define VVM_FLAG_FIXED_FORCING 1
 
 /* Fills a descriptor with the reference's constants for an NX x NZ grid. */
 void vvm_gpu_desc_default(vvm_gpu_desc* d, int NX, int NZ, double dx, double dz, double dt);
@@ -133,6 +138,25 @@ int vvm_gpu_pqv(vvm_gpu_ctx* ctx);          /* Iteration::pqv_pt, Iteration.cpp:
 int vvm_gpu_pqc(vvm_gpu_ctx* ctx);          /* Iteration::pqc_pt, Iteration.cpp:100-107 */
 int vvm_gpu_pqr(vvm_gpu_ctx* ctx);          /* Iteration::pqr_pt, Iteration.cpp:109-124 */
 int vvm_gpu_add_forcing(vvm_gpu_ctx* ctx);  /* vvm::AddForcing, AddForcing.cpp:6-28 */
+/* Init::RandomPerturbation(model, t, min_range, max_range, standard_deviation)
+ * (src/Init.cpp:488-515): the random theta forcing field of step t, made on
+ * the host with the reference's own generator (std::mt19937 seeded with t,
+ * std::normal_distribution<> redrawn until inside [min_range, max_range], in
+ * the cells with z = (k - 0.5) dz < 200 m, k outer and i inner), so the same
+ * numbers as the reference, and written to the device's init_th_forcing.
+ * TimeMarching calls it before AddForcing while step*dt <= addforcingtime
+ * with (step, -0.001, 0.001, 1.); vvm_gpu_step does the same unless
+ * VVM_FLAG_FIXED_FORCING is set. EINVAL when min_range > max_range or
+ * standard_deviation <= 0 (the reference's redraw loop would not end). */
+int vvm_gpu_random_perturbation(vvm_gpu_ctx* ctx, int t, double min_range, double max_range,
+                                double standard_deviation);
+/* The same field for an NX x NZ grid of level spacing dz, on the host only
+ * (no context, no device): out is [NX+2][NZ+2] in the reference layout, its
+ * ghost cells filled as BoundaryProcess2D_center fills them
+ * (src/Boundary.cpp:9-19). Init2d adds the t = 0 field to th when
+ * addforcingtime > 0 (src/Init.cpp:193-196). */
+int vvm_gpu_random_perturbation_host(int NX, int NZ, double dz, int t, double min_range,
+                                     double max_range, double standard_deviation, double* out);
 int vvm_gpu_halo_all(vvm_gpu_ctx* ctx);     /* BoundaryProcess2D_all, Boundary.cpp:32-52 */
 int vvm_gpu_pubartop(vvm_gpu_ctx* ctx);     /* PoissonSolver::pubarTop_pt, PoissonSolver.cpp:655-676 */
 int vvm_gpu_cal_w(vvm_gpu_ctx* ctx);        /* PoissonSolver::cal_w, PoissonSolver.cpp:439-479 */

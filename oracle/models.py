@@ -210,6 +210,15 @@ class RefModel(_CModel):
             self.L.ref_init_poisson(self.h)
             self._poisson_ready = True
 
+    def random_perturbation(self, t: int, min_range: float = -0.001, max_range: float = 0.001,
+                            standard_deviation: float = 1.0) -> np.ndarray:
+        """vvm::Init::RandomPerturbation (src/Init.cpp:488-515): the reference's
+        own field of step t, returned as a copy of init_th_forcing [nx][nz]."""
+        self.L.ref_random_perturbation.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_double] * 3
+        self.L.ref_random_perturbation(self.h, int(t), float(min_range), float(max_range),
+                                       float(standard_deviation))
+        return np.array(self.field("init_th_forcing"))
+
     def time_marching(self, nsteps: int):
         """vvm::Iteration::TimeMarching from step 0 (src/Iteration.cpp:208-438)."""
         self.L.ref_time_marching.argtypes = [ctypes.c_void_p, ctypes.c_int]

@@ -221,6 +221,12 @@ int ref_call(void* h, const char* name) {
     return 0;
 }
 
+// vvm::Init::RandomPerturbation(model, t, min_range, max_range,
+// standard_deviation) (src/Init.cpp:488-515) into model.init_th_forcing.
+void ref_random_perturbation(void* h, int t, double min_range, double max_range, double standard_deviation) {
+    vvm::Init::RandomPerturbation(*static_cast<vvm*>(h), t, min_range, max_range, standard_deviation);
+}
+
 // Runs vvm::Iteration::TimeMarching for nsteps from step 0
 // (src/Iteration.cpp:208-438); TIMEEND = nsteps * dt.
 void ref_time_marching(void* h, int nsteps) {

@@ -228,7 +228,8 @@ def test_other_grids_match_oracle(gpu, NX, NZ):
 
 def test_case2_moisture_nudging_and_forcing(gpu):
     """CASE 2 (no zeta nudging), Nudge_qv on, large-scale Q1/Q2 forcing and
-    the random th forcing field while step*dt <= addforcingtime."""
+    an uploaded th forcing field kept while step*dt <= addforcingtime
+    (VVM_FLAG_FIXED_FORCING: the C restatement keeps its field too)."""
     from oracle.models import PortModel
     from vvm_b200.initial_state import warm_bubble
     st = warm_bubble(48, 66, case=2)
@@ -248,12 +249,66 @@ def test_case2_moisture_nudging_and_forcing(gpu):
     for _ in range(4):
         m.one_step()
     ref = m.dump()
-    g = gpu.VVMGpu(st.grid, addforcingtime=2.0)
+    g = gpu.VVMGpu(st.grid, addforcingtime=2.0, fixed_forcing=True)
     g.upload(st)
     g.step(4)
     out = g.download()
     for f in PROG:
         assert rel_l2(out.fields[f], ref.fields[f]) <= 1e-8, (f, rel_l2(out.fields[f], ref.fields[f]))
+
+
+FORCING_BARS = {0: {f: 1e-8 for f in PROG},
+                1: {"zeta": 1e-4, "th": 1e-7, "qv": 1e-6, "u": 1e-4, "w": 1e-4}}
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_forcing_regenerated_each_step_as_time_marching_does(gpu, precision):
+    """While step*dt <= addforcingtime, the step makes the random th forcing of
+    that step (Init::RandomPerturbation seeded with the step number,
+    src/Iteration.cpp:276-283) before AddForcing. The C restatement, fed the
+    same field before each of its steps, agrees; the generator itself equals
+    the reference's bit for bit (tests/test_forcing_rng.py). Levels at 50 and
+    150 m are forced for three steps, then two steps run without forcing."""
+    from oracle.models import PortModel
+    from vvm_b200.initial_state import warm_bubble
+    st = warm_bubble(48, 24, 100.0, 100.0)
+    m = PortModel(st.grid, addforcingtime=3.0)
+    m.load(st)
+    for _ in range(5):
+        m.field("init_th_forcing")[:] = gpu.random_perturbation_host(st.grid, m.step + 1)
+        m.one_step()
+    ref = m.dump()
+    g = gpu.VVMGpu(st.grid, precision=precision, addforcingtime=3.0)
+    g.upload(st)
+    g.step(5)
+    out = g.download()
+    for f, bar in FORCING_BARS[precision].items():
+        assert rel_l2(out.fields[f], ref.fields[f]) <= bar, (f, rel_l2(out.fields[f], ref.fields[f]))
+    # the forcing acted: a run without it is much farther from the reference
+    n = gpu.VVMGpu(st.grid, precision=precision)
+    n.upload(st)
+    n.step(5)
+    d_err = np.linalg.norm(out.fields["th"] - ref.fields["th"])
+    d_force = np.linalg.norm(n.download().fields["th"] - ref.fields["th"])
+    assert d_force > 10 * d_err, (d_force, d_err)
+    for h in (g, n):
+        h.close()
+
+
+def test_routine_sequence_makes_the_same_forcing(gpu):
+    """The per-routine C-ABI sequence with vvm_gpu_random_perturbation before
+    AddForcing equals the fused step bit for bit while forcing is on."""
+    from vvm_b200.initial_state import warm_bubble
+    st = warm_bubble(64, 32, 100.0, 100.0)
+    a = gpu.VVMGpu(st.grid, addforcingtime=2.0)
+    a.upload(st)
+    a.step(3)
+    b = gpu.VVMGpu(st.grid, addforcingtime=2.0)
+    b.upload(st)
+    b.time_marching_routines(3)
+    da, db = a.download(), b.download()
+    for f in PROG:
+        assert np.array_equal(da.fields[f], db.fields[f]), f
 
 
 def test_step_zero_ab2_branch(gpu):
