@@ -415,3 +415,82 @@ def squall_line(NX: int = 1024, NZ: int = 128, dx: float = 250.0, dz: float = 25
     u = np.zeros((nx, nz))
     u[1:nx - 1, 1:nz - 1] = (u_top * np.minimum(z / shear_depth, 1.0))[:, 1:nz - 1] * np.ones((nx - 2, 1))
     return _assemble(g, prof, th, u)
+
+
+def read_sounding(path) -> np.ndarray:
+    """The rows of a sounding file as the reference reads it (Init::LoadFile,
+    src/Init.cpp:301-312): a header line and the zero level are skipped, then
+    whitespace-separated rows of ZZ, ZT, RHO, THBAR, PBAR, PIBAR, QVBAR, Q1LS,
+    Q2LS, RHOZ, read while a whole row parses. Returns [rows][10]."""
+    with open(path) as fh:
+        lines = fh.read().split("\n")
+    words = " ".join(lines[2:]).split()
+    vals = []
+    for w in words:
+        try:
+            vals.append(float(w))
+        except ValueError:
+            break
+    n = len(vals) // 10
+    return np.array(vals[:10 * n], dtype=np.float64).reshape(n, 10)
+
+
+def sounding_state(path, NX: int, NZ: int, dx: float, dz: float, dt: float, case: int = 1) -> VVMState:
+    """The initial state of the reference's shipped configuration, which reads
+    its base state from a sounding file (LOADFILE) and adds the large-scale
+    Q1/Q2 forcing and the t = 0 random theta perturbation (TROPICALFORCING):
+
+    * Init::LoadFile (src/Init.cpp:301-370): row r of the file is level
+      k = r + 1 (thb, thb_init, qvb, pib, pb; rhou from RHOZ, rhow from RHO;
+      Q1LS and Q2LS times 6), ghost levels copied, rhow at the top from rhou
+      below it, then the Exner function from the pressure, pib = (pb/1e5)^(Rd/Cp);
+    * the rest of Init1d (src/Init.cpp:116-134): thvb = thb + 0.61 qvb (the
+      additive form of step 1), qvb0 = qvb, the level heights and lambda2;
+    * Init2d (src/Init.cpp:138-182, 231-255): qv = qvb everywhere, qc = qr = 0,
+      th = thb + the RandomPerturbation field of step 0 with the declaration's
+      default range, +-0.25 K (src/Declare.hpp:870; the reference's own
+      generator, made by the GPU library's host entry), u = w = zeta = 0.
+
+    The file must hold at most NZ rows (the reference writes past its arrays
+    otherwise); levels without a row keep zero, as the reference's arrays do."""
+    from .gpu import random_perturbation_host
+    g = GridSpec(NX, NZ, dx, dz, dt, case=case)
+    nx, nz = g.nx, g.nz
+    rows = read_sounding(path)
+    if len(rows) > nz - 2:
+        raise ValueError(f"sounding: {len(rows)} rows for {nz - 2} levels")
+    thb, thb_init, qvb, pib, pb, rhou, rhow, q1, q2 = (np.zeros(nz) for _ in range(9))
+    for r, (ZZ, ZT, RHO, THBAR, PBAR, PIBAR, QVBAR, Q1LS, Q2LS, RHOZ) in enumerate(rows):
+        k = r + 1
+        thb[k] = THBAR
+        thb_init[k] = thb[k]
+        qvb[k] = QVBAR
+        pib[k] = PIBAR
+        pb[k] = PBAR
+        rhou[k] = RHOZ
+        rhow[k] = RHO
+        q1[k] = Q1LS * 6.
+        q2[k] = Q2LS * 6.
+    for a in (thb, thb_init, qvb, pib, pb, rhou, rhow):
+        _center1d(a)
+    rhow[nz - 1] = rhou[nz - 2]
+    for k in range(nz - 1):
+        pib[k] = math.pow(pb[k] / 100000., RD / CP)
+    z = np.zeros(nz)
+    z_zeta = np.zeros(nz)
+    lambda2 = np.zeros(nz)
+    for k in range(1, nz - 1):
+        z[k] = (k - 0.5) * dz
+        z_zeta[k] = (k - 1) * dz
+        lambda2[k] = 1. / (1. / math.pow(0.23 * math.sqrt(dx * dz), 2) + 1. / math.pow(0.4 * 0.4 * z[k], 2))
+    z[0], z[nz - 1] = z[1], z[nz - 2]
+    z_zeta[0], z_zeta[nz - 1] = z_zeta[1], z_zeta[nz - 2]
+    prof = dict(thb=thb, thvb=thb + 0.61 * qvb, qvb=qvb, pib=pib, pb=pb, rhou=rhou, rhow=rhow,
+                thb_init=thb_init, qvb0=qvb.copy(), z=z, z_zeta=z_zeta, lambda2=lambda2, Q1LS=q1, Q2LS=q2)
+    forcing = random_perturbation_host(g, 0, -0.25, 0.25, 1.)
+    th = np.zeros((nx, nz))
+    th[1:nx - 1, 1:nz - 1] = thb[None, 1:nz - 1] + forcing[1:nx - 1, 1:nz - 1]
+    st = _assemble(g, prof, th, np.zeros((nx, nz)), np.zeros((nx, nz)))
+    st.fields["qv"][:] = qvb[None, :]
+    st.fields["init_th_forcing"] = forcing
+    return st

@@ -153,8 +153,9 @@ int vvm_gpu_random_perturbation(vvm_gpu_ctx* ctx, int t, double min_range, doubl
 /* The same field for an NX x NZ grid of level spacing dz, on the host only
  * (no context, no device): out is [NX+2][NZ+2] in the reference layout, its
  * ghost cells filled as BoundaryProcess2D_center fills them
- * (src/Boundary.cpp:9-19). Init2d adds the t = 0 field to th when
- * addforcingtime > 0 (src/Init.cpp:193-196). */
+ * (src/Boundary.cpp:9-19). Init2d adds the t = 0 field of the declaration's
+ * default range (-0.25, 0.25, 1., src/Declare.hpp:870) to th
+ * (src/Init.cpp:169-175 and :193-196). */
 int vvm_gpu_random_perturbation_host(int NX, int NZ, double dz, int t, double min_range,
                                      double max_range, double standard_deviation, double* out);
 int vvm_gpu_halo_all(vvm_gpu_ctx* ctx);     /* BoundaryProcess2D_all, Boundary.cpp:32-52 */

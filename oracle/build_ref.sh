@@ -18,6 +18,9 @@
 # Eigen is the copy vendored with the reference (include/Eigen, 3.3.91).
 #
 # usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# With REF_VARIANT=tropical it builds oracle/_ref/libvvmref_tropical.so from
+# oracle/ref_config_tropical.hpp instead (sounding file and Q1/Q2 forcing on),
+# reading the reference's own input/init.txt.
 set -euo pipefail
 REF=${1:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
@@ -27,13 +30,23 @@ if [ ! -f "$SRC/Declare.hpp" ]; then
     echo "build_ref.sh: reference sources not found under $REF" >&2
     exit 1
 fi
-mkdir -p "$OUT/obj"
+CONFIG="$HERE/ref_config.hpp"
+LIB=libvvmref.so
+OBJ="$OUT/obj"
+EXTRA=""
+if [ "${REF_VARIANT:-}" = tropical ]; then
+    CONFIG="$HERE/ref_config_tropical.hpp"
+    LIB=libvvmref_tropical.so
+    OBJ="$OUT/obj_tropical"
+    EXTRA="-DREF_INIT_PATH=\"$REF/input/init.txt\""
+fi
+mkdir -p "$OBJ"
 CXX=${CXX:-g++}
-FLAGS="-std=c++17 -O3 -fPIC -w -I$REF/include -I$SRC"
+FLAGS="-std=c++17 -O3 -fPIC -w -I$REF/include -I$SRC $EXTRA"
 UNITS="Advection Boundary Buoyancy MicroPhysics Turbulent NumericalProcess PoissonSolver Iteration AddForcing Init"
 
 emit_unit() {  # $1 = path of the .cpp to append after the shared header
-    cat "$HERE/ref_config.hpp"
+    cat "$CONFIG"
     sed '/#include "Config.hpp"/d' "$SRC/Declare.hpp"
     sed -e '/#include "Declare.hpp"/d' -e '/pb_lev_all/d' -e '/radiation_heating_rate/d' "$1"
 }
@@ -41,13 +54,13 @@ emit_unit() {  # $1 = path of the .cpp to append after the shared header
 pids=""
 for u in $UNITS ref_harness; do
     if [ "$u" = ref_harness ]; then f="$HERE/ref_harness.cpp"; else f="$SRC/$u.cpp"; fi
-    ( emit_unit "$f" | $CXX $FLAGS -x c++ -c - -o "$OUT/obj/$u.o" ) &
+    ( emit_unit "$f" | $CXX $FLAGS -x c++ -c - -o "$OBJ/$u.o" ) &
     pids="$pids $!"
 done
 for p in $pids; do wait "$p"; done
 objs=""
-for u in $UNITS ref_harness; do objs="$objs $OUT/obj/$u.o"; done
+for u in $UNITS ref_harness; do objs="$objs $OBJ/$u.o"; done
 # link the shared libstdc++ explicitly: with a static copy inside the .so,
 # std::cout is never constructed when the host process has no libstdc++ loaded
-$CXX -shared -o "$OUT/libvvmref.so" $objs -l:libstdc++.so.6
-echo "built $OUT/libvvmref.so"
+$CXX -shared -o "$OUT/$LIB" $objs -l:libstdc++.so.6
+echo "built $OUT/$LIB"

@@ -2,6 +2,9 @@
 
 * ``RefModel``  -- oracle/_ref/libvvmref.so: the reference's own sources built
   by oracle/build_ref.sh behind oracle/ref_harness.cpp (uniform dx = dz only).
+* ``RefTropicalModel`` -- oracle/_ref/libvvmref_tropical.so: the same sources
+  built with the reference's sounding file and Q1/Q2 forcing switched on
+  (oracle/ref_config_tropical.hpp), for the initial state read from it.
 * ``PortModel`` -- oracle/_build/libvvmoracle.so: the C restatement in
   oracle/vvm_oracle.c (exact elliptic solves).
 
@@ -18,6 +21,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libvvmref.so"
+REF_TROPICAL_LIB = HERE / "_ref" / "libvvmref_tropical.so"
 PORT_LIB = HERE / "_build" / "libvvmoracle.so"
 
 HIST_NAMES = ("dzeta_advect", "dth_buoyancy", "dth_advect", "dqv_advect", "dqc_advect",
@@ -57,6 +61,10 @@ def _load(path: Path, prefix: str):
 
 def ref_available() -> bool:
     return REF_LIB.exists()
+
+
+def ref_tropical_available() -> bool:
+    return REF_TROPICAL_LIB.exists()
 
 
 def port_available() -> bool:
@@ -236,6 +244,25 @@ class RefModel(_CModel):
         it, err = ctypes.c_int(), ctypes.c_double()
         rc = L.ref_solve_A(self.h, _dptr(b), _dptr(x), ctypes.byref(it), ctypes.byref(err))
         return x, it.value, err.value, rc
+
+
+class RefTropicalModel(RefModel):
+    """The reference built with LOADFILE and TROPICALFORCING: Init1d reads its
+    1D base state from the reference's input/init.txt (src/Init.cpp:301-370)."""
+    path = REF_TROPICAL_LIB
+
+    @classmethod
+    def init_path(cls) -> str:
+        """The sounding file the build reads (compiled in by build_ref.sh)."""
+        L = _load(cls.path, cls.prefix)
+        L.ref_init_path.restype = ctypes.c_char_p
+        return L.ref_init_path().decode()
+
+    def init(self):
+        """vvm::Init::Init1d then Init2d, as src/main.cpp:81-82 runs them."""
+        self.L.ref_init.argtypes = [ctypes.c_void_p]
+        self.L.ref_init(self.h)
+        self._after_load()   # the cal_w matrix, as after load()
 
 
 class PortModel(_CModel):

@@ -162,6 +162,9 @@ double* ref_prof(void* h, const char* name) {
         {"qvb", m.qvb}, {"qvb0", m.qvb0}, {"qvsb", m.qvsb}, {"pb", m.pb}, {"pb_lev", m.pb_lev},
         {"xi", m.xi}, {"uxi", m.uxi}, {"thvb", m.thvb}, {"thvbm", m.thvbm}, {"z", m.z},
         {"z_zeta", m.z_zeta}, {"lambda2", m.lambda2}, {"precip", m.precip},
+#if defined(TROPICALFORCING)
+        {"Q1LS", m.Q1LS}, {"Q2LS", m.Q2LS},
+#endif
     };
     for (auto& e : tab) if (std::strcmp(e.n, name) == 0) return e.p;
     return nullptr;
@@ -219,6 +222,23 @@ int ref_call(void* h, const char* name) {
     else if (n == "one_step") one_step(m);
     else return -1;
     return 0;
+}
+
+// The sounding file this build's Init1d reads ("" without LOADFILE).
+const char* ref_init_path() {
+#if defined(LOADFILE)
+    return LOADINITPATH;
+#else
+    return "";
+#endif
+}
+
+// vvm::Init::Init1d then Init2d, as src/main.cpp:81-82 runs them.
+void ref_init(void* h) {
+    vvm& m = *static_cast<vvm*>(h);
+    CoutMute mute;
+    vvm::Init::Init1d(m);
+    vvm::Init::Init2d(m);
 }
 
 // vvm::Init::RandomPerturbation(model, t, min_range, max_range,
