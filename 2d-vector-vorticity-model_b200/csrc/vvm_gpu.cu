@@ -2963,6 +2963,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     if (!(D.dx > 0) || !(D.dz > 0) || !(D.dt > 0)) return fail(nullptr, VVM_GPU_EINVAL, "create: dx, dz, dt must be > 0");
     if (D.precision != VVM_PREC_FP64 && D.precision != VVM_PREC_MIXED)
         return fail(nullptr, VVM_GPU_EINVAL, "create: unknown precision");
+    if (D.flags & ~VVM_FLAG_FIXED_FORCING) return fail(nullptr, VVM_GPU_EINVAL, "create: unknown flags");
     if (D.solver != VVM_SOLVER_MGPCG && D.solver != VVM_SOLVER_LEARNED && D.solver != VVM_SOLVER_SPECTRAL)
         return fail(nullptr, VVM_GPU_EINVAL, "create: unknown solver");
     if (D.solver == VVM_SOLVER_SPECTRAL && !Spectral<double>::supports(D.NX))
