@@ -36,11 +36,22 @@ def test_sounding_state_equals_reference_init():
     assert st.scalars["ubarTop"] == m.scalar("ubarTop")[0]
 
 
-def test_sounding_rows_beyond_the_levels_are_refused(tmp_path):
+def test_sounding_rows_beyond_the_levels_are_refused():
     path = RefTropicalModel.init_path()
     NZ = len(read_sounding(path))
     with pytest.raises(ValueError):
         sounding_state(path, 16, NZ - 1, 200.0, 200.0, 1.0)
+
+
+def test_reader_stops_at_the_first_row_that_does_not_parse(tmp_path):
+    """`inputFile >> ZZ >> ... >> RHOZ` stops at the first field that is not a
+    number; rows after it are not read (src/Init.cpp:312)."""
+    f = tmp_path / "snd.txt"
+    rows = np.arange(30, dtype=float).reshape(3, 10) + 1.0
+    text = "# header\n0 0 0 0 0 0 0 0 0 0\n" + "\n".join(" ".join(repr(float(v)) for v in r) for r in rows)
+    f.write_text(text + "\n1 2 3 x 5 6 7 8 9 10\n" + " ".join(["4"] * 10) + "\n")
+    got = read_sounding(f)
+    assert got.shape == (3, 10) and np.array_equal(got, rows)
 
 
 def test_restatement_follows_the_reference_steps(port_lib):
