@@ -171,11 +171,19 @@ void ck(cudaError_t e, const char* what) {
 std::mutex g_mu;
 double* g_addr[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device; looked up once
-// per device (the lookup may load the module onto the device).
-double* scratch_on(int dev) {
+// Device address of the scratch array on the current device. The first call
+// on a device looks it up (which may load the module onto the device); later
+// calls look it up again unless `st` is capturing, so a caller that reset the
+// device (cudaDeviceReset, which reloads the module and may move the array)
+// gets the new address. Under capture the address from the last call outside
+// capture is used.
+double* scratch_on(int dev, cudaStream_t st) {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    ck(cudaStreamIsCapturing(st, &cap), "cudaStreamIsCapturing");
+    if (!g_addr[dev] || cap == cudaStreamCaptureStatusNone) {
+        if (cap != cudaStreamCaptureStatusNone)
+            throw Fail{VVM_GPU_ESTATE, "poisson_solve_noalloc: the first call on a device may not be captured"};
         void* p = nullptr;
         ck(cudaGetSymbolAddress(&p, g_scratch), "cudaGetSymbolAddress");
         g_addr[dev] = static_cast<double*>(p);
@@ -236,8 +244,8 @@ int solve(int NX, int NZ, const double* rhou, const double* rhow, const double* 
     if (dev < 0 || dev >= kMaxDevices) throw Fail{VVM_GPU_EINVAL, "poisson_solve_noalloc: device index too large"};
     check_device_buffer(d_b, dev, "b");
     check_device_buffer(d_W, dev, "W");
-    double* S = scratch_on(dev);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    double* S = scratch_on(dev, st);
     ck(cudaMemcpyAsync(S + kOffRow, row.data(), row.size() * sizeof(double), cudaMemcpyHostToDevice, st),
        "copy of the row coefficients");
     Rows R{S + kOffRow, S + kOffRow + kMaxRows, S + kOffRow + 2 * kMaxRows, S + kOffRow + 3 * kMaxRows,

@@ -1,4 +1,4 @@
-"""The batched-ensemble workload and its sharding.
+"""The batched-ensemble workload (256 uneven warm-bubble cases) and its sharding.
 
 Each of `n` cases is a plain warm bubble whose grid and bubble are drawn from
 a seeded generator: NX from {256, 512, 1024, 2048}, NZ from {64, 96, 128},

@@ -6,16 +6,18 @@ NX=2048 x NZ=256 grid, dx = dz = 100 m, dt = 1 s, synthetic seeded initial
 state (theta = 300 K + 3 K/km, 80 % RH, +2 K cosine bubble of radius 2 km).
 A "step" is one call of the reference's TimeMarching body.
 
-Our arm (default): the mixed-precision step (FP32 fields and stencils, FP64
-Kessler arithmetic and reductions) with the cal_w solve by the exact
-Fourier-mode solve in FP64, residual-checked, CG only if the check fails
-(VVM_SOLVER_SPECTRAL) is the headline `value`. The plain FP64 multigrid-PCG step is timed the same way and
-reported beside it (`plain_fp64`), with the two other combinations under
-`variants`. Every timed step is bracketed by
-CUDA events on the stream the library launches on; L2 is flushed (a 256 MB
-write) between timed steps, outside the timed windows. `e2e` repeats the
-headline through the C ABI with the prognostic fields copied from pinned host
-memory before and back after every step.
+Our arm (default): the headline `value` is the step at the reference's
+precision, FP64 throughout, with the cal_w solve by the exact Fourier-mode
+solve in FP64, residual-checked against 1e-10, CG only if the check fails
+(VVM_SOLVER_SPECTRAL). The plain FP64 multigrid-PCG step is timed the same
+way (`plain_fp64`). The mixed-precision step (FP32 fields and stencils, FP64
+Kessler arithmetic, residual, refinement and reductions) is reported under
+`mixed`, with its accuracy after 600 steps against the FP64 step on the same
+grid (domain-mean th and qc within 1e-4 relative is its bar). Every timed step
+is bracketed by CUDA events on the stream the library launches on; L2 is
+flushed (a 256 MB write) between timed steps, outside the timed windows.
+`e2e` repeats the headline through the C ABI with the prognostic fields
+copied from pinned host memory before and back after every step.
 
 Reference arm (--impl reference): the reference's own TimeMarching, built from
 its sources into oracle/_ref/libvvmref.so (serial: its OpenMP loops race and
@@ -24,7 +26,7 @@ one full-grid reference step.
 
 Multi-GPU (torchrun): one independent replica per GPU ("replicas only": one
 2D domain does not shard), max time over ranks, value = all ranks' cell-steps
-per second. The `ensemble` object measures BASELINE configuration 3, 256
+per second. The `ensemble` object measures the batched-ensemble workload, 256
 independent cases of uneven grids in one CUDA graph a step, split over the
 ranks by cost (strong scaling: the ensemble is fixed).
 """
@@ -228,6 +230,32 @@ def cpu_baseline(steps_hint=1):
             "sample": f"{n} full-grid step(s) of the same workload, serial build, {dt:.1f} s"}
 
 
+def mixed_accuracy(steps=600):
+    """Domain means of the mixed-precision step (spectral solve) after
+    `steps` steps of the headline workload against the FP64 multigrid-PCG
+    step from the same initial state: relative differences of th, qc, qr,
+    surface rain and kinetic energy (the bar: th and qc within 1e-4)."""
+    from vvm_b200.gpu import VVM_PREC_FP64, VVM_PREC_MIXED, VVM_SOLVER_MGPCG, VVM_SOLVER_SPECTRAL, VVMGpu
+    from vvm_b200.initial_state import warm_bubble
+    from vvm_b200.precision_runs import NAMES, domain_means
+    st = warm_bubble(NX, NZ, DX, DX, DT)
+    means = {}
+    for name, prec, solver in (("fp64", VVM_PREC_FP64, VVM_SOLVER_MGPCG),
+                               ("mixed", VVM_PREC_MIXED, VVM_SOLVER_SPECTRAL)):
+        g = VVMGpu(st.grid, precision=prec, solver=solver)
+        g.upload(st)
+        g.step(steps)
+        means[name] = domain_means(g.download())
+        g.close()
+    rel = {n: (abs(a - r) / abs(r) if r != 0 else None)
+           for n, a, r in zip(NAMES, means["mixed"].tolist(), means["fp64"].tolist())}
+    return {"steps": steps, "against": "FP64 step, multigrid-PCG, same grid and initial state",
+            "rel_diff": rel, "fp64_means": dict(zip(NAMES, means["fp64"].tolist())),
+            "bar": "th and qc within 1e-4 relative",
+            "meets_bar": bool(rel["th"] is not None and rel["qc"] is not None
+                              and rel["th"] <= 1e-4 and rel["qc"] <= 1e-4)}
+
+
 def our_arm(args, rank, world, device):
     import torch
     torch.cuda.set_device(device)
@@ -239,9 +267,9 @@ def our_arm(args, rank, world, device):
                               VVM_SOLVER_SPECTRAL)
     hbm, peak_kind = peaks()
     results = {}
-    variants = (("mixed_spectral", VVM_PREC_MIXED, VVM_SOLVER_SPECTRAL),
+    variants = (("fp64_spectral", VVM_PREC_FP64, VVM_SOLVER_SPECTRAL),
                 ("fp64_mgpcg", VVM_PREC_FP64, VVM_SOLVER_MGPCG),
-                ("fp64_spectral", VVM_PREC_FP64, VVM_SOLVER_SPECTRAL),
+                ("mixed_spectral", VVM_PREC_MIXED, VVM_SOLVER_SPECTRAL),
                 ("mixed_mgpcg", VVM_PREC_MIXED, VVM_SOLVER_MGPCG))
     with ClockSampler(device) as clk:
         for name, prec, solver in variants:
@@ -250,15 +278,16 @@ def our_arm(args, rank, world, device):
             g, st, times, launches, prof, it, rel = run_variant(torch, prec, solver, args.steps,
                                                                  args.warmup, flush, device)
             results[name] = dict(g=g, st=st, times=times, launches=launches, prof=prof, it=it, rel=rel)
-            if name not in ("mixed_spectral",):
+            if name != "fp64_spectral":
                 g.close()
                 results[name]["g"] = None
     clocks = clk.summary()
-    head = results["mixed_spectral"]
+    head = results["fp64_spectral"]
     cells = NX * NZ
     vms = {name: dist_max(sum(r["times"])) for name, r in results.items()}
     value, total_ms = whole_job_rate(sum(head["times"]), world, cells, args.steps)
     fp64_value, fp64_ms = whole_job_rate(sum(results["fp64_mgpcg"]["times"]), world, cells, args.steps)
+    mixed_value, mixed_ms = whole_job_rate(sum(results["mixed_spectral"]["times"]), world, cells, args.steps)
 
     # e2e through the C ABI with host buffers (pinned) copied in and out each step
     g = head["g"]
@@ -284,13 +313,16 @@ def our_arm(args, rank, world, device):
     def poisson_ms(prof):
         return sum(prof[c][0] for c in ("poisson_rhs", "cg", "mg_sweep", "mg_restrict", "mg_coarse")) / 2
 
+    def solve_rec(r):
+        return {"poisson_ms_per_solve": poisson_ms(r["prof"]), "poisson_iterations_last": r["it"],
+                "poisson_relres_last": r["rel"]}
+
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "NX": NX, "NZ": NZ, "dx_m": DX, "dz_m": DX, "dt_s": DT,
-                   "precision": "mixed: FP32 fields/stencils, FP64 Kessler arithmetic, FP64 "
-                                "Poisson CG/residual/reductions",
+                   "precision": "FP64 throughout (fields, stencils, Kessler, solve, reductions)",
                    "solver": "direct Fourier-mode solve (row FFTs + per-mode z tridiagonal) in "
                              "FP64, residual-checked; FP64 CG preconditioned by it if the check "
                              "fails",
@@ -300,26 +332,30 @@ def our_arm(args, rank, world, device):
         "poisson_solves_per_s": 1e3 / poisson_ms(head["prof"]),
         "poisson_iterations_last": head["it"], "poisson_relres_last": head["rel"],
         "plain_fp64": {"solver": "multigrid-PCG", "value": fp64_value,
-                       "ms_per_step": fp64_ms / args.steps,
-                       "poisson_ms_per_solve": poisson_ms(results["fp64_mgpcg"]["prof"]),
-                       "poisson_iterations_last": results["fp64_mgpcg"]["it"],
-                       "poisson_relres_last": results["fp64_mgpcg"]["rel"],
+                       "ms_per_step": fp64_ms / args.steps, **solve_rec(results["fp64_mgpcg"]),
                        "roofline": roofline(results["fp64_mgpcg"]["prof"], head["st"].grid, 8, hbm,
                                             peak_kind, results["fp64_mgpcg"]["it"])},
         "speedup_vs_plain_fp64": value / fp64_value,
+        "mixed": {"precision": "FP32 fields/stencils, FP64 Kessler arithmetic, FP64 Poisson "
+                               "residual/refinement/reductions",
+                  "solver": "spectral", "dtype": "f32+f64", "value": mixed_value,
+                  "ms_per_step": mixed_ms / args.steps, **solve_rec(results["mixed_spectral"]),
+                  "roofline": roofline(results["mixed_spectral"]["prof"], head["st"].grid, 4, hbm,
+                                       peak_kind, results["mixed_spectral"]["it"]),
+                  "vs_plain_fp64": mixed_value / fp64_value},
         "variants": {name: {"value": world * cells * args.steps / (vms[name] * 1e-3),
-                            "ms_per_step": vms[name] / args.steps,
-                            "poisson_ms_per_solve": poisson_ms(results[name]["prof"]),
-                            "poisson_iterations_last": results[name]["it"],
-                            "poisson_relres_last": results[name]["rel"]}
-                     for name in ("fp64_spectral", "mixed_mgpcg")},
-        "roofline": roofline(head["prof"], head["st"].grid, 4, hbm, peak_kind, head["it"]),
+                            "ms_per_step": vms[name] / args.steps, **solve_rec(results[name])}
+                     for name in ("mixed_mgpcg",)},
+        "roofline": roofline(head["prof"], head["st"].grid, 8, hbm, peak_kind, head["it"]),
         "kernel_ms_per_step": {k: v[0] / 2 for k, v in head["prof"].items()},
         "e2e": {"value": world * cells * args.steps / (e2e_ms * 1e-3), "unit": METRIC,
                 "h2d_bytes_per_step": field_bytes, "d2h_bytes_per_step": field_bytes},
         "gpu_launches": head["launches"],
         "clocks": clocks,
     }
+    g.close()
+    if not args.no_accuracy:
+        line["mixed"]["accuracy_600_steps"] = mixed_accuracy()
     if not args.no_learned:
         line["learned"] = learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms / args.steps)
         line["poisson_stretched"] = stretched_poisson_arm(world, device)
@@ -409,7 +445,7 @@ def learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms_per_step, st
 
 
 def stretched_poisson_arm(world, device, reps=5):
-    """the cal_w solve on NX=2048, NZ=256 stretched
+    """The stretched-level Poisson workload: the cal_w solve on NX=2048, NZ=256 stretched
     levels (dz 100 m -> 500 m, tanh ramp; dx = 250 m), right-hand sides of
     seeded bubble/cold-pool vorticity dipoles. Learned-PCG (trained on 16 such
     right-hand sides plus 16 white-noise ones) against FP64 multigrid-PCG and
@@ -481,7 +517,7 @@ ENSEMBLE_CASES, ENSEMBLE_SEED = 256, 3
 
 
 def ensemble_arm(args, rank, world, device):
-    """256 seeded warm-bubble cases of uneven grids
+    """The batched-ensemble workload: 256 seeded warm-bubble cases of uneven grids
     (vvm_b200.ensemble), mixed precision with the spectral solve, one batch
     graph a step on each rank; the cases are split over the ranks by cost.
     The ensemble is fixed, so more ranks is strong scaling."""
@@ -599,6 +635,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-case batched ensemble")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner step")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the 600-step mixed-vs-FP64 domain means on the headline grid")
     ap.add_argument("--no-long-runs", action="store_true",
                     help="skip the 1800-step 8192x256 squall line (mixed vs FP64 domain means)")
     args = ap.parse_args()

@@ -326,8 +326,12 @@ int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len);
  * before reading it. The first call on each device does a one-time set-up
  * (it looks up the array's device address, which may load the library's
  * device code): make it, with that device current, before any stream capture
- * begins. Calls that overlap on one device (two host threads, or two streams
- * without ordering between them) share the one array and race: serialise them. */
+ * begins (a captured first call returns VVM_GPU_ESTATE). Each later call made
+ * outside capture looks the address up again, so a cudaDeviceReset between
+ * calls is harmless if the next call is not captured; a captured call uses
+ * the address of the last uncaptured one. Calls that overlap on one device
+ * (two host threads, or two streams without ordering between them) share the
+ * one array and race: serialise them. */
 #define VVM_NOALLOC_MAX_UNKNOWNS 131072
 #define VVM_NOALLOC_MAX_ROWS 1024
 #define VVM_NOALLOC_SCRATCH_BYTES 4251712

@@ -1,11 +1,15 @@
 """Long runs of the mixed-precision step against the FP64 step on sheared
-squall lines (vvm_b200.precision_runs): BASELINE configuration 5 (NX=8192,
-NZ=256, dx=dz=100 m, 1800 steps) and configuration 2's squall line on uniform
+squall lines (vvm_b200.precision_runs): the 8192-column squall line (NX=8192,
+NZ=256, dx=dz=100 m, 1800 steps) and the 1024-column squall line on uniform
 levels (NX=1024, NZ=128, dx=dz=250 m, dt=2 s, 3600 steps). The flow is
-convective, so fields diverge point by point; domain means stay close:
-th within 1e-6 relative, qc and qr within 5e-2, kinetic energy within 1e-3
-(observed: th 1e-10 / 7e-9, qc 5e-4 / 6e-4, qr 1e-3 / 8e-3, KE 5e-8 / 6e-5),
-and every Poisson solve meets its residual (the step raises otherwise)."""
+convective, so FP32 round-off grows point by point where cells cross
+saturation; domain means stay close: th within 1e-6 relative, qc within
+3e-3, qr within 2.5e-2, kinetic energy within 1e-3 (observed: th 1e-10 /
+7e-9, qc 4.6e-4 to 1.1e-3 / 5.7e-4, qr 1.4e-3 to 4.2e-3 / 8.4e-3, KE 5e-8 /
+6e-5; the spread at 8192 columns is between builds whose kernels associate FP32
+sums differently), and every Poisson solve meets its residual (the step
+raises otherwise). The bar of 1e-4 on th and qc is for 600 steps of the warm
+bubble at 2048x256 (tests/test_gpu_precision.py)."""
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -19,6 +23,6 @@ def test_mixed_step_domain_means_follow_fp64(case):
     out = run(case, variants=("fp64_mgpcg", "mixed_spectral"))
     d = out["mixed_spectral"]["rel_diff_vs_fp64"]
     assert d["th"] <= 1e-6, d
-    assert d["qc"] <= 5e-2 and d["qr"] <= 5e-2, d
+    assert d["qc"] <= 3e-3 and d["qr"] <= 2.5e-2, d
     assert d["ke"] <= 1e-3, d
     assert out["mixed_spectral"]["last_relres"] <= 1e-10 and out["fp64_mgpcg"]["last_relres"] <= 1e-10

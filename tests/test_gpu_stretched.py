@@ -1,4 +1,4 @@
-"""Poisson solves on stretched levels (BASELINE configuration 4's grid type:
+"""Poisson solves on stretched levels (the stretched-level Poisson workload's grid type:
 dz from 100 m to 500 m on a tanh ramp, dx = 250 m) against the restatement
 in oracle/stretched_poisson.py, solved directly by scipy: each solver reaches
 the reference's residual ||b - A W|| / ||b|| <= 1e-10 with the stretched A,
