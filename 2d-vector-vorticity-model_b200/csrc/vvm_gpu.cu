@@ -194,6 +194,56 @@ __global__ void k_w_from_W(Dims d, const double* rhow, const double* W, int pitc
     store_westdown(w, d, i, k, T(v));
 }
 
+// The streamfunction formulation (PoissonSolver::calpsiuw, STREAMFUNCTION,
+// src/PoissonSolver.cpp:124-177). Its matrix (src/PoissonSolver.cpp:726-756,
+// POISSONPARAM = 0) is -S with S the symmetric w-equation operator of
+// uniform levels; the right-hand side is b = zetap dx^2 over k = 2..nz-2,
+// i = 1..nx-2. So S psi = f with f = -b, and ||f - S psi|| / ||f|| is the
+// reference's ||b - A psi|| / ||b|| (an unweighted residual).
+template <typename T>
+__global__ void k_psi_rhs(Dims d, double dx, const T* zetap, double* f, int pitch_f, double* partial) {
+    __shared__ double sh[32];
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    double s[1] = {0};
+    if (ii < d.nx - 2 && kk < d.nz - 3) {
+        const double b = (double)zetap[d.at(ii + 1, kk + 2)] * dx * dx;
+        f[(size_t)kk * pitch_f + ii] = -b;
+        s[0] = b * b;
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
+}
+
+// psi with its ghosts (periodic columns, zero at k = 0, 1, nz-1), then
+//   u = -(rhow_{k+1} psi_{i,k+1} - rhow_k psi_{i,k}) rdz / rhou_k,
+//   w = (psi_{i+1,k} - psi_{i,k}) rdx,   i = 1..nx-2, k = 1..nz-2,
+// with u's centre halo and w's westdown halo (w = 0 at k = 0, 1, nz-1: the
+// routine's zeroing loop over i < nz, line 172, is overwritten by that halo).
+// One thread a cell of the padded [nz][pitch] arrays, ghosts included: a
+// ghost takes the value of the interior cell the halo copies into it.
+template <typename T>
+__global__ void k_psi_uw(Dims d, const double* rhou, const double* rhow, double rdx, double rdz, const double* X,
+                         int pitch_x, double* psi, T* u, T* w) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= d.nx || k >= d.nz) return;
+    const int NX = d.nx - 2, nz = d.nz;
+    auto P = [&](int ii, int kk) -> double {   // psi at interior column ii (1..NX, wrapped), level kk
+        if (kk <= 1 || kk >= nz - 1) return 0.0;
+        const int c = (ii - 1 + NX) % NX;
+        return X[(size_t)(kk - 2) * pitch_x + c];
+    };
+    const int iw = (i == 0) ? NX : (i == d.nx - 1 ? 1 : i);   // periodic ghost columns
+    psi[d.at(i, k)] = P(iw, k);
+    const int ku = k < 1 ? 1 : (k > nz - 2 ? nz - 2 : k);        // u: zero-gradient rows
+    const double uv = -(rhow[ku + 1] * P(iw, ku + 1) - rhow[ku] * P(iw, ku)) * rdz / rhou[ku];
+    u[d.at(i, k)] = T(uv);
+    double wv = 0.0;
+    if (k >= 2 && k <= nz - 2) wv = (P(iw + 1, k) - P(iw, k)) * rdx;
+    w[d.at(i, k)] = T(wv);
+}
+
 // Initial guess of the next cal_w from the last two solutions:
 // W <- 2 W - Wprev, Wprev <- W (old).
 __global__ void k_extrapolate(int NX, int NK, int pitch, double* W, double* Wprev) {
@@ -1227,8 +1277,10 @@ struct PCG {
     // S = -diag(1/rw) A in symmetric form: cx_k = a_k / rhow_k, ru_k = h_k /
     // rhou_k, rd_k = h_{k-1} / rhou_{k-1}, rw_k = rhow_k / a_k (a = h = 1 on
     // uniform levels: the reference's matrix, PoissonSolver.cpp:760-796).
+    // `unweighted`: residual weight 1 on every row (the streamfunction
+    // system, whose reference residual carries no rhow).
     void build(Arena& ar, int NXr, int NKr, const std::vector<double>& rhou, const std::vector<double>& rhow,
-               const std::vector<double>& a, const std::vector<double>& h) {
+               const std::vector<double>& a, const std::vector<double>& h, bool unweighted = false) {
         NX = NXr;
         NK = NKr;
         std::vector<double> cx0(NK), ru(NK), rd(NK), rw(NK);
@@ -1237,7 +1289,7 @@ struct PCG {
             cx0[kk] = a[k] / rhow[k];
             ru[kk] = h[k] / rhou[k];
             rd[kk] = h[k - 1] / rhou[k - 1];
-            rw[kk] = rhow[k] / a[k];
+            rw[kk] = unweighted ? 1.0 : rhow[k] / a[k];
         }
         mg.stats = stats;
         mg.build(ar, NX, NK, cx0, ru, rd);
@@ -1362,6 +1414,7 @@ struct Fields {
     T *d_auto = nullptr, *d_accr = nullptr, *d_evap = nullptr, *d_cond = nullptr;
     T *precip = nullptr, *th_forcing = nullptr;
     T *gsA = nullptr, *gsC = nullptr, *gsB = nullptr;   // Gauss-Seidel coefficients, [5][cells]
+    T *gsRight = nullptr, *gsTop = nullptr;             // Gauss-Seidel tile outflows (k_gs_tiles)
 };
 
 }  // namespace
@@ -1377,7 +1430,8 @@ struct vvm_gpu_ctx {
     Consts c{};
     bool mixed = false;
     bool spectral = false;   // VVM_SOLVER_SPECTRAL
-    int tune_gs_cs = 0;      // cap on the CTAs of a Gauss-Seidel cluster (0: automatic)
+    int tune_gs_tr = 0;      // rows of a Gauss-Seidel tile (0: automatic)
+    GSTileCtl* gsctl = nullptr;   // pass state of the Gauss-Seidel tiles
     // learned preconditioner (VVM_SOLVER_LEARNED)
     std::unique_ptr<LearnedNet> net;
     double* z64 = nullptr;   // preconditioned residual, solver layout
@@ -1394,6 +1448,13 @@ struct vvm_gpu_ctx {
     Fields<float> f32;
     int cur = 0;       // buffer index of the "now" time level
     int step = 0;
+    // The reference's nextTimeStep copies each future array into the present
+    // one (src/Iteration.cpp:153-204), so after a whole step the model's *p
+    // arrays equal the present ones. Here the rotation is a pointer swap and
+    // the future buffers keep the previous level until the next step
+    // overwrites them; true while that holds, so a state download returns the
+    // present level for the *p arrays, as the reference's model holds them.
+    bool fut_is_now = false;
     bool has_state = false, has_forcing_th = false, has_q = false;
     // profiles
     double *rhou = nullptr, *rhow = nullptr, *thvb = nullptr, *thb = nullptr, *qvb = nullptr,
@@ -1421,6 +1482,10 @@ struct vvm_gpu_ctx {
     std::unique_ptr<PCG<double>> pcg64;
     std::unique_ptr<PCG<float>> pcg32;
     double *Wf = nullptr, *W = nullptr, *r64 = nullptr;   // level-0 layout, FP64
+    // streamfunction formulation (VVM_FLAG_STREAMFUNCTION / vvm_gpu_calpsiuw)
+    std::unique_ptr<PCG<double>> pcg_psi;
+    double *psi_f = nullptr, *psi_x = nullptr;   // right-hand side and solution, solver layout
+    double* psi = nullptr;                       // [nz][pitch] field with its ghosts
     double* Wprev = nullptr;   // previous cal_w solution (initial-guess extrapolation)
     int nsolves = 0;
     // CUDA graphs of one whole step, by (time-level buffer, step parity)
@@ -1429,7 +1494,6 @@ struct vvm_gpu_ctx {
     cudaStream_t cap[2] = {};          // streams for capturing loop bodies
     CGCtl* wctl = nullptr;             // outer loop state of the mixed solve
     long long* d_exec = nullptr;       // kernels executed inside graph loops
-    int* d_err = nullptr;              // device error word (kGSErrWait), checked when the host syncs
     bool last_graph = false;           // the last cal_w ran inside a graph
     bool graphs_off = false;
     float *g32 = nullptr, *d32 = nullptr;
@@ -1456,6 +1520,7 @@ struct vvm_gpu_ctx {
             if (s) cudaStreamDestroy(s);
         if (pcg64) pcg64->release();
         if (pcg32) pcg32->release();
+        if (pcg_psi) pcg_psi->release();
         if (sc_host) cudaFreeHost(sc_host);
         if (own) cudaStreamDestroy(own);
     }
@@ -1492,9 +1557,6 @@ template <>
 Fields<float>& fields<float>(vvm_gpu_ctx* c) { return c->f32; }
 
 template <typename T>
-void gs_set_smem();
-
-template <typename T>
 void alloc_fields(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     size_t n = c->d.cells();
@@ -1520,7 +1582,11 @@ void alloc_fields(vvm_gpu_ctx* c) {
     F.gsA = c->ar.alloc<T>(5 * n);
     F.gsC = c->ar.alloc<T>(5 * n);
     F.gsB = c->ar.alloc<T>(5 * n);
-    gs_set_smem<T>();
+    // tile outflows for any tile height in kGSTileRows
+    const size_t nc = cdiv(c->d.pitch, kGTCols), rows = c->d.nz - 2;
+    F.gsRight = c->ar.alloc<T>(2 * 5 * nc * (rows + kGSTileRowsMax));
+    F.gsTop = c->ar.alloc<T>(2 * 5 * nc * (size_t)cdiv((int)rows, kGSTileRowsMin) * kGTCols);
+    if (!c->gsctl) c->gsctl = c->ar.alloc<GSTileCtl>(1);
 }
 
 // ---------------------------------------------------------------- routines
@@ -1630,78 +1696,96 @@ void launch_kessler(vvm_gpu_ctx* c, bool halo) {
     launch_apply<T>(c, halo ? (F_TH | F_QV | F_QC | F_QR) : (F_QV | F_QC | F_QR), F_QV | F_QC | F_QR, false, halo);
 }
 
-// Launch shape of k_gs_cluster for a padded row of `pitch` cells of `elem`
-// bytes: chunks of 32*kGSPer cells (one warp each) over a cluster of cs CTAs
-// of w warps, coefficient rows d ahead.
-constexpr int kGSPer = 4;
-struct GSPlan {
-    int cs, w, d;
-    size_t smem;
+cudaGraphConditionalHandle new_handle(cudaStream_t st) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g;
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, nullptr, nullptr));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    return h;
+}
+
+// Appends a WHILE node (condition h) to the graph being captured on st and
+// returns its body graph; capture on st continues after the node.
+cudaGraph_t add_while(cudaStream_t st, cudaGraphConditionalHandle h) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &p));
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return p.conditional.phGraph_out[0];
+}
+
+struct BodyCapture {   // stream capture into a conditional node's body graph
+    cudaStream_t s;
+    BodyCapture(cudaStream_t s_, cudaGraph_t body) : s(s_) {
+        CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    }
+    void end() {
+        cudaGraph_t g;
+        CK(cudaStreamEndCapture(s, &g));
+    }
 };
-// max_cs > 0 caps the CTAs of a cluster (the autotuner's knob); the cap
-// never goes below the size whose CTAs would need more than
-// kGSClusterWarps warps.
-inline GSPlan gs_plan(int pitch, int nz, size_t elem, int max_cs = 0) {
-    GSPlan p{};
-    const int gwn = cdiv(pitch, 32 * kGSPer);
-    p.cs = gwn >= 8 ? 8 : (gwn >= 4 ? 4 : (gwn >= 2 ? 2 : 1));
-    while (max_cs > 0 && p.cs > max_cs && cdiv(gwn, p.cs / 2) <= kGSClusterWarps) p.cs /= 2;
-    p.w = cdiv(gwn, p.cs);   // <= kGSClusterWarps for pitch <= 8224 (checked at create)
-    const size_t row = 3 * (size_t)p.w * 32 * kGSPer * elem;
-    const size_t tab = 2 * (size_t)nz * elem;   // nudging scalars
-    p.d = (8 * row + tab <= kGSRingBytes) ? 8 : (4 * row + tab <= kGSRingBytes ? 4 : 2);
-    p.smem = p.d * row + tab;
-    return p;
-}
 
-template <typename T, int D, int CS>
-void gs_launch(vvm_gpu_ctx* c, const GSArgs<T>& g, const GSPlan& p) {
-    LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_cluster<T, kGSPer, D, CS><<<5 * CS, 32 * p.w, p.smem, c->stream>>>(g));
-}
-
-template <typename T, int D>
-void gs_launch_d(vvm_gpu_ctx* c, const GSArgs<T>& g, const GSPlan& p) {
-    if (p.cs == 8) gs_launch<T, D, 8>(c, g, p);
-    else if (p.cs == 4) gs_launch<T, D, 4>(c, g, p);
-    else if (p.cs == 2) gs_launch<T, D, 2>(c, g, p);
-    else gs_launch<T, D, 1>(c, g, p);
-}
-
-template <typename T, int D>
-void gs_set_smem_d() {
-    const int mx = (int)kGSRingBytes;
-    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-}
+inline int gs_tile_rows(const vvm_gpu_ctx* c) { return c->tune_gs_tr ? c->tune_gs_tr : kGSTileRowsDefault; }
 
 template <typename T>
-void gs_set_smem() {
-    gs_set_smem_d<T, 8>();
-    gs_set_smem_d<T, 4>();
-    gs_set_smem_d<T, 2>();
-}
-
-template <typename T>
-void launch_turbulence(vvm_gpu_ctx* c, bool nudge) {
+void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops = nullptr) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     RKArgs<T> r{c->d, c->c, c->profiles(), F.u, F.w, F.th[fut], F.RKM, F.RKH};
     LAUNCH(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r));
     CKL();
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
-                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, F.gsC, F.gsB, c->d_err};
+                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, F.gsC, F.gsB};
     const int pitch = c->d.pitch;
     dim3 cb(64, 4), cg(cdiv(pitch, 64), cdiv(c->d.nz - 2, 4), 5);
     LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_coeffs<T><<<cg, cb, 0, c->stream>>>(g));
     CKL();
-    // the recurrence: one cluster per field (see k_gs_cluster)
-    const GSPlan p = gs_plan(pitch, c->d.nz, sizeof(T), c->tune_gs_cs);
-    if (p.d == 8) gs_launch_d<T, 8>(c, g, p);
-    else if (p.d == 4) gs_launch_d<T, 4>(c, g, p);
-    else gs_launch_d<T, 2>(c, g, p);
+    // the recurrence: tiles and passes (see k_gs_tiles)
+    const int tr = gs_tile_rows(c);
+    const int nb = cdiv(c->d.nz - 2, tr), nc = cdiv(pitch, kGTCols);
+    GSTileArgs<T> t{nb, nc, tr, F.gsRight, F.gsTop, c->gsctl, recorded_in_loops ? c->d_exec : nullptr};
+    const size_t nout = (size_t)5 * nb * nc * (tr + kGTCols);
+    const int iblocks = (int)((nout + 255) / 256);
+    const int tblocks = cdiv(5 * nb * nc, 4);
+    const int maxp = nb + nc - 1;
+    cudaStream_t st = c->stream;
+    if (recorded_in_loops) {   // graph capture: the passes as a WHILE node
+        cudaGraphConditionalHandle h = new_handle(st);
+        LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles_init<T><<<iblocks, 256, 0, st>>>(g, t, h));
+        CKL();
+        cudaGraph_t body = add_while(st, h);
+        BodyCapture bc(c->cap[0], body);
+        const long long n0 = c->stats.launches;
+        LAUNCH(&c->stats, VVM_K_GS, bc.s, k_gs_tiles<T><<<tblocks, 128, 0, bc.s>>>(g, t, h));
+        CKL();
+        bc.end();
+        *recorded_in_loops += c->stats.launches - n0;
+        return;
+    }
+    LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles_init<T><<<iblocks, 256, 0, st>>>(g, t, 0));
     CKL();
+    // host loop: the passes are idempotent once converged, so the flag is
+    // read every other pass from the third on
+    for (int p = 1; p <= maxp; p++) {
+        LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T><<<tblocks, 128, 0, st>>>(g, t, 0));
+        CKL();
+        if (p >= 3 && (p % 2 == 1 || p == maxp)) {
+            int more = 1;
+            CK(cudaMemcpyAsync(&more, &c->gsctl->more, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (!more) break;
+        }
+    }
 }
 
 template <typename T>
@@ -1977,45 +2061,6 @@ int solve_w(vvm_gpu_ctx* c, double bb, double tol, bool warm) {
 
 // ---------------------------------------------------------------- graphs
 
-cudaGraphConditionalHandle new_handle(cudaStream_t st) {
-    cudaStreamCaptureStatus status;
-    cudaGraph_t g;
-    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, nullptr, nullptr));
-    cudaGraphConditionalHandle h;
-    CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
-    return h;
-}
-
-// Appends a WHILE node (condition h) to the graph being captured on st and
-// returns its body graph; capture on st continues after the node.
-cudaGraph_t add_while(cudaStream_t st, cudaGraphConditionalHandle h) {
-    cudaStreamCaptureStatus status;
-    cudaGraph_t g;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t nd = 0;
-    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, &deps, &nd));
-    cudaGraphNodeParams p = {};
-    p.type = cudaGraphNodeTypeConditional;
-    p.conditional.handle = h;
-    p.conditional.type = cudaGraphCondTypeWhile;
-    p.conditional.size = 1;
-    cudaGraphNode_t node;
-    CK(cudaGraphAddNode(&node, g, deps, nd, &p));
-    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
-    return p.conditional.phGraph_out[0];
-}
-
-struct BodyCapture {   // stream capture into a conditional node's body graph
-    cudaStream_t s;
-    BodyCapture(cudaStream_t s_, cudaGraph_t body) : s(s_) {
-        CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    }
-    void end() {
-        cudaGraph_t g;
-        CK(cudaStreamEndCapture(s, &g));
-    }
-};
-
 // Records the cal_w solve with device-side loop control (graph capture on
 // c->stream). The FP64 step: one PCG loop to tol. The mixed step: FP64
 // residual refinement around an FP32 PCG loop. Returns the number of
@@ -2157,6 +2202,65 @@ void launch_cal_u(vvm_gpu_ctx* c) {
     CKL();
 }
 
+// The psi system's solver: the w-equation's operator on uniform levels with
+// an unweighted residual; the exact Fourier-mode solve when NX is a power of
+// two (checked, CG from there), multigrid-PCG otherwise.
+void ensure_psi(vvm_gpu_ctx* c) {
+    if (c->pcg_psi) return;
+    const int NX = c->d.nx - 2, NK = c->d.nz - 3;
+    std::vector<double> one(c->d.nz, 1.0);
+    c->pcg_psi.reset(new PCG<double>());
+    c->pcg_psi->stats = &c->stats;
+    c->pcg_psi->spectral = Spectral<double>::supports(NX);
+    c->pcg_psi->build(c->ar, NX, NK, c->h_rhou, c->h_rhow, one, one, true);
+    const int pitch = c->pcg_psi->pitch;
+    c->psi_f = c->ar.alloc<double>((size_t)NK * pitch);
+    c->psi_x = c->ar.alloc<double>((size_t)NK * pitch);
+    c->psi = c->ar.alloc<double>(c->d.cells());
+    if (!c->sc_host) CK(cudaMallocHost(&c->sc_host, sizeof(double)));
+    if (!c->wpartial) {
+        dim3 g(cdiv(NX, 64), cdiv(NK, 4));
+        c->wnpart = g.x * g.y;
+        c->wpartial = c->ar.alloc<double>(c->wnpart);
+    }
+}
+
+// PoissonSolver::calpsiuw (src/PoissonSolver.cpp:124-177): psi from zetap,
+// then u and w from psi, each with the halos the routine applies. The solve
+// starts from zero as the reference's does and stops at desc.poisson_tol.
+template <typename T>
+int launch_calpsiuw(vvm_gpu_ctx* c) {
+    ensure_psi(c);
+    PCG<double>& P = *c->pcg_psi;
+    Fields<T>& F = fields<T>(c);
+    const int fut = 1 - c->cur;
+    const int NX = c->d.nx - 2, NK = c->d.nz - 3, pitch = P.pitch;
+    dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
+    LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_psi_rhs<T><<<G, B, 0, c->stream>>>(c->d, c->c.dx, F.zeta[fut], c->psi_f, pitch, c->wpartial));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, c->stream, k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, P.sc, CG_SET_BB));
+    CKL();
+    CK(cudaMemcpyAsync(c->sc_host, &P.sc->bb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double bb = *c->sc_host;
+    const int maxit = c->desc.poisson_maxit > 0 ? c->desc.poisson_maxit : 200;
+    double rel = 0.0;
+    int it = 0;
+    if (bb == 0.0) {
+        CK(cudaMemsetAsync(c->psi_x, 0, (size_t)NK * pitch * sizeof(double), c->stream));
+    } else if (P.spectral) {
+        P.sp.apply_to(c->psi_f, c->psi_x, c->stream);
+        it = P.solve(c->psi_f, c->psi_x, true, bb, c->desc.poisson_tol, maxit, c->stream, &rel);
+    } else {
+        it = P.solve(c->psi_f, c->psi_x, false, bb, c->desc.poisson_tol, maxit, c->stream, &rel);
+    }
+    c->last_iters = it;
+    c->last_relres = rel;
+    LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_psi_uw<T><<<c->grid_all(), c->blk(), 0, c->stream>>>(c->d, c->rhou, c->rhow, c->c.rdx, c->c.rdz, c->psi_x, pitch, c->psi, F.u, F.w));
+    CKL();
+    return (rel <= c->desc.poisson_tol) ? VVM_GPU_OK : VVM_GPU_ENOCONV;
+}
+
 // ---------------------------------------------------------------- one step
 
 template <typename T>
@@ -2165,13 +2269,18 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     launch_pzeta<T>(c);                                        // pzeta_pt
     launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
     launch_apply<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true); // NVP, AddForcing, halos
-    launch_pubartop<T>(c);                                     // pubarTop_pt
-    int rc = launch_cal_w<T>(c, recorded_in_loops);            // cal_w
-    launch_cal_u<T>(c);                                        // cal_u
+    int rc = VVM_GPU_OK;
+    if (c->desc.flags & VVM_FLAG_STREAMFUNCTION) {
+        rc = launch_calpsiuw<T>(c);                            // calpsiuw (Iteration.cpp:289-290)
+    } else {
+        launch_pubartop<T>(c);                                 // pubarTop_pt
+        rc = launch_cal_w<T>(c, recorded_in_loops);            // cal_w
+        launch_cal_u<T>(c);                                    // cal_u
+    }
     launch_kessler<T>(c, true);                                // Kessler + NVP x3 + halos
     // The first updateMean of the step (Iteration.cpp:408) only writes thb,
     // qvb, thvb, which nextTimeStep's updateMean overwrites before any read.
-    launch_turbulence<T>(c, true);                             // RKM_RKH + diffusion + theta/zeta nudging
+    launch_turbulence<T>(c, true, recorded_in_loops);          // RKM_RKH + diffusion + theta/zeta nudging
     if (c->desc.moisture_nudge_time != 0.0) launch_nudge<T>(c, false, true);
     launch_update_mean<T>(c, true);                            // nextTimeStep: means, ubarTop
     c->cur = 1 - c->cur;                                       // time levels by pointer swap
@@ -2227,14 +2336,17 @@ int step_once(vvm_gpu_ctx* c) {
     const bool forcing_now = c->has_forcing_th && ((c->step + 1) * c->desc.dt <= c->desc.addforcingtime);
     const bool warm = c->desc.warm_start != 0;
     const bool use_graph = !c->graphs_off && !c->stats.on && c->step >= 0 && !forcing_now &&
-                           c->poisson_ready && (!warm || c->nsolves >= 2);
+                           c->poisson_ready && (!warm || c->nsolves >= 2) &&
+                           !(c->desc.flags & VVM_FLAG_STREAMFUNCTION);
     if (!use_graph) {
         c->last_graph = false;
         // TimeMarching makes the step's forcing field before AddForcing
         // (src/Iteration.cpp:276-283); nothing before AddForcing reads it
         if (forcing_now && !(c->desc.flags & VVM_FLAG_FIXED_FORCING))
             if (int rc = regen_forcing(c, c->step + 1, -0.001, 0.001, 1.)) return rc;
-        return run_step<T>(c);
+        const int rc = run_step<T>(c);
+        c->fut_is_now = true;
+        return rc;
     }
     cudaGraphExec_t ex = step_graph<T>(c);
     const int b = c->cur, par = (c->step + 1) & 1;
@@ -2244,6 +2356,7 @@ int step_once(vvm_gpu_ctx* c) {
     c->cur = 1 - c->cur;
     c->nsolves++;
     c->last_graph = true;
+    c->fut_is_now = true;
     return VVM_GPU_OK;
 }
 
@@ -2254,6 +2367,7 @@ int step_once(vvm_gpu_ctx* c) {
 struct Snapshot {
     std::vector<void*> copies;
     int step = 0, cur = 0, nsolves = 0, last_iters = 0;
+    bool fut_is_now = false;
     double last_relres = 0;
     long long launches = 0;
     void take(vvm_gpu_ctx* c) {
@@ -2267,6 +2381,7 @@ struct Snapshot {
         CK(cudaStreamSynchronize(c->stream));
         step = c->step;
         cur = c->cur;
+        fut_is_now = c->fut_is_now;
         nsolves = c->nsolves;
         last_iters = c->last_iters;
         last_relres = c->last_relres;
@@ -2279,6 +2394,7 @@ struct Snapshot {
         CK(cudaStreamSynchronize(c->stream));
         c->step = step;
         c->cur = cur;
+        c->fut_is_now = fut_is_now;
         c->nsolves = nsolves;
         c->last_iters = last_iters;
         c->last_relres = last_relres;
@@ -2295,7 +2411,7 @@ bool graph_ready(vvm_gpu_ctx* c) {
     const bool forcing_now = c->has_forcing_th && ((c->step + 1) * c->desc.dt <= c->desc.addforcingtime);
     const bool warm = c->desc.warm_start != 0;
     return !c->graphs_off && !c->stats.on && c->step >= 0 && !forcing_now && c->poisson_ready &&
-           (!warm || c->nsolves >= 2);
+           (!warm || c->nsolves >= 2) && !(c->desc.flags & VVM_FLAG_STREAMFUNCTION);
 }
 
 }  // namespace
@@ -2451,6 +2567,7 @@ int batch_step(vvm_gpu_batch* b, int nsteps) {
             c->cur = 1 - c->cur;
             c->nsolves++;
             c->last_graph = true;
+            c->fut_is_now = true;
         }
     }
     if (on_batch) batch_fence(b, false);
@@ -2507,10 +2624,10 @@ int batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
         }
         groups[gi].push_back((int)i);
     }
-    auto set_all = [&](const std::vector<int>& idx, int cs, int fft) {
+    auto set_all = [&](const std::vector<int>& idx, int tr, int fft) {
         for (int i : idx) {
             vvm_gpu_ctx* c = b->cases[i];
-            c->tune_gs_cs = cs;
+            c->tune_gs_tr = tr;
             c->tune_fft = fft;
             apply_tuning(c);
         }
@@ -2518,14 +2635,14 @@ int batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
     for (size_t gi = 0; gi < groups.size() && rc == VVM_GPU_OK; gi++) {
         const std::vector<int>& idx = groups[gi];
         vvm_gpu_ctx* c = b->cases[idx[0]];
-        int best_cs = c->tune_gs_cs, best_fft = c->tune_fft;
+        int best_cs = c->tune_gs_tr, best_fft = c->tune_fft;
         double best = batch_time(b, idx, reps);
-        for (int cs : {8, 4, 2, 1}) {
-            set_all(idx, cs, best_fft);
+        for (int tr : {4, 8, 16, 32}) {   // rows of a Gauss-Seidel tile
+            set_all(idx, tr, best_fft);
             const double t = batch_time(b, idx, reps);
             if (t < best) {
                 best = t;
-                best_cs = cs;
+                best_cs = tr;
             }
         }
         set_all(idx, best_cs, best_fft);
@@ -2833,7 +2950,7 @@ template <typename T>
 int download_state_t(vvm_gpu_ctx* c, vvm_gpu_host_state* s) {
     Fields<T>& F = fields<T>(c);
     download_prognostic_t<T>(c, s);
-    int fut = 1 - c->cur;
+    const int fut = c->fut_is_now ? c->cur : 1 - c->cur;
     struct { double* h; T* dptr; const double* ref; } m[] = {
         {s->zetap, F.zeta[fut], nullptr}, {s->thp, F.th[fut], c->offset_th()}, {s->qvp, F.qv[fut], c->offset_qv()},
         {s->qcp, F.qc[fut], nullptr}, {s->qrp, F.qr[fut], nullptr}, {s->RKM, F.RKM, nullptr},
@@ -2902,16 +3019,6 @@ int need_uniform(vvm_gpu_ctx* c) {
                         : VVM_GPU_OK;
 }
 
-// Reads and clears the device error word (after the stream's work is done).
-int device_errors(vvm_gpu_ctx* c) {
-    if (!c->d_err) return VVM_GPU_OK;
-    int h = 0;
-    CK(cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (!h) return VVM_GPU_OK;
-    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    return fail(c, VVM_GPU_ECUDA, "Gauss-Seidel diffusion: a wait between warps gave up; the state is invalid");
-}
 
 }  // namespace
 
@@ -2950,8 +3057,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     *out = nullptr;
     const vvm_gpu_desc& D = *desc;
     if (D.NX < 4 || D.NZ < 4) return fail(nullptr, VVM_GPU_EINVAL, "create: NX and NZ must be >= 4");
-    if (D.NX > kGSMaxNX || gs_plan(round_up(D.NX + 2, kPad), D.NZ + 2, 8).w > kGSClusterWarps)
-        return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
+    if (D.NX > kGSMaxNX) return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
     if (D.NZ - 1 > 32 * kMaxSeg)
         return fail(nullptr, VVM_GPU_EINVAL, "create: NZ exceeds 1025");
     {
@@ -2963,7 +3069,8 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     if (!(D.dx > 0) || !(D.dz > 0) || !(D.dt > 0)) return fail(nullptr, VVM_GPU_EINVAL, "create: dx, dz, dt must be > 0");
     if (D.precision != VVM_PREC_FP64 && D.precision != VVM_PREC_MIXED)
         return fail(nullptr, VVM_GPU_EINVAL, "create: unknown precision");
-    if (D.flags & ~VVM_FLAG_FIXED_FORCING) return fail(nullptr, VVM_GPU_EINVAL, "create: unknown flags");
+    if (D.flags & ~(VVM_FLAG_FIXED_FORCING | VVM_FLAG_STREAMFUNCTION))
+        return fail(nullptr, VVM_GPU_EINVAL, "create: unknown flags");
     if (D.solver != VVM_SOLVER_MGPCG && D.solver != VVM_SOLVER_LEARNED && D.solver != VVM_SOLVER_SPECTRAL)
         return fail(nullptr, VVM_GPU_EINVAL, "create: unknown solver");
     if (D.solver == VVM_SOLVER_SPECTRAL && !Spectral<double>::supports(D.NX))
@@ -3023,7 +3130,6 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         c->staging = c->ar.alloc<double>((size_t)c->d.nx * c->d.nz * 2);
         c->wctl = c->ar.alloc<CGCtl>(1);
         c->d_exec = c->ar.alloc<long long>(1);
-        c->d_err = c->ar.alloc<int>(1);
         for (auto& cs : c->cap) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     } catch (const CudaError& e) {
         cudaSetDevice(prev);
@@ -3054,7 +3160,7 @@ int vvm_gpu_set_stream(vvm_gpu_ctx* ctx, void* stream) {
 int vvm_gpu_synchronize(vvm_gpu_ctx* ctx) {
     return guarded(ctx, [&] {
         CK(cudaStreamSynchronize(ctx->stream));
-        return device_errors(ctx);
+        return VVM_GPU_OK;
     });
 }
 
@@ -3080,6 +3186,7 @@ int vvm_gpu_upload_state(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st) {
         if (rc) return rc;
         CK(cudaStreamSynchronize(ctx->stream));
         ctx->has_state = true;
+        ctx->fut_is_now = false;
         return VVM_GPU_OK;
     });
 }
@@ -3088,8 +3195,7 @@ int vvm_gpu_download_state(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
     if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
     return guarded(ctx, [&] {
         if (int rc = need_state(ctx)) return rc;
-        if (int rc = DISPATCH(ctx, download_state_t)(ctx, st)) return rc;
-        return device_errors(ctx);
+        return DISPATCH(ctx, download_state_t)(ctx, st);
     });
 }
 
@@ -3102,8 +3208,7 @@ int vvm_gpu_download_prognostic(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
     if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
     return guarded(ctx, [&] {
         if (int rc = need_state(ctx)) return rc;
-        if (int rc = DISPATCH(ctx, download_prognostic_t)(ctx, st)) return rc;
-        return device_errors(ctx);
+        return DISPATCH(ctx, download_prognostic_t)(ctx, st);
     });
 }
 
@@ -3124,6 +3229,7 @@ int vvm_gpu_get_step(vvm_gpu_ctx* ctx, int* step) {
         return guarded(ctx, [&]() -> int {                                    \
             if (int rc = need_state(ctx)) return rc;                          \
             if (int rc = need_uniform(ctx)) return rc;                        \
+            ctx->fut_is_now = false;                                          \
             __VA_ARGS__;                                                      \
         });                                                                   \
     }
@@ -3169,14 +3275,26 @@ ROUTINE(vvm_gpu_cal_w, { ctx->last_graph = false; return DISPATCH(ctx, launch_ca
 ROUTINE(vvm_gpu_cal_u, { DISPATCH(ctx, launch_cal_u)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_kessler, { DISPATCH(ctx, launch_kessler)(ctx, false); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_update_mean, { DISPATCH(ctx, launch_update_mean)(ctx, false); return VVM_GPU_OK; })
-ROUTINE(vvm_gpu_turbulence, { DISPATCH(ctx, launch_turbulence)(ctx, false); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_turbulence, { DISPATCH(ctx, launch_turbulence)(ctx, false, nullptr); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_nudge, {
     DISPATCH(ctx, launch_nudge)(ctx, true, ctx->desc.moisture_nudge_time != 0.0);
     return VVM_GPU_OK;
 })
+ROUTINE(vvm_gpu_calpsiuw, { return DISPATCH(ctx, launch_calpsiuw)(ctx); })
+
+int vvm_gpu_download_psi(vvm_gpu_ctx* ctx, double* psi) {
+    return guarded(ctx, [&]() -> int {
+        if (!psi) return fail(ctx, VVM_GPU_EINVAL, "download_psi: NULL argument");
+        if (!ctx->psi) return fail(ctx, VVM_GPU_ESTATE, "download_psi: calpsiuw has not run");
+        download_field<double>(ctx, ctx->psi, 1, 0, psi, false);
+        return VVM_GPU_OK;
+    });
+}
+
 ROUTINE(vvm_gpu_next_step, {
     DISPATCH(ctx, launch_update_mean)(ctx, true);
     ctx->cur = 1 - ctx->cur;
+    ctx->fut_is_now = true;
     return VVM_GPU_OK;
 })
 
@@ -3546,13 +3664,13 @@ int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back) {
     return VVM_GPU_OK;
 }
 
-int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_cluster_ctas, int fft_threads) {
+int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_tile_rows, int fft_threads) {
     if (!ctx) return VVM_GPU_EINVAL;
-    if (gs_cluster_ctas < 0 || gs_cluster_ctas > 8 || fft_threads < 0 || fft_threads > 1024)
+    if ((gs_tile_rows != 0 && !gs_tile_rows_ok(gs_tile_rows)) || fft_threads < 0 || fft_threads > 1024)
         return fail(ctx, VVM_GPU_EINVAL, "set_tuning: knob out of range");
     return guarded(ctx, [&]() -> int {
         CK(cudaStreamSynchronize(ctx->stream));
-        ctx->tune_gs_cs = gs_cluster_ctas;
+        ctx->tune_gs_tr = gs_tile_rows;
         ctx->tune_fft = fft_threads;
         apply_tuning(ctx);
         ctx->drop_graphs();
@@ -3560,10 +3678,9 @@ int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_cluster_ctas, int fft_threads) {
     });
 }
 
-int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_cluster_ctas, int* fft_threads) {
+int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_tile_rows_out, int* fft_threads) {
     if (!ctx) return VVM_GPU_EINVAL;
-    const size_t elem = ctx->mixed ? sizeof(float) : sizeof(double);
-    if (gs_cluster_ctas) *gs_cluster_ctas = gs_plan(ctx->d.pitch, ctx->d.nz, elem, ctx->tune_gs_cs).cs;
+    if (gs_tile_rows_out) *gs_tile_rows_out = gs_tile_rows(ctx);
     if (fft_threads) {
         *fft_threads = 0;
         if (ctx->spectral) {
@@ -3581,6 +3698,9 @@ int vvm_gpu_batch_create(const vvm_gpu_desc* descs, int ncases, int device, vvm_
     std::unique_ptr<vvm_gpu_batch> b(new vvm_gpu_batch());
     b->device = device;
     for (int i = 0; i < ncases; i++) {
+        if (descs[i].flags & VVM_FLAG_STREAMFUNCTION)   // its solve reads its residual on the host
+            return fail(nullptr, VVM_GPU_EINVAL, "batch_create: case " + std::to_string(i) +
+                                                     ": the streamfunction formulation runs single contexts only");
         vvm_gpu_ctx* c = nullptr;
         int rc = vvm_gpu_create(&descs[i], device, &c);
         if (rc != VVM_GPU_OK) {
@@ -3642,7 +3762,6 @@ int vvm_gpu_batch_synchronize(vvm_gpu_batch* b) {
         for (size_t i = 0; i < b->cases.size(); i++) {
             vvm_gpu_ctx* c = b->cases[i];
             CK(cudaStreamSynchronize(c->stream));
-            if (int rc = device_errors(c)) return batch_fail(b, rc, "case " + std::to_string(i) + ": " + c->err);
         }
         return VVM_GPU_OK;
     });

@@ -25,6 +25,7 @@ LIB_PATH = PKG / "lib" / "libvvmgpu.so"
 VVM_PREC_FP64, VVM_PREC_MIXED = 0, 1
 VVM_SOLVER_MGPCG, VVM_SOLVER_LEARNED, VVM_SOLVER_SPECTRAL = 0, 1, 2
 VVM_FLAG_FIXED_FORCING = 1
+VVM_FLAG_STREAMFUNCTION = 2
 STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOCONV", 4: "ESTATE"}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -67,7 +68,7 @@ KERNEL_CLASSES = ("pzeta", "padv", "apply", "pubar", "poisson_rhs", "cg", "mg_sw
                   "mg_coarse", "cal_u", "kessler", "rkm", "gs", "mean", "learned", "conv")
 
 ROUTINES = ("pzeta", "pth", "pqv", "pqc", "pqr", "add_forcing", "halo_all", "pubartop", "cal_w",
-            "cal_u", "kessler", "update_mean", "turbulence", "nudge", "next_step")
+            "cal_u", "kessler", "update_mean", "turbulence", "nudge", "next_step", "calpsiuw")
 
 EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu_set_stream",
            "vvm_gpu_synchronize", "vvm_gpu_last_error", "vvm_gpu_upload_state",
@@ -81,7 +82,8 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_conv3x3_c32", "vvm_gpu_learned_shape", "vvm_gpu_learned_weights",
            "vvm_gpu_learned_eval", "vvm_gpu_learned_train", "vvm_gpu_learned_config",
            "vvm_gpu_learned_last", "vvm_gpu_learned_time", "vvm_gpu_learned_train_rhs",
-           "vvm_gpu_random_perturbation", "vvm_gpu_random_perturbation_host") + tuple(
+           "vvm_gpu_random_perturbation", "vvm_gpu_random_perturbation_host",
+           "vvm_gpu_download_psi") + tuple(
                "vvm_gpu_" + r for r in ROUTINES)
 
 _lib = None
@@ -143,6 +145,7 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_profile.argtypes = [vp, ip]
     L.vvm_gpu_profile_read.argtypes = [vp, ip, _dp, ctypes.POINTER(ctypes.c_longlong)]
     L.vvm_gpu_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.vvm_gpu_download_psi.argtypes = [vp, _dp]
     for r in ROUTINES:
         getattr(L, "vvm_gpu_" + r).argtypes = [vp]
     if path is None:
@@ -194,12 +197,13 @@ class VVMGpu:
 
     def __init__(self, grid, precision: int = VVM_PREC_FP64, solver: int = VVM_SOLVER_MGPCG,
                  poisson_tol: float = 1e-10, warm_start: bool = True, device: int = 0,
-                 addforcingtime: float = 0.0, poisson_maxit: int = 200, fixed_forcing: bool = False):
+                 addforcingtime: float = 0.0, poisson_maxit: int = 200, fixed_forcing: bool = False,
+                 streamfunction: bool = False):
         self.L = load_library()
         self.grid = grid
         self.owned = True
         d = self.make_desc(self.L, grid, precision, solver, poisson_tol, warm_start, addforcingtime,
-                           poisson_maxit, fixed_forcing)
+                           poisson_maxit, fixed_forcing, streamfunction)
         self.desc = d
         h = ctypes.c_void_p()
         rc = self.L.vvm_gpu_create(ctypes.byref(d), int(device), ctypes.byref(h))
@@ -210,10 +214,13 @@ class VVMGpu:
 
     @staticmethod
     def make_desc(L, grid, precision=VVM_PREC_FP64, solver=VVM_SOLVER_MGPCG, poisson_tol=1e-10,
-                  warm_start=True, addforcingtime=0.0, poisson_maxit=200, fixed_forcing=False):
+                  warm_start=True, addforcingtime=0.0, poisson_maxit=200, fixed_forcing=False,
+                  streamfunction=False):
         """vvm_gpu_desc of a grid (reference defaults, then the options).
         fixed_forcing keeps the uploaded init_th_forcing at every forced step
-        instead of regenerating it each step as TimeMarching does."""
+        instead of regenerating it each step as TimeMarching does;
+        streamfunction steps with calpsiuw in place of pubarTop_pt, cal_w and
+        cal_u (the reference's STREAMFUNCTION switch)."""
         d = Desc()
         L.vvm_gpu_desc_default(ctypes.byref(d), grid.NX, grid.NZ, float(grid.dx),
                                     float(grid.dz), float(grid.dt))
@@ -225,7 +232,8 @@ class VVMGpu:
         d.poisson_tol = float(poisson_tol)
         d.poisson_maxit = int(poisson_maxit)
         d.warm_start = 1 if warm_start else 0
-        d.flags = VVM_FLAG_FIXED_FORCING if fixed_forcing else 0
+        d.flags = (VVM_FLAG_FIXED_FORCING if fixed_forcing else 0) | \
+            (VVM_FLAG_STREAMFUNCTION if streamfunction else 0)
         return d
 
     @classmethod
@@ -368,9 +376,16 @@ class VVMGpu:
                 self.call(r)
             if step * self.desc.dt <= self.desc.addforcingtime and not (self.desc.flags & VVM_FLAG_FIXED_FORCING):
                 self.random_perturbation(step)
-            for r in ("add_forcing", "halo_all", "pubartop", "cal_w", "cal_u", "halo_all", "kessler",
+            poisson = ("calpsiuw",) if self.desc.flags & VVM_FLAG_STREAMFUNCTION else ("pubartop", "cal_w", "cal_u")
+            for r in ("add_forcing", "halo_all", *poisson, "halo_all", "kessler",
                       "halo_all", "update_mean", "turbulence", "nudge", "next_step"):
                 self.call(r)
+
+    def download_psi(self) -> np.ndarray:
+        """The streamfunction of the last calpsiuw, [nx][nz] with ghosts."""
+        out = np.empty((self.grid.nx, self.grid.nz))
+        self._check(self.L.vvm_gpu_download_psi(self.h, _ptr(out)))
+        return out
 
     def random_perturbation(self, t: int, min_range: float = -0.001, max_range: float = 0.001,
                             standard_deviation: float = 1.0):
@@ -404,9 +419,9 @@ class VVMGpu:
         self._check(self.L.vvm_gpu_launch_count(self.h, ctypes.byref(n)))
         return n.value
 
-    def set_tuning(self, gs_cluster_ctas: int = 0, fft_threads: int = 0):
+    def set_tuning(self, gs_tile_rows: int = 0, fft_threads: int = 0):
         """Launch-shape knobs (0: automatic); results do not change."""
-        self._check(self.L.vvm_gpu_set_tuning(self.h, int(gs_cluster_ctas), int(fft_threads)))
+        self._check(self.L.vvm_gpu_set_tuning(self.h, int(gs_tile_rows), int(fft_threads)))
 
     def tuning(self) -> tuple[int, int]:
         a, b = ctypes.c_int(), ctypes.c_int()

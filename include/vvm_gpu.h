@@ -80,6 +80,12 @@ typedef struct vvm_gpu_desc {
  * of regenerating it each step the way TimeMarching does
  * (src/Iteration.cpp:276-283; see vvm_gpu_random_perturbation). */
 #define VVM_FLAG_FIXED_FORCING 1
+/* desc.flags: the streamfunction formulation (the reference's STREAMFUNCTION
+ * switch, src/Config.hpp:8, which it ships off and marks as debugging):
+ * vvm_gpu_step calls vvm_gpu_calpsiuw where TimeMarching would call
+ * pubarTop_pt, cal_w and cal_u (src/Iteration.cpp:289-295). Its steps run
+ * the host loop (no CUDA graph); batches refuse it. */
+#define VVM_FLAG_STREAMFUNCTION 2
 
 /* Fills a descriptor with the reference's constants for an NX x NZ grid. */
 void vvm_gpu_desc_default(vvm_gpu_desc* d, int NX, int NZ, double dx, double dz, double dt);
@@ -121,7 +127,11 @@ int vvm_gpu_synchronize(vvm_gpu_ctx* ctx);
 int vvm_gpu_last_error(vvm_gpu_ctx* ctx, char* buf, size_t len);
 
 /* -- state transfer (host [i][k] <-> device [k][i]) -----------------------
- * Replaces Init::Init1d/Init2d as the source of the state (src/Init.cpp:14-266). */
+ * Replaces Init::Init1d/Init2d as the source of the state (src/Init.cpp:14-266).
+ * After a whole step (vvm_gpu_step, or vvm_gpu_next_step) the future arrays
+ * zetap, thp, qvp, qcp, qrp come back equal to the present ones, as the
+ * reference's nextTimeStep leaves them (src/Iteration.cpp:153-204); between
+ * routine calls inside a step they come back as the routines left them. */
 int vvm_gpu_upload_state(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st);
 int vvm_gpu_download_state(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st);
 /* Prognostic fields only (zeta, th, qv, qc, qr, u, w): the per-step traffic
@@ -172,6 +182,18 @@ int vvm_gpu_turbulence(vvm_gpu_ctx* ctx);   /* Turbulence::RKM_RKH, Turbulent.cp
 /* Nudge_theta, Nudge_zeta (case != 2), Nudge_qv (NumericalProcess.cpp:60-96). */
 int vvm_gpu_nudge(vvm_gpu_ctx* ctx);
 int vvm_gpu_next_step(vvm_gpu_ctx* ctx);    /* Iteration::nextTimeStep, Iteration.cpp:153-204 */
+/* PoissonSolver::calpsiuw, PoissonSolver.cpp:124-177 (STREAMFUNCTION): solves
+ * A_psi psi = zetap dx^2 with the matrix of InitPoissonMatrix's
+ * STREAMFUNCTION branch (PoissonSolver.cpp:726-756) to
+ * ||b - A_psi psi|| / ||b|| <= desc.poisson_tol, from zero, then sets psi's
+ * ghosts, u = -d(rhow psi)/dz / rhou and w = d(psi)/dx with the routine's
+ * halos. The reference defines the diagonal shift POISSONPARAM nowhere (a
+ * compile error upstream); this entry takes it as 0, which makes A_psi the
+ * negative of the symmetric w-equation operator. Uniform levels only. */
+int vvm_gpu_calpsiuw(vvm_gpu_ctx* ctx);
+/* The psi field of the last vvm_gpu_calpsiuw, [nx][nz] with ghosts
+ * (model.psi, src/Declare.hpp:584-586); VVM_GPU_ESTATE before the first. */
+int vvm_gpu_download_psi(vvm_gpu_ctx* ctx, double* psi);
 
 /* -- fused path -------------------------------------------------------------
  * nsteps complete steps of TimeMarching's body (step++ first), with fused
@@ -268,12 +290,14 @@ int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back);
 
 /* -- launch-shape knobs --------------------------------------------------------
  * Neither changes any result (the arithmetic of every cell is the same):
- * gs_cluster_ctas caps the CTAs of each Gauss-Seidel cluster (1, 2, 4, 8; the
- * cap never goes below what the row needs), fft_threads sets the threads of a
- * row-FFT block of the spectral solve; 0 selects the automatic value. Setting
- * them drops the context's captured graphs. get returns the values in use. */
-int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_cluster_ctas, int fft_threads);
-int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_cluster_ctas, int* fft_threads);
+ * gs_tile_rows sets the rows of a Gauss-Seidel tile (4, 8, 16, 32; each tile
+ * is 128 columns and one warp, and the passes run to the same fixed point
+ * whatever its height), fft_threads sets the threads of a row-FFT block of
+ * the spectral solve; 0 selects the automatic value (8 rows; 512 threads or
+ * half the row). Setting them drops the context's captured graphs. get
+ * returns the values in use. */
+int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_tile_rows, int fft_threads);
+int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_tile_rows, int* fft_threads);
 
 /* -- batches of independent cases ------------------------------------------------
  * The reference runs one case per process. A batch holds many cases of any

@@ -5,8 +5,18 @@
 * ``RefTropicalModel`` -- oracle/_ref/libvvmref_tropical.so: the same sources
   built with the reference's sounding file and Q1/Q2 forcing switched on
   (oracle/ref_config_tropical.hpp), for the initial state read from it.
+* ``RefStreamModel`` -- oracle/_ref/libvvmref_stream.so: the same sources
+  built with the streamfunction formulation (STREAMFUNCTION) switched on
+  (oracle/ref_config_stream.hpp), for calpsiuw.
+* ``RefDropinModel`` -- oracle/_ref/libvvmref_dropin.so: the reference model
+  as a maintainer builds it with GPU_STEP, TimeMarching taken from the
+  committed binding 2d-vector-vorticity-model_b200/integration/
+  Iteration_GPU.cpp (the B200 step through libvvmgpu.so). Not an oracle: the
+  thing the tests check against RefModel.
 * ``PortModel`` -- oracle/_build/libvvmoracle.so: the C restatement in
   oracle/vvm_oracle.c (exact elliptic solves).
+* ``PortMTModel`` -- oracle/_build/libvvmoracle_mt.so: the same source built
+  with OpenMP and FFT-based cal_w, the race-free multi-core CPU baseline.
 
 Test infrastructure only: used by tests/, the fixture generator under
 tests/golden/, __graft_entry__.smoke() and bench.py's CPU-baseline leg. Arrays
@@ -22,7 +32,10 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libvvmref.so"
 REF_TROPICAL_LIB = HERE / "_ref" / "libvvmref_tropical.so"
+REF_STREAM_LIB = HERE / "_ref" / "libvvmref_stream.so"
+REF_DROPIN_LIB = HERE / "_ref" / "libvvmref_dropin.so"
 PORT_LIB = HERE / "_build" / "libvvmoracle.so"
+PORT_MT_LIB = HERE / "_build" / "libvvmoracle_mt.so"
 
 HIST_NAMES = ("dzeta_advect", "dth_buoyancy", "dth_advect", "dqv_advect", "dqc_advect",
               "dqr_advect", "dqr_VT")
@@ -67,8 +80,20 @@ def ref_tropical_available() -> bool:
     return REF_TROPICAL_LIB.exists()
 
 
+def ref_stream_available() -> bool:
+    return REF_STREAM_LIB.exists()
+
+
+def ref_dropin_available() -> bool:
+    return REF_DROPIN_LIB.exists()
+
+
 def port_available() -> bool:
     return PORT_LIB.exists()
+
+
+def port_mt_available() -> bool:
+    return PORT_MT_LIB.exists()
 
 
 def _view(ptr, shape):
@@ -265,6 +290,24 @@ class RefTropicalModel(RefModel):
         self._after_load()   # the cal_w matrix, as after load()
 
 
+class RefStreamModel(RefModel):
+    """The reference built with STREAMFUNCTION (POISSONPARAM = 0): its one_step
+    calls calpsiuw in place of pubarTop_pt + cal_w + cal_u
+    (src/Iteration.cpp:289-295), and apply_A is the psi matrix
+    (src/PoissonSolver.cpp:726-756)."""
+    path = REF_STREAM_LIB
+
+    def psi(self) -> np.ndarray:
+        return self.field("psi")
+
+
+class RefDropinModel(RefModel):
+    """The reference model whose TimeMarching is the GPU_STEP binding: its
+    time_marching(n) runs n steps on the GPU through the C ABI, exactly as a
+    maintainer's GPU_STEP build would."""
+    path = REF_DROPIN_LIB
+
+
 class PortModel(_CModel):
     """The C restatement (oracle/vvm_oracle.c)."""
     prefix = "orc_"
@@ -281,6 +324,20 @@ class PortModel(_CModel):
         return L.orc_create(g.NX, g.NZ, float(g.dx), float(g.dz), float(g.dt), int(g.case),
                             float(g.moisture_nudge_time), float(self._aft))
 
+    def set_streamfunction(self, on: bool = True):
+        """one_step calls calpsiuw in place of pubarTop_pt + cal_w + cal_u."""
+        self.L.orc_set_streamfunction.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        self.L.orc_set_streamfunction(self.h, int(bool(on)))
+
+    def apply_psi(self, x: np.ndarray) -> np.ndarray:
+        """y = A_psi x, the streamfunction matrix (src/PoissonSolver.cpp:726-756)."""
+        self.L.orc_apply_psi.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_double)]
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        self.L.orc_apply_psi(self.h, _dptr(x), _dptr(y))
+        return y
+
     def solve_A(self, b: np.ndarray) -> np.ndarray:
         self.L.orc_solve_A.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double)]
@@ -288,3 +345,15 @@ class PortModel(_CModel):
         x = np.empty_like(b)
         self.L.orc_solve_A(self.h, _dptr(b), _dptr(x))
         return x
+
+
+class PortMTModel(PortModel):
+    """The C restatement built with OpenMP (rows split across threads, the
+    five Gauss-Seidel sweeps concurrent, per-thread domain sums) and radix-2
+    FFTs in cal_w: the race-free multi-core CPU baseline. Its results equal
+    the serial restatement's to round-off (sum order and transform)."""
+    path = PORT_MT_LIB
+
+    def threads(self) -> int:
+        self.L.orc_threads.restype = ctypes.c_int
+        return int(self.L.orc_threads())

@@ -68,9 +68,13 @@ void one_step(vvm& model) {
     model.AddForcing(model);
     vvm::BoundaryProcess2D_all(model);
 
+#if defined(STREAMFUNCTION)
+    vvm::PoissonSolver::calpsiuw(model);
+#else
     vvm::PoissonSolver::pubarTop_pt(model);
     vvm::PoissonSolver::cal_w(model);
     vvm::PoissonSolver::cal_u(model);
+#endif
     vvm::BoundaryProcess2D_all(model);
 
     vvm::MicroPhysics::autoconversion(model);
@@ -135,6 +139,9 @@ double* ref_field(void* h, const char* name) {
         {"init_th_forcing", m.init_th_forcingcont},
         {"evaporation", m.evaporationcont}, {"accretion", m.accretioncont},
         {"autoconversion", m.autoconversioncont}, {"condensation", m.condensationcont},
+#if defined(STREAMFUNCTION)
+        {"psi", m.psi[0]},
+#endif
     };
     for (auto& e : tab) if (std::strcmp(e.n, name) == 0) return e.p;
     return nullptr;
@@ -203,9 +210,13 @@ int ref_call(void* h, const char* name) {
     else if (n == "Advection_qrVT") vvm::Advection_qrVT(m);
     else if (n == "AddForcing") m.AddForcing(m);
     else if (n == "BoundaryProcess2D_all") vvm::BoundaryProcess2D_all(m);
+#if defined(STREAMFUNCTION)
+    else if (n == "calpsiuw") vvm::PoissonSolver::calpsiuw(m);
+#else
     else if (n == "pubarTop_pt") vvm::PoissonSolver::pubarTop_pt(m);
     else if (n == "cal_w") vvm::PoissonSolver::cal_w(m);
     else if (n == "cal_u") vvm::PoissonSolver::cal_u(m);
+#endif
     else if (n == "autoconversion") vvm::MicroPhysics::autoconversion(m);
     else if (n == "accretion") vvm::MicroPhysics::accretion(m);
     else if (n == "evaporation") vvm::MicroPhysics::evaporation(m);

@@ -9,19 +9,36 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* The threaded CPU baseline (Makefile target _build/libvvmoracle_mt.so) is
+ * this file built with -fopenmp -DORC_FAST_SOLVE: loops over rows split
+ * across threads (every temporary is local to its iteration, so no thread
+ * writes what another reads), the five Gauss-Seidel sweeps run concurrently
+ * (each is serial within its field, as the reference's in-place update
+ * requires), domain sums reduce per thread, and cal_w's Fourier transforms
+ * are radix-2 FFTs when NX is a power of two. The serial build (the checker
+ * pinned to the reference) compiles none of that: ORC_PAR is empty there. */
+#ifdef _OPENMP
+#define ORC_PAR _Pragma("omp parallel for schedule(static)")
+#else
+#define ORC_PAR
+#endif
 
 #define F2(a, i, k) ((a)[(size_t)(i) * m->nz + (k)])
 #define H3(a, i, k, s) ((a)[((size_t)(i) * m->nz + (k)) * 2 + (s)])
 
 struct orc_model {
-    int nx, nz, step, CASE, status_for_adding_forcing;
+    int nx, nz, step, CASE, status_for_adding_forcing, streamfunction;
     double dx, dz, dt, d2t, rdx, r2dx, rdz, r2dz, rdx2, rdz2;
     double GRAVITY, Cp, Cv, Rd, Lv, P0, PSURF, CRAD, addforcingtime, moisture_nudge_time;
     double ubarTopp, ubarTop, ubarTopm, dubarTop_advect[2];
     /* 2D */
     double *zeta, *zetam, *zetap, *th, *thm, *thp, *u, *w, *qv, *qvm, *qvp, *qc, *qcm, *qcp;
     double *qr, *qrm, *qrp, *RKM, *RKH, *U_w, *W_u, *init_th_forcing;
-    double *evaporation, *accretion, *autoconversion, *condensation;
+    double *evaporation, *accretion, *autoconversion, *condensation, *psi;
     /* AB2 */
     double *dth_advect, *dth_buoyancy, *dzeta_advect, *dqv_advect, *dqc_advect, *dqr_advect, *dqr_VT;
     /* 1D */
@@ -51,7 +68,7 @@ orc_model* orc_create(int NX, int NZ, double dx, double dz, double dt, int CASE,
                       &m->qv, &m->qvm, &m->qvp, &m->qc, &m->qcm, &m->qcp, &m->qr, &m->qrm,
                       &m->qrp, &m->RKM, &m->RKH, &m->U_w, &m->W_u, &m->init_th_forcing,
                       &m->evaporation, &m->accretion, &m->autoconversion, &m->condensation,
-                      &m->flux_u, &m->flux_w};
+                      &m->flux_u, &m->flux_w, &m->psi};
     for (size_t j = 0; j < sizeof(two) / sizeof(two[0]); j++) *two[j] = alloc0(n2);
     double** hist[] = {&m->dth_advect, &m->dth_buoyancy, &m->dzeta_advect, &m->dqv_advect,
                        &m->dqc_advect, &m->dqr_advect, &m->dqr_VT};
@@ -74,7 +91,7 @@ void orc_destroy(orc_model* m) {
                      m->dth_buoyancy, m->dzeta_advect, m->dqv_advect, m->dqc_advect,
                      m->dqr_advect, m->dqr_VT, m->thb, m->thbm, m->thb_zeta, m->thb_init,
                      m->rhou, m->rhow, m->pib, m->qvb, m->qvb0, m->pb, m->thvb, m->thvbm, m->z,
-                     m->z_zeta, m->lambda2, m->Q1LS, m->Q2LS, m->xi, m->uxi, m->precip, m->work};
+                     m->z_zeta, m->lambda2, m->Q1LS, m->Q2LS, m->xi, m->uxi, m->precip, m->work, m->psi};
     for (size_t j = 0; j < sizeof(all) / sizeof(all[0]); j++) free(all[j]);
     free(m);
 }
@@ -89,7 +106,7 @@ double* orc_field(orc_model* m, const char* n) {
         {"qr", m->qr}, {"qrm", m->qrm}, {"qrp", m->qrp}, {"RKM", m->RKM}, {"RKH", m->RKH},
         {"U_w", m->U_w}, {"W_u", m->W_u}, {"init_th_forcing", m->init_th_forcing},
         {"evaporation", m->evaporation}, {"accretion", m->accretion},
-        {"autoconversion", m->autoconversion}, {"condensation", m->condensation}};
+        {"autoconversion", m->autoconversion}, {"condensation", m->condensation}, {"psi", m->psi}};
     for (size_t j = 0; j < sizeof(t) / sizeof(t[0]); j++) if (!strcmp(t[j].n, n)) return t[j].p;
     return NULL;
 }
@@ -174,6 +191,7 @@ static void advect_scalar(orc_model* m, const double* now, double* future, doubl
     double *fu = m->flux_u, *fw = m->flux_w, *u = m->u, *w = m->w, *rhou = m->rhou, *rhow = m->rhow;
     memset(fu, 0, sizeof(double) * nx * nz);
     memset(fw, 0, sizeof(double) * nx * nz);
+    ORC_PAR
     for (int k = 1; k <= nz - 1; k++) {
         for (int i = 1; i <= nx - 1; i++) {
             F2(fu, i, k) = rhou[k] * F2(u, i, k) * (F2(now, i, k) + F2(now, i - 1, k));
@@ -196,6 +214,7 @@ static void advect_scalar(orc_model* m, const double* now, double* future, doubl
     bc2d_center(m, fw);
     for (int i = 0; i < nx; i++) { F2(fw, i, 0) = 0.; F2(fw, i, nz - 1) = 0.; }
     int sn = (m->step + 1) % 2, so = m->step % 2;
+    ORC_PAR
     for (int k = 1; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
             double px = (F2(fu, i + 1, k) - F2(fu, i, k)) * m->r2dx / rhou[k];
@@ -212,6 +231,7 @@ static void advect_zeta(orc_model* m) {
     int nx = m->nx, nz = m->nz;
     double *Uw = m->U_w, *Wu = m->W_u, *u = m->u, *w = m->w, *z = m->zeta;
     double *rhou = m->rhou, *rhow = m->rhow, *fu = m->flux_u, *fw = m->flux_w;
+    ORC_PAR
     for (int k = 1; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
             F2(Uw, i, k) = 0.25 * (rhou[k] * (F2(u, i + 1, k) + F2(u, i, k)) + rhou[k - 1] * (F2(u, i + 1, k - 1) + F2(u, i, k - 1)));
@@ -223,6 +243,7 @@ static void advect_zeta(orc_model* m) {
     for (int i = 0; i < nx; i++) { F2(Wu, i, 0) = 0.; F2(Wu, i, nz - 1) = 0.; }
     memset(fu, 0, sizeof(double) * nx * nz);
     memset(fw, 0, sizeof(double) * nx * nz);
+    ORC_PAR
     for (int k = 1; k <= nz - 2; k++) {
         for (int i = 0; i <= nx - 2; i++) {
             F2(fu, i, k) = F2(Uw, i, k) * (F2(z, i + 1, k) + F2(z, i, k));
@@ -243,6 +264,7 @@ static void advect_zeta(orc_model* m) {
     bc2d_center(m, fw);
     for (int i = 0; i < nx; i++) { F2(fw, i, 0) = 0.; F2(fw, i, nz - 1) = 0.; }
     int sn = (m->step + 1) % 2, so = m->step % 2;
+    ORC_PAR
     for (int k = 2; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
             double px = (F2(fu, i, k) - F2(fu, i - 1, k)) * m->r2dx / rhow[k];
@@ -259,6 +281,7 @@ static void advect_qr_vt(orc_model* m) {
     int nx = m->nx, nz = m->nz;
     double *fw = m->flux_w, *qr = m->qr, *rhow = m->rhow, *rhou = m->rhou;
     memset(fw, 0, sizeof(double) * nx * nz);
+    ORC_PAR
     for (int k = 1; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
             double VT = 1E-2 * (3634 * pow(1E-3 * rhow[k] * 0.5 * (F2(qr, i, k) + F2(qr, i, k - 1)), 0.1346) * pow(rhow[k] / rhow[1], -0.5));
@@ -268,6 +291,7 @@ static void advect_qr_vt(orc_model* m) {
     bc2d_center(m, fw);
     for (int i = 0; i < nx; i++) { F2(fw, i, 0) = 0.; F2(fw, i, nz - 1) = 0.; }
     int sn = (m->step + 1) % 2, so = m->step % 2;
+    ORC_PAR
     for (int k = 1; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
             double p = (F2(fw, i, k + 1) - F2(fw, i, k)) * m->r2dz / rhou[k];
@@ -288,6 +312,7 @@ static double thv(orc_model* m, int i, int k) {  /* src/Buoyancy.cpp:3-9 */
 static void buoyancy(orc_model* m) {
     int nx = m->nx, nz = m->nz, sn = (m->step + 1) % 2, so = m->step % 2;
     double *rhow = m->rhow, *thvb = m->thvb, *qc = m->qc, *qr = m->qr, g = m->GRAVITY;
+    ORC_PAR
     for (int k = 2; k < nz - 1; k++) {
         for (int i = 1; i < nx - 1; i++) {
             double b = g / rhow[k] * 0.5 * ((thv(m, i, k) - thv(m, i - 1, k)) / thvb[k] + (thv(m, i, k - 1) - thv(m, i - 1, k - 1)) / thvb[k - 1]) * m->rdx;
@@ -309,6 +334,9 @@ static void buoyancy(orc_model* m) {
 static void negative_value_process(orc_model* m, double* v) {
     int nx = m->nx, nz = m->nz;
     double pos = 0., neg = 0.;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) reduction(+ : pos, neg)
+#endif
     for (int k = 1; k <= nz - 2; k++)
         for (int i = 1; i <= nx - 2; i++) {
             if (F2(v, i, k) >= 0.) pos += F2(v, i, k);
@@ -316,6 +344,7 @@ static void negative_value_process(orc_model* m, double* v) {
         }
     if (pos == 0. || fabs(neg) > pos) return;
     double ratio = 1. - fabs(neg / pos);
+    ORC_PAR
     for (int k = 1; k <= nz - 2; k++)
         for (int i = 1; i <= nx - 2; i++)
             if (F2(v, i, k) > 0) F2(v, i, k) = F2(v, i, k) * ratio;
@@ -324,6 +353,7 @@ static void negative_value_process(orc_model* m, double* v) {
 /* src/MicroPhysics.cpp:29-51 */
 static void autoconversion(orc_model* m) {
     double autort = 0.001, autotr = 0.001;
+    ORC_PAR
     for (int k = 1; k <= m->nz - 2; k++)
         for (int i = 1; i <= m->nx - 2; i++) {
             double qcplus = maxd(0., F2(m->qcp, i, k));
@@ -339,6 +369,7 @@ static void autoconversion(orc_model* m) {
 /* src/MicroPhysics.cpp:54-77 */
 static void accretion(orc_model* m) {
     double accrrt = 2.2;
+    ORC_PAR
     for (int k = 1; k <= m->nz - 2; k++)
         for (int i = 1; i <= m->nx - 2; i++) {
             double qcplus = maxd(0., F2(m->qcp, i, k));
@@ -353,6 +384,7 @@ static void accretion(orc_model* m) {
 
 /* src/MicroPhysics.cpp:80-114 */
 static void evaporation(orc_model* m) {
+    ORC_PAR
     for (int k = 1; k <= m->nz - 2; k++) {
         double pc = 380. / (pow(m->pib[k], m->Cp / m->Rd) * m->P0);
         for (int i = 1; i <= m->nx - 2; i++) {
@@ -373,6 +405,7 @@ static void evaporation(orc_model* m) {
 
 /* Saturation adjustment (src/MicroPhysics.cpp:7-26). */
 static void condensation(orc_model* m) {
+    ORC_PAR
     for (int k = 1; k <= m->nz - 2; k++) {
         double pc = 380. / (pow(m->pib[k], m->Cp / m->Rd) * m->P0);
         for (int i = 1; i <= m->nx - 2; i++) {
@@ -402,6 +435,7 @@ static void precip_diag(orc_model* m) {
  * that are zero unless a caller sets them; the random th forcing is added
  * while status_for_adding_forcing holds. */
 static void add_forcing(orc_model* m) {
+    ORC_PAR
     for (int k = 1; k <= m->nz - 2; k++)
         for (int i = 1; i <= m->nx - 2; i++) {
             double dt = m->dt;
@@ -420,8 +454,111 @@ static void add_forcing(orc_model* m) {
  * periodic in i, x = 0 beyond k = 2 and k = nz-2. A real DFT in i turns the
  * x-part of mode p into -4 sin^2(pi p / NX); each mode then needs one
  * tridiagonal solve in k. */
+/* Row (kk, j) of a separable operator with level coefficients cx, ru, rd:
+ *   cx[kk] (x[j-1] + x[j+1] - 2 x) + ru[kk] (x[kk+1] - x) + rd[kk] (x[kk-1] - x) = b,
+ * periodic in j, x = 0 beyond the first and last rows; solved exactly. */
+static void solve_separable(int NX, int NK, const double* cxk, const double* ruk, const double* rdk,
+                            const double* b, double* x);
+
 void orc_solve_A(orc_model* m, const double* b, double* x) {
-    int NX = m->nx - 2, NK = m->nz - 3;
+    int NK = m->nz - 3;
+    double* cf = (double*)malloc(sizeof(double) * 3 * NK);
+    for (int kk = 0; kk < NK; kk++) {
+        int k = kk + 2;
+        cf[kk] = 1.0;
+        cf[NK + kk] = m->rhow[k] / m->rhou[k];
+        cf[2 * NK + kk] = m->rhow[k] / m->rhou[k - 1];
+    }
+    solve_separable(m->nx - 2, NK, cf, cf + NK, cf + 2 * NK, b, x);
+    free(cf);
+}
+
+#ifdef ORC_FAST_SOLVE
+/* In-place iterative radix-2 FFT of n = 2^q complex values (Cooley-Tukey,
+ * decimation in time): bit-reversal permutation, then log2(n) butterfly
+ * stages; sign -1 forward, +1 backward (unscaled). Twiddles come from a
+ * table of cos / sin(2 pi j / n), j < n/2. */
+static void fft_radix2(double* re, double* im, int n, const double* tc, const double* ts, int sign) {
+    for (int i = 1, j = 0; i < n; i++) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            double t = re[i]; re[i] = re[j]; re[j] = t;
+            t = im[i]; im[i] = im[j]; im[j] = t;
+        }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        const int half = len >> 1, stride = n / len;
+        for (int i = 0; i < n; i += len)
+            for (int k = 0; k < half; k++) {
+                const double wr = tc[k * stride], wi = sign * ts[k * stride];
+                const int a = i + k, b = a + half;
+                const double vr = re[b] * wr - im[b] * wi, vi = re[b] * wi + im[b] * wr;
+                re[b] = re[a] - vr; im[b] = im[a] - vi;
+                re[a] += vr; im[a] += vi;
+            }
+    }
+}
+
+/* solve_separable for NX a power of two: FFT each row, one real tridiagonal
+ * solve per mode applied to the real and imaginary parts, inverse FFT. */
+static void solve_separable_fft(int NX, int NK, const double* cxk, const double* ruk, const double* rdk,
+                                const double* b, double* x) {
+    const double twopi = 6.283185307179586476925286766559;
+    double* tc = (double*)malloc(sizeof(double) * (NX / 2 + 1));
+    double* ts = (double*)malloc(sizeof(double) * (NX / 2 + 1));
+    for (int j = 0; j < NX / 2; j++) { tc[j] = cos(twopi * j / NX); ts[j] = sin(twopi * j / NX); }
+    double* hr = (double*)malloc(sizeof(double) * (size_t)NX * NK);
+    double* hi = (double*)malloc(sizeof(double) * (size_t)NX * NK);
+    ORC_PAR
+    for (int kk = 0; kk < NK; kk++) {
+        double* r = hr + (size_t)kk * NX;
+        double* q = hi + (size_t)kk * NX;
+        for (int j = 0; j < NX; j++) { r[j] = b[(size_t)kk * NX + j]; q[j] = 0.; }
+        fft_radix2(r, q, NX, tc, ts, -1);
+    }
+    ORC_PAR
+    for (int p = 0; p < NX; p++) {
+        double* cp = (double*)malloc(sizeof(double) * NK);
+        const int pm = p <= NX / 2 ? p : NX - p;
+        const double lam = -4.0 * pow(sin(3.14159265358979323846264338327950 * pm / NX), 2);
+        double den0 = cxk[0] * lam - (ruk[0] + rdk[0]);
+        cp[0] = (NK > 1 ? ruk[0] : 0.) / den0;
+        hr[p] /= den0;
+        hi[p] /= den0;
+        for (int kk = 1; kk < NK; kk++) {
+            const double up = kk < NK - 1 ? ruk[kk] : 0., lw = rdk[kk];
+            const double den = cxk[kk] * lam - (ruk[kk] + rdk[kk]) - lw * cp[kk - 1];
+            cp[kk] = up / den;
+            hr[(size_t)kk * NX + p] = (hr[(size_t)kk * NX + p] - lw * hr[(size_t)(kk - 1) * NX + p]) / den;
+            hi[(size_t)kk * NX + p] = (hi[(size_t)kk * NX + p] - lw * hi[(size_t)(kk - 1) * NX + p]) / den;
+        }
+        for (int kk = NK - 2; kk >= 0; kk--) {
+            hr[(size_t)kk * NX + p] -= cp[kk] * hr[(size_t)(kk + 1) * NX + p];
+            hi[(size_t)kk * NX + p] -= cp[kk] * hi[(size_t)(kk + 1) * NX + p];
+        }
+        free(cp);
+    }
+    ORC_PAR
+    for (int kk = 0; kk < NK; kk++) {
+        double* r = hr + (size_t)kk * NX;
+        double* q = hi + (size_t)kk * NX;
+        fft_radix2(r, q, NX, tc, ts, +1);
+        for (int j = 0; j < NX; j++) x[(size_t)kk * NX + j] = r[j] / NX;
+    }
+    free(tc); free(ts); free(hr); free(hi);
+}
+#endif
+
+static void solve_separable(int NX, int NK, const double* cxk, const double* ruk, const double* rdk,
+                            const double* b, double* x) {
+#ifdef ORC_FAST_SOLVE
+    if (NX >= 2 && (NX & (NX - 1)) == 0) {
+        solve_separable_fft(NX, NK, cxk, ruk, rdk, b, x);
+        return;
+    }
+#endif
     double* c = (double*)malloc(sizeof(double) * NX);
     double* s = (double*)malloc(sizeof(double) * NX);
     double* hat = (double*)calloc((size_t)NX * NK, sizeof(double));
@@ -451,9 +588,8 @@ void orc_solve_A(orc_model* m, const double* b, double* x) {
         int p = col <= P ? col : NX - col;
         double lam = -4.0 * pow(sin(3.14159265358979323846264338327950 * p / NX), 2);
         for (int kk = 0; kk < NK; kk++) {
-            int k = kk + 2;
-            double ru = m->rhow[k] / m->rhou[k], rd = m->rhow[k] / m->rhou[k - 1];
-            di[kk] = lam - (ru + rd);
+            double ru = ruk[kk], rd = rdk[kk];
+            di[kk] = cxk[kk] * lam - (ru + rd);
             up[kk] = kk < NK - 1 ? ru : 0.;
             lo[kk] = kk > 0 ? rd : 0.;
         }
@@ -514,6 +650,83 @@ static void cal_w(orc_model* m) {
         for (int i = 1; i <= nx - 2; i++) F2(m->w, i, k) = x[cnt++] / m->rhow[k];
     (void)NX;
     bc2d_westdown(m, m->w);
+}
+
+/* The streamfunction formulation (STREAMFUNCTION), which the reference ships
+ * switched off and unfinished (src/Config.hpp:8). Its matrix
+ * (src/PoissonSolver.cpp:726-756), row (k, i), k = 2..nz-2, i = 1..nx-2:
+ *   (x[i-1] + x[i+1]) / rhow_k + x[k+1] / rhou_k + x[k-1] / rhou_{k-1}
+ *     - (2 / rhow_k + 1 / rhou_k + 1 / rhou_{k-1} - POISSONPARAM) x = b,
+ * periodic in i, with POISSONPARAM = 0 (the reference defines it nowhere). */
+void orc_apply_psi(orc_model* m, const double* x, double* y) {
+    int NX = m->nx - 2, NK = m->nz - 3;
+    for (int kk = 0; kk < NK; kk++) {
+        int k = kk + 2;
+        double cx = 1. / m->rhow[k], ru = 1. / m->rhou[k], rd = 1. / m->rhou[k - 1];
+        for (int j = 0; j < NX; j++) {
+            double xc = x[(size_t)kk * NX + j];
+            double v = -(2. * cx + ru + rd) * xc
+                       + cx * (x[(size_t)kk * NX + (j + NX - 1) % NX] + x[(size_t)kk * NX + (j + 1) % NX]);
+            if (kk + 1 < NK) v += ru * x[(size_t)(kk + 1) * NX + j];
+            if (kk > 0) v += rd * x[(size_t)(kk - 1) * NX + j];
+            y[(size_t)kk * NX + j] = v;
+        }
+    }
+}
+
+void orc_solve_psi(orc_model* m, const double* b, double* x) {
+    int NK = m->nz - 3;
+    double* cf = (double*)malloc(sizeof(double) * 3 * NK);
+    for (int kk = 0; kk < NK; kk++) {
+        int k = kk + 2;
+        cf[kk] = 1. / m->rhow[k];
+        cf[NK + kk] = 1. / m->rhou[k];
+        cf[2 * NK + kk] = 1. / m->rhou[k - 1];
+    }
+    solve_separable(m->nx - 2, NK, cf, cf + NK, cf + 2 * NK, b, x);
+    free(cf);
+}
+
+/* src/PoissonSolver.cpp:124-177 (Eigen branch) with an exact solve: psi from
+ * zeta (b = zetap dx^2), its ghosts, then u and w from psi. The routine's
+ * w-zeroing loop runs over i < nz (line 172), which the westdown halo that
+ * follows makes immaterial: w = 0 at k = 0, 1, nz-1 for every i. */
+static void calpsiuw(orc_model* m) {
+    int nx = m->nx, nz = m->nz;
+    double* b = m->work;
+    double* x = m->work + (size_t)nx * nz;
+    int cnt = 0;
+    for (int k = 2; k <= nz - 2; k++)
+        for (int i = 1; i <= nx - 2; i++) b[cnt++] = F2(m->zetap, i, k) * m->dx * m->dx;
+    orc_solve_psi(m, b, x);
+    cnt = 0;
+    for (int k = 2; k <= nz - 2; k++)
+        for (int i = 1; i <= nx - 2; i++) F2(m->psi, i, k) = x[cnt++];
+    for (int k = 2; k <= nz - 2; k++) {
+        F2(m->psi, 0, k) = F2(m->psi, nx - 2, k);
+        F2(m->psi, nx - 1, k) = F2(m->psi, 1, k);
+    }
+    for (int i = 0; i <= nx - 1; i++) F2(m->psi, i, 0) = F2(m->psi, i, 1) = F2(m->psi, i, nz - 1) = 0.;
+    bc2d_westdown(m, m->psi);
+    for (int i = 1; i <= nx - 2; i++) {
+        for (int k = 1; k <= nz - 2; k++) {
+            F2(m->u, i, k) = -(m->rhow[k + 1] * F2(m->psi, i, k + 1) - m->rhow[k] * F2(m->psi, i, k)) * m->rdz / m->rhou[k];
+            F2(m->w, i, k) = (F2(m->psi, i + 1, k) - F2(m->psi, i, k)) * m->rdx;
+        }
+    }
+    for (int i = 0; i < nz && i < nx; i++) F2(m->w, i, nz - 1) = F2(m->w, i, 0) = F2(m->w, i, 1) = 0.;
+    bc2d_center(m, m->u);
+    bc2d_westdown(m, m->w);
+}
+
+void orc_set_streamfunction(orc_model* m, int on) { m->streamfunction = on; }
+
+int orc_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
 }
 
 /* src/PoissonSolver.cpp:580-653 (Eigen branch). The chi problem
@@ -613,6 +826,7 @@ static void hparam(orc_model* m, double* v) {
 static void rkm_rkh(orc_model* m) {
     int nx = m->nx, nz = m->nz;
     double *u = m->u, *w = m->w, *thp = m->thp;
+    ORC_PAR
     for (int k = 1; k <= nz - 2; k++)
         for (int i = 1; i <= nx - 2; i++) {
             double Rzeta = 0.5 * ((F2(w, i + 1, k + 1) + F2(w, i + 1, k)) - (F2(w, i - 1, k + 1) + F2(w, i - 1, k))) * m->r2dx +
@@ -639,11 +853,20 @@ static void rkm_rkh(orc_model* m) {
         }
     bc2d_center(m, m->RKM);
     bc2d_center(m, m->RKH);
+#ifdef _OPENMP
+    /* five independent in-place sweeps: one field a thread */
+#pragma omp parallel for schedule(static, 1)
+    for (int f = 0; f < 5; f++) {
+        if (f == 0) mparam(m, m->zetap);
+        else hparam(m, f == 1 ? m->thp : f == 2 ? m->qvp : f == 3 ? m->qcp : m->qrp);
+    }
+#else
     mparam(m, m->zetap);
     hparam(m, m->thp);
     hparam(m, m->qvp);
     hparam(m, m->qcp);
     hparam(m, m->qrp);
+#endif
 }
 
 /* ---------------------------------------------------------------- nudge */
@@ -677,6 +900,7 @@ static void nudge_qv(orc_model* m) {  /* src/NumericalProcess.cpp:87-96 */
 static void update_mean(orc_model* m) {
     int nx = m->nx, nz = m->nz;
     for (int k = 0; k < nz; k++) { m->thbm[k] = m->thb[k]; m->thvbm[k] = m->thvb[k]; }
+    ORC_PAR
     for (int k = 1; k < nz - 1; k++) {
         double tb = 0., qb = 0.;
         for (int i = 1; i < nx - 1; i++) { tb += F2(m->thp, i, k); qb += F2(m->qvp, i, k); }
@@ -719,7 +943,8 @@ static void one_step(orc_model* m) {
     m->status_for_adding_forcing = (m->step * m->dt <= m->addforcingtime);
     add_forcing(m);
     bc_all(m);
-    pubar_top(m); cal_w(m); cal_u(m);
+    if (m->streamfunction) calpsiuw(m);   /* src/Iteration.cpp:289-295 */
+    else { pubar_top(m); cal_w(m); cal_u(m); }
     bc_all(m);
     autoconversion(m); accretion(m); evaporation(m); condensation(m);
     negative_value_process(m, m->qvp);
@@ -749,6 +974,7 @@ int orc_call(orc_model* m, const char* n) {
     else if (!strcmp(n, "pubarTop_pt")) pubar_top(m);
     else if (!strcmp(n, "cal_w")) cal_w(m);
     else if (!strcmp(n, "cal_u")) cal_u(m);
+    else if (!strcmp(n, "calpsiuw")) calpsiuw(m);
     else if (!strcmp(n, "autoconversion")) autoconversion(m);
     else if (!strcmp(n, "accretion")) accretion(m);
     else if (!strcmp(n, "evaporation")) evaporation(m);

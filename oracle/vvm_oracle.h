@@ -44,6 +44,16 @@ int orc_call(orc_model* m, const char* name);
  * unknown index (k-2)*(nx-2) + (i-1). */
 void orc_solve_A(orc_model* m, const double* b, double* x);
 void orc_apply_A(orc_model* m, const double* x, double* y);
+/* The streamfunction formulation (STREAMFUNCTION, src/PoissonSolver.cpp:14-177,
+ * matrix 726-756 with POISSONPARAM = 0): y = A_psi x, x = A_psi^{-1} b exactly,
+ * and the switch that makes "one_step" call calpsiuw in place of
+ * pubarTop_pt + cal_w + cal_u (src/Iteration.cpp:289-295). */
+void orc_apply_psi(orc_model* m, const double* x, double* y);
+void orc_solve_psi(orc_model* m, const double* b, double* x);
+void orc_set_streamfunction(orc_model* m, int on);
+/* Threads the library runs its loops on: 1 for the serial checker, the
+ * OpenMP team size for the threaded CPU baseline (libvvmoracle_mt.so). */
+int orc_threads(void);
 
 #ifdef __cplusplus
 }

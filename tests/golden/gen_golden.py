@@ -17,6 +17,14 @@ Fixtures (all float64, numpy .npz, reference [nx][nz] layout):
                        matrix (the reference's own POISSONTEST idea,
                        src/PoissonSolver.cpp:815-828): b = A x, the reference's
                        BiCGSTAB solution and its true residual
+  halo_kat.npz         BoundaryProcess2D_all (src/Boundary.cpp:36-58) on the
+                       34x18 routine state with every ghost cell of the fields
+                       it touches overwritten by seeded noise first
+  stream_kat.npz       the streamfunction formulation (oracle/_ref/
+                       libvvmref_stream.so, STREAMFUNCTION with
+                       POISSONPARAM = 0): calpsiuw (src/PoissonSolver.cpp:
+                       124-177) on the 34x18 routine state, and 1 and 10 steps
+                       of a 64x32 warm bubble (dx = dz = 200 m, dt = 1 s)
 """
 from __future__ import annotations
 
@@ -29,7 +37,7 @@ REPO = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(REPO / "2d-vector-vorticity-model_b200"))
 sys.path.insert(0, str(REPO))
 
-from oracle.models import RefModel  # noqa: E402
+from oracle.models import RefModel, RefStreamModel  # noqa: E402
 from vvm_b200.initial_state import random_state, warm_bubble  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -131,8 +139,58 @@ def gen_poisson():
                         rhou=st.prof["rhou"], rhow=st.prof["rhow"])
 
 
+HALO_FIELDS = ("zetap", "thp", "w", "u", "qvp", "qcp", "qrp")
+
+
+def ghost_mask(nx, nz):
+    m = np.zeros((nx, nz), dtype=bool)
+    m[0, :] = m[-1, :] = True
+    m[:, 0] = m[:, -1] = True
+    return m
+
+
+def gen_halo():
+    st = kat_input()
+    rng = np.random.default_rng(11)
+    g = ghost_mask(st.grid.nx, st.grid.nz)
+    for n in HALO_FIELDS:
+        a = st.fields[n]
+        a[g] = rng.standard_normal(int(g.sum())) * (np.abs(a).max() + 1.0)
+    m = RefModel(st.grid)
+    m.load(st)
+    m.call("BoundaryProcess2D_all")
+    d = m.dump()
+    np.savez_compressed(OUT / "halo_kat.npz", **{f"in_{n}": st.fields[n] for n in HALO_FIELDS},
+                        **{f"out_{n}": d.fields[n] for n in HALO_FIELDS})
+
+
+def gen_stream():
+    st = kat_input()
+    m = RefStreamModel(st.grid)
+    m.load(st)
+    m.call("calpsiuw")
+    out = {"calpsiuw__psi": m.psi().copy(), "calpsiuw__u": m.field("u").copy(),
+           "calpsiuw__w": m.field("w").copy()}
+    m.close()
+    st = warm_bubble(64, 32)
+    m = RefStreamModel(st.grid)
+    m.load(st)
+    for s in range(1, 11):
+        m.one_step()
+        if s in (1, 10):
+            d = m.dump()
+            for n in PROG:
+                out[f"step{s}__{n}"] = d.fields[n]
+            out[f"step{s}__psi"] = m.psi().copy()
+    np.savez_compressed(OUT / "stream_kat.npz", **out)
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["poisson", "routines", "config1"]
+    which = sys.argv[1:] or ["poisson", "routines", "config1", "halo", "stream"]
+    if "halo" in which:
+        gen_halo()
+    if "stream" in which:
+        gen_stream()
     if "poisson" in which:
         gen_poisson()
     if "routines" in which:

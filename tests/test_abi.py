@@ -63,7 +63,7 @@ def test_invalid_descriptor_is_rejected_before_any_device_call(lib):
     assert b"NX and NZ" in buf.value
     d.NX, d.precision = 64, 7
     assert lib.vvm_gpu_create(ctypes.byref(d), 0, ctypes.byref(h)) == 1
-    d.precision, d.flags = 0, 2                                             # no such flag
+    d.precision, d.flags = 0, 4                                             # no such flag
     assert lib.vvm_gpu_create(ctypes.byref(d), 0, ctypes.byref(h)) == 1
     lib.vvm_gpu_last_error(None, buf, 256)
     assert b"flags" in buf.value

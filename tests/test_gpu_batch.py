@@ -70,8 +70,8 @@ def test_autotune_restores_state_and_keeps_results(gpu):
     for x, y in zip(before, after):
         assert _same(x, y)
     for c in b.cases:
-        cs, fft = c.tuning()
-        assert cs in (1, 2, 4, 8) and fft in (128, 256, 512, 32, 64)
+        tr, fft = c.tuning()
+        assert tr in (4, 8, 16, 32) and fft in (128, 256, 512, 32, 64)
     b.step(4)
     b.synchronize()
     for st, c in zip(sts, b.cases):
@@ -82,14 +82,18 @@ def test_autotune_restores_state_and_keeps_results(gpu):
 def test_knobs_leave_results_unchanged(gpu):
     st = _states([(512, 32)])[0]
     ref = _alone(gpu, st, 5, 1, 2)
-    for cs, fft in ((1, 128), (2, 512), (4, 64)):
+    for tr, fft in ((4, 128), (16, 512), (32, 64)):
         g = gpu.VVMGpu(st.grid, precision=1, solver=2)
-        g.set_tuning(cs, fft)
+        g.set_tuning(tr, fft)
         g.upload(st)
         g.step(5)
-        assert g.tuning()[0] <= max(cs, 1) or cs == 1
-        assert _same(g.download(), ref), (cs, fft)
+        assert g.tuning()[0] == tr
+        assert _same(g.download(), ref), (tr, fft)
         g.close()
+    g = gpu.VVMGpu(st.grid, precision=1, solver=2)
+    with pytest.raises(gpu.VVMGpuError):
+        g.set_tuning(12, 0)                  # not a tile height
+    g.close()
 
 
 def test_batch_rejects_cases_at_different_steps(gpu):

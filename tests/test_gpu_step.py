@@ -427,3 +427,21 @@ def test_fp64_600_steps_domain_means(gpu):
     assert abs(got[0] - ref[0]) / abs(ref[0]) <= 1e-10
     for j in (1, 2, 3, 4):
         assert abs(got[j] - ref[j]) <= 1e-6 * max(abs(ref[j]), 1e-30), (j, got[j], ref[j])
+
+
+def test_halo_all_rewrites_scrambled_ghosts(gpu):
+    """BoundaryProcess2D_all on a state whose ghost cells hold noise
+    (tests/golden/halo_kat.npz, from the reference): every ghost of zetap,
+    thp, w, u, qvp, qcp, qrp rewritten from the interior, bit for bit."""
+    st, _ = kat_state()
+    z = golden("halo_kat.npz")
+    names = ("zetap", "thp", "w", "u", "qvp", "qcp", "qrp")
+    for n in names:
+        st.fields[n] = z[f"in_{n}"].copy()
+    g = gpu.VVMGpu(st.grid)
+    g.upload(st)
+    g.call("halo_all")
+    out = g.download()
+    g.close()
+    for n in names:
+        assert np.array_equal(out.fields[n], z[f"out_{n}"]), n

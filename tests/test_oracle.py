@@ -161,3 +161,116 @@ class TestAgainstReferenceBuild:
                     assert rel_l2(db.fields[f], da.fields[f]) <= tol, (r, f)
                 else:
                     assert np.array_equal(db.fields[f], da.fields[f], equal_nan=True), (r, f)
+
+
+def _halo_state():
+    st, _ = kat_state()
+    z = golden("halo_kat.npz")
+    for n in ("zetap", "thp", "w", "u", "qvp", "qcp", "qrp"):
+        st.fields[n] = z[f"in_{n}"].copy()
+    return st, z
+
+
+def test_port_halo_all_rewrites_scrambled_ghosts(port_lib):
+    """BoundaryProcess2D_all on a state whose ghost cells hold noise: every
+    ghost is rewritten from the interior exactly as the reference does."""
+    st, z = _halo_state()
+    m = port_lib.PortModel(st.grid)
+    m.load(st)
+    m.call("BoundaryProcess2D_all")
+    for n in ("zetap", "thp", "w", "u", "qvp", "qcp", "qrp"):
+        assert not np.array_equal(z[f"in_{n}"], z[f"out_{n}"]), n   # the call changed something
+        assert np.array_equal(m.field(n), z[f"out_{n}"]), n
+
+
+class TestStreamfunction:
+    """The streamfunction formulation (STREAMFUNCTION): the restatement's
+    exact solve against the reference built with it (fixture
+    stream_kat.npz; POISSONPARAM = 0)."""
+
+    def test_port_calpsiuw_matches_reference_fixture(self, port_lib):
+        st, _ = kat_state()
+        z = golden("stream_kat.npz")
+        m = port_lib.PortModel(st.grid)
+        m.load(st)
+        m.call("calpsiuw")
+        for n in ("psi", "u", "w"):
+            assert rel_l2(m.field(n), z[f"calpsiuw__{n}"]) <= 1e-12, (n, rel_l2(m.field(n), z[f"calpsiuw__{n}"]))
+
+    def test_port_psi_solution_meets_the_reference_matrix(self, port_lib):
+        """psi solves the reference's psi matrix (src/PoissonSolver.cpp:726-756)
+        to round-off: ||b - A psi|| / ||b|| with b = zetap dx^2."""
+        st, _ = kat_state()
+        m = port_lib.PortModel(st.grid)
+        m.load(st)
+        m.call("calpsiuw")
+        x = m.field("psi")[1:-1, 2:-1].T.reshape(-1)
+        b = (st.fields["zetap"][1:-1, 2:-1] * st.grid.dx ** 2).T.reshape(-1)
+        assert np.linalg.norm(b - m.apply_psi(x)) / np.linalg.norm(b) <= 1e-13
+
+    @pytest.mark.parametrize("steps", [1, 10])
+    def test_port_stream_steps_match_reference_fixture(self, steps, port_lib):
+        from vvm_b200.initial_state import warm_bubble
+        st = warm_bubble(64, 32)
+        z = golden("stream_kat.npz")
+        m = port_lib.PortModel(st.grid)
+        m.load(st)
+        m.set_streamfunction(True)
+        for _ in range(steps):
+            m.one_step()
+        for n in ("zeta", "th", "qv", "u", "w", "psi"):
+            bound = 1e-13 if n in ("th", "qv") else 1e-10
+            e = rel_l2(m.field(n), z[f"step{steps}__{n}"])
+            assert e <= bound, (n, e)
+
+    def test_reference_stream_build_reproduces_fixture(self):
+        from oracle.models import RefStreamModel, ref_stream_available
+        if not ref_stream_available():
+            pytest.skip("oracle/_ref/libvvmref_stream.so is not built")
+        st, _ = kat_state()
+        z = golden("stream_kat.npz")
+        m = RefStreamModel(st.grid)
+        m.load(st)
+        m.call("calpsiuw")
+        assert np.array_equal(m.psi(), z["calpsiuw__psi"])
+        assert np.array_equal(m.field("w"), z["calpsiuw__w"])
+
+
+class TestThreadedBaseline:
+    """The race-free multi-core CPU baseline (oracle/_build/libvvmoracle_mt.so):
+    the restatement with OpenMP loops and FFT-based cal_w equals the serial
+    restatement to round-off, with more than one thread."""
+
+    @pytest.fixture(scope="class")
+    def models(self):
+        from oracle import models
+        if not models.port_mt_available():
+            import subprocess
+            from conftest import REPO
+            subprocess.run(["make", "-s", "-C", str(REPO / "oracle")], check=True)
+        return models
+
+    @pytest.mark.parametrize("NX,NZ", [(128, 64), (48, 20)])   # FFT path, DFT path
+    def test_threaded_steps_equal_serial(self, models, NX, NZ):
+        from vvm_b200.initial_state import random_state
+        st = random_state(NX, NZ, seed=4)
+        a = models.PortModel(st.grid)
+        a.load(st)
+        b = models.PortMTModel(st.grid)
+        b.load(st)
+        assert b.threads() >= 1
+        for _ in range(3):
+            a.one_step()
+            b.one_step()
+        for n in ("zeta", "th", "qv", "qc", "qr", "u", "w"):
+            assert rel_l2(b.field(n), a.field(n)) <= 1e-12, n
+
+    def test_fft_cal_w_meets_the_reference_matrix(self, models):
+        from vvm_b200.initial_state import warm_bubble
+        st = warm_bubble(256, 32)
+        m = models.PortMTModel(st.grid)
+        m.load(st)
+        rng = np.random.default_rng(3)
+        b = rng.standard_normal(st.grid.NX * (st.grid.NZ - 1))
+        x = m.solve_A(b)
+        assert np.linalg.norm(b - m.apply_A(x)) / np.linalg.norm(b) <= 1e-13
