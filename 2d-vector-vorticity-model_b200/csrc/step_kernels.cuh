@@ -656,14 +656,42 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
 // (i-1) and lower (k-1) neighbours, so cell (i, k) obeys
 //   v'(i,k) = A0(i,k) + C(i,k) v'(i,k-1) + B(i,k) v'(i-1,k),
 // where A0, C and B depend on old values only: B is the left-face
-// coefficient, C the lower-face one, A0 collects the rest. Two kernels:
-// k_gs_coeffs forms A0, C, B for every cell of the five fields in parallel;
-// k_gs_cluster then runs the recurrence, one thread-block cluster per field.
-// Row k is a first-order linear recurrence along i (v'(0,k) the untouched
-// ghost), solved as a scan of affine maps: each thread composes the maps of
-// its PER contiguous cells and the warp scans those with shuffles; warps pass
-// the carry along the row to the next warp, so consecutive warps work on
-// consecutive rows at the same time (a wavefront across the cluster).
+// coefficient, C the lower-face one, A0 collects the rest.
+//
+// The recurrence is lower triangular in (k, i): a cell depends on the cells
+// left of it in its row and below it in its column. The padded rows are cut
+// into tiles of tr rows (from k = 1) by 128 columns (from i = 0), one warp a
+// tile, 4 cells a lane. A pass computes every tile at once from inflows left
+// by the previous pass: the value left of each of its rows (the right outflow
+// of the tile on its left) and the row below it (the top outflow of the tile
+// below). Inside a tile each row is exact: a scan over the warp of the affine
+// maps y_i = a_i + B_i y_{i-1}, a_i = A0 + C x (x the value below), the
+// lanes' maps composed with shuffles, then applied cell by cell from the
+// inflow.
+//
+// A tile's outputs are final once its inflows are, so the tiles of the d-th
+// anti-diagonal (b + c = d) are final after pass d + 1, and nb + nc - 1 passes
+// reproduce the sequential sweep over the tiles. The passes stop earlier, as
+// soon as no outflow that another tile reads changed bit for bit from one
+// pass to the next: the following pass would then read the same inflows and
+// repeat every value, so that is the fixed point the full count reaches. With
+// diffusion coefficients of a step (B, C ~ dt K / dx^2, 1e-3 for the minimum
+// K = 10 m^2/s at dx = 100 m) an inflow error shrinks about a thousandfold a
+// pass; three passes are typical.
+//
+// Pass 1 reads the old values: it forms A0 from them and stores it, takes
+// its inflows from them (the guess), and writes no field, so every tile of it
+// reads the old state. Passes 2 on read A0, form B and C from the eddy
+// coefficients (which no pass changes) and write the field; at least two
+// passes run.
+//
+// Buffers (parity q = pass & 1 written by a pass, q ^ 1 read):
+//   right[q][f][b][c][r]   y at the tile's last column, rows r = 0..tr-1
+//   top[q][f][b][c][col]   y of the tile's top row, col = 0..127
+// The last block of a pass (a thread-fence and counter, no waiting) decides
+// whether another pass follows, and sets the graph's WHILE condition when the
+// passes run as a conditional node; the last pass of a sweep resets the pass
+// state for the next one (the host also clears it before each sweep).
 
 template <typename T>
 struct GSArgs {
@@ -674,94 +702,12 @@ struct GSArgs {
     const T *RKM, *RKH;
     int mask;         // bit f: diffuse field f
     int nudge;        // fuse Nudge_theta (field 1) and Nudge_zeta (field 0)
-    T *A0, *C, *B;    // per-cell coefficients, [5][cells] each
+    T* A0;            // per-cell constant term, [5][cells] (written by pass 1)
 };
 
 constexpr int kGSMaxNX = 8192;
 constexpr int kGSMaxPerThread = 8;      // cells a thread of the cal_u column integral
 
-// A0, C, B of cell (i, k) of field blockIdx.z, i = 0..pitch-1, k = 1..nz-2
-// (Turbulent.cpp:83-88 for zeta, :107-112 for the scalars). The ghost i = 0
-// gets the constant map v'(0, k) = v(0, k) (never updated), cells beyond
-// NX the identity map, so a row's scan needs no edge cases.
-template <typename T>
-__global__ void k_gs_coeffs(GSArgs<T> a) {
-    const int f = blockIdx.z;
-    if (!(a.mask & (1 << f))) return;
-    const Dims& d = a.d;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= d.pitch || k > d.nz - 2) return;
-    const T* v = a.v[f];
-    if (i == 0 || i > d.nx - 2) {
-        const size_t e = (size_t)f * d.cells() + d.at(i, k);
-        a.A0[e] = (i == 0) ? v[d.at(0, k)] : T(0);
-        a.C[e] = T(0);
-        a.B[e] = (i == 0) ? T(0) : T(1);
-        return;
-    }
-    const bool mom = (f == 0);
-    const T* K = mom ? a.RKM : a.RKH;
-    const T cx = T(a.c.rdx2 * a.c.dt);
-    const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
-    T v0 = v[d.at(i, k)], vr = v[d.at(i + 1, k)], vu = v[d.at(i, k + 1)];
-    T ax, bx, czu, czd;
-    if (mom) {
-        T Kc = K[d.at(i, k)], Kd = K[d.at(i, k - 1)], Kl = K[d.at(i - 1, k)], Kld = K[d.at(i - 1, k - 1)];
-        ax = T(0.5) * (Kc + Kd);
-        bx = T(0.5) * (Kl + Kld);
-        czu = T(a.p.rhou[k]) * T(0.5) * (Kc + Kl);
-        czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd + Kld);
-    } else {
-        T Kc = K[d.at(i, k)], Kr = K[d.at(i + 1, k)], Kl = K[d.at(i - 1, k)];
-        T Ku = K[d.at(i, k + 1)], Kd = K[d.at(i, k - 1)];
-        ax = T(0.5) * (Kr + Kc);
-        bx = T(0.5) * (Kc + Kl);
-        czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku + Kc);
-        czd = T(a.p.rhow[k]) * T(0.5) * (Kc + Kd);
-    }
-    T du = vu - v0, dd = v0;
-    if (kPert<T> && (f == 1 || f == 2)) {   // th', qv' about a profile
-        du += T(a.p.d0[f - 1][k + 1]);
-        dd += T(a.p.d0[f - 1][k]);
-    }
-    // v + cx (ax (vr - v) - bx (v - v'[i-1])) + cz (czu du - czd (dd - v'below))
-    const size_t e = (size_t)f * d.cells() + d.at(i, k);
-    a.A0[e] = v0 + cx * (ax * (vr - v0) - bx * v0) + cz * (czu * du - czd * dd);
-    a.C[e] = cz * czd;
-    a.B[e] = cx * bx;
-}
-
-// ---------------------------------------------------------------------------
-// The Gauss-Seidel recurrence by tiles and passes.
-//
-// v'(i,k) = A0 + C v'(i,k-1) + B v'(i-1,k) (coefficients from k_gs_coeffs) is
-// lower triangular in (k, i): a cell depends on the cells left of it in its
-// row and below it in its column. The padded rows are cut into tiles of TR
-// rows (from k = 1) by 128 columns (from i = 0), one warp a tile, 4 cells a
-// lane. A pass computes every tile at once from inflows left by the previous
-// pass: the value left of each of its rows (the right outflow of the tile on
-// its left) and the row below it (the top outflow of the tile below). Inside
-// a tile each row is exact: a scan over the warp of the affine maps
-// y_i = a_i + B_i y_{i-1}, a_i = A0 + C x (the value below), the lanes' maps
-// composed with shuffles, then applied cell by cell from the inflow.
-//
-// A tile's outputs are final once its inflows are, so the tiles of the d-th
-// anti-diagonal (b + c = d) are final after pass d + 1, and nb + nc - 1 passes
-// reproduce the sequential sweep over the tiles. The passes stop earlier, as
-// soon as no outflow that another tile reads changed bit for bit from one
-// pass to the next: the following pass would then read the same inflows and
-// repeat every value, so that is the fixed point the full count reaches. With
-// diffusion coefficients of a step (B, C ~ dt K / dx^2, 1e-3 for the minimum
-// K = 10 m^2/s at dx = 100 m) an inflow error shrinks about a thousandfold a
-// pass. Pass 1 starts from the old values (k_gs_tiles_init).
-//
-// Buffers (parity q = pass & 1 written by a pass, q ^ 1 read):
-//   right[q][f][b][c][r]   y at the tile's last column, rows r = 0..TR-1
-//   top[q][f][b][c][col]   y of the tile's top row, col = 0..127
-// The last block of a pass (a thread-fence and counter, no waiting) decides
-// whether another pass follows, advances the pass counter, and sets the
-// graph's WHILE condition when the passes run as a conditional node.
 constexpr int kGTCols = 128;   // columns of a tile: 32 lanes x 4 cells
 constexpr int kGTPer = 4;
 // Rows of a tile: the autotuner's knob (the passes a sweep needs do not
@@ -769,11 +715,10 @@ constexpr int kGTPer = 4;
 constexpr int kGSTileRowsMin = 4, kGSTileRowsMax = 32, kGSTileRowsDefault = 8;
 inline bool gs_tile_rows_ok(int tr) { return tr == 4 || tr == 8 || tr == 16 || tr == 32; }
 
-struct GSTileCtl {
-    int pass;         // the pass the next launch runs (1, 2, ...)
+struct GSTileCtl {    // zeroed before a sweep
+    int pass;         // passes of the sweep completed
     int changed[2];   // by parity of the pass that wrote an outflow differing from its previous one
     int done;         // blocks of the current pass that finished
-    int maxp;         // nb + nc - 1: every tile final by then
     int more;         // another pass follows (read by the host loop)
     int passes;       // passes run by the last sweep
 };
@@ -793,91 +738,170 @@ struct GSTileArgs {
     }
 };
 
-// The parity-0 outflows from the old values (the inflows of pass 1), and the
-// loop state; one thread an outflow value.
+// 4 consecutive cells of one row (16-byte aligned: i a multiple of 4, rows of
+// a multiple of 32 cells).
 template <typename T>
-__global__ void k_gs_tiles_init(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) {
-    const Dims& d = a.d;
-    const int kend = d.nz - 2;
-    const size_t nr = (size_t)5 * t.nb * t.nc * t.tr, nt = (size_t)5 * t.nb * t.nc * kGTCols;
-    const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j == 0) {
-        t.ctl->pass = 1;
-        t.ctl->changed[0] = t.ctl->changed[1] = 0;
-        t.ctl->done = 0;
-        t.ctl->maxp = t.nb + t.nc - 1;
-        t.ctl->more = 1;
-        t.ctl->passes = 0;
-        if (h) cudaGraphSetConditional(h, 1u);
-    }
-    if (j < nr) {
-        const int r = (int)(j % t.tr);
-        const size_t tile = j / t.tr;
-        const int c = (int)(tile % t.nc), b = (int)((tile / t.nc) % t.nb), f = (int)(tile / ((size_t)t.nc * t.nb));
-        const int i = c * kGTCols + kGTCols - 1, k = 1 + b * t.tr + r;
-        t.right[j] = (i < d.pitch && k <= kend) ? a.v[f][d.at(i, k)] : T(0);
-    } else if (j < nr + nt) {
-        const size_t jj = j - nr;
-        const int col = (int)(jj % kGTCols);
-        const size_t tile = jj / kGTCols;
-        const int c = (int)(tile % t.nc), b = (int)((tile / t.nc) % t.nb), f = (int)(tile / ((size_t)t.nc * t.nb));
-        const int i = c * kGTCols + col, k = min(1 + b * t.tr + t.tr - 1, kend);
-        t.top[jj] = (i < d.pitch) ? a.v[f][d.at(i, k)] : T(0);
+__device__ __forceinline__ void gs_ld4(const T* p, T (&x)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 u = __ldg(reinterpret_cast<const float4*>(p));
+        x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w;
+    } else {
+        const double2 u = __ldg(reinterpret_cast<const double2*>(p)), w = __ldg(reinterpret_cast<const double2*>(p) + 1);
+        x[0] = u.x, x[1] = u.y, x[2] = w.x, x[3] = w.y;
     }
 }
 
-// One pass over every tile: 4 warps (tiles) a block. Stores the nudged
-// values (Nudge_zeta, Nudge_theta fused as in k_gs_cluster) of interior
-// cells, carries the un-nudged ones.
-template <typename T>
-__global__ void __launch_bounds__(128) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) {
+// One pass over every tile: 4 warps (tiles) a block. Each lane keeps its
+// cells' rows of K (k-1, k and, in pass 1, k+1) and, in pass 1, of the old
+// field (k, k+1) in registers, rolled up a row at a time; the next row's
+// loads are issued before the current row's scan. Left and right neighbours
+// come from the adjacent lane by shuffle (the tile's edge lanes load theirs).
+// B, C (and in pass 1 A0) follow Turbulent.cpp:83-88 for zeta and :107-112
+// for the scalars term by term. The ghost i = 0 gets the constant map
+// v'(0, k) = v(0, k) (never updated), cells beyond NX the identity map, so a
+// row's scan needs no edge cases. Stores the nudged values (Nudge_zeta,
+// Nudge_theta) of interior cells, carries the un-nudged ones.
+// FIRST: pass 1 (launched on its own, before the loop of the later passes).
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) {
     __shared__ int any_changed;
     const Dims& d = a.d;
     const int NX = d.nx - 2, kend = d.nz - 2;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (threadIdx.x == 0) any_changed = 0;
     __syncthreads();
-    const int pass = t.ctl->pass;
+    constexpr bool first = FIRST;
+    const int pass = FIRST ? 1 : t.ctl->pass + 1;
     const int q = pass & 1, qp = q ^ 1;
     const int tile = blockIdx.x * 4 + wid;
     const int ntiles = 5 * t.nb * t.nc;
     const int c = tile % t.nc, b = (tile / t.nc) % t.nb, f = tile / (t.nc * t.nb);
-    if (tile < ntiles && (a.mask & (1 << f))) {
+    if (tile < ntiles && (a.mask & (1 << f))) {   // uniform over the warp
         T* v = a.v[f];
-        const size_t fo = (size_t)f * d.cells();
-        const T *A0 = a.A0 + fo, *Cc = a.C + fo, *Bc = a.B + fo;
+        const bool mom = (f == 0);
+        const T* K = mom ? a.RKM : a.RKH;
+        T* A0s = a.A0 + (size_t)f * d.cells();
         const int i0 = c * kGTCols + lane * kGTPer;
         const bool act = i0 < d.pitch;   // pitch is a multiple of 32, so of kGTPer
+        const int k0 = 1 + b * t.tr;
+        const int rows = min(t.tr, kend - k0 + 1);
+        const int ilast = c * kGTCols + kGTCols - 1;   // the tile's last column
+        const bool edge_l = (lane == 0 && i0 >= 1);             // its left neighbour is in another tile
+        const bool edge_r = (lane == 31 && act && i0 + 3 <= NX); // its right neighbour is needed
+        const T cx = T(a.c.rdx2 * a.c.dt);
+        const bool pert = kPert<T> && (f == 1 || f == 2);
+        auto row4 = [&](const T* base, int k, T (&x)[4]) {
+            if (act) gs_ld4(base + d.at(i0, k), x);
+            else x[0] = x[1] = x[2] = x[3] = T(0);
+        };
         bool diff = false;
-        // the row below the tile: the old row 0 (never updated) or the top outflow below
+        // the row below the tile: the old row 0 (never updated), or the top
+        // outflow of the tile below (pass 1: the old values there)
         T below[kGTPer];
+        if (b == 0 || first) {
+            row4(v, k0 - 1, below);
+            if (b == 0) {
 #pragma unroll
-        for (int e = 0; e < kGTPer; e++) {
-            const int i = i0 + e;
-            if (b == 0) below[e] = (act && i >= 1 && i <= NX) ? v[d.at(i, 0)] : T(0);
-            else below[e] = t.top[t.ti(qp, f, b - 1, c) + lane * kGTPer + e];
+                for (int e = 0; e < kGTPer; e++)
+                    if (!(i0 + e >= 1 && i0 + e <= NX)) below[e] = T(0);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < kGTPer; e++) below[e] = t.top[t.ti(qp, f, b - 1, c) + lane * kGTPer + e];
+        }
+        // rolling windows: K rows k-1 (Kd), k (Kc), k+1 (Ku); old field rows k (v0), k+1 (vu)
+        T Kd[4], Kc[4], Ku[4], v0[4], vu[4], An[4];
+        row4(K, k0 - 1, Kd);
+        row4(K, k0, Kc);
+        if (first) {
+            row4(K, k0 + 1, Ku);
+            row4(v, k0, v0);
+            row4(v, k0 + 1, vu);
+        } else {
+            row4(A0s, k0, An);
         }
         const T* rin = t.right + t.ri(qp, f, b, c - 1);   // read only when c > 0
         T* rout = t.right + t.ri(q, f, b, c);
         const T* rold = t.right + t.ri(qp, f, b, c);
-        const int k0 = 1 + b * t.tr;
-        const int rows = min(t.tr, kend - k0 + 1);
         for (int r = 0; r < rows; r++) {
             const int k = k0 + r;
+            const bool more_rows = r + 1 < rows;
+            // the next row's loads, in flight during this row's work
+            T Kn[4], vn[4], An2[4];
+            if (more_rows) {
+                if (first) {
+                    row4(K, k + 2, Kn);
+                    row4(v, k + 2, vn);
+                } else {
+                    row4(K, k + 1, Kn);
+                    row4(A0s, k + 1, An2);
+                }
+            }
+            // neighbours across lanes (edge lanes load theirs)
+            T Kl0 = __shfl_up_sync(0xffffffffu, Kc[3], 1);
+            T Kld0 = __shfl_up_sync(0xffffffffu, Kd[3], 1);
+            T Kr3 = __shfl_down_sync(0xffffffffu, Kc[0], 1);
+            T vr3 = __shfl_down_sync(0xffffffffu, first ? v0[0] : T(0), 1);
+            if (edge_l) {
+                Kl0 = K[d.at(i0 - 1, k)];
+                if (mom) Kld0 = K[d.at(i0 - 1, k - 1)];
+            }
+            if (first && edge_r) {
+                Kr3 = K[d.at(i0 + 4, k)];
+                vr3 = v[d.at(i0 + 4, k)];
+            }
+            const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
             T aa[kGTPer], bb[kGTPer];
-            if (act) {
-                const size_t e0 = d.at(i0, k);
 #pragma unroll
-                for (int e = 0; e < kGTPer; e++) {
-                    aa[e] = A0[e0 + e] + Cc[e0 + e] * below[e];
-                    bb[e] = Bc[e0 + e];
+            for (int e = 0; e < kGTPer; e++) {
+                const int i = i0 + e;
+                T A0, B, C;
+                if (!act || i > NX) {          // beyond NX: identity
+                    A0 = T(0);
+                    B = T(1);
+                    C = T(0);
+                } else if (i == 0) {           // the ghost: constant map
+                    A0 = first ? v0[0] : An[0];
+                    B = T(0);
+                    C = T(0);
+                } else {
+                    const T Kl = (e == 0) ? Kl0 : Kc[e - 1];
+                    T ax = T(0), bx, czu = T(0), czd;
+                    if (mom) {
+                        const T Kld = (e == 0) ? Kld0 : Kd[e - 1];
+                        bx = T(0.5) * (Kl + Kld);
+                        czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd[e] + Kld);
+                        if (first) {
+                            ax = T(0.5) * (Kc[e] + Kd[e]);
+                            czu = T(a.p.rhou[k]) * T(0.5) * (Kc[e] + Kl);
+                        }
+                    } else {
+                        bx = T(0.5) * (Kc[e] + Kl);
+                        czd = T(a.p.rhow[k]) * T(0.5) * (Kc[e] + Kd[e]);
+                        if (first) {
+                            const T Kr = (e == 3) ? Kr3 : Kc[e + 1];
+                            ax = T(0.5) * (Kr + Kc[e]);
+                            czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku[e] + Kc[e]);
+                        }
+                    }
+                    C = cz * czd;
+                    B = cx * bx;
+                    if (first) {
+                        const T vc = v0[e], vr = (e == 3) ? vr3 : v0[e + 1];
+                        T du = vu[e] - vc, dd = vc;
+                        if (pert) {   // th', qv' about a profile
+                            du += T(a.p.d0[f - 1][k + 1]);
+                            dd += T(a.p.d0[f - 1][k]);
+                        }
+                        // v + cx (ax (vr - v) - bx (v - v'[i-1])) + cz (czu du - czd (dd - v'below))
+                        A0 = vc + cx * (ax * (vr - vc) - bx * vc) + cz * (czu * du - czd * dd);
+                    } else {
+                        A0 = An[e];
+                    }
                 }
-            } else {
-#pragma unroll
-                for (int e = 0; e < kGTPer; e++) {
-                    aa[e] = T(0);
-                    bb[e] = T(1);
-                }
+                if (first && act) A0s[d.at(i0, k) + e] = A0;
+                aa[e] = A0 + C * below[e];
+                bb[e] = B;
             }
             // the lane's map over its cells: y_out = P + M y_in
             T P = T(0), M = T(1);
@@ -894,7 +918,9 @@ __global__ void __launch_bounds__(128) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, 
                     M = M * qM;
                 }
             }
-            const T x = (c > 0) ? rin[r] : T(0);   // chunk 0 starts at the ghost (B = 0)
+            // the inflow left of the row (chunk 0 starts at the ghost, B = 0)
+            T x = T(0);
+            if (c > 0) x = first ? v[d.at(c * kGTCols - 1, k)] : rin[r];
             const T eP = __shfl_up_sync(0xffffffffu, P, 1), eM = __shfl_up_sync(0xffffffffu, M, 1);
             T y = (lane == 0) ? x : eP + eM * x;
             T dn = T(0), tn = T(0);   // nudging of row k: out = y - dn (y - tn)
@@ -910,7 +936,7 @@ __global__ void __launch_bounds__(128) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, 
                 below[e] = y;
                 out[e] = y - dn * (y - tn);
             }
-            if (act) {
+            if (act && !first) {
                 T* dst = v + d.at(i0, k);
                 if (i0 >= 1 && i0 + kGTPer - 1 <= NX) {
                     if constexpr (sizeof(T) == 4) {
@@ -928,15 +954,38 @@ __global__ void __launch_bounds__(128) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, 
             const T yr = __shfl_sync(0xffffffffu, y, 31);   // y at the tile's last column
             if (lane == 0) {
                 rout[r] = yr;
-                if (c + 1 < t.nc && !(yr == rold[r])) diff = true;   // read by the tile on the right
+                if (c + 1 < t.nc) {   // read by the tile on the right
+                    const T prev = first ? v[d.at(ilast, k)] : rold[r];
+                    if (!(yr == prev)) diff = true;
+                }
+            }
+            // roll the windows up a row
+            if (more_rows) {
+#pragma unroll
+                for (int e = 0; e < kGTPer; e++) {
+                    Kd[e] = Kc[e];
+                    if (first) {
+                        Kc[e] = Ku[e];
+                        Ku[e] = Kn[e];
+                        v0[e] = vu[e];
+                        vu[e] = vn[e];
+                    } else {
+                        Kc[e] = Kn[e];
+                        An[e] = An2[e];
+                    }
+                }
             }
         }
         T* tout = t.top + t.ti(q, f, b, c) + lane * kGTPer;
         const T* told = t.top + t.ti(qp, f, b, c) + lane * kGTPer;
+        const int ktop = k0 + rows - 1;
 #pragma unroll
         for (int e = 0; e < kGTPer; e++) {
             tout[e] = below[e];
-            if (b + 1 < t.nb && !(below[e] == told[e])) diff = true;   // read by the tile above
+            if (b + 1 < t.nb) {   // read by the tile above
+                const T prev = first ? (act ? v[d.at(i0 + e, ktop)] : T(0)) : told[e];
+                if (!(below[e] == prev)) diff = true;
+            }
         }
         if (__any_sync(0xffffffffu, diff) && lane == 0) any_changed = 1;
     }
@@ -948,12 +997,19 @@ __global__ void __launch_bounds__(128) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, 
         if (prev == (int)gridDim.x - 1) {   // the last block of the pass decides
             __threadfence();
             const int ch = *(volatile int*)&t.ctl->changed[q];
-            const int more = ch && pass < t.ctl->maxp;
-            t.ctl->changed[qp] = 0;          // the next pass writes that parity
+            // pass 1 writes no field: a second pass always follows; every tile
+            // is final after nb + nc - 1 passes
+            const int more = (first || ch) && pass < max(2, t.nb + t.nc - 1);
             t.ctl->done = 0;
-            t.ctl->pass = pass + 1;
             t.ctl->passes = pass;
             t.ctl->more = more;
+            if (more) {
+                t.ctl->changed[qp] = 0;   // the next pass writes that parity
+                t.ctl->pass = pass;
+            } else {                      // ready for the next sweep
+                t.ctl->changed[0] = t.ctl->changed[1] = 0;
+                t.ctl->pass = 0;
+            }
             if (t.exec) *t.exec += 1;
             if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
         }

@@ -451,36 +451,6 @@ struct HostLine {   // host copy of one level's line factors
     std::vector<double> band;
 };
 
-// Dense inverse by Gauss-Jordan with partial pivoting (n <= 64).
-static void invert(std::vector<double>& A, int n) {
-    std::vector<double> I((size_t)n * n, 0.0);
-    for (int i = 0; i < n; i++) I[(size_t)i * n + i] = 1.0;
-    for (int c = 0; c < n; c++) {
-        int piv = c;
-        for (int r = c + 1; r < n; r++)
-            if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)piv * n + c])) piv = r;
-        if (piv != c)
-            for (int j = 0; j < n; j++) {
-                std::swap(A[(size_t)c * n + j], A[(size_t)piv * n + j]);
-                std::swap(I[(size_t)c * n + j], I[(size_t)piv * n + j]);
-            }
-        double d = A[(size_t)c * n + c];
-        for (int j = 0; j < n; j++) {
-            A[(size_t)c * n + j] /= d;
-            I[(size_t)c * n + j] /= d;
-        }
-        for (int r = 0; r < n; r++) {
-            if (r == c) continue;
-            double f = A[(size_t)r * n + c];
-            if (f == 0.0) continue;
-            for (int j = 0; j < n; j++) {
-                A[(size_t)r * n + j] -= f * A[(size_t)c * n + j];
-                I[(size_t)r * n + j] -= f * I[(size_t)c * n + j];
-            }
-        }
-    }
-    A.swap(I);
-}
 
 // Segment factors, spikes and reduced inverse of tridiag(-rd, xdiag + ru + rd, -ru)
 // (first row without the -rd coupling, last without -ru: W = 0 beyond).
@@ -1413,7 +1383,7 @@ struct Fields {
     T* hist[NHIST][2] = {};
     T *d_auto = nullptr, *d_accr = nullptr, *d_evap = nullptr, *d_cond = nullptr;
     T *precip = nullptr, *th_forcing = nullptr;
-    T *gsA = nullptr, *gsC = nullptr, *gsB = nullptr;   // Gauss-Seidel coefficients, [5][cells]
+    T* gsA = nullptr;                                   // Gauss-Seidel constant terms, [5][cells]
     T *gsRight = nullptr, *gsTop = nullptr;             // Gauss-Seidel tile outflows (k_gs_tiles)
 };
 
@@ -1432,6 +1402,7 @@ struct vvm_gpu_ctx {
     bool spectral = false;   // VVM_SOLVER_SPECTRAL
     int tune_gs_tr = 0;      // rows of a Gauss-Seidel tile (0: automatic)
     GSTileCtl* gsctl = nullptr;   // pass state of the Gauss-Seidel tiles
+    int* sc_host_i = nullptr;     // pinned: the tiles' "another pass" flag read by the host loop
     // learned preconditioner (VVM_SOLVER_LEARNED)
     std::unique_ptr<LearnedNet> net;
     double* z64 = nullptr;   // preconditioned residual, solver layout
@@ -1522,6 +1493,7 @@ struct vvm_gpu_ctx {
         if (pcg32) pcg32->release();
         if (pcg_psi) pcg_psi->release();
         if (sc_host) cudaFreeHost(sc_host);
+        if (sc_host_i) cudaFreeHost(sc_host_i);
         if (own) cudaStreamDestroy(own);
     }
 
@@ -1580,13 +1552,12 @@ void alloc_fields(vvm_gpu_ctx* c) {
     F.precip = c->ar.alloc<T>(c->d.nx);
     F.th_forcing = c->ar.alloc<T>(n);
     F.gsA = c->ar.alloc<T>(5 * n);
-    F.gsC = c->ar.alloc<T>(5 * n);
-    F.gsB = c->ar.alloc<T>(5 * n);
     // tile outflows for any tile height in kGSTileRows
     const size_t nc = cdiv(c->d.pitch, kGTCols), rows = c->d.nz - 2;
     F.gsRight = c->ar.alloc<T>(2 * 5 * nc * (rows + kGSTileRowsMax));
     F.gsTop = c->ar.alloc<T>(2 * 5 * nc * (size_t)cdiv((int)rows, kGSTileRowsMin) * kGTCols);
     if (!c->gsctl) c->gsctl = c->ar.alloc<GSTileCtl>(1);
+    if (!c->sc_host_i) CK(cudaMallocHost(&c->sc_host_i, sizeof(int)));
 }
 
 // ---------------------------------------------------------------- routines
@@ -1745,46 +1716,38 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops 
     LAUNCH(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r));
     CKL();
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
-                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, F.gsC, F.gsB};
-    const int pitch = c->d.pitch;
-    dim3 cb(64, 4), cg(cdiv(pitch, 64), cdiv(c->d.nz - 2, 4), 5);
-    LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_coeffs<T><<<cg, cb, 0, c->stream>>>(g));
-    CKL();
+                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA};
     // the recurrence: tiles and passes (see k_gs_tiles)
     const int tr = gs_tile_rows(c);
-    const int nb = cdiv(c->d.nz - 2, tr), nc = cdiv(pitch, kGTCols);
+    const int nb = cdiv(c->d.nz - 2, tr), nc = cdiv(c->d.pitch, kGTCols);
     GSTileArgs<T> t{nb, nc, tr, F.gsRight, F.gsTop, c->gsctl, recorded_in_loops ? c->d_exec : nullptr};
-    const size_t nout = (size_t)5 * nb * nc * (tr + kGTCols);
-    const int iblocks = (int)((nout + 255) / 256);
     const int tblocks = cdiv(5 * nb * nc, 4);
-    const int maxp = nb + nc - 1;
+    const int maxp = std::max(2, nb + nc - 1);
     cudaStream_t st = c->stream;
-    if (recorded_in_loops) {   // graph capture: the passes as a WHILE node
-        cudaGraphConditionalHandle h = new_handle(st);
-        LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles_init<T><<<iblocks, 256, 0, st>>>(g, t, h));
-        CKL();
+    CK(cudaMemsetAsync(c->gsctl, 0, sizeof(GSTileCtl), st));   // a fresh sweep
+    LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T, true><<<tblocks, 128, 0, st>>>(g, t, 0));   // pass 1
+    CKL();
+    if (recorded_in_loops) {   // graph capture: passes 2.. as a WHILE node, entered every launch
+        cudaStreamCaptureStatus status;
+        cudaGraph_t cg;
+        CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &cg, nullptr, nullptr));
+        cudaGraphConditionalHandle h;
+        CK(cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault));
         cudaGraph_t body = add_while(st, h);
         BodyCapture bc(c->cap[0], body);
         const long long n0 = c->stats.launches;
-        LAUNCH(&c->stats, VVM_K_GS, bc.s, k_gs_tiles<T><<<tblocks, 128, 0, bc.s>>>(g, t, h));
+        LAUNCH(&c->stats, VVM_K_GS, bc.s, k_gs_tiles<T, false><<<tblocks, 128, 0, bc.s>>>(g, t, h));
         CKL();
         bc.end();
         *recorded_in_loops += c->stats.launches - n0;
         return;
     }
-    LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles_init<T><<<iblocks, 256, 0, st>>>(g, t, 0));
-    CKL();
-    // host loop: the passes are idempotent once converged, so the flag is
-    // read every other pass from the third on
-    for (int p = 1; p <= maxp; p++) {
-        LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T><<<tblocks, 128, 0, st>>>(g, t, 0));
+    for (int p = 2; p <= maxp; p++) {
+        LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T, false><<<tblocks, 128, 0, st>>>(g, t, 0));
         CKL();
-        if (p >= 3 && (p % 2 == 1 || p == maxp)) {
-            int more = 1;
-            CK(cudaMemcpyAsync(&more, &c->gsctl->more, sizeof(int), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            if (!more) break;
-        }
+        CK(cudaMemcpyAsync(c->sc_host_i, &c->gsctl->more, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (!*c->sc_host_i) break;
     }
 }
 
