@@ -713,6 +713,7 @@ constexpr int kGTPer = 4;
 // Rows of a tile: the autotuner's knob (the passes a sweep needs do not
 // depend on it; taller tiles mean fewer, longer tiles a pass).
 constexpr int kGSTileRowsMin = 4, kGSTileRowsMax = 32, kGSTileRowsDefault = 8;
+constexpr int kGSRowVals = 9;   // scalars a tile row keeps in shared memory
 inline bool gs_tile_rows_ok(int tr) { return tr == 4 || tr == 8 || tr == 16 || tr == 32; }
 
 struct GSTileCtl {    // zeroed before a sweep
@@ -765,6 +766,10 @@ __device__ __forceinline__ void gs_ld4(const T* p, T (&x)[4]) {
 template <typename T, bool FIRST>
 __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) {
     __shared__ int any_changed;
+    // per warp and row of its tile: cz, the czd and czu density factors,
+    // nudging dn and tn, the inflow left of the row and its previous value,
+    // and (pass 1, th' and qv') the profile differences at k and k+1
+    __shared__ T rowv[4][kGSTileRowsMax][kGSRowVals];
     const Dims& d = a.d;
     const int NX = d.nx - 2, kend = d.nz - 2;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -820,14 +825,57 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
         } else {
             row4(A0s, k0, An);
         }
+        // the edge lanes' neighbours in the next tiles, a row ahead as well:
+        // lane 0 K(i0-1, k) (and, rolled, K(i0-1, k-1)); lane 31 in pass 1
+        // K(i0+4, k) and v(i0+4, k)
+        T eKl = T(0), eKld = T(0), eKr = T(0), evr = T(0);
+        if (edge_l) {
+            eKl = K[d.at(i0 - 1, k0)];
+            eKld = K[d.at(i0 - 1, k0 - 1)];
+        }
+        if (first && edge_r) {
+            eKr = K[d.at(i0 + 4, k0)];
+            evr = v[d.at(i0 + 4, k0)];
+        }
         const T* rin = t.right + t.ri(qp, f, b, c - 1);   // read only when c > 0
         T* rout = t.right + t.ri(q, f, b, c);
         const T* rold = t.right + t.ri(qp, f, b, c);
+        // the rows' scalars, one lane a row, all loads at once
+        if (lane < rows) {
+            const int k = k0 + lane;
+            T* rv = rowv[wid][lane];
+            if (mom) {
+                rv[0] = T(a.c.rdz2 * a.c.dt / a.p.rhow[k]);
+                rv[1] = T(a.p.rhou[k - 1]);
+                rv[2] = T(a.p.rhou[k]);
+            } else {
+                rv[0] = T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
+                rv[1] = T(a.p.rhow[k]);
+                rv[2] = T(a.p.rhow[k + 1]);
+            }
+            T dn = T(0), tn = T(0);   // nudging of row k: out = y - dn (y - tn)
+            if (a.nudge && f == 0) dn = T(a.p.dtcgr_zeta[k]);
+            if (a.nudge && f == 1) {
+                dn = T(a.p.dtcgr_th[k]);
+                tn = kPert<T> ? T(-a.p.dn[0][k]) : T(a.p.thb_init[k]);
+            }
+            rv[3] = dn;
+            rv[4] = tn;
+            rv[5] = (c > 0) ? (first ? v[d.at(c * kGTCols - 1, k)] : rin[lane]) : T(0);
+            rv[6] = (c + 1 < t.nc) ? (first ? v[d.at(ilast, k)] : rold[lane]) : T(0);
+            if (first && pert) {
+                rv[7] = T(a.p.d0[f - 1][k]);
+                rv[8] = T(a.p.d0[f - 1][k + 1]);
+            }
+        }
+        __syncwarp();
         for (int r = 0; r < rows; r++) {
+            const T* rv = rowv[wid][r];
             const int k = k0 + r;
             const bool more_rows = r + 1 < rows;
             // the next row's loads, in flight during this row's work
             T Kn[4], vn[4], An2[4];
+            T eKl_n = T(0), eKr_n = T(0), evr_n = T(0);
             if (more_rows) {
                 if (first) {
                     row4(K, k + 2, Kn);
@@ -836,21 +884,26 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
                     row4(K, k + 1, Kn);
                     row4(A0s, k + 1, An2);
                 }
+                if (edge_l) eKl_n = K[d.at(i0 - 1, k + 1)];
+                if (first && edge_r) {
+                    eKr_n = K[d.at(i0 + 4, k + 1)];
+                    evr_n = v[d.at(i0 + 4, k + 1)];
+                }
             }
-            // neighbours across lanes (edge lanes load theirs)
+            // neighbours across lanes (the edge lanes' from the next tiles)
             T Kl0 = __shfl_up_sync(0xffffffffu, Kc[3], 1);
             T Kld0 = __shfl_up_sync(0xffffffffu, Kd[3], 1);
             T Kr3 = __shfl_down_sync(0xffffffffu, Kc[0], 1);
             T vr3 = __shfl_down_sync(0xffffffffu, first ? v0[0] : T(0), 1);
             if (edge_l) {
-                Kl0 = K[d.at(i0 - 1, k)];
-                if (mom) Kld0 = K[d.at(i0 - 1, k - 1)];
+                Kl0 = eKl;
+                Kld0 = eKld;
             }
             if (first && edge_r) {
-                Kr3 = K[d.at(i0 + 4, k)];
-                vr3 = v[d.at(i0 + 4, k)];
+                Kr3 = eKr;
+                vr3 = evr;
             }
-            const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
+            const T cz = rv[0], rhod = rv[1], rhou_ = rv[2];
             T aa[kGTPer], bb[kGTPer];
 #pragma unroll
             for (int e = 0; e < kGTPer; e++) {
@@ -870,18 +923,18 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
                     if (mom) {
                         const T Kld = (e == 0) ? Kld0 : Kd[e - 1];
                         bx = T(0.5) * (Kl + Kld);
-                        czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd[e] + Kld);
+                        czd = rhod * T(0.5) * (Kd[e] + Kld);
                         if (first) {
                             ax = T(0.5) * (Kc[e] + Kd[e]);
-                            czu = T(a.p.rhou[k]) * T(0.5) * (Kc[e] + Kl);
+                            czu = rhou_ * T(0.5) * (Kc[e] + Kl);
                         }
                     } else {
                         bx = T(0.5) * (Kc[e] + Kl);
-                        czd = T(a.p.rhow[k]) * T(0.5) * (Kc[e] + Kd[e]);
+                        czd = rhod * T(0.5) * (Kc[e] + Kd[e]);
                         if (first) {
                             const T Kr = (e == 3) ? Kr3 : Kc[e + 1];
                             ax = T(0.5) * (Kr + Kc[e]);
-                            czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku[e] + Kc[e]);
+                            czu = rhou_ * T(0.5) * (Ku[e] + Kc[e]);
                         }
                     }
                     C = cz * czd;
@@ -890,8 +943,8 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
                         const T vc = v0[e], vr = (e == 3) ? vr3 : v0[e + 1];
                         T du = vu[e] - vc, dd = vc;
                         if (pert) {   // th', qv' about a profile
-                            du += T(a.p.d0[f - 1][k + 1]);
-                            dd += T(a.p.d0[f - 1][k]);
+                            du += rv[8];
+                            dd += rv[7];
                         }
                         // v + cx (ax (vr - v) - bx (v - v'[i-1])) + cz (czu du - czd (dd - v'below))
                         A0 = vc + cx * (ax * (vr - vc) - bx * vc) + cz * (czu * du - czd * dd);
@@ -919,16 +972,10 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
                 }
             }
             // the inflow left of the row (chunk 0 starts at the ghost, B = 0)
-            T x = T(0);
-            if (c > 0) x = first ? v[d.at(c * kGTCols - 1, k)] : rin[r];
+            const T x = rv[5];
             const T eP = __shfl_up_sync(0xffffffffu, P, 1), eM = __shfl_up_sync(0xffffffffu, M, 1);
             T y = (lane == 0) ? x : eP + eM * x;
-            T dn = T(0), tn = T(0);   // nudging of row k: out = y - dn (y - tn)
-            if (a.nudge && f == 0) dn = T(a.p.dtcgr_zeta[k]);
-            if (a.nudge && f == 1) {
-                dn = T(a.p.dtcgr_th[k]);
-                tn = kPert<T> ? T(-a.p.dn[0][k]) : T(a.p.thb_init[k]);
-            }
+            const T dn = rv[3], tn = rv[4];
             T out[kGTPer];
 #pragma unroll
             for (int e = 0; e < kGTPer; e++) {
@@ -954,13 +1001,14 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
             const T yr = __shfl_sync(0xffffffffu, y, 31);   // y at the tile's last column
             if (lane == 0) {
                 rout[r] = yr;
-                if (c + 1 < t.nc) {   // read by the tile on the right
-                    const T prev = first ? v[d.at(ilast, k)] : rold[r];
-                    if (!(yr == prev)) diff = true;
-                }
+                if (c + 1 < t.nc && !(yr == rv[6])) diff = true;   // read by the tile on the right
             }
             // roll the windows up a row
             if (more_rows) {
+                eKld = eKl;
+                eKl = eKl_n;
+                eKr = eKr_n;
+                evr = evr_n;
 #pragma unroll
                 for (int e = 0; e < kGTPer; e++) {
                     Kd[e] = Kc[e];

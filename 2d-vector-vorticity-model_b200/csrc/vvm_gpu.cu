@@ -1706,7 +1706,12 @@ struct BodyCapture {   // stream capture into a conditional node's body graph
     }
 };
 
-inline int gs_tile_rows(const vvm_gpu_ctx* c) { return c->tune_gs_tr ? c->tune_gs_tr : kGSTileRowsDefault; }
+// Automatic tile height: 16 rows in FP64, 8 in FP32 (the fastest at
+// 2048 x 256 on a B200: FP64 0.365 / 0.376 ms a step with 16 / 8 rows, FP32
+// 0.305 / 0.301 ms).
+inline int gs_tile_rows(const vvm_gpu_ctx* c) {
+    return c->tune_gs_tr ? c->tune_gs_tr : (c->mixed ? kGSTileRowsDefault : 2 * kGSTileRowsDefault);
+}
 
 template <typename T>
 void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops = nullptr) {

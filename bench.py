@@ -134,8 +134,9 @@ def class_bytes(cls: str, launches: int, grid, elem: int, cg_iters: float) -> fl
         "apply": 8 * cells * elem,         # 4 fields in place
         "kessler": 12 * cells * elem,      # 4 in, 4 out, 4 rates out
         "rkm": 5 * cells * elem,           # u w thp in; RKM RKH out
-        "gs": 6 * cells * elem,            # 5 fields in place + RKM RKH, over the
-                                           # coefficient pass and the recurrence
+        "gs": 12 * cells * elem,           # per STEP, not per launch: 5 fields read
+                                           # and written in place + RKM, RKH (the
+                                           # tile passes' count varies, 3 typical)
         "cal_u": 3 * cells * elem / 2,     # w zetap in, u out (two launches)
     }
     if cls in per_launch:
@@ -193,9 +194,14 @@ def run_variant(torch, precision, solver, steps, warmup, flush, device):
     return g, st, times, launches, prof, it, rel
 
 
-def roofline(prof, grid, elem, hbm, peak_kind, iters_per_step):
+PER_STEP_CLASSES = ("gs",)   # byte model per step: the launches a step vary
+
+
+def roofline(prof, grid, elem, hbm, peak_kind, iters_per_step, steps=2):
+    """The dominant kernel class over `steps` profiled steps: algorithmic bytes
+    over its event-timed device time."""
     cls, (ms, n) = max(prof.items(), key=lambda kv: kv[1][0])
-    nbytes = class_bytes(cls, n, grid, elem, iters_per_step * 2)
+    nbytes = class_bytes(cls, steps if cls in PER_STEP_CLASSES else n, grid, elem, iters_per_step * 2)
     achieved = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
     traffic = None
     tf = REPO / "profiles" / "roofline_traffic.txt"
@@ -204,10 +210,14 @@ def roofline(prof, grid, elem, hbm, peak_kind, iters_per_step):
             f = ln.split()
             if len(f) >= 3 and f[0] == cls and f[1] == ("fp32" if elem == 4 else "fp64"):
                 traffic = float(f[2])
+    per_step = cls in PER_STEP_CLASSES
     return {"kernel": cls, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None, "peak_source": peak_kind,
             "algorithmic_bytes_per_launch": nbytes / max(n, 1), "avg_launch_us": 1e3 * ms / max(n, 1),
-            "launches": n, "traffic": traffic}
+            "launches": n, "traffic": traffic,
+            "per": "step" if per_step else "launch",
+            "algorithmic_bytes_per_step": nbytes / steps if per_step else None,
+            "us_per_step": 1e3 * ms / steps}
 
 
 def cpu_baseline(sample_s=10.0):

@@ -293,8 +293,8 @@ int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back);
  * gs_tile_rows sets the rows of a Gauss-Seidel tile (4, 8, 16, 32; each tile
  * is 128 columns and one warp, and the passes run to the same fixed point
  * whatever its height), fft_threads sets the threads of a row-FFT block of
- * the spectral solve; 0 selects the automatic value (8 rows; 512 threads or
- * half the row). Setting them drops the context's captured graphs. get
+ * the spectral solve; 0 selects the automatic value (16 rows in FP64, 8 in
+ * the mixed step; 512 threads or half the row). Setting them drops the context's captured graphs. get
  * returns the values in use. */
 int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_tile_rows, int fft_threads);
 int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_tile_rows, int* fft_threads);
