@@ -689,9 +689,12 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
 //   right[q][f][b][c][r]   y at the tile's last column, rows r = 0..tr-1
 //   top[q][f][b][c][col]   y of the tile's top row, col = 0..127
 // The last block of a pass (a thread-fence and counter, no waiting) decides
-// whether another pass follows, and sets the graph's WHILE condition when the
-// passes run as a conditional node; the last pass of a sweep resets the pass
-// state for the next one (the host also clears it before each sweep).
+// whether another pass follows, and sets the condition of the graph's WHILE
+// node when the passes run in a graph; the last pass of a sweep resets the
+// pass state for the next one (the host also clears it before each sweep). A
+// later pass launched after the sweep converged returns at once, so a graph
+// runs the typical count unconditionally and enters its WHILE node only when
+// more passes are needed.
 
 template <typename T>
 struct GSArgs {
@@ -702,7 +705,9 @@ struct GSArgs {
     const T *RKM, *RKH;
     int mask;         // bit f: diffuse field f
     int nudge;        // fuse Nudge_theta (field 1) and Nudge_zeta (field 0)
-    T* A0;            // per-cell constant term, [5][cells] (written by pass 1)
+    T* A0;            // per-cell constant term, [5][cells] (written by pass 1 / k_gs_coeffs)
+    T *C, *B;         // per-cell lower and left coefficients (the cluster schedule only)
+    int* err;         // device error word (kGSErrWait, the cluster schedule), may be null
 };
 
 constexpr int kGSMaxNX = 8192;
@@ -776,6 +781,8 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
     if (threadIdx.x == 0) any_changed = 0;
     __syncthreads();
     constexpr bool first = FIRST;
+    // a pass launched after the sweep converged has nothing to do
+    if (!FIRST && !*(volatile int*)&t.ctl->more) return;
     const int pass = FIRST ? 1 : t.ctl->pass + 1;
     const int q = pass & 1, qp = q ^ 1;
     const int tile = blockIdx.x * 4 + wid;
@@ -1062,6 +1069,413 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
             if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// The second schedule of the same recurrence: one thread-block cluster a field.
+// k_gs_coeffs forms A0, C, B for every cell of the five fields in parallel;
+// k_gs_cluster then runs the recurrence, one cluster per field. Row k is a
+// first-order linear recurrence along i (v'(0,k) the untouched ghost), solved
+// as a scan of affine maps: each thread composes the maps of its PER
+// contiguous cells and the warp scans those with shuffles; warps pass the
+// carry along the row to the next warp, so consecutive warps work on
+// consecutive rows at the same time (a wavefront across the cluster). One
+// pass and no repeated arithmetic: the schedule for many cases stepping at
+// once (a batch), where the GPU is busy with other cases while a cluster's
+// chain runs; the tiles are for one case alone, where the chain is the
+// step's critical path. Results agree with the tiles' to round-off (the
+// carries associate differently).
+
+// A0, C, B of cell (i, k) of field blockIdx.z, i = 0..pitch-1, k = 1..nz-2
+// (Turbulent.cpp:83-88 for zeta, :107-112 for the scalars). The ghost i = 0
+// gets the constant map v'(0, k) = v(0, k) (never updated), cells beyond
+// NX the identity map, so a row's scan needs no edge cases.
+template <typename T>
+__global__ void k_gs_coeffs(GSArgs<T> a) {
+    const int f = blockIdx.z;
+    if (!(a.mask & (1 << f))) return;
+    const Dims& d = a.d;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= d.pitch || k > d.nz - 2) return;
+    const T* v = a.v[f];
+    if (i == 0 || i > d.nx - 2) {
+        const size_t e = (size_t)f * d.cells() + d.at(i, k);
+        a.A0[e] = (i == 0) ? v[d.at(0, k)] : T(0);
+        a.C[e] = T(0);
+        a.B[e] = (i == 0) ? T(0) : T(1);
+        return;
+    }
+    const bool mom = (f == 0);
+    const T* K = mom ? a.RKM : a.RKH;
+    const T cx = T(a.c.rdx2 * a.c.dt);
+    const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
+    T v0 = v[d.at(i, k)], vr = v[d.at(i + 1, k)], vu = v[d.at(i, k + 1)];
+    T ax, bx, czu, czd;
+    if (mom) {
+        T Kc = K[d.at(i, k)], Kd = K[d.at(i, k - 1)], Kl = K[d.at(i - 1, k)], Kld = K[d.at(i - 1, k - 1)];
+        ax = T(0.5) * (Kc + Kd);
+        bx = T(0.5) * (Kl + Kld);
+        czu = T(a.p.rhou[k]) * T(0.5) * (Kc + Kl);
+        czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd + Kld);
+    } else {
+        T Kc = K[d.at(i, k)], Kr = K[d.at(i + 1, k)], Kl = K[d.at(i - 1, k)];
+        T Ku = K[d.at(i, k + 1)], Kd = K[d.at(i, k - 1)];
+        ax = T(0.5) * (Kr + Kc);
+        bx = T(0.5) * (Kc + Kl);
+        czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku + Kc);
+        czd = T(a.p.rhow[k]) * T(0.5) * (Kc + Kd);
+    }
+    T du = vu - v0, dd = v0;
+    if (kPert<T> && (f == 1 || f == 2)) {   // th', qv' about a profile
+        du += T(a.p.d0[f - 1][k + 1]);
+        dd += T(a.p.d0[f - 1][k]);
+    }
+    // v + cx (ax (vr - v) - bx (v - v'[i-1])) + cz (czu du - czd (dd - v'below))
+    const size_t e = (size_t)f * d.cells() + d.at(i, k);
+    a.A0[e] = v0 + cx * (ax * (vr - v0) - bx * v0) + cz * (czu * du - czd * dd);
+    a.C[e] = cz * czd;
+    a.B[e] = cx * bx;
+}
+
+// cp.async helpers: 16-byte global -> shared copies, grouped per row.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+constexpr int kGSSpinLimit = 1 << 22;   // polls before a wait gives up
+constexpr int kGSErrWait = 1;           // device error word: a Gauss-Seidel wait gave up
+constexpr size_t kGSRingBytes = 200 * 1024;   // cp.async ring of coefficient rows
+constexpr int kGSCarry = 64;            // inbox slots (rows) of a warp
+constexpr int kGSAckEvery = 16;         // rows between acknowledgements
+
+// Flags between CTAs of a cluster: acquire / release at cluster scope through
+// generic addresses (local shared memory, or a peer CTA's mapped into the
+// cluster window).
+__device__ __forceinline__ int ld_acquire_cluster(const int* p) {
+    int v;
+    asm volatile("ld.acquire.cluster.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cluster(int* p, int v) {
+    asm volatile("st.release.cluster.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_cluster_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.cluster.b64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_cluster_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.cluster.b64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// A carry travels as row-tagged 64-bit words: (row << 32) | 32 bits of the
+// value (one word for float, two for double). A 64-bit store is seen whole,
+// so a reader that finds its row in every word holds that row's value; no
+// flag and no fence is needed.
+template <typename T>
+struct Tagged {
+    static constexpr int kWords = sizeof(T) / 4;
+    __device__ static void put(unsigned long long* w, T x, int row) {
+        const unsigned long long tag = (unsigned long long)(unsigned)row << 32;
+        if constexpr (sizeof(T) == 4) {
+            st_relaxed_cluster_u64(w, tag | __float_as_uint(x));
+        } else {
+            const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+            st_relaxed_cluster_u64(w, tag | (b >> 32));
+            st_relaxed_cluster_u64(w + 1, tag | (b & 0xffffffffull));
+        }
+    }
+    // true and x set when every word carries `row`
+    __device__ static bool get(const unsigned long long* w, int row, T& x) {
+        const unsigned long long w0 = ld_relaxed_cluster_u64(w);
+        if ((int)(w0 >> 32) != row) return false;
+        if constexpr (sizeof(T) == 4) {
+            x = __uint_as_float((unsigned)w0);
+        } else {
+            const unsigned long long w1 = ld_relaxed_cluster_u64(w + 1);
+            if ((int)(w1 >> 32) != row) return false;
+            x = __longlong_as_double((long long)((w0 << 32) | (w1 & 0xffffffffull)));
+        }
+        return true;
+    }
+};
+
+// The recurrence of one field spread over a cluster of CS CTAs. The padded
+// row is cut into chunks of 32*PER cells, one per warp; global warp g sits in
+// CTA g / W as its warp g % W (W warps a CTA). Each warp walks the rows in
+// order on its own: it waits for the carry-in that warp g-1 left, row-tagged,
+// in its own inbox (written locally, or into this CTA's shared memory from
+// the previous CTA through the cluster window), acknowledges every
+// kGSAckEvery-th row in warp g-1's shared memory (a release store, so its
+// reads of the inbox come first), and, once warp g+1 has acknowledged the row
+// that last used the inbox slot it is about to reuse, writes its carry-out
+// into warp g+1's inbox. Everything is polled in local shared memory. Cluster barriers open (all inboxes
+// initialised before any peer writes) and close (no CTA exits while a peer may
+// still write into it) the kernel. Each wait polls at most kGSSpinLimit
+// times; a warp that gives up raises the abort flag of every CTA of the
+// cluster and the device error word, so every wait ends. Coefficient rows are
+// staged in shared memory by cp.async, D rows ahead (a thread reads back only
+// what it copied); the rows' nudging scalars are tabulated in shared memory at
+// the start. Dynamic shared memory: D * 3 * blockDim.x * PER values of T, then
+// 2 * nz values of T.
+constexpr int kGSClusterWarps = 10;   // warps a CTA at most (NX = 8192: 9)
+
+// The carry of a row pair: two row-tagged values (the pair's first row as tag).
+template <typename T>
+struct Tagged2 {
+    static constexpr int kWords = 2 * Tagged<T>::kWords;
+    __device__ static void put(unsigned long long* w, T x0, T x1, int row) {
+        Tagged<T>::put(w, x0, row);
+        Tagged<T>::put(w + Tagged<T>::kWords, x1, row);
+    }
+    __device__ static bool get(const unsigned long long* w, int row, T& x0, T& x1) {
+        return Tagged<T>::get(w, row, x0) && Tagged<T>::get(w + Tagged<T>::kWords, row, x1);
+    }
+};
+
+// Two rows a step. With V_i = (v'(i, k), v'(i, k+1)) the pair obeys
+// V_i = alpha_i + M_i V_{i-1}, M_i = [[B_k, 0], [C_{k+1} B_k, B_{k+1}]],
+// alpha_i = (a_i, A0_{k+1} + C_{k+1} a_i), a_i = A0_k + C_k v'(i, k-1): one scan
+// over the row advances both rows, so the serial chain has half as many
+// steps, each with five values a shuffle round instead of two (the rounds'
+// shuffles are independent and overlap). The cells are then applied with the
+// scalar formulas, row k first. An odd last row runs as a pair whose second
+// row is the identity and is not stored.
+template <typename T, int PER, int D, int CS>
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(32 * kGSClusterWarps) k_gs_cluster(GSArgs<T> a) {
+    static_assert(D % 2 == 0, "the ring holds whole row pairs");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int kW = Tagged2<T>::kWords;
+    __shared__ unsigned long long inbox[kGSClusterWarps][kGSCarry][kW];
+    __shared__ int ack_in[kGSClusterWarps], abort_flag;
+    namespace cgx = cooperative_groups;
+    cgx::cluster_group cl = cgx::this_cluster();
+    const int crank = (int)cl.block_rank();
+    const int f = blockIdx.x / CS;
+    const Dims& d = a.d;
+    const int NX = d.nx - 2, kend = d.nz - 2;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, W = blockDim.x >> 5;
+    for (int j = tid; j < kGSClusterWarps * kGSCarry * kW; j += blockDim.x)
+        (&inbox[0][0][0])[j] = 0ull;    // tag 0: no row
+    if (tid < kGSClusterWarps) ack_in[tid] = 0;
+    if (tid == 0) abort_flag = 0;
+    // nudging of row k: out = x - dn[k] (x - tn[k]) (dn = 0: none)
+    T* dn_tab = reinterpret_cast<T*>(smem_raw) + (size_t)D * 3 * blockDim.x * PER;
+    T* tn_tab = dn_tab + d.nz;
+    for (int k = tid; k < d.nz; k += blockDim.x) {
+        T dn = T(0), tn = T(0);
+        if (a.nudge && f == 0) dn = T(a.p.dtcgr_zeta[k]);                      // Nudge_zeta
+        if (a.nudge && f == 1) {                                                 // Nudge_theta
+            dn = T(a.p.dtcgr_th[k]);
+            tn = kPert<T> ? T(-a.p.dn[0][k]) : T(a.p.thb_init[k]);
+        }
+        dn_tab[k] = dn;
+        tn_tab[k] = tn;
+    }
+    cl.sync();
+    const int gwn = (d.pitch + 32 * PER - 1) / (32 * PER);   // warps with cells
+    const int g = crank * W + wid;
+    const bool run = (a.mask & (1 << f)) && g < gwn;
+    if (run) {
+        T* v = a.v[f];
+        const int i0 = (g * 32 + lane) * PER;
+        const bool act = i0 < d.pitch;       // pitch is a multiple of PER
+        const size_t fo = (size_t)f * d.cells();
+        const T* gsrc[3] = {a.A0 + fo, a.C + fo, a.B + fo};
+        T* ring = reinterpret_cast<T*>(smem_raw);
+        constexpr int kVec = 16 / sizeof(T);
+        auto slot = [&](int r, int arr) { return ring + ((size_t)(r * 3 + arr) * blockDim.x + tid) * PER; };
+        auto issue = [&](int k, int r) {
+            if (act && k <= kend) {
+#pragma unroll
+                for (int arr = 0; arr < 3; arr++) {
+                    const T* src = gsrc[arr] + d.at(i0, k);
+                    T* dst = slot(r, arr);
+#pragma unroll
+                    for (int q = 0; q < PER; q += kVec) cp_async16(dst + q, src + q);
+                }
+            }
+            cp_async_commit();
+        };
+        // neighbours in the chain and their flags
+        const bool has_pred = g > 0, has_succ = g + 1 < gwn;
+        const int pc = (g - 1) / W, pw = (g - 1) % W, sc = (g + 1) / W, sw = (g + 1) % W;
+        int* pred_ack = has_pred ? cl.map_shared_rank(&ack_in[pw], pc) : nullptr;
+        unsigned long long* succ_box = has_succ ? cl.map_shared_rank(&inbox[sw][0][0], sc) : nullptr;
+        auto give_up = [&]() {   // lane 0 of a warp whose wait ran out: stop the cluster
+            for (int r = 0; r < CS; r++) *(volatile int*)cl.map_shared_rank(&abort_flag, r) = 1;
+            if (a.err) atomicOr(a.err, kGSErrWait);
+        };
+        auto wait_carry = [&](int k, T& x0, T& x1) {   // all lanes; warp-uniform result
+            bool okw = false;
+            const unsigned long long* w = &inbox[wid][k % kGSCarry][0];
+            for (int it = 0; it < kGSSpinLimit; it++) {
+                if (Tagged2<T>::get(w, k, x0, x1)) {
+                    okw = true;
+                    break;
+                }
+                if (*(volatile int*)&abort_flag) break;
+            }
+            const bool all = __all_sync(0xffffffffu, okw);
+            if (!all && lane == 0 && !*(volatile int*)&abort_flag) give_up();
+            return all;
+        };
+        auto wait_ge = [&](const int* p, int target) {   // all lanes; warp-uniform result
+            bool okw = false;
+            for (int it = 0; it < kGSSpinLimit; it++) {
+                if (ld_acquire_cluster(p) >= target) {
+                    okw = true;
+                    break;
+                }
+                if (*(volatile int*)&abort_flag) break;
+            }
+            const bool all = __all_sync(0xffffffffu, okw);
+            if (!all && lane == 0 && !*(volatile int*)&abort_flag) give_up();
+            return all;
+        };
+        T vdn[PER];
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+            const int i = i0 + e;
+            vdn[e] = (act && i >= 1 && i <= NX) ? v[d.at(i, 0)] : T(0);
+        }
+#pragma unroll
+        for (int r = 0; r < D; r++) issue(1 + r, r);
+        bool ok = true;
+        int ack_seen = 0;   // last acknowledgement read from warp g+1
+        auto pair = [&](int k, int r) {   // rows k and k+1 (k+1 may be past the last row)
+            const bool two = k + 1 <= kend;
+            const T dn0 = dn_tab[k], tn0 = tn_tab[k];
+            const T dn1 = two ? dn_tab[k + 1] : T(0), tn1 = two ? tn_tab[k + 1] : T(0);
+            const int s = k % kGSCarry;
+            // read the carry-in early: when warp g-1 is ahead it is there
+            T x0 = T(0), x1 = T(0);   // warp 0 starts at the ghost's constant map
+            bool have = !has_pred || Tagged2<T>::get(&inbox[wid][s][0], k, x0, x1);
+            cp_async_wait<D - 2>();
+            T Aa[PER], Bk[PER], A2[PER], C2[PER], B2[PER];
+            if (act) {
+                const T* sa = slot(r, 0);
+                const T* scc = slot(r, 1);
+                const T* sb = slot(r, 2);
+                const T* ta = slot(r + 1, 0);
+                const T* tc = slot(r + 1, 1);
+                const T* tb = slot(r + 1, 2);
+#pragma unroll
+                for (int e = 0; e < PER; e++) {
+                    Aa[e] = sa[e] + scc[e] * vdn[e];
+                    Bk[e] = sb[e];
+                    A2[e] = two ? ta[e] : T(0);
+                    C2[e] = two ? tc[e] : T(0);
+                    B2[e] = two ? tb[e] : T(1);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < PER; e++) {
+                    Aa[e] = T(0);
+                    Bk[e] = T(1);
+                    A2[e] = T(0);
+                    C2[e] = T(0);
+                    B2[e] = T(1);
+                }
+            }
+            // the lane's map over its cells: (p0, p1) offsets, M = [[m00, 0], [m10, m11]]
+            T p0 = T(0), p1 = T(0), m00 = T(1), m10 = T(0), m11 = T(1);
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+                const T c0 = Aa[e], c1 = A2[e] + C2[e] * Aa[e];
+                const T n00 = Bk[e], n10 = C2[e] * Bk[e], n11 = B2[e];
+                p1 = c1 + n10 * p0 + n11 * p1;
+                p0 = c0 + n00 * p0;
+                m10 = n10 * m00 + n11 * m10;
+                m00 = n00 * m00;
+                m11 = n11 * m11;
+            }
+            issue(k + D, r);
+            issue(k + 1 + D, r + 1);
+            T s0 = p0, s1 = p1, s00 = m00, s10 = m10, s11 = m11;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T q0 = __shfl_up_sync(0xffffffffu, s0, o), q1 = __shfl_up_sync(0xffffffffu, s1, o);
+                const T q00 = __shfl_up_sync(0xffffffffu, s00, o), q10 = __shfl_up_sync(0xffffffffu, s10, o);
+                const T q11 = __shfl_up_sync(0xffffffffu, s11, o);
+                if (lane >= o) {   // own map after the lower lanes'
+                    s1 = s1 + s10 * q0 + s11 * q1;
+                    s0 = s0 + s00 * q0;
+                    s10 = s10 * q00 + s11 * q10;
+                    s00 = s00 * q00;
+                    s11 = s11 * q11;
+                }
+            }
+            const T t0 = __shfl_sync(0xffffffffu, s0, 31), t1 = __shfl_sync(0xffffffffu, s1, 31);
+            const T t00 = __shfl_sync(0xffffffffu, s00, 31), t10 = __shfl_sync(0xffffffffu, s10, 31);
+            const T t11 = __shfl_sync(0xffffffffu, s11, 31);
+            T e0 = __shfl_up_sync(0xffffffffu, s0, 1), e1 = __shfl_up_sync(0xffffffffu, s1, 1);
+            T e00 = __shfl_up_sync(0xffffffffu, s00, 1), e10 = __shfl_up_sync(0xffffffffu, s10, 1);
+            T e11 = __shfl_up_sync(0xffffffffu, s11, 1);
+            if (lane == 0) {
+                e0 = T(0);
+                e1 = T(0);
+                e00 = T(1);
+                e10 = T(0);
+                e11 = T(1);
+            }
+            if (has_pred) {
+                if (!__all_sync(0xffffffffu, have)) ok = ok && wait_carry(k, x0, x1);
+                if (((k - 1) >> 1) % (kGSAckEvery / 2) == 0) {   // every kGSAckEvery rows
+                    __syncwarp();
+                    if (lane == 0) st_release_cluster(pred_ack, k);
+                }
+            }
+            if (has_succ) {
+                // slot s last held the pair at row k - kGSCarry
+                if (ack_seen < k - kGSCarry) {
+                    ok = ok && wait_ge(&ack_in[wid], k - kGSCarry);
+                    ack_seen = ld_acquire_cluster(&ack_in[wid]);
+                }
+                if (lane == 0) Tagged2<T>::put(succ_box + (size_t)s * kW, t0 + t00 * x0, t1 + t10 * x0 + t11 * x1, k);
+            }
+            T y0 = e0 + e00 * x0, y1 = e1 + e10 * x0 + e11 * x1;
+            T out0[PER], out1[PER];
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+                y0 = Aa[e] + Bk[e] * y0;
+                y1 = (A2[e] + C2[e] * y0) + B2[e] * y1;
+                vdn[e] = y1;
+                out0[e] = y0 - dn0 * (y0 - tn0);
+                out1[e] = y1 - dn1 * (y1 - tn1);
+            }
+            auto store = [&](int kk, const T (&out)[PER]) {
+                T* dst = v + d.at(i0, kk);
+                if (act && i0 >= 1 && i0 + PER - 1 <= NX) {
+#pragma unroll
+                    for (int q = 0; q < PER; q += kVec) {
+                        if constexpr (sizeof(T) == 4)
+                            *reinterpret_cast<float4*>(dst + q) = make_float4(out[q], out[q + 1], out[q + 2], out[q + 3]);
+                        else
+                            *reinterpret_cast<double2*>(dst + q) = make_double2(out[q], out[q + 1]);
+                    }
+                } else if (act) {
+#pragma unroll
+                    for (int e = 0; e < PER; e++)
+                        if (i0 + e >= 1 && i0 + e <= NX) dst[e] = out[e];
+                }
+            };
+            store(k, out0);
+            if (two) store(k + 1, out1);
+        };
+        for (int k = 1; k <= kend && ok; k += D) {
+#pragma unroll
+            for (int r = 0; r < D; r += 2)
+                if (k + r <= kend && ok) pair(k + r, r);
+        }
+        cp_async_wait<0>();
+    }
+    cl.sync();
 }
 
 // ---------------------------------------------------------------------------

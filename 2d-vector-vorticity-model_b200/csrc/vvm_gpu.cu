@@ -1384,6 +1384,7 @@ struct Fields {
     T *d_auto = nullptr, *d_accr = nullptr, *d_evap = nullptr, *d_cond = nullptr;
     T *precip = nullptr, *th_forcing = nullptr;
     T* gsA = nullptr;                                   // Gauss-Seidel constant terms, [5][cells]
+    T *gsC = nullptr, *gsB = nullptr;                   // and coefficients (cluster schedule; on first use)
     T *gsRight = nullptr, *gsTop = nullptr;             // Gauss-Seidel tile outflows (k_gs_tiles)
 };
 
@@ -1465,6 +1466,7 @@ struct vvm_gpu_ctx {
     cudaStream_t cap[2] = {};          // streams for capturing loop bodies
     CGCtl* wctl = nullptr;             // outer loop state of the mixed solve
     long long* d_exec = nullptr;       // kernels executed inside graph loops
+    int* d_err = nullptr;              // device error word (kGSErrWait), checked when the host syncs
     bool last_graph = false;           // the last cal_w ran inside a graph
     bool graphs_off = false;
     float *g32 = nullptr, *d32 = nullptr;
@@ -1706,12 +1708,101 @@ struct BodyCapture {   // stream capture into a conditional node's body graph
     }
 };
 
-// Automatic tile height: 16 rows in FP64, 8 in FP32 (the fastest at
+// The cluster schedule's launch shape for a padded row of `pitch` cells of
+// `elem` bytes: chunks of 32*kGSPer cells (one warp each) over a cluster of cs
+// CTAs of w warps, coefficient rows d ahead.
+constexpr int kGSPer = 4;
+struct GSPlan {
+    int cs, w, d;
+    size_t smem;
+};
+inline GSPlan gs_plan(int pitch, int nz, size_t elem) {
+    GSPlan p{};
+    const int gwn = cdiv(pitch, 32 * kGSPer);
+    p.cs = gwn >= 8 ? 8 : (gwn >= 4 ? 4 : (gwn >= 2 ? 2 : 1));
+    p.w = cdiv(gwn, p.cs);   // <= kGSClusterWarps for pitch <= 8224 (checked at create)
+    const size_t row = 3 * (size_t)p.w * 32 * kGSPer * elem;
+    const size_t tab = 2 * (size_t)nz * elem;   // nudging scalars
+    p.d = (8 * row + tab <= kGSRingBytes) ? 8 : (4 * row + tab <= kGSRingBytes ? 4 : 2);
+    p.smem = p.d * row + tab;
+    return p;
+}
+
+template <typename T, int D, int CS>
+void gs_launch(vvm_gpu_ctx* c, const GSArgs<T>& g, const GSPlan& p) {
+    LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_cluster<T, kGSPer, D, CS><<<5 * CS, 32 * p.w, p.smem, c->stream>>>(g));
+}
+
+template <typename T, int D>
+void gs_launch_d(vvm_gpu_ctx* c, const GSArgs<T>& g, const GSPlan& p) {
+    if (p.cs == 8) gs_launch<T, D, 8>(c, g, p);
+    else if (p.cs == 4) gs_launch<T, D, 4>(c, g, p);
+    else if (p.cs == 2) gs_launch<T, D, 2>(c, g, p);
+    else gs_launch<T, D, 1>(c, g, p);
+}
+
+template <typename T, int D>
+void gs_set_smem_d() {
+    const int mx = (int)kGSRingBytes;
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    CK(cudaFuncSetAttribute(k_gs_cluster<T, kGSPer, D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+}
+
+template <typename T>
+void gs_set_smem() {
+    gs_set_smem_d<T, 8>();
+    gs_set_smem_d<T, 4>();
+    gs_set_smem_d<T, 2>();
+}
+
+// The cluster schedule's coefficient arrays and shared-memory limits, made
+// when the schedule is chosen (never during a graph capture).
+template <typename T>
+void ensure_gs_cluster_t(vvm_gpu_ctx* c) {
+    Fields<T>& F = fields<T>(c);
+    if (F.gsC) return;
+    CK(cudaStreamSynchronize(c->stream));
+    F.gsC = c->ar.alloc<T>(5 * c->d.cells());
+    F.gsB = c->ar.alloc<T>(5 * c->d.cells());
+    gs_set_smem<T>();
+}
+inline void ensure_gs_cluster(vvm_gpu_ctx* c) {
+    if (c->mixed) ensure_gs_cluster_t<float>(c);
+    else ensure_gs_cluster_t<double>(c);
+}
+
+// The cluster schedule: coefficients, then one cluster a field (k_gs_cluster).
+template <typename T>
+void launch_gs_cluster(vvm_gpu_ctx* c, GSArgs<T> g) {
+    Fields<T>& F = fields<T>(c);
+    if (!F.gsC) throw CudaError{"Gauss-Seidel cluster schedule used before it was set up"};
+    g.C = F.gsC;
+    g.B = F.gsB;
+    g.err = c->d_err;
+    dim3 cb(64, 4), cgr(cdiv(c->d.pitch, 64), cdiv(c->d.nz - 2, 4), 5);
+    LAUNCH(&c->stats, VVM_K_GS, c->stream, k_gs_coeffs<T><<<cgr, cb, 0, c->stream>>>(g));
+    CKL();
+    const GSPlan p = gs_plan(c->d.pitch, c->d.nz, sizeof(T));
+    if (p.d == 8) gs_launch_d<T, 8>(c, g, p);
+    else if (p.d == 4) gs_launch_d<T, 4>(c, g, p);
+    else gs_launch_d<T, 2>(c, g, p);
+    CKL();
+}
+
+// Later Gauss-Seidel passes a step graph runs before its WHILE node (the
+// typical sweep is pass 1 and two more).
+constexpr int kGSGraphPasses = 2;
+// The Gauss-Seidel schedule: kGSSchedCluster (one cluster a field) or a tile
+// height. Automatic: tiles of 16 rows in FP64, 8 in FP32 (the fastest at
 // 2048 x 256 on a B200: FP64 0.365 / 0.376 ms a step with 16 / 8 rows, FP32
-// 0.305 / 0.301 ms).
+// 0.305 / 0.301 ms); a batch's autotuner also tries the cluster schedule.
+constexpr int kGSSchedCluster = 1;
 inline int gs_tile_rows(const vvm_gpu_ctx* c) {
     return c->tune_gs_tr ? c->tune_gs_tr : (c->mixed ? kGSTileRowsDefault : 2 * kGSTileRowsDefault);
 }
+inline bool gs_schedule_ok(int v) { return v == 0 || v == kGSSchedCluster || gs_tile_rows_ok(v); }
 
 template <typename T>
 void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops = nullptr) {
@@ -1721,7 +1812,11 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops 
     LAUNCH(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r));
     CKL();
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
-                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA};
+                F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, nullptr, nullptr, nullptr};
+    if (c->tune_gs_tr == kGSSchedCluster) {
+        launch_gs_cluster<T>(c, g);
+        return;
+    }
     // the recurrence: tiles and passes (see k_gs_tiles)
     const int tr = gs_tile_rows(c);
     const int nb = cdiv(c->d.nz - 2, tr), nc = cdiv(c->d.pitch, kGTCols);
@@ -1732,12 +1827,22 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops 
     CK(cudaMemsetAsync(c->gsctl, 0, sizeof(GSTileCtl), st));   // a fresh sweep
     LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T, true><<<tblocks, 128, 0, st>>>(g, t, 0));   // pass 1
     CKL();
-    if (recorded_in_loops) {   // graph capture: passes 2.. as a WHILE node, entered every launch
+    if (recorded_in_loops) {
+        // graph capture: the typical passes 2..kGSGraphPasses+1 unconditionally
+        // (each returns at once if the sweep already converged, and the last
+        // block of each sets the condition below), then a WHILE node that runs
+        // further passes only when they are needed
         cudaStreamCaptureStatus status;
         cudaGraph_t cg;
         CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &cg, nullptr, nullptr));
         cudaGraphConditionalHandle h;
-        CK(cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault));
+        CK(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+        GSTileArgs<T> tu = t;
+        tu.exec = nullptr;   // counted with the graph's static kernels
+        for (int p = 0; p < kGSGraphPasses; p++) {
+            LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T, false><<<tblocks, 128, 0, st>>>(g, tu, h));
+            CKL();
+        }
         cudaGraph_t body = add_while(st, h);
         BodyCapture bc(c->cap[0], body);
         const long long n0 = c->stats.launches;
@@ -2595,6 +2700,7 @@ int batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
     auto set_all = [&](const std::vector<int>& idx, int tr, int fft) {
         for (int i : idx) {
             vvm_gpu_ctx* c = b->cases[i];
+            if (tr == kGSSchedCluster) ensure_gs_cluster(c);
             c->tune_gs_tr = tr;
             c->tune_fft = fft;
             apply_tuning(c);
@@ -2605,7 +2711,7 @@ int batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
         vvm_gpu_ctx* c = b->cases[idx[0]];
         int best_cs = c->tune_gs_tr, best_fft = c->tune_fft;
         double best = batch_time(b, idx, reps);
-        for (int tr : {4, 8, 16, 32}) {   // rows of a Gauss-Seidel tile
+        for (int tr : {kGSSchedCluster, 4, 8, 16, 32}) {   // Gauss-Seidel schedule: cluster, tile rows
             set_all(idx, tr, best_fft);
             const double t = batch_time(b, idx, reps);
             if (t < best) {
@@ -2988,6 +3094,18 @@ int need_uniform(vvm_gpu_ctx* c) {
 }
 
 
+// Reads and clears the device error word (after the stream's work is done).
+int device_errors(vvm_gpu_ctx* c) {
+    if (!c->d_err) return VVM_GPU_OK;
+    int h = 0;
+    CK(cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!h) return VVM_GPU_OK;
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return fail(c, VVM_GPU_ECUDA, "Gauss-Seidel diffusion (cluster schedule): a wait between warps gave up; "
+                                  "the state is invalid");
+}
+
 }  // namespace
 
 // Message of a failed context-free entry, returned by vvm_gpu_last_error(NULL, ...).
@@ -3025,7 +3143,8 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     *out = nullptr;
     const vvm_gpu_desc& D = *desc;
     if (D.NX < 4 || D.NZ < 4) return fail(nullptr, VVM_GPU_EINVAL, "create: NX and NZ must be >= 4");
-    if (D.NX > kGSMaxNX) return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
+    if (D.NX > kGSMaxNX || gs_plan(round_up(D.NX + 2, kPad), D.NZ + 2, 8).w > kGSClusterWarps)
+        return fail(nullptr, VVM_GPU_EINVAL, "create: NX exceeds 8192");
     if (D.NZ - 1 > 32 * kMaxSeg)
         return fail(nullptr, VVM_GPU_EINVAL, "create: NZ exceeds 1025");
     {
@@ -3098,6 +3217,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         c->staging = c->ar.alloc<double>((size_t)c->d.nx * c->d.nz * 2);
         c->wctl = c->ar.alloc<CGCtl>(1);
         c->d_exec = c->ar.alloc<long long>(1);
+        c->d_err = c->ar.alloc<int>(1);
         for (auto& cs : c->cap) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     } catch (const CudaError& e) {
         cudaSetDevice(prev);
@@ -3128,7 +3248,7 @@ int vvm_gpu_set_stream(vvm_gpu_ctx* ctx, void* stream) {
 int vvm_gpu_synchronize(vvm_gpu_ctx* ctx) {
     return guarded(ctx, [&] {
         CK(cudaStreamSynchronize(ctx->stream));
-        return VVM_GPU_OK;
+        return device_errors(ctx);
     });
 }
 
@@ -3163,7 +3283,8 @@ int vvm_gpu_download_state(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
     if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
     return guarded(ctx, [&] {
         if (int rc = need_state(ctx)) return rc;
-        return DISPATCH(ctx, download_state_t)(ctx, st);
+        if (int rc = DISPATCH(ctx, download_state_t)(ctx, st)) return rc;
+        return device_errors(ctx);
     });
 }
 
@@ -3176,7 +3297,8 @@ int vvm_gpu_download_prognostic(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st) {
     if (!st) return fail(ctx, VVM_GPU_EINVAL, "download: NULL state");
     return guarded(ctx, [&] {
         if (int rc = need_state(ctx)) return rc;
-        return DISPATCH(ctx, download_prognostic_t)(ctx, st);
+        if (int rc = DISPATCH(ctx, download_prognostic_t)(ctx, st)) return rc;
+        return device_errors(ctx);
     });
 }
 
@@ -3634,10 +3756,11 @@ int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back) {
 
 int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_tile_rows, int fft_threads) {
     if (!ctx) return VVM_GPU_EINVAL;
-    if ((gs_tile_rows != 0 && !gs_tile_rows_ok(gs_tile_rows)) || fft_threads < 0 || fft_threads > 1024)
+    if (!gs_schedule_ok(gs_tile_rows) || fft_threads < 0 || fft_threads > 1024)
         return fail(ctx, VVM_GPU_EINVAL, "set_tuning: knob out of range");
     return guarded(ctx, [&]() -> int {
         CK(cudaStreamSynchronize(ctx->stream));
+        if (gs_tile_rows == kGSSchedCluster) ensure_gs_cluster(ctx);
         ctx->tune_gs_tr = gs_tile_rows;
         ctx->tune_fft = fft_threads;
         apply_tuning(ctx);
@@ -3648,7 +3771,7 @@ int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_tile_rows, int fft_threads) {
 
 int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_tile_rows_out, int* fft_threads) {
     if (!ctx) return VVM_GPU_EINVAL;
-    if (gs_tile_rows_out) *gs_tile_rows_out = gs_tile_rows(ctx);
+    if (gs_tile_rows_out) *gs_tile_rows_out = gs_tile_rows(ctx);   // kGSSchedCluster: the cluster schedule
     if (fft_threads) {
         *fft_threads = 0;
         if (ctx->spectral) {
@@ -3730,6 +3853,7 @@ int vvm_gpu_batch_synchronize(vvm_gpu_batch* b) {
         for (size_t i = 0; i < b->cases.size(); i++) {
             vvm_gpu_ctx* c = b->cases[i];
             CK(cudaStreamSynchronize(c->stream));
+            if (int rc = device_errors(c)) return batch_fail(b, rc, "case " + std::to_string(i) + ": " + c->err);
         }
         return VVM_GPU_OK;
     });

@@ -420,7 +420,8 @@ class VVMGpu:
         return n.value
 
     def set_tuning(self, gs_tile_rows: int = 0, fft_threads: int = 0):
-        """Launch-shape knobs (0: automatic); results do not change."""
+        """Launch-shape knobs (0: automatic): the Gauss-Seidel schedule (tile
+        rows 4/8/16/32, or 1 for one cluster a field) and the row-FFT block."""
         self._check(self.L.vvm_gpu_set_tuning(self.h, int(gs_tile_rows), int(fft_threads)))
 
     def tuning(self) -> tuple[int, int]:

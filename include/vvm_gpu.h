@@ -289,12 +289,15 @@ int vvm_gpu_learned_time(vvm_gpu_ctx* ctx, int reps, double* ms_forward, double*
 int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back);
 
 /* -- launch-shape knobs --------------------------------------------------------
- * Neither changes any result (the arithmetic of every cell is the same):
- * gs_tile_rows sets the rows of a Gauss-Seidel tile (4, 8, 16, 32; each tile
- * is 128 columns and one warp, and the passes run to the same fixed point
- * whatever its height), fft_threads sets the threads of a row-FFT block of
- * the spectral solve; 0 selects the automatic value (16 rows in FP64, 8 in
- * the mixed step; 512 threads or half the row). Setting them drops the context's captured graphs. get
+ * gs_tile_rows selects the Gauss-Seidel schedule: 4, 8, 16 or 32 = tiles of
+ * that many rows (128 columns and one warp each; the passes run to the same
+ * fixed point whatever the height, so results are identical across heights);
+ * 1 = one thread-block cluster a field (a single pass, the schedule for many
+ * cases stepping at once; it agrees with the tiles to round-off, its carries
+ * associate differently). fft_threads sets the threads of a row-FFT block of
+ * the spectral solve (no result changes). 0 selects the automatic value
+ * (tiles of 16 rows in FP64, 8 in the mixed step; 512 threads or half the
+ * row). Setting them drops the context's captured graphs. get
  * returns the values in use. */
 int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_tile_rows, int fft_threads);
 int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_tile_rows, int* fft_threads);

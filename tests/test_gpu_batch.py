@@ -2,9 +2,12 @@
 
 A batch runs every case's step as a branch of one CUDA graph, with the same
 kernels a single context launches, so each case must come out bit for bit
-equal to the same case stepped on its own. The knobs the autotuner turns
-(Gauss-Seidel cluster size, row-FFT block) change no arithmetic, so results
-stay bit-identical under any setting, and the autotuner must leave every
+equal to the same case stepped on its own with the same knobs. The knobs
+the autotuner turns: the Gauss-Seidel schedule (tiles of 4 to 32 rows, or one
+cluster a field) and the row-FFT block. The tile heights and the FFT block
+change no arithmetic, so results stay bit-identical across them; the cluster
+schedule associates the recurrence's carries differently, so it agrees with
+the tiles to round-off (1e-13 relative). The autotuner must leave every
 case's state exactly as it found it.
 """
 import numpy as np
@@ -27,8 +30,10 @@ def _states(shapes):
     return [warm_bubble(nx, nz, 200.0, 200.0, radius=max(400.0, nx * 200 / 8)) for nx, nz in shapes]
 
 
-def _alone(G, st, n, precision, solver):
+def _alone(G, st, n, precision, solver, tuning=None):
     g = G.VVMGpu(st.grid, precision=precision, solver=solver)
+    if tuning is not None:
+        g.set_tuning(*tuning)
     g.upload(st)
     g.step(n)
     out = g.download()
@@ -71,11 +76,11 @@ def test_autotune_restores_state_and_keeps_results(gpu):
         assert _same(x, y)
     for c in b.cases:
         tr, fft = c.tuning()
-        assert tr in (4, 8, 16, 32) and fft in (128, 256, 512, 32, 64)
+        assert tr in (1, 4, 8, 16, 32) and fft in (128, 256, 512, 32, 64)
     b.step(4)
     b.synchronize()
     for st, c in zip(sts, b.cases):
-        assert _same(c.download(), _alone(gpu, st, 7, 1, 2))
+        assert _same(c.download(), _alone(gpu, st, 7, 1, 2, c.tuning()))
     b.close()
 
 
@@ -94,6 +99,17 @@ def test_knobs_leave_results_unchanged(gpu):
     with pytest.raises(gpu.VVMGpuError):
         g.set_tuning(12, 0)                  # not a tile height
     g.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_cluster_schedule_agrees_with_tiles(gpu, precision):
+    """The two Gauss-Seidel schedules, each exact to round-off, on 5 steps."""
+    from conftest import rel_l2
+    st = _states([(512, 48)])[0]
+    a = _alone(gpu, st, 5, precision, 2)
+    b = _alone(gpu, st, 5, precision, 2, (1, 0))
+    for f in PROG:
+        assert rel_l2(b.fields[f], a.fields[f]) <= (1e-13 if precision == 0 else 1e-6), f
 
 
 def test_batch_rejects_cases_at_different_steps(gpu):
