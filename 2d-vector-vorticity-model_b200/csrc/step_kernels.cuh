@@ -34,6 +34,17 @@ struct Profiles {
     // For each: d0[k] = ref[k] - ref[k-1], s0[k] = ref[k] + ref[k-1],
     // g0[k] = ref[k+1] - ref[k-1], dn[k] = ref[k] - (nudging target)[k].
     const double *ref[2], *d0[2], *s0[2], *g0[2], *dn[2];
+    // Vertical level metric (the reference's constants on uniform levels,
+    // exactly; see upload_profiles): flux divergences at centres (r2dzc =
+    // 1/(2 dc)) and faces (r2dzw = 1/(2 dw)), the w gradient across a centre
+    // (rdzc = 1/dc), gradients across two centres (r2dzcc = 1/(z[k+1]-z[k-1])),
+    // the eddy-coefficient cap (kmax = 0.8 dx dc / dt), the Gauss-Seidel
+    // vertical factors of Mparam (gsM_*) and Hparam (gsS_*): cz = rdz2_k dt /
+    // rho and the down term's density times its spacing ratio, and cal_u's
+    // centre-to-centre spacing (dzw) and top factor (hfac = dx / dc_top, 1 on
+    // uniform levels as the reference has it); pubarTop's top spacings.
+    const double *r2dzc, *r2dzw, *rdzc, *r2dzcc, *kmax, *gsM_cz, *gsM_rhod, *gsS_cz, *gsS_rhod, *dzw;
+    double rdz_up, rdz_dn, rdz_c, hfac;
 };
 
 // True for the mixed step, whose th and qv arrays hold perturbations.
@@ -152,7 +163,7 @@ __global__ void k_pzeta(PZetaArgs<T> a) {
     T fw_m = zeta_flux_w(a, i, k - 1);
     T rw = T(a.p.rhow[k]);
     T px = (fu_i - fu_m) * T(a.c.r2dx) / rw;
-    T pz = (fw_k - fw_m) * T(a.c.r2dz) / rw;
+    T pz = (fw_k - fw_m) * T(a.p.r2dzw[k]) / rw;
     T tz = -px - pz;
     T oz = ab2_push(a.hz_n, a.hz_o, id, tz, a.ab);
     T zp = a.zeta[id] + dt15 * tz - dt05 * oz;
@@ -304,7 +315,7 @@ __global__ void __launch_bounds__(256, (kPert<T> ? 4 : 1)) k_padv(PAdvArgs<T> a)
         const T ru = T(a.p.rhou[k]);
         // mixed step: one division for the cell's flux divergences (the FP64
         // step keeps the reference's (difference * r2d) / rhou per term)
-        const T sx = kPert<T> ? T(a.c.r2dx) / ru : T(0), sz = kPert<T> ? T(a.c.r2dz) / ru : T(0);
+        const T sx = kPert<T> ? T(a.c.r2dx) / ru : T(0), sz = kPert<T> ? T(a.p.r2dzc[k]) / ru : T(0);
         // velocity parts of the four faces, shared by the four fields;
         // flux_u at nx-1 is the halo copy of flux_u at 1, flux_w at nz-1 is
         // zeroed (Advection.cpp:55-58)
@@ -336,7 +347,7 @@ __global__ void __launch_bounds__(256, (kPert<T> ? 4 : 1)) k_padv(PAdvArgs<T> a)
                     pz = (fw_p - fw_0) * sz;
                 } else {
                     px = (fu_p - fu_0) * T(a.c.r2dx) / ru;
-                    pz = (fw_p - fw_0) * T(a.c.r2dz) / ru;
+                    pz = (fw_p - fw_0) * T(a.p.r2dzc[k]) / ru;
                 }
             } else {
                 // v = v0(k) + v': the v0 parts of both fluxes are added in
@@ -365,7 +376,7 @@ __global__ void __launch_bounds__(256, (kPert<T> ? 4 : 1)) k_padv(PAdvArgs<T> a)
             if (f == 3 && a.do_vt) {
                 T gp = (k == d.nz - 2) ? T(0) : vt_flux(a, v, i, k + 1);
                 T g0 = vt_flux(a, v, i, k);
-                T tv = kPert<T> ? (gp - g0) * sz : (gp - g0) * T(a.c.r2dz) / ru;
+                T tv = kPert<T> ? (gp - g0) * sz : (gp - g0) * T(a.p.r2dzc[k]) / ru;
                 T ov = ab2_push(a.hvt_n, a.hvt_o, id, tv, a.ab);
                 out += dt15 * tv - dt05 * ov;
             }
@@ -615,8 +626,8 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
     const T* u = a.u;
     const T* w = a.w;
     T Rzeta = T(0.5) * ((w[d.at(i + 1, k + 1)] + w[d.at(i + 1, k)]) - (w[d.at(i - 1, k + 1)] + w[d.at(i - 1, k)])) * T(a.c.r2dx) +
-              T(0.5) * ((u[d.at(i + 1, k + 1)] + u[d.at(i, k + 1)]) - (u[d.at(i + 1, k - 1)] + u[d.at(i, k - 1)])) * T(a.c.r2dz);
-    T rot = (u[d.at(i + 1, k)] - u[d.at(i, k)]) * T(a.c.rdx) + (w[d.at(i, k + 1)] - w[d.at(i, k)]) * T(a.c.rdz);
+              T(0.5) * ((u[d.at(i + 1, k + 1)] + u[d.at(i, k + 1)]) - (u[d.at(i + 1, k - 1)] + u[d.at(i, k - 1)])) * T(a.p.r2dzcc[k]);
+    T rot = (u[d.at(i + 1, k)] - u[d.at(i, k)]) * T(a.c.rdx) + (w[d.at(i, k + 1)] - w[d.at(i, k)]) * T(a.p.rdzc[k]);
     T Rotat = rot * rot;
     T th0 = a.thp[d.at(i, k)];
     T dth = a.thp[d.at(i, k + 1)] - a.thp[d.at(i, k - 1)];
@@ -625,7 +636,7 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
         dth += T(a.p.g0[0][k]);
     }
     T def2 = Rzeta * Rzeta + T(2.) * Rotat;
-    T Ri = (T(a.c.gravity) / th0 * dth * T(a.c.r2dz)) / def2;
+    T Ri = (T(a.c.gravity) / th0 * dth * T(a.p.r2dzcc[k])) / def2;
     T lam = T(a.p.lambda2[k]);
     T km, kh;
     if (Ri < T(0)) {
@@ -638,7 +649,7 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
         km = T(0.);
         kh = T(0.);
     }
-    const T kmax = T(0.8 * a.c.dx * a.c.dz / a.c.dt);
+    const T kmax = T(a.p.kmax[k]);
     km = smax(km, T(10.));
     kh = smax(kh, T(10.));
     km = smin(km, kmax);
@@ -852,12 +863,12 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
             const int k = k0 + lane;
             T* rv = rowv[wid][lane];
             if (mom) {
-                rv[0] = T(a.c.rdz2 * a.c.dt / a.p.rhow[k]);
-                rv[1] = T(a.p.rhou[k - 1]);
+                rv[0] = T(a.p.gsM_cz[k]);
+                rv[1] = T(a.p.gsM_rhod[k]);
                 rv[2] = T(a.p.rhou[k]);
             } else {
-                rv[0] = T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
-                rv[1] = T(a.p.rhow[k]);
+                rv[0] = T(a.p.gsS_cz[k]);
+                rv[1] = T(a.p.gsS_rhod[k]);
                 rv[2] = T(a.p.rhow[k + 1]);
             }
             T dn = T(0), tn = T(0);   // nudging of row k: out = y - dn (y - tn)
@@ -1109,7 +1120,7 @@ __global__ void k_gs_coeffs(GSArgs<T> a) {
     const bool mom = (f == 0);
     const T* K = mom ? a.RKM : a.RKH;
     const T cx = T(a.c.rdx2 * a.c.dt);
-    const T cz = mom ? T(a.c.rdz2 * a.c.dt / a.p.rhow[k]) : T(a.c.rdz2 * a.c.dt / a.p.rhou[k]);
+    const T cz = mom ? T(a.p.gsM_cz[k]) : T(a.p.gsS_cz[k]);
     T v0 = v[d.at(i, k)], vr = v[d.at(i + 1, k)], vu = v[d.at(i, k + 1)];
     T ax, bx, czu, czd;
     if (mom) {
@@ -1117,14 +1128,14 @@ __global__ void k_gs_coeffs(GSArgs<T> a) {
         ax = T(0.5) * (Kc + Kd);
         bx = T(0.5) * (Kl + Kld);
         czu = T(a.p.rhou[k]) * T(0.5) * (Kc + Kl);
-        czd = T(a.p.rhou[k - 1]) * T(0.5) * (Kd + Kld);
+        czd = T(a.p.gsM_rhod[k]) * T(0.5) * (Kd + Kld);
     } else {
         T Kc = K[d.at(i, k)], Kr = K[d.at(i + 1, k)], Kl = K[d.at(i - 1, k)];
         T Ku = K[d.at(i, k + 1)], Kd = K[d.at(i, k - 1)];
         ax = T(0.5) * (Kr + Kc);
         bx = T(0.5) * (Kc + Kl);
         czu = T(a.p.rhow[k + 1]) * T(0.5) * (Ku + Kc);
-        czd = T(a.p.rhow[k]) * T(0.5) * (Kc + Kd);
+        czd = T(a.p.gsS_rhod[k]) * T(0.5) * (Kc + Kd);
     }
     T du = vu - v0, dd = v0;
     if (kPert<T> && (f == 1 || f == 2)) {   // th', qv' about a profile
@@ -1582,16 +1593,16 @@ __global__ void k_pubartop(PubarArgs<T> a) {
         const T* K = a.RKM;
         s[0] += 0.25 * (rhou[t] * ut + rhou[b] * ub) * (wt + wtm);
         s[1] += rhow[top] * 0.25 * ((double)K[d.at(i, top)] + K[d.at(i, t)] + K[d.at(i - 1, top)] + K[d.at(i - 1, t)]) *
-                (a.c.rdz * (utop - ut));
+                (a.p.rdz_up * (utop - ut));
         s[2] += rhow[t] * 0.25 * ((double)K[d.at(i, t)] + K[d.at(i, b)] + K[d.at(i - 1, t)] + K[d.at(i - 1, b)]) *
-                (a.c.rdx * (wt - wtm) + a.c.rdz * (ut - ub));
+                (a.c.rdx * (wt - wtm) + a.p.rdz_dn * (ut - ub));
     }
     block_sum(s, sh);
     if (threadIdx.x == 0) {
         double n = (double)(d.nx - 2.);
         double down = s[0] / n, kup = s[1] / n, kdown = s[2] / n;
-        double pa = (-down) * a.c.rdz / rhou[t];
-        double pb = (kup - kdown) * a.c.rdz / rhou[t];
+        double pa = (-down) * a.p.rdz_c / rhou[t];
+        double pb = (kup - kdown) * a.p.rdz_c / rhou[t];
         double tend = -pa + pb;
         double old = a.ab.first ? tend : a.dubar[a.ab.so];
         a.dubar[a.ab.sn] = tend;
@@ -1639,7 +1650,7 @@ __global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) {
         int i = i0 + e;
         h[e] = 0;
         if (e < per && i <= NX) {
-            h[e] = -(0. - a.p.rhow[t] * (double)a.w[d.at(i, t)]) / a.p.rhou[t] * a.c.dx;
+            h[e] = -(0. - a.p.rhow[t] * (double)a.w[d.at(i, t)]) / a.p.rhou[t] * a.c.dx * a.p.hfac;
             s[0] += h[e];
         }
     }
@@ -1716,9 +1727,10 @@ __global__ void __launch_bounds__(32 * kColSeg) k_cal_u_columns(CalUArgs<T> a) {
     const int t = d.nz - 2, nrow = d.nz - 3;               // rows k = 1..nz-3
     // segment s covers rows from the top: k in (khi - len, khi]
     const int r0 = (s * nrow) / kColSeg, r1 = ((s + 1) * nrow) / kColSeg;
-    const T rdx = T(a.c.rdx), mdz = T(-a.c.dz);
+    const T rdx = T(a.c.rdx);
     auto term = [&](int k) -> T {
-        return ((a.w[d.at(i, k + 1)] - a.w[d.at(i - 1, k + 1)]) * rdx - T(a.p.rhow[k + 1]) * a.zetap[d.at(i, k + 1)]) * mdz;
+        return ((a.w[d.at(i, k + 1)] - a.w[d.at(i - 1, k + 1)]) * rdx - T(a.p.rhow[k + 1]) * a.zetap[d.at(i, k + 1)]) *
+               T(-a.p.dzw[k + 1]);
     };
     T sum = T(0);
     if (act)

@@ -1444,6 +1444,10 @@ struct vvm_gpu_ctx {
     std::vector<double> h_forcing;   // [nx][nz] host copy of the last regenerated th forcing
     bool stretched = false;
     double* rwres = nullptr;   // [nz] residual weight rw_k = rhow_k / a_k
+    // vertical level metric of the step's stencils (Profiles::r2dzc ...)
+    double *lv_r2dzc = nullptr, *lv_r2dzw = nullptr, *lv_rdzc = nullptr, *lv_r2dzcc = nullptr, *lv_kmax = nullptr,
+           *gsM_cz = nullptr, *gsM_rhod = nullptr, *gsS_cz = nullptr, *gsS_rhod = nullptr, *lv_dzw = nullptr;
+    double lv_rdz_up = 0, lv_rdz_dn = 0, lv_rdz_c = 0, lv_hfac = 1;
     double* ubar = nullptr;   // [0] ubarTop, [1] ubarTopp
     double* dubar = nullptr;  // [2]
     double *partial = nullptr, *nvp = nullptr;
@@ -1503,7 +1507,9 @@ struct vvm_gpu_ctx {
         return Profiles{rhou, rhow, thvb, thb_init, qvb0, pib, pb, lambda2, vt_c1, vt_fac, pc,
                         dtcgr_th, dtcgr_zeta, q1ls, q2ls, pf1, pf2,
                         {pref[0], pref[1]}, {pd0[0], pd0[1]}, {ps0[0], ps0[1]}, {pg0[0], pg0[1]},
-                        {pdn[0], pdn[1]}};
+                        {pdn[0], pdn[1]},
+                        lv_r2dzc, lv_r2dzw, lv_rdzc, lv_r2dzcc, lv_kmax, gsM_cz, gsM_rhod, gsS_cz, gsS_rhod, lv_dzw,
+                        lv_rdz_up, lv_rdz_dn, lv_rdz_c, lv_hfac};
     }
     // profile subtracted from a stored field (mixed step: th and qv only)
     const double* offset_th() const { return mixed ? pref[0] : nullptr; }
@@ -2918,7 +2924,86 @@ int upload_profiles(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
         vtf[k] = std::pow(s->rhow[k] / s->rhow[1], -0.5);
         pc[k] = 380. / (std::pow(s->pib[k], D.cp / D.rd) * D.p0);    // MicroPhysics.cpp:10
     }
-    int ks = (int)(12000. / D.dz + 1);                               // NumericalProcess.cpp:62
+    // Vertical level metric of the stencils (the C restatement's levels(),
+    // oracle/vvm_oracle.c, formula for formula): with dc[k] = 2 (z[k] -
+    // z_zeta[k]) the thickness of centre cell k and dw[k] = z[k] - z[k-1] the
+    // distance between the centres around face k (mirror centres beyond the
+    // surface and the top: dw[1] = dc[1], dw[nz-1] = dc[nz-2]), a flux
+    // divergence at a centre is over dc, at a face over dw, a gradient across
+    // two centres over z[k+1] - z[k-1]. Uniform levels (every spacing within
+    // 1e-9 dz of dz) take the reference's constants exactly.
+    bool lv_uniform = true;
+    for (int k = 1; k <= nz - 2; k++)
+        if (std::fabs(2.0 * (s->z[k] - s->z_zeta[k]) - D.dz) > 1e-9 * D.dz) lv_uniform = false;
+    for (int k = 2; k <= nz - 2; k++)
+        if (std::fabs((s->z[k] - s->z[k - 1]) - D.dz) > 1e-9 * D.dz) lv_uniform = false;
+    {
+        std::vector<double> r2c(nz), r2w(nz), rc(nz), r2cc(nz), km(nz), mcz(nz), mrd(nz), scz(nz), srd(nz), dzw(nz);
+        const double rdz = 1.0 / D.dz, r2dz = rdz / 2.0, rdz2 = rdz * rdz;
+        if (lv_uniform) {
+            for (int k = 0; k < nz; k++) {
+                r2c[k] = r2dz; r2w[k] = r2dz; rc[k] = rdz; r2cc[k] = r2dz;
+                km[k] = 0.8 * D.dx * D.dz / D.dt;
+                mcz[k] = rdz2 * D.dt / s->rhow[k];       // Turbulent.cpp:84
+                mrd[k] = k > 0 ? 1.0 * s->rhou[k - 1] : 0.0;
+                scz[k] = rdz2 * D.dt / s->rhou[k];       // Turbulent.cpp:108
+                srd[k] = 1.0 * s->rhow[k];
+                dzw[k] = D.dz;
+            }
+            c->lv_rdz_up = c->lv_rdz_dn = c->lv_rdz_c = rdz;
+            c->lv_hfac = 1.0;
+        } else {
+            std::vector<double> dc(nz), dw(nz);
+            for (int k = 1; k <= nz - 2; k++) dc[k] = 2.0 * (s->z[k] - s->z_zeta[k]);
+            dc[0] = dc[1];
+            dc[nz - 1] = dc[nz - 2];
+            for (int k = 2; k <= nz - 2; k++) dw[k] = s->z[k] - s->z[k - 1];
+            dw[1] = dc[1];
+            dw[0] = dc[1];
+            dw[nz - 1] = dc[nz - 2];
+            for (int k = 0; k < nz; k++) {
+                r2c[k] = (1.0 / dc[k]) / 2.0;
+                r2w[k] = (1.0 / dw[k]) / 2.0;
+                rc[k] = 1.0 / dc[k];
+                km[k] = 0.8 * D.dx * dc[k] / D.dt;
+                dzw[k] = dw[k];
+                r2cc[k] = r2dz;
+                mcz[k] = scz[k] = 0.0;
+                mrd[k] = srd[k] = 0.0;
+            }
+            for (int k = 1; k <= nz - 2; k++) {
+                const double zm = (k == 1) ? s->z[1] - dc[1] : s->z[k - 1];
+                const double zp = (k == nz - 2) ? s->z[nz - 2] + dc[nz - 2] : s->z[k + 1];
+                r2cc[k] = 1.0 / (zp - zm);
+                mcz[k] = ((1.0 / dw[k]) * (1.0 / dc[k])) * D.dt / s->rhow[k];
+                mrd[k] = (dc[k] / dc[k - 1]) * s->rhou[k - 1];
+                scz[k] = ((1.0 / dc[k]) * (1.0 / dw[k + 1])) * D.dt / s->rhou[k];
+                srd[k] = (dw[k + 1] / dw[k]) * s->rhow[k];
+            }
+            c->lv_rdz_up = 1.0 / dw[nz - 1];
+            c->lv_rdz_dn = 1.0 / dw[nz - 2];
+            c->lv_rdz_c = 1.0 / dc[nz - 2];
+            c->lv_hfac = D.dx / dc[nz - 2];
+        }
+        upload_profile(c, r2c.data(), c->lv_r2dzc);
+        upload_profile(c, r2w.data(), c->lv_r2dzw);
+        upload_profile(c, rc.data(), c->lv_rdzc);
+        upload_profile(c, r2cc.data(), c->lv_r2dzcc);
+        upload_profile(c, km.data(), c->lv_kmax);
+        upload_profile(c, mcz.data(), c->gsM_cz);
+        upload_profile(c, mrd.data(), c->gsM_rhod);
+        upload_profile(c, scz.data(), c->gsS_cz);
+        upload_profile(c, srd.data(), c->gsS_rhod);
+        upload_profile(c, dzw.data(), c->lv_dzw);
+    }
+    // the first nudged level (NumericalProcess.cpp:62: 12000 / dz + 1); on
+    // stretched levels the last face at or below 12 km
+    int ks = (int)(12000. / D.dz + 1);
+    if (!lv_uniform) {
+        ks = 1;
+        for (int k = 1; k <= nz - 1; k++)
+            if (s->z_zeta[k] <= 12000.) ks = k;
+    }
     if (ks < nz - 1 && (nz - 1) - ks >= 0) {
         const double* z = s->z;
         const double* zz = s->z_zeta;
@@ -3084,12 +3169,11 @@ int need_state(vvm_gpu_ctx* c) {
     return c->has_state ? VVM_GPU_OK : fail(c, VVM_GPU_ESTATE, "no state uploaded");
 }
 
-// The step's stencils use one level spacing dz (the reference's); a state on
-// stretched levels supports the Poisson entries only.
+// The streamfunction formulation keeps the reference's psi matrix, which
+// assumes uniform levels; every other entry takes stretched levels.
 int need_uniform(vvm_gpu_ctx* c) {
     return c->stretched ? fail(c, VVM_GPU_EINVAL,
-                               "stretched vertical levels: only the Poisson solve and the learned "
-                               "preconditioner's entries support them")
+                               "stretched vertical levels: the streamfunction formulation needs uniform levels")
                         : VVM_GPU_OK;
 }
 
@@ -3199,7 +3283,9 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         int nz = c->d.nz;
         double** profs[] = {&c->rhou, &c->rhow, &c->thvb, &c->thb, &c->qvb, &c->thb_init, &c->qvb0,
                             &c->pib, &c->pb, &c->lambda2, &c->z, &c->z_zeta, &c->vt_c1, &c->vt_fac,
-                            &c->pc, &c->dtcgr_th, &c->dtcgr_zeta, &c->q1ls, &c->q2ls, &c->rwres};
+                            &c->pc, &c->dtcgr_th, &c->dtcgr_zeta, &c->q1ls, &c->q2ls, &c->rwres,
+                            &c->lv_r2dzc, &c->lv_r2dzw, &c->lv_rdzc, &c->lv_r2dzcc, &c->lv_kmax, &c->gsM_cz,
+                            &c->gsM_rhod, &c->gsS_cz, &c->gsS_rhod, &c->lv_dzw};
         for (double** p : profs) *p = c->ar.alloc<double>(nz);
         for (int j = 0; j < 2; j++) {
             c->pref[j] = c->ar.alloc<double>(nz);
@@ -3318,7 +3404,6 @@ int vvm_gpu_get_step(vvm_gpu_ctx* ctx, int* step) {
     int name(vvm_gpu_ctx* ctx) {                                              \
         return guarded(ctx, [&]() -> int {                                    \
             if (int rc = need_state(ctx)) return rc;                          \
-            if (int rc = need_uniform(ctx)) return rc;                        \
             ctx->fut_is_now = false;                                          \
             __VA_ARGS__;                                                      \
         });                                                                   \
@@ -3370,7 +3455,10 @@ ROUTINE(vvm_gpu_nudge, {
     DISPATCH(ctx, launch_nudge)(ctx, true, ctx->desc.moisture_nudge_time != 0.0);
     return VVM_GPU_OK;
 })
-ROUTINE(vvm_gpu_calpsiuw, { return DISPATCH(ctx, launch_calpsiuw)(ctx); })
+ROUTINE(vvm_gpu_calpsiuw, {
+    if (int rc = need_uniform(ctx)) return rc;   // the reference's psi matrix assumes uniform levels
+    return DISPATCH(ctx, launch_calpsiuw)(ctx);
+})
 
 int vvm_gpu_download_psi(vvm_gpu_ctx* ctx, double* psi) {
     return guarded(ctx, [&]() -> int {
@@ -3392,7 +3480,8 @@ int vvm_gpu_step(vvm_gpu_ctx* ctx, int nsteps) {
     return guarded(ctx, [&]() -> int {
         if (int rc = need_state(ctx)) return rc;
         if (nsteps < 0) return fail(ctx, VVM_GPU_EINVAL, "step: nsteps < 0");
-        if (int rc = need_uniform(ctx)) return rc;
+        if (ctx->desc.flags & VVM_FLAG_STREAMFUNCTION)
+            if (int rc = need_uniform(ctx)) return rc;
         int worst = VVM_GPU_OK;
         for (int s = 0; s < nsteps; s++) {
             int rc = DISPATCH(ctx, step_once)(ctx);

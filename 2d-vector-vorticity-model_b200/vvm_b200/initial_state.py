@@ -209,7 +209,8 @@ def base_state(g: GridSpec, theta_of_z, rh: float | np.ndarray, qv_of_z=None,
 
 
 def _assemble(g: GridSpec, prof: dict, th: np.ndarray, u: np.ndarray,
-              w: np.ndarray | None = None, qv: np.ndarray | None = None) -> VVMState:
+              w: np.ndarray | None = None, qv: np.ndarray | None = None,
+              stretched: bool = False) -> VVMState:
     nx, nz = g.nx, g.nz
     st = VVMState(g)
     f = st.fields
@@ -229,7 +230,14 @@ def _assemble(g: GridSpec, prof: dict, th: np.ndarray, u: np.ndarray,
     uu, ww, rhow = f["u"], f["w"], prof["rhow"]
     zeta = f["zeta"]
     pw_px = (ww[1:nx - 1, 1:nz - 1] - ww[0:nx - 2, 1:nz - 1]) * (1.0 / g.dx)
-    pu_pz = (uu[1:nx - 1, 1:nz - 1] - uu[1:nx - 1, 0:nz - 2]) * (1.0 / g.dz)
+    if stretched:   # centre-to-centre spacing around each face (the first is never used: u[0] = u[1])
+        zc = prof["z"]
+        dzw = np.empty(nz - 2)
+        dzw[0] = 1.0
+        dzw[1:] = zc[2:nz - 1] - zc[1:nz - 2]
+        pu_pz = (uu[1:nx - 1, 1:nz - 1] - uu[1:nx - 1, 0:nz - 2]) / dzw[None, :]
+    else:
+        pu_pz = (uu[1:nx - 1, 1:nz - 1] - uu[1:nx - 1, 0:nz - 2]) * (1.0 / g.dz)
     zeta[1:nx - 1, 1:nz - 1] = (pw_px - pu_pz) / rhow[None, 1:nz - 1]
     _westdown2d(zeta)
     # ubarTop: src/Init.cpp:244-248 (sequential sum, as the reference does)
@@ -248,22 +256,23 @@ def _assemble(g: GridSpec, prof: dict, th: np.ndarray, u: np.ndarray,
 def warm_bubble(NX: int = 128, NZ: int = 64, dx: float = 200.0, dz: float = 200.0,
                 dt: float = 1.0, amp: float = 2.0, radius: float = 2000.0,
                 xc_frac: float = 0.5, zc: float = 2000.0, dthdz: float = 3e-3,
-                rh: float = 0.8, case: int = 1) -> VVMState:
+                rh: float = 0.8, case: int = 1, zf: np.ndarray | None = None) -> VVMState:
     """Plain VVM warm bubble: theta = 300 K + dthdz*z, qv at ``rh`` of saturation,
     a cosine bubble of amplitude ``amp`` and radius ``radius`` centred at
-    (``xc_frac`` of the domain, ``zc``), u = w = 0."""
+    (``xc_frac`` of the domain, ``zc``), u = w = 0. ``zf``: face heights of
+    stretched levels (stretched_faces; ``dz`` is then its lowest spacing)."""
     g = GridSpec(NX, NZ, dx, dz, dt, case)
-    prof = base_state(g, lambda z: 300.0 + dthdz * z, rh)
+    prof = base_state(g, lambda z: 300.0 + dthdz * z, rh, zf=zf)
     nx, nz = g.nx, g.nz
     i = np.arange(nx)[:, None]
     k = np.arange(nz)[None, :]
     x = (i - 0.5) * dx
-    z = (k - 0.5) * dz
+    z = (k - 0.5) * dz if zf is None else prof["z"][None, :]
     r = np.sqrt(((x - xc_frac * NX * dx) / radius) ** 2 + ((z - zc) / radius) ** 2)
     bubble = np.where(r <= 1.0, 0.5 * amp * (np.cos(np.pi * r) + 1.0), 0.0)
     th = np.zeros((nx, nz))
     th[1:nx - 1, 1:nz - 1] = prof["thb"][None, 1:nz - 1] + bubble[1:nx - 1, 1:nz - 1]
-    return _assemble(g, prof, th, np.zeros((nx, nz)))
+    return _assemble(g, prof, th, np.zeros((nx, nz)), stretched=zf is not None)
 
 
 def random_state(NX: int = 32, NZ: int = 16, dx: float = 200.0, dz: float = 200.0,
@@ -382,7 +391,8 @@ def poisson_rhs(st: VVMState, field: str = "zeta") -> np.ndarray:
 
 def squall_line(NX: int = 1024, NZ: int = 128, dx: float = 250.0, dz: float = 250.0, dt: float = 2.0,
                 seed: int = 2, pool_amp: float = -3.0, pool_width: float = 10000.0,
-                pool_depth: float = 1500.0, u_top: float = 10.0, shear_depth: float = 2500.0) -> VVMState:
+                pool_depth: float = 1500.0, u_top: float = 10.0, shear_depth: float = 2500.0,
+                zf: np.ndarray | None = None) -> VVMState:
     """Sheared squall line on uniform levels: theta from stratified_theta
     (300 K + 3 K/km to 12 km, a stratosphere above, so deep domains stay warmer
     than the Tetens formula's 36 K singularity), qv at
@@ -391,13 +401,18 @@ def squall_line(NX: int = 1024, NZ: int = 128, dx: float = 250.0, dz: float = 25
     rising linearly from 0 to u_top over the lowest shear_depth, constant
     above; a cold pool of pool_amp (cosine-tapered, pool_width wide,
     pool_depth deep) at mid-domain; seeded N(0, 0.1 K) noise in the lowest
-    1 km. w = 0; zeta follows from the shear."""
+    1 km. w = 0; zeta follows from the shear. ``zf``: face heights of
+    stretched levels (stretched_faces; ``dz`` is then its lowest spacing)."""
     g = GridSpec(NX, NZ, dx, dz, dt, 1)
     nz = g.nz
     zc = (np.arange(nz) - 0.5) * dz
+    if zf is not None:
+        zc = np.zeros(nz)
+        zc[1:nz - 1] = 0.5 * (zf[1:nz - 1] + zf[2:nz])
+        zc[0], zc[nz - 1] = zc[1], zc[nz - 2]
     rh = np.clip(np.where(zc <= 1500.0, 0.9, 0.9 - 0.6 * (zc - 1500.0) / 8500.0), 0.3, 0.9)
     rh = np.where(zc <= 10000.0, rh, dry_aloft(zc, 0.3))
-    prof = base_state(g, stratified_theta, rh)
+    prof = base_state(g, stratified_theta, rh, zf=zf)
     nx = g.nx
     i = np.arange(nx)[:, None]
     x = (i - 0.5) * dx
@@ -414,7 +429,7 @@ def squall_line(NX: int = 1024, NZ: int = 128, dx: float = 250.0, dz: float = 25
                               + noise[1:nx - 1, 1:nz - 1])
     u = np.zeros((nx, nz))
     u[1:nx - 1, 1:nz - 1] = (u_top * np.minimum(z / shear_depth, 1.0))[:, 1:nz - 1] * np.ones((nx - 2, 1))
-    return _assemble(g, prof, th, u)
+    return _assemble(g, prof, th, u, stretched=zf is not None)
 
 
 def read_sounding(path) -> np.ndarray:

@@ -46,6 +46,12 @@ struct orc_model {
     double *z, *z_zeta, *lambda2, *xi, *uxi, *precip, *Q1LS, *Q2LS;
     /* scratch */
     double *flux_u, *flux_w, *work;
+    /* vertical level metric (levels()): per-level factors that equal the
+     * reference's constants on uniform levels */
+    int stretched, lv_ks;
+    double *lv_r2dzc, *lv_r2dzw, *lv_rdzc, *lv_r2dzcc, *lv_kmax, *lv_rdz2M, *lv_rdM, *lv_rdz2S, *lv_rdS,
+        *lv_dzw, *lv_wa, *lv_wh;
+    double lv_rdz_up, lv_rdz_dn, lv_rdz_c, lv_hfac;
 };
 
 static double* alloc0(size_t n) { return (double*)calloc(n ? n : 1, sizeof(double)); }
@@ -78,6 +84,9 @@ orc_model* orc_create(int NX, int NZ, double dx, double dz, double dt, int CASE,
                       &m->z_zeta, &m->lambda2, &m->Q1LS, &m->Q2LS};
     for (size_t j = 0; j < sizeof(one) / sizeof(one[0]); j++) *one[j] = alloc0(nz);
     m->xi = alloc0(nx); m->uxi = alloc0(nx); m->precip = alloc0(nx);
+    double** lv[] = {&m->lv_r2dzc, &m->lv_r2dzw, &m->lv_rdzc, &m->lv_r2dzcc, &m->lv_kmax, &m->lv_rdz2M,
+                     &m->lv_rdM, &m->lv_rdz2S, &m->lv_rdS, &m->lv_dzw, &m->lv_wa, &m->lv_wh};
+    for (size_t j = 0; j < sizeof(lv) / sizeof(lv[0]); j++) *lv[j] = alloc0(nz);
     m->work = alloc0(4 * n2 + 8 * (nx + nz));
     return m;
 }
@@ -91,7 +100,9 @@ void orc_destroy(orc_model* m) {
                      m->dth_buoyancy, m->dzeta_advect, m->dqv_advect, m->dqc_advect,
                      m->dqr_advect, m->dqr_VT, m->thb, m->thbm, m->thb_zeta, m->thb_init,
                      m->rhou, m->rhow, m->pib, m->qvb, m->qvb0, m->pb, m->thvb, m->thvbm, m->z,
-                     m->z_zeta, m->lambda2, m->Q1LS, m->Q2LS, m->xi, m->uxi, m->precip, m->work, m->psi};
+                     m->z_zeta, m->lambda2, m->Q1LS, m->Q2LS, m->xi, m->uxi, m->precip, m->work, m->psi,
+                     m->lv_r2dzc, m->lv_r2dzw, m->lv_rdzc, m->lv_r2dzcc, m->lv_kmax, m->lv_rdz2M, m->lv_rdM,
+                     m->lv_rdz2S, m->lv_rdS, m->lv_dzw, m->lv_wa, m->lv_wh};
     for (size_t j = 0; j < sizeof(all) / sizeof(all[0]); j++) free(all[j]);
     free(m);
 }
@@ -141,6 +152,86 @@ double* orc_scalar(orc_model* m, const char* n) {
 }
 
 int* orc_step_ptr(orc_model* m) { return &m->step; }
+
+/* ---------------------------------------------------------------- levels */
+
+/* The vertical metric of the column. The reference's levels are uniform
+ * (src/Init.cpp:125-129) and its operators assume one spacing dz (and, in
+ * cal_w and cal_u, dx = dz). On levels with face heights z_zeta[k] and centre
+ * heights z[k] midway between faces, with
+ *   dc[k] = 2 (z[k] - z_zeta[k])     the thickness of centre cell k,
+ *   dw[k] = z[k] - z[k-1]            the distance between the centres around face k
+ *                                    (mirror centres below the surface and above the top
+ *                                    face: dw[1] = dc[1], dw[nz-1] = dc[nz-2]),
+ * each vertical difference is divided by the spacing it spans: a flux
+ * divergence at a centre by dc, at a face by dw; a gradient across two
+ * centres by z[k+1] - z[k-1]. The Gauss-Seidel diffusion's down-gradient
+ * is scaled by the ratio of its spacing to the up-gradient's (lv_rdM,
+ * lv_rdS) so that one factor (lv_rdz2M, lv_rdz2S) multiplies the bracket
+ * as in the reference. cal_w takes the stretched matrix of
+ * oracle/stretched_poisson.py; cal_u integrates over dw and takes the
+ * top divergence over dc (lv_hfac = dx / dc[nz-2], where the reference's
+ * dx stands for dz). When every spacing is within 1e-9 dz of dz the factors
+ * are the reference's constants (and the down ratios exactly 1), so the
+ * routines reproduce the reference bit for bit. Nudging starts at the last
+ * face at or below 12 km (the reference's 12000 / dz + 1 on uniform levels). */
+static void levels(orc_model* m) {
+    int nz = m->nz;
+    double *z = m->z, *zz = m->z_zeta;
+    int uniform = 1;
+    for (int k = 1; k <= nz - 2; k++)
+        if (fabs(2.0 * (z[k] - zz[k]) - m->dz) > 1e-9 * m->dz) uniform = 0;
+    for (int k = 2; k <= nz - 2; k++)
+        if (fabs((z[k] - z[k - 1]) - m->dz) > 1e-9 * m->dz) uniform = 0;
+    m->stretched = !uniform;
+    if (uniform) {
+        for (int k = 0; k < nz; k++) {
+            m->lv_r2dzc[k] = m->r2dz; m->lv_r2dzw[k] = m->r2dz; m->lv_rdzc[k] = m->rdz;
+            m->lv_r2dzcc[k] = m->r2dz; m->lv_kmax[k] = 0.8 * m->dx * m->dz / m->dt;
+            m->lv_rdz2M[k] = m->rdz2; m->lv_rdM[k] = 1.0; m->lv_rdz2S[k] = m->rdz2; m->lv_rdS[k] = 1.0;
+            m->lv_dzw[k] = m->dz; m->lv_wa[k] = 1.0; m->lv_wh[k] = 1.0;
+        }
+        m->lv_rdz_up = m->lv_rdz_dn = m->lv_rdz_c = m->rdz;
+        m->lv_hfac = 1.0;
+        m->lv_ks = 12000. / m->dz + 1;
+        return;
+    }
+    double* dw = m->lv_dzw;
+    double* tmp = (double*)malloc(sizeof(double) * nz);
+    for (int k = 1; k <= nz - 2; k++) tmp[k] = 2.0 * (z[k] - zz[k]);
+    tmp[0] = tmp[1]; tmp[nz - 1] = tmp[nz - 2];
+    for (int k = 2; k <= nz - 2; k++) dw[k] = z[k] - z[k - 1];
+    dw[1] = tmp[1]; dw[0] = tmp[1]; dw[nz - 1] = tmp[nz - 2];
+    for (int k = 0; k < nz; k++) {
+        m->lv_r2dzc[k] = (1.0 / tmp[k]) / 2.0;
+        m->lv_r2dzw[k] = (1.0 / dw[k]) / 2.0;
+        m->lv_rdzc[k] = 1.0 / tmp[k];
+        m->lv_kmax[k] = 0.8 * m->dx * tmp[k] / m->dt;
+    }
+    for (int k = 1; k <= nz - 2; k++) {
+        double zm = (k == 1) ? z[1] - tmp[1] : z[k - 1];          /* mirror centre below the surface */
+        double zp = (k == nz - 2) ? z[nz - 2] + tmp[nz - 2] : z[k + 1];   /* and above the top face */
+        m->lv_r2dzcc[k] = 1.0 / (zp - zm);
+        /* Mparam (zeta at face k): bracket over dw[k]; up difference over dc[k], down over dc[k-1] */
+        m->lv_rdz2M[k] = (1.0 / dw[k]) * (1.0 / tmp[k]);
+        m->lv_rdM[k] = tmp[k] / tmp[k - 1];
+        /* Hparam (centre k): bracket over dc[k]; up difference over dw[k+1], down over dw[k] */
+        m->lv_rdz2S[k] = (1.0 / tmp[k]) * (1.0 / dw[k + 1]);
+        m->lv_rdS[k] = dw[k + 1] / dw[k];
+    }
+    m->lv_rdz_up = 1.0 / dw[nz - 1];
+    m->lv_rdz_dn = 1.0 / dw[nz - 2];
+    m->lv_rdz_c = 1.0 / tmp[nz - 2];
+    m->lv_hfac = m->dx / tmp[nz - 2];
+    /* cal_w's metric (oracle/stretched_poisson.py): a_k = dw[k] / dx, h_k = dx / dc[k] */
+    for (int k = 0; k < nz; k++) { m->lv_wa[k] = 1.0; m->lv_wh[k] = 1.0; }
+    for (int k = 2; k <= nz - 2; k++) m->lv_wa[k] = (z[k] - z[k - 1]) / m->dx;
+    for (int k = 1; k <= nz - 2; k++) m->lv_wh[k] = m->dx / (2.0 * (z[k] - zz[k]));
+    int ks = 1;
+    for (int k = 1; k <= nz - 1; k++) if (zz[k] <= 12000.) ks = k;
+    m->lv_ks = ks;
+    free(tmp);
+}
 
 /* ---------------------------------------------------------------- halos */
 
@@ -218,7 +309,7 @@ static void advect_scalar(orc_model* m, const double* now, double* future, doubl
     for (int k = 1; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
             double px = (F2(fu, i + 1, k) - F2(fu, i, k)) * m->r2dx / rhou[k];
-            double pz = (F2(fw, i, k + 1) - F2(fw, i, k)) * m->r2dz / rhou[k];
+            double pz = (F2(fw, i, k + 1) - F2(fw, i, k)) * m->lv_r2dzc[k] / rhou[k];
             H3(dvar, i, k, sn) = -px - pz;
             if (m->step == 0) H3(dvar, i, k, 0) = H3(dvar, i, k, 1);
             F2(future, i, k) = F2(now, i, k) + 1.5 * m->dt * H3(dvar, i, k, sn) - 0.5 * m->dt * H3(dvar, i, k, so);
@@ -268,7 +359,7 @@ static void advect_zeta(orc_model* m) {
     for (int k = 2; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
             double px = (F2(fu, i, k) - F2(fu, i - 1, k)) * m->r2dx / rhow[k];
-            double pz = (F2(fw, i, k) - F2(fw, i, k - 1)) * m->r2dz / rhow[k];
+            double pz = (F2(fw, i, k) - F2(fw, i, k - 1)) * m->lv_r2dzw[k] / rhow[k];
             H3(m->dzeta_advect, i, k, sn) = -px - pz;
             if (m->step == 0) H3(m->dzeta_advect, i, k, 0) = H3(m->dzeta_advect, i, k, 1);
             F2(m->zetap, i, k) = F2(z, i, k) + 1.5 * m->dt * H3(m->dzeta_advect, i, k, sn) - 0.5 * m->dt * H3(m->dzeta_advect, i, k, so);
@@ -294,7 +385,7 @@ static void advect_qr_vt(orc_model* m) {
     ORC_PAR
     for (int k = 1; k <= nz - 2; k++) {
         for (int i = 1; i <= nx - 2; i++) {
-            double p = (F2(fw, i, k + 1) - F2(fw, i, k)) * m->r2dz / rhou[k];
+            double p = (F2(fw, i, k + 1) - F2(fw, i, k)) * m->lv_r2dzc[k] / rhou[k];
             H3(m->dqr_VT, i, k, sn) = p;
             if (m->step == 0) H3(m->dqr_VT, i, k, 0) = H3(m->dqr_VT, i, k, 1);
             F2(m->qrp, i, k) += 1.5 * m->dt * H3(m->dqr_VT, i, k, sn) - 0.5 * m->dt * H3(m->dqr_VT, i, k, so);
@@ -620,6 +711,24 @@ static void solve_separable(int NX, int NK, const double* cxk, const double* ruk
     free(c); free(s); free(hat); free(sol); free(lo); free(di); free(up); free(cp); free(dp);
 }
 
+/* The cal_w system on stretched levels (oracle/stretched_poisson.py): row
+ * (k, i) as orc_solve_A's with ru_k = rhow_k h_k / (a_k rhou_k) and
+ * rd_k = rhow_k h_{k-1} / (a_k rhou_{k-1}), a and h from levels(). */
+void orc_solve_W(orc_model* m, const double* b, double* x) {
+    int NK = m->nz - 3;
+    levels(m);
+    double* cf = (double*)malloc(sizeof(double) * 3 * NK);
+    for (int kk = 0; kk < NK; kk++) {
+        int k = kk + 2;
+        double a = m->lv_wa[k];
+        cf[kk] = 1.0;
+        cf[NK + kk] = m->rhow[k] * m->lv_wh[k] / (a * m->rhou[k]);
+        cf[2 * NK + kk] = m->rhow[k] * m->lv_wh[k - 1] / (a * m->rhou[k - 1]);
+    }
+    solve_separable(m->nx - 2, NK, cf, cf + NK, cf + 2 * NK, b, x);
+    free(cf);
+}
+
 void orc_apply_A(orc_model* m, const double* x, double* y) {
     int NX = m->nx - 2, NK = m->nz - 3;
     for (int kk = 0; kk < NK; kk++) {
@@ -644,7 +753,8 @@ static void cal_w(orc_model* m) {
     for (int k = 2; k <= nz - 2; k++)
         for (int i = 1; i <= nx - 2; i++)
             b[cnt++] = m->rhow[k] * m->rhow[k] * (F2(m->zetap, i + 1, k) - F2(m->zetap, i, k)) * m->dx;
-    orc_solve_A(m, b, x);
+    if (m->stretched) orc_solve_W(m, b, x);
+    else orc_solve_A(m, b, x);
     cnt = 0;
     for (int k = 2; k <= nz - 2; k++)
         for (int i = 1; i <= nx - 2; i++) F2(m->w, i, k) = x[cnt++] / m->rhow[k];
@@ -739,7 +849,7 @@ static void cal_u(orc_model* m) {
     double* h = m->work;
     double tmp = 0.;
     for (int i = 1; i <= nx - 2; i++) {
-        h[i - 1] = -(0. - m->rhow[nz - 2] * F2(m->w, i, nz - 2)) / m->rhou[nz - 2] * m->dx;
+        h[i - 1] = -(0. - m->rhow[nz - 2] * F2(m->w, i, nz - 2)) / m->rhou[nz - 2] * m->dx * m->lv_hfac;
         tmp += h[i - 1];
     }
     tmp /= (nx - 2);
@@ -761,7 +871,7 @@ static void cal_u(orc_model* m) {
     for (int i = 1; i <= nx - 2; i++) {
         double area = 0.;
         for (int k = nz - 3; k >= 1; k--) {
-            area += ((F2(m->w, i, k + 1) - F2(m->w, i - 1, k + 1)) * m->rdx - m->rhow[k + 1] * F2(m->zetap, i, k + 1)) * -m->dz;
+            area += ((F2(m->w, i, k + 1) - F2(m->w, i - 1, k + 1)) * m->rdx - m->rhow[k + 1] * F2(m->zetap, i, k + 1)) * -m->lv_dzw[k + 1];
             F2(m->u, i, k) = area + F2(m->u, i, nz - 2);
         }
     }
@@ -776,15 +886,15 @@ static void pubar_top(orc_model* m) {
     for (int i = 1; i < nx - 1; i++) {
         down += 0.25 * (rhou[nz - 2] * F2(u, i, nz - 2) + rhou[nz - 3] * F2(u, i, nz - 3)) * (F2(w, i, nz - 2) + F2(w, i - 1, nz - 2));
         kup += rhow[nz - 1] * 0.25 * (F2(K, i, nz - 1) + F2(K, i, nz - 2) + F2(K, i - 1, nz - 1) + F2(K, i - 1, nz - 2))
-               * (m->rdz * (F2(u, i, nz - 1) - F2(u, i, nz - 2)));
+               * (m->lv_rdz_up * (F2(u, i, nz - 1) - F2(u, i, nz - 2)));
         kdown += rhow[nz - 2] * 0.25 * (F2(K, i, nz - 2) + F2(K, i, nz - 3) + F2(K, i - 1, nz - 2) + F2(K, i - 1, nz - 3))
-                 * (m->rdx * (F2(w, i, nz - 2) - F2(w, i - 1, nz - 2)) + m->rdz * (F2(u, i, nz - 2) - F2(u, i, nz - 3)));
+                 * (m->rdx * (F2(w, i, nz - 2) - F2(w, i - 1, nz - 2)) + m->lv_rdz_dn * (F2(u, i, nz - 2) - F2(u, i, nz - 3)));
     }
     down /= ((double)(nx - 2.));
     kup /= ((double)(nx - 2.));
     kdown /= ((double)(nx - 2.));
-    double a = (-down) * m->rdz / rhou[nz - 2];
-    double b = (kup - kdown) * m->rdz / rhou[nz - 2];
+    double a = (-down) * m->lv_rdz_c / rhou[nz - 2];
+    double b = (kup - kdown) * m->lv_rdz_c / rhou[nz - 2];
     int sn = (m->step + 1) % 2, so = m->step % 2;
     m->dubarTop_advect[sn] = -a + b;
     if (m->step == 0) m->dubarTop_advect[0] = m->dubarTop_advect[1];
@@ -802,9 +912,9 @@ static void mparam(orc_model* m, double* v) {
             F2(v, i, k) += m->rdx2 * m->dt *
                 (0.5 * (F2(K, i, k) + F2(K, i, k - 1)) * (F2(v, i + 1, k) - F2(v, i, k)) -
                  0.5 * (F2(K, i - 1, k) + F2(K, i - 1, k - 1)) * (F2(v, i, k) - F2(v, i - 1, k)))
-                + m->rdz2 * m->dt / rhow[k] *
+                + m->lv_rdz2M[k] * m->dt / rhow[k] *
                 (rhou[k] * 0.5 * (F2(K, i, k) + F2(K, i - 1, k)) * (F2(v, i, k + 1) - F2(v, i, k)) -
-                 rhou[k - 1] * 0.5 * (F2(K, i, k - 1) + F2(K, i - 1, k - 1)) * (F2(v, i, k) - F2(v, i, k - 1)));
+                 (m->lv_rdM[k] * rhou[k - 1]) * 0.5 * (F2(K, i, k - 1) + F2(K, i - 1, k - 1)) * (F2(v, i, k) - F2(v, i, k - 1)));
 }
 
 /* src/Turbulent.cpp:92-114 */
@@ -816,9 +926,9 @@ static void hparam(orc_model* m, double* v) {
             F2(v, i, k) += m->rdx2 * m->dt *
                 (0.5 * (F2(K, i + 1, k) + F2(K, i, k)) * (F2(v, i + 1, k) - F2(v, i, k)) -
                  0.5 * (F2(K, i, k) + F2(K, i - 1, k)) * (F2(v, i, k) - F2(v, i - 1, k)))
-                + m->rdz2 * m->dt / rhou[k] *
+                + m->lv_rdz2S[k] * m->dt / rhou[k] *
                 (rhow[k + 1] * 0.5 * (F2(K, i, k + 1) + F2(K, i, k)) * (F2(v, i, k + 1) - F2(v, i, k)) -
-                 rhow[k] * 0.5 * (F2(K, i, k) + F2(K, i, k - 1)) * (F2(v, i, k) - F2(v, i, k - 1)));
+                 (m->lv_rdS[k] * rhow[k]) * 0.5 * (F2(K, i, k) + F2(K, i, k - 1)) * (F2(v, i, k) - F2(v, i, k - 1)));
 }
 
 /* Eddy viscosity/diffusivity from deformation and Richardson number, then the
@@ -830,9 +940,9 @@ static void rkm_rkh(orc_model* m) {
     for (int k = 1; k <= nz - 2; k++)
         for (int i = 1; i <= nx - 2; i++) {
             double Rzeta = 0.5 * ((F2(w, i + 1, k + 1) + F2(w, i + 1, k)) - (F2(w, i - 1, k + 1) + F2(w, i - 1, k))) * m->r2dx +
-                           0.5 * ((F2(u, i + 1, k + 1) + F2(u, i, k + 1)) - (F2(u, i + 1, k - 1) + F2(u, i, k - 1))) * m->r2dz;
-            double Rotat = pow((F2(u, i + 1, k) - F2(u, i, k)) * m->rdx + (F2(w, i, k + 1) - F2(w, i, k)) * m->rdz, 2);
-            double Ri = (m->GRAVITY / F2(thp, i, k) * (F2(thp, i, k + 1) - F2(thp, i, k - 1)) * m->r2dz) / (pow(Rzeta, 2) + 2. * Rotat);
+                           0.5 * ((F2(u, i + 1, k + 1) + F2(u, i, k + 1)) - (F2(u, i + 1, k - 1) + F2(u, i, k - 1))) * m->lv_r2dzcc[k];
+            double Rotat = pow((F2(u, i + 1, k) - F2(u, i, k)) * m->rdx + (F2(w, i, k + 1) - F2(w, i, k)) * m->lv_rdzc[k], 2);
+            double Ri = (m->GRAVITY / F2(thp, i, k) * (F2(thp, i, k + 1) - F2(thp, i, k - 1)) * m->lv_r2dzcc[k]) / (pow(Rzeta, 2) + 2. * Rotat);
             double km, kh;
             if (Ri < 0) {
                 km = m->lambda2[k] * sqrt(pow(Rzeta, 2) + 2. * Rotat) * sqrt(1. - 16. * Ri);
@@ -846,8 +956,8 @@ static void rkm_rkh(orc_model* m) {
             }
             km = maxd(km, 10.);
             kh = maxd(kh, 10.);
-            km = mind(km, 0.8 * m->dx * m->dz / m->dt);
-            kh = mind(kh, 0.8 * m->dx * m->dz / m->dt);
+            km = mind(km, m->lv_kmax[k]);
+            kh = mind(kh, m->lv_kmax[k]);
             F2(m->RKM, i, k) = km;
             F2(m->RKH, i, k) = kh;
         }
@@ -872,7 +982,7 @@ static void rkm_rkh(orc_model* m) {
 /* ---------------------------------------------------------------- nudge */
 
 static void nudge_theta(orc_model* m) {  /* src/NumericalProcess.cpp:60-71 */
-    int nz = m->nz, ks = 12000. / m->dz + 1;
+    int nz = m->nz, ks = m->lv_ks;
     for (int k = ks; k < nz - 1; k++) {
         double CGR = m->CRAD * (m->z[k] - m->z[(nz - 1) - ks]) / (m->z[nz - 1] - m->z[(nz - 1) - ks]);
         for (int i = 1; i < m->nx - 1; i++) F2(m->thp, i, k) -= m->dt * CGR * (F2(m->thp, i, k) - m->thb_init[k]);
@@ -880,7 +990,7 @@ static void nudge_theta(orc_model* m) {  /* src/NumericalProcess.cpp:60-71 */
 }
 
 static void nudge_zeta(orc_model* m) {  /* src/NumericalProcess.cpp:73-85 */
-    int nz = m->nz, ks = 12000. / m->dz + 1;
+    int nz = m->nz, ks = m->lv_ks;
     for (int k = ks; k < nz - 1; k++) {
         double CGR = (1. / 360.) * (m->z_zeta[k] - m->z_zeta[(nz - 1) - ks]) / (m->z_zeta[nz - 1] - m->z_zeta[(nz - 1) - ks]);
         for (int i = 1; i < m->nx - 1; i++) F2(m->zetap, i, k) -= m->dt * CGR * (F2(m->zetap, i, k));
@@ -931,6 +1041,7 @@ static void next_time_step(orc_model* m) {
 
 /* The step body of src/Iteration.cpp:246-434 (AB2, WATER, Kessler). */
 static void one_step(orc_model* m) {
+    levels(m);
     m->step++;
     advect_zeta(m); buoyancy(m); bc2d_westdown(m, m->zetap);                 /* pzeta_pt */
     advect_scalar(m, m->th, m->thp, m->dth_advect); bc2d_center(m, m->thp);  /* pth_pt */
@@ -960,6 +1071,7 @@ static void one_step(orc_model* m) {
 }
 
 int orc_call(orc_model* m, const char* n) {
+    levels(m);
     if (!strcmp(n, "pzeta_pt")) { advect_zeta(m); buoyancy(m); bc2d_westdown(m, m->zetap); }
     else if (!strcmp(n, "pth_pt")) { advect_scalar(m, m->th, m->thp, m->dth_advect); bc2d_center(m, m->thp); }
     else if (!strcmp(n, "pqv_pt")) { advect_scalar(m, m->qv, m->qvp, m->dqv_advect); negative_value_process(m, m->qvp); bc2d_center(m, m->qvp); }

@@ -44,6 +44,9 @@ int orc_call(orc_model* m, const char* name);
  * unknown index (k-2)*(nx-2) + (i-1). */
 void orc_solve_A(orc_model* m, const double* b, double* x);
 void orc_apply_A(orc_model* m, const double* x, double* y);
+/* The cal_w system on the model's (possibly stretched) levels: the matrix of
+ * oracle/stretched_poisson.py, the reference's on uniform levels. */
+void orc_solve_W(orc_model* m, const double* b, double* x);
 /* The streamfunction formulation (STREAMFUNCTION, src/PoissonSolver.cpp:14-177,
  * matrix 726-756 with POISSONPARAM = 0): y = A_psi x, x = A_psi^{-1} b exactly,
  * and the switch that makes "one_step" call calpsiuw in place of
