@@ -3,8 +3,8 @@
     python -m vvm_b200.precision_runs {config2,config5} [steps]
 
 config5: NX=8192, NZ=256, dx=dz=100 m, dt=1 s, sheared squall line, 1800 steps;
-config2: NX=1024, NZ=128, dx=dz=250 m, dt=2 s, sheared squall line, 3600 steps
-(uniform levels: the step's stencils take one spacing). Each case runs the
+config2: NX=1024, NZ=128, dx=250 m, stretched levels dz 100 m -> 500 m (tanh
+ramp, stretched_faces), dt=2 s, sheared squall line, 3600 steps. Each case runs the
 mixed step (FP32 fields and stencils, FP64 Poisson residual and reductions)
 with the spectral solve and with the FP32-inner / FP64-refined multigrid
 PCG, against the FP64 step with multigrid PCG, and prints one JSON line with
@@ -21,7 +21,7 @@ import numpy as np
 
 CASES = {
     "config5": dict(NX=8192, NZ=256, dx=100.0, dz=100.0, dt=1.0, steps=1800),
-    "config2": dict(NX=1024, NZ=128, dx=250.0, dz=250.0, dt=2.0, steps=3600),
+    "config2": dict(NX=1024, NZ=128, dx=250.0, dz=100.0, dt=2.0, steps=3600, dz_top=500.0),
 }
 NAMES = ("th", "qc", "qr", "rain", "ke")
 
@@ -42,11 +42,12 @@ VARIANTS = ("fp64_mgpcg", "mixed_spectral", "mixed_mgpcg_refined")
 
 def run(case: str, steps: int | None = None, variants=VARIANTS) -> dict:
     from vvm_b200.gpu import VVM_PREC_FP64, VVM_PREC_MIXED, VVM_SOLVER_MGPCG, VVM_SOLVER_SPECTRAL, VVMGpu
-    from vvm_b200.initial_state import squall_line
+    from vvm_b200.initial_state import squall_line, stretched_faces
     c = CASES[case]
     n = steps or c["steps"]
-    st = squall_line(c["NX"], c["NZ"], c["dx"], c["dz"], c["dt"])
-    out = {"case": case, "steps": n, "grid": {k: c[k] for k in ("NX", "NZ", "dx", "dz", "dt")}}
+    zf = stretched_faces(c["NZ"], c["dz"], c["dz_top"]) if "dz_top" in c else None
+    st = squall_line(c["NX"], c["NZ"], c["dx"], c["dz"], c["dt"], zf=zf)
+    out = {"case": case, "steps": n, "grid": {k: c[k] for k in ("NX", "NZ", "dx", "dz", "dt", "dz_top") if k in c}}
     means = {}
     spec = {"fp64_mgpcg": (VVM_PREC_FP64, VVM_SOLVER_MGPCG),
             "mixed_spectral": (VVM_PREC_MIXED, VVM_SOLVER_SPECTRAL),
