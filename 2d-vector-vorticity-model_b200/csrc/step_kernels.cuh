@@ -299,10 +299,12 @@ __device__ __forceinline__ T vt_flux(const PAdvArgs<T>& a, const T* qr, int i, i
 }
 
 // Mixed step: at most 64 registers a thread, four 256-thread blocks a SM
-// (the kernel is latency-bound; 72 registers allowed three). The FP64 step
-// keeps its register count: a cap would spill.
+// (the kernel is latency-bound; 72 registers allowed three). FP64 step: two
+// blocks a SM, at most 128 registers, which it fits without spills (with the
+// per-level metric loads it would otherwise take 134 and run one block a SM,
+// 1.8x slower).
 template <typename T>
-__global__ void __launch_bounds__(256, (kPert<T> ? 4 : 1)) k_padv(PAdvArgs<T> a) {
+__global__ void __launch_bounds__(256, (kPert<T> ? 4 : 2)) k_padv(PAdvArgs<T> a) {
     __shared__ double sh[32 * 6];
     const Dims& d = a.d;
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;

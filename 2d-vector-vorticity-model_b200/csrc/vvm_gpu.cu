@@ -3694,7 +3694,7 @@ static int learned_train_impl(vvm_gpu_ctx* ctx, int npairs, int steps, int batch
         VecArgs<double> v = P.vargs();
         dim3 B = P.block(), G = P.grid(), g0(cdiv(P.NX, 64), cdiv(N.H[0], 4));
         int rc = VVM_GPU_OK;
-        const int nmodel = (b_host || c->stretched) ? 0 : (npairs + 1) / 2;   // the rest: white noise
+        const int nmodel = b_host ? 0 : (npairs + 1) / 2;   // the rest: white noise
         const int nb = b_host ? npairs / 2 : 0;
         const size_t nun = (size_t)P.NX * P.NK;
         for (int i = 0; i < npairs && rc == VVM_GPU_OK; i++) {

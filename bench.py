@@ -389,8 +389,15 @@ def our_arm(args, rank, world, device):
     if not args.no_accuracy:
         line["mixed"]["accuracy_600_steps"] = mixed_accuracy()
     if not args.no_learned:
-        line["learned"] = learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms / args.steps)
-        line["poisson_stretched"] = stretched_poisson_arm(world, device)
+        from vvm_b200.learned_training import train_on_small_workloads
+        t0 = time.perf_counter()
+        w, trec = train_on_small_workloads(device=device)
+        trec["seconds"] = time.perf_counter() - t0
+        trec["pairs_from"] = ("the plain FP64 multigrid-PCG solver's own pairs: the warm bubble at 128x64 "
+                              "and the squall line at 1024x128 on stretched levels (each half model "
+                              "steps, half white noise); the weights then serve both grids below")
+        line["learned"] = learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms / args.steps, w, trec)
+        line["poisson_stretched"] = stretched_poisson_arm(world, device, w, trec)
     if not args.no_long_runs:
         from vvm_b200.precision_runs import run as long_run
         line["config5_squall_line"] = long_run("config5", variants=("fp64_mgpcg", "mixed_spectral"))
@@ -414,33 +421,23 @@ def net_figures(grid):
     return {"convs": sum(per_level), "pixels": px, "bytes": 128.0 * px, "flops": 2.0 * 9 * 32 * 32 * px}
 
 
-def learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms_per_step, steps=3):
+def learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms_per_step, w, trec, steps=3):
     """Learned-preconditioned step (mixed-precision fields, FP64 flexible CG
-    to the same residual 1e-10) on the headline grid: the network is trained
-    on the model's own solves first (bounded: 32 pairs, 300 Adam steps), then
-    `steps` steps are timed with it and without it (the ablation). The
+    to the same residual 1e-10) on the headline grid with the weights `w`
+    trained on the small workloads (vvm_b200.learned_training), timed over
+    `steps` steps with the network and without it (the ablation). The
     convolutions' roofline comes from repeated forward passes timed between
     one pair of events."""
     import torch
     from vvm_b200.gpu import VVM_PREC_MIXED, VVM_SOLVER_LEARNED, VVMGpu
     from vvm_b200.initial_state import warm_bubble
     st = warm_bubble(NX, NZ, DX, DX, DT)
-    out = {}
-    w = None
+    out = {"training": trec}
     for mode, name in ((0, "with_net"), (1, "without_net")):
         g = VVMGpu(st.grid, precision=VVM_PREC_MIXED, solver=VVM_SOLVER_LEARNED, device=device)
         g.set_stream(torch.cuda.current_stream().cuda_stream)
         g.upload(st)
-        if w is None:
-            t0 = time.perf_counter()
-            lf, ll = g.learned_train(npairs=32, steps=300, batch=2, lr=2e-3, seed=2)
-            g.synchronize()
-            out["training"] = {"pairs": 32, "adam_steps": 300, "batch": 2, "seconds": time.perf_counter() - t0,
-                               "loss_first": lf, "loss_last": ll,
-                               "pairs_from": "16 model steps solved by multigrid-PCG + 16 white-noise rhs"}
-            w = g.learned_weights()
-        else:
-            g.learned_weights(w)
+        g.learned_weights(w)
         g.learned_config(mode=mode, cap=4000)
         g.step(1)
         g.synchronize()
@@ -476,12 +473,12 @@ def learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms_per_step, st
     return out
 
 
-def stretched_poisson_arm(world, device, reps=5):
+def stretched_poisson_arm(world, device, w, trec, reps=5):
     """The stretched-level Poisson workload: the cal_w solve on NX=2048, NZ=256 stretched
     levels (dz 100 m -> 500 m, tanh ramp; dx = 250 m), right-hand sides of
-    seeded bubble/cold-pool vorticity dipoles. Learned-PCG (trained on 16 such
-    right-hand sides plus 16 white-noise ones) against FP64 multigrid-PCG and
-    the spectral solve, each to ||b - A W|| / ||b|| <= 1e-10 from W = 0, device
+    seeded bubble/cold-pool vorticity dipoles. Learned-PCG (the weights `w`
+    trained on the small workloads) against FP64 multigrid-PCG and the
+    spectral solve, each to ||b - A W|| / ||b|| <= 1e-10 from W = 0, device
     buffers, event-timed on the library's stream; `ms_per_solve` is the mean of
     `reps` solves after two warm-up solves."""
     import torch
@@ -493,9 +490,8 @@ def stretched_poisson_arm(world, device, reps=5):
     dev = torch.device(f"cuda:{device}")
     d_b = torch.from_numpy(b).to(dev)
     d_W = torch.zeros_like(d_b)
-    train = np.stack([poisson_rhs(stretched_poisson_case(nx, nz, seed=100 + s)) for s in range(16)])
     out = {"workload": "cal_w on NX=2048 NZ=256 stretched levels dz 100->500 m (tanh), dx=250 m; "
-                       "rhs from 6 seeded vorticity dipoles", "tol": 1e-10}
+                       "rhs from 6 seeded vorticity dipoles", "tol": 1e-10, "training": trec}
     stream = torch.cuda.current_stream()
     for name, solver, mode in (("mgpcg_fp64", VVM_SOLVER_MGPCG, None), ("spectral_fp64", VVM_SOLVER_SPECTRAL, None),
                                ("learned_pcg", VVM_SOLVER_LEARNED, 0), ("learned_cycle_without_net", VVM_SOLVER_LEARNED, 1)):
@@ -504,14 +500,7 @@ def stretched_poisson_arm(world, device, reps=5):
         g.upload(st)
         rec = {}
         if mode is not None:
-            if mode == 0:
-                t0 = time.perf_counter()
-                rec["train"] = g.learned_train_rhs(train, steps=300, batch=2, lr=2e-3, seed=3)
-                g.synchronize()
-                rec["train_s"] = time.perf_counter() - t0
-                w = g.learned_weights()
-            else:
-                g.learned_weights(w)
+            g.learned_weights(w)
             g.learned_config(mode=mode, cap=4000)
         for _ in range(2):
             d_W.zero_()

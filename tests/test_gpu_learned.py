@@ -225,3 +225,35 @@ def test_learned_solve_meets_the_residual_and_beats_the_method_without_it(G):
     assert it_net < it_plain, (it_net, it_plain)
     for h in (g, ref, g2):
         h.close()
+
+
+def test_weights_from_small_workloads_serve_the_large_stretched_solve():
+    """The network trained on the plain solver's pairs from the 128x64 warm
+    bubble and the 1024x128 stretched squall line (few pairs here, to keep
+    the test short) cuts the flexible-CG iterations of the 2048x256
+    stretched-level solve against the same cycle without it, and the solve
+    still meets the FP64 residual."""
+    import torch
+    from vvm_b200 import build
+    from vvm_b200.gpu import VVM_SOLVER_LEARNED, VVMGpu
+    from vvm_b200.initial_state import poisson_rhs, stretched_poisson_case
+    from vvm_b200.learned_training import train_on_small_workloads
+    build.build()
+    w, rec = train_on_small_workloads(pairs_each=400, steps_each=150, batch=4)
+    assert all(g["loss_last"] < g["loss_first"] for g in rec["grids"]), rec
+    st = stretched_poisson_case(2048, 256, seed=7)
+    b = poisson_rhs(st)
+    d_b = torch.from_numpy(b).cuda()
+    its = {}
+    for mode in (0, 1):
+        g = VVMGpu(st.grid, solver=VVM_SOLVER_LEARNED)
+        g.upload(st)
+        g.learned_weights(w)
+        g.learned_config(mode=mode, cap=4000)
+        d_W = torch.zeros_like(d_b)
+        it, rel = g.poisson_solve_device(d_b.data_ptr(), d_W.data_ptr())
+        fcg, fell = g.learned_last()
+        assert not fell and rel <= 1e-10
+        its[mode] = fcg
+        g.close()
+    assert its[0] * 3 < its[1], its
