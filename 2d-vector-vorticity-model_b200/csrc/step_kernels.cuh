@@ -298,18 +298,151 @@ __device__ __forceinline__ T vt_flux(const PAdvArgs<T>& a, const T* qr, int i, i
     return T(a.p.rhow[k]) * VT * s;
 }
 
-// Mixed step: at most 64 registers a thread, four 256-thread blocks a SM
-// (the kernel is latency-bound; 72 registers allowed three). FP64 step: two
-// blocks a SM, at most 128 registers, which it fits without spills (with the
-// per-level metric loads it would otherwise take 134 and run one block a SM,
-// 1.8x slower).
+// cp.async helpers: 16-byte global -> shared copies, grouped per row.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Tile of k_padv: 32 x 8 cells a block of 32 x 8 threads. The four fields
+// are staged into shared memory with two halo cells a side (cp.async, issued
+// first); every face of the tile (33 x 8 x-faces, 32 x 9 z-faces) is then
+// evaluated once, by one thread: its velocity part (in registers) once for
+// all fields, its flux once per field and, for qr, its sedimentation flux,
+// into shared memory; a cell differences the four fluxes around it. The expressions are the per-cell ones of
+// Advection.cpp:36-58, so each cell's tendency is what a thread computing
+// its own four faces would get, at about half the arithmetic (two square
+// roots a face, one pow a sedimentation face) and with every stencil read
+// from shared memory.
+constexpr int kPAdvBX = 32, kPAdvBZ = 8;
+
 template <typename T>
-__global__ void __launch_bounds__(256, (kPert<T> ? 4 : 2)) k_padv(PAdvArgs<T> a) {
-    __shared__ double sh[32 * 6];
+struct PAdvShared {
+    static constexpr int BX = kPAdvBX, BZ = kPAdvBZ, VX = BX + 4, VZ = BZ + 4;
+    T v[4][VZ][VX];           // th, qv, qc, qr at rows k0-2.., columns i0-2..
+    T fx[4][BZ][BX + 1];      // x fluxes of each field
+    T fz[4][BZ + 1][BX];      // z fluxes of each field
+    T gz[BZ + 1][BX];         // sedimentation fluxes of qr
+    double red[32 * 6];       // block_sum scratch
+};
+
+// One element global -> shared, asynchronous (cp.async, 4 or 8 bytes).
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+// Sedimentation flux from s = qr(k) + qr(k-1) at (i, k-1/2) (vt_flux's expression).
+template <typename T>
+__device__ __forceinline__ T vt_flux_s(const PAdvArgs<T>& a, T s, int k) {
+    T VT = T(1E-2) * (T(3634) * pow(T(a.p.vt_c1[k]) * s, T(0.1346)) * T(a.p.vt_fac[k]));
+    return T(a.p.rhow[k]) * VT * s;
+}
+
+// Dynamic shared memory: sizeof(PAdvShared<T>) (about 35 KB FP64, 18 KB
+// mixed). At most 64 registers a thread, four blocks a SM (neither step
+// spills).
+template <typename T>
+__global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
+    constexpr int BX = kPAdvBX, BZ = kPAdvBZ, VX = BX + 4, VZ = BZ + 4;
+    extern __shared__ __align__(16) unsigned char padv_smem[];
+    PAdvShared<T>& S = *reinterpret_cast<PAdvShared<T>*>(padv_smem);
     const Dims& d = a.d;
-    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + BX * ty;
+    const int i0 = 1 + blockIdx.x * BX, k0 = 1 + blockIdx.y * BZ;
+    const int i = i0 + tx, k = k0 + ty;
     const bool act = (i <= d.nx - 2 && k <= d.nz - 2);
+
+    // Stage the fields: only points inside the array are copied; the ones
+    // outside (row -1, column -1, beyond nz-1 or nx-1) are never read, since
+    // a face reads its outer neighbours only where the third-order bracket
+    // applies (2 <= index <= n-3).
+    for (int f = 0; f < 4; f++) {
+        if (!(a.mask & (1 << f))) continue;
+        const T* v = a.now[f];
+        for (int t = tid; t < VZ * VX; t += BX * BZ) {
+            const int r = t / VX, c = t - r * VX;
+            const int kk = k0 - 2 + r, ii = i0 - 2 + c;
+            if (kk >= 0 && kk <= d.nz - 1 && ii >= 0 && ii <= d.nx - 1) cp_async_elem(&S.v[f][r][c], v + d.at(ii, kk));
+        }
+    }
+    cp_async_commit();
+
+    // Faces: x face (r, c) is fi = i0 + c, between cells fi-1 and fi, on row
+    // k0 + r; the east face of cell nx-2 is the halo copy of face 1
+    // (BoundaryProcess2D_center on flux_u, Advection.cpp:55). z face (r, c) is
+    // fk = k0 + r, between cells fk-1 and fk, in column i0 + c; face nz-1
+    // carries no flux (Advection.cpp:57-58).
+    auto xface_ok = [&](int r, int c) { return k0 + r <= d.nz - 2 && i0 + c <= d.nx - 1; };
+    auto zface_ok = [&](int r, int c) { return k0 + r <= d.nz - 2 && i0 + c <= d.nx - 2; };
+    auto zflux_ok = [&](int r, int c) { return k0 + r <= d.nz - 1 && i0 + c <= d.nx - 2; };
+    auto xface_i = [&](int c) { int fi = i0 + c; return fi == d.nx - 1 ? 1 : fi; };
+
+    // velocity parts of the thread's own faces, its cell's west and bottom
+    // ones, while the copies are in flight
+    const bool xo = xface_ok(ty, tx), zo = zface_ok(ty, tx), zfo = zflux_ok(ty, tx);
+    Face<T> Fx{}, Fz{};
+    if (xo) Fx = face_u(a, xface_i(tx), k0 + ty);
+    if (zo) Fz = face_w(a, i0 + tx, k0 + ty);
+    cp_async_wait<0>();
+    __syncthreads();
+
+    auto xflux = [&](const Face<T>& F, int f, int r, int c) {
+        if (i0 + c == d.nx - 1) {   // face 1 (no bracket), read where it lies
+            const T* v = a.now[f];
+            return face_flux(F, T(0), v[d.at(0, k0 + r)], v[d.at(1, k0 + r)], T(0));
+        }
+        const T* row = &S.v[f][r + 2][c];   // columns fi-2 .. fi+1
+        return face_flux(F, F.hi ? row[0] : T(0), row[1], row[2], F.hi ? row[3] : T(0));
+    };
+    // th and qv of the mixed step take the perturbation form (third-order
+    // differences with the profile's d0)
+    auto zflux = [&](const Face<T>& F, int f, int r, int c) {
+        const int fk = k0 + r;
+        if (fk == d.nz - 1) return T(0);
+        const T vmm = S.v[f][r][c + 2], vm = S.v[f][r + 1][c + 2], v0 = S.v[f][r + 2][c + 2],
+                vp = S.v[f][r + 3][c + 2];   // rows fk-2 .. fk+1
+        if (kPert<T> && f < 2 && F.hi) {
+            const double* d0 = a.p.d0[f];
+            return face_flux_pert(F, vmm, vm, v0, vp, T(d0[fk - 1]), T(d0[fk]), T(d0[fk + 1]));
+        }
+        return face_flux(F, F.hi ? vmm : T(0), vm, v0, F.hi ? vp : T(0));
+    };
+    auto gflux = [&](int r, int c) {
+        const int fk = k0 + r;
+        return fk == d.nz - 1 ? T(0) : vt_flux_s(a, S.v[3][r + 2][c + 2] + S.v[3][r + 1][c + 2], fk);
+    };
+
+    const bool vt = (a.mask & F_QR) && a.do_vt;
+    for (int f = 0; f < 4; f++) {
+        if (!(a.mask & (1 << f))) continue;
+        if (xo) S.fx[f][ty][tx] = xflux(Fx, f, ty, tx);
+        if (zfo) S.fz[f][ty][tx] = zflux(Fz, f, ty, tx);
+    }
+    if (vt && zfo) S.gz[ty][tx] = gflux(ty, tx);
+    // the tile's east column of x faces (warp 0, lanes 0..7, one a row) and
+    // its top row of z faces (warp 1)
+    if (ty == 0 && tx < BZ && xface_ok(tx, BX)) {
+        const Face<T> F = face_u(a, xface_i(BX), k0 + tx);
+        for (int f = 0; f < 4; f++)
+            if (a.mask & (1 << f)) S.fx[f][tx][BX] = xflux(F, f, tx, BX);
+    }
+    if (ty == 1 && zflux_ok(BZ, tx)) {
+        Face<T> F{};
+        if (zface_ok(BZ, tx)) F = face_w(a, i0 + tx, k0 + BZ);
+        for (int f = 0; f < 4; f++)
+            if (a.mask & (1 << f)) S.fz[f][BZ][tx] = zflux(F, f, BZ, tx);
+        if (vt) S.gz[BZ][tx] = gflux(BZ, tx);
+    }
+    __syncthreads();
+
     double sums[6] = {0, 0, 0, 0, 0, 0};
     if (act) {
         const size_t id = d.at(i, k);
@@ -318,32 +451,14 @@ __global__ void __launch_bounds__(256, (kPert<T> ? 4 : 2)) k_padv(PAdvArgs<T> a)
         // mixed step: one division for the cell's flux divergences (the FP64
         // step keeps the reference's (difference * r2d) / rhou per term)
         const T sx = kPert<T> ? T(a.c.r2dx) / ru : T(0), sz = kPert<T> ? T(a.p.r2dzc[k]) / ru : T(0);
-        // velocity parts of the four faces, shared by the four fields;
-        // flux_u at nx-1 is the halo copy of flux_u at 1, flux_w at nz-1 is
-        // zeroed (Advection.cpp:55-58)
         const int ip = (i == d.nx - 2) ? 1 : i + 1;
-        const Face<T> Fu0 = face_u(a, i, k), Fup = face_u(a, ip, k);
-        const Face<T> Fw0 = face_w(a, i, k);
         const bool top = (k == d.nz - 2);
-        Face<T> Fwp = Fw0;
-        if (!top) Fwp = face_w(a, i, k + 1);
-        auto X = [&](const T* v, int ii, int kk) { return v[d.at(ii, kk)]; };
         for (int f = 0; f < 4; f++) {
             if (!(a.mask & (1 << f))) continue;
-            const T* v = a.now[f];
-            // x faces i-1/2 and ip-1/2, z faces k-1/2 and k+1/2 (third-order
-            // neighbours read only where the bracket applies)
-            T fu_0 = face_flux(Fu0, Fu0.hi ? X(v, i - 2, k) : T(0), X(v, i - 1, k), X(v, i, k),
-                               Fu0.hi ? X(v, i + 1, k) : T(0));
-            T fu_p = face_flux(Fup, Fup.hi ? X(v, ip - 2, k) : T(0), X(v, ip - 1, k), X(v, ip, k),
-                               Fup.hi ? X(v, ip + 1, k) : T(0));
+            const T fu_0 = S.fx[f][ty][tx], fu_p = S.fx[f][ty][tx + 1];
+            const T fw_0 = S.fz[f][ty][tx], fw_p = S.fz[f][ty + 1][tx];
             T px, pz;
             if (!kPert<T> || f >= 2) {
-                T fw_0 = face_flux(Fw0, Fw0.hi ? X(v, i, k - 2) : T(0), X(v, i, k - 1), X(v, i, k),
-                                   Fw0.hi ? X(v, i, k + 1) : T(0));
-                T fw_p = top ? T(0)
-                             : face_flux(Fwp, Fwp.hi ? X(v, i, k - 1) : T(0), X(v, i, k), X(v, i, k + 1),
-                                         Fwp.hi ? X(v, i, k + 2) : T(0));
                 if constexpr (kPert<T>) {
                     px = (fu_p - fu_0) * sx;
                     pz = (fw_p - fw_0) * sz;
@@ -355,15 +470,6 @@ __global__ void __launch_bounds__(256, (kPert<T> ? 4 : 2)) k_padv(PAdvArgs<T> a)
                 // v = v0(k) + v': the v0 parts of both fluxes are added in
                 // difference form, 2 v0 (u[i+1] - u[i]) in x and
                 // s0[k+1] (m[k+1] - m[k]) + m[k] g0[k] in z, m = rhow w.
-                const double* d0 = a.p.d0[f];
-                T fw_0 = Fw0.hi ? face_flux_pert(Fw0, X(v, i, k - 2), X(v, i, k - 1), X(v, i, k), X(v, i, k + 1),
-                                                 T(d0[k - 1]), T(d0[k]), T(d0[k + 1]))
-                                : face_flux(Fw0, T(0), X(v, i, k - 1), X(v, i, k), T(0));
-                T fw_p = T(0);
-                if (!top)
-                    fw_p = Fwp.hi ? face_flux_pert(Fwp, X(v, i, k - 1), X(v, i, k), X(v, i, k + 1), X(v, i, k + 2),
-                                                   T(d0[k]), T(d0[k + 1]), T(d0[k + 2]))
-                                  : face_flux(Fwp, T(0), X(v, i, k), X(v, i, k + 1), T(0));
                 T m0 = T(a.p.rhow[k]) * a.w[d.at(i, k)];
                 T refz = top ? -m0 * T(a.p.s0[f][k])
                              : T(a.p.s0[f][k + 1]) * (T(a.p.rhow[k + 1]) * a.w[d.at(i, k + 1)] - m0) +
@@ -374,10 +480,9 @@ __global__ void __launch_bounds__(256, (kPert<T> ? 4 : 2)) k_padv(PAdvArgs<T> a)
             }
             T t = -px - pz;
             T o = ab2_push(a.hn[f], a.ho[f], id, t, a.ab);
-            T out = v[id] + dt15 * t - dt05 * o;
-            if (f == 3 && a.do_vt) {
-                T gp = (k == d.nz - 2) ? T(0) : vt_flux(a, v, i, k + 1);
-                T g0 = vt_flux(a, v, i, k);
+            T out = S.v[f][ty + 2][tx + 2] + dt15 * t - dt05 * o;
+            if (f == 3 && vt) {
+                const T gp = S.gz[ty + 1][tx], g0 = S.gz[ty][tx];
                 T tv = kPert<T> ? (gp - g0) * sz : (gp - g0) * T(a.p.r2dzc[k]) / ru;
                 T ov = ab2_push(a.hvt_n, a.hvt_o, id, tv, a.ab);
                 out += dt15 * tv - dt05 * ov;
@@ -399,8 +504,8 @@ __global__ void __launch_bounds__(256, (kPert<T> ? 4 : 2)) k_padv(PAdvArgs<T> a)
         }
     }
     if (a.nvp_mask) {
-        block_sum(sums, sh);
-        if (threadIdx.x == 0 && threadIdx.y == 0) {
+        block_sum(sums, S.red);
+        if (tid == 0) {
             double* out = a.partial + (size_t)(blockIdx.x + gridDim.x * blockIdx.y) * 6;
 #pragma unroll
             for (int j = 0; j < 6; j++) out[j] = sums[j];
@@ -1150,15 +1255,6 @@ __global__ void k_gs_coeffs(GSArgs<T> a) {
     a.C[e] = cz * czd;
     a.B[e] = cx * bx;
 }
-
-// cp.async helpers: 16-byte global -> shared copies, grouped per row.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 constexpr int kGSSpinLimit = 1 << 22;   // polls before a wait gives up
 constexpr int kGSErrWait = 1;           // device error word: a Gauss-Seidel wait gave up

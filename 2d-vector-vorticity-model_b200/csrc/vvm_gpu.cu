@@ -1516,6 +1516,9 @@ struct vvm_gpu_ctx {
     const double* offset_qv() const { return mixed ? pref[1] : nullptr; }
     dim3 blk() const { return dim3(64, 4); }
     dim3 grid_interior(int k0) const { return dim3(cdiv(d.nx - 2, 64), cdiv(d.nz - 1 - k0, 4)); }
+    // k_padv's tiles of kPAdvBX x kPAdvBZ interior cells
+    dim3 padv_blk() const { return dim3(kPAdvBX, kPAdvBZ); }
+    dim3 padv_grid() const { return dim3(cdiv(d.nx - 2, kPAdvBX), cdiv(d.nz - 2, kPAdvBZ)); }
     dim3 grid_all() const { return dim3(cdiv(d.nx, 64), cdiv(d.nz, 4)); }
 };
 
@@ -1611,8 +1614,9 @@ void launch_padv(vvm_gpu_ctx* c, int mask, int nvp_mask, bool vt, bool precip) {
     a.do_vt = vt;
     a.do_precip = precip;
     a.ab = ab;
-    dim3 g = c->grid_interior(1);
-    LAUNCH(&c->stats, VVM_K_PADV, c->stream, k_padv<T><<<g, c->blk(), 0, c->stream>>>(a));
+    dim3 g = c->padv_grid();
+    LAUNCH(&c->stats, VVM_K_PADV, c->stream,
+           k_padv<T><<<g, c->padv_blk(), sizeof(PAdvShared<T>), c->stream>>>(a));
     CKL();
     if (nvp_mask) {
         LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp));
@@ -3296,9 +3300,14 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         }
         c->ubar = c->ar.alloc<double>(2);
         c->dubar = c->ar.alloc<double>(2);
-        dim3 g = c->grid_interior(1);
-        c->npart = g.x * g.y;
+        // block partials of k_padv and k_kessler (NegativeValueProcess sums)
+        dim3 g = c->grid_interior(1), ga = c->padv_grid();
+        c->npart = std::max(g.x * g.y, ga.x * ga.y);
         c->partial = c->ar.alloc<double>((size_t)c->npart * 6);
+        CK(cudaFuncSetAttribute(k_padv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(PAdvShared<double>)));
+        CK(cudaFuncSetAttribute(k_padv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(PAdvShared<float>)));
         c->nvp = c->ar.alloc<double>(6);
         c->staging = c->ar.alloc<double>((size_t)c->d.nx * c->d.nz * 2);
         c->wctl = c->ar.alloc<CGCtl>(1);
