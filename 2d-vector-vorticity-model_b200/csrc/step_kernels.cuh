@@ -67,6 +67,25 @@ __device__ __forceinline__ T ab2_push(T* hn, T* ho, size_t idx, T tend, const AB
     return old;
 }
 
+// cp.async helpers: 16-byte global -> shared copies, grouped per row.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// One element global -> shared, asynchronous (cp.async, 4 or 8 bytes).
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Vorticity advection + buoyancy + westdown halo of zetap
 // (Iteration::pzeta_pt: Advection.cpp:84-149, Buoyancy.cpp:11-58,
@@ -84,104 +103,161 @@ struct PZetaArgs {
     AB2 ab;
 };
 
-// Staggered mass fluxes of Advection_zeta (Advection.cpp:90-91), interior only.
+// x-face mass flux Uw of Advection_zeta (Advection.cpp:90) from global
+// memory: the halo face of k_pzeta's first tile.
 template <typename T>
 __device__ __forceinline__ T zeta_Uw(const PZetaArgs<T>& a, int i, int k) {
     const Dims& d = a.d;
     return T(0.25) * (T(a.p.rhou[k]) * (a.u[d.at(i + 1, k)] + a.u[d.at(i, k)]) +
                       T(a.p.rhou[k - 1]) * (a.u[d.at(i + 1, k - 1)] + a.u[d.at(i, k - 1)]));
 }
-template <typename T>
-__device__ __forceinline__ T zeta_Wu(const PZetaArgs<T>& a, int i, int k) {
-    const Dims& d = a.d;
-    return T(0.25) * (T(a.p.rhow[k + 1]) * (a.w[d.at(i, k + 1)] + a.w[d.at(i - 1, k + 1)]) +
-                      T(a.p.rhow[k]) * (a.w[d.at(i, k)] + a.w[d.at(i - 1, k)]));
-}
 
-// x flux at face (i+1/2, k) for i = 1..nx-2 (Advection.cpp:107,111-114).
+// Tile of k_pzeta: 32 x 8 zeta points a block of 32 x 8 threads. zeta, u, w,
+// th, qv, qc and qr are staged into shared memory (cp.async); the staggered
+// mass fluxes Uw, Wu (Advection.cpp:90-91) are formed once a face point, the
+// x and z fluxes once a face, and each point then differences its four
+// fluxes and forms its buoyancy from the staged values.
+constexpr int kPZBX = 32, kPZBZ = 8;
+
 template <typename T>
-__device__ __forceinline__ T zeta_flux_u(const PZetaArgs<T>& a, int i, int k) {
+struct PZetaShared {
+    static constexpr int BX = kPZBX, BZ = kPZBZ;
+    T z[BZ + 4][BX + 4];      // zeta: rows k0-2.., columns i0-2..
+    T u[BZ + 1][BX + 4];      // u: rows k0-1.., columns i0-2..
+    T w[BZ + 4][BX + 1];      // w: rows k0-2.., columns i0-1..
+    T q[4][BZ + 1][BX + 1];   // th, qv, qc, qr: rows k0-1.., columns i0-1..
+    T U[BZ][BX + 3];          // Uw at x faces fi = i0-2.., rows k0..
+    T W[BZ + 3][BX];          // Wu at z faces fk = k0-2.., columns i0..
+    T fu[BZ][BX + 1];         // flux_u at fi = i0-1..
+    T fw[BZ + 1][BX];         // flux_w at fk = k0-1..
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kPZBX * kPZBZ) k_pzeta(PZetaArgs<T> a) {
+    constexpr int BX = kPZBX, BZ = kPZBZ, NT = BX * BZ;
+    __shared__ PZetaShared<T> S;
     const Dims& d = a.d;
-    const T* z = a.zeta;
-    T U = zeta_Uw(a, i, k);
-    T f = U * (z[d.at(i + 1, k)] + z[d.at(i, k)]);
-    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
-        T Um = zeta_Uw(a, i - 1, k), Up = zeta_Uw(a, i + 1, k);
-        T z0 = z[d.at(i - 1, k)], z1 = z[d.at(i, k)], z2 = z[d.at(i + 1, k)], z3 = z[d.at(i + 2, k)];
-        f += T(-1. / 3.) * (plus_part(U) * (z2 - z1) - sqrt(plus_part(U) * plus_part(Um)) * (z1 - z0) -
-                            minus_part(U) * (z2 - z1) - sqrt(fabs(minus_part(U) * minus_part(Up))) * (z3 - z2));
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + BX * ty;
+    const int i0 = 1 + blockIdx.x * BX, k0 = 2 + blockIdx.y * BZ;
+    const int i = i0 + tx, k = k0 + ty;
+    const bool act = (i <= d.nx - 2 && k <= d.nz - 2);
+
+    // Stage: points outside the array are skipped; none of them is read (a
+    // flux reads its outer neighbours only where the third-order bracket
+    // applies, 2 <= index <= n-3).
+    auto stage = [&](T* dst, const T* src, int rows, int cols, int kb, int ib) {
+        for (int t = tid; t < rows * cols; t += NT) {
+            const int r = t / cols, c = t - r * cols;
+            const int kk = kb + r, ii = ib + c;
+            if (kk >= 0 && kk <= d.nz - 1 && ii >= 0 && ii <= d.nx - 1) cp_async_elem(dst + t, src + d.at(ii, kk));
+        }
+    };
+    stage(&S.z[0][0], a.zeta, BZ + 4, BX + 4, k0 - 2, i0 - 2);
+    stage(&S.u[0][0], a.u, BZ + 1, BX + 4, k0 - 1, i0 - 2);
+    stage(&S.w[0][0], a.w, BZ + 4, BX + 1, k0 - 2, i0 - 1);
+    const T* qs[4] = {a.th, a.qv, a.qc, a.qr};
+#pragma unroll
+    for (int f = 0; f < 4; f++) stage(&S.q[f][0][0], qs[f], BZ + 1, BX + 1, k0 - 1, i0 - 1);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+
+    // Uw(fi, k), fi = 0..nx-2, and Wu(i, fk), fk = 1..nz-2 (Advection.cpp:90-91)
+    for (int t = tid; t < BZ * (BX + 3); t += NT) {
+        const int r = t / (BX + 3), c = t - r * (BX + 3);
+        const int fi = i0 - 2 + c, kk = k0 + r;
+        if (fi >= 0 && fi <= d.nx - 2 && kk <= d.nz - 2) {
+            const int uc = c, ur = r + 1;   // u at (fi, kk) in the staged tile
+            S.U[r][c] = T(0.25) * (T(a.p.rhou[kk]) * (S.u[ur][uc + 1] + S.u[ur][uc]) +
+                                   T(a.p.rhou[kk - 1]) * (S.u[ur - 1][uc + 1] + S.u[ur - 1][uc]));
+        }
     }
-    return f;
-}
-
-// z flux at face (i, k+1/2) for k = 1..nz-2 (Advection.cpp:108,115-118).
-template <typename T>
-__device__ __forceinline__ T zeta_flux_w(const PZetaArgs<T>& a, int i, int k) {
-    const Dims& d = a.d;
-    const T* z = a.zeta;
-    T W = zeta_Wu(a, i, k);
-    T f = W * (z[d.at(i, k + 1)] + z[d.at(i, k)]);
-    if (i >= 2 && i <= d.nx - 3 && k >= 2 && k <= d.nz - 3) {
-        T Wm = zeta_Wu(a, i, k - 1), Wp = zeta_Wu(a, i, k + 1);
-        T z0 = z[d.at(i, k - 1)], z1 = z[d.at(i, k)], z2 = z[d.at(i, k + 1)], z3 = z[d.at(i, k + 2)];
-        f += T(-1. / 3.) * (plus_part(W) * (z2 - z1) - sqrt(plus_part(W) * plus_part(Wm)) * (z1 - z0) -
-                            minus_part(W) * (z2 - z1) - sqrt(fabs(minus_part(W) * minus_part(Wp))) * (z3 - z2));
+    for (int t = tid; t < (BZ + 3) * BX; t += NT) {
+        const int r = t / BX, c = t - r * BX;
+        const int fk = k0 - 2 + r, ii = i0 + c;
+        if (fk >= 1 && fk <= d.nz - 2 && ii <= d.nx - 2) {
+            const int wc = c + 1, wr = r;   // w at (ii, fk)
+            S.W[r][c] = T(0.25) * (T(a.p.rhow[fk + 1]) * (S.w[wr + 1][wc] + S.w[wr + 1][wc - 1]) +
+                                   T(a.p.rhow[fk]) * (S.w[wr][wc] + S.w[wr][wc - 1]));
+        }
     }
-    return f;
-}
+    __syncthreads();
 
-template <typename T>
-__device__ __forceinline__ T thv_at(const PZetaArgs<T>& a, int i, int k) {  // Buoyancy.cpp:3-9
-    size_t id = a.d.at(i, k);
-    return a.th[id] * (T(1) + T(0.608) * a.qv[id]);
-}
+    // x flux at face (fi+1/2, k), fi = 1..nx-2 (Advection.cpp:107,111-114);
+    // the west face of point 1 is the halo copy of face nx-2 (Advection.cpp:123)
+    for (int t = tid; t < BZ * (BX + 1); t += NT) {
+        const int r = t / (BX + 1), c = t - r * (BX + 1);
+        const int fi = i0 - 1 + c, kk = k0 + r;
+        if (kk > d.nz - 2 || fi > d.nx - 2) continue;
+        T f;
+        if (fi == 0) {
+            const int e = d.nx - 2;   // no bracket at nx-2
+            f = zeta_Uw(a, e, kk) * (a.zeta[d.at(e + 1, kk)] + a.zeta[d.at(e, kk)]);
+        } else {
+            const T U = S.U[r][c + 1];
+            const T* zr = &S.z[r + 2][c];   // zeta at fi-1 .. fi+2
+            f = U * (zr[2] + zr[1]);
+            if (fi >= 2 && fi <= d.nx - 3 && kk >= 2 && kk <= d.nz - 3) {
+                const T Um = S.U[r][c], Up = S.U[r][c + 2];
+                const T z0 = zr[0], z1 = zr[1], z2 = zr[2], z3 = zr[3];
+                f += T(-1. / 3.) * (plus_part(U) * (z2 - z1) - sqrt(plus_part(U) * plus_part(Um)) * (z1 - z0) -
+                                    minus_part(U) * (z2 - z1) - sqrt(fabs(minus_part(U) * minus_part(Up))) * (z3 - z2));
+            }
+        }
+        S.fu[r][c] = f;
+    }
+    // z flux at face (i, fk+1/2), fk = 1..nz-2 (Advection.cpp:108,115-118)
+    for (int t = tid; t < (BZ + 1) * BX; t += NT) {
+        const int r = t / BX, c = t - r * BX;
+        const int fk = k0 - 1 + r, ii = i0 + c;
+        if (fk > d.nz - 2 || ii > d.nx - 2) continue;
+        const T W = S.W[r + 1][c];
+        const int zc = c + 2, zr = r + 1;   // zeta (ii, fk) in the staged tile
+        T f = W * (S.z[zr + 1][zc] + S.z[zr][zc]);
+        if (ii >= 2 && ii <= d.nx - 3 && fk >= 2 && fk <= d.nz - 3) {
+            const T Wm = S.W[r][c], Wp = S.W[r + 2][c];
+            const T z0 = S.z[zr - 1][zc], z1 = S.z[zr][zc], z2 = S.z[zr + 1][zc], z3 = S.z[zr + 2][zc];
+            f += T(-1. / 3.) * (plus_part(W) * (z2 - z1) - sqrt(plus_part(W) * plus_part(Wm)) * (z1 - z0) -
+                                minus_part(W) * (z2 - z1) - sqrt(fabs(minus_part(W) * minus_part(Wp))) * (z3 - z2));
+        }
+        S.fw[r][c] = f;
+    }
+    __syncthreads();
+    if (!act) return;
 
-// thv(i,k) - thv(i-1,k) from perturbations th', qv' about th0(k), qv0(k):
-// dth' + 0.608 (th0 dqv' + qv0 dth' + (th'q')_i - (th'q')_{i-1}); the large
-// reference values never enter a difference.
-template <typename T>
-__device__ __forceinline__ T thv_dx(const PZetaArgs<T>& a, int i, int k) {
-    size_t id = a.d.at(i, k), im = a.d.at(i - 1, k);
-    T t1 = a.th[id], t0 = a.th[im], q1 = a.qv[id], q0 = a.qv[im];
-    T dt = t1 - t0, dq = q1 - q0;
-    return dt + T(0.608) * (T(a.p.ref[0][k]) * dq + T(a.p.ref[1][k]) * dt + (t1 * q1 - t0 * q0));
-}
-
-template <typename T>
-__global__ void k_pzeta(PZetaArgs<T> a) {
-    const Dims& d = a.d;
-    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = 2 + blockIdx.y * blockDim.y + threadIdx.y;
-    if (i > d.nx - 2 || k > d.nz - 2) return;
     const size_t id = d.at(i, k);
     const T dt15 = T(1.5 * a.c.dt), dt05 = T(0.5 * a.c.dt);
-    // Advection_zeta: flux differences; flux_u at i-1 = 0 is the halo copy of
-    // flux_u at nx-2 (BoundaryProcess2D_center on flux_u, Advection.cpp:123).
-    T fu_i = zeta_flux_u(a, i, k);
-    T fu_m = zeta_flux_u(a, (i == 1) ? d.nx - 2 : i - 1, k);
-    T fw_k = zeta_flux_w(a, i, k);
-    T fw_m = zeta_flux_w(a, i, k - 1);
+    const T fu_i = S.fu[ty][tx + 1], fu_m = S.fu[ty][tx];
+    const T fw_k = S.fw[ty + 1][tx], fw_m = S.fw[ty][tx];
     T rw = T(a.p.rhow[k]);
     T px = (fu_i - fu_m) * T(a.c.r2dx) / rw;
     T pz = (fw_k - fw_m) * T(a.p.r2dzw[k]) / rw;
     T tz = -px - pz;
     T oz = ab2_push(a.hz_n, a.hz_o, id, tz, a.ab);
-    T zp = a.zeta[id] + dt15 * tz - dt05 * oz;
-    // Bouyancy (Buoyancy.cpp:25-48)
+    T zp = S.z[ty + 2][tx + 2] + dt15 * tz - dt05 * oz;
+    // Bouyancy (Buoyancy.cpp:25-48); staged q[f][r][c] is (i0-1+c, k0-1+r)
+    const int r1 = ty + 1, r0 = ty, c1 = tx + 1, c0 = tx;
+    auto Q = [&](int f, int r, int c) { return S.q[f][r][c]; };
     T g_rw = T(a.c.gravity) / rw;
     T b;
     if constexpr (!kPert<T>) {
+        auto thv = [&](int r, int c) { return Q(0, r, c) * (T(1) + T(0.608) * Q(1, r, c)); };   // Buoyancy.cpp:3-9
         b = g_rw * T(0.5) *
-            ((thv_at(a, i, k) - thv_at(a, i - 1, k)) / T(a.p.thvb[k]) +
-             (thv_at(a, i, k - 1) - thv_at(a, i - 1, k - 1)) / T(a.p.thvb[k - 1])) * T(a.c.rdx);
-    } else {
-        b = g_rw * T(0.5) * (thv_dx(a, i, k) / T(a.p.thvb[k]) + thv_dx(a, i, k - 1) / T(a.p.thvb[k - 1])) *
+            ((thv(r1, c1) - thv(r1, c0)) / T(a.p.thvb[k]) + (thv(r0, c1) - thv(r0, c0)) / T(a.p.thvb[k - 1])) *
             T(a.c.rdx);
+    } else {
+        // thv(i) - thv(i-1) from perturbations th', qv' about th0(k), qv0(k):
+        // dth' + 0.608 (th0 dqv' + qv0 dth' + (th'q')_i - (th'q')_{i-1}); the
+        // large reference values never enter a difference
+        auto thv_dx = [&](int r, int kk) {
+            T t1 = Q(0, r, c1), t0 = Q(0, r, c0), q1 = Q(1, r, c1), q0 = Q(1, r, c0);
+            T dt = t1 - t0, dq = q1 - q0;
+            return dt + T(0.608) * (T(a.p.ref[0][kk]) * dq + T(a.p.ref[1][kk]) * dt + (t1 * q1 - t0 * q0));
+        };
+        b = g_rw * T(0.5) * (thv_dx(r1, k) / T(a.p.thvb[k]) + thv_dx(r0, k - 1) / T(a.p.thvb[k - 1])) * T(a.c.rdx);
     }
-    T bc = g_rw * (T(0.5) * (a.qc[id] + a.qc[d.at(i, k - 1)]) -
-                   T(0.5) * (a.qc[d.at(i - 1, k)] + a.qc[d.at(i - 1, k - 1)])) * T(a.c.rdx);
-    T br = g_rw * (T(0.5) * (a.qr[id] + a.qr[d.at(i, k - 1)]) -
-                   T(0.5) * (a.qr[d.at(i - 1, k)] + a.qr[d.at(i - 1, k - 1)])) * T(a.c.rdx);
+    T bc = g_rw * (T(0.5) * (Q(2, r1, c1) + Q(2, r0, c1)) - T(0.5) * (Q(2, r1, c0) + Q(2, r0, c0))) * T(a.c.rdx);
+    T br = g_rw * (T(0.5) * (Q(3, r1, c1) + Q(3, r0, c1)) - T(0.5) * (Q(3, r1, c0) + Q(3, r0, c0))) * T(a.c.rdx);
     T tb = b + (-bc - br);
     T ob = ab2_push(a.hb_n, a.hb_o, id, tb, a.ab);
     zp += (dt15 * tb) - (dt05 * ob);
@@ -298,15 +374,6 @@ __device__ __forceinline__ T vt_flux(const PAdvArgs<T>& a, const T* qr, int i, i
     return T(a.p.rhow[k]) * VT * s;
 }
 
-// cp.async helpers: 16-byte global -> shared copies, grouped per row.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
 // Tile of k_padv: 32 x 8 cells a block of 32 x 8 threads. The four fields
 // are staged into shared memory with two halo cells a side (cp.async, issued
 // first); every face of the tile (33 x 8 x-faces, 32 x 9 z-faces) is then
@@ -328,16 +395,6 @@ struct PAdvShared {
     T gz[BZ + 1][BX];         // sedimentation fluxes of qr
     double red[32 * 6];       // block_sum scratch
 };
-
-// One element global -> shared, asynchronous (cp.async, 4 or 8 bytes).
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
-    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    if constexpr (sizeof(T) == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
 
 // Sedimentation flux from s = qr(k) + qr(k-1) at (i, k-1/2) (vt_flux's expression).
 template <typename T>
@@ -1812,8 +1869,10 @@ __global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) {
 // from the top down (PoissonSolver.cpp:644-651), with the center halo of u.
 // A block owns 32 columns (lanes) and kColSeg z-segments (warps): each thread
 // sums its segment, the segment totals are scanned from the top in shared
-// memory, then each thread writes its rows.
-constexpr int kColSeg = 8;
+// memory, then each thread writes its rows. Thirty-two segments give the 64
+// blocks of a 2048-column grid 32 warps each (about 8 rows a thread at
+// NZ = 256), so the short chains, not a few long ones, set the time.
+constexpr int kColSeg = 32;
 
 template <typename T>
 __global__ void __launch_bounds__(32 * kColSeg) k_cal_u_columns(CalUArgs<T> a) {

@@ -1581,7 +1581,8 @@ void launch_pzeta(vvm_gpu_ctx* c) {
     PZetaArgs<T> a{c->d, c->c, c->profiles(), F.zeta[now], F.u, F.w, F.th[now], F.qv[now], F.qc[now], F.qr[now],
                    F.zeta[fut], F.hist[H_ZETA][ab.sn], F.hist[H_ZETA][ab.so], F.hist[H_BUOY][ab.sn],
                    F.hist[H_BUOY][ab.so], ab};
-    LAUNCH(&c->stats, VVM_K_PZETA, c->stream, k_pzeta<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(a));
+    dim3 g(cdiv(c->d.nx - 2, kPZBX), cdiv(c->d.nz - 3, kPZBZ));
+    LAUNCH(&c->stats, VVM_K_PZETA, c->stream, k_pzeta<T><<<g, dim3(kPZBX, kPZBZ), 0, c->stream>>>(a));
     CKL();
 }
 
