@@ -668,4 +668,51 @@ __global__ void k_loop_outer(const CGScalars* sc64, CGCtl* ctl, const CGCtl* inn
                              cudaGraphConditionalHandle h, double tol2, int maxit, int init, long long* exec,
                              int body_kernels);
 
+// The check that opens a graph-recorded solve, in one launch (what
+// k_zero_if_b0, k_cg_residual, k_cg_scalar and k_loop_plain do in turn):
+// W = 0 when ||b|| = 0 (r = f then, and W is not read), r = f - S W and
+// ||rhow r||^2 in per-block partials; the block that arrives last
+// (arrive_last) totals them in a fixed order into sc->rr, starts the loop
+// state (ctl) and sets the condition of the WHILE node that follows:
+// continue while ||rhow r||^2 > tol^2 ||b||^2 and maxit > 0.
+template <typename P>
+__global__ void k_cg_check(VecArgs<P> v, const P* f, P* x, P* r, double* partial, CGScalars* sc, CGCtl* ctl,
+                           unsigned* arrive, cudaGraphConditionalHandle h, double tol2, int maxit) {
+    __shared__ double sh[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool zero = (sc->bb == 0.0);
+    double s[1] = {0};
+    if (i < v.nx && kk < v.NK) {
+        const size_t id = (size_t)kk * v.pitch + i;
+        P rv;
+        if (zero) {
+            x[id] = P(0);
+            rv = f[id];
+        } else {
+            rv = f[id] - s_apply(x, v.pitch, v.nx, v.NK, v.z, v.cx, kk, i);
+        }
+        r[id] = rv;
+        const double wr = v.rhow_k[kk] * (double)rv;
+        s[0] = wr * wr;
+    }
+    block_sum(s, sh);
+    const unsigned nb = gridDim.x * gridDim.y;
+    if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
+    if (!arrive_last(arrive, nb)) return;
+    const int nt = blockDim.x * blockDim.y, tid = threadIdx.x + blockDim.x * threadIdx.y;
+    double t[1] = {0};
+    for (int b = tid; b < (int)nb; b += nt) t[0] += __ldcg(partial + b);
+    block_sum(t, sh);
+    if (tid == 0) {
+        const double rr = t[0], bb = sc->bb;
+        sc->rr = rr;
+        ctl->it = 0;
+        ctl->total = 0;
+        ctl->relres = (bb > 0.0) ? sqrt(rr / bb) : 0.0;
+        const bool more = (bb > 0.0) && (rr > tol2 * bb) && (maxit > 0) && isfinite(rr);
+        cudaGraphSetConditional(h, more ? 1u : 0u);
+    }
+}
+
 }  // namespace vvm

@@ -374,6 +374,44 @@ __device__ __forceinline__ T vt_flux(const PAdvArgs<T>& a, const T* qr, int i, i
     return T(a.p.rhow[k]) * VT * s;
 }
 
+// Final sums of NegativeValueProcess and its rescaling factor
+// (MicroPhysics.cpp:125-127): nvp[2f] = 1 if positives are rescaled,
+// nvp[2f+1] = 1 - |neg/pos|. One block (k_nvp_final); fixed summation
+// order. `sh`: 32 * 6 doubles. (Finishing the sums in the producer's last
+// block instead costs every block of the producer a fence and an atomic
+// before it retires, more than this launch.)
+__device__ __forceinline__ void nvp_finish(const double* partial, int nblocks, double* nvp, double* sh) {
+    const int nt = blockDim.x * blockDim.y, tid = threadIdx.x + blockDim.x * threadIdx.y;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    // four partials a round in flight (a few round trips to L2, not one a partial)
+    int b = tid;
+    for (; b + 3 * nt < nblocks; b += 4 * nt) {
+        double x[4][6];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int j = 0; j < 6; j++) x[q][j] = __ldcg(partial + (size_t)(b + q * nt) * 6 + j);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int j = 0; j < 6; j++) s[j] += x[q][j];
+    }
+    for (; b < nblocks; b += nt)
+#pragma unroll
+        for (int j = 0; j < 6; j++) s[j] += __ldcg(partial + (size_t)b * 6 + j);
+    block_sum(s, sh);
+    if (tid == 0) {
+        for (int f = 0; f < 3; f++) {
+            const double pos = s[2 * f], neg = s[2 * f + 1];
+            const bool skip = (pos == 0. || fabs(neg) > pos);
+            nvp[2 * f] = skip ? 0.0 : 1.0;
+            nvp[2 * f + 1] = skip ? 1.0 : 1. - fabs(neg / pos);
+        }
+    }
+}
+
+__global__ void k_nvp_final(const double* partial, int nblocks, double* nvp);
+
 // Tile of k_padv: 32 x 8 cells a block of 32 x 8 threads. The four fields
 // are staged into shared memory with two halo cells a side (cp.async, issued
 // first); every face of the tile (33 x 8 x-faces, 32 x 9 z-faces) is then
@@ -569,11 +607,6 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
         }
     }
 }
-
-// Final sums of NegativeValueProcess and its rescaling factor
-// (MicroPhysics.cpp:125-127): nvp[2f] = 1 if positives are rescaled,
-// nvp[2f+1] = 1 - |neg/pos|. One block; fixed summation order.
-__global__ void k_nvp_final(const double* partial, int nblocks, double* nvp);
 
 // ---------------------------------------------------------------------------
 // Finishes th, qv, qc, qr after advection or microphysics: the rescaling of

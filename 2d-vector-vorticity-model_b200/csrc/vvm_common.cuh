@@ -118,4 +118,23 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* sh) {
     __syncthreads();
 }
 
+// Grid-wide finish of per-block partial sums without a second launch. Every
+// block calls it once, after its thread 0 has written the block's partial;
+// it returns true in the one block that arrives last (thread 0 fences its
+// partial, then counts in: no block waits for another), which may then read
+// all partials (__ldcg) and finish the sum in a fixed order. That block also
+// puts the counter back to 0 for the next launch; `count` starts at 0.
+__device__ __forceinline__ bool arrive_last(unsigned* count, unsigned nblocks) {
+    __shared__ int last;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(count, 1u);
+        last = (prev == nblocks - 1);
+        if (last) atomicExch(count, 0u);
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last != 0;
+}
+
 }  // namespace vvm

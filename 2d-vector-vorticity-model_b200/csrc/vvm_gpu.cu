@@ -33,20 +33,7 @@ namespace vvm {
 
 __global__ void k_nvp_final(const double* partial, int nblocks, double* nvp) {
     __shared__ double sh[32 * 6];
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-#pragma unroll
-        for (int j = 0; j < 6; j++) s[j] += partial[(size_t)b * 6 + j];
-    block_sum(s, sh);
-    if (threadIdx.x == 0) {
-        for (int f = 0; f < 3; f++) {
-            double pos = s[2 * f], neg = s[2 * f + 1];
-            // MicroPhysics.cpp:125-127
-            bool skip = (pos == 0. || fabs(neg) > pos);
-            nvp[2 * f] = skip ? 0.0 : 1.0;
-            nvp[2 * f + 1] = skip ? 1.0 : 1. - fabs(neg / pos);
-        }
-    }
+    nvp_finish(partial, nblocks, nvp, sh);
 }
 
 __global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mode) {
@@ -1242,6 +1229,7 @@ struct PCG {
     CGScalars* sc = nullptr;
     CGScalars* sc_host = nullptr;
     CGCtl* ctl = nullptr;   // loop state of graph-captured solves
+    unsigned* arrive = nullptr;   // arrival counter of k_cg_check's last block
     Stats* stats = nullptr;
 
     // S = -diag(1/rw) A in symmetric form: cx_k = a_k / rhow_k, ru_k = h_k /
@@ -1278,6 +1266,7 @@ struct PCG {
         upload_now(rhow_k, rw.data(), NK * sizeof(double));
         sc = ar.alloc<CGScalars>(1);
         ctl = ar.alloc<CGCtl>(1);
+        arrive = ar.alloc<unsigned>(1);
         CK(cudaMallocHost(&sc_host, sizeof(CGScalars)));
     }
     void release() {
@@ -2158,15 +2147,11 @@ long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
     long long in_bodies = 0;
     if (c->spectral) P64.sp.apply_to(c->Wf, c->W, st);   // direct solve; the loop below checks it
     else if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
-    LAUNCH(&c->stats, VVM_K_CG, st, k_zero_if_b0<<<G, B, 0, st>>>(P64.NX, P64.NK, P64.pitch, P64.sc, c->W));
-    CKL();
     if (!c->mixed || c->spectral) {
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P64.r, P64.partial));
-        CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P64.partial, P64.npart, P64.sc, CG_SET_RR));
-        CKL();
         cudaGraphConditionalHandle h = new_handle(st);
-        LAUNCH(&c->stats, VVM_K_CG, st, k_loop_plain<<<1, 1, 0, st>>>(P64.sc, P64.ctl, h, tol * tol, maxit, 1, c->d_exec, 0));
+        LAUNCH(&c->stats, VVM_K_CG, st,
+               k_cg_check<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P64.r, P64.partial, P64.sc, P64.ctl, P64.arrive, h,
+                                                    tol * tol, maxit));
         CKL();
         cudaGraph_t body = add_while(st, h);
         BodyCapture bc(c->cap[0], body);
@@ -2180,6 +2165,8 @@ long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
     }
     PCG<float>& P32 = *c->pcg32;
     VecArgs<float> v32 = P32.vargs();
+    LAUNCH(&c->stats, VVM_K_CG, st, k_zero_if_b0<<<G, B, 0, st>>>(P64.NX, P64.NK, P64.pitch, P64.sc, c->W));
+    CKL();
     LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->W, c->r64, c->wpartial));
     CKL();
     LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(c->wpartial, c->wnpart, P64.sc, CG_SET_RR));
