@@ -841,16 +841,24 @@ __global__ void k_net_out(const float* z, int NX, int NK, int pitch, double* a, 
 // Truncated flexible CG of the learned preconditioner (fcg_learned): up to
 // kFcgM-1 earlier directions (or their S images), in ring slots `slot`.
 constexpr int kFcgM = 8;
-constexpr int kFcgCheck = 4;   // iterations between the host's convergence checks
-struct FcgSet {
-    const double* a[kFcgM];
-    int slot[kFcgM];
-    int cnt;
+// Device state of the flexible-CG loop. Iteration k (from 0) writes ring
+// slot k % kFcgM and orthogonalises against the fcg_cnt(k) slots before it,
+// newest first, so the kernels of one recorded iteration serve every pass of
+// a graph loop.
+struct FcgCtl {
+    int k;           // iterations done
+    int converged;   // the loop stopped on the tolerance (or ||b|| = 0)
 };
+__device__ __forceinline__ int fcg_cnt(int k) { return k < kFcgM - 1 ? k : kFcgM - 1; }
+__device__ __forceinline__ int fcg_prev(int k, int j) { return (k - 1 - j) % kFcgM; }
 
-// Partials of (z, q_j), j < cnt: row j of `partial` holds one value a block.
-__global__ void k_fcg_multidot(VecArgs<double> v, const double* z, FcgSet q, double* partial) {
+// The direction ring in device memory: ring[s] = p_s, ring[kFcgM + s] = q_s = S p_s.
+using FcgRing = double* const*;
+
+// Partials of (z, q_j), j < fcg_cnt(k): row j of `partial` holds one value a block.
+__global__ void k_fcg_multidot(VecArgs<double> v, const double* z, FcgRing ring, const FcgCtl* ctl, double* partial) {
     __shared__ double sh[kFcgM * 32];
+    const int k = ctl->k, cnt = fcg_cnt(k);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int kk = blockIdx.y * blockDim.y + threadIdx.y;
     double s[kFcgM] = {};
@@ -859,42 +867,70 @@ __global__ void k_fcg_multidot(VecArgs<double> v, const double* z, FcgSet q, dou
         const double zv = z[id];
 #pragma unroll
         for (int j = 0; j < kFcgM; j++)
-            if (j < q.cnt) s[j] = zv * q.a[j][id];
+            if (j < cnt) s[j] = zv * ring[kFcgM + fcg_prev(k, j)][id];
     }
     block_sum(s, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         const int b = blockIdx.x + gridDim.x * blockIdx.y, nb = gridDim.x * gridDim.y;
-        for (int j = 0; j < q.cnt; j++) partial[(size_t)j * nb + b] = s[j];
+        for (int j = 0; j < cnt; j++) partial[(size_t)j * nb + b] = s[j];
     }
 }
 
 // beta_j = (z, q_j) / (p_j, q_j), the sums finished in a fixed order (one block).
-__global__ void k_fcg_beta(const double* partial, int npart, FcgSet q, const double* pq, double* beta) {
+__global__ void k_fcg_beta(const double* partial, int npart, const FcgCtl* ctl, const double* pq, double* beta) {
     __shared__ double sh[32];
-    for (int j = 0; j < q.cnt; j++) {
+    const int k = ctl->k, cnt = fcg_cnt(k);
+    for (int j = 0; j < cnt; j++) {
         double s[1] = {0};
         for (int b = threadIdx.x; b < npart; b += blockDim.x) s[0] += partial[(size_t)j * npart + b];
         block_sum(s, sh);
         if (threadIdx.x == 0) {
-            const double d = pq[q.slot[j]];
+            const double d = pq[fcg_prev(k, j)];
             beta[j] = (d != 0.0) ? s[0] / d : 0.0;
         }
     }
 }
 
-// out = z - sum_j beta_j p_j.
-__global__ void k_fcg_dir(VecArgs<double> v, const double* z, FcgSet p, const double* beta, double* out) {
+// p_k = z - sum_j beta_j p_j.
+__global__ void k_fcg_dir(VecArgs<double> v, const double* z, FcgRing ring, const FcgCtl* ctl, const double* beta) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int kk = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= v.nx || kk >= v.NK) return;
+    const int k = ctl->k, cnt = fcg_cnt(k);
     const size_t id = (size_t)kk * v.pitch + i;
     double y = z[id];
-    for (int j = 0; j < p.cnt; j++) y -= beta[j] * p.a[j][id];
-    out[id] = y;
+    for (int j = 0; j < cnt; j++) y -= beta[j] * ring[fcg_prev(k, j)][id];
+    ring[k % kFcgM][id] = y;
+}
+
+// q_k = S p_k and the partials of (p_k, q_k) and (p_k, r).
+__global__ void k_fcg_spmv(VecArgs<double> v, FcgRing ring, const FcgCtl* ctl, const double* r, double* ppq,
+                           double* ppr) {
+    __shared__ double sh[2 * 32];
+    const int slot = ctl->k % kFcgM;
+    const double* p = ring[slot];
+    double* q = ring[kFcgM + slot];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    double s[2] = {0, 0};
+    if (i < v.nx && kk < v.NK) {
+        const double y = s_apply(p, v.pitch, v.nx, v.NK, v.z, v.cx, kk, i);
+        const size_t id = (size_t)kk * v.pitch + i;
+        q[id] = y;
+        s[0] = p[id] * y;
+        s[1] = p[id] * r[id];
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const int b = blockIdx.x + gridDim.x * blockIdx.y;
+        ppq[b] = s[0];
+        ppr[b] = s[1];
+    }
 }
 
 // alpha = (p, r) / (p, q) from the partials of both; keeps (p, q) for the ring slot.
-__global__ void k_fcg_alpha(const double* ppq, const double* ppr, int npart, CGScalars* sc, double* pq, int slot) {
+__global__ void k_fcg_alpha(const double* ppq, const double* ppr, int npart, CGScalars* sc, double* pq,
+                            const FcgCtl* ctl) {
     __shared__ double sh[64];
     double s[2] = {0, 0};
     for (int b = threadIdx.x; b < npart; b += blockDim.x) {
@@ -905,7 +941,56 @@ __global__ void k_fcg_alpha(const double* ppq, const double* ppr, int npart, CGS
     if (threadIdx.x == 0) {
         sc->pq = s[0];
         sc->alpha = (s[0] != 0.0) ? s[1] / s[0] : 0.0;
-        pq[slot] = s[0];
+        pq[ctl->k % kFcgM] = s[0];
+    }
+}
+
+// x += alpha p_k; r -= alpha q_k; partial ||rhow r||^2.
+__global__ void k_fcg_update(VecArgs<double> v, const CGScalars* sc, FcgRing ring, const FcgCtl* ctl, double* x,
+                             double* r, double* partial) {
+    __shared__ double sh[32];
+    const int slot = ctl->k % kFcgM;
+    const double* p = ring[slot];
+    const double* q = ring[kFcgM + slot];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int kk = blockIdx.y * blockDim.y + threadIdx.y;
+    double s[1] = {0};
+    if (i < v.nx && kk < v.NK) {
+        const double al = sc->alpha;
+        const size_t id = (size_t)kk * v.pitch + i;
+        x[id] = x[id] + al * p[id];
+        const double rn = r[id] - al * q[id];
+        r[id] = rn;
+        const double wr = v.rhow_k[kk] * rn;
+        s[0] = wr * wr;
+    }
+    block_sum(s, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
+}
+
+// Loop condition of the flexible-CG loop (one block): ||rhow r||^2 from the
+// partials, in a fixed order, into sc->rr; `init` starts the loop (k = 0),
+// otherwise iteration k has finished (k + 1, and its body's kernels counted
+// in *exec). Continues while ||rhow r||^2 > tol^2 ||b||^2 and k < cap.
+__global__ void k_fcg_loop(const double* partial, int npart, CGScalars* sc, FcgCtl* ctl,
+                           cudaGraphConditionalHandle h, double tol2, int cap, int init, long long* exec,
+                           int body_kernels) {
+    __shared__ double sh[32];
+    double s[1] = {0};
+    for (int b = threadIdx.x; b < npart; b += blockDim.x) s[0] += partial[b];
+    block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        const double rr = s[0], bb = sc->bb;
+        sc->rr = rr;
+        if (init) {
+            ctl->k = 0;
+        } else {
+            ctl->k++;
+            *exec += body_kernels;
+        }
+        const bool above = (bb > 0.0) && !(rr <= tol2 * bb);   // a NaN residual counts as above
+        ctl->converged = !above;
+        cudaGraphSetConditional(h, (above && isfinite(rr) && ctl->k < cap) ? 1u : 0u);
     }
 }
 
@@ -1399,6 +1484,13 @@ struct vvm_gpu_ctx {
     double *za64 = nullptr, *r164 = nullptr, *d64 = nullptr, *sd64 = nullptr;   // the learned cycle's work arrays
     double *fcg_p[kFcgM] = {}, *fcg_q[kFcgM] = {};   // flexible-CG direction ring and its S images
     double *fcg_part = nullptr, *fcg_pq = nullptr, *fcg_beta = nullptr;
+    double** fcg_ring = nullptr;        // device copy of {fcg_p, fcg_q} (FcgRing)
+    FcgCtl* fcg_ctl = nullptr;          // flexible-CG loop state
+    FcgCtl* fcg_host = nullptr;         // pinned copy of it
+    cudaGraphExec_t fcg_exec = nullptr; // the flexible-CG loop alone (fcg_graph)
+    double fcg_tol = 0;
+    int fcg_cap = 0, fcg_mode = -1;
+    long long fcg_static = 0;           // kernels of fcg_exec outside its loop
     int learned_mode = 0;    // 0: the cycle with the network; 1: without it; 2: identity
     int learned_cap = 200;   // flexible-CG iterations before the multigrid-PCG fallback
     int learned_iters = 0, learned_fallback = 0;
@@ -1478,10 +1570,13 @@ struct vvm_gpu_ctx {
                     cudaGraphExecDestroy(g);
                     g = nullptr;
                 }
+        if (fcg_exec) cudaGraphExecDestroy(fcg_exec);
+        fcg_exec = nullptr;
     }
 
     ~vvm_gpu_ctx() {
         drop_graphs();
+        if (fcg_host) cudaFreeHost(fcg_host);
         for (auto s : cap)
             if (s) cudaStreamDestroy(s);
         if (pcg64) pcg64->release();
@@ -1950,6 +2045,16 @@ void ensure_learned(vvm_gpu_ctx* c) {
     c->fcg_part = c->ar.alloc<double>((size_t)kFcgM * c->pcg64->npart);
     c->fcg_pq = c->ar.alloc<double>(kFcgM);
     c->fcg_beta = c->ar.alloc<double>(kFcgM);
+    double* ring[2 * kFcgM];
+    for (int j = 0; j < kFcgM; j++) {
+        ring[j] = c->fcg_p[j];
+        ring[kFcgM + j] = c->fcg_q[j];
+    }
+    c->fcg_ring = c->ar.alloc<double*>(2 * kFcgM);
+    upload_now(c->fcg_ring, ring, sizeof(ring));
+    c->fcg_ctl = c->ar.alloc<FcgCtl>(1);
+    CK(cudaMallocHost(&c->fcg_host, sizeof(FcgCtl)));
+    (void)conv_rows_per_cta(c->net->H[0], c->net->W[0]);   // the convolution's one-time setup, outside any capture
 }
 
 // z64 = M r: a two-level cycle whose coarse correction is the network.
@@ -2008,12 +2113,14 @@ void learned_precond(vvm_gpu_ctx* c, const double* r, cudaStream_t st) {
 // nonlinear), keeping only the previous direction loses the Krylov speed-up;
 // a few more restore it. Directions and their S images live in a ring of
 // kFcgM slots. On S W = Wf from W = 0, preconditioned by learned_precond, to
-// the FP64 residual ||rhow r||^2 <= tol^2 bb. The host reads the residual
-// every kFcgCheck iterations only, so it stays ahead of the device instead of
-// waiting on it each iteration; the up to kFcgCheck - 1 iterations past
-// convergence leave a smaller residual (the step lengths are guarded against
-// zero). Returns the iterations run, or -cap if not converged.
-int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) {
+// the FP64 residual ||rhow r||^2 <= tol^2 bb, at most `cap` iterations.
+//
+// Recorded into the stream's capture as a WHILE node whose body is one
+// iteration: the kernels take the ring slots from the iteration count on the
+// device (FcgCtl), and k_fcg_loop tests the residual after every iteration,
+// so the host never waits inside the loop. Returns the kernels recorded
+// inside the loop body.
+long long record_fcg(vvm_gpu_ctx* c, double tol, int cap) {
     PCG<double>& P = *c->pcg64;
     VecArgs<double> v = P.vargs();
     dim3 B = P.block(), G = P.grid();
@@ -2021,48 +2128,99 @@ int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) 
     CK(cudaMemsetAsync(c->W, 0, (size_t)P.NK * P.pitch * sizeof(double), st));
     LAUNCH(&c->stats, VVM_K_CG, st, k_cg_residual<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P.r, P.partial));
     CKL();
-    LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RR));
+    cudaGraphConditionalHandle h = new_handle(st);
+    LAUNCH(&c->stats, VVM_K_CG, st,
+           k_fcg_loop<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, c->fcg_ctl, h, tol * tol, cap, 1, c->d_exec, 0));
     CKL();
-    double rr = P.read_rr(st);
-    const double stop2 = tol * tol * bb;
-    *relres = std::sqrt(rr / bb);
-    if (!(rr > stop2)) return 0;
-    for (int it = 1; it <= cap; it++) {
-        learned_precond(c, P.r, st);
-        const int k = it - 1, slot = k % kFcgM, cnt = std::min(k, kFcgM - 1);
-        FcgSet ps{}, qs{};
-        for (int j = 0; j < cnt; j++) {
-            const int sj = (k - 1 - j) % kFcgM;
-            ps.a[j] = c->fcg_p[sj];
-            qs.a[j] = c->fcg_q[sj];
-            ps.slot[j] = qs.slot[j] = sj;
-        }
-        ps.cnt = qs.cnt = cnt;
-        if (cnt > 0) {
-            LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_multidot<<<G, B, 0, st>>>(v, c->z64, qs, c->fcg_part));
-            CKL();
-            LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_beta<<<1, 1024, 0, st>>>(c->fcg_part, P.npart, qs, c->fcg_pq, c->fcg_beta));
-            CKL();
-        }
-        LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_dir<<<G, B, 0, st>>>(v, c->z64, ps, c->fcg_beta, c->fcg_p[slot]));
-        CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_spmv<double><<<G, B, 0, st>>>(v, c->fcg_p[slot], c->fcg_q[slot], P.partial));
-        CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_dot<double><<<G, B, 0, st>>>(v, c->fcg_p[slot], P.r, c->fcg_part));
-        CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_fcg_alpha<<<1, 1024, 0, st>>>(P.partial, c->fcg_part, P.npart, P.sc, c->fcg_pq, slot));
-        CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_update<double><<<G, B, 0, st>>>(v, P.sc, c->W, P.r, c->fcg_p[slot], c->fcg_q[slot], P.partial));
-        CKL();
-        LAUNCH(&c->stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(P.partial, P.npart, P.sc, CG_SET_RR));
-        CKL();
-        if (it % kFcgCheck != 0 && it != cap) continue;
-        rr = P.read_rr(st);
-        *relres = std::sqrt(rr / bb);
-        if (!(rr > stop2)) return it;
-        if (!std::isfinite(rr)) break;
+    cudaGraph_t body = add_while(st, h);
+    BodyCapture bc(c->cap[0], body);
+    cudaStream_t bs = bc.s;
+    const long long n0 = c->stats.launches;
+    learned_precond(c, P.r, bs);
+    LAUNCH(&c->stats, VVM_K_CG, bs, k_fcg_multidot<<<G, B, 0, bs>>>(v, c->z64, c->fcg_ring, c->fcg_ctl, c->fcg_part));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, bs, k_fcg_beta<<<1, 1024, 0, bs>>>(c->fcg_part, P.npart, c->fcg_ctl, c->fcg_pq, c->fcg_beta));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, bs, k_fcg_dir<<<G, B, 0, bs>>>(v, c->z64, c->fcg_ring, c->fcg_ctl, c->fcg_beta));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, bs, k_fcg_spmv<<<G, B, 0, bs>>>(v, c->fcg_ring, c->fcg_ctl, P.r, P.partial, c->fcg_part));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, bs, k_fcg_alpha<<<1, 1024, 0, bs>>>(P.partial, c->fcg_part, P.npart, P.sc, c->fcg_pq, c->fcg_ctl));
+    CKL();
+    LAUNCH(&c->stats, VVM_K_CG, bs, k_fcg_update<<<G, B, 0, bs>>>(v, P.sc, c->fcg_ring, c->fcg_ctl, c->W, P.r, P.partial));
+    CKL();
+    const int nb = (int)(c->stats.launches - n0);
+    LAUNCH(&c->stats, VVM_K_CG, bs,
+           k_fcg_loop<<<1, 1024, 0, bs>>>(P.partial, P.npart, P.sc, c->fcg_ctl, h, tol * tol, cap, 0, c->d_exec, nb + 1));
+    CKL();
+    bc.end();
+    return c->stats.launches - n0;
+}
+
+// The flexible-CG loop alone as an instantiated graph, kept per context for
+// its (tol, cap, mode).
+cudaGraphExec_t fcg_graph(vvm_gpu_ctx* c, double tol, int cap) {
+    if (c->fcg_exec && c->fcg_tol == tol && c->fcg_cap == cap && c->fcg_mode == c->learned_mode) return c->fcg_exec;
+    if (c->fcg_exec) cudaGraphExecDestroy(c->fcg_exec);
+    c->fcg_exec = nullptr;
+    const long long l0 = c->stats.launches;
+    const bool timing = c->stats.on;   // no per-launch events inside a capture
+    c->stats.on = false;
+    cudaStream_t saved = c->stream;
+    c->stream = c->own;
+    cudaGraph_t g = nullptr;
+    long long in_loop = 0;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    try {
+        in_loop = record_fcg(c, tol, cap);
+    } catch (...) {
+        cudaStreamEndCapture(c->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        c->stream = saved;
+        c->stats.launches = l0;
+        c->stats.on = timing;
+        throw;
     }
-    return -cap;
+    CK(cudaStreamEndCapture(c->stream, &g));
+    c->stream = saved;
+    c->stats.on = timing;
+    c->fcg_static = c->stats.launches - l0 - in_loop;
+    c->stats.launches = l0;
+    cudaGraphExec_t ex = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) throw CudaError{std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+    c->fcg_exec = ex;
+    c->fcg_tol = tol;
+    c->fcg_cap = cap;
+    c->fcg_mode = c->learned_mode;
+    return ex;
+}
+
+// Runs the flexible-CG loop (one graph launch, one wait at the end). Returns
+// the iterations run, or -cap if the tolerance was not reached.
+int fcg_learned(vvm_gpu_ctx* c, double bb, double tol, int cap, double* relres) {
+    cudaGraphExec_t ex = fcg_graph(c, tol, cap);
+    cudaEvent_t e0 = nullptr;   // profiling: the whole loop counts as the learned class
+    if (c->stats.on) {
+        e0 = c->stats.ev();
+        CK(cudaEventRecord(e0, c->stream));
+    }
+    CK(cudaGraphLaunch(ex, c->stream));
+    if (e0) {
+        cudaEvent_t e1 = c->stats.ev();
+        CK(cudaEventRecord(e1, c->stream));
+        c->stats.pending.push_back({VVM_K_LEARNED, e0, e1});
+    }
+    c->stats.launches += c->fcg_static;
+    PCG<double>& P = *c->pcg64;
+    CK(cudaMemcpyAsync(P.sc_host, P.sc, sizeof(CGScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(c->fcg_host, c->fcg_ctl, sizeof(FcgCtl), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const FcgCtl h = *c->fcg_host;
+    const double rr = P.sc_host->rr;
+    *relres = (bb > 0.0) ? std::sqrt(rr / bb) : 0.0;
+    return h.converged ? h.k : -cap;
 }
 
 // Solves S W = Wf (FP64 rhs in c->Wf, ||b||^2 = bb) into c->W.
@@ -2145,9 +2303,13 @@ long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
     VecArgs<double> v = P64.vargs();
     const long long n_start = c->stats.launches;
     long long in_bodies = 0;
+    const bool learned = (c->desc.solver == VVM_SOLVER_LEARNED && !c->learned_collect);
+    // learned: the flexible-CG loop, then the check below, whose plain PCG
+    // loop runs only if the flexible CG stopped at its cap (the fallback)
+    if (learned) in_bodies += record_fcg(c, tol, c->learned_cap);
     if (c->spectral) P64.sp.apply_to(c->Wf, c->W, st);   // direct solve; the loop below checks it
-    else if (!warm) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
-    if (!c->mixed || c->spectral) {
+    else if (!warm && !learned) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
+    if (!c->mixed || c->spectral || learned) {
         cudaGraphConditionalHandle h = new_handle(st);
         LAUNCH(&c->stats, VVM_K_CG, st,
                k_cg_check<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P64.r, P64.partial, P64.sc, P64.ctl, P64.arrive, h,
@@ -2367,6 +2529,7 @@ cudaGraphExec_t step_graph(vvm_gpu_ctx* c) {
     const int b = c->cur, par = (c->step + 1) & 1;
     if (c->gexec[b][par]) return c->gexec[b][par];
     ensure_poisson(c);
+    if (c->desc.solver == VVM_SOLVER_LEARNED) ensure_learned(c);   // allocations stay outside the capture
     const int step0 = c->step, cur0 = c->cur, ns0 = c->nsolves;
     const long long l0 = c->stats.launches;
     cudaStream_t saved = c->stream;
@@ -2402,12 +2565,32 @@ cudaGraphExec_t step_graph(vvm_gpu_ctx* c) {
 
 int regen_forcing(vvm_gpu_ctx* c, int t, double lo, double hi, double sd);
 
+// After a graph step the solve's loop state lives on the device: brings
+// last_iters / last_relres (and the learned solver's counts) to the host.
+void sync_graph_solve(vvm_gpu_ctx* c) {
+    if (!c->last_graph || !c->poisson_ready) return;
+    CGCtl h{};
+    CK(cudaStreamSynchronize(c->stream));
+    const bool learned = (c->desc.solver == VVM_SOLVER_LEARNED) && c->fcg_ctl;
+    const bool refined = c->mixed && !c->spectral && !learned;   // FP32 inner loops in an FP64 outer loop
+    CK(cudaMemcpy(&h, refined ? c->wctl : c->pcg64->ctl, sizeof(CGCtl), cudaMemcpyDeviceToHost));
+    c->last_iters = h.total;
+    c->last_relres = h.relres;
+    if (learned) {
+        FcgCtl f{};
+        CK(cudaMemcpy(&f, c->fcg_ctl, sizeof(FcgCtl), cudaMemcpyDeviceToHost));
+        c->learned_iters = f.k;
+        c->learned_fallback = f.converged ? 0 : 1;
+        c->last_iters += f.k;
+    }
+}
+
 template <typename T>
 int step_once(vvm_gpu_ctx* c) {
     const bool forcing_now = c->has_forcing_th && ((c->step + 1) * c->desc.dt <= c->desc.addforcingtime);
     const bool warm = c->desc.warm_start != 0;
     const bool use_graph = !c->graphs_off && !c->stats.on && c->step >= 0 && !forcing_now &&
-                           c->poisson_ready && (!warm || c->nsolves >= 2) &&
+                           c->poisson_ready && (!warm || c->nsolves >= 2) && !c->learned_collect &&
                            !(c->desc.flags & VVM_FLAG_STREAMFUNCTION);
     if (!use_graph) {
         c->last_graph = false;
@@ -2482,7 +2665,7 @@ bool graph_ready(vvm_gpu_ctx* c) {
     const bool forcing_now = c->has_forcing_th && ((c->step + 1) * c->desc.dt <= c->desc.addforcingtime);
     const bool warm = c->desc.warm_start != 0;
     return !c->graphs_off && !c->stats.on && c->step >= 0 && !forcing_now && c->poisson_ready &&
-           (!warm || c->nsolves >= 2) && !(c->desc.flags & VVM_FLAG_STREAMFUNCTION);
+           (!warm || c->nsolves >= 2) && !c->learned_collect && !(c->desc.flags & VVM_FLAG_STREAMFUNCTION);
 }
 
 }  // namespace
@@ -2542,6 +2725,7 @@ cudaGraphExec_t batch_capture(vvm_gpu_batch* b, const std::vector<int>& idx, std
     for (int i : idx) {
         vvm_gpu_ctx* c = b->cases[i];
         ensure_poisson(c);
+        if (c->desc.solver == VVM_SOLVER_LEARNED) ensure_learned(c);
         sv.push_back({c->stream, c->step, c->cur, c->nsolves, c->stats.launches});
     }
     auto put_back = [&]() {
@@ -3244,7 +3428,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
     c->mixed = (D.precision == VVM_PREC_MIXED);
     c->spectral = (D.solver == VVM_SOLVER_SPECTRAL);
     // the learned solver's iterations are checked on the host (no graph)
-    c->graphs_off = (D.solver == VVM_SOLVER_LEARNED);
+    c->graphs_off = false;
     int prev = 0;
     cudaGetDevice(&prev);
     try {
@@ -3828,16 +4012,23 @@ int vvm_gpu_learned_time(vvm_gpu_ctx* ctx, int reps, double* ms_forward, double*
 int vvm_gpu_learned_config(vvm_gpu_ctx* ctx, int mode, int cap) {
     if (!ctx) return VVM_GPU_EINVAL;
     if (mode < 0 || mode > 2 || cap < 1) return fail(ctx, VVM_GPU_EINVAL, "learned_config: bad arguments");
-    ctx->learned_mode = mode;
-    ctx->learned_cap = cap;
-    return VVM_GPU_OK;
+    return guarded(ctx, [&]() -> int {
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->learned_mode = mode;
+        ctx->learned_cap = cap;
+        ctx->drop_graphs();   // mode and cap are recorded into the graphs
+        return VVM_GPU_OK;
+    });
 }
 
 int vvm_gpu_learned_last(vvm_gpu_ctx* ctx, int* fcg_iters, int* fell_back) {
     if (!ctx) return VVM_GPU_EINVAL;
-    if (fcg_iters) *fcg_iters = ctx->learned_iters;
-    if (fell_back) *fell_back = ctx->learned_fallback;
-    return VVM_GPU_OK;
+    return guarded(ctx, [&]() -> int {
+        sync_graph_solve(ctx);
+        if (fcg_iters) *fcg_iters = ctx->learned_iters;
+        if (fell_back) *fell_back = ctx->learned_fallback;
+        return VVM_GPU_OK;
+    });
 }
 
 int vvm_gpu_set_tuning(vvm_gpu_ctx* ctx, int gs_tile_rows, int fft_threads) {
@@ -3969,14 +4160,7 @@ int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len) {
 int vvm_gpu_last_solve(vvm_gpu_ctx* ctx, int* iters, double* relres) {
     if (!ctx) return VVM_GPU_EINVAL;
     return guarded(ctx, [&]() -> int {
-        if (ctx->last_graph && ctx->poisson_ready) {   // loop state lives on the device
-            CGCtl h{};
-            CK(cudaStreamSynchronize(ctx->stream));
-            const bool refined = ctx->mixed && !ctx->spectral;   // FP32 inner loops in an FP64 outer loop
-            CK(cudaMemcpy(&h, refined ? ctx->wctl : ctx->pcg64->ctl, sizeof(CGCtl), cudaMemcpyDeviceToHost));
-            ctx->last_iters = h.total;
-            ctx->last_relres = h.relres;
-        }
+        sync_graph_solve(ctx);
         if (iters) *iters = ctx->last_iters;
         if (relres) *relres = ctx->last_relres;
         return VVM_GPU_OK;
