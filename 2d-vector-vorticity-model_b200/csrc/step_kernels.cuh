@@ -635,6 +635,37 @@ __device__ __forceinline__ T nvp_apply(T v, const double* nvp, int f) {
     return v;
 }
 
+// What k_apply does to one value of field f at (id, row k): the rescaling of
+// NegativeValueProcess, then AddForcing. Shared with the fused form at the
+// top of k_kessler, so both give the same bits.
+template <typename T>
+struct AdvFinish {
+    const double* nvp;       // [6] from k_nvp_final
+    const T* th_forcing;     // init_th_forcing (may be null)
+    int nvp_mask;            // fields to clip/rescale
+    int forcing;             // add Q1LS/Q2LS
+    int forcing_th;          // add dt*init_th_forcing
+};
+
+template <typename T>
+__device__ __forceinline__ T finish_value(const AdvFinish<T>& a, const Profiles& p, T dt, int f, T v, int k,
+                                          size_t id) {
+    if (f >= 1 && (a.nvp_mask & (1 << f))) {
+        if (kPert<T> && f == 1) {   // NegativeValueProcess acts on the full qv
+            double full = p.ref[1][k] + (double)v;
+            v = T(nvp_apply(full, a.nvp, 0) - p.ref[1][k]);
+        } else {
+            v = nvp_apply(v, a.nvp, f - 1);
+        }
+    }
+    if (f == 0) {
+        if (a.forcing) v += dt * T(p.q1ls[k]);
+        if (a.forcing_th) v += dt * a.th_forcing[id];
+    }
+    if (f == 1 && a.forcing) v += dt * T(p.q2ls[k]);
+    return v;
+}
+
 template <typename T>
 __global__ void k_apply(ApplyArgs<T> a) {
     const Dims& d = a.d;
@@ -643,22 +674,10 @@ __global__ void k_apply(ApplyArgs<T> a) {
     if (i > d.nx - 2 || k > d.nz - 2) return;
     const size_t id = d.at(i, k);
     const T dt = T(a.c.dt);
+    const AdvFinish<T> fin{a.nvp, a.th_forcing, a.nvp_mask, a.forcing, a.forcing_th};
     for (int f = 0; f < 4; f++) {
         if (!(a.mask & (1 << f))) continue;
-        T v = a.fut[f][id];
-        if (f >= 1 && (a.nvp_mask & (1 << f))) {
-            if (kPert<T> && f == 1) {   // NegativeValueProcess acts on the full qv
-                double full = a.p.ref[1][k] + (double)v;
-                v = T(nvp_apply(full, a.nvp, 0) - a.p.ref[1][k]);
-            } else {
-                v = nvp_apply(v, a.nvp, f - 1);
-            }
-        }
-        if (f == 0) {
-            if (a.forcing) v += dt * T(a.p.q1ls[k]);
-            if (a.forcing_th) v += dt * a.th_forcing[id];
-        }
-        if (f == 1 && a.forcing) v += dt * T(a.p.q2ls[k]);
+        const T v = finish_value(fin, a.p, dt, f, a.fut[f][id], k, id);
         if (a.halo) store_center(a.fut[f], d, i, k, v);
         else a.fut[f][id] = v;
     }
@@ -704,6 +723,11 @@ struct KesslerArgs {
     T *d_auto, *d_accr, *d_evap, *d_cond;  // diagnostics (may be null)
     double* partial;
     int nvp;  // accumulate NVP sums
+    // The finish of the advection step (k_apply's rescaling and forcing of
+    // th, qv, qc, qr) applied to each value as it is read, in place of a
+    // k_apply launch whose halo images the apply after Kessler rewrites.
+    AdvFinish<T> pre;
+    int do_pre;
 };
 
 // One cell of Kessler warm rain in compute type C; writes the four rates.
@@ -768,7 +792,15 @@ __global__ void k_kessler(KesslerArgs<T> a) {
     if (act) {
         const size_t id = d.at(i, k);
         const C th0 = kPert<T> ? a.p.ref[0][k] : 0.0, qv0 = kPert<T> ? a.p.ref[1][k] : 0.0;
-        C th = th0 + (C)a.thp[id], qv = qv0 + (C)a.qvp[id], qc = a.qcp[id], qr = a.qrp[id];
+        T tv = a.thp[id], qvv = a.qvp[id], qcv = a.qcp[id], qrv = a.qrp[id];
+        if (a.do_pre) {
+            const T dt = T(a.c.dt);
+            tv = finish_value(a.pre, a.p, dt, 0, tv, k, id);
+            qvv = finish_value(a.pre, a.p, dt, 1, qvv, k, id);
+            qcv = finish_value(a.pre, a.p, dt, 2, qcv, k, id);
+            qrv = finish_value(a.pre, a.p, dt, 3, qrv, k, id);
+        }
+        C th = th0 + (C)tv, qv = qv0 + (C)qvv, qc = qcv, qr = qrv;
         C rates[4];
         kessler_cell<C>(th, qv, qc, qr, a.c.dt, a.c.lv, a.c.cp, a.p.pib[k], a.p.rhou[k], a.p.pc[k], a.p.pb[k],
                         rates);

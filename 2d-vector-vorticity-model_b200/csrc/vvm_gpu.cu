@@ -1750,12 +1750,24 @@ void launch_pubartop(vvm_gpu_ctx* c) {
     CKL();
 }
 
+// finish_advection: the step's own sequence, where the finish of the
+// advection (k_apply's NVP rescaling and AddForcing of th, qv, qc, qr, whose
+// NVP sums k_padv left) is applied as Kessler reads each value.
 template <typename T>
-void launch_kessler(vvm_gpu_ctx* c, bool halo) {
+void launch_kessler(vvm_gpu_ctx* c, bool halo, bool finish_advection = false) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     KesslerArgs<T> a{c->d, c->c, c->profiles(), F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut],
                      F.d_auto, F.d_accr, F.d_evap, F.d_cond, c->partial, 1};
+    if (finish_advection) {
+        a.do_pre = 1;
+        a.pre.nvp = c->nvp;
+        a.pre.th_forcing = F.th_forcing;
+        a.pre.nvp_mask = F_QV | F_QC | F_QR;
+        a.pre.forcing = c->has_q;
+        // status_for_adding_forcing (Iteration.cpp:276-277), as launch_apply forms it
+        a.pre.forcing_th = c->has_forcing_th && (c->step * c->desc.dt <= c->desc.addforcingtime);
+    }
     dim3 g = c->grid_interior(1);
     LAUNCH(&c->stats, VVM_K_KESSLER, c->stream, k_kessler<T><<<g, c->blk(), 0, c->stream>>>(a));
     CKL();
@@ -2501,7 +2513,8 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     c->step++;                                                 // Iteration.cpp:246
     launch_pzeta<T>(c);                                        // pzeta_pt
     launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
-    launch_apply<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true); // NVP, AddForcing, halos
+    // NVP and AddForcing of the advected fields run inside Kessler's kernel
+    // (nothing before it reads th, qv, qc, qr; their halos come after it)
     int rc = VVM_GPU_OK;
     if (c->desc.flags & VVM_FLAG_STREAMFUNCTION) {
         rc = launch_calpsiuw<T>(c);                            // calpsiuw (Iteration.cpp:289-290)
@@ -2510,7 +2523,7 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
         rc = launch_cal_w<T>(c, recorded_in_loops);            // cal_w
         launch_cal_u<T>(c);                                    // cal_u
     }
-    launch_kessler<T>(c, true);                                // Kessler + NVP x3 + halos
+    launch_kessler<T>(c, true, true);                          // NVP + AddForcing, Kessler + NVP x3 + halos
     // The first updateMean of the step (Iteration.cpp:408) only writes thb,
     // qvb, thvb, which nextTimeStep's updateMean overwrites before any read.
     launch_turbulence<T>(c, true, recorded_in_loops);          // RKM_RKH + diffusion + theta/zeta nudging
@@ -3629,7 +3642,7 @@ ROUTINE(vvm_gpu_halo_all, { DISPATCH(ctx, launch_halo_all)(ctx); return VVM_GPU_
 ROUTINE(vvm_gpu_pubartop, { DISPATCH(ctx, launch_pubartop)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_cal_w, { ctx->last_graph = false; return DISPATCH(ctx, launch_cal_w)(ctx, nullptr); })
 ROUTINE(vvm_gpu_cal_u, { DISPATCH(ctx, launch_cal_u)(ctx); return VVM_GPU_OK; })
-ROUTINE(vvm_gpu_kessler, { DISPATCH(ctx, launch_kessler)(ctx, false); return VVM_GPU_OK; })
+ROUTINE(vvm_gpu_kessler, { DISPATCH(ctx, launch_kessler)(ctx, false, false); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_update_mean, { DISPATCH(ctx, launch_update_mean)(ctx, false); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_turbulence, { DISPATCH(ctx, launch_turbulence)(ctx, false, nullptr); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_nudge, {
