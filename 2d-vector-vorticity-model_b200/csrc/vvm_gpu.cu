@@ -1549,6 +1549,9 @@ struct vvm_gpu_ctx {
     cudaGraphExec_t gexec[2][2] = {};
     long long gstatic[2][2] = {};      // kernels outside the solver loops
     cudaStream_t cap[2] = {};          // streams for capturing loop bodies
+    cudaStream_t side[2] = {};         // branches of a step that run beside the main chain
+    cudaEvent_t fork_ev[4] = {};       // their fork and join points
+    bool branches = true;              // use them (off inside a batch: the cases are the branches)
     CGCtl* wctl = nullptr;             // outer loop state of the mixed solve
     long long* d_exec = nullptr;       // kernels executed inside graph loops
     int* d_err = nullptr;              // device error word (kGSErrWait), checked when the host syncs
@@ -1579,6 +1582,10 @@ struct vvm_gpu_ctx {
         if (fcg_host) cudaFreeHost(fcg_host);
         for (auto s : cap)
             if (s) cudaStreamDestroy(s);
+        for (auto s : side)
+            if (s) cudaStreamDestroy(s);
+        for (auto e : fork_ev)
+            if (e) cudaEventDestroy(e);
         if (pcg64) pcg64->release();
         if (pcg32) pcg32->release();
         if (pcg_psi) pcg_psi->release();
@@ -2508,22 +2515,68 @@ int launch_calpsiuw(vvm_gpu_ctx* c) {
 
 // ---------------------------------------------------------------- one step
 
+// Fork/join of a step's side branches: side stream s waits for everything
+// issued on the context's stream so far (fork), and the context's stream
+// waits for everything issued on side s (join). Inside a stream capture
+// these become branches of the graph.
+void fork_to(vvm_gpu_ctx* c, int s, int e) {
+    CK(cudaEventRecord(c->fork_ev[e], c->stream));
+    CK(cudaStreamWaitEvent(c->side[s], c->fork_ev[e], 0));
+}
+void join_from(vvm_gpu_ctx* c, int s, int e) {
+    CK(cudaEventRecord(c->fork_ev[e], c->side[s]));
+    CK(cudaStreamWaitEvent(c->stream, c->fork_ev[e], 0));
+}
+struct OnStream {   // issues a scope's launches on another stream
+    vvm_gpu_ctx* c;
+    cudaStream_t saved;
+    OnStream(vvm_gpu_ctx* c_, cudaStream_t s) : c(c_), saved(c_->stream) { c->stream = s; }
+    ~OnStream() { c->stream = saved; }
+};
+
 template <typename T>
 int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     c->step++;                                                 // Iteration.cpp:246
+    const bool sf = (c->desc.flags & VVM_FLAG_STREAMFUNCTION) != 0;
+    // Two branches run beside the main chain (in a captured step they are
+    // parallel branches of the graph; the results are those of the
+    // reference's order, since neither branch reads what the other writes):
+    //  side 0: pubarTop_pt, which reads u, w, RKM and writes only ubar,
+    //          dubar (read by cal_u), beside the advection kernels;
+    //  side 1: the NVP rescaling and AddForcing of the advected fields,
+    //          Kessler, its NVP and the halos of th, qv, qc, qr, beside
+    //          cal_w and cal_u (which touch zeta, w, u only).
+    // A batch's cases are already parallel branches of its graph: there every
+    // case runs as one chain, in the order below.
+    const bool br = c->branches;
+    if (!sf && br) {
+        fork_to(c, 0, 0);
+        OnStream os(c, c->side[0]);
+        launch_pubartop<T>(c);                                 // pubarTop_pt
+    }
     launch_pzeta<T>(c);                                        // pzeta_pt
     launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
-    // NVP and AddForcing of the advected fields run inside Kessler's kernel
-    // (nothing before it reads th, qv, qc, qr; their halos come after it)
-    int rc = VVM_GPU_OK;
-    if (c->desc.flags & VVM_FLAG_STREAMFUNCTION) {
-        rc = launch_calpsiuw<T>(c);                            // calpsiuw (Iteration.cpp:289-290)
-    } else {
-        launch_pubartop<T>(c);                                 // pubarTop_pt
-        rc = launch_cal_w<T>(c, recorded_in_loops);            // cal_w
-        launch_cal_u<T>(c);                                    // cal_u
+    if (br) {
+        fork_to(c, 1, 1);
+        OnStream os(c, c->side[1]);
+        launch_kessler<T>(c, true, true);                      // NVP + AddForcing, Kessler + NVP x3 + halos
     }
-    launch_kessler<T>(c, true, true);                          // NVP + AddForcing, Kessler + NVP x3 + halos
+    int rc = VVM_GPU_OK;
+    try {
+        if (sf) {
+            rc = launch_calpsiuw<T>(c);                        // calpsiuw (Iteration.cpp:289-290)
+        } else {
+            if (br) join_from(c, 0, 2);                        // ubar, dubar before cal_u; u, w read
+            else launch_pubartop<T>(c);
+            rc = launch_cal_w<T>(c, recorded_in_loops);        // cal_w
+            launch_cal_u<T>(c);                                // cal_u
+        }
+    } catch (...) {
+        if (br) join_from(c, 1, 3);
+        throw;
+    }
+    if (br) join_from(c, 1, 3);
+    else launch_kessler<T>(c, true, true);
     // The first updateMean of the step (Iteration.cpp:408) only writes thb,
     // qvb, thvb, which nextTimeStep's updateMean overwrites before any read.
     launch_turbulence<T>(c, true, recorded_in_loops);          // RKM_RKH + diffusion + theta/zeta nudging
@@ -2761,8 +2814,15 @@ cudaGraphExec_t batch_capture(vvm_gpu_batch* b, const std::vector<int>& idx, std
             CK(cudaStreamWaitEvent(c->own, b->fork, 0));
             const long long l0 = c->stats.launches;
             long long in_loops = 0;
-            if (c->mixed) run_step<float>(c, &in_loops);
-            else run_step<double>(c, &in_loops);
+            c->branches = false;   // one chain a case: the cases are the graph's branches
+            try {
+                if (c->mixed) run_step<float>(c, &in_loops);
+                else run_step<double>(c, &in_loops);
+            } catch (...) {
+                c->branches = true;
+                throw;
+            }
+            c->branches = true;
             gstatic[i] = c->stats.launches - l0 - in_loops;
             CK(cudaEventRecord(b->joins[i], c->own));
             CK(cudaStreamWaitEvent(b->stream, b->joins[i], 0));
@@ -3499,6 +3559,8 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         c->d_exec = c->ar.alloc<long long>(1);
         c->d_err = c->ar.alloc<int>(1);
         for (auto& cs : c->cap) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        for (auto& cs : c->side) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        for (auto& e : c->fork_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     } catch (const CudaError& e) {
         cudaSetDevice(prev);
         return fail(nullptr, VVM_GPU_ECUDA, e.msg);
