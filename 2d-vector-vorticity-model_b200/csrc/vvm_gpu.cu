@@ -2540,21 +2540,25 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     const bool sf = (c->desc.flags & VVM_FLAG_STREAMFUNCTION) != 0;
     // Two branches run beside the main chain (in a captured step they are
     // parallel branches of the graph; the results are those of the
-    // reference's order, since neither branch reads what the other writes):
-    //  side 0: pubarTop_pt, which reads u, w, RKM and writes only ubar,
-    //          dubar (read by cal_u), beside the advection kernels;
+    // reference's order, since no branch reads what another writes):
+    //  side 0: pubarTop_pt (reads u, w, RKM; writes only ubar, dubar, read by
+    //          cal_u) and pzeta_pt (writes zetap and its tendencies), beside
+    //          the scalar advection, which writes th, qv, qc, qr's future
+    //          values and tendencies only;
     //  side 1: the NVP rescaling and AddForcing of the advected fields,
     //          Kessler, its NVP and the halos of th, qv, qc, qr, beside
     //          cal_w and cal_u (which touch zeta, w, u only).
     // A batch's cases are already parallel branches of its graph: there every
     // case runs as one chain, in the order below.
     const bool br = c->branches;
-    if (!sf && br) {
+    if (br) {
         fork_to(c, 0, 0);
         OnStream os(c, c->side[0]);
-        launch_pubartop<T>(c);                                 // pubarTop_pt
+        if (!sf) launch_pubartop<T>(c);                        // pubarTop_pt
+        launch_pzeta<T>(c);                                    // pzeta_pt
+    } else {
+        launch_pzeta<T>(c);
     }
-    launch_pzeta<T>(c);                                        // pzeta_pt
     launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
     if (br) {
         fork_to(c, 1, 1);
@@ -2563,11 +2567,11 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     }
     int rc = VVM_GPU_OK;
     try {
+        if (br) join_from(c, 0, 2);                            // zetap; ubar, dubar; u, w read
         if (sf) {
             rc = launch_calpsiuw<T>(c);                        // calpsiuw (Iteration.cpp:289-290)
         } else {
-            if (br) join_from(c, 0, 2);                        // ubar, dubar before cal_u; u, w read
-            else launch_pubartop<T>(c);
+            if (!br) launch_pubartop<T>(c);
             rc = launch_cal_w<T>(c, recorded_in_loops);        // cal_w
             launch_cal_u<T>(c);                                // cal_u
         }
