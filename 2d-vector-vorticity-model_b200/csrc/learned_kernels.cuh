@@ -37,10 +37,6 @@ constexpr int kConvSpan = kConvTile + 2;
 constexpr int kNetErrWait = 2;   // device error word: an MMA completion wait gave up
 constexpr int kMmaSpinLimit = 1 << 22;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
 // Shared-memory matrix descriptor of tcgen05 (K-major, no swizzle): start
 // address, the byte offset between the two 8-element K chunks (LBO) and
 // between groups of 8 rows (SBO), all in 16-byte units; version 1.
@@ -230,18 +226,6 @@ struct ConvStreamArgs {
     int H, W, R;               // R: output rows per CTA
     int* err;
 };
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
 
 // Bounded wait on one phase of an mbarrier; gives up early when *abort is set.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {

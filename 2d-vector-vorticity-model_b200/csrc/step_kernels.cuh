@@ -287,6 +287,7 @@ struct PAdvArgs {
     T *hvt_n, *hvt_o;  // dqr_VT
     T* precip;         // [nx]
     double* partial;   // [gridDim.x*gridDim.y][6]: (pos, neg) of qv, qc, qr
+    int* err;          // device error word (kStageErrWait), may be null
     int mask;          // F_* fields to advect
     int nvp_mask;      // F_* fields whose NVP sums are wanted
     int do_vt;         // sedimentation of qr (with F_QR)
@@ -413,8 +414,8 @@ __device__ __forceinline__ void nvp_finish(const double* partial, int nblocks, d
 __global__ void k_nvp_final(const double* partial, int nblocks, double* nvp);
 
 // Tile of k_padv: 32 x 8 cells a block of 32 x 8 threads. The four fields
-// are staged into shared memory with two halo cells a side (cp.async, issued
-// first); every face of the tile (33 x 8 x-faces, 32 x 9 z-faces) is then
+// are staged into shared memory with two halo cells a side (one TMA box a
+// field, issued first); every face of the tile (33 x 8 x-faces, 32 x 9 z-faces) is then
 // evaluated once, by one thread: its velocity part (in registers) once for
 // all fields, its flux once per field and, for qr, its sedimentation flux,
 // into shared memory; a cell differences the four fluxes around it. The expressions are the per-cell ones of
@@ -423,11 +424,19 @@ __global__ void k_nvp_final(const double* partial, int nblocks, double* nvp);
 // roots a face, one pow a sedimentation face) and with every stencil read
 // from shared memory.
 constexpr int kPAdvBX = 32, kPAdvBZ = 8;
+constexpr int kStageErrWait = 4;   // device error word: a stencil's TMA staging wait gave up
+
+// The staged box of one field: rows k0-2 .. k0+BZ+1 and 40 columns from x0,
+// the halo's first column i0-2 rounded down to a 16-byte boundary (TMA
+// requires x * element size to be a multiple of 16): x0 = i0-2 - kPAdvOff.
+constexpr int kPAdvVX = 40, kPAdvVZ = kPAdvBZ + 4;
+template <typename T>
+constexpr int kPAdvOff = sizeof(T) == 8 ? 1 : 3;
 
 template <typename T>
 struct PAdvShared {
-    static constexpr int BX = kPAdvBX, BZ = kPAdvBZ, VX = BX + 4, VZ = BZ + 4;
-    T v[4][VZ][VX];           // th, qv, qc, qr at rows k0-2.., columns i0-2..
+    static constexpr int BX = kPAdvBX, BZ = kPAdvBZ, VX = kPAdvVX, VZ = kPAdvVZ;
+    T v[4][VZ][VX];           // th, qv, qc, qr: rows k0-2.., columns x0.. (each box a multiple of 128 bytes)
     T fx[4][BZ][BX + 1];      // x fluxes of each field
     T fz[4][BZ + 1][BX];      // z fluxes of each field
     T gz[BZ + 1][BX];         // sedimentation fluxes of qr
@@ -441,13 +450,16 @@ __device__ __forceinline__ T vt_flux_s(const PAdvArgs<T>& a, T s, int k) {
     return T(a.p.rhow[k]) * VT * s;
 }
 
-// Dynamic shared memory: sizeof(PAdvShared<T>) (about 35 KB FP64, 18 KB
+// Dynamic shared memory: sizeof(PAdvShared<T>) (about 36 KB FP64, 19 KB
 // mixed). At most 64 registers a thread, four blocks a SM (neither step
-// spills).
+// spills). map[f]: the tensor map of a.now[f], box {kPAdvVX, kPAdvVZ}.
 template <typename T>
-__global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
-    constexpr int BX = kPAdvBX, BZ = kPAdvBZ, VX = BX + 4, VZ = BZ + 4;
-    extern __shared__ __align__(16) unsigned char padv_smem[];
+__global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4)
+    k_padv(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
+           const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3, PAdvArgs<T> a) {
+    constexpr int BX = kPAdvBX, BZ = kPAdvBZ, VX = kPAdvVX, VZ = kPAdvVZ, OFF = kPAdvOff<T>;
+    extern __shared__ __align__(128) unsigned char padv_smem[];
+    __shared__ uint64_t stage_bar;
     PAdvShared<T>& S = *reinterpret_cast<PAdvShared<T>*>(padv_smem);
     const Dims& d = a.d;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + BX * ty;
@@ -455,20 +467,21 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
     const int i = i0 + tx, k = k0 + ty;
     const bool act = (i <= d.nx - 2 && k <= d.nz - 2);
 
-    // Stage the fields: only points inside the array are copied; the ones
-    // outside (row -1, column -1, beyond nz-1 or nx-1) are never read, since
-    // a face reads its outer neighbours only where the third-order bracket
-    // applies (2 <= index <= n-3).
-    for (int f = 0; f < 4; f++) {
-        if (!(a.mask & (1 << f))) continue;
-        const T* v = a.now[f];
-        for (int t = tid; t < VZ * VX; t += BX * BZ) {
-            const int r = t / VX, c = t - r * VX;
-            const int kk = k0 - 2 + r, ii = i0 - 2 + c;
-            if (kk >= 0 && kk <= d.nz - 1 && ii >= 0 && ii <= d.nx - 1) cp_async_elem(&S.v[f][r][c], v + d.at(ii, kk));
-        }
+    // Stage the fields, one TMA box each: points outside the array read as
+    // zero and are never used, since a face reads its outer neighbours only
+    // where the third-order bracket applies (2 <= index <= n-3).
+    const uint32_t bar = smem_u32(&stage_bar);
+    if (tid == 0) mbar_init1(bar);
+    __syncthreads();
+    if (tid == 0) {
+        const CUtensorMap* maps[4] = {&m0, &m1, &m2, &m3};
+        uint32_t bytes = 0;
+        for (int f = 0; f < 4; f++)
+            if (a.mask & (1 << f)) bytes += VZ * VX * sizeof(T);
+        mbar_expect_tx(bar, bytes);
+        for (int f = 0; f < 4; f++)
+            if (a.mask & (1 << f)) tma_load_2d(smem_u32(&S.v[f][0][0]), maps[f], i0 - 2 - OFF, k0 - 2, bar);
     }
-    cp_async_commit();
 
     // Faces: x face (r, c) is fi = i0 + c, between cells fi-1 and fi, on row
     // k0 + r; the east face of cell nx-2 is the halo copy of face 1
@@ -486,15 +499,20 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
     Face<T> Fx{}, Fz{};
     if (xo) Fx = face_u(a, xface_i(tx), k0 + ty);
     if (zo) Fz = face_w(a, i0 + tx, k0 + ty);
-    cp_async_wait<0>();
-    __syncthreads();
+    const bool ok = mbar_wait_bounded(bar, 0);
+    if (__syncthreads_or(!ok)) {   // the copies never landed: report and leave
+        if (tid == 0 && a.err) atomicOr(a.err, kStageErrWait);
+        mbar_wait_bounded(bar, 0);
+        return;
+    }
 
+    // staged column of index ii: ii - (i0 - 2) + OFF
     auto xflux = [&](const Face<T>& F, int f, int r, int c) {
         if (i0 + c == d.nx - 1) {   // face 1 (no bracket), read where it lies
             const T* v = a.now[f];
             return face_flux(F, T(0), v[d.at(0, k0 + r)], v[d.at(1, k0 + r)], T(0));
         }
-        const T* row = &S.v[f][r + 2][c];   // columns fi-2 .. fi+1
+        const T* row = &S.v[f][r + 2][c + OFF];   // columns fi-2 .. fi+1
         return face_flux(F, F.hi ? row[0] : T(0), row[1], row[2], F.hi ? row[3] : T(0));
     };
     // th and qv of the mixed step take the perturbation form (third-order
@@ -502,8 +520,8 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
     auto zflux = [&](const Face<T>& F, int f, int r, int c) {
         const int fk = k0 + r;
         if (fk == d.nz - 1) return T(0);
-        const T vmm = S.v[f][r][c + 2], vm = S.v[f][r + 1][c + 2], v0 = S.v[f][r + 2][c + 2],
-                vp = S.v[f][r + 3][c + 2];   // rows fk-2 .. fk+1
+        const T vmm = S.v[f][r][c + 2 + OFF], vm = S.v[f][r + 1][c + 2 + OFF], v0 = S.v[f][r + 2][c + 2 + OFF],
+                vp = S.v[f][r + 3][c + 2 + OFF];   // rows fk-2 .. fk+1
         if (kPert<T> && f < 2 && F.hi) {
             const double* d0 = a.p.d0[f];
             return face_flux_pert(F, vmm, vm, v0, vp, T(d0[fk - 1]), T(d0[fk]), T(d0[fk + 1]));
@@ -512,7 +530,7 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
     };
     auto gflux = [&](int r, int c) {
         const int fk = k0 + r;
-        return fk == d.nz - 1 ? T(0) : vt_flux_s(a, S.v[3][r + 2][c + 2] + S.v[3][r + 1][c + 2], fk);
+        return fk == d.nz - 1 ? T(0) : vt_flux_s(a, S.v[3][r + 2][c + 2 + OFF] + S.v[3][r + 1][c + 2 + OFF], fk);
     };
 
     const bool vt = (a.mask & F_QR) && a.do_vt;
@@ -575,7 +593,7 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4) k_padv(PAdvArgs<T> a) {
             }
             T t = -px - pz;
             T o = ab2_push(a.hn[f], a.ho[f], id, t, a.ab);
-            T out = S.v[f][ty + 2][tx + 2] + dt15 * t - dt05 * o;
+            T out = S.v[f][ty + 2][tx + 2 + OFF] + dt15 * t - dt05 * o;
             if (f == 3 && vt) {
                 const T gp = S.gz[ty + 1][tx], g0 = S.gz[ty][tx];
                 T tv = kPert<T> ? (gp - g0) * sz : (gp - g0) * T(a.p.r2dzc[k]) / ru;

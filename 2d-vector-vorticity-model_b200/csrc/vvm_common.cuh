@@ -118,6 +118,55 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* sh) {
     __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// Shared-memory barriers and TMA loads (sm_100a PTX).
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// One-arrival barrier for a block's TMA loads (call from one thread, then
+// __syncthreads before any thread waits on it).
+__device__ __forceinline__ void mbar_init1(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// Waits for phase `parity` of the barrier, polling at most kStageSpinLimit
+// times; false if it gave up.
+constexpr int kStageSpinLimit = 1 << 22;
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    for (int it = 0; it < kStageSpinLimit; it++)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
+// 2D tiled TMA load of a box at (x, y) into shared memory (no multicast);
+// completion counted on `bar`. x times the element size must be a multiple
+// of 16 bytes; y and x may be negative or out of range (zero fill).
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
 // Grid-wide finish of per-block partial sums without a second launch. Every
 // block calls it once, after its thread 0 has written the block's partial;
 // it returns true in the one block that arrives last (thread 0 fences its

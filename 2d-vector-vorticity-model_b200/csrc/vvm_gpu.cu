@@ -1014,14 +1014,11 @@ __global__ void k_net_galerkin(int NX, int NK, int pitch, const CGScalars* sc, c
 // chunk-major BF16 activations, boxes {64, 18, 1} and {64, 1, 1}) are encoded
 // through the driver's cuTensorMapEncodeTiled and cached per (tensor, H, W,
 // box width): the map is a function of those alone.
-CUtensorMap conv_map(const void* p, int H, int W, int boxw) {
+// The driver's tensor-map encoder (looked up once).
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
     static std::mutex mu;
-    static std::map<std::tuple<const void*, int, int, int>, CUtensorMap> cache;
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
     std::lock_guard<std::mutex> lock(mu);
-    auto key = std::make_tuple(p, H, W, boxw);
-    auto it = cache.find(key);
-    if (it != cache.end()) return it->second;
     if (!enc) {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q{};
@@ -1029,6 +1026,41 @@ CUtensorMap conv_map(const void* p, int H, int W, int boxw) {
         if (!fn || q != cudaDriverEntryPointSuccess) throw CudaError{"cuTensorMapEncodeTiled: not found in the driver"};
         enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
+    return enc;
+}
+
+// Tensor map of one field buffer for the stencils' TMA staging: nz rows of
+// nx columns (the pitch padding outside it, so loads past column nx-1 or row
+// nz-1 fill zeros), element size 8 (FP64) or 4 (FP32), box {bx, by}. Cached
+// per (buffer, shape, box): the map is a function of those alone.
+CUtensorMap field_map(const void* p, int nx, int nz, int pitch, int elem, int bx, int by) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, int, int, int, int>, CUtensorMap> cache;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_tuple(p, nx, nz, pitch, elem, bx, by);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)nz};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * (cuuint64_t)elem};
+    cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by}, es[2] = {1, 1};
+    CUresult r = enc(&m, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                     const_cast<void*>(p), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw CudaError{"cuTensorMapEncodeTiled (field) failed"};
+    cache.emplace(key, m);
+    return m;
+}
+
+CUtensorMap conv_map(const void* p, int H, int W, int boxw) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, int>, CUtensorMap> cache;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_tuple(p, H, W, boxw);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
     // chunk-major activations as {64 elements (8 pixels x 8 channels), W / 8
     // pixel blocks, 4 H chunk rows}; boxw counts pixels (a multiple of 8)
     CUtensorMap m;
@@ -1706,9 +1738,13 @@ void launch_padv(vvm_gpu_ctx* c, int mask, int nvp_mask, bool vt, bool precip) {
     a.do_vt = vt;
     a.do_precip = precip;
     a.ab = ab;
+    a.err = c->d_err;
     dim3 g = c->padv_grid();
+    CUtensorMap m[4];
+    for (int f = 0; f < 4; f++)
+        m[f] = field_map(a.now[f], c->d.nx, c->d.nz, c->d.pitch, (int)sizeof(T), kPAdvVX, kPAdvVZ);
     LAUNCH(&c->stats, VVM_K_PADV, c->stream,
-           k_padv<T><<<g, c->padv_blk(), sizeof(PAdvShared<T>), c->stream>>>(a));
+           k_padv<T><<<g, c->padv_blk(), sizeof(PAdvShared<T>), c->stream>>>(m[0], m[1], m[2], m[3], a));
     CKL();
     if (nvp_mask) {
         LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp));
@@ -2549,8 +2585,9 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     //          Kessler, its NVP and the halos of th, qv, qc, qr, beside
     //          cal_w and cal_u (which touch zeta, w, u only).
     // A batch's cases are already parallel branches of its graph: there every
-    // case runs as one chain, in the order below.
-    const bool br = c->branches;
+    // case runs as one chain, in the order below; so does a profiled step,
+    // whose event timers should each see one kernel at a time.
+    const bool br = c->branches && !c->stats.on;
     if (br) {
         fork_to(c, 0, 0);
         OnStream os(c, c->side[0]);
