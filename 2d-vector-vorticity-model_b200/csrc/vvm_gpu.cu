@@ -1581,8 +1581,8 @@ struct vvm_gpu_ctx {
     cudaGraphExec_t gexec[2][2] = {};
     long long gstatic[2][2] = {};      // kernels outside the solver loops
     cudaStream_t cap[2] = {};          // streams for capturing loop bodies
-    cudaStream_t side[2] = {};         // branches of a step that run beside the main chain
-    cudaEvent_t fork_ev[4] = {};       // their fork and join points
+    cudaStream_t side = nullptr;       // the step's second chain (run_step)
+    cudaEvent_t fork_ev[3] = {};       // its fork, meeting and join points
     bool branches = true;              // use them (off inside a batch: the cases are the branches)
     CGCtl* wctl = nullptr;             // outer loop state of the mixed solve
     long long* d_exec = nullptr;       // kernels executed inside graph loops
@@ -1614,8 +1614,7 @@ struct vvm_gpu_ctx {
         if (fcg_host) cudaFreeHost(fcg_host);
         for (auto s : cap)
             if (s) cudaStreamDestroy(s);
-        for (auto s : side)
-            if (s) cudaStreamDestroy(s);
+        if (side) cudaStreamDestroy(side);
         for (auto e : fork_ev)
             if (e) cudaEventDestroy(e);
         if (pcg64) pcg64->release();
@@ -2434,7 +2433,9 @@ long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
 }
 
 template <typename T>
-int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
+// before_w: an event the velocity update (k_w_from_W, which writes w) waits
+// for, when kernels that read w run beside the solve.
+int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr, cudaEvent_t before_w = nullptr) {
     ensure_poisson(c);
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
@@ -2454,6 +2455,7 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
         }
         *recorded_in_loops = record_solve(c, c->desc.poisson_tol, maxit, warm);
         c->nsolves++;
+        if (before_w) CK(cudaStreamWaitEvent(c->stream, before_w, 0));
         LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_w_from_W<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(c->d, c->rhow, c->W, pitch, F.w));
         CKL();
         return VVM_GPU_OK;
@@ -2474,6 +2476,7 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     }
     int rc = solve_w(c, bb, c->desc.poisson_tol, warm);
     c->nsolves++;
+    if (before_w) CK(cudaStreamWaitEvent(c->stream, before_w, 0));
     LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_w_from_W<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(c->d, c->rhow, c->W, pitch, F.w));
     CKL();
     return rc;
@@ -2551,16 +2554,16 @@ int launch_calpsiuw(vvm_gpu_ctx* c) {
 
 // ---------------------------------------------------------------- one step
 
-// Fork/join of a step's side branches: side stream s waits for everything
+// Fork/join of a step's second chain: the side stream waits for everything
 // issued on the context's stream so far (fork), and the context's stream
-// waits for everything issued on side s (join). Inside a stream capture
-// these become branches of the graph.
-void fork_to(vvm_gpu_ctx* c, int s, int e) {
+// waits for everything issued on the side stream (join). Inside a stream
+// capture these become branches of the graph.
+void fork_side(vvm_gpu_ctx* c, int e) {
     CK(cudaEventRecord(c->fork_ev[e], c->stream));
-    CK(cudaStreamWaitEvent(c->side[s], c->fork_ev[e], 0));
+    CK(cudaStreamWaitEvent(c->side, c->fork_ev[e], 0));
 }
-void join_from(vvm_gpu_ctx* c, int s, int e) {
-    CK(cudaEventRecord(c->fork_ev[e], c->side[s]));
+void join_side(vvm_gpu_ctx* c, int e) {
+    CK(cudaEventRecord(c->fork_ev[e], c->side));
     CK(cudaStreamWaitEvent(c->stream, c->fork_ev[e], 0));
 }
 struct OnStream {   // issues a scope's launches on another stream
@@ -2574,50 +2577,60 @@ template <typename T>
 int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     c->step++;                                                 // Iteration.cpp:246
     const bool sf = (c->desc.flags & VVM_FLAG_STREAMFUNCTION) != 0;
-    // Two branches run beside the main chain (in a captured step they are
-    // parallel branches of the graph; the results are those of the
-    // reference's order, since no branch reads what another writes):
-    //  side 0: pubarTop_pt (reads u, w, RKM; writes only ubar, dubar, read by
-    //          cal_u) and pzeta_pt (writes zetap and its tendencies), beside
-    //          the scalar advection, which writes th, qv, qc, qr's future
-    //          values and tendencies only;
-    //  side 1: the NVP rescaling and AddForcing of the advected fields,
-    //          Kessler, its NVP and the halos of th, qv, qc, qr, beside
-    //          cal_w and cal_u (which touch zeta, w, u only).
-    // A batch's cases are already parallel branches of its graph: there every
-    // case runs as one chain, in the order below; so does a profiled step,
-    // whose event timers should each see one kernel at a time.
+    // The step's kernels form two chains (in a captured step, two branches of
+    // the graph; the results are those of the reference's order, since
+    // neither chain reads what the other writes before they meet):
+    //  main: pubarTop_pt (reads u, w, RKM; writes ubar, dubar), pzeta_pt
+    //        (writes zetap and its tendencies), cal_w up to its solution W,
+    //        then, once the scalar advection has read w and u, w from W
+    //        and cal_u;
+    //  side: the scalar advection (writes the future th, qv, qc, qr and
+    //        their tendencies), their NVP rescaling and AddForcing, Kessler,
+    //        its NVP and the halos of th, qv, qc, qr.
+    // They meet before the turbulence. A batch's cases are already parallel
+    // branches of its graph: there every case runs as one chain, in the
+    // reference's order; so does a profiled step, whose event timers should
+    // each see one kernel at a time.
     const bool br = c->branches && !c->stats.on;
-    if (br) {
-        fork_to(c, 0, 0);
-        OnStream os(c, c->side[0]);
-        if (!sf) launch_pubartop<T>(c);                        // pubarTop_pt
-        launch_pzeta<T>(c);                                    // pzeta_pt
-    } else {
-        launch_pzeta<T>(c);
-    }
-    launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
-    if (br) {
-        fork_to(c, 1, 1);
-        OnStream os(c, c->side[1]);
-        launch_kessler<T>(c, true, true);                      // NVP + AddForcing, Kessler + NVP x3 + halos
-    }
     int rc = VVM_GPU_OK;
-    try {
-        if (br) join_from(c, 0, 2);                            // zetap; ubar, dubar; u, w read
-        if (sf) {
-            rc = launch_calpsiuw<T>(c);                        // calpsiuw (Iteration.cpp:289-290)
-        } else {
-            if (!br) launch_pubartop<T>(c);
-            rc = launch_cal_w<T>(c, recorded_in_loops);        // cal_w
-            launch_cal_u<T>(c);                                // cal_u
+    if (br) {
+        fork_side(c, 0);
+        {
+            OnStream os(c, c->side);
+            launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
+            CK(cudaEventRecord(c->fork_ev[1], c->side));   // u and w read
+            launch_kessler<T>(c, true, true);                  // NVP + AddForcing, Kessler + NVP x3 + halos
         }
-    } catch (...) {
-        if (br) join_from(c, 1, 3);
-        throw;
+        try {
+            if (!sf) launch_pubartop<T>(c);                    // pubarTop_pt
+            launch_pzeta<T>(c);                                // pzeta_pt
+            if (sf) {
+                CK(cudaStreamWaitEvent(c->stream, c->fork_ev[1], 0));
+                rc = launch_calpsiuw<T>(c);                    // calpsiuw (Iteration.cpp:289-290)
+            } else {
+                rc = launch_cal_w<T>(c, recorded_in_loops, c->fork_ev[1]);   // cal_w
+                launch_cal_u<T>(c);                            // cal_u
+            }
+        } catch (...) {
+            join_side(c, 2);
+            throw;
+        }
+        join_side(c, 2);
+    } else {
+        launch_pzeta<T>(c);                                    // pzeta_pt
+        launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
+        if (sf) {
+            rc = launch_calpsiuw<T>(c);
+        } else {
+            launch_pubartop<T>(c);
+            rc = launch_cal_w<T>(c, recorded_in_loops);
+            launch_cal_u<T>(c);
+        }
+        // NVP and AddForcing of the advected fields run inside Kessler's
+        // kernel (nothing before it reads th, qv, qc, qr; their halos come
+        // after it)
+        launch_kessler<T>(c, true, true);
     }
-    if (br) join_from(c, 1, 3);
-    else launch_kessler<T>(c, true, true);
     // The first updateMean of the step (Iteration.cpp:408) only writes thb,
     // qvb, thvb, which nextTimeStep's updateMean overwrites before any read.
     launch_turbulence<T>(c, true, recorded_in_loops);          // RKM_RKH + diffusion + theta/zeta nudging
@@ -3600,7 +3613,7 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         c->d_exec = c->ar.alloc<long long>(1);
         c->d_err = c->ar.alloc<int>(1);
         for (auto& cs : c->cap) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        for (auto& cs : c->side) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
         for (auto& e : c->fork_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     } catch (const CudaError& e) {
         cudaSetDevice(prev);
@@ -3743,7 +3756,7 @@ int vvm_gpu_random_perturbation_host(int NX, int NZ, double dz, int t, double mi
 }
 ROUTINE(vvm_gpu_halo_all, { DISPATCH(ctx, launch_halo_all)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_pubartop, { DISPATCH(ctx, launch_pubartop)(ctx); return VVM_GPU_OK; })
-ROUTINE(vvm_gpu_cal_w, { ctx->last_graph = false; return DISPATCH(ctx, launch_cal_w)(ctx, nullptr); })
+ROUTINE(vvm_gpu_cal_w, { ctx->last_graph = false; return DISPATCH(ctx, launch_cal_w)(ctx, nullptr, nullptr); })
 ROUTINE(vvm_gpu_cal_u, { DISPATCH(ctx, launch_cal_u)(ctx); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_kessler, { DISPATCH(ctx, launch_kessler)(ctx, false, false); return VVM_GPU_OK; })
 ROUTINE(vvm_gpu_update_mean, { DISPATCH(ctx, launch_update_mean)(ctx, false); return VVM_GPU_OK; })
