@@ -158,6 +158,9 @@ def class_bytes(cls: str, launches: int, grid, elem: int, cg_iters: float) -> fl
 
 # ----------------------------------------------------------------- our arm
 
+GRAPH_WARMUP = 4   # steps until both of a context's step graphs exist
+
+
 def timed_steps(torch, g, steps, flush):
     import torch as T
     st = T.cuda.current_stream()
@@ -180,7 +183,9 @@ def run_variant(torch, precision, solver, steps, warmup, flush, device):
     g = VVMGpu(st.grid, precision=precision, solver=solver, device=device)
     g.set_stream(torch.cuda.current_stream().cuda_stream)
     g.upload(st)
-    g.step(warmup)
+    # at least GRAPH_WARMUP untimed steps: a step runs as one of two CUDA
+    # graphs (one per step parity), each captured on its first use
+    g.step(max(warmup, GRAPH_WARMUP))
     g.synchronize()
     n0 = g.launch_count
     times = timed_steps(torch, g, steps, flush)
@@ -359,6 +364,7 @@ def our_arm(args, rank, world, device):
                              "FP64, residual-checked; FP64 CG preconditioned by it if the check "
                              "fails",
                    "poisson_tol": 1e-10, "l2": "flushed (256 MB write) between timed steps",
+                   "graph_warmup": f"max(warmup, {GRAPH_WARMUP}) untimed steps, so both step graphs (one per step parity) are captured before timing",
                    "parallelism": f"replicas x{world}"},
         "poisson_ms_per_solve": poisson_ms(head["prof"]),
         "poisson_solves_per_s": 1e3 / poisson_ms(head["prof"]),
@@ -439,7 +445,7 @@ def learned_arm(args, world, device, flush, hbm, peak_kind, fp64_ms_per_step, w,
         g.upload(st)
         g.learned_weights(w)
         g.learned_config(mode=mode, cap=4000)
-        g.step(1)
+        g.step(GRAPH_WARMUP)   # both step graphs captured before the timed steps
         g.synchronize()
         if dist_on():
             dist_barrier()
