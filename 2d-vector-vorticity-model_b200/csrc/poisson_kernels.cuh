@@ -541,7 +541,7 @@ struct VecArgs {
 
 // q = S p and partial <p, q>.
 template <typename P>
-__global__ void k_cg_spmv(VecArgs<P> v, const P* p, P* q, double* partial) {
+__device__ __forceinline__ void k_cg_spmv_body(const VecArgs<P>& v, const P* p, P* q, double* partial) {
     __shared__ double sh[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int kk = blockIdx.y * blockDim.y + threadIdx.y;
@@ -555,10 +555,12 @@ __global__ void k_cg_spmv(VecArgs<P> v, const P* p, P* q, double* partial) {
     block_sum(s, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
 }
+template <typename P>
+__global__ void k_cg_spmv(VecArgs<P> v, const P* p, P* q, double* partial) { k_cg_spmv_body<P>(v, p, q, partial); }
 
 // x += alpha p; r -= alpha q; partial ||rhow r||^2.
 template <typename P>
-__global__ void k_cg_update(VecArgs<P> v, const CGScalars* sc, P* x, P* r, const P* p, const P* q,
+__device__ __forceinline__ void k_cg_update_body(const VecArgs<P>& v, const CGScalars* sc, P* x, P* r, const P* p, const P* q,
                             double* partial) {
     __shared__ double sh[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -576,10 +578,13 @@ __global__ void k_cg_update(VecArgs<P> v, const CGScalars* sc, P* x, P* r, const
     block_sum(s, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
 }
+template <typename P>
+__global__ void k_cg_update(VecArgs<P> v, const CGScalars* sc, P* x, P* r, const P* p, const P* q,
+                            double* partial) { k_cg_update_body<P>(v, sc, x, r, p, q, partial); }
 
 // partial <r, z>.
 template <typename P>
-__global__ void k_cg_dot(VecArgs<P> v, const P* r, const P* z, double* partial) {
+__device__ __forceinline__ void k_cg_dot_body(const VecArgs<P>& v, const P* r, const P* z, double* partial) {
     __shared__ double sh[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int kk = blockIdx.y * blockDim.y + threadIdx.y;
@@ -591,6 +596,8 @@ __global__ void k_cg_dot(VecArgs<P> v, const P* r, const P* z, double* partial) 
     block_sum(s, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
 }
+template <typename P>
+__global__ void k_cg_dot(VecArgs<P> v, const P* r, const P* z, double* partial) { k_cg_dot_body<P>(v, r, z, partial); }
 
 // p = z + beta p (beta = 0 on the first iteration).
 template <typename P>
@@ -629,7 +636,7 @@ struct CGCtl {
     int it;          // CG iterations of the current (inner) solve
     int total;       // CG iterations summed over refinement passes
     int outer;       // refinement passes
-    int pad;
+    int more;        // the loop's last decision (1: another iteration), for grouped launches
     double rr0;      // squared initial residual of the inner solve
     double relres;   // final ||b - A W|| / ||b||
 };
@@ -641,7 +648,7 @@ __global__ void k_cg_scalar_it(const double* partial, int n, CGScalars* sc, cons
 
 // p = z (first iteration of ctl) or z + beta p.
 template <typename P>
-__global__ void k_cg_dir_it(VecArgs<P> v, const CGScalars* sc, const CGCtl* ctl, const P* z, P* p) {
+__device__ __forceinline__ void k_cg_dir_it_body(const VecArgs<P>& v, const CGScalars* sc, const CGCtl* ctl, const P* z, P* p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int kk = blockIdx.y * blockDim.y + threadIdx.y;
     if (i < v.nx && kk < v.NK) {
@@ -649,6 +656,8 @@ __global__ void k_cg_dir_it(VecArgs<P> v, const CGScalars* sc, const CGCtl* ctl,
         p[id] = (ctl->it == 0) ? z[id] : P((double)z[id] + sc->beta * (double)p[id]);
     }
 }
+template <typename P>
+__global__ void k_cg_dir_it(VecArgs<P> v, const CGScalars* sc, const CGCtl* ctl, const P* z, P* p) { k_cg_dir_it_body<P>(v, sc, ctl, z, p); }
 
 // W = 0 when ||b|| = 0 (the solution of A W = 0), read on the device.
 __global__ void k_zero_if_b0(int NX, int NK, int pitch, const CGScalars* sc, double* W);
@@ -676,7 +685,7 @@ __global__ void k_loop_outer(const CGScalars* sc64, CGCtl* ctl, const CGCtl* inn
 // state (ctl) and sets the condition of the WHILE node that follows:
 // continue while ||rhow r||^2 > tol^2 ||b||^2 and maxit > 0.
 template <typename P>
-__global__ void k_cg_check(VecArgs<P> v, const P* f, P* x, P* r, double* partial, CGScalars* sc, CGCtl* ctl,
+__device__ __forceinline__ void k_cg_check_body(const VecArgs<P>& v, const P* f, P* x, P* r, double* partial, CGScalars* sc, CGCtl* ctl,
                            unsigned* arrive, cudaGraphConditionalHandle h, double tol2, int maxit) {
     __shared__ double sh[32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -711,8 +720,12 @@ __global__ void k_cg_check(VecArgs<P> v, const P* f, P* x, P* r, double* partial
         ctl->total = 0;
         ctl->relres = (bb > 0.0) ? sqrt(rr / bb) : 0.0;
         const bool more = (bb > 0.0) && (rr > tol2 * bb) && (maxit > 0) && isfinite(rr);
-        cudaGraphSetConditional(h, more ? 1u : 0u);
+        ctl->more = more ? 1 : 0;
+        if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
     }
 }
+template <typename P>
+__global__ void k_cg_check(VecArgs<P> v, const P* f, P* x, P* r, double* partial, CGScalars* sc, CGCtl* ctl,
+                           unsigned* arrive, cudaGraphConditionalHandle h, double tol2, int maxit) { k_cg_check_body<P>(v, f, x, r, partial, sc, ctl, arrive, h, tol2, maxit); }
 
 }  // namespace vvm

@@ -126,7 +126,7 @@ __device__ __forceinline__ int bitrev(int j, int logN) { return (int)(__brev((un
 
 // Spectra of rows 2b and 2b+1 of r ([NK][pitch]).
 template <typename P>
-__global__ void k_spec_forward(SpecArgs<P> a, const P* r) {
+__device__ __forceinline__ void k_spec_forward_body(const SpecArgs<P>& a, const P* r) {
     extern __shared__ unsigned char smem_raw[];
     P* re = reinterpret_cast<P*>(smem_raw);
     P* im = re + a.NX;
@@ -154,6 +154,8 @@ __global__ void k_spec_forward(SpecArgs<P> a, const P* r) {
         }
     }
 }
+template <typename P>
+__global__ void k_spec_forward(SpecArgs<P> a, const P* r) { k_spec_forward_body<P>(a, r); }
 
 // The z solve of every mode m = 0..NX/2 in place on the spectra, by the
 // twisted factorisation precomputed per mode (inv, cp, den): rows 0..mid are
@@ -171,7 +173,7 @@ __global__ void k_spec_forward(SpecArgs<P> a, const P* r) {
 constexpr int kModeSegs = 16;
 
 template <typename P>
-__global__ void __launch_bounds__(64 * kModeSegs) k_spec_modes_seg(SpecArgs<P> a) {
+__device__ __forceinline__ void k_spec_modes_seg_body(const SpecArgs<P>& a) {
     __shared__ P shA[2][kModeSegs][32][3];   // (A re, A im, B) per half, segment, lane
     __shared__ P shY[2][32][2];              // the halves' last rows after elimination
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -284,10 +286,12 @@ __global__ void __launch_bounds__(64 * kModeSegs) k_spec_modes_seg(SpecArgs<P> a
         }
     }
 }
+template <typename P>
+__global__ void __launch_bounds__(64 * kModeSegs) k_spec_modes_seg(SpecArgs<P> a) { k_spec_modes_seg_body<P>(a); }
 
 // Rows 2b and 2b+1 of out ([NK][pitch]) from their spectra, scaled by 1/NX.
 template <typename P>
-__global__ void k_spec_inverse(SpecArgs<P> a, P* out) {
+__device__ __forceinline__ void k_spec_inverse_body(const SpecArgs<P>& a, P* out) {
     extern __shared__ unsigned char smem_raw[];
     P* re = reinterpret_cast<P*>(smem_raw);
     P* im = re + a.NX;
@@ -319,5 +323,7 @@ __global__ void k_spec_inverse(SpecArgs<P> a, P* out) {
         if (two) out[(size_t)k1 * a.pitch + j] = im[j] * scale;
     }
 }
+template <typename P>
+__global__ void k_spec_inverse(SpecArgs<P> a, P* out) { k_spec_inverse_body<P>(a, out); }
 
 }  // namespace vvm

@@ -133,7 +133,7 @@ struct PZetaShared {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(kPZBX * kPZBZ) k_pzeta(PZetaArgs<T> a) {
+__device__ __forceinline__ void k_pzeta_body(const PZetaArgs<T>& a) {
     constexpr int BX = kPZBX, BZ = kPZBZ, NT = BX * BZ;
     __shared__ PZetaShared<T> S;
     const Dims& d = a.d;
@@ -263,6 +263,8 @@ __global__ void __launch_bounds__(kPZBX * kPZBZ) k_pzeta(PZetaArgs<T> a) {
     zp += (dt15 * tb) - (dt05 * ob);
     store_westdown(a.zetap, d, i, k, zp);
 }
+template <typename T>
+__global__ void __launch_bounds__(kPZBX * kPZBZ) k_pzeta(PZetaArgs<T> a) { k_pzeta_body<T>(a); }
 
 // ---------------------------------------------------------------------------
 // Scalar advection (Advection_thermo, Advection.cpp:25-81) of th, qv, qc, qr,
@@ -453,10 +455,11 @@ __device__ __forceinline__ T vt_flux_s(const PAdvArgs<T>& a, T s, int k) {
 // Dynamic shared memory: sizeof(PAdvShared<T>) (about 36 KB FP64, 19 KB
 // mixed). At most 64 registers a thread, four blocks a SM (neither step
 // spills). map[f]: the tensor map of a.now[f], box {kPAdvVX, kPAdvVZ}.
+// The maps are read where they lie (a kernel parameter, or global memory
+// for a grouped launch): TMA takes their addresses.
 template <typename T>
-__global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4)
-    k_padv(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
-           const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3, PAdvArgs<T> a) {
+__device__ __forceinline__ void k_padv_body(const CUtensorMap* m0, const CUtensorMap* m1, const CUtensorMap* m2,
+                                            const CUtensorMap* m3, const PAdvArgs<T>& a) {
     constexpr int BX = kPAdvBX, BZ = kPAdvBZ, VX = kPAdvVX, VZ = kPAdvVZ, OFF = kPAdvOff<T>;
     extern __shared__ __align__(128) unsigned char padv_smem[];
     __shared__ uint64_t stage_bar;
@@ -474,7 +477,7 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4)
     if (tid == 0) mbar_init1(bar);
     __syncthreads();
     if (tid == 0) {
-        const CUtensorMap* maps[4] = {&m0, &m1, &m2, &m3};
+        const CUtensorMap* maps[4] = {m0, m1, m2, m3};
         uint32_t bytes = 0;
         for (int f = 0; f < 4; f++)
             if (a.mask & (1 << f)) bytes += VZ * VX * sizeof(T);
@@ -625,6 +628,12 @@ __global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4)
         }
     }
 }
+template <typename T>
+__global__ void __launch_bounds__(kPAdvBX * kPAdvBZ, 4)
+    k_padv(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
+           const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3, PAdvArgs<T> a) {
+    k_padv_body<T>(&m0, &m1, &m2, &m3, a);
+}
 
 // ---------------------------------------------------------------------------
 // Finishes th, qv, qc, qr after advection or microphysics: the rescaling of
@@ -685,7 +694,7 @@ __device__ __forceinline__ T finish_value(const AdvFinish<T>& a, const Profiles&
 }
 
 template <typename T>
-__global__ void k_apply(ApplyArgs<T> a) {
+__device__ __forceinline__ void k_apply_body(const ApplyArgs<T>& a) {
     const Dims& d = a.d;
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -700,6 +709,8 @@ __global__ void k_apply(ApplyArgs<T> a) {
         else a.fut[f][id] = v;
     }
 }
+template <typename T>
+__global__ void k_apply(ApplyArgs<T> a) { k_apply_body<T>(a); }
 
 // ---------------------------------------------------------------------------
 // BoundaryProcess2D_all (Boundary.cpp:32-52) as a standalone pass.
@@ -799,7 +810,7 @@ __device__ __forceinline__ void kessler_cell(C& th, C& qv, C& qc, C& qr, C dt, C
 // the saturation adjustment subtracts qvs from qv, which cancel to a few
 // units of the FP32 epsilon near saturation.
 template <typename T>
-__global__ void k_kessler(KesslerArgs<T> a) {
+__device__ __forceinline__ void k_kessler_body(const KesslerArgs<T>& a) {
     using C = double;
     __shared__ double sh[32 * 6];
     const Dims& d = a.d;
@@ -850,6 +861,8 @@ __global__ void k_kessler(KesslerArgs<T> a) {
         }
     }
 }
+template <typename T>
+__global__ void k_kessler(KesslerArgs<T> a) { k_kessler_body<T>(a); }
 
 // ---------------------------------------------------------------------------
 // Eddy coefficients (Turbulence::RKM_RKH, Turbulent.cpp:5-45) with their
@@ -865,7 +878,7 @@ struct RKArgs {
 };
 
 template <typename T>
-__global__ void k_rkm_rkh(RKArgs<T> a) {
+__device__ __forceinline__ void k_rkm_rkh_body(const RKArgs<T>& a) {
     const Dims& d = a.d;
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 1 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -904,6 +917,8 @@ __global__ void k_rkm_rkh(RKArgs<T> a) {
     store_center(a.RKM, d, i, k, km);
     store_center(a.RKH, d, i, k, kh);
 }
+template <typename T>
+__global__ void k_rkm_rkh(RKArgs<T> a) { k_rkm_rkh_body<T>(a); }
 
 // ---------------------------------------------------------------------------
 // In-place Gauss-Seidel diffusion (Turbulence::Mparam / Hparam,
@@ -1027,7 +1042,7 @@ __device__ __forceinline__ void gs_ld4(const T* p, T (&x)[4]) {
 // Nudge_theta) of interior cells, carries the un-nudged ones.
 // FIRST: pass 1 (launched on its own, before the loop of the later passes).
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) {
+__device__ __forceinline__ void k_gs_tiles_body(const GSArgs<T>& a, const GSTileArgs<T>& t, cudaGraphConditionalHandle h) {
     __shared__ int any_changed;
     // per warp and row of its tile: cz, the czd and czu density factors,
     // nudging dn and tn, the inflow left of the row and its previous value,
@@ -1328,6 +1343,8 @@ __global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> 
         }
     }
 }
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) { k_gs_tiles_body<T, FIRST>(a, t, h); }
 
 // ---------------------------------------------------------------------------
 // The second schedule of the same recurrence: one thread-block cluster a field.
@@ -1742,7 +1759,7 @@ struct NudgeArgs {
 };
 
 template <typename T>
-__global__ void k_nudge(NudgeArgs<T> a) {
+__device__ __forceinline__ void k_nudge_body(const NudgeArgs<T>& a) {
     const Dims& d = a.d;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1761,6 +1778,8 @@ __global__ void k_nudge(NudgeArgs<T> a) {
     if (a.tau != 0.0)  // every cell, ghosts included (NumericalProcess.cpp:90-94)
         a.qvp[id] = a.qvp[id] + T(a.c.dt) * ((kPert<T> ? T(-a.p.dn[1][k]) : T(a.p.qvb0[k])) - a.qv[id]) / T(a.tau);
 }
+template <typename T>
+__global__ void k_nudge(NudgeArgs<T> a) { k_nudge_body<T>(a); }
 
 // ---------------------------------------------------------------------------
 // Horizontal means (Iteration::updateMean, Iteration.cpp:42-86): thb, qvb and
@@ -1778,7 +1797,7 @@ struct MeanArgs {
 };
 
 template <typename T>
-__global__ void k_update_mean(MeanArgs<T> a) {
+__device__ __forceinline__ void k_update_mean_body(const MeanArgs<T>& a) {
     __shared__ double sh[32 * 2];
     const Dims& d = a.d;
     const int k = 1 + blockIdx.x;
@@ -1801,6 +1820,8 @@ __global__ void k_update_mean(MeanArgs<T> a) {
         if (k == 1 && a.rotate_ubar) a.ubar[0] = a.ubar[1];
     }
 }
+template <typename T>
+__global__ void k_update_mean(MeanArgs<T> a) { k_update_mean_body<T>(a); }
 
 // ---------------------------------------------------------------------------
 // Domain-mean top wind tendency (PoissonSolver::pubarTop_pt,
@@ -1818,7 +1839,7 @@ struct PubarArgs {
 };
 
 template <typename T>
-__global__ void k_pubartop(PubarArgs<T> a) {
+__device__ __forceinline__ void k_pubartop_body(const PubarArgs<T>& a) {
     __shared__ double sh[32 * 3];
     const Dims& d = a.d;
     const int t = d.nz - 2, b = d.nz - 3, top = d.nz - 1;
@@ -1848,6 +1869,8 @@ __global__ void k_pubartop(PubarArgs<T> a) {
         a.ubar[1] = a.ubar[0] + 1.5 * a.c.dt * tend - 0.5 * a.c.dt * old;
     }
 }
+template <typename T>
+__global__ void k_pubartop(PubarArgs<T> a) { k_pubartop_body<T>(a); }
 
 // ---------------------------------------------------------------------------
 // cal_u (PoissonSolver.cpp:580-653): the top-row wind from the periodic chi
@@ -1872,7 +1895,7 @@ struct CalUArgs {
 constexpr int kCalUThreads = 1024;
 
 template <typename T>
-__global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) {
+__device__ __forceinline__ void k_cal_u_top_body(const CalUArgs<T>& a) {
     __shared__ double sh[32 * 1];
     __shared__ double scan[32];
     const Dims& d = a.d;
@@ -1947,6 +1970,8 @@ __global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) {
         }
     }
 }
+template <typename T>
+__global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) { k_cal_u_top_body<T>(a); }
 
 // Column integral u(i, k) = u(i, nz-2) + sum_{m=k}^{nz-3} (dw/dx - rhow zeta)(-dz)
 // from the top down (PoissonSolver.cpp:644-651), with the center halo of u.
@@ -1958,7 +1983,7 @@ __global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) {
 constexpr int kColSeg = 32;
 
 template <typename T>
-__global__ void __launch_bounds__(32 * kColSeg) k_cal_u_columns(CalUArgs<T> a) {
+__device__ __forceinline__ void k_cal_u_columns_body(const CalUArgs<T>& a) {
     __shared__ T tot[kColSeg][32];
     const Dims& d = a.d;
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
@@ -1988,5 +2013,7 @@ __global__ void __launch_bounds__(32 * kColSeg) k_cal_u_columns(CalUArgs<T> a) {
         store_center(a.u, d, i, k, area + utop);
     }
 }
+template <typename T>
+__global__ void __launch_bounds__(32 * kColSeg) k_cal_u_columns(CalUArgs<T> a) { k_cal_u_columns_body<T>(a); }
 
 }  // namespace vvm

@@ -23,6 +23,7 @@
 #include "spectral_kernels.cuh"
 #include "learned_kernels.cuh"
 #include "step_kernels.cuh"
+#include "grouped.cuh"
 
 using namespace vvm;
 
@@ -31,12 +32,13 @@ using namespace vvm;
 
 namespace vvm {
 
-__global__ void k_nvp_final(const double* partial, int nblocks, double* nvp) {
+__device__ __forceinline__ void k_nvp_final_body(const double* partial, int nblocks, double* nvp) {
     __shared__ double sh[32 * 6];
     nvp_finish(partial, nblocks, nvp, sh);
 }
+__global__ void k_nvp_final(const double* partial, int nblocks, double* nvp) { k_nvp_final_body(partial, nblocks, nvp); }
 
-__global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mode) {
+__device__ __forceinline__ void k_cg_scalar_body(const double* partial, int n, CGScalars* sc, int mode) {
     __shared__ double sh[32];
     double s[1] = {0};
     for (int b = threadIdx.x; b < n; b += blockDim.x) s[0] += partial[b];
@@ -60,8 +62,9 @@ __global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mod
         }
     }
 }
+__global__ void k_cg_scalar(const double* partial, int n, CGScalars* sc, int mode) { k_cg_scalar_body(partial, n, sc, mode); }
 
-__global__ void k_cg_scalar_it(const double* partial, int n, CGScalars* sc, const CGCtl* ctl) {
+__device__ __forceinline__ void k_cg_scalar_it_body(const double* partial, int n, CGScalars* sc, const CGCtl* ctl) {
     __shared__ double sh[32];
     double s[1] = {0};
     for (int b = threadIdx.x; b < n; b += blockDim.x) s[0] += partial[b];
@@ -73,6 +76,7 @@ __global__ void k_cg_scalar_it(const double* partial, int n, CGScalars* sc, cons
         sc->rz = v;
     }
 }
+__global__ void k_cg_scalar_it(const double* partial, int n, CGScalars* sc, const CGCtl* ctl) { k_cg_scalar_it_body(partial, n, sc, ctl); }
 
 __global__ void k_zero_if_b0(int NX, int NK, int pitch, const CGScalars* sc, double* W) {
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
@@ -80,7 +84,7 @@ __global__ void k_zero_if_b0(int NX, int NK, int pitch, const CGScalars* sc, dou
     if (ii < NX && kk < NK && sc->bb == 0.0) W[(size_t)kk * pitch + ii] = 0.0;
 }
 
-__global__ void k_loop_plain(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double tol2,
+__device__ __forceinline__ void k_loop_plain_body(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double tol2,
                              int maxit, int init, long long* exec, int body_kernels) {
     if (init) ctl->it = 0;
     else { ctl->it++; *exec += body_kernels; }
@@ -88,8 +92,11 @@ __global__ void k_loop_plain(const CGScalars* sc, CGCtl* ctl, cudaGraphCondition
     bool more = (bb > 0.0) && (rr > tol2 * bb) && (ctl->it < maxit) && isfinite(rr);
     ctl->total = ctl->it;
     ctl->relres = (bb > 0.0) ? sqrt(rr / bb) : 0.0;
-    cudaGraphSetConditional(h, more ? 1u : 0u);
+    ctl->more = more ? 1 : 0;
+    if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
 }
+__global__ void k_loop_plain(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double tol2,
+                             int maxit, int init, long long* exec, int body_kernels) { k_loop_plain_body(sc, ctl, h, tol2, maxit, init, exec, body_kernels); }
 
 __global__ void k_loop_inner(const CGScalars* sc, CGCtl* ctl, cudaGraphConditionalHandle h, double rtol2,
                              int maxit, int init, long long* exec, int body_kernels) {
@@ -127,7 +134,7 @@ __global__ void k_loop_outer(const CGScalars* sc64, CGCtl* ctl, const CGCtl* inn
 // is the row's residual weight: rhow_k on uniform levels, rhow_k / a_k on
 // stretched ones (a_k the centre spacing around face k over dx).
 template <typename T>
-__global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const double* rw, const T* zetap, double* f,
+__device__ __forceinline__ void k_poisson_rhs_body(const Dims& d, double dx, const double* rhow, const double* rw, const T* zetap, double* f,
                               int pitch_f, double* partial) {
     __shared__ double sh[32];
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
@@ -142,6 +149,9 @@ __global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const doubl
     block_sum(s, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
 }
+template <typename T>
+__global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const double* rw, const T* zetap, double* f,
+                              int pitch_f, double* partial) { k_poisson_rhs_body<T>(d, dx, rhow, rw, zetap, f, pitch_f, partial); }
 
 // Reference-ordered b vector ((k-2)*NX + (i-1)) to f = -b/rw_k, partial ||b||^2.
 __global__ void k_rhs_from_b(int NX, int NK, const double* rw, const double* b, double* f,
@@ -173,13 +183,15 @@ __global__ void k_unpack_solution(int NX, int NK, const double* in, double* x, i
 
 // w = W / rhow_k for k = 2..nz-2 (PoissonSolver.cpp:469-475), westdown halo.
 template <typename T>
-__global__ void k_w_from_W(Dims d, const double* rhow, const double* W, int pitch_f, T* w) {
+__device__ __forceinline__ void k_w_from_W_body(const Dims& d, const double* rhow, const double* W, int pitch_f, T* w) {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 2 + blockIdx.y * blockDim.y + threadIdx.y;
     if (i > d.nx - 2 || k > d.nz - 2) return;
     double v = W[(size_t)(k - 2) * pitch_f + (i - 1)] / rhow[k];
     store_westdown(w, d, i, k, T(v));
 }
+template <typename T>
+__global__ void k_w_from_W(Dims d, const double* rhow, const double* W, int pitch_f, T* w) { k_w_from_W_body<T>(d, rhow, W, pitch_f, w); }
 
 // The streamfunction formulation (PoissonSolver::calpsiuw, STREAMFUNCTION,
 // src/PoissonSolver.cpp:124-177). Its matrix (src/PoissonSolver.cpp:726-756,
@@ -357,10 +369,13 @@ constexpr int kMaxOddCoarse = 256;
 // and the reduced-system bands, next to 32 KB of static tiles within 227 KB).
 constexpr int kModeSmemMax = 192 * 1024;
 
+struct Recorder;
+
 // Launch counter and, when enabled, per-kernel-class device time from CUDA
 // events recorded around each launch on the launching stream.
 struct Stats {
     bool on = false;
+    Recorder* rec = nullptr;   // set while a step is recorded for a grouped launch (no work issued)
     long long launches = 0;
     double ms[VVM_K_COUNT] = {};
     long long cnt[VVM_K_COUNT] = {};
@@ -410,6 +425,8 @@ struct Timed {
     cudaEvent_t a = nullptr;
     Timed(Stats* s_, int id_, cudaStream_t st_) : s(s_), id(id_), st(st_) {
         if (!s) return;
+        // a recording issues no work: a launch here has no grouped form
+        if (s->rec) throw CudaError{"grouped launch: a kernel of the step has no grouped form"};
         s->launches++;
         if (s->on) {
             a = s->ev();
@@ -430,6 +447,90 @@ struct Timed {
         Timed t_((S), (ID), (ST));  \
         __VA_ARGS__;                \
     } while (0)
+
+// ---------------------------------------------------------------- recording
+//
+// A batch steps the cases of one shape as grouped launches (grouped.cuh).
+// To build them, each case's step is first recorded instead of issued: the
+// kernels with their launch shapes and argument packs, the clears of small
+// control blocks, and the graph loops with the points where a case decides
+// whether its loop goes on (its flag, an int in device memory). The batch
+// then checks that the recordings of a group agree op for op and replays
+// them side by side.
+struct RecOp {
+    enum Kind { KERNEL, ZERO, COND_NEXT, COND_LOOP, LOOP_BEGIN, LOOP_END } kind = KERNEL;
+    const void* fn = nullptr;           // KERNEL: the grouped kernel
+    dim3 grid, block;
+    size_t smem = 0;
+    std::vector<unsigned char> pack;    // KERNEL: this case's arguments
+    size_t align = 16;
+    void* ptr = nullptr;                // ZERO: what to clear; COND_*: the case's loop flag (int)
+    size_t bytes = 0;                   // ZERO
+};
+struct Recorder {
+    std::vector<RecOp> ops;
+};
+
+template <typename X>
+struct same_t {
+    using type = X;
+};
+
+inline void record_kernel(Stats* s, const void* fn, dim3 g, dim3 b, size_t smem, const void* pack, size_t size,
+                          size_t align) {
+    RecOp op;
+    op.kind = RecOp::KERNEL;
+    op.fn = fn;
+    op.grid = g;
+    op.block = b;
+    op.smem = smem;
+    op.pack.assign(static_cast<const unsigned char*>(pack), static_cast<const unsigned char*>(pack) + size);
+    op.align = align;
+    s->rec->ops.push_back(std::move(op));
+}
+
+// Launches kernel k (body Body) on st, or records it when a step is being
+// recorded. MAXT and MINB: the launch bounds of its grouped form, the
+// largest block it is launched with and the blocks a SM its own
+// __launch_bounds__ asks for.
+template <auto Body, int MAXT, int MINB = 1, typename... A>
+void klaunch(Stats* s, int id, cudaStream_t st, void (*k)(A...), dim3 g, dim3 b, size_t smem,
+             typename same_t<A>::type... args) {
+    if (s && s->rec) {
+        if ((int)(b.x * b.y * b.z) > MAXT) throw CudaError{"grouped launch: block larger than its launch bounds"};
+        const KPack<A...> p = kpack<A...>(args...);
+        record_kernel(s, reinterpret_cast<const void*>(&k_grouped<Body, MAXT, MINB, A...>), g, b, smem, &p,
+                      sizeof(p), alignof(KPack<A...>));
+        return;
+    }
+    LAUNCH(s, id, st, k<<<g, b, smem, st>>>(args...));
+    CKL();
+}
+
+// cudaMemsetAsync(p, 0, bytes, st), or its record.
+inline void zero_async(Stats* s, void* p, size_t bytes, cudaStream_t st) {
+    if (s && s->rec) {
+        RecOp op;
+        op.kind = RecOp::ZERO;
+        op.ptr = p;
+        op.bytes = bytes;
+        s->rec->ops.push_back(std::move(op));
+        return;
+    }
+    CK(cudaMemsetAsync(p, 0, bytes, st));
+}
+
+// Marks where a case has decided whether a graph loop runs (another) pass:
+// its flag `more` (next: the loop that opens next; else the innermost open
+// loop). Only recordings keep it: a case's own graph sets its conditions in
+// the deciding kernels.
+inline void record_cond(Stats* s, int* more, bool next) {
+    if (!(s && s->rec)) return;
+    RecOp op;
+    op.kind = next ? RecOp::COND_NEXT : RecOp::COND_LOOP;
+    op.ptr = more;
+    s->rec->ops.push_back(std::move(op));
+}
 
 struct HostLine {   // host copy of one level's line factors
     std::vector<double> lo, inv, cp, gL, gR;
@@ -769,12 +870,12 @@ struct Spectral {
     // dst = S^{-1} r (to round-off).
     void apply_to(const P* r, P* dst, cudaStream_t st) {
         const int rows2 = cdiv(a.NK, 2);
-        LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_forward<P><<<rows2, threads, smem, st>>>(a, r));
-        CKL();
-        LAUNCH(stats, VVM_K_MG_COARSE, st, k_spec_modes_seg<P><<<cdiv(a.NX / 2 + 1, 32), 64 * kModeSegs, 0, st>>>(a));
-        CKL();
-        LAUNCH(stats, VVM_K_MG_SWEEP, st, k_spec_inverse<P><<<rows2, threads, smem, st>>>(a, dst));
-        CKL();
+        klaunch<k_spec_forward_body<P>, 1024>(stats, VVM_K_MG_SWEEP, st, k_spec_forward<P>, dim3(rows2), dim3(threads),
+                                              smem, a, r);
+        klaunch<k_spec_modes_seg_body<P>, 64 * kModeSegs>(stats, VVM_K_MG_COARSE, st, k_spec_modes_seg<P>,
+                                                          dim3(cdiv(a.NX / 2 + 1, 32)), dim3(64 * kModeSegs), 0, a);
+        klaunch<k_spec_inverse_body<P>, 1024>(stats, VVM_K_MG_SWEEP, st, k_spec_inverse<P>, dim3(rows2), dim3(threads),
+                                              smem, a, dst);
     }
     // z = S^{-1} r; returns the buffer holding z.
     P* apply(const P* r, cudaStream_t st) {
@@ -1410,20 +1511,18 @@ struct PCG {
         VecArgs<P> v = vargs();
         dim3 B = block(), G = grid();
         P* z = precond(r, st);
-        LAUNCH(stats, VVM_K_CG, st, k_cg_dot<P><<<G, B, 0, st>>>(v, r, z, partial));
-        CKL();
-        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar_it<<<1, 1024, 0, st>>>(partial, npart, sc, ctl));
-        CKL();
-        LAUNCH(stats, VVM_K_CG, st, k_cg_dir_it<P><<<G, B, 0, st>>>(v, sc, ctl, z, p));
-        CKL();
-        LAUNCH(stats, VVM_K_CG, st, k_cg_spmv<P><<<G, B, 0, st>>>(v, p, q, partial));
-        CKL();
-        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_PQ_ALPHA));
-        CKL();
-        LAUNCH(stats, VVM_K_CG, st, k_cg_update<P><<<G, B, 0, st>>>(v, sc, x, r, p, q, partial));
-        CKL();
-        LAUNCH(stats, VVM_K_CG, st, k_cg_scalar<<<1, 1024, 0, st>>>(partial, npart, sc, CG_SET_RR));
-        CKL();
+        klaunch<k_cg_dot_body<P>, 256>(stats, VVM_K_CG, st, k_cg_dot<P>, G, B, 0, v, (const P*)r, (const P*)z, partial);
+        klaunch<k_cg_scalar_it_body, 1024>(stats, VVM_K_CG, st, k_cg_scalar_it, dim3(1), dim3(1024), 0,
+                                           (const double*)partial, npart, sc, (const CGCtl*)ctl);
+        klaunch<k_cg_dir_it_body<P>, 256>(stats, VVM_K_CG, st, k_cg_dir_it<P>, G, B, 0, v, (const CGScalars*)sc,
+                                          (const CGCtl*)ctl, (const P*)z, p);
+        klaunch<k_cg_spmv_body<P>, 256>(stats, VVM_K_CG, st, k_cg_spmv<P>, G, B, 0, v, (const P*)p, q, partial);
+        klaunch<k_cg_scalar_body, 1024>(stats, VVM_K_CG, st, k_cg_scalar, dim3(1), dim3(1024), 0,
+                                        (const double*)partial, npart, sc, (int)CG_PQ_ALPHA);
+        klaunch<k_cg_update_body<P>, 256>(stats, VVM_K_CG, st, k_cg_update<P>, G, B, 0, v, (const CGScalars*)sc, x, r,
+                                          (const P*)p, (const P*)q, partial);
+        klaunch<k_cg_scalar_body, 1024>(stats, VVM_K_CG, st, k_cg_scalar, dim3(1), dim3(1024), 0,
+                                        (const double*)partial, npart, sc, (int)CG_SET_RR);
         return (int)(stats->launches - n0);
     }
 
@@ -1528,6 +1627,7 @@ struct vvm_gpu_ctx {
     int learned_iters = 0, learned_fallback = 0;
     bool learned_collect = false;   // training-pair collection: solve with the plain solver
     int tune_fft = 0;        // threads of a row-FFT block (0: automatic)
+    int tune_group = 0;      // in a batch: cases a grouped launch takes at most (0: the batch's limit)
     Arena ar;
     Fields<double> f64;
     Fields<float> f32;
@@ -1704,8 +1804,7 @@ void launch_pzeta(vvm_gpu_ctx* c) {
                    F.zeta[fut], F.hist[H_ZETA][ab.sn], F.hist[H_ZETA][ab.so], F.hist[H_BUOY][ab.sn],
                    F.hist[H_BUOY][ab.so], ab};
     dim3 g(cdiv(c->d.nx - 2, kPZBX), cdiv(c->d.nz - 3, kPZBZ));
-    LAUNCH(&c->stats, VVM_K_PZETA, c->stream, k_pzeta<T><<<g, dim3(kPZBX, kPZBZ), 0, c->stream>>>(a));
-    CKL();
+    klaunch<k_pzeta_body<T>, kPZBX * kPZBZ>(&c->stats, VVM_K_PZETA, c->stream, k_pzeta<T>, g, dim3(kPZBX, kPZBZ), 0, a);
 }
 
 template <typename T>
@@ -1742,13 +1841,20 @@ void launch_padv(vvm_gpu_ctx* c, int mask, int nvp_mask, bool vt, bool precip) {
     CUtensorMap m[4];
     for (int f = 0; f < 4; f++)
         m[f] = field_map(a.now[f], c->d.nx, c->d.nz, c->d.pitch, (int)sizeof(T), kPAdvVX, kPAdvVZ);
-    LAUNCH(&c->stats, VVM_K_PADV, c->stream,
-           k_padv<T><<<g, c->padv_blk(), sizeof(PAdvShared<T>), c->stream>>>(m[0], m[1], m[2], m[3], a));
-    CKL();
-    if (nvp_mask) {
-        LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp));
+    if (c->stats.rec) {
+        PAdvPack<T> p;
+        for (int f = 0; f < 4; f++) p.m[f] = m[f];
+        p.a = a;
+        record_kernel(&c->stats, reinterpret_cast<const void*>(&k_padv_grouped<T>), g, c->padv_blk(),
+                      sizeof(PAdvShared<T>), &p, sizeof(p), alignof(PAdvPack<T>));
+    } else {
+        LAUNCH(&c->stats, VVM_K_PADV, c->stream,
+               k_padv<T><<<g, c->padv_blk(), sizeof(PAdvShared<T>), c->stream>>>(m[0], m[1], m[2], m[3], a));
         CKL();
     }
+    if (nvp_mask)
+        klaunch<k_nvp_final_body, 1024>(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final, dim3(1), dim3(1024), 0,
+                                        (const double*)c->partial, (int)(g.x * g.y), c->nvp);
 }
 
 template <typename T>
@@ -1771,8 +1877,7 @@ void launch_apply(vvm_gpu_ctx* c, int mask, int nvp_mask, bool forcing, bool hal
     // status_for_adding_forcing (Iteration.cpp:276-277)
     a.forcing_th = forcing && c->has_forcing_th && (c->step * c->desc.dt <= c->desc.addforcingtime);
     a.halo = halo;
-    LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_apply<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(a));
-    CKL();
+    klaunch<k_apply_body<T>, 256>(&c->stats, VVM_K_APPLY, c->stream, k_apply<T>, c->grid_interior(1), c->blk(), 0, a);
 }
 
 template <typename T>
@@ -1788,8 +1893,7 @@ template <typename T>
 void launch_pubartop(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     PubarArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.RKM, c->ubar, c->dubar, AB2::of(c->step)};
-    LAUNCH(&c->stats, VVM_K_PUBAR, c->stream, k_pubartop<T><<<1, 1024, 0, c->stream>>>(a));
-    CKL();
+    klaunch<k_pubartop_body<T>, 1024>(&c->stats, VVM_K_PUBAR, c->stream, k_pubartop<T>, dim3(1), dim3(1024), 0, a);
 }
 
 // finish_advection: the step's own sequence, where the finish of the
@@ -1811,10 +1915,9 @@ void launch_kessler(vvm_gpu_ctx* c, bool halo, bool finish_advection = false) {
         a.pre.forcing_th = c->has_forcing_th && (c->step * c->desc.dt <= c->desc.addforcingtime);
     }
     dim3 g = c->grid_interior(1);
-    LAUNCH(&c->stats, VVM_K_KESSLER, c->stream, k_kessler<T><<<g, c->blk(), 0, c->stream>>>(a));
-    CKL();
-    LAUNCH(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final<<<1, 1024, 0, c->stream>>>(c->partial, g.x * g.y, c->nvp));
-    CKL();
+    klaunch<k_kessler_body<T>, 256>(&c->stats, VVM_K_KESSLER, c->stream, k_kessler<T>, g, c->blk(), 0, a);
+    klaunch<k_nvp_final_body, 1024>(&c->stats, VVM_K_APPLY, c->stream, k_nvp_final, dim3(1), dim3(1024), 0,
+                                    (const double*)c->partial, (int)(g.x * g.y), c->nvp);
     launch_apply<T>(c, halo ? (F_TH | F_QV | F_QC | F_QR) : (F_QV | F_QC | F_QR), F_QV | F_QC | F_QR, false, halo);
 }
 
@@ -1825,6 +1928,23 @@ cudaGraphConditionalHandle new_handle(cudaStream_t st) {
     cudaGraphConditionalHandle h;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
     return h;
+}
+
+// A handle for a WHILE node of the graph being captured on st whose value
+// resets to 0 at each launch of the graph; 0 while a step is recorded (the
+// recorded kernels then set no condition: the group's own kernel does).
+cudaGraphConditionalHandle new_handle_reset(Stats* s, cudaStream_t st) {
+    if (s && s->rec) return 0;
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g;
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &g, nullptr, nullptr));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    return h;
+}
+cudaGraphConditionalHandle new_handle(Stats* s, cudaStream_t st) {
+    if (s && s->rec) return 0;
+    return new_handle(st);
 }
 
 // Appends a WHILE node (condition h) to the graph being captured on st and
@@ -1846,12 +1966,31 @@ cudaGraph_t add_while(cudaStream_t st, cudaGraphConditionalHandle h) {
     return p.conditional.phGraph_out[0];
 }
 
+// add_while, or the start of a loop in a recording (no body graph).
+cudaGraph_t add_while(Stats* s, cudaStream_t st, cudaGraphConditionalHandle h) {
+    if (s && s->rec) {
+        RecOp op;
+        op.kind = RecOp::LOOP_BEGIN;
+        s->rec->ops.push_back(std::move(op));
+        return nullptr;
+    }
+    return add_while(st, h);
+}
+
 struct BodyCapture {   // stream capture into a conditional node's body graph
     cudaStream_t s;
-    BodyCapture(cudaStream_t s_, cudaGraph_t body) : s(s_) {
+    Stats* stats = nullptr;   // recording: the loop's end is marked instead
+    BodyCapture(cudaStream_t s_, cudaGraph_t body, Stats* st = nullptr) : s(s_), stats(st) {
+        if (stats && stats->rec) return;
         CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     }
     void end() {
+        if (stats && stats->rec) {
+            RecOp op;
+            op.kind = RecOp::LOOP_END;
+            stats->rec->ops.push_back(std::move(op));
+            return;
+        }
         cudaGraph_t g;
         CK(cudaStreamEndCapture(s, &g));
     }
@@ -1958,8 +2097,7 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops 
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     RKArgs<T> r{c->d, c->c, c->profiles(), F.u, F.w, F.th[fut], F.RKM, F.RKH};
-    LAUNCH(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T><<<c->grid_interior(1), c->blk(), 0, c->stream>>>(r));
-    CKL();
+    klaunch<k_rkm_rkh_body<T>, 256>(&c->stats, VVM_K_RKM, c->stream, k_rkm_rkh<T>, c->grid_interior(1), c->blk(), 0, r);
     GSArgs<T> g{c->d, c->c, c->profiles(), {F.zeta[fut], F.th[fut], F.qv[fut], F.qc[fut], F.qr[fut]},
                 F.RKM, F.RKH, 0x1f, nudge ? 1 : 0, F.gsA, nullptr, nullptr, nullptr};
     if (c->tune_gs_tr == kGSSchedCluster) {
@@ -1973,30 +2111,27 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops 
     const int tblocks = cdiv(5 * nb * nc, 4);
     const int maxp = std::max(2, nb + nc - 1);
     cudaStream_t st = c->stream;
-    CK(cudaMemsetAsync(c->gsctl, 0, sizeof(GSTileCtl), st));   // a fresh sweep
-    LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T, true><<<tblocks, 128, 0, st>>>(g, t, 0));   // pass 1
-    CKL();
+    zero_async(&c->stats, c->gsctl, sizeof(GSTileCtl), st);   // a fresh sweep
+    klaunch<k_gs_tiles_body<T, true>, 128, 4>(&c->stats, VVM_K_GS, st, k_gs_tiles<T, true>, dim3(tblocks), dim3(128), 0,
+                                              g, t, (cudaGraphConditionalHandle)0);   // pass 1
     if (recorded_in_loops) {
         // graph capture: the typical passes 2..kGSGraphPasses+1 unconditionally
         // (each returns at once if the sweep already converged, and the last
         // block of each sets the condition below), then a WHILE node that runs
         // further passes only when they are needed
-        cudaStreamCaptureStatus status;
-        cudaGraph_t cg;
-        CK(cudaStreamGetCaptureInfo(st, &status, nullptr, &cg, nullptr, nullptr));
-        cudaGraphConditionalHandle h;
-        CK(cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault));
+        const cudaGraphConditionalHandle h = new_handle_reset(&c->stats, st);
         GSTileArgs<T> tu = t;
         tu.exec = nullptr;   // counted with the graph's static kernels
-        for (int p = 0; p < kGSGraphPasses; p++) {
-            LAUNCH(&c->stats, VVM_K_GS, st, k_gs_tiles<T, false><<<tblocks, 128, 0, st>>>(g, tu, h));
-            CKL();
-        }
-        cudaGraph_t body = add_while(st, h);
-        BodyCapture bc(c->cap[0], body);
+        for (int p = 0; p < kGSGraphPasses; p++)
+            klaunch<k_gs_tiles_body<T, false>, 128, 4>(&c->stats, VVM_K_GS, st, k_gs_tiles<T, false>, dim3(tblocks),
+                                                       dim3(128), 0, g, tu, h);
+        record_cond(&c->stats, &c->gsctl->more, true);
+        cudaGraph_t body = add_while(&c->stats, st, h);
+        BodyCapture bc(c->cap[0], body, &c->stats);
         const long long n0 = c->stats.launches;
-        LAUNCH(&c->stats, VVM_K_GS, bc.s, k_gs_tiles<T, false><<<tblocks, 128, 0, bc.s>>>(g, t, h));
-        CKL();
+        klaunch<k_gs_tiles_body<T, false>, 128, 4>(&c->stats, VVM_K_GS, bc.s, k_gs_tiles<T, false>, dim3(tblocks),
+                                                   dim3(128), 0, g, t, h);
+        record_cond(&c->stats, &c->gsctl->more, false);
         bc.end();
         *recorded_in_loops += c->stats.launches - n0;
         return;
@@ -2017,7 +2152,7 @@ void launch_nudge(vvm_gpu_ctx* c, bool th_zeta, bool qv) {
     NudgeArgs<T> a{c->d, c->c, c->profiles(), F.th[fut], F.zeta[fut], F.qv[fut], F.qv[now],
                    th_zeta ? 1 : 0, (th_zeta && c->desc.case_id != 2) ? 1 : 0,
                    qv ? c->desc.moisture_nudge_time : 0.0};
-    LAUNCH(&c->stats, VVM_K_MEAN, c->stream, k_nudge<T><<<c->grid_all(), c->blk(), 0, c->stream>>>(a));
+    klaunch<k_nudge_body<T>, 256>(&c->stats, VVM_K_MEAN, c->stream, k_nudge<T>, c->grid_all(), c->blk(), 0, a);
     CKL();
 }
 
@@ -2027,8 +2162,8 @@ void launch_update_mean(vvm_gpu_ctx* c, bool rotate) {
     int fut = 1 - c->cur;
     MeanArgs<T> a{c->d, c->offset_th(), c->offset_qv(), F.th[fut], F.qv[fut], c->thb, c->qvb, c->thvb,
                   c->ubar, rotate ? 1 : 0};
-    LAUNCH(&c->stats, VVM_K_MEAN, c->stream, k_update_mean<T><<<c->d.nz - 2, 256, 0, c->stream>>>(a));
-    CKL();
+    klaunch<k_update_mean_body<T>, 256>(&c->stats, VVM_K_MEAN, c->stream, k_update_mean<T>, dim3(c->d.nz - 2),
+                                        dim3(256), 0, a);
 }
 
 // ---------------------------------------------------------------- Poisson
@@ -2364,17 +2499,18 @@ long long record_solve(vvm_gpu_ctx* c, double tol, int maxit, bool warm) {
     if (c->spectral) P64.sp.apply_to(c->Wf, c->W, st);   // direct solve; the loop below checks it
     else if (!warm && !learned) CK(cudaMemsetAsync(c->W, 0, (size_t)P64.NK * P64.pitch * sizeof(double), st));
     if (!c->mixed || c->spectral || learned) {
-        cudaGraphConditionalHandle h = new_handle(st);
-        LAUNCH(&c->stats, VVM_K_CG, st,
-               k_cg_check<double><<<G, B, 0, st>>>(v, c->Wf, c->W, P64.r, P64.partial, P64.sc, P64.ctl, P64.arrive, h,
-                                                    tol * tol, maxit));
-        CKL();
-        cudaGraph_t body = add_while(st, h);
-        BodyCapture bc(c->cap[0], body);
+        cudaGraphConditionalHandle h = new_handle(&c->stats, st);
+        klaunch<k_cg_check_body<double>, 256>(&c->stats, VVM_K_CG, st, k_cg_check<double>, G, B, 0, v,
+                                              (const double*)c->Wf, c->W, P64.r, P64.partial, P64.sc, P64.ctl,
+                                              P64.arrive, h, tol * tol, maxit);
+        record_cond(&c->stats, &P64.ctl->more, true);
+        cudaGraph_t body = add_while(&c->stats, st, h);
+        BodyCapture bc(c->cap[0], body, &c->stats);
         const long long n0 = c->stats.launches;
         int nb = P64.record_iteration(c->W, bc.s);
-        LAUNCH(&c->stats, VVM_K_CG, bc.s, k_loop_plain<<<1, 1, 0, bc.s>>>(P64.sc, P64.ctl, h, tol * tol, maxit, 0, c->d_exec, nb + 1));
-        CKL();
+        klaunch<k_loop_plain_body, 32>(&c->stats, VVM_K_CG, bc.s, k_loop_plain, dim3(1), dim3(1), 0,
+                                       (const CGScalars*)P64.sc, P64.ctl, h, tol * tol, maxit, 0, c->d_exec, nb + 1);
+        record_cond(&c->stats, &P64.ctl->more, false);
         bc.end();
         in_bodies += c->stats.launches - n0;
         return in_bodies;
@@ -2442,10 +2578,11 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr, cudaEve
     int NX = c->d.nx - 2, NK = c->d.nz - 3;
     int pitch = c->pcg64->pitch;
     dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
-    LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_poisson_rhs<T><<<G, B, 0, c->stream>>>(c->d, c->c.dx, c->rhow, c->rwres, F.zeta[fut], c->Wf, pitch, c->wpartial));
-    CKL();
-    LAUNCH(&c->stats, VVM_K_CG, c->stream, k_cg_scalar<<<1, 1024, 0, c->stream>>>(c->wpartial, c->wnpart, c->pcg64->sc, CG_SET_BB));
-    CKL();
+    klaunch<k_poisson_rhs_body<T>, 256>(&c->stats, VVM_K_POISSON_RHS, c->stream, k_poisson_rhs<T>, G, B, 0, c->d,
+                                        c->c.dx, (const double*)c->rhow, (const double*)c->rwres,
+                                        (const T*)F.zeta[fut], c->Wf, pitch, c->wpartial);
+    klaunch<k_cg_scalar_body, 1024>(&c->stats, VVM_K_CG, c->stream, k_cg_scalar, dim3(1), dim3(1024), 0,
+                                    (const double*)c->wpartial, c->wnpart, c->pcg64->sc, (int)CG_SET_BB);
     const bool warm = c->desc.warm_start != 0;
     const int maxit = c->desc.poisson_maxit > 0 ? c->desc.poisson_maxit : 200;
     if (recorded_in_loops) {   // graph capture: the loops run on the device
@@ -2456,8 +2593,8 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr, cudaEve
         *recorded_in_loops = record_solve(c, c->desc.poisson_tol, maxit, warm);
         c->nsolves++;
         if (before_w) CK(cudaStreamWaitEvent(c->stream, before_w, 0));
-        LAUNCH(&c->stats, VVM_K_POISSON_RHS, c->stream, k_w_from_W<T><<<c->grid_interior(2), c->blk(), 0, c->stream>>>(c->d, c->rhow, c->W, pitch, F.w));
-        CKL();
+        klaunch<k_w_from_W_body<T>, 256>(&c->stats, VVM_K_POISSON_RHS, c->stream, k_w_from_W<T>, c->grid_interior(2),
+                                         c->blk(), 0, c->d, (const double*)c->rhow, (const double*)c->W, pitch, F.w);
         return VVM_GPU_OK;
     }
     CK(cudaMemcpyAsync(c->sc_host, &c->pcg64->sc->bb, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -2487,10 +2624,10 @@ void launch_cal_u(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     CalUArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.zeta[fut], c->ubar};
-    LAUNCH(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_top<T><<<1, kCalUThreads, 0, c->stream>>>(a));
-    CKL();
-    LAUNCH(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_columns<T><<<cdiv(c->d.nx - 2, 32), 32 * kColSeg, 0, c->stream>>>(a));
-    CKL();
+    klaunch<k_cal_u_top_body<T>, kCalUThreads>(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_top<T>, dim3(1),
+                                               dim3(kCalUThreads), 0, a);
+    klaunch<k_cal_u_columns_body<T>, 32 * kColSeg>(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_columns<T>,
+                                                   dim3(cdiv(c->d.nx - 2, 32)), dim3(32 * kColSeg), 0, a);
 }
 
 // The psi system's solver: the w-equation's operator on uniform levels with
@@ -2792,6 +2929,18 @@ bool graph_ready(vvm_gpu_ctx* c) {
 
 // ---------------------------------------------------------------- batches
 
+// Cases a grouped launch takes at most, unless the autotuner chose otherwise:
+// larger groups of a shape are split into parallel sub-groups.
+constexpr int kGroupMaxDefault = 32;
+// Grids of more cells step case by case unless the autotuner chose grouped
+// launches for them. Measured on a B200 (mixed step, spectral cal_w), ms a
+// step grouped / case by case: 256 cases of 256 x 64 2.0 / 10.4, 64 of
+// 512 x 96 1.40 / 1.83, 64 of 1024 x 96 2.6 / 2.38, 48 of 2048 x 128 4.8 / 3.9.
+// A small case's step is launch-bound, so one launch for many cases wins; a
+// large case fills the GPU itself, and independent chains of kernels (one a
+// case) then overlap their phases, which a group's lock-step launches cannot.
+constexpr long long kGroupCellsMax = 65536;
+
 // Independent cases of any sizes that advance together: one CUDA graph per
 // step holds every case's step as a parallel branch (captured by forking the
 // batch stream to each case's stream and joining back), keyed like a case's
@@ -2804,15 +2953,21 @@ struct vvm_gpu_batch {
     std::vector<cudaEvent_t> joins;
     cudaGraphExec_t gexec[2][2] = {};
     std::vector<long long> gstatic[2][2];   // kernels outside loops, per case
+    std::vector<void*> gbufs[2][2];         // device arrays of the grouped launches of gexec
+    int group_max = kGroupMaxDefault;       // cases a grouped launch takes at most (0: no grouping)
+    int last_groups = 0;                    // grouped groups of the last capture
     std::string err;
 
     void drop_graphs() {
-        for (auto& row : gexec)
-            for (auto& g : row)
-                if (g) {
-                    cudaGraphExecDestroy(g);
-                    g = nullptr;
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++) {
+                if (gexec[i][j]) {
+                    cudaGraphExecDestroy(gexec[i][j]);
+                    gexec[i][j] = nullptr;
                 }
+                for (void* q : gbufs[i][j]) cudaFree(q);
+                gbufs[i][j].clear();
+            }
     }
     ~vvm_gpu_batch() {
         drop_graphs();
@@ -2832,9 +2987,190 @@ int batch_fail(vvm_gpu_batch* b, int code, const std::string& msg) {
     return code;
 }
 
+// ------------------------------------------------------- grouped launches
+//
+// Cases of one grid shape, precision and tuning whose step runs the exact
+// Fourier-mode cal_w and the tiled Gauss-Seidel passes step as grouped
+// launches (grouped.cuh): each case's step is recorded, the recordings are
+// checked to agree op for op (kernel, launch shape, pack size, loop
+// structure), and then replayed side by side, one launch a kernel for the
+// whole group, blockIdx.z the case. Groups whose recordings differ step case
+// by case.
+
+bool groupable(const vvm_gpu_ctx* c) {
+    return c->spectral && c->desc.solver != VVM_SOLVER_LEARNED && c->tune_gs_tr != kGSSchedCluster &&
+           !(c->desc.flags & VVM_FLAG_STREAMFUNCTION) && !c->stats.on;
+}
+
+// Records case c's next step into r without issuing work; false when some
+// launch of it has no grouped form. The case's host-side step state is put
+// back.
+bool record_step(vvm_gpu_ctx* c, Recorder& r) {
+    const int step = c->step, cur = c->cur, ns = c->nsolves;
+    const long long l0 = c->stats.launches;
+    c->stats.rec = &r;
+    c->branches = false;
+    bool ok = true;
+    long long in_loops = 0;
+    try {
+        if (c->mixed) run_step<float>(c, &in_loops);
+        else run_step<double>(c, &in_loops);
+    } catch (const CudaError&) {
+        ok = false;
+    }
+    c->stats.rec = nullptr;
+    c->branches = true;
+    c->step = step;
+    c->cur = cur;
+    c->nsolves = ns;
+    c->stats.launches = l0;
+    return ok;
+}
+
+// The most cases a grouped launch of c's shape takes (< 2: none).
+int group_limit(const vvm_gpu_batch* b, const vvm_gpu_ctx* c) {
+    if (b->group_max < 2) return 0;
+    if (c->tune_group > 0) return std::min(c->tune_group, b->group_max);
+    return (long long)(c->d.nx - 2) * (c->d.nz - 2) <= kGroupCellsMax ? b->group_max : 1;
+}
+
+bool same_ops(const Recorder& a, const Recorder& b) {
+    if (a.ops.size() != b.ops.size()) return false;
+    for (size_t j = 0; j < a.ops.size(); j++) {
+        const RecOp &x = a.ops[j], &y = b.ops[j];
+        if (x.kind != y.kind) return false;
+        if (x.kind == RecOp::KERNEL &&
+            (x.fn != y.fn || x.grid.x != y.grid.x || x.grid.y != y.grid.y || x.grid.z != 1 || y.grid.z != 1 ||
+             x.block.x != y.block.x || x.block.y != y.block.y || x.block.z != y.block.z || x.smem != y.smem ||
+             x.pack.size() != y.pack.size()))
+            return false;
+        if (x.kind == RecOp::ZERO && x.bytes != y.bytes) return false;
+    }
+    return true;
+}
+
+// The device arrays of one group's replay: per kernel op the n argument
+// packs, per clear the n targets, per condition point the n flags.
+struct GroupArrays {
+    std::vector<size_t> off;   // per op: offset of its array in the blob
+    std::vector<unsigned char> host;
+    void* dev = nullptr;
+};
+
+GroupArrays group_arrays(const std::vector<Recorder>& recs) {
+    const size_t n = recs.size(), nops = recs[0].ops.size();
+    GroupArrays A;
+    A.off.assign(nops, 0);
+    size_t at = 0;
+    auto place = [&](size_t bytes) {
+        at = (at + 255) / 256 * 256;
+        const size_t o = at;
+        at += bytes;
+        return o;
+    };
+    std::vector<size_t> stride(nops, 0);
+    for (size_t j = 0; j < nops; j++) {
+        const RecOp& op = recs[0].ops[j];
+        if (op.kind == RecOp::KERNEL) {
+            stride[j] = op.pack.size();   // sizeof the pack: the kernel indexes packs[blockIdx.z]
+            A.off[j] = place(stride[j] * n);
+        } else if (op.kind == RecOp::ZERO || op.kind == RecOp::COND_NEXT || op.kind == RecOp::COND_LOOP) {
+            A.off[j] = place(sizeof(void*) * n);
+        }
+    }
+    A.host.assign(std::max<size_t>(at, 1), 0);
+    for (size_t j = 0; j < nops; j++) {
+        const RecOp::Kind k = recs[0].ops[j].kind;
+        for (size_t i = 0; i < n; i++) {
+            const RecOp& op = recs[i].ops[j];
+            if (k == RecOp::KERNEL) memcpy(&A.host[A.off[j] + i * stride[j]], op.pack.data(), op.pack.size());
+            else if (k == RecOp::ZERO || k == RecOp::COND_NEXT || k == RecOp::COND_LOOP)
+                memcpy(&A.host[A.off[j] + i * sizeof(void*)], &op.ptr, sizeof(void*));
+        }
+    }
+    CK(cudaMalloc(&A.dev, A.host.size()));
+    upload_now(A.dev, A.host.data(), A.host.size());
+    for (size_t j = 0; j < nops; j++) {   // kernels needing more than 48 KB of dynamic shared memory
+        const RecOp& op = recs[0].ops[j];
+        if (op.kind == RecOp::KERNEL && op.smem > 48 * 1024)
+            CK(cudaFuncSetAttribute(op.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)op.smem));
+    }
+    return A;
+}
+
+// Issues the group's step on st (under capture): one launch a kernel op,
+// blockIdx.z the case; loops as WHILE nodes whose condition a one-block
+// kernel sets from the cases' flags. Loop bodies are captured on cap[depth].
+// Returns the kernels issued outside loops.
+long long group_replay(const std::vector<Recorder>& recs, const GroupArrays& A, cudaStream_t st,
+                       const cudaStream_t* cap, int ncap) {
+    const int n = (int)recs.size();
+    const std::vector<RecOp>& ops = recs[0].ops;
+    char* base = static_cast<char*>(A.dev);
+    struct Loop {
+        cudaGraphConditionalHandle h;
+        void* flags;
+        std::unique_ptr<BodyCapture> bc;
+    };
+    std::vector<Loop> open;
+    cudaGraphConditionalHandle next_h = 0;
+    void* next_flags = nullptr;
+    long long outside = 0;
+    auto cur = [&]() { return open.empty() ? st : open.back().bc->s; };
+    for (size_t j = 0; j < ops.size(); j++) {
+        const RecOp& op = ops[j];
+        void* arr = base + A.off[j];
+        switch (op.kind) {
+        case RecOp::KERNEL: {
+            void* gate = open.empty() ? nullptr : open.back().flags;
+            void* args[2] = {&arr, &gate};
+            CK(cudaLaunchKernel(op.fn, dim3(op.grid.x, op.grid.y, n), op.block, args, op.smem, cur()));
+            if (open.empty()) outside++;
+            break;
+        }
+        case RecOp::ZERO:
+            k_group_zero<<<dim3(1, 1, n), 128, 0, cur()>>>(reinterpret_cast<unsigned char* const*>(arr), op.bytes);
+            CKL();
+            if (open.empty()) outside++;
+            break;
+        case RecOp::COND_NEXT:
+            next_h = new_handle(cur());
+            next_flags = arr;
+            k_group_cond<<<1, 256, 0, cur()>>>(reinterpret_cast<const int* const*>(arr), n, next_h);
+            CKL();
+            if (open.empty()) outside++;
+            break;
+        case RecOp::COND_LOOP:
+            if (open.empty()) throw CudaError{"grouped launch: a loop condition outside a loop"};
+            k_group_cond<<<1, 256, 0, cur()>>>(reinterpret_cast<const int* const*>(arr), n, open.back().h);
+            CKL();
+            break;
+        case RecOp::LOOP_BEGIN: {
+            if (!next_flags || (int)open.size() >= ncap) throw CudaError{"grouped launch: unsupported loop"};
+            cudaGraph_t body = add_while(cur(), next_h);
+            Loop L{next_h, next_flags, nullptr};
+            L.bc.reset(new BodyCapture(cap[open.size()], body));
+            open.push_back(std::move(L));
+            next_flags = nullptr;
+            break;
+        }
+        case RecOp::LOOP_END:
+            if (open.empty()) throw CudaError{"grouped launch: unbalanced loop"};
+            open.back().bc->end();
+            open.pop_back();
+            break;
+        }
+    }
+    if (!open.empty()) throw CudaError{"grouped launch: unbalanced loop"};
+    return outside;
+}
+
 // Captures one step of the cases `idx` as a graph on the batch stream;
-// gstatic receives each case's kernel count outside loops.
-cudaGraphExec_t batch_capture(vvm_gpu_batch* b, const std::vector<int>& idx, std::vector<long long>& gstatic) {
+// gstatic receives each case's kernel count outside loops (a grouped
+// launch counts once, for the group's first case); bufs the device arrays
+// the graph's grouped launches read.
+cudaGraphExec_t batch_capture(vvm_gpu_batch* b, const std::vector<int>& idx, std::vector<long long>& gstatic,
+                              std::vector<void*>& bufs) {
     gstatic.assign(b->cases.size(), 0);
     struct Saved {
         cudaStream_t stream;
@@ -2858,11 +3194,74 @@ cudaGraphExec_t batch_capture(vvm_gpu_batch* b, const std::vector<int>& idx, std
             c->stats.launches = sv[j].launches;
         }
     };
+    // groups of cases that can step as grouped launches, recorded and checked
+    std::vector<std::vector<int>> groups;
+    std::vector<std::vector<Recorder>> recs;
+    std::vector<int> alone;
+    {
+        std::vector<std::vector<int>> cand;
+        std::vector<std::array<int, 5>> keys;
+        for (int i : idx) {
+            vvm_gpu_ctx* c = b->cases[i];
+            const int lim = group_limit(b, c);
+            if (lim < 2 || !groupable(c)) {
+                alone.push_back(i);
+                continue;
+            }
+            const std::array<int, 5> k = {c->d.nx, c->d.nz, c->mixed ? 1 : 0, c->tune_gs_tr, c->tune_fft};
+            size_t gi = 0;
+            while (gi < keys.size() && keys[gi] != k) gi++;
+            if (gi == keys.size()) {
+                keys.push_back(k);
+                cand.emplace_back();
+            }
+            cand[gi].push_back(i);
+        }
+        // split each shape's cases into sub-groups of at most `lim`, sizes as even as possible
+        std::vector<std::vector<int>> parts;
+        for (auto& gidx : cand) {
+            const int lim = group_limit(b, b->cases[gidx[0]]);
+            const int m = (int)gidx.size(), np = (m + lim - 1) / lim;
+            for (int q = 0, at = 0; q < np; q++) {
+                const int sz = m / np + (q < m % np ? 1 : 0);
+                parts.emplace_back(gidx.begin() + at, gidx.begin() + at + sz);
+                at += sz;
+            }
+        }
+        for (auto& gidx : parts) {
+            std::vector<Recorder> r(gidx.size());
+            bool ok = gidx.size() >= 2;
+            for (size_t j = 0; ok && j < gidx.size(); j++) ok = record_step(b->cases[gidx[j]], r[j]);
+            for (size_t j = 1; ok && j < gidx.size(); j++) ok = same_ops(r[0], r[j]);
+            if (ok) {
+                groups.push_back(gidx);
+                recs.push_back(std::move(r));
+            } else {
+                alone.insert(alone.end(), gidx.begin(), gidx.end());
+            }
+        }
+    }
+    std::vector<GroupArrays> arrays;
+    try {
+        for (auto& r : recs) arrays.push_back(group_arrays(r));
+    } catch (...) {
+        for (auto& A : arrays) cudaFree(A.dev);
+        throw;
+    }
+    for (auto& A : arrays) bufs.push_back(A.dev);
+    b->last_groups = (int)groups.size();
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
     try {
         CK(cudaEventRecord(b->fork, b->stream));
-        for (int i : idx) {
+        for (size_t gi = 0; gi < groups.size(); gi++) {
+            vvm_gpu_ctx* c0 = b->cases[groups[gi][0]];
+            CK(cudaStreamWaitEvent(c0->own, b->fork, 0));
+            gstatic[groups[gi][0]] = group_replay(recs[gi], arrays[gi], c0->own, c0->cap, 2);
+            CK(cudaEventRecord(b->joins[groups[gi][0]], c0->own));
+            CK(cudaStreamWaitEvent(b->stream, b->joins[groups[gi][0]], 0));
+        }
+        for (int i : alone) {
             vvm_gpu_ctx* c = b->cases[i];
             c->stream = c->own;
             CK(cudaStreamWaitEvent(c->own, b->fork, 0));
@@ -2936,7 +3335,7 @@ int batch_step(vvm_gpu_batch* b, int nsteps) {
             continue;
         }
         const int bi = c0->cur, par = (c0->step + 1) & 1;
-        if (!b->gexec[bi][par]) b->gexec[bi][par] = batch_capture(b, all, b->gstatic[bi][par]);
+        if (!b->gexec[bi][par]) b->gexec[bi][par] = batch_capture(b, all, b->gstatic[bi][par], b->gbufs[bi][par]);
         if (!on_batch) {
             batch_fence(b, true);
             on_batch = true;
@@ -2960,23 +3359,37 @@ int batch_step(vvm_gpu_batch* b, int nsteps) {
 // warm up, then `reps` timed launches of the same graph on the batch stream).
 double batch_time(vvm_gpu_batch* b, const std::vector<int>& idx, int reps) {
     std::vector<long long> gs;
-    cudaGraphExec_t ex = batch_capture(b, idx, gs);
-    CK(cudaGraphLaunch(ex, b->stream));
-    CK(cudaEventRecord(b->t0, b->stream));
-    for (int r = 0; r < reps; r++) CK(cudaGraphLaunch(ex, b->stream));
-    CK(cudaEventRecord(b->t1, b->stream));
-    CK(cudaEventSynchronize(b->t1));
+    std::vector<void*> bufs;
+    struct Free {
+        std::vector<void*>& v;
+        ~Free() {
+            for (void* q : v) cudaFree(q);
+        }
+    } free_bufs{bufs};
+    cudaGraphExec_t ex = batch_capture(b, idx, gs, bufs);
     float ms = 0;
-    CK(cudaEventElapsedTime(&ms, b->t0, b->t1));
+    try {
+        CK(cudaGraphLaunch(ex, b->stream));
+        CK(cudaEventRecord(b->t0, b->stream));
+        for (int r = 0; r < reps; r++) CK(cudaGraphLaunch(ex, b->stream));
+        CK(cudaEventRecord(b->t1, b->stream));
+        CK(cudaEventSynchronize(b->t1));
+        CK(cudaEventElapsedTime(&ms, b->t0, b->t1));
+    } catch (...) {
+        cudaStreamSynchronize(b->stream);
+        cudaGraphExecDestroy(ex);
+        throw;
+    }
     cudaGraphExecDestroy(ex);
     return ms / std::max(reps, 1);
 }
 
 // Autotuner: for each group of cases with the same grid, precision and
 // solver, coordinate descent over the launch-shape knobs that leave the
-// arithmetic unchanged (the Gauss-Seidel cluster size, the row-FFT block),
-// timing one step of the group's cases as a graph per candidate. Every case
-// is put back exactly afterwards.
+// arithmetic unchanged (the Gauss-Seidel schedule: tile height or one cluster
+// a field; the row-FFT block; the cases a grouped launch takes), timing one
+// step of the group's cases as a graph per candidate. Every case is put back
+// exactly afterwards.
 int batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
     const size_t n = b->cases.size();
     CK(cudaStreamSynchronize(b->stream));
@@ -3040,6 +3453,22 @@ int batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups) {
             }
         }
         set_all(idx, best_cs, best_fft);
+        // cases a grouped launch takes: one launch for all of them, sub-groups
+        // as parallel branches, or (1) every case its own branch
+        if (idx.size() >= 2 && groupable(c)) {
+            const int m = (int)idx.size();
+            int best_grp = 0;
+            for (int gsz : {1, m, (m + 1) / 2, (m + 3) / 4, (m + 7) / 8}) {
+                if (gsz < 2 && gsz != 1) continue;
+                for (int i : idx) b->cases[i]->tune_group = gsz;
+                const double t = batch_time(b, idx, reps);
+                if (t < best) {
+                    best = t;
+                    best_grp = gsz;
+                }
+            }
+            for (int i : idx) b->cases[i]->tune_group = best_grp;
+        }
     }
     CK(cudaStreamSynchronize(b->stream));
     for (size_t i = 0; i < n; i++) {
@@ -4278,6 +4707,19 @@ int vvm_gpu_batch_stream(vvm_gpu_batch* b, void** stream) {
     if (!b || !stream) return VVM_GPU_EINVAL;
     *stream = b->stream;
     return VVM_GPU_OK;
+}
+
+int vvm_gpu_batch_grouping(vvm_gpu_batch* b, int max_cases, int* groups) {
+    return batch_guarded(b, [&]() -> int {
+        if (max_cases >= 0 && max_cases != b->group_max) {
+            CK(cudaStreamSynchronize(b->stream));
+            b->group_max = max_cases;
+            for (auto* c : b->cases) c->tune_group = 0;
+            b->drop_graphs();
+        }
+        if (groups) *groups = b->last_groups;
+        return VVM_GPU_OK;
+    });
 }
 
 int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len) {

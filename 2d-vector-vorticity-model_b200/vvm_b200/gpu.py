@@ -79,6 +79,7 @@ EXPORTS = ("vvm_gpu_desc_default", "vvm_gpu_create", "vvm_gpu_destroy", "vvm_gpu
            "vvm_gpu_set_tuning", "vvm_gpu_get_tuning", "vvm_gpu_batch_create", "vvm_gpu_batch_destroy",
            "vvm_gpu_batch_case", "vvm_gpu_batch_step", "vvm_gpu_batch_synchronize",
            "vvm_gpu_batch_autotune", "vvm_gpu_batch_last_error", "vvm_gpu_batch_stream",
+           "vvm_gpu_batch_grouping",
            "vvm_gpu_conv3x3_c32", "vvm_gpu_learned_shape", "vvm_gpu_learned_weights",
            "vvm_gpu_learned_eval", "vvm_gpu_learned_train", "vvm_gpu_learned_config",
            "vvm_gpu_learned_last", "vvm_gpu_learned_time", "vvm_gpu_learned_train_rhs",
@@ -128,6 +129,7 @@ def load_library(path: Path | None = None):
     L.vvm_gpu_batch_autotune.argtypes = [vp, ip, ctypes.POINTER(ip)]
     L.vvm_gpu_batch_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
     L.vvm_gpu_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.vvm_gpu_batch_grouping.argtypes = [vp, ip, ctypes.POINTER(ip)]
     _fp = ctypes.POINTER(ctypes.c_float)
     L.vvm_gpu_conv3x3_c32.argtypes = [_fp, _fp, _fp, ip, ip, ip, ip]
     L.vvm_gpu_learned_shape.argtypes = [vp, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip)]
@@ -560,6 +562,17 @@ class VVMBatch:
         p = ctypes.c_void_p()
         self._check(self.L.vvm_gpu_batch_stream(self.h, ctypes.byref(p)))
         return p.value or 0
+
+    def grouping(self, max_cases: int | bool | None = None) -> int:
+        """Sets the most cases one grouped launch takes (False or 0: no
+        grouped launches; True: the default of 32; None: unchanged); returns
+        the number of grouped launch groups in the last captured step graph."""
+        if max_cases is True:
+            max_cases = 32
+        v = -1 if max_cases is None else int(max_cases)
+        n = ctypes.c_int()
+        self._check(self.L.vvm_gpu_batch_grouping(self.h, v, ctypes.byref(n)))
+        return n.value
 
     def autotune(self, reps: int = 3) -> int:
         n = ctypes.c_int()

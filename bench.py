@@ -573,6 +573,19 @@ def ensemble_arm(args, rank, world, device):
     e1.synchronize()
     b.synchronize()
     max_ms = dist_max(e0.elapsed_time(e1))
+    grouped = b.grouping()
+    # the same steps with every case its own branch of the graph (no grouped launches)
+    b.grouping(False)
+    b.step(2)
+    b.synchronize()
+    if dist_on():
+        dist_barrier()
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    b.synchronize()
+    ungrouped_ms = dist_max(e0.elapsed_time(e1))
     total = sum(costs)
     b.close()
     return {"workload": f"{ENSEMBLE_CASES} warm-bubble cases (seed {ENSEMBLE_SEED}): NX in "
@@ -582,8 +595,12 @@ def ensemble_arm(args, rank, world, device):
             "ms_per_step": max_ms / args.steps, "cells_per_step": total, "cases": ENSEMBLE_CASES,
             "cases_this_rank": len(mine), "scaling": "strong",
             "sharding": "by cells, longest first to the least-loaded rank; no exchange",
-            "precision": "mixed", "solver": "spectral", "graph": "one CUDA graph a step for all cases",
-            "autotune_groups": groups, "l2": "working set larger than L2"}
+            "precision": "mixed", "solver": "spectral",
+            "graph": "one CUDA graph a step; the cases of each grid shape as grouped launches "
+                     "(one launch a kernel for the group, blockIdx.z the case)",
+            "grouped_groups": grouped, "autotune_groups": groups,
+            "ungrouped_ms_per_step": ungrouped_ms / args.steps,
+            "l2": "working set larger than L2"}
 
 
 # ----------------------------------------------------------- reference arm

@@ -306,13 +306,19 @@ int vvm_gpu_get_tuning(vvm_gpu_ctx* ctx, int* gs_tile_rows, int* fft_threads);
  * The reference runs one case per process. A batch holds many cases of any
  * sizes (one context each, created from descs[i] on `device`) that advance
  * together: from the third step on, one CUDA graph per step runs every
- * case's step as a parallel branch, launched on the batch's own stream.
+ * case's step, launched on the batch's own stream. Cases with the same grid,
+ * precision and tuning whose step uses the exact Fourier-mode solve and the
+ * tiled Gauss-Seidel passes step as grouped launches: one launch a kernel
+ * for all cases of the group (each case reads its own arguments and loop
+ * flags), each group a parallel branch; other cases run as branches of
+ * their own. Either way each case's results are those it computes alone.
  * vvm_gpu_batch_case returns case i's context, owned by the batch, for
  * upload, download, queries and the routine entries; every case must be at
  * the same step when vvm_gpu_batch_step runs (VVM_GPU_ESTATE otherwise).
  * vvm_gpu_batch_autotune times one step of each group of cases with the same
  * grid, precision and solver for each value of the launch-shape knobs above
- * (`reps` graph launches per candidate), keeps the fastest, and restores
+ * and for the cases a grouped launch takes (`reps` graph launches per
+ * candidate), keeps the fastest, and restores
  * every case's state exactly; *ngroups receives the number of groups.
  * vvm_gpu_batch_synchronize waits for the batch and reports any case's
  * device error. Failures of batch calls: vvm_gpu_batch_last_error. */
@@ -325,6 +331,15 @@ int vvm_gpu_batch_synchronize(vvm_gpu_batch* b);
 int vvm_gpu_batch_autotune(vvm_gpu_batch* b, int reps, int* ngroups);
 /* The stream the batch graphs run on (cudaStream_t), for events around them. */
 int vvm_gpu_batch_stream(vvm_gpu_batch* b, void** stream);
+/* The most cases one grouped launch takes (default 32; a shape with more
+ * cases is split into sub-groups of even size, parallel branches of the
+ * graph); 0 or 1: no grouped launches, every case its own branch; < 0 leaves
+ * the setting. Grids of more than 65536 cells step case by case unless
+ * vvm_gpu_batch_autotune found grouped launches faster for them. Setting it
+ * clears the autotuner's per-group choice and drops the batch's graphs. *groups (may be null) receives the number of grouped
+ * launch groups in the last captured step graph. No counterpart in the
+ * reference, which runs one case per process (src/main.cpp:29-147). */
+int vvm_gpu_batch_grouping(vvm_gpu_batch* b, int max_cases, int* groups);
 int vvm_gpu_batch_last_error(vvm_gpu_batch* b, char* buf, size_t len);
 
 /* -- elliptic solve that allocates nothing ------------------------------------

@@ -121,3 +121,67 @@ def test_batch_rejects_cases_at_different_steps(gpu):
         b.step(1)
     assert e.value.code == 4
     b.close()
+
+
+def _varied(shapes):
+    """Distinct cases of each shape: bubbles of other amplitudes, places and
+    sizes (amplitude 0: a resting atmosphere, whose cal_w right-hand side is
+    zero)."""
+    from vvm_b200.initial_state import warm_bubble
+    out = []
+    for j, (nx, nz) in enumerate(shapes):
+        amp = (0.0, 1.0, 2.5, 6.0)[j % 4]
+        out.append(warm_bubble(nx, nz, 200.0, 200.0, amp=amp, radius=max(400.0, nx * 200 / (6 + j % 3)),
+                               xc_frac=0.3 + 0.1 * (j % 5)))
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_grouped_launches_equal_cases_alone(gpu, precision):
+    """Cases of one shape step as grouped launches (one launch a kernel for
+    the group, blockIdx.z the case); each case must still equal itself
+    stepped alone, bit for bit, and equal the batch with grouping off."""
+    shapes = [(64, 32)] * 4 + [(128, 48)] * 3 + [(256, 32)]
+    sts = _varied(shapes)
+    outs = {}
+    # at most 32 cases a launch (both shapes one group each), at most 2 (4 cases
+    # in two groups, 3 in a group of 2 and one case alone), none
+    for limit, groups in ((32, 2), (2, 3), (0, 0)):
+        b = gpu.VVMBatch([s.grid for s in sts], precision=precision, solver=2)
+        b.grouping(limit)
+        b.upload(sts)
+        b.step(3)
+        b.step(5)
+        b.synchronize()
+        assert b.grouping() == groups, limit
+        outs[limit] = [c.download() for c in b.cases]
+        b.close()
+    for j, st in enumerate(sts):
+        alone = _alone(gpu, st, 8, precision, 2)
+        for limit in outs:
+            assert _same(outs[limit][j], alone), (j, limit)
+
+
+def test_grouped_loop_gates_cases(gpu):
+    """A tolerance the direct solve's check does not meet makes CG iterate in
+    the moving cases of a group while the resting case (zero right-hand
+    side) leaves its loop at once: the grouped loop runs while any case
+    needs it, and a case that has left it must not iterate."""
+    shapes = [(128, 48)] * 4
+    sts = _varied(shapes)
+    tol = 1e-14
+    b = gpu.VVMBatch([s.grid for s in sts], precision=0, solver=2, poisson_tol=tol)
+    b.upload(sts)
+    b.step(3)
+    b.step(3)
+    b.synchronize()
+    assert b.grouping() == 1
+    iters = [c.last_solve()[0] for c in b.cases]
+    assert iters[0] == 0 and max(iters) > 0, iters
+    for st, c in zip(sts, b.cases):
+        g = gpu.VVMGpu(st.grid, precision=0, solver=2, poisson_tol=tol)
+        g.upload(st)
+        g.step(6)
+        assert _same(c.download(), g.download())
+        g.close()
+    b.close()
