@@ -1880,7 +1880,9 @@ __global__ void k_pubartop(PubarArgs<T> a) { k_pubartop_body<T>(a); }
 // uxi = (chi[i] - chi[i-1])/dx with its mean removed. The differences satisfy
 // d[i+1] - d[i] = h[i], so uxi is an exclusive prefix sum of h (any constant
 // cancels in the mean removal); the reference reaches the same values with
-// CG to 1e-12. One block.
+// CG to 1e-12. Every block of the column kernel computes the whole top row
+// (one block's worth of work, the same arithmetic in every block) and keeps
+// its own 32 columns: no second launch waits for a one-block kernel.
 
 template <typename T>
 struct CalUArgs {
@@ -1894,8 +1896,10 @@ struct CalUArgs {
 
 constexpr int kCalUThreads = 1024;
 
+// The top-row u of columns own_lo .. own_lo+31 into own[] (kCalUThreads
+// threads, one block).
 template <typename T>
-__device__ __forceinline__ void k_cal_u_top_body(const CalUArgs<T>& a) {
+__device__ __forceinline__ void cal_u_top_row(const CalUArgs<T>& a, T* own, int own_lo) {
     __shared__ double sh[32 * 1];
     __shared__ double scan[32];
     const Dims& d = a.d;
@@ -1962,19 +1966,13 @@ __device__ __forceinline__ void k_cal_u_top_body(const CalUArgs<T>& a) {
 #pragma unroll
     for (int e = 0; e < kGSMaxPerThread; e++) {
         int i = i0 + e;
-        if (e < per && i <= NX) {
-            T v = T((ux[e] - umean) + ubarp);
-            a.u[d.at(i, t)] = v;
-            if (i == NX) a.u[d.at(0, t)] = v;
-            if (i == 1) a.u[d.at(d.nx - 1, t)] = v;
-        }
+        if (e < per && i <= NX && i >= own_lo && i < own_lo + 32) own[i - own_lo] = T((ux[e] - umean) + ubarp);
     }
 }
-template <typename T>
-__global__ void __launch_bounds__(kCalUThreads) k_cal_u_top(CalUArgs<T> a) { k_cal_u_top_body<T>(a); }
 
 // Column integral u(i, k) = u(i, nz-2) + sum_{m=k}^{nz-3} (dw/dx - rhow zeta)(-dz)
-// from the top down (PoissonSolver.cpp:644-651), with the center halo of u.
+// from the top down (PoissonSolver.cpp:644-651), with the center halo of u;
+// u(i, nz-2), the top row, comes from cal_u_top_row in the same block.
 // A block owns 32 columns (lanes) and kColSeg z-segments (warps): each thread
 // sums its segment, the segment totals are scanned from the top in shared
 // memory, then each thread writes its rows. Thirty-two segments give the 64
@@ -1984,7 +1982,9 @@ constexpr int kColSeg = 32;
 
 template <typename T>
 __device__ __forceinline__ void k_cal_u_columns_body(const CalUArgs<T>& a) {
+    static_assert(32 * kColSeg == kCalUThreads, "the top row takes the column kernel's block");
     __shared__ T tot[kColSeg][32];
+    __shared__ T utop_sh[32];
     const Dims& d = a.d;
     const int lane = threadIdx.x & 31, s = threadIdx.x >> 5;
     const int i = 1 + blockIdx.x * 32 + lane;
@@ -1997,13 +1997,14 @@ __device__ __forceinline__ void k_cal_u_columns_body(const CalUArgs<T>& a) {
         return ((a.w[d.at(i, k + 1)] - a.w[d.at(i - 1, k + 1)]) * rdx - T(a.p.rhow[k + 1]) * a.zetap[d.at(i, k + 1)]) *
                T(-a.p.dzw[k + 1]);
     };
+    cal_u_top_row(a, utop_sh, 1 + blockIdx.x * 32);
     T sum = T(0);
     if (act)
         for (int r = r0; r < r1; r++) sum += term(t - 1 - r);
     tot[s][lane] = sum;
     __syncthreads();
     if (!act) return;
-    const T utop = a.u[d.at(i, t)];
+    const T utop = utop_sh[lane];
     T area = T(0);
     for (int q = 0; q < s; q++) area += tot[q][lane];
     if (s == 0) store_center(a.u, d, i, t, utop);

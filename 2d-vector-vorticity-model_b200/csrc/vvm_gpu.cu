@@ -130,12 +130,14 @@ __global__ void k_loop_outer(const CGScalars* sc64, CGCtl* ctl, const CGCtl* inn
 }
 
 // b = rhow_k^2 (zetap[i+1][k] - zetap[i][k]) dx for k = 2..nz-2, i = 1..nx-2
-// (PoissonSolver.cpp:444-450); stores f = -b / rw_k and partial ||b||^2. rw_k
-// is the row's residual weight: rhow_k on uniform levels, rhow_k / a_k on
-// stretched ones (a_k the centre spacing around face k over dx).
+// (PoissonSolver.cpp:444-450); stores f = -b / rw_k and the block partials of
+// ||b||^2, which the block that arrives last sums in a fixed order into
+// sc->bb (arrive: a counter at 0, left at 0). rw_k is the row's residual
+// weight: rhow_k on uniform levels, rhow_k / a_k on stretched ones (a_k the
+// centre spacing around face k over dx).
 template <typename T>
 __device__ __forceinline__ void k_poisson_rhs_body(const Dims& d, double dx, const double* rhow, const double* rw, const T* zetap, double* f,
-                              int pitch_f, double* partial) {
+                              int pitch_f, double* partial, unsigned* arrive, CGScalars* sc) {
     __shared__ double sh[32];
     const int ii = blockIdx.x * blockDim.x + threadIdx.x;
     const int kk = blockIdx.y * blockDim.y + threadIdx.y;
@@ -148,10 +150,19 @@ __device__ __forceinline__ void k_poisson_rhs_body(const Dims& d, double dx, con
     }
     block_sum(s, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) partial[blockIdx.x + gridDim.x * blockIdx.y] = s[0];
+    const unsigned nb = gridDim.x * gridDim.y;
+    if (!arrive_last(arrive, nb)) return;
+    const int nt = blockDim.x * blockDim.y, tid = threadIdx.x + blockDim.x * threadIdx.y;
+    double t[1] = {0};
+    for (int q = tid; q < (int)nb; q += nt) t[0] += __ldcg(partial + q);
+    block_sum(t, sh);
+    if (tid == 0) sc->bb = t[0];
 }
 template <typename T>
 __global__ void k_poisson_rhs(Dims d, double dx, const double* rhow, const double* rw, const T* zetap, double* f,
-                              int pitch_f, double* partial) { k_poisson_rhs_body<T>(d, dx, rhow, rw, zetap, f, pitch_f, partial); }
+                              int pitch_f, double* partial, unsigned* arrive, CGScalars* sc) {
+    k_poisson_rhs_body<T>(d, dx, rhow, rw, zetap, f, pitch_f, partial, arrive, sc);
+}
 
 // Reference-ordered b vector ((k-2)*NX + (i-1)) to f = -b/rw_k, partial ||b||^2.
 __global__ void k_rhs_from_b(int NX, int NK, const double* rw, const double* b, double* f,
@@ -2580,9 +2591,8 @@ int launch_cal_w(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr, cudaEve
     dim3 B(64, 4), G(cdiv(NX, 64), cdiv(NK, 4));
     klaunch<k_poisson_rhs_body<T>, 256>(&c->stats, VVM_K_POISSON_RHS, c->stream, k_poisson_rhs<T>, G, B, 0, c->d,
                                         c->c.dx, (const double*)c->rhow, (const double*)c->rwres,
-                                        (const T*)F.zeta[fut], c->Wf, pitch, c->wpartial);
-    klaunch<k_cg_scalar_body, 1024>(&c->stats, VVM_K_CG, c->stream, k_cg_scalar, dim3(1), dim3(1024), 0,
-                                    (const double*)c->wpartial, c->wnpart, c->pcg64->sc, (int)CG_SET_BB);
+                                        (const T*)F.zeta[fut], c->Wf, pitch, c->wpartial, c->pcg64->arrive,
+                                        c->pcg64->sc);   // sets sc->bb
     const bool warm = c->desc.warm_start != 0;
     const int maxit = c->desc.poisson_maxit > 0 ? c->desc.poisson_maxit : 200;
     if (recorded_in_loops) {   // graph capture: the loops run on the device
@@ -2624,8 +2634,6 @@ void launch_cal_u(vvm_gpu_ctx* c) {
     Fields<T>& F = fields<T>(c);
     int fut = 1 - c->cur;
     CalUArgs<T> a{c->d, c->c, c->profiles(), F.u, F.w, F.zeta[fut], c->ubar};
-    klaunch<k_cal_u_top_body<T>, kCalUThreads>(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_top<T>, dim3(1),
-                                               dim3(kCalUThreads), 0, a);
     klaunch<k_cal_u_columns_body<T>, 32 * kColSeg>(&c->stats, VVM_K_CAL_U, c->stream, k_cal_u_columns<T>,
                                                    dim3(cdiv(c->d.nx - 2, 32)), dim3(32 * kColSeg), 0, a);
 }
@@ -2717,13 +2725,13 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
     // The step's kernels form two chains (in a captured step, two branches of
     // the graph; the results are those of the reference's order, since
     // neither chain reads what the other writes before they meet):
-    //  main: pubarTop_pt (reads u, w, RKM; writes ubar, dubar), pzeta_pt
-    //        (writes zetap and its tendencies), cal_w up to its solution W,
-    //        then, once the scalar advection has read w and u, w from W
-    //        and cal_u;
-    //  side: the scalar advection (writes the future th, qv, qc, qr and
-    //        their tendencies), their NVP rescaling and AddForcing, Kessler,
-    //        its NVP and the halos of th, qv, qc, qr.
+    //  main: pzeta_pt (writes zetap and its tendencies), cal_w up to its
+    //        solution W, then, once the side chain has read w and u and
+    //        written ubarTopp, w from W and cal_u (which reads ubarTopp);
+    //  side: pubarTop_pt (reads u, w, RKM; writes ubar, dubar), the scalar
+    //        advection (writes the future th, qv, qc, qr and their
+    //        tendencies), their NVP rescaling and AddForcing, Kessler, its
+    //        NVP and the halos of th, qv, qc, qr.
     // They meet before the turbulence. A batch's cases are already parallel
     // branches of its graph: there every case runs as one chain, in the
     // reference's order; so does a profiled step, whose event timers should
@@ -2734,12 +2742,12 @@ int run_step(vvm_gpu_ctx* c, long long* recorded_in_loops = nullptr) {
         fork_side(c, 0);
         {
             OnStream os(c, c->side);
+            if (!sf) launch_pubartop<T>(c);                    // pubarTop_pt
             launch_padv<T>(c, F_TH | F_QV | F_QC | F_QR, F_QV | F_QC | F_QR, true, true);  // pth, pqv, pqc, pqr
-            CK(cudaEventRecord(c->fork_ev[1], c->side));   // u and w read
+            CK(cudaEventRecord(c->fork_ev[1], c->side));   // u and w read, ubarTopp written
             launch_kessler<T>(c, true, true);                  // NVP + AddForcing, Kessler + NVP x3 + halos
         }
         try {
-            if (!sf) launch_pubartop<T>(c);                    // pubarTop_pt
             launch_pzeta<T>(c);                                // pzeta_pt
             if (sf) {
                 CK(cudaStreamWaitEvent(c->stream, c->fork_ev[1], 0));
