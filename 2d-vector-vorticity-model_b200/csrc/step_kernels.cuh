@@ -993,6 +993,12 @@ constexpr int kGTPer = 4;
 constexpr int kGSTileRowsMin = 4, kGSTileRowsMax = 32, kGSTileRowsDefault = 8;
 constexpr int kGSRowVals = 9;   // scalars a tile row keeps in shared memory
 inline bool gs_tile_rows_ok(int tr) { return tr == 4 || tr == 8 || tr == 16 || tr == 32; }
+// Blocks a SM the tile kernel is compiled for: three in FP64 (up to 168
+// registers a thread: pass 1 then keeps its rolling windows without spilling;
+// the 1360 tiles of the 2048 x 256 default still fit in one wave), four in
+// FP32.
+template <typename T>
+constexpr int kGSTileMinBlocks = sizeof(T) == 8 ? 3 : 4;
 
 struct GSTileCtl {    // zeroed before a sweep
     int pass;         // passes of the sweep completed
@@ -1344,7 +1350,7 @@ __device__ __forceinline__ void k_gs_tiles_body(const GSArgs<T>& a, const GSTile
     }
 }
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(128, 4) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) { k_gs_tiles_body<T, FIRST>(a, t, h); }
+__global__ void __launch_bounds__(128, kGSTileMinBlocks<T>) k_gs_tiles(GSArgs<T> a, GSTileArgs<T> t, cudaGraphConditionalHandle h) { k_gs_tiles_body<T, FIRST>(a, t, h); }
 
 // ---------------------------------------------------------------------------
 // The second schedule of the same recurrence: one thread-block cluster a field.

@@ -2123,7 +2123,7 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops 
     const int maxp = std::max(2, nb + nc - 1);
     cudaStream_t st = c->stream;
     zero_async(&c->stats, c->gsctl, sizeof(GSTileCtl), st);   // a fresh sweep
-    klaunch<k_gs_tiles_body<T, true>, 128, 4>(&c->stats, VVM_K_GS, st, k_gs_tiles<T, true>, dim3(tblocks), dim3(128), 0,
+    klaunch<k_gs_tiles_body<T, true>, 128, kGSTileMinBlocks<T>>(&c->stats, VVM_K_GS, st, k_gs_tiles<T, true>, dim3(tblocks), dim3(128), 0,
                                               g, t, (cudaGraphConditionalHandle)0);   // pass 1
     if (recorded_in_loops) {
         // graph capture: the typical passes 2..kGSGraphPasses+1 unconditionally
@@ -2134,13 +2134,13 @@ void launch_turbulence(vvm_gpu_ctx* c, bool nudge, long long* recorded_in_loops 
         GSTileArgs<T> tu = t;
         tu.exec = nullptr;   // counted with the graph's static kernels
         for (int p = 0; p < kGSGraphPasses; p++)
-            klaunch<k_gs_tiles_body<T, false>, 128, 4>(&c->stats, VVM_K_GS, st, k_gs_tiles<T, false>, dim3(tblocks),
+            klaunch<k_gs_tiles_body<T, false>, 128, kGSTileMinBlocks<T>>(&c->stats, VVM_K_GS, st, k_gs_tiles<T, false>, dim3(tblocks),
                                                        dim3(128), 0, g, tu, h);
         record_cond(&c->stats, &c->gsctl->more, true);
         cudaGraph_t body = add_while(&c->stats, st, h);
         BodyCapture bc(c->cap[0], body, &c->stats);
         const long long n0 = c->stats.launches;
-        klaunch<k_gs_tiles_body<T, false>, 128, 4>(&c->stats, VVM_K_GS, bc.s, k_gs_tiles<T, false>, dim3(tblocks),
+        klaunch<k_gs_tiles_body<T, false>, 128, kGSTileMinBlocks<T>>(&c->stats, VVM_K_GS, bc.s, k_gs_tiles<T, false>, dim3(tblocks),
                                                    dim3(128), 0, g, t, h);
         record_cond(&c->stats, &c->gsctl->more, false);
         bc.end();
