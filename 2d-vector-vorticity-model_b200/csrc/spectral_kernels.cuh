@@ -42,13 +42,28 @@ struct SpecArgs {
     P *sre, *sim;            // spectra, [NK][mpitch]
 };
 
+// Shared-memory slot of point i of a row: i with its low four bits XORed with
+// bits 2-5 and 8-11 (a permutation of 0..N-1). Eight-byte words fall in 16
+// bank pairs; unswizzled, the bit-reversed stores and the first two double
+// passes of fft_shared put 4 to 16 of a half-warp's words in one pair (1.6 M
+// bank conflicts a launch at NX = 2048). With the swizzle every access
+// pattern of these kernels averages about 1.1 wavefronts a half-warp at NX =
+// 2048 and 8192. Only the slot changes, so the arithmetic is the same.
+__device__ __forceinline__ int sw(int i) { return i ^ (((i >> 2) ^ (i >> 8)) & 15); }
+// The twiddle table's slot of entry j (a permutation of 0..N/2-1): the passes
+// read entries j * N / 2^s of up to 16 distinct j a half-warp, which all fall
+// in one bank pair unswizzled; XORing the low four bits with bits 4-7 and
+// 8-11 spreads them.
+__device__ __forceinline__ int twz(int j) { return j ^ (((j >> 4) ^ (j >> 8)) & 15); }
+
 // The twiddles exp(-2 pi i j / N), j < N/2, copied into shared memory (tw:
-// N values, real parts then imaginary) before the first barrier of a kernel.
+// N values, real parts then imaginary, entry j at slot twz(j)) before the
+// first barrier of a kernel.
 template <typename P>
 __device__ __forceinline__ void load_twiddles(P* tw, const SpecArgs<P>& a) {
     for (int j = threadIdx.x; j < a.NX / 2; j += blockDim.x) {
-        tw[j] = a.twr[j];
-        tw[a.NX / 2 + j] = a.twi[j];
+        tw[twz(j)] = a.twr[j];
+        tw[a.NX / 2 + twz(j)] = a.twi[j];
     }
 }
 
@@ -85,23 +100,23 @@ __device__ __forceinline__ void fft_shared(P* re, P* im, const P* tw, const Spec
         for (int t = threadIdx.x; t < N / 4; t += blockDim.x) {
             const int j = t & (h - 1);
             const int b0 = ((t >> (s - 1)) << (s + 1)) + j;
-            P r0 = re[b0], i0 = im[b0], r1 = re[b0 + h], i1 = im[b0 + h];
-            P r2 = re[b0 + 2 * h], i2 = im[b0 + 2 * h], r3 = re[b0 + 3 * h], i3 = im[b0 + 3 * h];
-            const P w1r = twr[j * ts1], w1i = sg * twi[j * ts1];
+            P r0 = re[sw(b0)], i0 = im[sw(b0)], r1 = re[sw(b0 + h)], i1 = im[sw(b0 + h)];
+            P r2 = re[sw(b0 + 2 * h)], i2 = im[sw(b0 + 2 * h)], r3 = re[sw(b0 + 3 * h)], i3 = im[sw(b0 + 3 * h)];
+            const P w1r = twr[twz(j * ts1)], w1i = sg * twi[twz(j * ts1)];
             fft_bfly(r0, i0, r1, i1, w1r, w1i);   // stage s: (b0, b0+h), (b0+2h, b0+3h)
             fft_bfly(r2, i2, r3, i3, w1r, w1i);
-            const P w2r = twr[j * ts2], w2i = sg * twi[j * ts2];
-            const P w3r = twr[(j + h) * ts2], w3i = sg * twi[(j + h) * ts2];
+            const P w2r = twr[twz(j * ts2)], w2i = sg * twi[twz(j * ts2)];
+            const P w3r = twr[twz((j + h) * ts2)], w3i = sg * twi[twz((j + h) * ts2)];
             fft_bfly(r0, i0, r2, i2, w2r, w2i);   // stage s+1: (b0, b0+2h), (b0+h, b0+3h)
             fft_bfly(r1, i1, r3, i3, w3r, w3i);
-            re[b0] = r0;
-            im[b0] = i0;
-            re[b0 + h] = r1;
-            im[b0 + h] = i1;
-            re[b0 + 2 * h] = r2;
-            im[b0 + 2 * h] = i2;
-            re[b0 + 3 * h] = r3;
-            im[b0 + 3 * h] = i3;
+            re[sw(b0)] = r0;
+            im[sw(b0)] = i0;
+            re[sw(b0 + h)] = r1;
+            im[sw(b0 + h)] = i1;
+            re[sw(b0 + 2 * h)] = r2;
+            im[sw(b0 + 2 * h)] = i2;
+            re[sw(b0 + 3 * h)] = r3;
+            im[sw(b0 + 3 * h)] = i3;
         }
         __syncthreads();
     }
@@ -111,12 +126,12 @@ __device__ __forceinline__ void fft_shared(P* re, P* im, const P* tw, const Spec
         for (int t = threadIdx.x; t < N / 2; t += blockDim.x) {
             const int j = t & (half - 1);
             const int i0 = ((t >> (s - 1)) << s) + j, i1 = i0 + half;
-            P ur = re[i0], ui = im[i0], xr = re[i1], xi = im[i1];
-            fft_bfly(ur, ui, xr, xi, twr[j * tstride], sg * twi[j * tstride]);
-            re[i0] = ur;
-            im[i0] = ui;
-            re[i1] = xr;
-            im[i1] = xi;
+            P ur = re[sw(i0)], ui = im[sw(i0)], xr = re[sw(i1)], xi = im[sw(i1)];
+            fft_bfly(ur, ui, xr, xi, twr[twz(j * tstride)], sg * twi[twz(j * tstride)]);
+            re[sw(i0)] = ur;
+            im[sw(i0)] = ui;
+            re[sw(i1)] = xr;
+            im[sw(i1)] = xi;
         }
         __syncthreads();
     }
@@ -135,7 +150,7 @@ __device__ __forceinline__ void k_spec_forward_body(const SpecArgs<P>& a, const 
     const bool two = k1 < a.NK;
     load_twiddles(tw, a);
     for (int j = threadIdx.x; j < a.NX; j += blockDim.x) {
-        const int jr = bitrev(j, a.logN);
+        const int jr = sw(bitrev(j, a.logN));
         re[jr] = r[(size_t)k0 * a.pitch + j];
         im[jr] = two ? r[(size_t)k1 * a.pitch + j] : P(0);
     }
@@ -144,7 +159,7 @@ __device__ __forceinline__ void k_spec_forward_body(const SpecArgs<P>& a, const 
     const int N = a.NX;
     for (int m = threadIdx.x; m <= N / 2; m += blockDim.x) {
         const int mn = (N - m) & (N - 1);
-        const P zr = re[m], zi = im[m], nr = re[mn], ni = im[mn];
+        const P zr = re[sw(m)], zi = im[sw(m)], nr = re[sw(mn)], ni = im[sw(mn)];
         // X0 = (Z[m] + conj Z[N-m]) / 2,  X1 = (Z[m] - conj Z[N-m]) / 2i
         a.sre[(size_t)k0 * a.mpitch + m] = P(0.5) * (zr + nr);
         a.sim[(size_t)k0 * a.mpitch + m] = P(0.5) * (zi - ni);
@@ -311,7 +326,7 @@ __device__ __forceinline__ void k_spec_inverse_body(const SpecArgs<P>& a, P* out
             br = a.sre[(size_t)k1 * a.mpitch + m];
             bi = sg * a.sim[(size_t)k1 * a.mpitch + m];
         }
-        const int jr = bitrev(j, a.logN);
+        const int jr = sw(bitrev(j, a.logN));
         re[jr] = ar - bi;   // Z = X0 + i X1
         im[jr] = ai + br;
     }
@@ -319,8 +334,8 @@ __device__ __forceinline__ void k_spec_inverse_body(const SpecArgs<P>& a, P* out
     fft_shared(re, im, tw, a, true);
     const P scale = P(1) / P(N);
     for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        out[(size_t)k0 * a.pitch + j] = re[j] * scale;
-        if (two) out[(size_t)k1 * a.pitch + j] = im[j] * scale;
+        out[(size_t)k0 * a.pitch + j] = re[sw(j)] * scale;
+        if (two) out[(size_t)k1 * a.pitch + j] = im[sw(j)] * scale;
     }
 }
 template <typename P>
