@@ -1694,6 +1694,8 @@ struct vvm_gpu_ctx {
     cudaStream_t cap[2] = {};          // streams for capturing loop bodies
     cudaStream_t side = nullptr;       // the step's second chain (run_step)
     cudaEvent_t fork_ev[3] = {};       // its fork, meeting and join points
+    cudaStream_t xfer = nullptr;       // host copies of the prognostic transfers
+    cudaEvent_t xev[2][2] = {};        // per staging slot: [0] its copy done, [1] its layout kernel done
     bool branches = true;              // use them (off inside a batch: the cases are the branches)
     CGCtl* wctl = nullptr;             // outer loop state of the mixed solve
     long long* d_exec = nullptr;       // kernels executed inside graph loops
@@ -1728,6 +1730,10 @@ struct vvm_gpu_ctx {
         if (side) cudaStreamDestroy(side);
         for (auto e : fork_ev)
             if (e) cudaEventDestroy(e);
+        if (xfer) cudaStreamDestroy(xfer);
+        for (auto& row : xev)
+            for (auto e : row)
+                if (e) cudaEventDestroy(e);
         if (pcg64) pcg64->release();
         if (pcg32) pcg32->release();
         if (pcg_psi) pcg_psi->release();
@@ -3593,13 +3599,30 @@ int upload_prognostic_t(vvm_gpu_ctx* c, const vvm_gpu_host_state* s) {
     const double* req[] = {s->zeta, s->th, s->qv, s->qc, s->qr, s->u, s->w};
     for (const double* p : req)
         if (!p) return fail(c, VVM_GPU_EINVAL, "upload: prognostic field pointer is NULL");
-    upload_field<T>(c, s->zeta, 1, 0, F.zeta[now]);
-    upload_field<T>(c, s->th, 1, 0, F.th[now], c->offset_th());
-    upload_field<T>(c, s->qv, 1, 0, F.qv[now], c->offset_qv());
-    upload_field<T>(c, s->qc, 1, 0, F.qc[now]);
-    upload_field<T>(c, s->qr, 1, 0, F.qr[now]);
-    upload_field<T>(c, s->u, 1, 0, F.u);
-    upload_field<T>(c, s->w, 1, 0, F.w);
+    // the fields' copies back to back on the copy stream, two staging slots
+    // alternating, each slot's layout kernel on the context's stream: the
+    // link stays busy while the previous field is rearranged
+    struct { const double* h; T* dptr; const double* ref; } m[] = {
+        {s->zeta, F.zeta[now], nullptr}, {s->th, F.th[now], c->offset_th()}, {s->qv, F.qv[now], c->offset_qv()},
+        {s->qc, F.qc[now], nullptr}, {s->qr, F.qr[now], nullptr}, {s->u, F.u, nullptr}, {s->w, F.w, nullptr}};
+    const size_t n = (size_t)c->d.nx * c->d.nz;
+    const dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
+    // no copy into staging before the work already on the context's stream
+    // (which may read it) is done
+    CK(cudaEventRecord(c->xev[0][1], c->stream));
+    CK(cudaEventRecord(c->xev[1][1], c->stream));
+    for (int f = 0; f < 7; f++) {
+        const int slot = f & 1;
+        double* st = c->staging + slot * n;
+        CK(cudaStreamWaitEvent(c->xfer, c->xev[slot][1], 0));   // the slot's last reader is done
+        CK(cudaMemcpyAsync(st, m[f].h, n * sizeof(double), cudaMemcpyHostToDevice, c->xfer));
+        CK(cudaEventRecord(c->xev[slot][0], c->xfer));
+        CK(cudaStreamWaitEvent(c->stream, c->xev[slot][0], 0));
+        LAUNCH(&c->stats, VVM_K_MEAN, c->stream,
+               k_from_host_layout<T><<<g, b, 0, c->stream>>>(c->d, st, 1, 0, m[f].ref, m[f].dptr));
+        CKL();
+        CK(cudaEventRecord(c->xev[slot][1], c->stream));
+    }
     (void)fut;
     return VVM_GPU_OK;
 }
@@ -3840,8 +3863,29 @@ int download_prognostic_t(vvm_gpu_ctx* c, vvm_gpu_host_state* s) {
     struct { double* h; T* dptr; const double* ref; } m[] = {
         {s->zeta, F.zeta[now], nullptr}, {s->th, F.th[now], c->offset_th()}, {s->qv, F.qv[now], c->offset_qv()},
         {s->qc, F.qc[now], nullptr}, {s->qr, F.qr[now], nullptr}, {s->u, F.u, nullptr}, {s->w, F.w, nullptr}};
-    for (auto& e : m)
-        if (e.h) download_field<T>(c, e.dptr, 1, 0, e.h, false, e.ref);
+    // each field's layout kernel into one of two staging slots on the
+    // context's stream, its copy to the host on the copy stream: the link
+    // stays busy while the next field is rearranged; one wait at the end
+    const size_t n = (size_t)c->d.nx * c->d.nz;
+    const dim3 b(32, 8), g(cdiv(c->d.nx, 32), cdiv(c->d.nz, 8));
+    int f = 0;
+    for (auto& e : m) {
+        if (!e.h) continue;
+        const int slot = f++ & 1;
+        double* st = c->staging + slot * n;
+        CK(cudaStreamWaitEvent(c->stream, c->xev[slot][0], 0));   // the slot's last copy is done
+        LAUNCH(&c->stats, VVM_K_MEAN, c->stream,
+               k_to_host_layout<T><<<g, b, 0, c->stream>>>(c->d, e.dptr, 1, 0, e.ref, st));
+        CKL();
+        CK(cudaEventRecord(c->xev[slot][1], c->stream));
+        CK(cudaStreamWaitEvent(c->xfer, c->xev[slot][1], 0));
+        CK(cudaMemcpyAsync(e.h, st, n * sizeof(double), cudaMemcpyDeviceToHost, c->xfer));
+        CK(cudaEventRecord(c->xev[slot][0], c->xfer));
+    }
+    // later work on the context's stream may reuse the staging slots
+    CK(cudaEventRecord(c->xev[0][0], c->xfer));
+    CK(cudaStreamWaitEvent(c->stream, c->xev[0][0], 0));
+    CK(cudaStreamSynchronize(c->xfer));
     return VVM_GPU_OK;
 }
 
@@ -4052,6 +4096,9 @@ int vvm_gpu_create(const vvm_gpu_desc* desc, int device, vvm_gpu_ctx** out) {
         for (auto& cs : c->cap) CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
         for (auto& e : c->fork_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        CK(cudaStreamCreateWithFlags(&c->xfer, cudaStreamNonBlocking));
+        for (auto& row : c->xev)
+            for (auto& e : row) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     } catch (const CudaError& e) {
         cudaSetDevice(prev);
         return fail(nullptr, VVM_GPU_ECUDA, e.msg);
