@@ -3005,7 +3005,9 @@ int batch_fail(vvm_gpu_batch* b, int code, const std::string& msg) {
 //
 // Cases of one grid shape, precision and tuning whose step runs the exact
 // Fourier-mode cal_w and the tiled Gauss-Seidel passes step as grouped
-// launches (grouped.cuh): each case's step is recorded, the recordings are
+// launches (grouped.cuh), up to group_limit cases a group (small grids by
+// default, larger ones where the autotuner chose it): each case's step is
+// recorded, the recordings are
 // checked to agree op for op (kernel, launch shape, pack size, loop
 // structure), and then replayed side by side, one launch a kernel for the
 // whole group, blockIdx.z the case. Groups whose recordings differ step case
