@@ -135,7 +135,11 @@ int vvm_gpu_last_error(vvm_gpu_ctx* ctx, char* buf, size_t len);
 int vvm_gpu_upload_state(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st);
 int vvm_gpu_download_state(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st);
 /* Prognostic fields only (zeta, th, qv, qc, qr, u, w): the per-step traffic
- * of an output call. */
+ * of an output call. The copies run on the context's own copy stream, each
+ * field's copy beside the previous field's layout kernel. The upload returns
+ * once the work is queued (work on the context's stream that follows sees the
+ * fields; the host buffers must stay unchanged until then, as for any
+ * asynchronous copy); the download returns with the host buffers filled. */
 int vvm_gpu_upload_prognostic(vvm_gpu_ctx* ctx, const vvm_gpu_host_state* st);
 int vvm_gpu_download_prognostic(vvm_gpu_ctx* ctx, vvm_gpu_host_state* st);
 int vvm_gpu_set_step(vvm_gpu_ctx* ctx, int step);
