@@ -1997,9 +1997,11 @@ cudaGraph_t add_while(Stats* s, cudaStream_t st, cudaGraphConditionalHandle h) {
 struct BodyCapture {   // stream capture into a conditional node's body graph
     cudaStream_t s;
     Stats* stats = nullptr;   // recording: the loop's end is marked instead
+    bool active = false;      // capturing on s (not yet ended)
     BodyCapture(cudaStream_t s_, cudaGraph_t body, Stats* st = nullptr) : s(s_), stats(st) {
         if (stats && stats->rec) return;
         CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        active = true;
     }
     void end() {
         if (stats && stats->rec) {
@@ -2008,8 +2010,17 @@ struct BodyCapture {   // stream capture into a conditional node's body graph
             stats->rec->ops.push_back(std::move(op));
             return;
         }
+        active = false;
         cudaGraph_t g;
         CK(cudaStreamEndCapture(s, &g));
+    }
+    // An error between the start and end() leaves the stream out of capture
+    // mode again, so the context's capture streams stay usable.
+    ~BodyCapture() {
+        if (!active) return;
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        (void)cudaGetLastError();
     }
 };
 
